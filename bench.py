@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""MLS-MPM substep throughput on B200: particle-substeps/s, warm-started vs plain HB return.
+
+Workload (default): the large HB slump with the learned warm start — 256^3 grid (dx = 1/256 m),
+128^3-cell paste column at 8 particles per cell (16,777,216 particles, seed 2), config-0 paste
+(rho 1200, G 2e4, K 1e5, tau_y ~ U(20, 100) Pa per particle, K_s 5, n 0.5), sticky floor and
+slip walls, dt 1e-4, HB tolerance 1e-10.  A "step" is one substep attempt of the whole column
+(binning, P2G, wall traction, grid update, G2P + constitutive update, accept/commit).
+
+Timed protocol per arm: the column is first advanced `--develop` substeps (so that material
+yields and the Newton solve is exercised), a snapshot is taken, then plain and warm-started
+runs each do W untimed warm-up attempts and K timed attempts from the same snapshot, bracketed
+by stream synchronisation and CUDA events on the library's stream; multi-GPU runs are
+independent replicas (the path does not shard), timed as the max over ranks.  The state
+(2 x 2.4 GB) is larger than L2, so no flush is needed between steps.
+
+`--impl reference` times the reference algorithm (the FP64 CPU oracle restatement) on the host
+cores instead; rank 0 alone prints its line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "litter-physics_b200"))
+
+METRIC = "particle-substeps/s, warm-started vs plain HB MPM on 1 B200 at equal residual"
+UNIT = "particle-substeps/s"
+G2P_BYTES_PER_PARTICLE = 176.0  # algorithmic: 52 B read + 124 B written per particle-substep
+P2G_BYTES_PER_PARTICLE = 92.0   # algorithmic: x, v, C, tau(sym), m, V0 read
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def committed_traffic(kernel: str) -> dict | None:
+    """Per-particle DRAM bytes of a kernel from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return d.get(kernel)
+
+
+def time_steps(sim, steps: int, stream, torch) -> tuple[float, int]:
+    """Run `steps` attempts on `stream`; returns (ms, accepted substeps)."""
+    c0 = sim.counters.step_count
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    sim.run_substeps(steps)
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    sim.sync()
+    return start.elapsed_time(end), int(sim.counters.step_count - c0)
+
+
+def train_warm_start(torch, log_steps: int, epochs: int):
+    """Collect Newton pairs from the config-0 slump and a small slump, train on the device."""
+    import numpy as np
+
+    from litter_physics_b200 import configs, warmstart
+    from litter_physics_b200.sim import Simulation
+
+    t0 = time.perf_counter()
+    raws, sigmas = [], []
+    for spec in (configs.config0(), configs.slump(32, (8, 8, 16), seed=5, yield_range=(20.0, 100.0))):
+        s = Simulation(spec)
+        raw, sigma = warmstart.collect(s, log_steps, capacity=4_000_000)
+        raws.append(raw)
+        sigmas.append(sigma)
+        s.close()
+    raw = np.concatenate(raws)
+    sigma = np.concatenate(sigmas)
+    x, y = warmstart.dataset(raw, sigma)
+    t1 = time.perf_counter()
+    w, loss = warmstart.train(x, y, epochs=epochs, batch=4096, lr=2e-3)
+    t2 = time.perf_counter()
+    return w, {"pairs": int(len(y)), "epochs": epochs, "final_loss": loss, "collect_s": round(t1 - t0, 2),
+               "train_s": round(t2 - t1, 2)}
+
+
+def cpu_baseline_run(spec_fn, steps: int, threads: int) -> dict:
+    """The FP64 oracle (reference algorithm restated) on a bounded sample, all host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    spec = spec_fn()
+    sim = oracle.OracleSim(spec, threads=threads)
+    n = int(oracle.lib().ora_sim_particle_count(sim._h))
+    sim.advance_to(spec.max_dt)  # one untimed substep
+    t0 = time.perf_counter()
+    sim.advance_to((1 + steps) * spec.max_dt)
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "particles": n, "steps": steps, "seconds": dt}
+
+
+def reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    from litter_physics_b200 import configs
+
+    threads = len(os.sched_getaffinity(0))
+    sample = configs.slump(256, (32, 32, 32), seed=2, yield_range=(20.0, 100.0))
+    spec_fn = lambda: sample  # noqa: E731
+    for _ in range(args.warmup):
+        pass  # each oracle run builds its own state; the first substep inside is untimed
+    res = cpu_baseline_run(spec_fn, max(1, args.steps // 10), threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / res["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "large HB slump sample: config-2 grid spacing and material, 32^3-cell column "
+                               "(262,144 particles), FP64 oracle restatement of the reference step"},
+        "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{res['steps']} substeps x {res['particles']} particles after 1 untimed"},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+
+    from litter_physics_b200 import _lib, configs
+    from litter_physics_b200.sim import Simulation
+
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = dist_mod
+    _lib.build()
+    stream = torch.cuda.Stream()
+
+    weights, train_info = train_warm_start(torch, args.log_steps, args.epochs)
+    spec = configs.config2() if args.workload == "config2" else configs.config0()
+    t0 = time.perf_counter()
+    sim = Simulation(spec)
+    sim.set_stream(stream.cuda_stream)
+    sim.use_graph(args.graph)
+    n = sim.particle_count()
+    log(f"rank {rank}: {n} particles, setup {time.perf_counter() - t0:.1f}s")
+    # develop the column so that material yields
+    sim.run_substeps(args.develop)
+    sim.sync()
+    snap = sim.particles()
+    led, cnt = sim.ledger, sim.counters
+
+    def restore():
+        sim.set_particles(snap)
+        sim.set_ledger(led)
+        sim.set_counters(cnt)
+
+    results = {}
+    clocks = None
+    launches = {}
+    for arm in ("plain", "warm"):
+        restore()
+        sim.set_warm_start(weights if arm == "warm" else None)
+        sim.use_graph(args.graph)
+        sim.run_substeps(args.warmup)
+        sim.sync()
+        it0 = sim.counters.newton_iterations
+        if dist is not None:
+            dist.barrier()
+        sampler = ClockSampler(local) if arm == "warm" else None
+        if sampler:
+            sampler.start()
+        l0 = _lib.kernel_launches()
+        ms, accepted = time_steps(sim, args.steps, stream, torch)
+        launches[arm] = _lib.kernel_launches() - l0
+        if sampler:
+            clocks = sampler.stop()
+        it1 = sim.counters.newton_iterations
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        results[arm] = {"ms": ms, "accepted": accepted, "newton_iterations": int(it1 - it0),
+                        "value": ws * n * accepted / (ms / 1e3)}
+    # per-kernel live timing (CUDA events on the same stream), warm arm
+    ktimes = sim.kernel_times(args.kernel_steps)
+    # end to end through the C ABI with host buffers: import -> advance -> export
+    restore()
+    sim.set_warm_start(weights)
+    e2e_steps = args.e2e_steps
+    bytes_in = sum(v.nbytes for v in snap.values())
+    torch.cuda.synchronize()
+    te0 = time.perf_counter()
+    sim.set_particles(snap)
+    t_target = sim.time + e2e_steps * spec.max_dt
+    sim.advance_to(t_target)
+    out = sim.particles()
+    te1 = time.perf_counter()
+    steps_done = e2e_steps
+    bytes_out = sum(v.nbytes for v in out.values())
+    e2e_value = ws * n * steps_done / (te1 - te0)
+    if dist is not None:
+        t = torch.tensor([te1 - te0], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = ws * n * steps_done / float(t.item())
+        dist.barrier()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    peaks = measured_peaks()
+    g2p_ms = ktimes.get("k_g2p", float("nan"))
+    achieved = G2P_BYTES_PER_PARTICLE * n / (g2p_ms / 1e3) / 1e9
+    traffic = committed_traffic("k_g2p")
+    threads = len(os.sched_getaffinity(0))
+    cpu = cpu_baseline_run(lambda: configs.slump(256, (32, 32, 32), seed=2, yield_range=(20.0, 100.0)), 2, threads)
+    warm, plain = results["warm"], results["plain"]
+    line = {
+        "metric": METRIC,
+        "value": warm["value"],
+        "unit": UNIT,
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": warm["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "large HB slump, warm-started (config 2): 256^3 grid, 128^3-cell column, "
+                        f"{n} particles, tau_y U(20,100) Pa per particle, dt 1e-4, HB tol 1e-10",
+            "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+            "develop_substeps": args.develop,
+            "l2": "state (2 x 2.4 GB) larger than L2; no flush",
+            "precision": "f32 particle/grid arithmetic, f64 HB Newton and ledgers, int64 fixed-point grid sums",
+        },
+        "plain": {"value": plain["value"], "ms_per_step": plain["ms"] / args.steps,
+                  "newton_iterations_per_step": plain["newton_iterations"] / max(plain["accepted"], 1)},
+        "warm": {"newton_iterations_per_step": warm["newton_iterations"] / max(warm["accepted"], 1),
+                 "mlp": train_info},
+        "warm_over_plain": warm["value"] / plain["value"],
+        "kernel_ms": {k: round(v, 5) for k, v in ktimes.items()},
+        "roofline": {"kernel": "k_g2p", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "peak_source": peaks["source"],
+                     "algorithmic_bytes_per_particle": G2P_BYTES_PER_PARTICLE,
+                     "traffic": (traffic["bytes_per_particle"] * n if traffic else None)},
+        "cpu_baseline": {"value": cpu["value"], "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"FP64 oracle, 32^3-cell column at config-2 resolution ({cpu['particles']} "
+                                   f"particles), {cpu['steps']} substeps after 1 untimed"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_in / steps_done,
+                "d2h_bytes_per_step": bytes_out / steps_done,
+                "path": "lp_sim_import_particles -> lp_sim_advance -> lp_sim_export_particles (host FP64 buffers)",
+                "steps": steps_done},
+        "gpu_launches": int(launches["warm"]),
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config0"])
+    ap.add_argument("--develop", type=int, default=150)
+    ap.add_argument("--graph", type=int, default=0)
+    ap.add_argument("--log-steps", type=int, default=300)
+    ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--kernel-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    ws, rank, local = dist_info()
+    if args.impl == "reference":
+        reference_arm(args, ws, rank)
+        return
+    ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -169,6 +169,9 @@ int32_t lp_abi_version(void);
 const char* lp_last_error(void);
 /* Number of CUDA kernels this library launched since load (for launch accounting). */
 uint64_t lp_kernel_launches(void);
+/* sizeof of lp_material, lp_fixture_spec, lp_ledger, lp_counters, lp_particles, lp_pellet
+ * (lets bindings check their struct mirrors without a GPU). */
+void lp_abi_struct_sizes(uint64_t out[6]);
 
 /* ---------------- materials (constitutive.rs:146-243) ---------------- */
 lp_material lp_material_paste(double density, double young_modulus, double poisson_ratio,
@@ -215,6 +218,14 @@ lp_status lp_sim_observables(lp_sim* sim, char* names, double* values, int32_t c
 lp_status lp_sim_energies(lp_sim* sim, double out[9]);
 /* Enable the learned Newton warm start (weights from lp_mlp_*); 0 disables. */
 lp_status lp_sim_set_warm_start(lp_sim* sim, const float* weights, int32_t nweights, int32_t enable);
+/* Conservation probe: scatter the committed state to the grid with step dt (P2G only) and
+ * return out[0] = grid mass, out[1..3] = grid momentum (exact fixed-point sums over nodes),
+ * out[4] = particle mass, out[5..7] = particle momentum (FP64 sums); the grid is then cleared. */
+lp_status lp_sim_grid_totals(lp_sim* sim, double dt, double out[8]);
+/* Time `steps` attempts kernel by kernel with CUDA events on the simulation's stream:
+ * ms[k] = mean duration of kernel k, names = 32-char slots; *count = kernels per attempt. */
+lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* names, int32_t capacity,
+                              int32_t* count);
 /* Capture run_substeps into a CUDA graph of `steps` attempts (0 disables graphs). */
 lp_status lp_sim_use_graph(lp_sim* sim, int32_t steps);
 

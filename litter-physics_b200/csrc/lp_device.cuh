@@ -1,0 +1,481 @@
+// lp_device.cuh - device data layout and per-particle constitutive math of the B200 MLS-MPM step.
+//
+// Layout (one "ensemble" = one or more independent simulations, "instances"):
+//   * particle state: FP32 structure of arrays, component-major (component c of slot s at
+//     state[c * cap + s]); two buffers (current / trial) selected per instance by a parity bit
+//     so a rejected trial never touches the committed state (solver.rs:11-14);
+//   * grid: dense padded node arrays per instance (grid.rs:71, n+3 nodes per axis):
+//     int64 fixed-point mass / momentum accumulators, int64 wall-reaction accumulators split by
+//     face side, and a float4 (velocity, mass) array written by the grid update;
+//   * bins: particles are counting-sorted every attempt by their stencil base cell
+//     (floor(x/dx - 0.5) + 1 per axis), bins grouped in tiles of TX x TY x TZ so that one
+//     CTA of the scatter owns one tile and its (TX+2)(TY+2)(TZ+2)-node halo.
+//
+// Precision: particle and grid arithmetic in FP32.  The deformation gradient is stored as
+// H = F - I and the liquid volume ratio as J - 1, so that near-identity strains keep full FP32
+// relative precision.  The Herschel-Bulkley scalar return runs in FP64, and so do the ledger
+// reductions.  Grid mass/momentum accumulate as exact int64 fixed-point sums (order
+// independent, hence deterministic).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lp_mlp.cuh"
+
+namespace lp {
+
+// ---------------------------------------------------------------- tiling constants
+constexpr int TX = 4, TY = 4, TZ = 8;            // bins per tile
+constexpr int TB = TX * TY * TZ;                 // 128 bins per tile
+constexpr int HX = TX + 2, HY = TY + 2, HZ = TZ + 2;
+constexpr int HN = HX * HY * HZ;                 // 360 halo nodes per tile
+constexpr int P2G_THREADS = 3 * TB;              // 3 slab threads per bin
+constexpr int NB = 4;                            // node block edge (grid update / activity)
+constexpr int GU_BLOCKS_PER_CTA = 4;             // node blocks per grid-update CTA
+constexpr int GU_THREADS = NB * NB * NB * GU_BLOCKS_PER_CTA;  // 256
+constexpr int G2P_THREADS = 256;
+constexpr int SLOT_ALIGN = G2P_THREADS;          // instance slot ranges are aligned to this
+constexpr int KEY_CHUNK = 1024;                  // scan chunk; instance key ranges aligned to it
+
+// state components (component-major)
+enum Comp : int {
+  C_X = 0,    // 3
+  C_V = 3,    // 3
+  C_C = 6,    // 9 (row-major)
+  C_H = 15,   // 9 (F - I, row-major)
+  C_TAU = 24, // 6: xx yy zz xy xz yz
+  C_EP = 30,
+  C_M = 31,
+  C_V0 = 32,
+  C_YS = 33,
+  C_JM1 = 34,
+  NCOMP = 35
+};
+
+// failure codes (worst wins)
+enum Fail : int {
+  F_OK = 0,
+  F_CONST_INVERTED = 1,
+  F_CONST_EIGEN = 2,
+  F_CONST_STRETCH = 3,
+  F_CONST_NOT_CONVERGED = 4,
+  F_CONST_NONFINITE = 5,
+  F_GRID_NONFINITE = 6,
+  F_DISPLACEMENT = 7,
+  F_PELLET_NONFINITE = 8,
+  F_TRACTION_NONFINITE = 9,
+  F_OUTFLOW = 10
+};
+
+enum Status : int { S_RUNNING = 0, S_REACHED = 1, S_MIN_STEP = 2, S_ERROR = 3 };
+
+// per-instance constants (set at creation)
+struct InstDesc {
+  double dx, inv_dx;
+  int cells[3], nodes[3];
+  int bins[3], tiles[3];
+  int nblk[3];
+  int kind;  // 0 paste, 1 liquid
+  int per_particle_yield;
+  int face_mode;
+  int has_pellet;
+  int64_t node_off;   // first node of this instance in the global node arrays
+  int64_t tile_off;   // first global tile
+  int64_t key_off;    // first global bin key (= tile_off * TB)
+  int64_t nkeys;      // keys incl. the trailing outflow key, aligned to KEY_CHUNK
+  int64_t blk_off;    // first global node block
+  int64_t gcta_off, gcta_cnt;  // grid-update CTAs
+  int64_t slot_off, slot_cap;  // particle slots
+  int64_t pcta_off, pcta_cnt;  // G2P CTAs
+  // material (constitutive.rs:111-131), FP64 master copy
+  double density, mu, lambda, bulk, yield, consistency, flow_index, tait_gamma;
+  // config (solver.rs:48-62)
+  double gravity[3];
+  double friction;
+  double face_mu[6];
+  int face_sticky[6];
+  double cfl, max_dt, min_dt, tol;
+  double contact_k, contact_e, contact_mu;
+  double extent[3];
+  double s_mass;  // fixed-point scale of node mass
+};
+
+// pellet state (rigid.rs:30-49), FP64
+struct PelletState {
+  double radius, length, mass;
+  double inertia[3];
+  double pos[3];
+  double q[4];  // i j k w
+  double vel[3];
+  double L[3];
+  int nsph;
+  int pad;
+  double off[64];
+};
+
+// FP64 ledger, same order as lp_ledger
+struct LedgerD {
+  double initial_mass, outflow_mass, initial_momentum[3], initial_mech, gravity_impulse[3], wall_impulse[3],
+      pellet_wall_impulse[3], coupling_impulse[3], coupling_angular[3], proj, fric, trac, pellet_work, cgrid,
+      cpellet, plastic, outflow_momentum[3];
+};
+
+// per-instance mutable control block (device resident)
+struct Control {
+  double time, target;
+  double dt, dt_scale, limit;
+  double forced_dt;      // > 0: lp_sim_try_step mode (exact dt, no control)
+  double max_speed;      // of the committed state
+  double bbound;         // momentum bound of the committed state (for the fixed-point scale)
+  double s_mom;          // fixed-point scale of node momentum for the current attempt
+  double total_mass;     // FP64 sum of particle masses
+  double min_dt_used, max_dt_used;
+  uint64_t step_count, limited_steps, rejected_steps;
+  uint64_t newton_iterations, yielded;
+  int active, status, limited, parity;
+  int fail, last_fail, epoch, pad;
+  int64_t count;         // particle count
+  int64_t outflow;       // particles detected outside the padded grid this attempt
+  double fail_value;
+  LedgerD ledger;
+  PelletState pellet, pellet_trial;
+  // pellet-step results of the current attempt
+  double c_impulse[3], c_angular[3], c_grid_energy, c_pellet_energy, pw_impulse[3], pw_work;
+  int pellet_fail, warm_start;
+};
+
+// partial results of one grid-update CTA
+struct GridPartial {
+  double wall_impulse[3];
+  double proj, fric, trac;
+  int fail;
+  int pad;
+};
+// partial results of one G2P CTA
+struct ParticlePartial {
+  double diss, bbound, mass;
+  float max_speed, max_disp;
+  int fail;
+  int iterations;
+  int yielded;
+  int pad;
+  double fail_value;
+};
+
+// ---------------------------------------------------------------- small helpers
+__device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+
+// fixed-point conversion of an FP64 value (round to nearest)
+__device__ __forceinline__ long long to_fixed(double v, double scale) { return __double2ll_rn(v * scale); }
+
+__device__ __forceinline__ void atomic_add_ll(long long* p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+}
+
+// ---------------------------------------------------------------- HB scalar return (FP64)
+// Bracketed Newton of constitutive.rs:280-362, with an optional start value sigma0 in
+// (yield, trial) (the learned warm start); the plain solver starts at the midpoint.
+// Returns failure code; iterations through *iters.
+__device__ inline int hb_return_d(double trial, double ys, double k, double n, double mu, double dt, double tol_rel,
+                                  double sigma0, double* sigma_out, double* dep_out, int* iters) {
+  *iters = 0;
+  if (!(isfinite(trial) && isfinite(ys) && isfinite(k) && isfinite(n) && isfinite(mu) && isfinite(dt)))
+    return F_CONST_NONFINITE;
+  const double viscous_scale = 3.0 * mu * dt;
+  if (trial <= ys) {
+    *sigma_out = trial;
+    *dep_out = 0.0;
+    return F_OK;
+  }
+  if (k <= 0.0) {
+    *sigma_out = ys;
+    *dep_out = (trial - ys) / (3.0 * mu);
+    return F_OK;
+  }
+  const double exponent = 1.0 / n;
+  double lower = ys, upper = trial;
+  double sigma = (sigma0 > lower && sigma0 < upper) ? sigma0 : 0.5 * (lower + upper);
+  const double tolerance = tol_rel * fmax(trial, 1.0);
+  double over = fmax((sigma - ys) / k, 0.0);
+  double last = sigma - trial + viscous_scale * pow(over, exponent);
+  for (int it = 1; it <= 200; ++it) {
+    if (fabs(last) <= tolerance || (upper - lower) <= tolerance) {
+      *sigma_out = sigma;
+      *dep_out = (trial - sigma) / (3.0 * mu);
+      *iters = it;
+      return F_OK;
+    }
+    if (last > 0.0) upper = sigma;
+    else lower = sigma;
+    over = fmax((sigma - ys) / k, 0.0);
+    double newton;
+    if (over > 0.0) {
+      double derivative = 1.0 + viscous_scale * exponent * pow(over, exponent - 1.0) / k;
+      newton = sigma - last / derivative;
+    } else {
+      newton = sigma;  // infinite derivative: the reference's Newton step is a no-op here
+    }
+    sigma = (isfinite(newton) && newton > lower && newton < upper) ? newton : 0.5 * (lower + upper);
+    over = fmax((sigma - ys) / k, 0.0);
+    last = sigma - trial + viscous_scale * pow(over, exponent);
+    if (!isfinite(last)) {
+      *iters = it;
+      return F_CONST_NONFINITE;
+    }
+  }
+  *iters = 200;
+  return F_CONST_NOT_CONVERGED;
+}
+
+// ---------------------------------------------------------------- symmetric 3x3 eigen (Jacobi)
+// Cyclic Jacobi as constitutive.rs:373-425; FP32 version with an FP32-appropriate stopping
+// rule, FP64 version with the reference's rule (used when FP32 stalls).
+template <typename T>
+__device__ inline bool jacobi3(T d[3][3], T v[3][3], int max_sweeps, T tol) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) v[i][j] = (i == j) ? T(1) : T(0);
+  T scale = T(0);
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) scale += d[i][j] * d[i][j];
+  const int P[3] = {0, 0, 1}, Q[3] = {1, 2, 2};
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    T off = d[0][1] * d[0][1] + d[0][2] * d[0][2] + d[1][2] * d[1][2];
+    if (off <= tol * scale) return true;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int p = P[r], q = Q[r];
+      T apq = d[p][q];
+      if (apq == T(0)) continue;
+      T theta = (d[q][q] - d[p][p]) / (T(2) * apq);
+      T at = theta < T(0) ? -theta : theta;
+      T sgn = signbit(theta) ? T(-1) : T(1);
+      T tangent = at > T(1e18) ? sgn / (T(2) * at) : sgn / (at + sqrt(theta * theta + T(1)));
+      T c = T(1) / sqrt(tangent * tangent + T(1));
+      T s = tangent * c;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        T akp = d[k][p], akq = d[k][q];
+        d[k][p] = c * akp - s * akq;
+        d[k][q] = s * akp + c * akq;
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        T apk = d[p][k], aqk = d[q][k];
+        d[p][k] = c * apk - s * aqk;
+        d[q][k] = s * apk + c * aqk;
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        T vkp = v[k][p], vkq = v[k][q];
+        v[k][p] = c * vkp - s * vkq;
+        v[k][q] = s * vkp + c * vkq;
+      }
+    }
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------- paste update (H = F - I)
+// update_paste of constitutive.rs:456-531 rewritten on the displacement gradient:
+//   H_tr = H + dt C + dt C H            (F_tr = (I + dt C) F)
+//   B    = H_tr + H_tr^T + H_tr H_tr^T  (b - I, b = F_tr F_tr^T)
+//   eps_i = log1p(beta_i) / 2           (Hencky strain from the eigenvalues beta of B)
+//   F_new = U diag(exp(eps_new - eps)) U^T F_tr  ->  H_new = H_tr + U diag(expm1(delta)) U^T (I + H_tr)
+// Identical mathematics, FP32 rounding kept relative to the strain rather than to 1.
+struct PasteOut {
+  float H[9];
+  float tau[6];
+  double dep, diss_density, eq, trial;
+  int iters;
+  int fail;
+  int yielded;
+};
+
+// warm_w: learned warm-start weights (null: the reference's midpoint start)
+__device__ inline void paste_update(const float Htr[9], float mu, float lambda, double mu_d, double ys, double k,
+                                    double n, double dt, double tol, const float* warm_w, PasteOut& o) {
+  o.fail = F_OK;
+  o.iters = 0;
+  o.yielded = 0;
+  o.dep = 0.0;
+  o.diss_density = 0.0;
+  // det(I + H_tr) > 0
+  const float f00 = 1.f + Htr[0], f01 = Htr[1], f02 = Htr[2];
+  const float f10 = Htr[3], f11 = 1.f + Htr[4], f12 = Htr[5];
+  const float f20 = Htr[6], f21 = Htr[7], f22 = 1.f + Htr[8];
+  const float det = f00 * (f11 * f22 - f21 * f12) - f01 * (f10 * f22 - f20 * f12) + f02 * (f10 * f21 - f20 * f11);
+  if (!isfinite(det)) {
+    o.fail = F_CONST_NONFINITE;
+    return;
+  }
+  if (det <= 0.f) {
+    o.fail = F_CONST_INVERTED;
+    return;
+  }
+  // B = H + H^T + H H^T
+  float B[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float hh = Htr[3 * i + 0] * Htr[3 * j + 0] + Htr[3 * i + 1] * Htr[3 * j + 1] + Htr[3 * i + 2] * Htr[3 * j + 2];
+      B[i][j] = Htr[3 * i + j] + Htr[3 * j + i] + hh;
+    }
+  float U[3][3];
+  float beta[3];
+  {
+    float d[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) d[i][j] = 0.5f * (B[i][j] + B[j][i]);
+    bool ok = jacobi3<float>(d, U, 12, 1e-13f);
+    if (ok) {
+      beta[0] = d[0][0];
+      beta[1] = d[1][1];
+      beta[2] = d[2][2];
+    } else {
+      double dd[3][3], uu[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) dd[i][j] = 0.5 * ((double)B[i][j] + (double)B[j][i]);
+      if (!jacobi3<double>(dd, uu, 64, 1e-30)) {
+        o.fail = F_CONST_EIGEN;
+        return;
+      }
+      for (int i = 0; i < 3; ++i) {
+        beta[i] = (float)dd[i][i];
+        for (int j = 0; j < 3; ++j) U[i][j] = (float)uu[i][j];
+      }
+    }
+  }
+  float eps[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float lam = 1.f + beta[a];  // squared stretch
+    if (!isfinite(beta[a]) || !(lam >= 1e-12f)) {
+      o.fail = F_CONST_STRETCH;
+      return;
+    }
+    eps[a] = 0.5f * log1pf(beta[a]);
+  }
+  const float vol = eps[0] + eps[1] + eps[2];
+  const float mean = vol / 3.f;
+  float dev[3] = {eps[0] - mean, eps[1] - mean, eps[2] - mean};
+  const float dnorm = sqrtf(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  const double trial_eq = 1.2247448713915890 * 2.0 * mu_d * (double)dnorm;  // sqrt(3/2) 2 mu |dev|
+  double scale = 1.0;
+  o.eq = trial_eq;
+  o.trial = trial_eq;
+  if (trial_eq > ys && dnorm > 0.f) {
+    double sigma, dep;
+    int iters;
+    double sigma0 = -1.0;
+    if (warm_w != nullptr) {
+      const double frac = warm_fraction(warm_w, trial_eq, ys, k, n, mu_d, dt);
+      if (frac > 0.0) sigma0 = ys + frac * (trial_eq - ys);
+    }
+    int e = hb_return_d(trial_eq, ys, k, n, mu_d, dt, tol, sigma0, &sigma, &dep, &iters);
+    o.iters = iters;
+    if (e != F_OK) {
+      o.fail = e;
+      return;
+    }
+    scale = sigma / trial_eq;
+    o.dep = dep;
+    o.eq = sigma;
+    o.yielded = 1;
+  }
+  const float sc = (float)scale;
+  float eps_new[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) eps_new[a] = dev[a] * sc + mean;
+  // Kirchhoff stress tau = U diag(2 mu eps_new + lambda vol) U^T
+  float ps[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) ps[a] = eps_new[a] * (2.f * mu) + lambda * vol;
+  float T[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) T[i][j] = U[i][0] * ps[0] * U[j][0] + U[i][1] * ps[1] * U[j][1] + U[i][2] * ps[2] * U[j][2];
+  o.tau[0] = T[0][0];
+  o.tau[1] = T[1][1];
+  o.tau[2] = T[2][2];
+  o.tau[3] = 0.5f * (T[0][1] + T[1][0]);
+  o.tau[4] = 0.5f * (T[0][2] + T[2][0]);
+  o.tau[5] = 0.5f * (T[1][2] + T[2][1]);
+  for (int i = 0; i < 6; ++i)
+    if (!isfinite(o.tau[i])) {
+      o.fail = F_CONST_NONFINITE;
+      return;
+    }
+  if (o.yielded) {
+    // H_new = H_tr + U diag(expm1(delta)) U^T (I + H_tr), delta = dev (scale - 1)
+    float r[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r[a] = expm1f(dev[a] * (sc - 1.f));
+    float M[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) M[i][j] = U[i][0] * r[0] * U[j][0] + U[i][1] * r[1] * U[j][1] + U[i][2] * r[2] * U[j][2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        float s = M[i][j] + (M[i][0] * Htr[0 * 3 + j] + M[i][1] * Htr[1 * 3 + j] + M[i][2] * Htr[2 * 3 + j]);
+        o.H[3 * i + j] = Htr[3 * i + j] + s;
+      }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) o.H[i] = Htr[i];
+  }
+  o.diss_density = o.eq * o.dep;
+}
+
+// ---------------------------------------------------------------- liquid update (J - 1)
+// update_liquid of constitutive.rs:557-589 on jm1 = J - 1, plus the Tait EOS extension
+// p = (K/gamma) (J^-gamma - 1) (gamma == 1 is the reference's K (1/J - 1)).
+struct LiquidOut {
+  float jm1;
+  float tau[6];
+  float pressure;
+  int fail;
+};
+__device__ inline void liquid_update(float jm1, const float C[9], float bulk, float visc, float gamma, float dt,
+                                     LiquidOut& o) {
+  o.fail = F_OK;
+  const float tr = C[0] + C[4] + C[8];
+  const float g = dt * tr;
+  const float nj = jm1 + g + jm1 * g;  // (1 + jm1)(1 + g) - 1
+  const float J = 1.f + nj;
+  if (!isfinite(nj)) {
+    o.fail = F_CONST_NONFINITE;
+    return;
+  }
+  if (J <= 1e-6f) {
+    o.fail = F_CONST_INVERTED;
+    return;
+  }
+  float p;
+  if (gamma == 1.f) p = -bulk * nj / J;
+  else p = bulk / gamma * expm1f(-gamma * log1pf(nj));
+  const float third = (C[0] + C[4] + C[8]) / 3.f;
+  const float s = 2.f * visc * J;
+  o.tau[0] = -p * J + s * (C[0] - third);
+  o.tau[1] = -p * J + s * (C[4] - third);
+  o.tau[2] = -p * J + s * (C[8] - third);
+  o.tau[3] = s * 0.5f * (C[1] + C[3]);
+  o.tau[4] = s * 0.5f * (C[2] + C[6]);
+  o.tau[5] = s * 0.5f * (C[5] + C[7]);
+  for (int i = 0; i < 6; ++i)
+    if (!isfinite(o.tau[i])) {
+      o.fail = F_CONST_NONFINITE;
+      return;
+    }
+  o.jm1 = nj;
+  o.pressure = p;
+}
+
+}  // namespace lp

@@ -1,0 +1,1536 @@
+// lp_host.cu - host runtime and C ABI (include/lp_mpm.h) of the B200 MLS-MPM substep.
+//
+// The runtime owns every device buffer of an "ensemble" (one simulation, or a batch of
+// independent simulations sharing one launch sequence), builds fixtures (setup only, host FP64
+// restatement of fixtures.rs:272-349 so that GPU and reference start from identical seeded
+// inputs), drives advance_while's loop in chunks of device-controlled attempts (optionally
+// replayed from a CUDA graph), and converts state to and from the reference's FP64 particle
+// layout at the boundary.  It never computes a substep on the host: without a CUDA device every
+// entry point that needs one fails with LP_DEVICE.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/lp_mpm.h"
+#include "lp_kernels.h"
+
+using lp::Control;
+using lp::InstDesc;
+
+namespace {
+
+thread_local std::string g_err;
+
+lp_status set_error(lp_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+#define CUDA_CK(expr)                                                                                   \
+  do {                                                                                                  \
+    cudaError_t _e = (expr);                                                                            \
+    if (_e != cudaSuccess) return set_error(LP_DEVICE, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+constexpr double kPi = 3.14159265358979323846;
+
+// ---------------------------------------------------------------- SplitMix64 (rng.rs:35-47)
+struct SplitMix64 {
+  uint64_t state;
+  uint64_t next_u64() {
+    state += 0x9E3779B97F4A7C15ull;
+    uint64_t z = state;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  }
+  double next_unit() { return (double)(next_u64() >> 11) * (1.0 / (double)(1ull << 53)); }
+};
+
+// ---------------------------------------------------------------- host fixture
+struct HostParticles {
+  std::vector<double> x, v, H, tau;  // 3, 3, 9 (F - I), 9 per particle
+  std::vector<double> jm1, m, V0, ys;
+  std::vector<uint32_t> id;
+  size_t size() const { return id.size(); }
+};
+
+struct HostInstance {
+  lp_fixture_spec spec;
+  int64_t cells[3], nodes[3];
+  HostParticles P;
+  bool has_pellet = false;
+  lp::PelletState pellet;
+};
+
+int64_t axis_count(double size, double spacing) {
+  double sub = spacing / 2.0;
+  return (int64_t)std::fmax(std::round(size / sub), 1.0);
+}
+
+// grid.rs:105-154
+lp_status make_layout(const lp_fixture_spec& s, HostInstance& h) {
+  if (!(std::isfinite(s.grid_spacing) && s.grid_spacing > 0.0))
+    return set_error(LP_INVALID, "`grid_spacing_m` must be positive and finite");
+  double total = 1.0;
+  for (int a = 0; a < 3; ++a) {
+    double extent = s.domain[a];
+    if (!(std::isfinite(extent) && extent > 0.0)) return set_error(LP_INVALID, "`domain_m` must be positive and finite");
+    double ratio = extent / s.grid_spacing, rounded = std::round(ratio);
+    if (!std::isfinite(ratio) || rounded > 4294967295.0)
+      return set_error(LP_INVALID, "grid axis exceeds the node allocation cap");
+    if (std::fabs(ratio - rounded) > 1e-6 * std::fmax(rounded, 1.0))
+      return set_error(LP_INVALID, "`domain_m` is not an integer multiple of `grid_spacing_m`");
+    if (rounded < 2.0) return set_error(LP_INVALID, "`domain_m` must span at least two cells");
+    h.cells[a] = (int64_t)rounded;
+    h.nodes[a] = h.cells[a] + 3;
+    total *= (double)h.nodes[a];
+  }
+  if (total > (double)s.max_nodes) return set_error(LP_INVALID, "grid would allocate too many nodes, exceeding the cap");
+  return LP_OK;
+}
+
+// fixtures.rs:152-229
+lp_status validate_spec(const lp_fixture_spec& s) {
+  for (int a = 0; a < 3; ++a) {
+    if (s.initial_size[a] > s.domain[a] + 1e-12) return set_error(LP_INVALID, "`initial_size_m` exceeds `domain_m`");
+    if (s.initial_size[a] < s.grid_spacing) return set_error(LP_INVALID, "`initial_size_m` must span at least one cell");
+  }
+  double count = 1.0;
+  for (int a = 0; a < 3; ++a) count *= (double)axis_count(s.initial_size[a], s.grid_spacing);
+  if (count > (double)s.max_particles)
+    return set_error(LP_INVALID, "fixture would allocate too many particles, exceeding the cap");
+  if (count > 2147483647.0) return set_error(LP_INVALID, "particle count exceeds the 32-bit slot range");
+  const double m = s.material.kind;
+  if (m != LP_PASTE && m != LP_LIQUID) return set_error(LP_INVALID, "unknown material kind");
+  switch (s.fixture) {
+    case LP_HYDROSTATIC: {
+      for (int a = 0; a < 2; ++a)
+        if (std::fabs(s.initial_size[a] - s.domain[a]) > 1e-9)
+          return set_error(LP_INVALID,
+                           "`hydrostatic` requires `initial_size_m` to equal `domain_m` so the column spans the domain");
+      double v2 = 0;
+      for (int a = 0; a < 3; ++a) v2 += s.initial_velocity[a] * s.initial_velocity[a];
+      if (v2 > 0.0) return set_error(LP_INVALID, "`hydrostatic` requires zero `initial_velocity_m_s`");
+      if (s.initial_size[2] >= s.domain[2]) return set_error(LP_INVALID, "`hydrostatic` requires free space above the column");
+      if (s.material.kind == LP_LIQUID && s.material.tait_gamma != 0.0 && s.material.tait_gamma != 1.0)
+        return set_error(LP_UNSUPPORTED, "`hydrostatic` prestress is defined for the linear EOS only");
+      break;
+    }
+    case LP_COUPLED_PATCH: {
+      if (!s.has_pellet) return set_error(LP_INVALID, "`coupled_patch` requires exactly one box supplying pellet geometry");
+      if (s.material.kind != LP_PASTE) return set_error(LP_INVALID, "`coupled_patch` is implemented for `paste` only");
+      if (s.pellet_radius < 1.5 * s.grid_spacing) return set_error(LP_INVALID, "`pellet_radius_m` is under-resolved");
+      double top = s.initial_size[2] + 2.0 * s.grid_spacing + 2.0 * s.pellet_radius;
+      if (top > s.domain[2] || s.pellet_length > s.domain[0] || 2.0 * s.pellet_radius > s.domain[1])
+        return set_error(LP_INVALID, "`coupled_patch` pellet does not fit above the block inside `domain_m`");
+      break;
+    }
+    case LP_SLUMP:
+    case LP_DAM_BREAK:
+      if (s.has_pellet)
+        return set_error(LP_INVALID, "fixture does not accept boxes; only `coupled_patch` uses pellet geometry");
+      break;
+    default:
+      return set_error(LP_INVALID, "unknown fixture");
+  }
+  return LP_OK;
+}
+
+// rigid.rs:115-182
+lp_status make_pellet(double r, double len, double rho, const double pos[3], lp::PelletState& p) {
+  if (!(std::isfinite(r) && r > 0.0)) return set_error(LP_INVALID, "pellet radius must be positive");
+  if (!(std::isfinite(len) && len >= 2.0 * r)) return set_error(LP_INVALID, "pellet length must be at least twice the radius");
+  if (!(std::isfinite(rho) && rho > 0.0)) return set_error(LP_INVALID, "pellet density must be positive");
+  std::memset(&p, 0, sizeof(p));
+  p.radius = r;
+  p.length = len;
+  p.mass = rho * kPi * r * r * len;
+  p.inertia[0] = 0.5 * p.mass * r * r;
+  p.inertia[1] = p.mass * (3.0 * r * r + len * len) / 12.0;
+  p.inertia[2] = p.inertia[1];
+  for (int a = 0; a < 3; ++a) p.pos[a] = pos[a];
+  p.q[3] = 1.0;
+  double hs = 0.5 * len - r;
+  int count = 1;
+  if (hs > 0.0) {
+    double ratio = std::ceil(2.0 * hs / r);
+    if (!std::isfinite(ratio) || ratio > 63.0) return set_error(LP_INVALID, "pellet proxy exceeds the sphere cap");
+    count = (int)ratio + 1;
+  }
+  p.nsph = count;
+  for (int i = 0; i < count; ++i) p.off[i] = count == 1 ? 0.0 : -hs + 2.0 * hs * (double)i / (double)(count - 1);
+  return LP_OK;
+}
+
+// fixtures.rs:238-349 (placement with SplitMix64 jitter, hydrostatic prestress)
+lp_status build_instance(const lp_fixture_spec& s, HostInstance& h) {
+  lp_status st = validate_spec(s);
+  if (st != LP_OK) return st;
+  st = make_layout(s, h);
+  if (st != LP_OK) return st;
+  h.spec = s;
+  const lp_material& M = s.material;
+  SplitMix64 rng{s.seed};
+  int64_t counts[3];
+  for (int a = 0; a < 3; ++a) counts[a] = axis_count(s.initial_size[a], s.grid_spacing);
+  const double sub = s.grid_spacing / 2.0;
+  double origin[3] = {0, 0, 0};
+  if (s.fixture == LP_SLUMP || s.fixture == LP_COUPLED_PATCH) {
+    origin[0] = 0.5 * (s.domain[0] - s.initial_size[0]);
+    origin[1] = 0.5 * (s.domain[1] - s.initial_size[1]);
+  }
+  const double jitter = s.fixture == LP_HYDROSTATIC ? 0.0 : 0.1 * sub;
+  const double height = s.initial_size[2];
+  const double gnorm = std::sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] + s.gravity[2] * s.gravity[2]);
+  const size_t n = (size_t)(counts[0] * counts[1] * counts[2]);
+  HostParticles& P = h.P;
+  P.x.resize(3 * n);
+  P.v.resize(3 * n);
+  P.H.assign(9 * n, 0.0);
+  P.tau.assign(9 * n, 0.0);
+  P.jm1.assign(n, 0.0);
+  P.m.resize(n);
+  P.V0.resize(n);
+  P.ys.assign(n, M.yield_stress);
+  P.id.resize(n);
+  size_t idx = 0;
+  for (int64_t i = 0; i < counts[0]; ++i)
+    for (int64_t j = 0; j < counts[1]; ++j)
+      for (int64_t k = 0; k < counts[2]; ++k) {
+        double pos[3] = {origin[0] + ((double)i + 0.5) * sub, origin[1] + ((double)j + 0.5) * sub,
+                         origin[2] + ((double)k + 0.5) * sub};
+        if (jitter > 0.0)
+          for (int a = 0; a < 3; ++a) pos[a] += (rng.next_unit() - 0.5) * 2.0 * jitter;
+        const double cur = sub * sub * sub;
+        double J = 1.0;
+        if (s.fixture == LP_HYDROSTATIC) {
+          const double depth = height - pos[2];
+          if (M.kind == LP_LIQUID) {
+            const double arg = -M.density * gnorm * depth / M.bulk_modulus;
+            J = std::exp(arg);
+            P.jm1[idx] = std::expm1(arg);
+            const double pr = M.bulk_modulus * (1.0 / J - 1.0);
+            for (int a = 0; a < 3; ++a) P.tau[9 * idx + 4 * a] = -pr * J;
+          } else {
+            const double modulus = M.lame_lambda + 2.0 * M.shear_modulus;
+            const double strain = -M.density * gnorm * depth / modulus;
+            J = std::exp(strain);
+            P.H[9 * idx + 8] = std::expm1(strain);
+            P.tau[9 * idx + 0] = M.lame_lambda * strain;
+            P.tau[9 * idx + 4] = M.lame_lambda * strain;
+            P.tau[9 * idx + 8] = modulus * strain;
+          }
+        }
+        const double vol0 = cur / J;
+        for (int a = 0; a < 3; ++a) {
+          P.x[3 * idx + a] = pos[a];
+          P.v[3 * idx + a] = s.initial_velocity[a];
+        }
+        P.m[idx] = M.density * vol0;
+        P.V0[idx] = vol0;
+        P.id[idx] = (uint32_t)idx;
+        ++idx;
+      }
+  if (s.yield_random)
+    for (size_t p = 0; p < n; ++p) P.ys[p] = s.yield_min + (s.yield_max - s.yield_min) * rng.next_unit();
+  h.has_pellet = false;
+  if (s.fixture == LP_COUPLED_PATCH && s.has_pellet) {
+    const double center[3] = {0.5 * s.domain[0], 0.5 * s.domain[1],
+                              s.initial_size[2] + 2.0 * s.grid_spacing + s.pellet_radius};
+    st = make_pellet(s.pellet_radius, s.pellet_length, s.pellet_density, center, h.pellet);
+    if (st != LP_OK) return st;
+    h.has_pellet = true;
+  }
+  return LP_OK;
+}
+
+int64_t round_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+// ---------------------------------------------------------------- ensemble
+struct Ensemble {
+  int n = 0;
+  std::vector<lp_fixture_spec> specs;
+  std::vector<InstDesc> desc;
+  std::vector<int> has_pellet;
+  lp::DeviceArrays A;
+  std::vector<void*> allocs;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  // graph of `graph_steps` attempts
+  int graph_steps = 0;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  int graph_kernels = 0;
+  std::vector<Control> ctrl_h;
+  double* d_diag = nullptr;
+  float* d_mlp = nullptr;
+  int warm = 0;
+
+  ~Ensemble() { release(); }
+  void release() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+    for (void* p : allocs) cudaFree(p);
+    allocs.clear();
+    if (own_stream) cudaStreamDestroy(own_stream);
+    own_stream = nullptr;
+  }
+  template <class T>
+  lp_status alloc(T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return set_error(LP_DEVICE, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(q);
+    *p = (T*)q;
+    e = cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(T), stream);
+    if (e != cudaSuccess) return set_error(LP_DEVICE, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    return LP_OK;
+  }
+  void invalidate_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+  }
+};
+
+lp_status pull_ctrl(Ensemble& E) {
+  E.ctrl_h.resize(E.n);
+  CUDA_CK(cudaMemcpyAsync(E.ctrl_h.data(), E.A.ctrl, sizeof(Control) * E.n, cudaMemcpyDeviceToHost, E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  return LP_OK;
+}
+lp_status push_ctrl(Ensemble& E) {
+  CUDA_CK(cudaMemcpyAsync(E.A.ctrl, E.ctrl_h.data(), sizeof(Control) * E.n, cudaMemcpyHostToDevice, E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  return LP_OK;
+}
+
+// refresh bbound / max speed / total mass of the committed state
+lp_status refresh_stats(Ensemble& E) {
+  lp::launch_state_stats(E.A, E.stream);
+  CUDA_CK(cudaGetLastError());
+  std::vector<lp::ParticlePartial> part(E.A.n_pcta);
+  CUDA_CK(cudaMemcpyAsync(part.data(), E.A.ppart, sizeof(lp::ParticlePartial) * E.A.n_pcta, cudaMemcpyDeviceToHost,
+                          E.stream));
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  for (int i = 0; i < E.n; ++i) {
+    const InstDesc& D = E.desc[i];
+    double bb = 0.0, mass = 0.0;
+    float ms = 0.0f;
+    for (int64_t c = 0; c < D.pcta_cnt; ++c) {
+      const lp::ParticlePartial& P = part[D.pcta_off + c];
+      bb += P.bbound;
+      mass += P.mass;
+      ms = std::max(ms, P.max_speed);
+    }
+    E.ctrl_h[i].bbound = bb;
+    E.ctrl_h[i].max_speed = ms;
+    E.ctrl_h[i].total_mass = mass;
+  }
+  return push_ctrl(E);
+}
+
+struct Diag {
+  double ke, pe, ee, mass, mom[3], max_speed, max_ep, yielded, min_x, max_x, min_y, max_y, max_z, hsq, hmax, column;
+};
+
+lp_status diagnostics(Ensemble& E, std::vector<Diag>& out) {
+  if (!E.d_diag) {
+    lp_status st = E.alloc(&E.d_diag, (size_t)E.A.n_pcta * lp::DIAG_N);
+    if (st != LP_OK) return st;
+  }
+  // hydrostatic / dam-break flags are per ensemble: batch members share fixture kind
+  const lp_fixture_spec& s0 = E.specs[0];
+  lp::launch_diagnostics(E.A, s0.fixture == LP_HYDROSTATIC, s0.initial_size[2], s0.fixture == LP_DAM_BREAK, E.d_diag,
+                         E.stream);
+  CUDA_CK(cudaGetLastError());
+  std::vector<double> raw((size_t)E.A.n_pcta * lp::DIAG_N);
+  CUDA_CK(cudaMemcpyAsync(raw.data(), E.d_diag, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost, E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  out.assign(E.n, Diag{});
+  for (int i = 0; i < E.n; ++i) {
+    const InstDesc& D = E.desc[i];
+    Diag d{};
+    d.min_x = d.min_y = 1e300;
+    d.max_x = d.max_y = d.max_z = -1e300;
+    d.column = -1e300;
+    for (int64_t c = 0; c < D.pcta_cnt; ++c) {
+      const double* v = &raw[(size_t)(D.pcta_off + c) * lp::DIAG_N];
+      d.ke += v[0];
+      d.pe += v[1];
+      d.ee += v[2];
+      d.mass += v[3];
+      d.mom[0] += v[4];
+      d.mom[1] += v[5];
+      d.mom[2] += v[6];
+      d.max_speed = std::max(d.max_speed, v[7]);
+      d.max_ep = std::max(d.max_ep, v[8]);
+      d.min_x = std::min(d.min_x, v[9]);
+      d.max_x = std::max(d.max_x, v[10]);
+      d.min_y = std::min(d.min_y, v[11]);
+      d.max_y = std::max(d.max_y, v[12]);
+      d.max_z = std::max(d.max_z, v[13]);
+      d.yielded += v[14];
+      d.hsq += v[15];
+      d.hmax = std::max(d.hmax, v[16]);
+      d.column = std::max(d.column, v[17]);
+    }
+    out[i] = d;
+  }
+  return LP_OK;
+}
+
+// pellet kinetic energy (rigid.rs:256-261) and helpers on the host FP64 copy
+void q_matrix(const double* q, double R[3][3]) {
+  const double i = q[0], j = q[1], k = q[2], w = q[3];
+  const double ww = w * w, ii = i * i, jj = j * j, kk = k * k;
+  const double ij = i * j * 2.0, wk = w * k * 2.0, wj = w * j * 2.0, ik = i * k * 2.0, jk = j * k * 2.0, wi = w * i * 2.0;
+  R[0][0] = ww + ii - jj - kk;
+  R[0][1] = ij - wk;
+  R[0][2] = wj + ik;
+  R[1][0] = wk + ij;
+  R[1][1] = ww - ii + jj - kk;
+  R[1][2] = jk - wi;
+  R[2][0] = ik - wj;
+  R[2][1] = wi + jk;
+  R[2][2] = ww - ii - jj + kk;
+}
+void pellet_omega_h(const lp::PelletState& P, double om[3]) {
+  double R[3][3];
+  q_matrix(P.q, R);
+  double bm[3], bo[3];
+  for (int a = 0; a < 3; ++a) bm[a] = R[0][a] * P.L[0] + R[1][a] * P.L[1] + R[2][a] * P.L[2];
+  for (int a = 0; a < 3; ++a) bo[a] = bm[a] / P.inertia[a];
+  for (int a = 0; a < 3; ++a) om[a] = R[a][0] * bo[0] + R[a][1] * bo[1] + R[a][2] * bo[2];
+}
+double pellet_ke_h(const lp::PelletState& P) {
+  double om[3];
+  pellet_omega_h(P, om);
+  return 0.5 * P.mass * (P.vel[0] * P.vel[0] + P.vel[1] * P.vel[1] + P.vel[2] * P.vel[2]) +
+         0.5 * (om[0] * P.L[0] + om[1] * P.L[1] + om[2] * P.L[2]);
+}
+
+struct Energies {
+  double ke, pe, ee, mech, mass_res, mom_res[3], e_res;
+};
+
+Energies energies_of(const Ensemble& E, int i, const Diag& d) {
+  const Control& c = E.ctrl_h[i];
+  const InstDesc& D = E.desc[i];
+  Energies r{};
+  r.ke = d.ke;
+  r.pe = d.pe;
+  r.ee = d.ee;
+  double mom[3] = {d.mom[0], d.mom[1], d.mom[2]};
+  if (D.has_pellet) {
+    r.ke += pellet_ke_h(c.pellet);
+    r.pe -= c.pellet.mass * (D.gravity[0] * c.pellet.pos[0] + D.gravity[1] * c.pellet.pos[1] + D.gravity[2] * c.pellet.pos[2]);
+    for (int a = 0; a < 3; ++a) mom[a] += c.pellet.vel[a] * c.pellet.mass;
+  }
+  r.mech = r.ke + r.pe + r.ee;
+  const lp::LedgerD& L = c.ledger;
+  r.mass_res = d.mass + L.outflow_mass - L.initial_mass;
+  for (int a = 0; a < 3; ++a)
+    r.mom_res[a] = mom[a] - L.initial_momentum[a] - L.gravity_impulse[a] + L.outflow_momentum[a] - L.wall_impulse[a] -
+                   L.pellet_wall_impulse[a];
+  const double ledgered = L.proj - L.fric + L.trac + L.pellet_work + L.cgrid + L.cpellet - L.plastic;
+  r.e_res = r.mech - L.initial_mech - ledgered;
+  return r;
+}
+
+lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) {
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+    return set_error(LP_DEVICE, "no CUDA device: the MLS-MPM substep runs on the GPU only");
+  if (count <= 0) return set_error(LP_INVALID, "ensemble needs at least one instance");
+  std::vector<HostInstance> H(count);
+  for (int i = 0; i < count; ++i) {
+    lp_status st = build_instance(specs[i], H[i]);
+    if (st != LP_OK) return count > 1 ? set_error(st, "instance " + std::to_string(i) + ": " + g_err) : st;
+    if (specs[i].fixture != specs[0].fixture)
+      return set_error(LP_UNSUPPORTED, "batched instances must share one fixture kind");
+  }
+  E.n = count;
+  E.specs.assign(specs, specs + count);
+  CUDA_CK(cudaStreamCreateWithFlags(&E.own_stream, cudaStreamNonBlocking));
+  E.stream = E.own_stream;
+  // geometry and offsets
+  E.desc.resize(count);
+  int64_t node_off = 0, tile_off = 0, key_off = 0, blk_off = 0, gcta_off = 0, slot_off = 0;
+  std::vector<int> tile_inst, gcta_inst, pcta_inst, chunk_inst;
+  int any_pellet = 0;
+  for (int i = 0; i < count; ++i) {
+    const lp_fixture_spec& s = specs[i];
+    HostInstance& h = H[i];
+    InstDesc D;
+    std::memset(&D, 0, sizeof(D));
+    D.dx = s.grid_spacing;
+    D.inv_dx = 1.0 / s.grid_spacing;
+    for (int a = 0; a < 3; ++a) {
+      D.cells[a] = (int)h.cells[a];
+      D.nodes[a] = (int)h.nodes[a];
+      D.bins[a] = D.cells[a] + 1;
+      D.extent[a] = (double)h.cells[a] * s.grid_spacing;
+    }
+    D.tiles[0] = (D.bins[0] + lp::TX - 1) / lp::TX;
+    D.tiles[1] = (D.bins[1] + lp::TY - 1) / lp::TY;
+    D.tiles[2] = (D.bins[2] + lp::TZ - 1) / lp::TZ;
+    for (int a = 0; a < 3; ++a) D.nblk[a] = (D.nodes[a] + lp::NB - 1) / lp::NB;
+    D.kind = s.material.kind;
+    D.per_particle_yield = s.yield_random ? 1 : 0;
+    D.face_mode = s.face_mode_enabled ? 1 : 0;
+    D.has_pellet = h.has_pellet ? 1 : 0;
+    any_pellet |= D.has_pellet;
+    const int64_t ntiles = (int64_t)D.tiles[0] * D.tiles[1] * D.tiles[2];
+    const int64_t nnodes = (int64_t)D.nodes[0] * D.nodes[1] * D.nodes[2];
+    const int64_t nblk = (int64_t)D.nblk[0] * D.nblk[1] * D.nblk[2];
+    D.node_off = node_off;
+    D.tile_off = tile_off;
+    D.key_off = key_off;
+    D.nkeys = round_up(ntiles * lp::TB + 1, lp::KEY_CHUNK);
+    D.blk_off = blk_off;
+    D.gcta_off = gcta_off;
+    D.gcta_cnt = (nblk + lp::GU_BLOCKS_PER_CTA - 1) / lp::GU_BLOCKS_PER_CTA;
+    D.slot_off = slot_off;
+    D.slot_cap = round_up(std::max<int64_t>((int64_t)h.P.size(), 1), lp::SLOT_ALIGN);
+    D.pcta_off = slot_off / lp::G2P_THREADS;
+    D.pcta_cnt = D.slot_cap / lp::G2P_THREADS;
+    const lp_material& M = s.material;
+    D.density = M.density;
+    D.mu = M.shear_modulus;
+    D.lambda = M.lame_lambda;
+    D.bulk = M.bulk_modulus;
+    D.yield = M.yield_stress;
+    D.consistency = M.consistency;
+    D.flow_index = M.flow_index;
+    D.tait_gamma = M.tait_gamma == 0.0 ? 1.0 : M.tait_gamma;
+    for (int a = 0; a < 3; ++a) D.gravity[a] = s.gravity[a];
+    D.friction = s.wall_friction;
+    for (int f = 0; f < 6; ++f) {
+      D.face_mu[f] = s.face_mode_enabled ? s.face_friction[f] : s.wall_friction;
+      D.face_sticky[f] = s.face_mode_enabled ? s.face_sticky[f] : 0;
+    }
+    D.cfl = s.cfl;
+    D.max_dt = s.max_dt;
+    D.min_dt = s.min_dt;
+    D.tol = s.newton_tolerance > 0.0 ? s.newton_tolerance : 1e-12;
+    D.contact_k = s.contact_stiffness;
+    D.contact_e = s.contact_restitution;
+    D.contact_mu = s.contact_friction;
+    double mass = 0.0;
+    for (size_t p = 0; p < h.P.size(); ++p) mass += (double)(float)h.P.m[p];
+    D.s_mass = std::ldexp(1.0, (int)std::floor(std::log2(4.611686018427388e18 / std::max(mass, 1e-300))));
+    E.desc[i] = D;
+    for (int64_t t = 0; t < ntiles; ++t) tile_inst.push_back(i);
+    for (int64_t t = 0; t < D.gcta_cnt; ++t) gcta_inst.push_back(i);
+    for (int64_t t = 0; t < D.pcta_cnt; ++t) pcta_inst.push_back(i);
+    for (int64_t t = 0; t < D.nkeys / lp::KEY_CHUNK; ++t) chunk_inst.push_back(i);
+    node_off += nnodes;
+    tile_off += ntiles;
+    key_off += D.nkeys;
+    blk_off += nblk;
+    gcta_off += D.gcta_cnt;
+    slot_off += D.slot_cap;
+    E.has_pellet.push_back(D.has_pellet);
+  }
+  if (slot_off > 0xFFFFFFFFll || key_off > 0xFFFFFFFFll) return set_error(LP_INVALID, "ensemble exceeds 32-bit slot/key range");
+  lp::DeviceArrays& A = E.A;
+  A.n_inst = count;
+  A.any_pellet = any_pellet;
+  A.cap = slot_off;
+  A.n_pcta = (int64_t)pcta_inst.size();
+  A.n_tiles = (int64_t)tile_inst.size();
+  A.n_gcta = (int64_t)gcta_inst.size();
+  A.n_chunks = (int64_t)chunk_inst.size();
+  A.node_total = node_off;
+  A.n_blk = blk_off;
+  lp_status st;
+#define ALLOC(ptr, n)                 \
+  st = E.alloc(&(ptr), (size_t)(n)); \
+  if (st != LP_OK) return st;
+  ALLOC(A.desc, count);
+  ALLOC(A.ctrl, count);
+  ALLOC(A.pcta_inst, A.n_pcta);
+  ALLOC(A.tile_inst, A.n_tiles);
+  ALLOC(A.gcta_inst, A.n_gcta);
+  ALLOC(A.chunk_inst, A.n_chunks);
+  ALLOC(A.st[0], (size_t)lp::NCOMP * A.cap);
+  ALLOC(A.st[1], (size_t)lp::NCOMP * A.cap);
+  ALLOC(A.id[0], A.cap);
+  ALLOC(A.id[1], A.cap);
+  ALLOC(A.keys, A.cap);
+  ALLOC(A.count, key_off);
+  ALLOC(A.start, key_off);
+  ALLOC(A.chunk_sum, A.n_chunks);
+  ALLOC(A.chunk_base, A.n_chunks);
+  ALLOC(A.perm, A.cap);
+  ALLOC(A.nw_list, A.cap);
+  ALLOC(A.nw_count, 1);
+  ALLOC(A.acc, 4 * A.node_total);
+  ALLOC(A.trac, 6 * A.node_total);
+  ALLOC(A.blk_epoch, A.n_blk);
+  ALLOC(A.vel, A.node_total);
+  ALLOC(A.gpart, A.n_gcta);
+  ALLOC(A.ppart, A.n_pcta);
+#undef ALLOC
+  CUDA_CK(cudaMemcpyAsync(A.desc, E.desc.data(), sizeof(InstDesc) * count, cudaMemcpyHostToDevice, E.stream));
+  CUDA_CK(cudaMemcpyAsync(A.pcta_inst, pcta_inst.data(), sizeof(int) * pcta_inst.size(), cudaMemcpyHostToDevice, E.stream));
+  CUDA_CK(cudaMemcpyAsync(A.tile_inst, tile_inst.data(), sizeof(int) * tile_inst.size(), cudaMemcpyHostToDevice, E.stream));
+  CUDA_CK(cudaMemcpyAsync(A.gcta_inst, gcta_inst.data(), sizeof(int) * gcta_inst.size(), cudaMemcpyHostToDevice, E.stream));
+  CUDA_CK(cudaMemcpyAsync(A.chunk_inst, chunk_inst.data(), sizeof(int) * chunk_inst.size(), cudaMemcpyHostToDevice,
+                          E.stream));
+  // particle state (FP32, component-major), ids
+  {
+    std::vector<float> st32((size_t)lp::NCOMP * A.cap, 0.0f);
+    std::vector<uint32_t> ids(A.cap, 0u);
+    for (int i = 0; i < count; ++i) {
+      const HostParticles& P = H[i].P;
+      const int64_t off = E.desc[i].slot_off;
+      for (size_t p = 0; p < P.size(); ++p) {
+        const int64_t s = off + (int64_t)p;
+        auto put = [&](int c, double v) { st32[(size_t)c * A.cap + s] = (float)v; };
+        for (int a = 0; a < 3; ++a) {
+          put(lp::C_X + a, P.x[3 * p + a]);
+          put(lp::C_V + a, P.v[3 * p + a]);
+        }
+        for (int a = 0; a < 9; ++a) put(lp::C_H + a, P.H[9 * p + a]);
+        const double* T = &P.tau[9 * p];
+        put(lp::C_TAU + 0, T[0]);
+        put(lp::C_TAU + 1, T[4]);
+        put(lp::C_TAU + 2, T[8]);
+        put(lp::C_TAU + 3, T[1]);
+        put(lp::C_TAU + 4, T[2]);
+        put(lp::C_TAU + 5, T[5]);
+        put(lp::C_M, P.m[p]);
+        put(lp::C_V0, P.V0[p]);
+        put(lp::C_YS, P.ys[p]);
+        put(lp::C_JM1, P.jm1[p]);
+        ids[s] = P.id[p];
+      }
+    }
+    CUDA_CK(cudaMemcpyAsync(A.st[0], st32.data(), sizeof(float) * st32.size(), cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(A.id[0], ids.data(), sizeof(uint32_t) * ids.size(), cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaStreamSynchronize(E.stream));
+  }
+  // control blocks
+  E.ctrl_h.assign(count, Control{});
+  for (int i = 0; i < count; ++i) {
+    Control& c = E.ctrl_h[i];
+    std::memset(&c, 0, sizeof(c));
+    c.dt_scale = 1.0;
+    c.min_dt_used = std::numeric_limits<double>::infinity();
+    c.count = (int64_t)H[i].P.size();
+    c.status = lp::S_RUNNING;
+    if (H[i].has_pellet) c.pellet = H[i].pellet;
+  }
+  lp_status s2 = push_ctrl(E);
+  if (s2 != LP_OK) return s2;
+  s2 = refresh_stats(E);
+  if (s2 != LP_OK) return s2;
+  // initial ledger (Simulation::new, solver.rs:357-394)
+  std::vector<Diag> d;
+  s2 = diagnostics(E, d);
+  if (s2 != LP_OK) return s2;
+  for (int i = 0; i < count; ++i) {
+    Control& c = E.ctrl_h[i];
+    Energies en = energies_of(E, i, d[i]);
+    c.ledger.initial_mass = d[i].mass;
+    for (int a = 0; a < 3; ++a)
+      c.ledger.initial_momentum[a] = d[i].mom[a] + (E.desc[i].has_pellet ? c.pellet.vel[a] * c.pellet.mass : 0.0);
+    c.ledger.initial_mech = en.mech;
+  }
+  return push_ctrl(E);
+}
+
+lp_status run_attempts(Ensemble& E, int steps) {
+  if (steps <= 0) return LP_OK;
+  if (E.graph_steps > 0 && steps == E.graph_steps) {
+    if (!E.graph_exec) {
+      cudaStream_t cs = E.stream;
+      CUDA_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      int kernels = 0;
+      for (int s = 0; s < steps; ++s) kernels += lp::launch_attempt(E.A, cs);
+      cudaGraph_t g = nullptr;
+      CUDA_CK(cudaStreamEndCapture(cs, &g));
+      E.graph = g;
+      CUDA_CK(cudaGraphInstantiate(&E.graph_exec, g, 0));
+      // kernels counted while capturing correspond to this first replay
+      E.graph_kernels = kernels;
+      CUDA_CK(cudaGraphLaunch(E.graph_exec, E.stream));
+      return LP_OK;
+    }
+    CUDA_CK(cudaGraphLaunch(E.graph_exec, E.stream));
+    lp::add_kernel_launches((uint64_t)E.graph_kernels);
+    return LP_OK;
+  }
+  for (int s = 0; s < steps; ++s) lp::launch_attempt(E.A, E.stream);
+  CUDA_CK(cudaGetLastError());
+  return LP_OK;
+}
+
+lp_status set_targets(Ensemble& E, double target, bool forced_reset) {
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  for (int i = 0; i < E.n; ++i) {
+    Control& c = E.ctrl_h[i];
+    if (forced_reset) c.forced_dt = 0.0;
+    if (c.status == lp::S_REACHED || c.status == lp::S_RUNNING) {
+      c.target = target;
+      c.status = (c.time < target) ? lp::S_RUNNING : lp::S_REACHED;
+    }
+  }
+  return push_ctrl(E);
+}
+
+lp_status ensemble_advance(Ensemble& E, double target, lp_keep_going_fn keep, void* ctx, int32_t* reached) {
+  if (reached) *reached = 0;
+  if (!std::isfinite(target)) return set_error(LP_INVALID, "invalid solver state: invalid target time");
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  for (int i = 0; i < E.n; ++i)
+    if (target < E.ctrl_h[i].time) return set_error(LP_INVALID, "invalid solver state: invalid target time");
+  st = set_targets(E, target, true);
+  if (st != LP_OK) return st;
+  const int chunk = E.graph_steps > 0 ? E.graph_steps : 16;
+  while (true) {
+    bool running = false;
+    for (int i = 0; i < E.n; ++i) running |= E.ctrl_h[i].status == lp::S_RUNNING;
+    if (!running) break;
+    if (keep && !keep(ctx)) return set_error(LP_BUDGET, "budget stop at a resumable step boundary");
+    st = run_attempts(E, chunk);
+    if (st != LP_OK) return st;
+    st = pull_ctrl(E);
+    if (st != LP_OK) return st;
+  }
+  bool all = true;
+  for (int i = 0; i < E.n; ++i) {
+    const Control& c = E.ctrl_h[i];
+    if (c.status == lp::S_MIN_STEP) {
+      char buf[256];
+      std::snprintf(buf, sizeof(buf),
+                    "solver aborted at t='%.17g' s: step '%.17g' s below minimum after '%llu' rejections; last failure code %d",
+                    c.time, c.dt, (unsigned long long)c.rejected_steps, c.last_fail);
+      return set_error(LP_MIN_STEP, (E.n > 1 ? "instance " + std::to_string(i) + ": " : std::string()) + buf);
+    }
+    if (c.status == lp::S_ERROR)
+      return set_error(LP_INVALID, "closed fixture leaked particles beyond the padded grid (outflow)");
+    all &= c.status == lp::S_REACHED;
+  }
+  if (reached) *reached = all ? 1 : 0;
+  return LP_OK;
+}
+
+const char* fail_text(int f) {
+  switch (f) {
+    case lp::F_CONST_INVERTED: return "constitutive update failed: trial deformation gradient inverted";
+    case lp::F_CONST_EIGEN: return "constitutive update failed: eigen-decomposition did not converge";
+    case lp::F_CONST_STRETCH: return "constitutive update failed: degenerate elastic stretch";
+    case lp::F_CONST_NOT_CONVERGED: return "constitutive update failed: Herschel-Bulkley return did not converge";
+    case lp::F_CONST_NONFINITE: return "constitutive update failed: non-finite constitutive quantity";
+    case lp::F_GRID_NONFINITE: return "non-finite grid velocity";
+    case lp::F_DISPLACEMENT: return "particle moved more than one cell in one step";
+    case lp::F_PELLET_NONFINITE: return "pellet state became non-finite";
+    case lp::F_TRACTION_NONFINITE: return "wall traction kinetic-energy jump became non-finite";
+    case lp::F_OUTFLOW: return "particle left the padded grid";
+  }
+  return "ok";
+}
+
+// ---------------------------------------------------------------- export / import
+lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const Control& c = E.ctrl_h[i];
+  const InstDesc& D = E.desc[i];
+  const int64_t n = c.count;
+  if ((int64_t)out->count < n) return set_error(LP_INVALID, "particle buffer too small");
+  const float* cur = E.A.st[c.parity];
+  std::vector<float> buf((size_t)lp::NCOMP * n);
+  for (int comp = 0; comp < lp::NCOMP; ++comp)
+    CUDA_CK(cudaMemcpyAsync(buf.data() + (size_t)comp * n, cur + (size_t)comp * E.A.cap + D.slot_off, sizeof(float) * n,
+                            cudaMemcpyDeviceToHost, E.stream));
+  std::vector<uint32_t> ids(n);
+  CUDA_CK(cudaMemcpyAsync(ids.data(), E.A.id[c.parity] + D.slot_off, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost,
+                          E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  auto g = [&](int comp, int64_t p) { return (double)buf[(size_t)comp * n + p]; };
+  for (int64_t p = 0; p < n; ++p) {
+    if (out->id) out->id[p] = ids[p];
+    for (int a = 0; a < 3; ++a) {
+      if (out->position) out->position[3 * p + a] = g(lp::C_X + a, p);
+      if (out->velocity) out->velocity[3 * p + a] = g(lp::C_V + a, p);
+    }
+    for (int a = 0; a < 9; ++a) {
+      if (out->affine) out->affine[9 * p + a] = g(lp::C_C + a, p);
+      if (out->deformation)
+        out->deformation[9 * p + a] = D.kind == 0 ? g(lp::C_H + a, p) + ((a % 4) == 0 ? 1.0 : 0.0) : ((a % 4) == 0 ? 1.0 : 0.0);
+    }
+    if (out->kirchhoff) {
+      const int map[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+      for (int a = 0; a < 9; ++a) out->kirchhoff[9 * p + a] = g(lp::C_TAU + map[a], p);
+    }
+    if (out->volume_ratio) out->volume_ratio[p] = D.kind == 1 ? 1.0 + g(lp::C_JM1, p) : 1.0;
+    if (out->plastic_strain) out->plastic_strain[p] = g(lp::C_EP, p);
+    if (out->mass) out->mass[p] = g(lp::C_M, p);
+    if (out->volume0) out->volume0[p] = g(lp::C_V0, p);
+    if (out->yield_stress) out->yield_stress[p] = D.per_particle_yield ? g(lp::C_YS, p) : D.yield;
+  }
+  out->count = (uint64_t)n;
+  return LP_OK;
+}
+
+lp_status import_particles(Ensemble& E, int i, const lp_particles* in) {
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  Control& c = E.ctrl_h[i];
+  const InstDesc& D = E.desc[i];
+  const int64_t n = (int64_t)in->count;
+  if (n > D.slot_cap) return set_error(LP_INVALID, "imported particle count exceeds the instance capacity");
+  for (int64_t p = 0; p < n; ++p) {
+    bool ok = std::isfinite(in->mass[p]) && in->mass[p] > 0.0 && std::isfinite(in->volume0[p]) && in->volume0[p] > 0.0;
+    for (int a = 0; a < 3 && ok; ++a) ok = std::isfinite(in->position[3 * p + a]) && std::isfinite(in->velocity[3 * p + a]);
+    if (!ok) return set_error(LP_INVALID, "particle id '" + std::to_string(in->id[p]) + "' has non-finite state");
+  }
+  std::vector<float> buf((size_t)lp::NCOMP * n, 0.0f);
+  auto put = [&](int comp, int64_t p, double v) { buf[(size_t)comp * n + p] = (float)v; };
+  for (int64_t p = 0; p < n; ++p) {
+    for (int a = 0; a < 3; ++a) {
+      put(lp::C_X + a, p, in->position[3 * p + a]);
+      put(lp::C_V + a, p, in->velocity[3 * p + a]);
+    }
+    for (int a = 0; a < 9; ++a) {
+      put(lp::C_C + a, p, in->affine[9 * p + a]);
+      put(lp::C_H + a, p, in->deformation[9 * p + a] - ((a % 4) == 0 ? 1.0 : 0.0));
+    }
+    const double* T = in->kirchhoff + 9 * p;
+    put(lp::C_TAU + 0, p, T[0]);
+    put(lp::C_TAU + 1, p, T[4]);
+    put(lp::C_TAU + 2, p, T[8]);
+    put(lp::C_TAU + 3, p, 0.5 * (T[1] + T[3]));
+    put(lp::C_TAU + 4, p, 0.5 * (T[2] + T[6]));
+    put(lp::C_TAU + 5, p, 0.5 * (T[5] + T[7]));
+    put(lp::C_EP, p, in->plastic_strain[p]);
+    put(lp::C_M, p, in->mass[p]);
+    put(lp::C_V0, p, in->volume0[p]);
+    put(lp::C_YS, p, in->yield_stress ? in->yield_stress[p] : D.yield);
+    put(lp::C_JM1, p, in->volume_ratio[p] - 1.0);
+  }
+  float* cur = E.A.st[c.parity];
+  for (int comp = 0; comp < lp::NCOMP; ++comp)
+    CUDA_CK(cudaMemcpyAsync(cur + (size_t)comp * E.A.cap + D.slot_off, buf.data() + (size_t)comp * n, sizeof(float) * n,
+                            cudaMemcpyHostToDevice, E.stream));
+  CUDA_CK(cudaMemcpyAsync(E.A.id[c.parity] + D.slot_off, in->id, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  c.count = n;
+  st = push_ctrl(E);
+  if (st != LP_OK) return st;
+  return refresh_stats(E);
+}
+
+void ledger_out(const lp::LedgerD& L, lp_ledger* o) {
+  static_assert(sizeof(lp::LedgerD) == sizeof(lp_ledger), "ledger layouts differ");
+  std::memcpy(o, &L, sizeof(L));
+}
+
+void counters_out(const Control& c, lp_counters* o) {
+  o->time = c.time;
+  o->step_count = c.step_count;
+  o->limited_steps = c.limited_steps;
+  o->rejected_steps = c.rejected_steps;
+  o->dt_scale = c.dt_scale;
+  o->min_dt_used = c.min_dt_used;
+  o->max_dt_used = c.max_dt_used;
+  o->particle_count = (uint64_t)c.count;
+  o->newton_iterations = c.newton_iterations;
+  o->yielded_particles = c.yielded;
+}
+
+// fixtures.rs:369-606 assembled from device reductions
+lp_status observables(Ensemble& E, int i, std::map<std::string, double>& out) {
+  std::vector<Diag> d;
+  lp_status st = diagnostics(E, d);
+  if (st != LP_OK) return st;
+  st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const Control& c = E.ctrl_h[i];
+  const InstDesc& D = E.desc[i];
+  const lp_fixture_spec& s = E.specs[i];
+  const Diag& g = d[i];
+  Energies en = energies_of(E, i, g);
+  const lp::LedgerD& L = c.ledger;
+  const double sub = s.grid_spacing / 2.0;
+  const double n = (double)c.count;
+  out["mass_residual_kg"] = en.mass_res;
+  out["momentum_residual_kg_m_s"] =
+      std::sqrt(en.mom_res[0] * en.mom_res[0] + en.mom_res[1] * en.mom_res[1] + en.mom_res[2] * en.mom_res[2]);
+  out["kinetic_energy_j"] = en.ke;
+  out["potential_energy_j"] = en.pe;
+  out["elastic_energy_j"] = en.ee;
+  out["mechanical_energy_j"] = en.mech;
+  out["plastic_dissipation_j"] = L.plastic;
+  out["wall_normal_projection_energy_j"] = L.proj;
+  out["wall_friction_dissipation_j"] = L.fric;
+  out["wall_normal_traction_energy_j"] = L.trac;
+  out["energy_residual_j"] = en.e_res;
+  out["outflow_kg"] = L.outflow_mass;
+  out["particle_count"] = n;
+  out["step_count"] = (double)c.step_count;
+  out["limited_steps"] = (double)c.limited_steps;
+  out["rejected_steps"] = (double)c.rejected_steps;
+  out["min_dt_s"] = std::isfinite(c.min_dt_used) ? c.min_dt_used : 0.0;
+  out["max_dt_s"] = c.max_dt_used;
+  out["max_speed_m_s"] = g.max_speed;
+  out["max_plastic_strain"] = g.max_ep;
+  out["yielded_fraction"] = n > 0 ? g.yielded / n : 0.0;
+  const double height = n > 0 ? g.max_z + 0.5 * sub : 0.0;
+  out["height_m"] = height;
+  out["spread_x_m"] = n > 0 ? g.max_x - g.min_x + sub : 0.0;
+  out["spread_y_m"] = n > 0 ? g.max_y - g.min_y + sub : 0.0;
+  const double gn = std::sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]);
+  if (s.fixture == LP_SLUMP) {
+    const double h0 = s.initial_size[2];
+    out["slump_m"] = h0 - height;
+    const double tp = (D.yield / std::sqrt(3.0)) / (D.density * gn * h0);
+    out["dimensionless_yield_stress"] = tp;
+    out["pashias_slump_m"] = tp >= 0.5 ? 0.0 : (tp <= 0.0 ? h0 : h0 * (1.0 - 2.0 * tp * (1.0 - std::log(2.0 * tp))));
+  } else if (s.fixture == LP_HYDROSTATIC) {
+    const double h0 = s.initial_size[2];
+    out["hydrostatic_rms_relative_error"] = n > 0 ? std::sqrt(g.hsq / n) : 0.0;
+    out["hydrostatic_max_relative_error"] = g.hmax;
+    out["reference_bottom_stress_pa"] =
+        D.kind == 1 ? D.bulk * (std::exp(D.density * gn * h0 / D.bulk) - 1.0) : D.density * gn * h0;
+    out["wave_speed_m_s"] = D.kind == 0 ? std::sqrt((D.lambda + 2.0 * D.mu) / D.density) : std::sqrt(D.bulk / D.density);
+  } else if (s.fixture == LP_DAM_BREAK) {
+    out["front_x_m"] = n > 0 ? g.max_x + 0.5 * sub : 0.0;
+    const double ritter = s.initial_size[0] + 2.0 * std::sqrt(gn * s.initial_size[2]) * c.time;
+    out["ritter_front_bound_m"] = std::min(ritter, s.domain[0]);
+    out["column_height_m"] = g.column > -1e299 ? g.column + 0.5 * sub : 0.0;
+  } else if (s.fixture == LP_COUPLED_PATCH && D.has_pellet) {
+    const lp::PelletState& P = c.pellet;
+    out["pellet_x_m"] = P.pos[0];
+    out["pellet_y_m"] = P.pos[1];
+    out["pellet_z_m"] = P.pos[2];
+    out["pellet_speed_m_s"] = std::sqrt(P.vel[0] * P.vel[0] + P.vel[1] * P.vel[1] + P.vel[2] * P.vel[2]);
+    double om[3];
+    pellet_omega_h(P, om);
+    out["pellet_angular_speed_rad_s"] = std::sqrt(om[0] * om[0] + om[1] * om[1] + om[2] * om[2]);
+    out["pellet_kinetic_energy_j"] = pellet_ke_h(P);
+    out["pellet_penetration_m"] = std::max(s.initial_size[2] + P.radius - P.pos[2], 0.0);
+    // tilt of the body axis R x_hat out of the horizontal plane
+    double R[3][3];
+    q_matrix(P.q, R);
+    out["pellet_axis_tilt_rad"] = std::asin(std::min(std::fabs(R[2][0]), 1.0));
+    out["coupling_impulse_x_kg_m_s"] = L.coupling_impulse[0];
+    out["coupling_impulse_y_kg_m_s"] = L.coupling_impulse[1];
+    out["coupling_impulse_z_kg_m_s"] = L.coupling_impulse[2];
+    out["coupling_angular_impulse_x_kg_m2_s"] = L.coupling_angular[0];
+    out["coupling_angular_impulse_y_kg_m2_s"] = L.coupling_angular[1];
+    out["coupling_angular_impulse_z_kg_m2_s"] = L.coupling_angular[2];
+    out["pellet_wall_impulse_z_kg_m_s"] = L.pellet_wall_impulse[2];
+    out["pellet_wall_work_j"] = L.pellet_work;
+    out["coupling_grid_energy_j"] = L.cgrid;
+    out["coupling_pellet_energy_j"] = L.cpellet;
+  }
+  return LP_OK;
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+struct lp_sim {
+  Ensemble E;
+};
+struct lp_batch {
+  Ensemble E;
+};
+
+extern "C" {
+
+int32_t lp_abi_version(void) { return LP_ABI_VERSION; }
+const char* lp_last_error(void) { return g_err.c_str(); }
+uint64_t lp_kernel_launches(void) { return lp::kernel_launch_count(); }
+void lp_abi_struct_sizes(uint64_t out[6]) {
+  out[0] = sizeof(lp_material);
+  out[1] = sizeof(lp_fixture_spec);
+  out[2] = sizeof(lp_ledger);
+  out[3] = sizeof(lp_counters);
+  out[4] = sizeof(lp_particles);
+  out[5] = sizeof(lp_pellet);
+}
+
+lp_material lp_material_paste(double density, double e, double nu, double ys, double k, double n) {
+  lp_material m;
+  std::memset(&m, 0, sizeof(m));
+  m.kind = LP_PASTE;
+  m.density = density;
+  m.shear_modulus = e / (2.0 * (1.0 + nu));
+  m.lame_lambda = e * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  m.bulk_modulus = m.lame_lambda + 2.0 * m.shear_modulus / 3.0;
+  m.yield_stress = ys;
+  m.consistency = k;
+  m.flow_index = n;
+  m.tait_gamma = 1.0;
+  return m;
+}
+lp_material lp_material_paste_from_shear_rheology(double density, double e, double nu, double tys, double ks, double n) {
+  return lp_material_paste(density, e, nu, std::sqrt(3.0) * tys, std::pow(3.0, (1.0 + n) / 2.0) * ks, n);
+}
+lp_material lp_material_liquid(double density, double e, double nu, double viscosity) {
+  lp_material m;
+  std::memset(&m, 0, sizeof(m));
+  m.kind = LP_LIQUID;
+  m.density = density;
+  m.bulk_modulus = e / (3.0 * (1.0 - 2.0 * nu));
+  m.consistency = viscosity;
+  m.flow_index = 1.0;
+  m.tait_gamma = 1.0;
+  return m;
+}
+double lp_material_wave_speed(const lp_material* m) {
+  const double modulus = m->kind == LP_PASTE ? m->lame_lambda + 2.0 * m->shear_modulus : m->bulk_modulus;
+  return std::sqrt(modulus / m->density);
+}
+double lp_material_diffusivity(const lp_material* m) { return m->kind == LP_PASTE ? 0.0 : m->consistency / m->density; }
+
+lp_status lp_sim_create(const lp_fixture_spec* spec, lp_sim** out) {
+  if (!spec || !out) return set_error(LP_INVALID, "null argument");
+  *out = nullptr;
+  lp_sim* s = new lp_sim();
+  lp_status st = ensemble_create(spec, 1, s->E);
+  if (st != LP_OK) {
+    delete s;
+    return st;
+  }
+  *out = s;
+  return LP_OK;
+}
+void lp_sim_destroy(lp_sim* sim) { delete sim; }
+
+lp_status lp_sim_set_stream(lp_sim* sim, void* stream) {
+  sim->E.invalidate_graph();
+  sim->E.stream = stream ? (cudaStream_t)stream : sim->E.own_stream;
+  return LP_OK;
+}
+
+lp_status lp_sim_advance(lp_sim* sim, double target, lp_keep_going_fn keep, void* ctx, int32_t* reached) {
+  return ensemble_advance(sim->E, target, keep, ctx, reached);
+}
+
+lp_status lp_sim_try_step(lp_sim* sim, double dt, int32_t* accepted, char* reason, size_t reason_len) {
+  Ensemble& E = sim->E;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return set_error(LP_INVALID, "dt must be positive and finite");
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  E.ctrl_h[0].forced_dt = dt;
+  st = push_ctrl(E);
+  if (st != LP_OK) return st;
+  lp::launch_attempt(E.A, E.stream);
+  CUDA_CK(cudaGetLastError());
+  st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  Control& c = E.ctrl_h[0];
+  const int ok = c.fail == lp::F_OK && c.status != lp::S_ERROR;
+  if (accepted) *accepted = ok;
+  if (reason && reason_len) std::snprintf(reason, reason_len, "%s", ok ? "" : fail_text(c.fail));
+  c.forced_dt = 0.0;
+  return push_ctrl(E);
+}
+
+lp_status lp_sim_run_substeps(lp_sim* sim, int32_t steps) {
+  Ensemble& E = sim->E;
+  if (E.ctrl_h.empty() || !std::isinf(E.ctrl_h[0].target)) {
+    lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
+    if (st != LP_OK) return st;
+  }
+  return run_attempts(E, steps);
+}
+lp_status lp_sim_sync(lp_sim* sim) {
+  CUDA_CK(cudaStreamSynchronize(sim->E.stream));
+  return pull_ctrl(sim->E);
+}
+
+lp_status lp_sim_stability_limit(lp_sim* sim, double* out) {
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  const Control& c = sim->E.ctrl_h[0];
+  const InstDesc& D = sim->E.desc[0];
+  const double wave = D.kind == 0 ? std::sqrt((D.lambda + 2.0 * D.mu) / D.density) : std::sqrt(D.bulk / D.density);
+  double limit = D.cfl * D.dx / (wave + c.max_speed);
+  const double diff = D.kind == 0 ? 0.0 : D.consistency / D.density;
+  if (diff > 0.0) limit = std::fmin(limit, 0.25 * D.dx * D.dx / diff);
+  if (D.has_pellet) {
+    limit = std::fmin(limit, 0.2 * std::sqrt(c.pellet.mass / D.contact_k));
+    const double ps = std::sqrt(c.pellet.vel[0] * c.pellet.vel[0] + c.pellet.vel[1] * c.pellet.vel[1] + c.pellet.vel[2] * c.pellet.vel[2]);
+    if (ps > 0.0) limit = std::fmin(limit, D.cfl * D.dx / ps);
+  }
+  *out = limit;
+  return LP_OK;
+}
+
+lp_status lp_sim_get_ledger(lp_sim* sim, lp_ledger* out) {
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  ledger_out(sim->E.ctrl_h[0].ledger, out);
+  return LP_OK;
+}
+lp_status lp_sim_set_ledger(lp_sim* sim, const lp_ledger* in) {
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  std::memcpy(&sim->E.ctrl_h[0].ledger, in, sizeof(lp_ledger));
+  return push_ctrl(sim->E);
+}
+lp_status lp_sim_get_counters(lp_sim* sim, lp_counters* out) {
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  counters_out(sim->E.ctrl_h[0], out);
+  return LP_OK;
+}
+lp_status lp_sim_set_counters(lp_sim* sim, const lp_counters* in) {
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  Control& c = sim->E.ctrl_h[0];
+  if (!(in->dt_scale > 0.0 && in->dt_scale <= 1.0) || !std::isfinite(in->time) || in->time < 0.0)
+    return set_error(LP_INVALID, "invalid counters");
+  c.time = in->time;
+  c.step_count = in->step_count;
+  c.limited_steps = in->limited_steps;
+  c.rejected_steps = in->rejected_steps;
+  c.dt_scale = in->dt_scale;
+  c.min_dt_used = in->min_dt_used;
+  c.max_dt_used = in->max_dt_used;
+  c.status = lp::S_RUNNING;
+  return push_ctrl(sim->E);
+}
+lp_status lp_sim_particle_count(lp_sim* sim, uint64_t* out) {
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  *out = (uint64_t)sim->E.ctrl_h[0].count;
+  return LP_OK;
+}
+lp_status lp_sim_export_particles(lp_sim* sim, lp_particles* out) { return export_particles(sim->E, 0, out); }
+lp_status lp_sim_import_particles(lp_sim* sim, const lp_particles* in) { return import_particles(sim->E, 0, in); }
+
+lp_status lp_sim_get_pellet(lp_sim* sim, lp_pellet* out, int32_t* has) {
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  *has = sim->E.desc[0].has_pellet;
+  if (!*has) return LP_OK;
+  const lp::PelletState& P = sim->E.ctrl_h[0].pellet;
+  std::memset(out, 0, sizeof(*out));
+  out->radius = P.radius;
+  out->length = P.length;
+  out->mass = P.mass;
+  for (int a = 0; a < 3; ++a) {
+    out->inertia_body[a] = P.inertia[a];
+    out->position[a] = P.pos[a];
+    out->velocity[a] = P.vel[a];
+    out->angular_momentum[a] = P.L[a];
+  }
+  for (int a = 0; a < 4; ++a) out->orientation[a] = P.q[a];
+  out->sphere_count = P.nsph;
+  for (int k = 0; k < P.nsph; ++k) out->sphere_offsets[k] = P.off[k];
+  return LP_OK;
+}
+lp_status lp_sim_set_pellet(lp_sim* sim, const lp_pellet* in) {
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  if (!sim->E.desc[0].has_pellet) return set_error(LP_INVALID, "simulation has no pellet");
+  if (in->sphere_count < 1 || in->sphere_count > 64) return set_error(LP_INVALID, "invalid pellet sphere count");
+  lp::PelletState& P = sim->E.ctrl_h[0].pellet;
+  P.radius = in->radius;
+  P.length = in->length;
+  P.mass = in->mass;
+  for (int a = 0; a < 3; ++a) {
+    P.inertia[a] = in->inertia_body[a];
+    P.pos[a] = in->position[a];
+    P.vel[a] = in->velocity[a];
+    P.L[a] = in->angular_momentum[a];
+  }
+  for (int a = 0; a < 4; ++a) P.q[a] = in->orientation[a];
+  P.nsph = in->sphere_count;
+  for (int k = 0; k < P.nsph; ++k) P.off[k] = in->sphere_offsets[k];
+  return push_ctrl(sim->E);
+}
+
+lp_status lp_sim_observables(lp_sim* sim, char* names, double* values, int32_t capacity, int32_t* count) {
+  std::map<std::string, double> obs;
+  lp_status st = observables(sim->E, 0, obs);
+  if (st != LP_OK) return st;
+  int32_t n = 0;
+  for (auto& kv : obs) {
+    if (n >= capacity) break;
+    std::snprintf(names + 64 * n, 64, "%s", kv.first.c_str());
+    values[n] = kv.second;
+    ++n;
+  }
+  *count = n;
+  return LP_OK;
+}
+
+lp_status lp_sim_energies(lp_sim* sim, double out[9]) {
+  std::vector<Diag> d;
+  lp_status st = diagnostics(sim->E, d);
+  if (st != LP_OK) return st;
+  st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  Energies en = energies_of(sim->E, 0, d[0]);
+  out[0] = en.ke;
+  out[1] = en.pe;
+  out[2] = en.ee;
+  out[3] = en.mech;
+  out[4] = en.mass_res;
+  out[5] = en.mom_res[0];
+  out[6] = en.mom_res[1];
+  out[7] = en.mom_res[2];
+  out[8] = en.e_res;
+  return LP_OK;
+}
+
+static lp_status set_warm(Ensemble& E, const float* w, int32_t nw, int32_t enable) {
+  if (enable) {
+    if (!w || nw != lp::MLP_NW) return set_error(LP_INVALID, "warm start needs the full MLP weight vector");
+    if (!E.d_mlp) {
+      lp_status st = E.alloc(&E.d_mlp, lp::MLP_NW);
+      if (st != LP_OK) return st;
+    }
+    CUDA_CK(cudaMemcpyAsync(E.d_mlp, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice, E.stream));
+    E.A.mlp = E.d_mlp;
+  }
+  E.invalidate_graph();
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  for (auto& c : E.ctrl_h) c.warm_start = enable ? 1 : 0;
+  return push_ctrl(E);
+}
+lp_status lp_sim_set_warm_start(lp_sim* sim, const float* w, int32_t nw, int32_t enable) {
+  return set_warm(sim->E, w, nw, enable);
+}
+lp_status lp_sim_grid_totals(lp_sim* sim, double dt, double out[8]) {
+  Ensemble& E = sim->E;
+  if (!(dt > 0.0)) return set_error(LP_INVALID, "dt must be positive");
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  E.ctrl_h[0].forced_dt = dt;
+  st = push_ctrl(E);
+  if (st != LP_OK) return st;
+  long long* d = nullptr;
+  CUDA_CK(cudaMalloc(&d, 4 * sizeof(long long)));
+  CUDA_CK(cudaMemsetAsync(d, 0, 4 * sizeof(long long), E.stream));
+  lp::launch_grid_totals(E.A, d, E.stream);
+  CUDA_CK(cudaGetLastError());
+  long long h[4];
+  CUDA_CK(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, E.stream));
+  CUDA_CK(cudaMemsetAsync(E.A.acc, 0, sizeof(long long) * 4 * E.A.node_total, E.stream));
+  CUDA_CK(cudaMemsetAsync(E.A.trac, 0, sizeof(long long) * 6 * E.A.node_total, E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  cudaFree(d);
+  st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const Control& c = E.ctrl_h[0];
+  out[0] = (double)h[0] / E.desc[0].s_mass;
+  for (int a = 0; a < 3; ++a) out[1 + a] = (double)h[1 + a] / c.s_mom;
+  std::vector<Diag> dg;
+  st = diagnostics(E, dg);
+  if (st != LP_OK) return st;
+  out[4] = dg[0].mass;
+  for (int a = 0; a < 3; ++a) out[5 + a] = dg[0].mom[a];
+  E.ctrl_h[0].forced_dt = 0.0;
+  return push_ctrl(E);
+}
+
+lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* names, int32_t capacity,
+                              int32_t* count) {
+  Ensemble& E = sim->E;
+  if (E.ctrl_h.empty() || !std::isinf(E.ctrl_h[0].target)) {
+    lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
+    if (st != LP_OK) return st;
+  }
+  cudaEvent_t ev[16];
+  for (int k = 0; k < 16; ++k) CUDA_CK(cudaEventCreate(&ev[k]));
+  std::vector<double> acc(16, 0.0);
+  int nk = 0;
+  for (int s = 0; s < steps; ++s) {
+    nk = lp::launch_attempt(E.A, E.stream, ev);
+    CUDA_CK(cudaGetLastError());
+    CUDA_CK(cudaEventSynchronize(ev[nk]));
+    for (int k = 0; k < nk; ++k) {
+      float t = 0.f;
+      CUDA_CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+      acc[k] += t;
+    }
+  }
+  for (int k = 0; k < 16; ++k) cudaEventDestroy(ev[k]);
+  const int n = std::min(nk, (int)capacity);
+  for (int k = 0; k < n; ++k) {
+    ms[k] = acc[k] / std::max(steps, 1);
+    std::snprintf(names + 32 * k, 32, "%s", lp::attempt_kernel_name(k, E.A.any_pellet));
+  }
+  *count = n;
+  return pull_ctrl(E);
+}
+
+lp_status lp_sim_use_graph(lp_sim* sim, int32_t steps) {
+  sim->E.invalidate_graph();
+  sim->E.graph_steps = steps > 0 ? steps : 0;
+  return LP_OK;
+}
+
+lp_status lp_sim_enable_newton_log(lp_sim* sim, int64_t capacity) {
+  Ensemble& E = sim->E;
+  E.invalidate_graph();
+  if (capacity <= 0) {
+    E.A.log_n = nullptr;
+    return LP_OK;
+  }
+  lp_status st = E.alloc(&E.A.log_x, (size_t)capacity * 6);
+  if (st != LP_OK) return st;
+  st = E.alloc(&E.A.log_y, (size_t)capacity);
+  if (st != LP_OK) return st;
+  st = E.alloc(&E.A.log_n, 1);
+  if (st != LP_OK) return st;
+  E.A.log_cap = capacity;
+  return LP_OK;
+}
+lp_status lp_sim_read_newton_log(lp_sim* sim, float* x, float* y, int64_t capacity, int64_t* count) {
+  Ensemble& E = sim->E;
+  if (!E.A.log_n) return set_error(LP_INVALID, "newton log not enabled");
+  unsigned long long n = 0;
+  CUDA_CK(cudaMemcpyAsync(&n, E.A.log_n, sizeof(n), cudaMemcpyDeviceToHost, E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  int64_t m = std::min<int64_t>((int64_t)n, std::min<int64_t>(capacity, E.A.log_cap));
+  if (m > 0) {
+    CUDA_CK(cudaMemcpyAsync(x, E.A.log_x, sizeof(float) * 6 * m, cudaMemcpyDeviceToHost, E.stream));
+    CUDA_CK(cudaMemcpyAsync(y, E.A.log_y, sizeof(float) * m, cudaMemcpyDeviceToHost, E.stream));
+    CUDA_CK(cudaStreamSynchronize(E.stream));
+  }
+  *count = m;
+  return LP_OK;
+}
+
+// ---------------- batch
+lp_status lp_batch_create(const lp_fixture_spec* specs, int32_t count, lp_batch** out) {
+  if (!specs || !out) return set_error(LP_INVALID, "null argument");
+  *out = nullptr;
+  lp_batch* b = new lp_batch();
+  lp_status st = ensemble_create(specs, count, b->E);
+  if (st != LP_OK) {
+    delete b;
+    return st;
+  }
+  *out = b;
+  return LP_OK;
+}
+void lp_batch_destroy(lp_batch* b) { delete b; }
+lp_status lp_batch_set_stream(lp_batch* b, void* stream) {
+  b->E.invalidate_graph();
+  b->E.stream = stream ? (cudaStream_t)stream : b->E.own_stream;
+  return LP_OK;
+}
+lp_status lp_batch_advance(lp_batch* b, double target, lp_keep_going_fn keep, void* ctx, int32_t* all) {
+  return ensemble_advance(b->E, target, keep, ctx, all);
+}
+lp_status lp_batch_run_substeps(lp_batch* b, int32_t steps) {
+  Ensemble& E = b->E;
+  if (E.ctrl_h.empty() || !std::isinf(E.ctrl_h[0].target)) {
+    lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
+    if (st != LP_OK) return st;
+  }
+  return run_attempts(E, steps);
+}
+lp_status lp_batch_sync(lp_batch* b) {
+  CUDA_CK(cudaStreamSynchronize(b->E.stream));
+  return pull_ctrl(b->E);
+}
+lp_status lp_batch_get_counters(lp_batch* b, int32_t i, lp_counters* out) {
+  if (i < 0 || i >= b->E.n) return set_error(LP_INVALID, "instance index out of range");
+  lp_status st = pull_ctrl(b->E);
+  if (st != LP_OK) return st;
+  counters_out(b->E.ctrl_h[i], out);
+  return LP_OK;
+}
+lp_status lp_batch_get_ledger(lp_batch* b, int32_t i, lp_ledger* out) {
+  if (i < 0 || i >= b->E.n) return set_error(LP_INVALID, "instance index out of range");
+  lp_status st = pull_ctrl(b->E);
+  if (st != LP_OK) return st;
+  ledger_out(b->E.ctrl_h[i].ledger, out);
+  return LP_OK;
+}
+lp_status lp_batch_export_particles(lp_batch* b, int32_t i, lp_particles* out) {
+  if (i < 0 || i >= b->E.n) return set_error(LP_INVALID, "instance index out of range");
+  return export_particles(b->E, i, out);
+}
+lp_status lp_batch_total_particles(lp_batch* b, uint64_t* out) {
+  lp_status st = pull_ctrl(b->E);
+  if (st != LP_OK) return st;
+  uint64_t t = 0;
+  for (auto& c : b->E.ctrl_h) t += (uint64_t)c.count;
+  *out = t;
+  return LP_OK;
+}
+lp_status lp_batch_set_warm_start(lp_batch* b, const float* w, int32_t nw, int32_t enable) {
+  return set_warm(b->E, w, nw, enable);
+}
+lp_status lp_batch_use_graph(lp_batch* b, int32_t steps) {
+  b->E.invalidate_graph();
+  b->E.graph_steps = steps > 0 ? steps : 0;
+  return LP_OK;
+}
+lp_status lp_batch_autotune(lp_batch* b, int32_t trial_steps, char* report, size_t report_len) {
+  // Candidates: attempts per graph replay.  Each candidate runs trial_steps attempts on the live
+  // batch (time advances; the committed state stays a valid trajectory) and is timed with events.
+  Ensemble& E = b->E;
+  const int cands[4] = {1, 4, 16, 64};
+  float best_ms = 1e30f;
+  int best = 0;
+  std::string rep;
+  cudaEvent_t e0, e1;
+  CUDA_CK(cudaEventCreate(&e0));
+  CUDA_CK(cudaEventCreate(&e1));
+  for (int ci = 0; ci < 4; ++ci) {
+    E.invalidate_graph();
+    E.graph_steps = cands[ci] > 1 ? cands[ci] : 0;
+    lp_status st = lp_batch_run_substeps(b, cands[ci]);  // warm (captures the graph)
+    if (st != LP_OK) return st;
+    const int reps = std::max(1, trial_steps / cands[ci]);
+    CUDA_CK(cudaEventRecord(e0, E.stream));
+    for (int r = 0; r < reps; ++r) {
+      st = run_attempts(E, cands[ci]);
+      if (st != LP_OK) return st;
+    }
+    CUDA_CK(cudaEventRecord(e1, E.stream));
+    CUDA_CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CUDA_CK(cudaEventElapsedTime(&ms, e0, e1));
+    const float per = ms / (float)(reps * cands[ci]);
+    char line[96];
+    std::snprintf(line, sizeof(line), "graph_attempts=%d ms_per_attempt=%.4f\n", cands[ci], per);
+    rep += line;
+    if (per < best_ms) {
+      best_ms = per;
+      best = cands[ci];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  E.invalidate_graph();
+  E.graph_steps = best > 1 ? best : 0;
+  char line[64];
+  std::snprintf(line, sizeof(line), "chosen=%d\n", best);
+  rep += line;
+  if (report && report_len) std::snprintf(report, report_len, "%s", rep.c_str());
+  return LP_OK;
+}
+
+// ---------------- constitutive unit kernels on host arrays
+lp_status lp_hb_return_batch(int64_t n, const double* trial, const double* yield, const double* consistency,
+                             const double* flow_index, const double* mu, const double* dt, double tol_rel,
+                             const float* mlp_weights, int32_t nweights, double* out, int32_t* status) {
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return set_error(LP_DEVICE, "no CUDA device");
+  if (n <= 0) return LP_OK;
+  if (mlp_weights && nweights != lp::MLP_NW) return set_error(LP_INVALID, "MLP weight count mismatch");
+  double* d = nullptr;
+  float* w = nullptr;
+  int* s = nullptr;
+  const size_t nb = sizeof(double) * (size_t)n;
+  CUDA_CK(cudaMalloc(&d, nb * 9));
+  CUDA_CK(cudaMalloc(&s, sizeof(int) * n));
+  if (mlp_weights) {
+    CUDA_CK(cudaMalloc(&w, sizeof(float) * lp::MLP_NW));
+    CUDA_CK(cudaMemcpy(w, mlp_weights, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
+  }
+  const double* src[6] = {trial, yield, consistency, flow_index, mu, dt};
+  for (int k = 0; k < 6; ++k) CUDA_CK(cudaMemcpy(d + k * n, src[k], nb, cudaMemcpyHostToDevice));
+  lp::launch_hb_return_batch(n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, tol_rel > 0 ? tol_rel : 1e-12, w,
+                             d + 6 * n, s, 0);
+  CUDA_CK(cudaGetLastError());
+  CUDA_CK(cudaMemcpy(out, d + 6 * n, nb * 3, cudaMemcpyDeviceToHost));
+  CUDA_CK(cudaMemcpy(status, s, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  cudaFree(s);
+  if (w) cudaFree(w);
+  return LP_OK;
+}
+
+lp_status lp_update_paste_batch(int64_t n, const double* f_trial, const lp_material* m, double dt, double* f_new,
+                                double* tau, double* dep, double* diss, double* eq, int32_t* status) {
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return set_error(LP_DEVICE, "no CUDA device");
+  if (n <= 0) return LP_OK;
+  double *df = nullptr, *dfn = nullptr, *dt9 = nullptr, *ds = nullptr;
+  int* st = nullptr;
+  CUDA_CK(cudaMalloc(&df, sizeof(double) * 9 * n));
+  CUDA_CK(cudaMalloc(&dfn, sizeof(double) * 9 * n));
+  CUDA_CK(cudaMalloc(&dt9, sizeof(double) * 9 * n));
+  CUDA_CK(cudaMalloc(&ds, sizeof(double) * 3 * n));
+  CUDA_CK(cudaMalloc(&st, sizeof(int) * n));
+  CUDA_CK(cudaMemcpy(df, f_trial, sizeof(double) * 9 * n, cudaMemcpyHostToDevice));
+  lp::launch_update_paste_batch(n, df, m->shear_modulus, m->lame_lambda, m->yield_stress, m->consistency, m->flow_index,
+                                dt, 1e-12, dfn, dt9, ds, st, 0);
+  CUDA_CK(cudaGetLastError());
+  std::vector<double> sc(3 * n);
+  CUDA_CK(cudaMemcpy(f_new, dfn, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost));
+  CUDA_CK(cudaMemcpy(tau, dt9, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost));
+  CUDA_CK(cudaMemcpy(sc.data(), ds, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+  CUDA_CK(cudaMemcpy(status, st, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  for (int64_t i = 0; i < n; ++i) {
+    if (dep) dep[i] = sc[3 * i];
+    if (diss) diss[i] = sc[3 * i + 1];
+    if (eq) eq[i] = sc[3 * i + 2];
+  }
+  cudaFree(df);
+  cudaFree(dfn);
+  cudaFree(dt9);
+  cudaFree(ds);
+  cudaFree(st);
+  return LP_OK;
+}
+
+lp_status lp_update_liquid_batch(int64_t n, const double* volume_ratio, const double* grad, const lp_material* m,
+                                 double dt, double* j_new, double* tau, double* pressure, int32_t* status) {
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return set_error(LP_DEVICE, "no CUDA device");
+  if (n <= 0) return LP_OK;
+  double *dj, *dg, *djn, *dtau, *dp;
+  int* st;
+  CUDA_CK(cudaMalloc(&dj, sizeof(double) * n));
+  CUDA_CK(cudaMalloc(&dg, sizeof(double) * 9 * n));
+  CUDA_CK(cudaMalloc(&djn, sizeof(double) * n));
+  CUDA_CK(cudaMalloc(&dtau, sizeof(double) * 9 * n));
+  CUDA_CK(cudaMalloc(&dp, sizeof(double) * n));
+  CUDA_CK(cudaMalloc(&st, sizeof(int) * n));
+  CUDA_CK(cudaMemcpy(dj, volume_ratio, sizeof(double) * n, cudaMemcpyHostToDevice));
+  CUDA_CK(cudaMemcpy(dg, grad, sizeof(double) * 9 * n, cudaMemcpyHostToDevice));
+  lp::launch_update_liquid_batch(n, dj, dg, m->bulk_modulus, m->consistency, m->tait_gamma == 0.0 ? 1.0 : m->tait_gamma,
+                                 dt, djn, dtau, dp, st, 0);
+  CUDA_CK(cudaGetLastError());
+  CUDA_CK(cudaMemcpy(j_new, djn, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CUDA_CK(cudaMemcpy(tau, dtau, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost));
+  CUDA_CK(cudaMemcpy(pressure, dp, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CUDA_CK(cudaMemcpy(status, st, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  cudaFree(dj);
+  cudaFree(dg);
+  cudaFree(djn);
+  cudaFree(dtau);
+  cudaFree(dp);
+  cudaFree(st);
+  return LP_OK;
+}
+
+void lp_hb_features(double trial, double yield, double consistency, double flow_index, double mu, double dt,
+                    float out[6]) {
+  lp::hb_features(trial, yield, consistency, flow_index, mu, dt, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,1688 @@
+// lp_kernels.cu - CUDA kernels of one MLS-MPM substep attempt (sm_100a).
+//
+// Attempt = begin -> bin (count, scan, scatter, id-sort) -> P2G -> wall traction -> grid update
+//           -> pellet coupling -> G2P + constitutive -> end (reduce, accept / reject, commit).
+// Every kernel reads dt, the fixed-point scales and the buffer parity of its instance from the
+// device control block, so one attempt is a fixed launch sequence that a CUDA graph can replay.
+//
+// Reference mapping (nredd/litter-physics):
+//   k_begin        solver.rs:418-441 (dt selection of advance_while), 477-498 (stability_limit)
+//   k_bin_*        replaces sort_particles (solver.rs:501-517): a counting sort by stencil cell
+//                  every attempt; ties ordered by id, so the order is deterministic
+//   k_p2g          deposit_particles (solver.rs:632-661), Grid::deposit (grid.rs:254-263)
+//   k_traction     wall_traction_to_grid (solver.rs:725-819), Grid::deposit_reaction (grid.rs:279-295)
+//   k_grid_update  grid_update (solver.rs:822-892), reduce_tangential_velocity (solver.rs:1145-1155)
+//   k_couple       couple_grid (rigid.rs:385-438), apply_impulse / integrate (rigid.rs:251-334)
+//   k_g2p          grid_to_particle (solver.rs:895-977) + update_paste / update_liquid
+//   k_end          try_step_captured's accept/reject and commit (solver.rs:540-611, 980-998),
+//                  advance_while's bookkeeping (solver.rs:442-468)
+#include "lp_device.cuh"
+#include "lp_kernels.h"
+
+#include <cstdio>
+
+namespace lp {
+
+// ============================================================== helpers
+__device__ __forceinline__ float* comp(float* base, int64_t cap, int c) { return base + (int64_t)c * cap; }
+__device__ __forceinline__ const float* comp(const float* base, int64_t cap, int c) {
+  return base + (int64_t)c * cap;
+}
+
+__device__ __forceinline__ int64_t node_index(const InstDesc& D, int i, int j, int k) {
+  return D.node_off + ((int64_t)i * D.nodes[1] + j) * D.nodes[2] + k;
+}
+
+// Stencil base (padded) of a coordinate: floor(x/dx - 0.5) + 1 (grid.rs:151-182).
+__device__ __forceinline__ float scaled_of(float x, float dx) { return x / dx; }
+
+__device__ __forceinline__ void weights_of(float fx, float dx, float w[3], float d[3]) {
+  const float a0 = 1.5f - fx, a1 = fx - 1.0f, a2 = fx - 0.5f;
+  w[0] = 0.5f * (a0 * a0);
+  w[1] = 0.75f - (a1 * a1);
+  w[2] = 0.5f * (a2 * a2);
+  d[0] = fx * -dx;
+  d[1] = (fx - 1.0f) * -dx;
+  d[2] = (fx - 2.0f) * -dx;
+}
+
+// block-wide deterministic reductions (fixed tree)
+template <int NT>
+__device__ double block_sum_d(double v, double* sh) {
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int s = NT / 2; s > 0; s >>= 1) {
+    if (t < s) sh[t] += sh[t + s];
+    __syncthreads();
+  }
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+template <int NT>
+__device__ long long block_sum_ll(long long v, long long* sh) {
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int s = NT / 2; s > 0; s >>= 1) {
+    if (t < s) sh[t] += sh[t + s];
+    __syncthreads();
+  }
+  long long r = sh[0];
+  __syncthreads();
+  return r;
+}
+template <int NT>
+__device__ float block_max_f(float v, float* sh) {
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int s = NT / 2; s > 0; s >>= 1) {
+    if (t < s) sh[t] = fmaxf(sh[t], sh[t + s]);
+    __syncthreads();
+  }
+  float r = sh[0];
+  __syncthreads();
+  return r;
+}
+template <int NT>
+__device__ int block_max_i(int v, int* sh) {
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int s = NT / 2; s > 0; s >>= 1) {
+    if (t < s) sh[t] = max(sh[t], sh[t + s]);
+    __syncthreads();
+  }
+  int r = sh[0];
+  __syncthreads();
+  return r;
+}
+template <int NT>
+__device__ long long block_sum_i(long long v, long long* sh) {
+  return block_sum_ll<NT>(v, sh);
+}
+
+// ============================================================== begin
+// One thread per instance: decides whether the instance attempts a step and with which dt.
+__global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, int n_inst,
+                        uint32_t* __restrict__ nw_count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *nw_count = 0u;
+  if (i >= n_inst) return;
+  const InstDesc& D = desc[i];
+  Control& c = ctrl[i];
+  c.fail = F_OK;
+  c.outflow = 0;
+  c.pellet_fail = 0;
+  c.epoch += 1;
+  // fixed-point momentum scale from the committed state's momentum bound
+  {
+    double b = c.bbound > 0.0 ? c.bbound : 1e-300;
+    int e = (int)floor(log2(2.305843009213694e18 / b));  // 2^61 / b
+    e = e > 200 ? 200 : (e < -200 ? -200 : e);
+    c.s_mom = ldexp(1.0, e);
+  }
+  if (c.forced_dt > 0.0) {
+    c.active = (c.status == S_RUNNING || c.status == S_REACHED) ? 1 : 0;
+    c.dt = c.forced_dt;
+    c.limited = 0;
+    return;
+  }
+  if (c.status != S_RUNNING || !(c.time < c.target)) {
+    c.active = 0;
+    return;
+  }
+  // stability_limit (solver.rs:477-498)
+  const double dx = D.dx;
+  const double wave = D.kind == 0 ? sqrt((D.lambda + 2.0 * D.mu) / D.density) : sqrt(D.bulk / D.density);
+  double limit = D.cfl * dx / (wave + c.max_speed);
+  const double diff = D.kind == 0 ? 0.0 : D.consistency / D.density;
+  if (diff > 0.0) limit = fmin(limit, 0.25 * dx * dx / diff);
+  if (D.has_pellet) {
+    limit = fmin(limit, 0.2 * sqrt(c.pellet.mass / D.contact_k));
+    const double ps = sqrt(c.pellet.vel[0] * c.pellet.vel[0] + c.pellet.vel[1] * c.pellet.vel[1] +
+                           c.pellet.vel[2] * c.pellet.vel[2]);
+    if (ps > 0.0) limit = fmin(limit, D.cfl * dx / ps);
+  }
+  // advance_while dt choice (solver.rs:424-441)
+  const double remaining = c.target - c.time;
+  const double scaled = c.dt_scale * limit;
+  const int limited = scaled < D.max_dt ? 1 : 0;
+  double dt = fmin(fmin(scaled, D.max_dt), remaining);
+  if (remaining - dt < 1e-12 * fmax(c.target, 1.0)) dt = remaining;
+  if (!isfinite(dt) || dt <= 0.0 || (dt < D.min_dt && remaining > D.min_dt)) {
+    c.status = S_MIN_STEP;
+    c.active = 0;
+    c.last_fail = -1;
+    c.fail_value = dt;
+    return;
+  }
+  c.limit = limit;
+  c.dt = dt;
+  c.limited = limited;
+  c.active = 1;
+}
+
+// ============================================================== binning
+__global__ void k_bin_count(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
+                            const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+                            const float* __restrict__ st1, int64_t cap, uint32_t* __restrict__ keys,
+                            uint32_t* __restrict__ count, uint32_t* __restrict__ nw_list,
+                            uint32_t* __restrict__ nw_count) {
+  const int inst = pcta_inst[blockIdx.x];
+  const Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const int64_t slot = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
+  if (slot - D.slot_off >= c.count) return;
+  const float* cur = c.parity ? st1 : st0;
+  const float dx = (float)D.dx;
+  int b[3];
+  bool ok = true;
+  bool near = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float x = cur[(int64_t)(C_X + a) * cap + slot];
+    const float s = scaled_of(x, dx);
+    const float bf = floorf(s - 0.5f);
+    const float padded = bf + 1.0f;
+    if (!(padded >= 0.0f) || padded + 2.0f >= (float)D.nodes[a]) ok = false;
+    b[a] = ok ? (int)padded : 0;
+    const float half = 0.5f * dx;
+    if (x < half || x > (float)D.extent[a] - half) near = true;
+  }
+  uint32_t key;
+  if (!ok) {
+    key = (uint32_t)(D.key_off + D.nkeys - 1);
+    atomicAdd((unsigned long long*)&ctrl[inst].outflow, 1ull);
+  } else {
+    const int tx = b[0] / TX, ty = b[1] / TY, tz = b[2] / TZ;
+    const int lx = b[0] % TX, ly = b[1] % TY, lz = b[2] % TZ;
+    const int64_t tile = ((int64_t)tx * D.tiles[1] + ty) * D.tiles[2] + tz;
+    key = (uint32_t)(D.key_off + tile * TB + (lx * TY + ly) * TZ + lz);
+    if (near) {
+      const uint32_t w = atomicAdd(nw_count, 1u);
+      nw_list[w] = (uint32_t)slot;
+    }
+  }
+  keys[slot] = key;
+  atomicAdd(&count[key], 1u);
+}
+
+// chunk sums of the key counts
+__global__ void k_scan_chunks(const uint32_t* __restrict__ count, uint32_t* __restrict__ chunk_sum,
+                              const int* __restrict__ chunk_inst, const Control* __restrict__ ctrl) {
+  __shared__ long long sh[256];
+  const int64_t chunk = blockIdx.x;
+  if (!ctrl[chunk_inst[chunk]].active) return;
+  long long s = 0;
+  const int64_t base = chunk * KEY_CHUNK;
+  for (int j = threadIdx.x; j < KEY_CHUNK; j += 256) s += count[base + j];
+  s = block_sum_ll<256>(s, sh);
+  if (threadIdx.x == 0) chunk_sum[chunk] = (uint32_t)s;
+}
+
+// per instance: exclusive scan of its chunk sums, offset by the instance's first slot
+__global__ void k_scan_instances(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                                 const uint32_t* __restrict__ chunk_sum, uint32_t* __restrict__ chunk_base) {
+  __shared__ uint32_t sh[1024];
+  const int inst = blockIdx.x;
+  if (!ctrl[inst].active) return;
+  const InstDesc& D = desc[inst];
+  const int64_t c0 = D.key_off / KEY_CHUNK, nc = D.nkeys / KEY_CHUNK;
+  uint32_t carry = (uint32_t)D.slot_off;
+  for (int64_t base = 0; base < nc; base += 1024) {
+    const int64_t j = base + threadIdx.x;
+    uint32_t v = j < nc ? chunk_sum[c0 + j] : 0u;
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+      uint32_t add = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
+      __syncthreads();
+      sh[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (j < nc) chunk_base[c0 + j] = carry + sh[threadIdx.x] - v;
+    const uint32_t total = sh[1023];
+    __syncthreads();
+    carry += total;
+  }
+}
+
+// per chunk: exclusive scan of counts -> bin start slots
+__global__ void k_scan_apply(const uint32_t* __restrict__ count, const uint32_t* __restrict__ chunk_base,
+                             uint32_t* __restrict__ start, const int* __restrict__ chunk_inst,
+                             const Control* __restrict__ ctrl) {
+  __shared__ uint32_t sh[KEY_CHUNK];
+  const int64_t chunk = blockIdx.x;
+  if (!ctrl[chunk_inst[chunk]].active) return;
+  const int64_t base = chunk * KEY_CHUNK;
+  // 1024 threads, one key each
+  const uint32_t v = count[base + threadIdx.x];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int off = 1; off < KEY_CHUNK; off <<= 1) {
+    uint32_t add = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
+    __syncthreads();
+    sh[threadIdx.x] += add;
+    __syncthreads();
+  }
+  start[base + threadIdx.x] = chunk_base[chunk] + sh[threadIdx.x] - v;
+}
+
+__global__ void k_bin_scatter(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                              const int* __restrict__ pcta_inst, const uint32_t* __restrict__ keys,
+                              uint32_t* __restrict__ count, const uint32_t* __restrict__ start,
+                              uint32_t* __restrict__ perm) {
+  const int inst = pcta_inst[blockIdx.x];
+  const Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const int64_t slot = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
+  if (slot - D.slot_off >= c.count) return;
+  const uint32_t key = keys[slot];
+  const uint32_t r = atomicSub(&count[key], 1u) - 1u;  // leaves count at zero for the next attempt
+  perm[start[key] + r] = (uint32_t)slot;
+}
+
+// order each bin by particle id (the reference's sort key ties), making the order deterministic
+__global__ void k_bin_sort(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                           const int* __restrict__ chunk_inst, const uint32_t* __restrict__ start,
+                           uint32_t* __restrict__ perm, const uint32_t* __restrict__ id0,
+                           const uint32_t* __restrict__ id1) {
+  const int64_t key = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int inst = chunk_inst[key / KEY_CHUNK];
+  const Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const int64_t lk = key - D.key_off;
+  if (lk >= D.nkeys) return;
+  const uint32_t s = start[key];
+  const uint32_t e = (lk == D.nkeys - 1) ? (uint32_t)(D.slot_off + c.count) : start[key + 1];
+  if (e <= s + 1) return;
+  const uint32_t* ids = c.parity ? id1 : id0;
+  for (uint32_t j = s + 1; j < e; ++j) {
+    const uint32_t pj = perm[j];
+    const uint32_t ij = ids[pj];
+    uint32_t k = j;
+    while (k > s && ids[perm[k - 1]] > ij) {
+      perm[k] = perm[k - 1];
+      --k;
+    }
+    perm[k] = pj;
+  }
+}
+
+// ============================================================== P2G
+// One CTA per tile of TX x TY x TZ bins; three threads per bin, one per slab a of the 3x3x3
+// stencil.  All particles of a bin share the same 27 target nodes, so each thread accumulates
+// its 9 nodes x (mass, momentum) in registers over the bin's particles, then the tile's halo is
+// combined in shared memory in 27 fixed rounds (deterministic, no atomics), converted to int64
+// fixed point with an exact-conservation correction, and flushed with one global atomic per
+// node component.
+__global__ void __launch_bounds__(P2G_THREADS, 1)
+    k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
+          const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
+          const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
+          int64_t node_total, uint32_t* __restrict__ blk_epoch) {
+  __shared__ float h[4][HN];
+  __shared__ long long hi[4][HN];
+  __shared__ long long red[P2G_THREADS];
+  __shared__ int bestidx[P2G_THREADS];
+
+  const int tile = blockIdx.x;
+  const int inst = tile_inst[tile];
+  const Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const int64_t ltile = tile - D.tile_off;
+  const int64_t key0 = D.key_off + ltile * TB;
+  if (start[key0] == start[key0 + TB]) return;  // empty tile (uniform across the CTA)
+
+  const int tz = (int)(ltile % D.tiles[2]);
+  const int ty = (int)((ltile / D.tiles[2]) % D.tiles[1]);
+  const int tx = (int)(ltile / ((int64_t)D.tiles[2] * D.tiles[1]));
+  const int t = threadIdx.x;
+  const int bin = t / 3, slab = t % 3;
+  const int lx = bin / (TY * TZ), ly = (bin / TZ) % TY, lz = bin % TZ;
+  const int bx = tx * TX + lx, by = ty * TY + ly, bz = tz * TZ + lz;
+
+  for (int j = t; j < 4 * HN; j += P2G_THREADS) (&h[0][0])[j] = 0.0f;
+
+  const float* cur = c.parity ? st1 : st0;
+  const float dx = (float)D.dx;
+  const float dt = (float)c.dt;
+  const float stress_scale = (float)(c.dt * 4.0 / (D.dx * D.dx));
+  const double s_m = D.s_mass, s_p = c.s_mom;
+
+  float acc9[3][3][4];
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc9[b][q][k] = 0.0f;
+  long long tm = 0, tq0 = 0, tq1 = 0, tq2 = 0;
+
+  const uint32_t s = start[key0 + bin], e = start[key0 + bin + 1];
+  const float basef[3] = {(float)(bx - 1), (float)(by - 1), (float)(bz - 1)};
+  for (uint32_t j = s; j < e; ++j) {
+    const int64_t src = perm[j];
+    float x[3], v[3], Cm[9], tau[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      x[a] = cur[(C_X + a) * cap + src];
+      v[a] = cur[(C_V + a) * cap + src];
+    }
+#pragma unroll
+    for (int a = 0; a < 9; ++a) Cm[a] = cur[(C_C + a) * cap + src];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) tau[a] = cur[(C_TAU + a) * cap + src];
+    const float m = cur[C_M * cap + src];
+    const float v0 = cur[C_V0 * cap + src];
+    float w[3][3], d[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) weights_of(scaled_of(x[a], dx) - basef[a], dx, w[a], d[a]);
+    // A = C m - tau (dt 4/dx^2 V0)
+    const float sv = stress_scale * v0;
+    const float T[9] = {tau[0], tau[3], tau[4], tau[3], tau[1], tau[5], tau[4], tau[5], tau[2]};
+    float A[9];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) A[a] = Cm[a] * m - T[a] * sv;
+    const float q[3] = {v[0] * m, v[1] * m, v[2] * m};
+    const float wa = w[0][slab], da = d[0][slab];
+    float u[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) u[r] = q[r] + A[3 * r + 0] * da;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const float wab = wa * w[1][b];
+      float ub[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) ub[r] = u[r] + A[3 * r + 1] * d[1][b];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        const float ww = wab * w[2][cc];
+        acc9[b][cc][0] += ww * m;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) acc9[b][cc][1 + r] += ww * (ub[r] + A[3 * r + 2] * d[2][cc]);
+      }
+    }
+    if (slab == 0) {
+      tm += to_fixed((double)m, s_m);
+      tq0 += to_fixed((double)q[0], s_p);
+      tq1 += to_fixed((double)q[1], s_p);
+      tq2 += to_fixed((double)q[2], s_p);
+    }
+  }
+  // mark the node blocks of this bin's stencil active for this attempt
+  if (e > s) {
+    for (int b = 0; b < 3; ++b)
+      for (int cc = 0; cc < 3; ++cc) {
+        const int nx = bx + slab, ny = by + b, nz = bz + cc;
+        const int64_t blk = D.blk_off + ((int64_t)(nx / NB) * D.nblk[1] + ny / NB) * D.nblk[2] + nz / NB;
+        blk_epoch[blk] = (uint32_t)c.epoch;
+      }
+  }
+  __syncthreads();
+  // halo combine: 27 rounds, each conflict-free
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        if (slab == a) {
+          const int n = ((lx + a) * HY + (ly + b)) * HZ + (lz + cc);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) h[k][n] += acc9[b][cc][k];
+        }
+        __syncthreads();
+      }
+  // exact per-tile totals
+  tm = block_sum_ll<P2G_THREADS>(tm, red);
+  tq0 = block_sum_ll<P2G_THREADS>(tq0, red);
+  tq1 = block_sum_ll<P2G_THREADS>(tq1, red);
+  tq2 = block_sum_ll<P2G_THREADS>(tq2, red);
+  // convert halo to fixed point
+  long long sm = 0, sp0 = 0, sp1 = 0, sp2 = 0;
+  for (int n = t; n < HN; n += P2G_THREADS) {
+    hi[0][n] = to_fixed((double)h[0][n], s_m);
+    hi[1][n] = to_fixed((double)h[1][n], s_p);
+    hi[2][n] = to_fixed((double)h[2][n], s_p);
+    hi[3][n] = to_fixed((double)h[3][n], s_p);
+    sm += hi[0][n];
+    sp0 += hi[1][n];
+    sp1 += hi[2][n];
+    sp2 += hi[3][n];
+  }
+  sm = block_sum_ll<P2G_THREADS>(sm, red);
+  sp0 = block_sum_ll<P2G_THREADS>(sp0, red);
+  sp1 = block_sum_ll<P2G_THREADS>(sp1, red);
+  sp2 = block_sum_ll<P2G_THREADS>(sp2, red);
+  const long long Dm = tm - sm, D0 = tq0 - sp0, D1 = tq1 - sp1, D2 = tq2 - sp2;
+  if (Dm != 0 || D0 != 0 || D1 != 0 || D2 != 0) {
+    // distribute the discrepancy in proportion to node mass, remainder to the heaviest node
+    long long cm = 0, c0 = 0, c1 = 0, c2 = 0;
+    long long bestv = LLONG_MIN;
+    int bestn = HN;
+    const double inv = sm > 0 ? 1.0 / (double)sm : 0.0;
+    for (int n = t; n < HN; n += P2G_THREADS) {
+      const double f = (double)hi[0][n] * inv;
+      if (hi[0][n] > bestv) {
+        bestv = hi[0][n];
+        bestn = n;
+      }
+      const long long a0 = __double2ll_rn((double)Dm * f), a1 = __double2ll_rn((double)D0 * f),
+                      a2 = __double2ll_rn((double)D1 * f), a3 = __double2ll_rn((double)D2 * f);
+      hi[0][n] += a0;
+      hi[1][n] += a1;
+      hi[2][n] += a2;
+      hi[3][n] += a3;
+      cm += a0;
+      c0 += a1;
+      c1 += a2;
+      c2 += a3;
+    }
+    cm = block_sum_ll<P2G_THREADS>(cm, red);
+    c0 = block_sum_ll<P2G_THREADS>(c0, red);
+    c1 = block_sum_ll<P2G_THREADS>(c1, red);
+    c2 = block_sum_ll<P2G_THREADS>(c2, red);
+    red[t] = bestv;
+    bestidx[t] = bestn;
+    __syncthreads();
+    if (t == 0) {
+      long long bv = LLONG_MIN;
+      int bn = 0;
+      for (int k = 0; k < P2G_THREADS; ++k)
+        if (red[k] > bv || (red[k] == bv && bestidx[k] < bn)) {
+          bv = red[k];
+          bn = bestidx[k];
+        }
+      hi[0][bn] += Dm - cm;
+      hi[1][bn] += D0 - c0;
+      hi[2][bn] += D1 - c1;
+      hi[3][bn] += D2 - c2;
+    }
+    __syncthreads();
+  }
+  // flush to the global grid
+  for (int n = t; n < HN; n += P2G_THREADS) {
+    const long long vm = hi[0][n], v0 = hi[1][n], v1 = hi[2][n], v2 = hi[3][n];
+    if ((vm | v0 | v1 | v2) == 0) continue;
+    const int hz = n % HZ, hy = (n / HZ) % HY, hx = n / (HZ * HY);
+    const int nx = tx * TX + hx, ny = ty * TY + hy, nz = tz * TZ + hz;
+    if (nx >= D.nodes[0] || ny >= D.nodes[1] || nz >= D.nodes[2]) continue;
+    const int64_t g = node_index(D, nx, ny, nz);
+    atomic_add_ll(acc + g, vm);
+    atomic_add_ll(acc + node_total + g, v0);
+    atomic_add_ll(acc + 2 * node_total + g, v1);
+    atomic_add_ll(acc + 3 * node_total + g, v2);
+  }
+}
+
+// ============================================================== wall traction
+__device__ void traction_particle(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                                  const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+                                  const float* __restrict__ st1, int64_t cap, int64_t slot,
+                                  const long long* __restrict__ acc, long long* __restrict__ trac,
+                                  int64_t node_total);
+// One thread per particle within half a cell of a face (listed while binning).
+__global__ void k_traction(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                           const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+                           const float* __restrict__ st1, int64_t cap, const uint32_t* __restrict__ nw_list,
+                           const uint32_t* __restrict__ nw_count, const long long* __restrict__ acc,
+                           long long* __restrict__ trac, int64_t node_total) {
+  const uint32_t n = *nw_count;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    traction_particle(desc, ctrl, pcta_inst, st0, st1, cap, nw_list[i], acc, trac, node_total);
+}
+
+__device__ void traction_particle(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                                  const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+                                  const float* __restrict__ st1, int64_t cap, int64_t slot,
+                                  const long long* __restrict__ acc, long long* __restrict__ trac,
+                                  int64_t node_total) {
+  const int inst = pcta_inst[slot / G2P_THREADS];
+  const Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const float* cur = c.parity ? st1 : st0;
+  const float dx = (float)D.dx;
+  const float dt = (float)c.dt;
+  const float half = 0.5f * dx;
+  const float force_scale = (float)(-c.dt * 4.0 / (D.dx * D.dx));
+  const float m = cur[C_M * cap + slot], v0 = cur[C_V0 * cap + slot];
+  float x[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) x[a] = cur[(C_X + a) * cap + slot];
+  const double s_m = D.s_mass, s_p = c.s_mom;
+  for (int axis = 0; axis < 3; ++axis) {
+    const float ext = (float)D.extent[axis];
+    float face;
+    if (x[axis] < half) face = 0.0f;
+    else if (x[axis] > ext - half) face = ext;
+    else continue;
+    float img[3] = {x[0], x[1], x[2]};
+    img[axis] = 2.0f * face - x[axis];
+    int base[3];
+    float w[3][3], d[3][3];
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float sc = scaled_of(img[a], dx);
+      const float bf = floorf(sc - 0.5f);
+      const float padded = bf + 1.0f;
+      if (!(padded >= 0.0f) || padded + 2.0f >= (float)D.nodes[a]) ok = false;
+      base[a] = (int)padded;
+      weights_of(sc - bf, dx, w[a], d[a]);
+    }
+    if (!ok) continue;
+    const int plane = face == 0.0f ? 1 : D.cells[axis] + 1;
+    const float inward = face == 0.0f ? 1.0f : -1.0f;
+    const float gax = (float)D.gravity[axis];
+    const float tau_aa = cur[(C_TAU + axis) * cap + slot];
+    const float ns = tau_aa * v0 - m * gax * (img[axis] - x[axis]);
+    if (ns >= 0.0f) continue;
+    const float wm = m * gax * dt;
+    long long* dst = trac + (int64_t)(axis + (inward > 0.f ? 0 : 3)) * node_total;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        for (int cc = 0; cc < 3; ++cc) {
+          int co[3] = {base[0] + a, base[1] + b, base[2] + cc};
+          const int ca = co[axis];
+          if (ca <= 1 || ca > D.cells[axis]) continue;
+          const float wt = w[0][a] * w[1][b] * w[2][cc];
+          if (wt == 0.0f) continue;
+          int pc[3] = {co[0], co[1], co[2]};
+          pc[axis] = plane;
+          const int64_t pi = node_index(D, pc[0], pc[1], pc[2]);
+          const long long pmf = acc[pi];
+          if (pmf <= 0) continue;
+          const float pm = (float)((double)pmf / s_m);
+          const float pp = (float)((double)acc[(1 + axis) * node_total + pi] / s_p);
+          const float trial = pp / pm + gax * dt;
+          if (trial * inward >= 0.0f) continue;
+          const int o = axis == 0 ? a : (axis == 1 ? b : cc);
+          const float dist = d[axis][o];
+          const float reaction = (ns * dist * force_scale + wm) * wt * inward;
+          if (!(reaction > 0.0f)) continue;
+          const int64_t ti = node_index(D, co[0], co[1], co[2]);
+          if (acc[ti] <= 0) continue;
+          atomic_add_ll(dst + ti, to_fixed((double)reaction, s_p));
+        }
+  }
+}
+
+// ============================================================== grid update
+__device__ __forceinline__ void reduce_tangential(float t[3], float reduction) {
+  if (reduction == 0.0f) return;
+  const float speed = sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  if (speed <= reduction) {
+    t[0] = t[1] = t[2] = 0.0f;
+  } else {
+    const float f = (speed - reduction) / speed;
+    t[0] *= f;
+    t[1] *= f;
+    t[2] *= f;
+  }
+}
+
+__global__ void __launch_bounds__(GU_THREADS)
+    k_grid_update(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                  const int* __restrict__ gcta_inst, long long* __restrict__ acc, long long* __restrict__ trac,
+                  int64_t node_total, const uint32_t* __restrict__ blk_epoch, float4* __restrict__ vel,
+                  GridPartial* __restrict__ part) {
+  __shared__ double shd[GU_THREADS];
+  __shared__ int shi[GU_THREADS];
+  const int inst = gcta_inst[blockIdx.x];
+  const Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const int t = threadIdx.x;
+  const int64_t lblk = (blockIdx.x - D.gcta_off) * GU_BLOCKS_PER_CTA + t / 64;
+  const int64_t nblk = (int64_t)D.nblk[0] * D.nblk[1] * D.nblk[2];
+  double wi0 = 0, wi1 = 0, wi2 = 0, proj = 0, fric = 0, tren = 0;
+  int fail = F_OK;
+  bool live = lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch;
+  int ni = 0, nj = 0, nk = 0;
+  if (live) {
+    const int bk = (int)(lblk % D.nblk[2]), bj = (int)((lblk / D.nblk[2]) % D.nblk[1]),
+              bi = (int)(lblk / ((int64_t)D.nblk[2] * D.nblk[1]));
+    const int l = t % 64;
+    ni = bi * NB + l / 16;
+    nj = bj * NB + (l / 4) % 4;
+    nk = bk * NB + l % 4;
+    live = ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2];
+  }
+  if (live) {
+    const int64_t g = node_index(D, ni, nj, nk);
+    const long long mf = acc[g];
+    if (mf <= 0) {
+      vel[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+      acc[g] = 0;
+      acc[node_total + g] = 0;
+      acc[2 * node_total + g] = 0;
+      acc[3 * node_total + g] = 0;
+    } else {
+      const double s_m = D.s_mass, s_p = c.s_mom;
+      const double md = (double)mf / s_m;
+      double p[3] = {(double)acc[node_total + g] / s_p, (double)acc[2 * node_total + g] / s_p,
+                     (double)acc[3 * node_total + g] / s_p};
+      acc[g] = 0;
+      acc[node_total + g] = 0;
+      acc[2 * node_total + g] = 0;
+      acc[3 * node_total + g] = 0;
+      const int co[3] = {ni, nj, nk};
+      float Tl[3] = {0.f, 0.f, 0.f}, Th[3] = {0.f, 0.f, 0.f};
+      bool shell = false;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (co[a] == 2 || co[a] == 3 || co[a] == D.cells[a] - 1 || co[a] == D.cells[a]) shell = true;
+      if (shell) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const long long l = trac[(int64_t)a * node_total + g], h = trac[(int64_t)(a + 3) * node_total + g];
+          if (l | h) {
+            trac[(int64_t)a * node_total + g] = 0;
+            trac[(int64_t)(a + 3) * node_total + g] = 0;
+            const double dl = (double)l / s_p, dh = (double)h / s_p;
+            const double S = dl - dh;
+            // telescoped kinetic-energy jump of the reaction deposits (grid.rs:279-295)
+            tren += S * (p[a] / md + S / (2.0 * md));
+            if (a == 0) wi0 += S;
+            if (a == 1) wi1 += S;
+            if (a == 2) wi2 += S;
+            p[a] += S;
+            Tl[a] = (float)dl;
+            Th[a] = (float)dh;
+          }
+        }
+      }
+      const float m = (float)md;
+      const float dt = (float)c.dt;
+      float v[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) v[a] = (float)p[a] / m + (float)D.gravity[a] * dt;
+      if (!(isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]))) {
+        fail = F_GRID_NONFINITE;
+        vel[g] = make_float4(0.f, 0.f, 0.f, m);
+      } else {
+        const float before[3] = {v[0], v[1], v[2]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          float sign = 0.0f;
+          if (co[a] <= 1) sign = 1.0f;
+          else if (co[a] > D.cells[a]) sign = -1.0f;
+          if (sign == 0.0f) continue;
+          const float nsp = v[a] * sign;
+          if (nsp >= 0.0f) continue;
+          proj -= 0.5 * (double)m * (double)nsp * (double)nsp;
+          v[a] = 0.0f;
+          const float t0 = v[0], t1 = v[1], t2 = v[2];
+          const int face = 2 * a + (sign > 0.f ? 0 : 1);
+          if (D.face_mode && D.face_sticky[face]) {
+            v[0] = v[1] = v[2] = 0.0f;
+          } else {
+            const float mu = D.face_mode ? (float)D.face_mu[face] : (float)D.friction;
+            reduce_tangential(v, mu * (-nsp));
+          }
+          fric += 0.5 * (double)m *
+                  ((double)(t0 * t0 + t1 * t1 + t2 * t2) - (double)(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float R = Tl[a] + Th[a];
+          if (!(R > 0.0f)) continue;
+          const float normal = v[a];
+          float tg[3] = {v[0], v[1], v[2]};
+          tg[a] = 0.0f;
+          const double t2b = (double)(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]);
+          if (D.face_mode) {
+            const bool stick = (Tl[a] > 0.f && D.face_sticky[2 * a]) || (Th[a] > 0.f && D.face_sticky[2 * a + 1]);
+            if (stick) tg[0] = tg[1] = tg[2] = 0.0f;
+            else reduce_tangential(tg, ((float)D.face_mu[2 * a] * Tl[a] + (float)D.face_mu[2 * a + 1] * Th[a]) / m);
+          } else {
+            reduce_tangential(tg, (float)D.friction * R / m);
+          }
+          fric += 0.5 * (double)m * (t2b - (double)(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]));
+          v[0] = tg[0];
+          v[1] = tg[1];
+          v[2] = tg[2];
+          v[a] = normal;
+        }
+        wi0 += (double)(v[0] - before[0]) * (double)m;
+        wi1 += (double)(v[1] - before[1]) * (double)m;
+        wi2 += (double)(v[2] - before[2]) * (double)m;
+        vel[g] = make_float4(v[0], v[1], v[2], m);
+      }
+    }
+  }
+  wi0 = block_sum_d<GU_THREADS>(wi0, shd);
+  wi1 = block_sum_d<GU_THREADS>(wi1, shd);
+  wi2 = block_sum_d<GU_THREADS>(wi2, shd);
+  proj = block_sum_d<GU_THREADS>(proj, shd);
+  fric = block_sum_d<GU_THREADS>(fric, shd);
+  tren = block_sum_d<GU_THREADS>(tren, shd);
+  fail = block_max_i<GU_THREADS>(fail, shi);
+  if (t == 0) {
+    GridPartial& P = part[blockIdx.x];
+    P.wall_impulse[0] = wi0;
+    P.wall_impulse[1] = wi1;
+    P.wall_impulse[2] = wi2;
+    P.proj = proj;
+    P.fric = fric;
+    P.trac = tren;
+    P.fail = fail;
+  }
+}
+
+// ============================================================== pellet (FP64 rigid body)
+struct Q4 {
+  double i, j, k, w;
+};
+__device__ inline void qmat(const double* q, double R[3][3]) {
+  const double i = q[0], j = q[1], k = q[2], w = q[3];
+  const double ww = w * w, ii = i * i, jj = j * j, kk = k * k;
+  const double ij = i * j * 2.0, wk = w * k * 2.0, wj = w * j * 2.0, ik = i * k * 2.0, jk = j * k * 2.0,
+               wi = w * i * 2.0;
+  R[0][0] = ww + ii - jj - kk;
+  R[0][1] = ij - wk;
+  R[0][2] = wj + ik;
+  R[1][0] = wk + ij;
+  R[1][1] = ww - ii + jj - kk;
+  R[1][2] = jk - wi;
+  R[2][0] = ik - wj;
+  R[2][1] = wi + jk;
+  R[2][2] = ww - ii - jj + kk;
+}
+__device__ inline void cross3(const double* a, const double* b, double* o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ inline void qrotv(const double* q, const double* r, double* o) {
+  double qv[3] = {q[0], q[1], q[2]}, t[3], cc[3];
+  cross3(qv, r, t);
+  t[0] *= 2.0;
+  t[1] *= 2.0;
+  t[2] *= 2.0;
+  cross3(qv, t, cc);
+  for (int a = 0; a < 3; ++a) o[a] = t[a] * q[3] + cc[a] + r[a];
+}
+__device__ inline void pellet_omega(const PelletState& P, double* om) {
+  double R[3][3];
+  qmat(P.q, R);
+  double bm[3], bo[3];
+  for (int a = 0; a < 3; ++a) bm[a] = R[0][a] * P.L[0] + R[1][a] * P.L[1] + R[2][a] * P.L[2];
+  for (int a = 0; a < 3; ++a) bo[a] = bm[a] / P.inertia[a];
+  for (int a = 0; a < 3; ++a) om[a] = R[a][0] * bo[0] + R[a][1] * bo[1] + R[a][2] * bo[2];
+}
+__device__ inline double pellet_ke(const PelletState& P) {
+  double om[3];
+  pellet_omega(P, om);
+  return 0.5 * P.mass * (P.vel[0] * P.vel[0] + P.vel[1] * P.vel[1] + P.vel[2] * P.vel[2]) +
+         0.5 * (om[0] * P.L[0] + om[1] * P.L[1] + om[2] * P.L[2]);
+}
+// rigid.rs:279-334
+__device__ inline void pellet_integrate(PelletState& P, double dt, const double* g, const double* ext, double k,
+                                        double e, double mu, double* impulse_out, double* work_out) {
+  double zeta;
+  if (e <= 0.0) zeta = 1.0;
+  else if (e >= 1.0) zeta = 0.0;
+  else {
+    const double lg = log(e);
+    zeta = -lg / sqrt(3.14159265358979323846 * 3.14159265358979323846 + lg * lg);
+  }
+  const double damping = 2.0 * zeta * sqrt(k * P.mass);
+  double force[3] = {0, 0, 0}, torque[3] = {0, 0, 0}, work = 0.0;
+  double om[3];
+  pellet_omega(P, om);
+  double ax[3];
+  const double ex[3] = {1.0, 0.0, 0.0};
+  qrotv(P.q, ex, ax);
+  for (int s = 0; s < P.nsph; ++s) {
+    double cen[3];
+    for (int a = 0; a < 3; ++a) cen[a] = P.pos[a] + ax[a] * P.off[s];
+    for (int axis = 0; axis < 3; ++axis) {
+      for (int f = 0; f < 2; ++f) {
+        const double fp = f == 0 ? 0.0 : ext[axis], sign = f == 0 ? 1.0 : -1.0;
+        const double gap = (cen[axis] - fp) * sign;
+        const double pen = P.radius - gap;
+        if (pen <= 0.0) continue;
+        double normal[3] = {0, 0, 0};
+        normal[axis] = sign;
+        double cp[3], lever[3], tmp[3], pv[3];
+        for (int a = 0; a < 3; ++a) cp[a] = cen[a] - normal[a] * P.radius;
+        for (int a = 0; a < 3; ++a) lever[a] = cp[a] - P.pos[a];
+        cross3(om, lever, tmp);
+        for (int a = 0; a < 3; ++a) pv[a] = P.vel[a] + tmp[a];
+        const double ns = pv[0] * normal[0] + pv[1] * normal[1] + pv[2] * normal[2];
+        const double nf = fmax(k * pen - damping * ns, 0.0);
+        double tg[3];
+        for (int a = 0; a < 3; ++a) tg[a] = pv[a] - normal[a] * ns;
+        const double ts = sqrt(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]);
+        double ff[3] = {0, 0, 0};
+        if (ts > 1e-12) {
+          const double limit = fmin(mu * nf, P.mass * ts / dt);
+          for (int a = 0; a < 3; ++a) ff[a] = -tg[a] / ts * limit;
+        }
+        double total[3];
+        for (int a = 0; a < 3; ++a) total[a] = normal[a] * nf + ff[a];
+        for (int a = 0; a < 3; ++a) force[a] += total[a];
+        cross3(lever, total, tmp);
+        for (int a = 0; a < 3; ++a) torque[a] += tmp[a];
+        work += (total[0] * pv[0] + total[1] * pv[1] + total[2] * pv[2]) * dt;
+      }
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    impulse_out[a] = force[a] * dt;
+    P.vel[a] = P.vel[a] + (g[a] * dt + impulse_out[a] / P.mass);
+  }
+  for (int a = 0; a < 3; ++a) P.L[a] += torque[a] * dt;
+  for (int a = 0; a < 3; ++a) P.pos[a] += P.vel[a] * dt;
+  double on[3];
+  pellet_omega(P, on);
+  double h[3] = {on[0] * dt / 2.0, on[1] * dt / 2.0, on[2] * dt / 2.0};
+  const double nn = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+  const double eps = 2.220446049250313e-16;
+  double inc[4] = {0, 0, 0, 1};
+  if (!(nn <= eps * eps)) {
+    const double n = sqrt(nn);
+    const double f = 1.0 * sin(n) / n;
+    inc[0] = h[0] * f;
+    inc[1] = h[1] * f;
+    inc[2] = h[2] * f;
+    inc[3] = cos(n);
+  }
+  const double* b = P.q;
+  double r[4];
+  r[0] = inc[3] * b[0] + inc[0] * b[3] + inc[1] * b[2] - inc[2] * b[1];
+  r[1] = inc[3] * b[1] - inc[0] * b[2] + inc[1] * b[3] + inc[2] * b[0];
+  r[2] = inc[3] * b[2] + inc[0] * b[1] - inc[1] * b[0] + inc[2] * b[3];
+  r[3] = inc[3] * b[3] - inc[0] * b[0] - inc[1] * b[1] - inc[2] * b[2];
+  for (int a = 0; a < 4; ++a) P.q[a] = r[a];
+  *work_out = work;
+}
+
+// One CTA per instance that has a pellet: constrain grid nodes inside the pellet against its
+// (start-of-step) surface velocity, reduce the equal and opposite impulses in FP64, then apply
+// them and integrate the pellet (the trial state is committed by k_end on acceptance).
+__global__ void k_couple(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
+                         const uint32_t* __restrict__ blk_epoch, float4* __restrict__ vel) {
+  __shared__ double shd[256];
+  const int inst = blockIdx.x;
+  Control& c = ctrl[inst];
+  const InstDesc& D = desc[inst];
+  if (!c.active || !D.has_pellet) return;
+  const PelletState& P = c.pellet;
+  double ax[3];
+  const double ex[3] = {1.0, 0.0, 0.0};
+  qrotv(P.q, ex, ax);
+  double hs = 0.0;
+  for (int s = 0; s < P.nsph; ++s) hs = fmax(hs, fabs(P.off[s]));
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    const double reach = fabs(ax[a]) * hs + P.radius;
+    lo[a] = P.pos[a] - reach;
+    hi[a] = P.pos[a] + reach;
+  }
+  int i0[3], n[3];
+  for (int a = 0; a < 3; ++a) {
+    int a0 = (int)floor(lo[a] / D.dx + 1.0) - 1, a1 = (int)ceil(hi[a] / D.dx + 1.0) + 1;
+    a0 = a0 < 0 ? 0 : a0;
+    a1 = a1 > D.nodes[a] - 1 ? D.nodes[a] - 1 : a1;
+    i0[a] = a0;
+    n[a] = a1 >= a0 ? a1 - a0 + 1 : 0;
+  }
+  double om[3];
+  pellet_omega(P, om);
+  double imp[3] = {0, 0, 0}, ang[3] = {0, 0, 0}, energy = 0.0;
+  const int64_t total = (int64_t)n[0] * n[1] * n[2];
+  for (int64_t l = threadIdx.x; l < total; l += blockDim.x) {
+    const int k = i0[2] + (int)(l % n[2]);
+    const int j = i0[1] + (int)((l / n[2]) % n[1]);
+    const int i = i0[0] + (int)(l / ((int64_t)n[2] * n[1]));
+    const int64_t blk = D.blk_off + ((int64_t)(i / NB) * D.nblk[1] + j / NB) * D.nblk[2] + k / NB;
+    if (blk_epoch[blk] != (uint32_t)c.epoch) continue;
+    const int64_t g = node_index(D, i, j, k);
+    const float4 nv = vel[g];
+    const double mass = nv.w;
+    if (!(mass > 0.0)) continue;
+    const double node[3] = {((double)i - 1.0) * D.dx, ((double)j - 1.0) * D.dx, ((double)k - 1.0) * D.dx};
+    bool outside = false;
+    for (int a = 0; a < 3; ++a)
+      if (node[a] < lo[a] || node[a] > hi[a]) outside = true;
+    if (outside) continue;
+    double best = 1e300, normal[3] = {0, 0, 1};
+    for (int s = 0; s < P.nsph; ++s) {
+      double d[3];
+      for (int a = 0; a < 3; ++a) d[a] = node[a] - (P.pos[a] + ax[a] * P.off[s]);
+      const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      const double phi = dist - P.radius;
+      if (phi < best) {
+        best = phi;
+        if (dist > 1e-12) {
+          normal[0] = d[0] / dist;
+          normal[1] = d[1] / dist;
+          normal[2] = d[2] / dist;
+        } else {
+          normal[0] = 0;
+          normal[1] = 0;
+          normal[2] = 1;
+        }
+      }
+    }
+    if (best > 0.0) continue;
+    double lever[3], tmp[3], bv[3];
+    for (int a = 0; a < 3; ++a) lever[a] = node[a] - P.pos[a];
+    cross3(om, lever, tmp);
+    for (int a = 0; a < 3; ++a) bv[a] = P.vel[a] + tmp[a];
+    const double v[3] = {nv.x, nv.y, nv.z};
+    double rel[3];
+    for (int a = 0; a < 3; ++a) rel[a] = v[a] - bv[a];
+    const double nsp = rel[0] * normal[0] + rel[1] * normal[1] + rel[2] * normal[2];
+    if (nsp >= 0.0) continue;
+    double tg[3];
+    for (int a = 0; a < 3; ++a) tg[a] = rel[a] - normal[a] * nsp;
+    const double ts = sqrt(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]);
+    const double fr = D.friction * (-nsp);
+    double tn[3] = {0, 0, 0};
+    if (!(ts <= fr || ts < 1e-14))
+      for (int a = 0; a < 3; ++a) tn[a] = tg[a] * ((ts - fr) / ts);
+    double nvv[3], dp[3];
+    for (int a = 0; a < 3; ++a) {
+      nvv[a] = bv[a] + tn[a];
+      dp[a] = (nvv[a] - v[a]) * mass;
+    }
+    energy += 0.5 * mass * ((nvv[0] * nvv[0] + nvv[1] * nvv[1] + nvv[2] * nvv[2]) - (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    double lx[3];
+    cross3(lever, dp, lx);
+    for (int a = 0; a < 3; ++a) {
+      imp[a] -= dp[a];
+      ang[a] -= lx[a];
+    }
+    vel[g] = make_float4((float)nvv[0], (float)nvv[1], (float)nvv[2], nv.w);
+  }
+  for (int a = 0; a < 3; ++a) imp[a] = block_sum_d<256>(imp[a], shd);
+  for (int a = 0; a < 3; ++a) ang[a] = block_sum_d<256>(ang[a], shd);
+  energy = block_sum_d<256>(energy, shd);
+  if (threadIdx.x == 0) {
+    PelletState T = P;
+    const double kb = pellet_ke(T);
+    for (int a = 0; a < 3; ++a) {
+      T.vel[a] += imp[a] / T.mass;
+      T.L[a] += ang[a];
+    }
+    const double pe = pellet_ke(T) - kb;
+    double wimp[3], work;
+    pellet_integrate(T, c.dt, D.gravity, D.extent, D.contact_k, D.contact_e, D.contact_mu, wimp, &work);
+    bool finite = isfinite(pe);
+    for (int a = 0; a < 3; ++a)
+      finite = finite && isfinite(T.pos[a]) && isfinite(T.vel[a]) && isfinite(T.L[a]);
+    for (int a = 0; a < 4; ++a) finite = finite && isfinite(T.q[a]);
+    c.pellet_trial = T;
+    for (int a = 0; a < 3; ++a) {
+      c.c_impulse[a] = imp[a];
+      c.c_angular[a] = ang[a];
+      c.pw_impulse[a] = wimp[a];
+    }
+    c.c_grid_energy = energy;
+    c.c_pellet_energy = pe;
+    c.pw_work = work;
+    c.pellet_fail = finite ? 0 : 1;
+  }
+}
+
+// ============================================================== G2P + constitutive
+__global__ void __launch_bounds__(G2P_THREADS)
+    k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ pcta_inst,
+          float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
+          int64_t cap, const uint32_t* __restrict__ perm, const float4* __restrict__ vel,
+          ParticlePartial* __restrict__ part, const float* __restrict__ mlp, float* __restrict__ log_x,
+          float* __restrict__ log_y, unsigned long long* __restrict__ log_n, long long log_cap) {
+  __shared__ double shd[G2P_THREADS];
+  __shared__ float shf[G2P_THREADS];
+  __shared__ int shi[G2P_THREADS];
+  __shared__ long long shl[G2P_THREADS];
+  const int inst = pcta_inst[blockIdx.x];
+  const Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const int64_t k = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
+  const int64_t valid_n = c.count - c.outflow;
+  double diss = 0.0, bb = 0.0, mass_sum = 0.0;
+  float max_speed = 0.0f, max_disp = 0.0f;
+  int fail = F_OK, iters = 0, yielded = 0;
+  double fail_value = 0.0;
+  if (k - D.slot_off < valid_n) {
+    const int64_t src = perm[k];
+    const float* cur = c.parity ? st1 : st0;
+    float* nxt = c.parity ? st0 : st1;
+    const uint32_t* idc = c.parity ? id1 : id0;
+    uint32_t* idn = c.parity ? id0 : id1;
+    const float dx = (float)D.dx;
+    const float dt = (float)c.dt;
+    float x[3];
+    int base[3];
+    float w[3][3], d[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      x[a] = cur[(C_X + a) * cap + src];
+      const float sc = scaled_of(x[a], dx);
+      const float bf = floorf(sc - 0.5f);
+      base[a] = (int)(bf + 1.0f);
+      weights_of(sc - bf, dx, w[a], d[a]);
+    }
+    float v[3] = {0.f, 0.f, 0.f};
+    float Cm[9];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) Cm[a] = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const int64_t row = node_index(D, base[0] + a, base[1] + b, base[2]);
+        const float wab = w[0][a] * w[1][b];
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const float4 nv = __ldg(&vel[row + cc]);
+          const float ww = wab * w[2][cc];
+          const float vx = nv.x * ww, vy = nv.y * ww, vz = nv.z * ww;
+          v[0] += vx;
+          v[1] += vy;
+          v[2] += vz;
+          const float dd[3] = {d[0][a], d[1][b], d[2][cc]};
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            Cm[0 * 3 + j] += vx * dd[j];
+            Cm[1 * 3 + j] += vy * dd[j];
+            Cm[2 * 3 + j] += vz * dd[j];
+          }
+        }
+      }
+    const float dx2_inv = 4.0f / (dx * dx);
+#pragma unroll
+    for (int a = 0; a < 9; ++a) Cm[a] *= dx2_inv;
+    const float speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const float disp = speed * dt / dx;
+    const float m = cur[C_M * cap + src];
+    const float v0 = cur[C_V0 * cap + src];
+    float tau[6];
+    float Hn[9];
+    float jm1n = 0.0f;
+    float ep = cur[C_EP * cap + src];
+    if (D.kind == 0) {
+      float H[9], Htr[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) H[a] = cur[(C_H + a) * cap + src];
+      // H_tr = H + dt C + dt C H
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const float ch = Cm[3 * i + 0] * H[0 * 3 + j] + Cm[3 * i + 1] * H[1 * 3 + j] + Cm[3 * i + 2] * H[2 * 3 + j];
+          Htr[3 * i + j] = H[3 * i + j] + dt * (Cm[3 * i + j] + ch);
+        }
+      const double ys = D.per_particle_yield ? (double)cur[C_YS * cap + src] : D.yield;
+      PasteOut o;
+      paste_update(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, D.consistency, D.flow_index, c.dt, D.tol,
+                   c.warm_start ? mlp : nullptr, o);
+      if (o.fail != F_OK) {
+        fail = o.fail;
+        fail_value = o.eq;
+      }
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Hn[a] = o.H[a];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
+      ep += (float)o.dep;
+      diss = o.diss_density * (double)v0;
+      iters = o.iters;
+      yielded = o.yielded;
+      if (log_n != nullptr && o.yielded && o.fail == F_OK) {
+        const unsigned long long slot = atomicAdd(log_n, 1ull);
+        if ((long long)slot < log_cap) {
+          // (trial stress, yield, consistency, flow index, mu, dt) -> returned stress
+          log_x[6 * slot + 0] = (float)o.trial;
+          log_x[6 * slot + 1] = (float)ys;
+          log_x[6 * slot + 2] = (float)D.consistency;
+          log_x[6 * slot + 3] = (float)D.flow_index;
+          log_x[6 * slot + 4] = (float)D.mu;
+          log_x[6 * slot + 5] = (float)c.dt;
+          log_y[slot] = (float)o.eq;
+        }
+      }
+    } else {
+      const float jm1 = cur[C_JM1 * cap + src];
+      LiquidOut o;
+      liquid_update(jm1, Cm, (float)D.bulk, (float)D.consistency, (float)D.tait_gamma, dt, o);
+      if (o.fail != F_OK) fail = o.fail;
+#pragma unroll
+      for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
+      jm1n = o.jm1;
+    }
+    // write the trial state in sorted slot order
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      nxt[(C_X + a) * cap + k] = x[a] + v[a] * dt;
+      nxt[(C_V + a) * cap + k] = v[a];
+    }
+#pragma unroll
+    for (int a = 0; a < 9; ++a) nxt[(C_C + a) * cap + k] = Cm[a];
+    if (D.kind == 0) {
+#pragma unroll
+      for (int a = 0; a < 9; ++a) nxt[(C_H + a) * cap + k] = Hn[a];
+    } else {
+      nxt[C_JM1 * cap + k] = jm1n;
+    }
+#pragma unroll
+    for (int a = 0; a < 6; ++a) nxt[(C_TAU + a) * cap + k] = tau[a];
+    nxt[C_EP * cap + k] = ep;
+    nxt[C_M * cap + k] = m;
+    nxt[C_V0 * cap + k] = v0;
+    if (D.per_particle_yield) nxt[C_YS * cap + k] = cur[C_YS * cap + src];
+    idn[k] = idc[src];
+    // momentum bound of the new state for the next attempt's fixed-point scale
+    const double mm = m;
+    const double cn = sqrt((double)(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] +
+                                    Cm[5] * Cm[5] + Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]));
+    const double tn = sqrt((double)(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]) +
+                           2.0 * (double)(tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]));
+    const double gn = sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]);
+    bb = mm * (double)speed + (cn * mm + tn * D.max_dt * 4.0 * (double)v0 / (D.dx * D.dx)) * 2.6 * D.dx +
+         6.0 * mm * gn * D.max_dt;
+    mass_sum = mm;
+    max_speed = speed;
+    max_disp = disp;
+  }
+  diss = block_sum_d<G2P_THREADS>(diss, shd);
+  bb = block_sum_d<G2P_THREADS>(bb, shd);
+  mass_sum = block_sum_d<G2P_THREADS>(mass_sum, shd);
+  max_speed = block_max_f<G2P_THREADS>(max_speed, shf);
+  max_disp = block_max_f<G2P_THREADS>(max_disp, shf);
+  const int fail_all = block_max_i<G2P_THREADS>(fail, shi);
+  const long long it_all = block_sum_ll<G2P_THREADS>(iters, shl);
+  const long long y_all = block_sum_ll<G2P_THREADS>(yielded, shl);
+  if (threadIdx.x == 0) {
+    ParticlePartial& P = part[blockIdx.x];
+    P.diss = diss;
+    P.bbound = bb;
+    P.mass = mass_sum;
+    P.max_speed = max_speed;
+    P.max_disp = max_disp;
+    P.fail = fail_all;
+    P.iterations = (int)it_all;
+    P.yielded = (int)y_all;
+    P.fail_value = fail_value;
+  }
+}
+
+// ============================================================== end of attempt
+__global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
+                      const GridPartial* __restrict__ gpart, const ParticlePartial* __restrict__ ppart) {
+  __shared__ double shd[256];
+  __shared__ float shf[256];
+  __shared__ int shi[256];
+  __shared__ long long shl[256];
+  const int inst = blockIdx.x;
+  Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const int t = threadIdx.x;
+  // fixed-order reductions
+  double wi[3] = {0, 0, 0}, proj = 0, fric = 0, trac = 0;
+  int fail = F_OK;
+  for (int64_t j = t; j < D.gcta_cnt; j += 256) {
+    const GridPartial& P = gpart[D.gcta_off + j];
+    // CTAs with no live block did not write; their entries were zeroed by the host at creation
+    wi[0] += P.wall_impulse[0];
+    wi[1] += P.wall_impulse[1];
+    wi[2] += P.wall_impulse[2];
+    proj += P.proj;
+    fric += P.fric;
+    trac += P.trac;
+    fail = max(fail, P.fail);
+  }
+  double diss = 0, bb = 0;
+  float ms = 0.f, md = 0.f;
+  long long its = 0, yl = 0;
+  int pfail = F_OK;
+  for (int64_t j = t; j < D.pcta_cnt; j += 256) {
+    const ParticlePartial& P = ppart[D.pcta_off + j];
+    diss += P.diss;
+    bb += P.bbound;
+    ms = fmaxf(ms, P.max_speed);
+    md = fmaxf(md, P.max_disp);
+    pfail = max(pfail, P.fail);
+    its += P.iterations;
+    yl += P.yielded;
+  }
+  for (int a = 0; a < 3; ++a) wi[a] = block_sum_d<256>(wi[a], shd);
+  proj = block_sum_d<256>(proj, shd);
+  fric = block_sum_d<256>(fric, shd);
+  trac = block_sum_d<256>(trac, shd);
+  diss = block_sum_d<256>(diss, shd);
+  bb = block_sum_d<256>(bb, shd);
+  ms = block_max_f<256>(ms, shf);
+  md = block_max_f<256>(md, shf);
+  fail = block_max_i<256>(fail, shi);
+  pfail = block_max_i<256>(pfail, shi);
+  its = block_sum_ll<256>(its, shl);
+  yl = block_sum_ll<256>(yl, shl);
+  if (t != 0) return;
+  int f = F_OK;
+  if (!isfinite(trac) || !isfinite(c.ledger.trac + trac)) f = F_TRACTION_NONFINITE;
+  else if (fail != F_OK) f = fail;
+  else if (D.has_pellet && c.pellet_fail) f = F_PELLET_NONFINITE;
+  else if (pfail != F_OK) f = pfail;
+  else if (md > 1.0f) f = F_DISPLACEMENT;
+  else if (c.outflow > 0) f = F_OUTFLOW;
+  const bool forced = c.forced_dt > 0.0;
+  if (f != F_OK) {
+    c.fail = f;
+    c.last_fail = f;
+    c.fail_value = f == F_DISPLACEMENT ? (double)md : 0.0;
+    if (f == F_OUTFLOW) {
+      c.status = S_ERROR;
+      return;
+    }
+    if (!forced) {
+      c.rejected_steps += 1;
+      c.dt_scale *= 0.5;
+      if (c.dt_scale * c.limit < D.min_dt) c.status = S_MIN_STEP;
+    }
+    return;
+  }
+  // commit (solver.rs:980-998 + pellet ledger of try_step_captured)
+  const double dt = c.dt;
+  c.parity ^= 1;
+  LedgerD& L = c.ledger;
+  L.plastic += diss;
+  for (int a = 0; a < 3; ++a) L.wall_impulse[a] += wi[a];
+  L.proj += proj;
+  L.fric += fric;
+  L.trac += trac;
+  for (int a = 0; a < 3; ++a) L.gravity_impulse[a] += D.gravity[a] * (c.total_mass * dt);
+  if (D.has_pellet) {
+    for (int a = 0; a < 3; ++a) {
+      L.gravity_impulse[a] += D.gravity[a] * (c.pellet_trial.mass * dt);
+      L.pellet_wall_impulse[a] += c.pw_impulse[a];
+      L.coupling_impulse[a] += c.c_impulse[a];
+      L.coupling_angular[a] += c.c_angular[a];
+    }
+    L.pellet_work += c.pw_work;
+    L.cgrid += c.c_grid_energy;
+    L.cpellet += c.c_pellet_energy;
+    c.pellet = c.pellet_trial;
+  }
+  c.max_speed = ms;
+  c.bbound = bb;
+  c.newton_iterations += (uint64_t)its;
+  c.yielded = (uint64_t)yl;
+  if (!forced) {
+    c.time += dt;
+    c.step_count += 1;
+    c.limited_steps += (uint64_t)c.limited;
+    c.min_dt_used = fmin(c.min_dt_used, dt);
+    c.max_dt_used = fmax(c.max_dt_used, dt);
+    c.dt_scale = fmin(c.dt_scale * 1.25, 1.0);
+    if (!(c.time < c.target)) {
+      c.time = c.target;
+      c.status = S_REACHED;
+    }
+  }
+}
+
+// ============================================================== setup / diagnostics
+// Committed-state reductions: max speed and the momentum bound (used by k_begin), FP64.
+__global__ void k_state_stats(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                              const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+                              const float* __restrict__ st1, int64_t cap, ParticlePartial* __restrict__ part) {
+  __shared__ double shd[G2P_THREADS];
+  __shared__ float shf[G2P_THREADS];
+  const int inst = pcta_inst[blockIdx.x];
+  const Control& c = ctrl[inst];
+  const InstDesc& D = desc[inst];
+  const int64_t k = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
+  double bb = 0.0, ms = 0.0;
+  float sp = 0.0f;
+  if (k - D.slot_off < c.count) {
+    const float* cur = c.parity ? st1 : st0;
+    float v[3], Cm[9], tau[6];
+    for (int a = 0; a < 3; ++a) v[a] = cur[(C_V + a) * cap + k];
+    for (int a = 0; a < 9; ++a) Cm[a] = cur[(C_C + a) * cap + k];
+    for (int a = 0; a < 6; ++a) tau[a] = cur[(C_TAU + a) * cap + k];
+    const double m = cur[C_M * cap + k], v0 = cur[C_V0 * cap + k];
+    // speed in FP64 from the FP32 components
+    const double speed = sqrt((double)v[0] * v[0] + (double)v[1] * v[1] + (double)v[2] * v[2]);
+    double cn = 0, tn = 0;
+    for (int a = 0; a < 9; ++a) cn += (double)Cm[a] * Cm[a];
+    for (int a = 0; a < 3; ++a) tn += (double)tau[a] * tau[a];
+    for (int a = 3; a < 6; ++a) tn += 2.0 * (double)tau[a] * tau[a];
+    const double gn = sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]);
+    bb = m * speed + (sqrt(cn) * m + sqrt(tn) * D.max_dt * 4.0 * v0 / (D.dx * D.dx)) * 2.6 * D.dx +
+         6.0 * m * gn * D.max_dt;
+    sp = (float)speed;
+    ms = m;
+  }
+  bb = block_sum_d<G2P_THREADS>(bb, shd);
+  ms = block_sum_d<G2P_THREADS>(ms, shd);
+  sp = block_max_f<G2P_THREADS>(sp, shf);
+  if (threadIdx.x == 0) {
+    ParticlePartial& P = part[blockIdx.x];
+    P.bbound = bb;
+    P.mass = ms;
+    P.max_speed = sp;
+    P.diss = 0.0;
+    P.max_disp = 0.f;
+    P.fail = 0;
+    P.iterations = 0;
+    P.yielded = 0;
+  }
+}
+
+// Energies and observables of the committed state (FP64 partials per CTA).
+// out per CTA (DIAG_N doubles): ke, pe, ee, mass, mom xyz, max speed, max ep, yielded count,
+// min x, max x, min y, max y, max z, hydro sum sq, hydro max, column height (dam break)
+__global__ void k_diagnostics(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                              const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+                              const float* __restrict__ st1, int64_t cap, int fixture_hydro, double h0,
+                              int fixture_dam, double* __restrict__ out) {
+  __shared__ double shd[G2P_THREADS];
+  const int inst = pcta_inst[blockIdx.x];
+  const Control& c = ctrl[inst];
+  const InstDesc& D = desc[inst];
+  const int64_t k = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
+  double vals[DIAG_N];
+  for (int j = 0; j < DIAG_N; ++j) vals[j] = 0.0;
+  vals[9] = 1e300;
+  vals[10] = -1e300;
+  vals[11] = 1e300;
+  vals[12] = -1e300;
+  vals[13] = -1e300;
+  if (k - D.slot_off < c.count) {
+    const float* cur = c.parity ? st1 : st0;
+    double x[3], v[3];
+    for (int a = 0; a < 3; ++a) {
+      x[a] = cur[(C_X + a) * cap + k];
+      v[a] = cur[(C_V + a) * cap + k];
+    }
+    const double m = cur[C_M * cap + k], v0 = cur[C_V0 * cap + k];
+    const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    vals[0] = 0.5 * m * v2;
+    vals[1] = -m * (D.gravity[0] * x[0] + D.gravity[1] * x[1] + D.gravity[2] * x[2]);
+    if (D.kind == 0) {
+      float Hh[9];
+      for (int a = 0; a < 9; ++a) Hh[a] = cur[(C_H + a) * cap + k];
+      double B[3][3], U[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          double hh = (double)Hh[3 * i] * Hh[3 * j] + (double)Hh[3 * i + 1] * Hh[3 * j + 1] +
+                      (double)Hh[3 * i + 2] * Hh[3 * j + 2];
+          B[i][j] = (double)Hh[3 * i + j] + (double)Hh[3 * j + i] + hh;
+        }
+      double e = 0.0;
+      if (jacobi3<double>(B, U, 64, 1e-30)) {
+        double h[3], tr = 0.0, n2 = 0.0;
+        for (int a = 0; a < 3; ++a) {
+          h[a] = 0.5 * log1p(fmax(B[a][a], -1.0 + 1e-300));
+          tr += h[a];
+          n2 += h[a] * h[a];
+        }
+        e = v0 * (D.mu * n2 + 0.5 * D.lambda * tr * tr);
+      } else {
+        e = nan("");
+      }
+      vals[2] = e;
+    } else {
+      const double jm1 = cur[C_JM1 * cap + k];
+      const double j = 1.0 + jm1;
+      vals[2] = v0 * D.bulk * (jm1 - log1p(jm1));
+      (void)j;
+    }
+    vals[3] = m;
+    vals[4] = m * v[0];
+    vals[5] = m * v[1];
+    vals[6] = m * v[2];
+    vals[7] = sqrt(v2);
+    const double ep = cur[C_EP * cap + k];
+    vals[8] = ep;
+    vals[14] = ep > 0.0 ? 1.0 : 0.0;
+    vals[9] = x[0];
+    vals[10] = x[0];
+    vals[11] = x[1];
+    vals[12] = x[1];
+    vals[13] = x[2];
+    if (fixture_hydro) {
+      const double g = sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]);
+      const double depth = fmax(h0 - x[2], 0.0);
+      double ref, meas;
+      if (D.kind == 1) {
+        ref = D.bulk * expm1(D.density * g * depth / D.bulk);
+        const double jm1 = cur[C_JM1 * cap + k];
+        meas = D.tait_gamma == 1.0 ? -D.bulk * jm1 / (1.0 + jm1) : D.bulk / D.tait_gamma * expm1(-D.tait_gamma * log1p(jm1));
+      } else {
+        ref = D.density * g * depth;
+        meas = -(double)cur[(C_TAU + 2) * cap + k];
+      }
+      const double scale = D.density * g * h0;
+      const double er = (meas - ref) / scale;
+      vals[15] = er * er;
+      vals[16] = fabs(er);
+    }
+    if (fixture_dam && x[0] < D.dx) vals[17] = x[2];
+    else vals[17] = -1e300;
+  } else {
+    vals[17] = -1e300;
+  }
+  // reduce: sums 0-6, 14, 15; max 7, 8, 10, 12, 13, 16, 17; min 9, 11
+  for (int j = 0; j < DIAG_N; ++j) {
+    const int t = threadIdx.x;
+    shd[t] = vals[j];
+    __syncthreads();
+    for (int s = G2P_THREADS / 2; s > 0; s >>= 1) {
+      if (t < s) {
+        const double a = shd[t], b = shd[t + s];
+        double r;
+        if (j <= 6 || j == 14 || j == 15) r = a + b;
+        else if (j == 9 || j == 11) r = fmin(a, b);
+        else r = fmax(a, b);
+        shd[t] = r;
+      }
+      __syncthreads();
+    }
+    if (t == 0) out[(int64_t)blockIdx.x * DIAG_N + j] = shd[0];
+    __syncthreads();
+  }
+}
+
+
+// ============================================================== unit kernels (host arrays API)
+__global__ void k_hb_batch(int64_t n, const double* trial, const double* ys, const double* k, const double* nn,
+                           const double* mu, const double* dt, double tol, const float* mlp, double* out,
+                           int* status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double sigma0 = -1.0;
+  if (mlp != nullptr) {
+    const double frac = warm_fraction(mlp, trial[i], ys[i], k[i], nn[i], mu[i], dt[i]);
+    if (frac > 0.0) sigma0 = ys[i] + frac * (trial[i] - ys[i]);
+  }
+  double sigma = 0.0, dep = 0.0;
+  int it = 0;
+  status[i] = hb_return_d(trial[i], ys[i], k[i], nn[i], mu[i], dt[i], tol, sigma0, &sigma, &dep, &it);
+  out[3 * i + 0] = sigma;
+  out[3 * i + 1] = dep;
+  out[3 * i + 2] = (double)it;
+}
+__global__ void k_paste_batch(int64_t n, const double* f, double mu, double lambda, double ys, double k, double nn,
+                              double dt, double tol, double* fnew, double* tau, double* scal, int* status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float Htr[9];
+  for (int a = 0; a < 9; ++a) Htr[a] = (float)(f[9 * i + a] - ((a % 4) == 0 ? 1.0 : 0.0));
+  PasteOut o;
+  paste_update(Htr, (float)mu, (float)lambda, mu, ys, k, nn, dt, tol, nullptr, o);
+  status[i] = o.fail;
+  if (o.fail != F_OK) return;
+  for (int a = 0; a < 9; ++a) fnew[9 * i + a] = (double)o.H[a] + ((a % 4) == 0 ? 1.0 : 0.0);
+  const int map[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+  for (int a = 0; a < 9; ++a) tau[9 * i + a] = o.tau[map[a]];
+  scal[3 * i + 0] = o.dep;
+  scal[3 * i + 1] = o.diss_density;
+  scal[3 * i + 2] = o.eq;
+}
+__global__ void k_liquid_batch(int64_t n, const double* j, const double* grad, double bulk, double visc,
+                               double gamma, double dt, double* jnew, double* tau, double* p, int* status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float C[9];
+  for (int a = 0; a < 9; ++a) C[a] = (float)grad[9 * i + a];
+  LiquidOut o;
+  liquid_update((float)(j[i] - 1.0), C, (float)bulk, (float)visc, (float)gamma, (float)dt, o);
+  status[i] = o.fail;
+  if (o.fail != F_OK) return;
+  jnew[i] = 1.0 + (double)o.jm1;
+  const int map[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+  for (int a = 0; a < 9; ++a) tau[9 * i + a] = o.tau[map[a]];
+  p[i] = o.pressure;
+}
+
+// ============================================================== launchers
+static uint64_t g_launches = 0;
+uint64_t kernel_launch_count() { return g_launches; }
+void add_kernel_launches(uint64_t n) { g_launches += n; }
+
+static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
+  int n = 0;
+  if (ev) cudaEventRecord(ev[0], s);
+  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+                                                          A.keys, A.count, A.nw_list, A.nw_count);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
+                                                            A.perm);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
+                                                                      A.perm, A.id[0], A.id[1]);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
+                                                     A.perm, A.acc, A.node_total, A.blk_epoch);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
+                                     A.acc, A.trac, A.node_total);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_grid_update<<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.trac,
+                                                           A.node_total, A.blk_epoch, A.vel, A.gpart);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  if (A.any_pellet) {
+    k_couple<<<A.n_inst, 256, 0, s>>>(A.desc, A.ctrl, A.blk_epoch, A.vel);
+    ++n;
+    if (ev) cudaEventRecord(ev[n], s);
+  }
+  k_g2p<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.id[0], A.id[1],
+                                                    A.cap, A.perm, A.vel, A.ppart, A.mlp, A.log_x, A.log_y, A.log_n,
+                                                    A.log_cap);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_end<<<A.n_inst, 256, 0, s>>>(A.desc, A.ctrl, A.gpart, A.ppart);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  g_launches += (uint64_t)n;
+  return n;
+}
+
+__global__ void k_grid_sums(const long long* __restrict__ acc, int64_t node_total, unsigned long long* __restrict__ out) {
+  long long v[4] = {0, 0, 0, 0};
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < node_total; g += (int64_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < 4; ++k) v[k] += acc[k * node_total + g];
+  for (int k = 0; k < 4; ++k) atomicAdd(out + k, (unsigned long long)v[k]);
+}
+
+int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
+  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count);
+  k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+                                                          A.keys, A.count, A.nw_list, A.nw_count);
+  k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
+  k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
+  k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
+  k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
+                                                            A.perm);
+  k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
+                                                                      A.perm, A.id[0], A.id[1]);
+  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
+                                                     A.perm, A.acc, A.node_total, A.blk_epoch);
+  k_grid_sums<<<148 * 4, 256, 0, s>>>(A.acc, A.node_total, (unsigned long long*)out);
+  g_launches += 9;
+  return 9;
+}
+
+int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return launch_attempt(A, s, nullptr); }
+
+const char* attempt_kernel_name(int k, int any_pellet) {
+  static const char* a[] = {"k_begin", "k_bin_count", "k_scan_chunks", "k_scan_instances", "k_scan_apply",
+                            "k_bin_scatter", "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple",
+                            "k_g2p", "k_end"};
+  if (!any_pellet && k >= 10) ++k;
+  return k < 13 ? a[k] : "?";
+}
+
+int launch_state_stats(const DeviceArrays& A, cudaStream_t s) {
+  k_state_stats<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+                                                            A.ppart);
+  g_launches += 1;
+  return 1;
+}
+
+int launch_diagnostics(const DeviceArrays& A, int hydro, double h0, int dam, double* out, cudaStream_t s) {
+  k_diagnostics<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+                                                            hydro, h0, dam, out);
+  g_launches += 1;
+  return 1;
+}
+
+int launch_hb_return_batch(int64_t n, const double* trial, const double* ys, const double* k, const double* nn,
+                           const double* mu, const double* dt, double tol, const float* mlp, double* out, int* status,
+                           cudaStream_t s) {
+  k_hb_batch<<<grid_of(n, 128), 128, 0, s>>>(n, trial, ys, k, nn, mu, dt, tol, mlp, out, status);
+  g_launches += 1;
+  return 1;
+}
+int launch_update_paste_batch(int64_t n, const double* f, double mu, double lambda, double ys, double k, double nn,
+                              double dt, double tol, double* fnew, double* tau, double* scal, int* status,
+                              cudaStream_t s) {
+  k_paste_batch<<<grid_of(n, 128), 128, 0, s>>>(n, f, mu, lambda, ys, k, nn, dt, tol, fnew, tau, scal, status);
+  g_launches += 1;
+  return 1;
+}
+int launch_update_liquid_batch(int64_t n, const double* j, const double* grad, double bulk, double visc, double gamma,
+                               double dt, double* jnew, double* tau, double* p, int* status, cudaStream_t s) {
+  k_liquid_batch<<<grid_of(n, 128), 128, 0, s>>>(n, j, grad, bulk, visc, gamma, dt, jnew, tau, p, status);
+  g_launches += 1;
+  return 1;
+}
+
+}  // namespace lp

@@ -1,0 +1,76 @@
+// lp_kernels.h - launch interface between the host runtime and the substep kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lp_device.cuh"
+
+namespace lp {
+
+constexpr int DIAG_N = 18;
+
+// All device buffers of one ensemble (owned by the host runtime).
+struct DeviceArrays {
+  InstDesc* desc = nullptr;
+  Control* ctrl = nullptr;
+  int n_inst = 0;
+  int any_pellet = 0;
+  int* pcta_inst = nullptr;  // G2P / per-slot CTA -> instance
+  int64_t n_pcta = 0;
+  int* tile_inst = nullptr;  // P2G tile -> instance
+  int64_t n_tiles = 0;
+  int* gcta_inst = nullptr;  // grid-update CTA -> instance
+  int64_t n_gcta = 0;
+  int* chunk_inst = nullptr;  // scan chunk -> instance
+  int64_t n_chunks = 0;
+  float* st[2] = {nullptr, nullptr};
+  uint32_t* id[2] = {nullptr, nullptr};
+  int64_t cap = 0;  // slots (multiple of SLOT_ALIGN)
+  uint32_t* keys = nullptr;
+  uint32_t* count = nullptr;
+  uint32_t* start = nullptr;
+  uint32_t* chunk_sum = nullptr;
+  uint32_t* chunk_base = nullptr;
+  uint32_t* perm = nullptr;
+  uint32_t* nw_list = nullptr;
+  uint32_t* nw_count = nullptr;
+  long long* acc = nullptr;   // 4 x node_total: mass, momentum xyz (int64 fixed point)
+  long long* trac = nullptr;  // 6 x node_total: reactions per axis, low faces then high faces
+  int64_t node_total = 0;
+  uint32_t* blk_epoch = nullptr;
+  int64_t n_blk = 0;
+  float4* vel = nullptr;
+  GridPartial* gpart = nullptr;
+  ParticlePartial* ppart = nullptr;
+  float* mlp = nullptr;  // warm-start weights (device) or null
+  float* log_x = nullptr;
+  float* log_y = nullptr;
+  unsigned long long* log_n = nullptr;
+  long long log_cap = 0;
+  int p2g_variant = 0;  // autotuner choice (reserved)
+};
+
+// One substep attempt for every active instance; returns the number of kernels launched.
+int launch_attempt(const DeviceArrays& A, cudaStream_t s);
+// same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 14 events)
+int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev);
+const char* attempt_kernel_name(int k, int any_pellet);
+int launch_state_stats(const DeviceArrays& A, cudaStream_t s);
+// begin + binning + P2G only (conservation probe), then exact node sums into out[4] (int64)
+int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s);
+int launch_diagnostics(const DeviceArrays& A, int hydro, double h0, int dam, double* out, cudaStream_t s);
+uint64_t kernel_launch_count();
+void add_kernel_launches(uint64_t n);
+
+// constitutive unit kernels on device arrays
+int launch_hb_return_batch(int64_t n, const double* trial, const double* ys, const double* k, const double* nn,
+                           const double* mu, const double* dt, double tol, const float* mlp, double* out, int* status,
+                           cudaStream_t s);
+int launch_update_paste_batch(int64_t n, const double* f, double mu, double lambda, double ys, double k, double nn,
+                              double dt, double tol, double* fnew, double* tau, double* scal, int* status,
+                              cudaStream_t s);
+int launch_update_liquid_batch(int64_t n, const double* j, const double* grad, double bulk, double visc, double gamma,
+                               double dt, double* jnew, double* tau, double* p, int* status, cudaStream_t s);
+
+}  // namespace lp

@@ -1,0 +1,322 @@
+// lp_mlp.cu - training of the Herschel-Bulkley warm-start network on the device
+// (forward, backward, Adam), no reference counterpart.
+//
+// Minibatch step, batch B:
+//   k_mlp_sample : per sample, forward pass and back-propagation of the squared error to the
+//                  hidden pre-activations (dZ1, dZ2), stored with the activations (H1, H2);
+//   k_mlp_wgrad  : weight gradients as fixed-order sums over the batch, split in S slices whose
+//                  partials are summed in slice order (deterministic);
+//   k_mlp_adam   : Adam update.
+// Loss = mean over the batch of (out - y)^2, with y = logit of the root fraction.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lp_mpm.h"
+#include "lp_kernels.h"
+#include "lp_mlp.cuh"
+
+namespace lp {
+
+constexpr int MLP_SPLIT = 16;
+
+__device__ __forceinline__ float silu_grad(float z) {
+  const float s = 1.0f / (1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+// per sample forward + backward to the pre-activations
+__global__ void k_mlp_sample(const float* __restrict__ W, const float* __restrict__ X, const float* __restrict__ Y,
+                             int64_t n, float* __restrict__ H1, float* __restrict__ H2, float* __restrict__ dZ1,
+                             float* __restrict__ dZ2, float* __restrict__ G3, float* __restrict__ loss_part) {
+  __shared__ float sw[MLP_NW];
+  __shared__ float sl[256];
+  for (int j = threadIdx.x; j < MLP_NW; j += blockDim.x) sw[j] = W[j];
+  __syncthreads();
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0.0f;
+  if (s < n) {
+    float x[MLP_IN];
+    for (int i = 0; i < MLP_IN; ++i) x[i] = X[s * MLP_IN + i];
+    float z1[MLP_H], h1[MLP_H];
+    for (int j = 0; j < MLP_H; ++j) {
+      float a = sw[MLP_B1 + j];
+      for (int i = 0; i < MLP_IN; ++i) a += sw[MLP_W1 + j * MLP_IN + i] * x[i];
+      z1[j] = a;
+      h1[j] = silu(a);
+      H1[s * MLP_H + j] = h1[j];
+    }
+    float out = sw[MLP_B3];
+    float z2[MLP_H];
+    for (int j = 0; j < MLP_H; ++j) {
+      float a = sw[MLP_B2 + j];
+      for (int i = 0; i < MLP_H; ++i) a += sw[MLP_W2 + j * MLP_H + i] * h1[i];
+      z2[j] = a;
+      const float h = silu(a);
+      H2[s * MLP_H + j] = h;
+      out += sw[MLP_W3 + j] * h;
+    }
+    const float e = out - Y[s];
+    l = e * e;
+    const float g3 = 2.0f * e / (float)n;
+    G3[s] = g3;
+    float dz2[MLP_H];
+    for (int j = 0; j < MLP_H; ++j) {
+      dz2[j] = g3 * sw[MLP_W3 + j] * silu_grad(z2[j]);
+      dZ2[s * MLP_H + j] = dz2[j];
+    }
+    for (int i = 0; i < MLP_H; ++i) {
+      float a = 0.0f;
+      for (int j = 0; j < MLP_H; ++j) a += sw[MLP_W2 + j * MLP_H + i] * dz2[j];
+      dZ1[s * MLP_H + i] = a * silu_grad(z1[i]);
+    }
+  }
+  sl[threadIdx.x] = l;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) sl[threadIdx.x] += sl[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) loss_part[blockIdx.x] = sl[0];
+}
+
+// weight gradients: partial sums over batch slice `blockIdx.y`, one thread per weight
+__global__ void k_mlp_wgrad(const float* __restrict__ X, const float* __restrict__ H1, const float* __restrict__ H2,
+                            const float* __restrict__ dZ1, const float* __restrict__ dZ2, const float* __restrict__ G3,
+                            int64_t n, float* __restrict__ part) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= MLP_NW) return;
+  const int slice = blockIdx.y;
+  const int64_t per = (n + MLP_SPLIT - 1) / MLP_SPLIT;
+  const int64_t s0 = slice * per, s1 = s0 + per < n ? s0 + per : n;
+  float acc = 0.0f;
+  if (w < MLP_B1) {
+    const int j = (w - MLP_W1) / MLP_IN, i = (w - MLP_W1) % MLP_IN;
+    for (int64_t s = s0; s < s1; ++s) acc += dZ1[s * MLP_H + j] * X[s * MLP_IN + i];
+  } else if (w < MLP_W2) {
+    const int j = w - MLP_B1;
+    for (int64_t s = s0; s < s1; ++s) acc += dZ1[s * MLP_H + j];
+  } else if (w < MLP_B2) {
+    const int j = (w - MLP_W2) / MLP_H, i = (w - MLP_W2) % MLP_H;
+    for (int64_t s = s0; s < s1; ++s) acc += dZ2[s * MLP_H + j] * H1[s * MLP_H + i];
+  } else if (w < MLP_W3) {
+    const int j = w - MLP_B2;
+    for (int64_t s = s0; s < s1; ++s) acc += dZ2[s * MLP_H + j];
+  } else if (w < MLP_B3) {
+    const int j = w - MLP_W3;
+    for (int64_t s = s0; s < s1; ++s) acc += G3[s] * H2[s * MLP_H + j];
+  } else {
+    for (int64_t s = s0; s < s1; ++s) acc += G3[s];
+  }
+  part[(int64_t)slice * MLP_NW + w] = acc;
+}
+
+__global__ void k_mlp_gsum(const float* __restrict__ part, float* __restrict__ grad) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= MLP_NW) return;
+  float g = 0.0f;
+  for (int s = 0; s < MLP_SPLIT; ++s) g += part[(int64_t)s * MLP_NW + w];
+  grad[w] = g;
+}
+
+__global__ void k_mlp_adam(float* __restrict__ W, const float* __restrict__ grad, float* __restrict__ m1,
+                           float* __restrict__ m2, float lr, float b1t, float b2t) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= MLP_NW) return;
+  const float g = grad[w];
+  const float a = 0.9f * m1[w] + 0.1f * g;
+  const float b = 0.999f * m2[w] + 0.001f * g * g;
+  m1[w] = a;
+  m2[w] = b;
+  const float ah = a / (1.0f - b1t), bh = b / (1.0f - b2t);
+  W[w] -= lr * ah / (sqrtf(bh) + 1e-8f);
+}
+
+__global__ void k_mlp_infer(const float* __restrict__ W, const float* __restrict__ X, int64_t n, float* __restrict__ Y) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  float f[MLP_IN];
+  for (int i = 0; i < MLP_IN; ++i) f[i] = X[s * MLP_IN + i];
+  Y[s] = mlp_forward(W, f);
+}
+
+}  // namespace lp
+
+namespace {
+thread_local std::string g_mlp_err;
+lp_status mlp_fail(lp_status s, const std::string& m) {
+  g_mlp_err = m;
+  std::fprintf(stderr, "lp_mlp: %s\n", m.c_str());
+  return s;
+}
+#define MCK(expr)                                                                                 \
+  do {                                                                                            \
+    cudaError_t _e = (expr);                                                                      \
+    if (_e != cudaSuccess) return mlp_fail(LP_DEVICE, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+struct MlpBuffers {
+  float *W = nullptr, *X = nullptr, *Y = nullptr, *H1 = nullptr, *H2 = nullptr, *dZ1 = nullptr, *dZ2 = nullptr,
+        *G3 = nullptr, *loss = nullptr, *part = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+  int64_t batch = 0;
+  ~MlpBuffers() {
+    float* ps[] = {W, X, Y, H1, H2, dZ1, dZ2, G3, loss, part, grad, m1, m2};
+    for (float* p : ps)
+      if (p) cudaFree(p);
+  }
+  lp_status alloc(int64_t b) {
+    batch = b;
+    MCK(cudaMalloc(&W, sizeof(float) * lp::MLP_NW));
+    MCK(cudaMalloc(&H1, sizeof(float) * b * lp::MLP_H));
+    MCK(cudaMalloc(&H2, sizeof(float) * b * lp::MLP_H));
+    MCK(cudaMalloc(&dZ1, sizeof(float) * b * lp::MLP_H));
+    MCK(cudaMalloc(&dZ2, sizeof(float) * b * lp::MLP_H));
+    MCK(cudaMalloc(&G3, sizeof(float) * b));
+    MCK(cudaMalloc(&loss, sizeof(float) * ((b + 255) / 256)));
+    MCK(cudaMalloc(&part, sizeof(float) * lp::MLP_SPLIT * lp::MLP_NW));
+    MCK(cudaMalloc(&grad, sizeof(float) * lp::MLP_NW));
+    MCK(cudaMalloc(&m1, sizeof(float) * lp::MLP_NW));
+    MCK(cudaMalloc(&m2, sizeof(float) * lp::MLP_NW));
+    MCK(cudaMemset(m1, 0, sizeof(float) * lp::MLP_NW));
+    MCK(cudaMemset(m2, 0, sizeof(float) * lp::MLP_NW));
+    return LP_OK;
+  }
+};
+
+// loss and gradient of one batch (X, Y device pointers) into B.grad; returns mean loss
+lp_status batch_grad(MlpBuffers& B, const float* X, const float* Y, int64_t n, float* loss_out) {
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  lp::k_mlp_sample<<<nb, 256>>>(B.W, X, Y, n, B.H1, B.H2, B.dZ1, B.dZ2, B.G3, B.loss);
+  dim3 g((lp::MLP_NW + 255) / 256, lp::MLP_SPLIT);
+  lp::k_mlp_wgrad<<<g, 256>>>(X, B.H1, B.H2, B.dZ1, B.dZ2, B.G3, n, B.part);
+  lp::k_mlp_gsum<<<(lp::MLP_NW + 255) / 256, 256>>>(B.part, B.grad);
+  lp::add_kernel_launches(3);
+  MCK(cudaGetLastError());
+  if (loss_out) {
+    std::vector<float> lp_(nb);
+    MCK(cudaMemcpy(lp_.data(), B.loss, sizeof(float) * nb, cudaMemcpyDeviceToHost));
+    double s = 0.0;
+    for (float v : lp_) s += v;
+    *loss_out = (float)(s / (double)n);
+  }
+  return LP_OK;
+}
+
+uint64_t splitmix(uint64_t& s) {
+  s += 0x9E3779B97F4A7C15ull;
+  uint64_t z = s;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+}  // namespace
+
+extern "C" {
+
+int32_t lp_mlp_weight_count(void) { return lp::MLP_NW; }
+
+lp_status lp_mlp_init(float* w, int32_t nw, uint64_t seed) {
+  if (!w || nw != lp::MLP_NW) return mlp_fail(LP_INVALID, "weight count mismatch");
+  uint64_t s = seed;
+  auto uni = [&]() { return (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0); };
+  const double a1 = std::sqrt(6.0 / (lp::MLP_IN + lp::MLP_H)), a2 = std::sqrt(6.0 / (2 * lp::MLP_H)),
+               a3 = std::sqrt(6.0 / (lp::MLP_H + 1));
+  for (int k = 0; k < lp::MLP_NW; ++k) {
+    double a = 0.0;
+    if (k < lp::MLP_B1) a = a1;
+    else if (k >= lp::MLP_W2 && k < lp::MLP_B2) a = a2;
+    else if (k >= lp::MLP_W3 && k < lp::MLP_B3) a = a3;
+    w[k] = (float)((2.0 * uni() - 1.0) * a);
+  }
+  return LP_OK;
+}
+
+lp_status lp_mlp_loss_grad(const float* w, int32_t nw, const float* x, const float* y, int64_t n, float* loss,
+                           float* grad) {
+  if (!w || nw != lp::MLP_NW || n <= 0) return mlp_fail(LP_INVALID, "bad arguments");
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return mlp_fail(LP_DEVICE, "no CUDA device");
+  MlpBuffers B;
+  lp_status st = B.alloc(n);
+  if (st != LP_OK) return st;
+  float *X = nullptr, *Y = nullptr;
+  MCK(cudaMalloc(&X, sizeof(float) * n * lp::MLP_IN));
+  MCK(cudaMalloc(&Y, sizeof(float) * n));
+  B.X = X;
+  B.Y = Y;
+  MCK(cudaMemcpy(B.W, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(X, x, sizeof(float) * n * lp::MLP_IN, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(Y, y, sizeof(float) * n, cudaMemcpyHostToDevice));
+  st = batch_grad(B, X, Y, n, loss);
+  if (st != LP_OK) return st;
+  MCK(cudaMemcpy(grad, B.grad, sizeof(float) * lp::MLP_NW, cudaMemcpyDeviceToHost));
+  return LP_OK;
+}
+
+lp_status lp_mlp_train(float* w, int32_t nw, const float* x, const float* y, int64_t n, int32_t epochs, int32_t batch,
+                       float lr, float* final_loss) {
+  if (!w || nw != lp::MLP_NW || n <= 0 || batch <= 0 || epochs <= 0) return mlp_fail(LP_INVALID, "bad arguments");
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return mlp_fail(LP_DEVICE, "no CUDA device");
+  const int64_t b = std::min<int64_t>(batch, n);
+  MlpBuffers B;
+  lp_status st = B.alloc(b);
+  if (st != LP_OK) return st;
+  float *X = nullptr, *Y = nullptr;
+  MCK(cudaMalloc(&X, sizeof(float) * n * lp::MLP_IN));
+  MCK(cudaMalloc(&Y, sizeof(float) * n));
+  B.X = X;
+  B.Y = Y;
+  MCK(cudaMemcpy(B.W, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(X, x, sizeof(float) * n * lp::MLP_IN, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(Y, y, sizeof(float) * n, cudaMemcpyHostToDevice));
+  double b1t = 1.0, b2t = 1.0;
+  float last = 0.0f;
+  const int64_t steps_per_epoch = n / b;
+  for (int e = 0; e < epochs; ++e) {
+    // the host shuffles sample order by choosing contiguous batches of a pre-shuffled set;
+    // callers pass shuffled data, batches cycle through it in order
+    double eloss = 0.0;
+    for (int64_t k = 0; k < steps_per_epoch; ++k) {
+      const float* xb = X + k * b * lp::MLP_IN;
+      const float* yb = Y + k * b;
+      float l = 0.0f;
+      const bool want = (k == steps_per_epoch - 1);
+      st = batch_grad(B, xb, yb, b, want ? &l : nullptr);
+      if (st != LP_OK) return st;
+      b1t *= 0.9;
+      b2t *= 0.999;
+      lp::k_mlp_adam<<<(lp::MLP_NW + 255) / 256, 256>>>(B.W, B.grad, B.m1, B.m2, lr, (float)b1t, (float)b2t);
+      lp::add_kernel_launches(1);
+      if (want) eloss = l;
+    }
+    last = (float)eloss;
+  }
+  MCK(cudaDeviceSynchronize());
+  MCK(cudaMemcpy(w, B.W, sizeof(float) * lp::MLP_NW, cudaMemcpyDeviceToHost));
+  if (final_loss) *final_loss = last;
+  return LP_OK;
+}
+
+lp_status lp_mlp_forward(const float* w, int32_t nw, const float* x, int64_t n, float* y) {
+  if (!w || nw != lp::MLP_NW || n <= 0) return mlp_fail(LP_INVALID, "bad arguments");
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return mlp_fail(LP_DEVICE, "no CUDA device");
+  float *W = nullptr, *X = nullptr, *Y = nullptr;
+  MCK(cudaMalloc(&W, sizeof(float) * lp::MLP_NW));
+  MCK(cudaMalloc(&X, sizeof(float) * n * lp::MLP_IN));
+  MCK(cudaMalloc(&Y, sizeof(float) * n));
+  MCK(cudaMemcpy(W, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(X, x, sizeof(float) * n * lp::MLP_IN, cudaMemcpyHostToDevice));
+  lp::k_mlp_infer<<<(unsigned)((n + 255) / 256), 256>>>(W, X, n, Y);
+  lp::add_kernel_launches(1);
+  MCK(cudaGetLastError());
+  MCK(cudaMemcpy(y, Y, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  cudaFree(W);
+  cudaFree(X);
+  cudaFree(Y);
+  return LP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+"""Benchmark workloads as fixture specs.
+
+Material parameters follow the reference's wire convention (research.rs:274-305): yield
+stress and consistency are shear-rheometer values converted to the von Mises form by
+`Material::paste_from_shear_rheology` (constitutive.rs:180-197).  Young's modulus and
+Poisson's ratio are derived from the stated shear and bulk moduli.  Extensions used here
+(labelled in the spec): per-face wall friction with a sticky floor, per-particle yield stress,
+the Tait EOS exponent, and the Newton tolerance.
+"""
+
+from __future__ import annotations
+
+import math
+
+from . import _abi
+from .research import base_spec, material_liquid, material_paste_shear
+
+
+def young_poisson(shear: float, bulk: float) -> tuple[float, float]:
+    e = 9.0 * bulk * shear / (3.0 * bulk + shear)
+    nu = (3.0 * bulk - 2.0 * shear) / (2.0 * (3.0 * bulk + shear))
+    return e, nu
+
+
+def _sticky_floor_slip_walls(s: _abi.FixtureSpec) -> None:
+    s.face_mode_enabled = 1
+    for f in range(6):
+        s.face_friction[f] = 0.0
+        s.face_sticky[f] = 0
+    s.face_sticky[4] = 1  # floor: axis 2, low face
+
+
+def slump(cells: int = 64, column=(16, 16, 32), seed: int = 0, yield_range=None, newton_tol: float = 1e-10,
+          dt: float = 1e-4, domain_m: float = 1.0) -> _abi.FixtureSpec:
+    """HB paste slump: rho 1200, G 2e4, K 1e5, tau_y 50, K_s 5, n 0.5, sticky floor, slip walls."""
+    dx = domain_m / cells
+    e, nu = young_poisson(2e4, 1e5)
+    s = base_spec(fixture=_abi.LP_SLUMP, grid_spacing=dx, domain=[domain_m] * 3,
+                  initial_size=[c * dx for c in column], initial_velocity=[0, 0, 0], seed=seed,
+                  wall_friction=0.0, max_dt=dt, min_dt=1e-12, contact_stiffness=1000.0,
+                  contact_restitution=0.2, contact_friction=0.4, max_particles=2**31 - 1, max_nodes=2**40)
+    s.material = material_paste_shear(1200.0, e, nu, 50.0, 5.0, 0.5)
+    _sticky_floor_slip_walls(s)
+    s.newton_tolerance = newton_tol
+    if yield_range is not None:
+        s.yield_random = 1
+        s.yield_min = math.sqrt(3.0) * yield_range[0]
+        s.yield_max = math.sqrt(3.0) * yield_range[1]
+    return s
+
+
+def config0() -> _abi.FixtureSpec:
+    """64^3 grid, 16x16x32-cell column, 65,536 particles, seed 0, dt 1e-4, 500 substeps."""
+    return slump(64, (16, 16, 32), seed=0)
+
+
+def config2() -> _abi.FixtureSpec:
+    """256^3 grid, 128^3-cell column, ~16.8M particles, seed 2, yield U(20, 100) per particle."""
+    return slump(256, (128, 128, 128), seed=2, yield_range=(20.0, 100.0))
+
+
+def dam_break(cells: int = 128, block=(64, 32, 64), seed: int = 1, gamma: float = 7.0,
+              dt: float = 5e-5) -> _abi.FixtureSpec:
+    """Weakly compressible water dam break: rho 1000, K 2e5, Tait gamma, eta 1e-3, slip walls."""
+    dx = 1.0 / cells
+    bulk = 2e5
+    nu = 0.2
+    e = 3.0 * bulk * (1.0 - 2.0 * nu)
+    s = base_spec(fixture=_abi.LP_DAM_BREAK, grid_spacing=dx, domain=[1.0] * 3,
+                  initial_size=[b * dx for b in block], initial_velocity=[0, 0, 0], seed=seed,
+                  wall_friction=0.0, max_dt=dt, min_dt=1e-12, contact_stiffness=1000.0,
+                  contact_restitution=0.2, contact_friction=0.4, max_particles=2**31 - 1, max_nodes=2**40)
+    s.material = material_liquid(1000.0, e, nu, 1e-3, tait_gamma=gamma)
+    return s
+
+
+def config1() -> _abi.FixtureSpec:
+    """128^3 grid, 64x32x64-cell water block, ~1.05M particles, seed 1, dt <= 5e-5, 2000 substeps."""
+    return dam_break()
+
+
+def sweep_instance(k: int, rng) -> _abi.FixtureSpec:
+    """One member of the batched calibration sweep (seed 100 + k).
+
+    Particle count log-uniform in 8k-260k: a column of a x a x 2a cells at 8 particles per cell
+    (16 a^3 particles) in a cubic domain 1.5 times the column height (3a cells), dx = 1 cm.
+    Yield U(10, 200) Pa, consistency U(1, 20) Pa s^n, flow index U(0.3, 1.0), shear modulus
+    U(5e3, 5e4) Pa (bulk modulus 1e5 Pa), rho 1200, sticky floor and slip walls, dt 1e-4.
+    """
+    n_target = math.exp(rng.uniform(math.log(8_000), math.log(260_000)))
+    a = max(2, round((n_target / 16.0) ** (1.0 / 3.0)))
+    cells = 3 * a
+    dx = 0.01
+    shear = rng.uniform(5e3, 5e4)
+    e, nu = young_poisson(shear, 1e5)
+    s = base_spec(fixture=_abi.LP_SLUMP, grid_spacing=dx, domain=[cells * dx] * 3,
+                  initial_size=[a * dx, a * dx, 2 * a * dx], initial_velocity=[0, 0, 0], seed=100 + k,
+                  wall_friction=0.0, max_dt=1e-4, min_dt=1e-12, contact_stiffness=1000.0,
+                  contact_restitution=0.2, contact_friction=0.4, max_particles=2**31 - 1, max_nodes=2**40)
+    s.material = material_paste_shear(1200.0, e, nu, rng.uniform(10.0, 200.0), rng.uniform(1.0, 20.0),
+                                      rng.uniform(0.3, 1.0))
+    _sticky_floor_slip_walls(s)
+    s.newton_tolerance = 1e-10
+    return s
+
+
+def config3(count: int = 256, seed: int = 2024) -> list[_abi.FixtureSpec]:
+    """256 independent HB slumps of uneven size (seeds 100-355), 300 substeps each."""
+    import random
+
+    rng = random.Random(seed)
+    return [sweep_instance(k, rng) for k in range(count)]

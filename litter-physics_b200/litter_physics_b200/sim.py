@@ -1,0 +1,270 @@
+"""Python mirror of the reference's `Simulation` / `FixtureSpec` API over the device library.
+
+`Simulation(spec)` corresponds to `FixtureSpec::build` (core/src/mpm/fixtures.rs:238-268) and
+exposes the calls the reference's tests and research driver make on a `Simulation`
+(core/src/mpm/solver.rs): `advance_to`, `advance_while`, `try_step`, `stability_limit`,
+`ledger`, the residual and energy accessors, `observables` (fixtures.rs:369-461), and
+checkpoint-style state export / import.  All arithmetic happens on the GPU; this module only
+marshals plain buffers across the C ABI.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable
+
+import numpy as np
+
+from . import _abi
+from ._lib import LPError, check, lib
+
+
+class Simulation:
+    """One MLS-MPM simulation resident on the GPU."""
+
+    def __init__(self, spec: _abi.FixtureSpec):
+        self.spec = spec
+        self._h = C.c_void_p()
+        check(lib().lp_sim_create(C.byref(spec), C.byref(self._h)))
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self) -> None:
+        if self._h:
+            lib().lp_sim_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------ stepping
+    def advance_while(self, target_time: float, should_continue: Callable[[], bool] | None = None) -> bool:
+        """solver.rs:413-472: returns False at a resumable budget stop."""
+        reached = C.c_int32()
+        cb = _abi.KEEP_GOING_FN(lambda _ctx: 1 if should_continue() else 0) if should_continue else \
+            _abi.KEEP_GOING_FN(0)
+        st = lib().lp_sim_advance(self._h, float(target_time), cb, None, C.byref(reached))
+        if st == _abi.LP_BUDGET:
+            return False
+        check(st)
+        return bool(reached.value)
+
+    def advance_to(self, target_time: float) -> None:
+        """solver.rs:402-404."""
+        self.advance_while(target_time)
+
+    def try_step(self, dt: float) -> tuple[bool, str]:
+        """One trial step of exactly dt (solver.rs:535-611); committed only on success."""
+        acc = C.c_int32()
+        reason = C.create_string_buffer(256)
+        check(lib().lp_sim_try_step(self._h, float(dt), C.byref(acc), reason, 256))
+        return bool(acc.value), reason.value.decode()
+
+    def run_substeps(self, steps: int) -> None:
+        """Queue `steps` controlled attempts on the stream without synchronising."""
+        check(lib().lp_sim_run_substeps(self._h, int(steps)))
+
+    def sync(self) -> None:
+        check(lib().lp_sim_sync(self._h))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib().lp_sim_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def use_graph(self, steps: int) -> None:
+        check(lib().lp_sim_use_graph(self._h, int(steps)))
+
+    def stability_limit(self) -> float:
+        out = C.c_double()
+        check(lib().lp_sim_stability_limit(self._h, C.byref(out)))
+        return out.value
+
+    # ------------------------------------------------------------------ state
+    @property
+    def ledger(self) -> _abi.Ledger:
+        led = _abi.Ledger()
+        check(lib().lp_sim_get_ledger(self._h, C.byref(led)))
+        return led
+
+    def set_ledger(self, led: _abi.Ledger) -> None:
+        check(lib().lp_sim_set_ledger(self._h, C.byref(led)))
+
+    @property
+    def counters(self) -> _abi.Counters:
+        c = _abi.Counters()
+        check(lib().lp_sim_get_counters(self._h, C.byref(c)))
+        return c
+
+    def set_counters(self, c: _abi.Counters) -> None:
+        check(lib().lp_sim_set_counters(self._h, C.byref(c)))
+
+    @property
+    def time(self) -> float:
+        return self.counters.time
+
+    def particle_count(self) -> int:
+        n = C.c_uint64()
+        check(lib().lp_sim_particle_count(self._h, C.byref(n)))
+        return int(n.value)
+
+    def particles(self) -> dict:
+        """Export the committed particle set (FP64 arrays in the reference layout, slot order)."""
+        arrays, view = _abi.particle_buffers(self.particle_count())
+        check(lib().lp_sim_export_particles(self._h, C.byref(view)))
+        return arrays
+
+    def set_particles(self, arrays: dict) -> None:
+        view = _abi.particle_view(arrays)
+        check(lib().lp_sim_import_particles(self._h, C.byref(view)))
+
+    def pellet(self) -> _abi.Pellet | None:
+        p = _abi.Pellet()
+        has = C.c_int32()
+        check(lib().lp_sim_get_pellet(self._h, C.byref(p), C.byref(has)))
+        return p if has.value else None
+
+    def set_pellet(self, p: _abi.Pellet) -> None:
+        check(lib().lp_sim_set_pellet(self._h, C.byref(p)))
+
+    def observables(self) -> dict:
+        cap = 128
+        names = C.create_string_buffer(64 * cap)
+        values = (C.c_double * cap)()
+        n = C.c_int32()
+        check(lib().lp_sim_observables(self._h, names, values, cap, C.byref(n)))
+        raw = names.raw
+        return {raw[64 * i:64 * i + 64].split(b"\0", 1)[0].decode(): values[i] for i in range(n.value)}
+
+    def energies(self) -> dict:
+        out = (C.c_double * 9)()
+        check(lib().lp_sim_energies(self._h, out))
+        keys = ["kinetic", "potential", "elastic", "mechanical", "mass_residual", "momentum_residual_x",
+                "momentum_residual_y", "momentum_residual_z", "energy_residual"]
+        return dict(zip(keys, list(out)))
+
+    def momentum_residual(self) -> np.ndarray:
+        e = self.energies()
+        return np.array([e["momentum_residual_x"], e["momentum_residual_y"], e["momentum_residual_z"]])
+
+    def mass_residual(self) -> float:
+        return self.energies()["mass_residual"]
+
+    def energy_residual(self) -> float:
+        return self.energies()["energy_residual"]
+
+    def grid_totals(self, dt: float) -> dict:
+        """Scatter the committed state (P2G only) and compare grid and particle totals."""
+        out = (C.c_double * 8)()
+        check(lib().lp_sim_grid_totals(self._h, float(dt), out))
+        return {"grid_mass": out[0], "grid_momentum": np.array(out[1:4]), "particle_mass": out[4],
+                "particle_momentum": np.array(out[5:8])}
+
+    def kernel_times(self, steps: int) -> dict:
+        """Mean per-kernel duration (ms) over `steps` attempts, CUDA events on the stream."""
+        cap = 16
+        ms = (C.c_double * cap)()
+        names = C.create_string_buffer(32 * cap)
+        n = C.c_int32()
+        check(lib().lp_sim_kernel_times(self._h, int(steps), ms, names, cap, C.byref(n)))
+        raw = names.raw
+        return {raw[32 * i:32 * i + 32].split(b"\0", 1)[0].decode(): ms[i] for i in range(n.value)}
+
+    # ------------------------------------------------------------------ learned warm start
+    def set_warm_start(self, weights: np.ndarray | None) -> None:
+        if weights is None:
+            check(lib().lp_sim_set_warm_start(self._h, None, 0, 0))
+            return
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        check(lib().lp_sim_set_warm_start(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size, 1))
+
+    def enable_newton_log(self, capacity: int) -> None:
+        check(lib().lp_sim_enable_newton_log(self._h, int(capacity)))
+
+    def read_newton_log(self, capacity: int) -> tuple[np.ndarray, np.ndarray]:
+        x = np.zeros((capacity, 6), dtype=np.float32)
+        y = np.zeros(capacity, dtype=np.float32)
+        n = C.c_int64()
+        check(lib().lp_sim_read_newton_log(self._h, x.ctypes.data_as(C.POINTER(C.c_float)),
+                                           y.ctypes.data_as(C.POINTER(C.c_float)), capacity, C.byref(n)))
+        return x[: n.value], y[: n.value]
+
+
+class Batch:
+    """Many independent simulations advanced by one device launch sequence (extension)."""
+
+    def __init__(self, specs: list[_abi.FixtureSpec]):
+        arr = (_abi.FixtureSpec * len(specs))(*specs)
+        self.specs = specs
+        self._h = C.c_void_p()
+        check(lib().lp_batch_create(arr, len(specs), C.byref(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().lp_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def advance_to(self, target_time: float) -> bool:
+        reached = C.c_int32()
+        check(lib().lp_batch_advance(self._h, float(target_time), _abi.KEEP_GOING_FN(0), None, C.byref(reached)))
+        return bool(reached.value)
+
+    def run_substeps(self, steps: int) -> None:
+        check(lib().lp_batch_run_substeps(self._h, int(steps)))
+
+    def sync(self) -> None:
+        check(lib().lp_batch_sync(self._h))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib().lp_batch_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def use_graph(self, steps: int) -> None:
+        check(lib().lp_batch_use_graph(self._h, int(steps)))
+
+    def autotune(self, trial_steps: int = 16) -> str:
+        buf = C.create_string_buffer(2048)
+        check(lib().lp_batch_autotune(self._h, int(trial_steps), buf, 2048))
+        return buf.value.decode()
+
+    def counters(self, i: int) -> _abi.Counters:
+        c = _abi.Counters()
+        check(lib().lp_batch_get_counters(self._h, i, C.byref(c)))
+        return c
+
+    def ledger(self, i: int) -> _abi.Ledger:
+        led = _abi.Ledger()
+        check(lib().lp_batch_get_ledger(self._h, i, C.byref(led)))
+        return led
+
+    def particles(self, i: int) -> dict:
+        n = self.counters(i).particle_count
+        arrays, view = _abi.particle_buffers(int(n))
+        check(lib().lp_batch_export_particles(self._h, i, C.byref(view)))
+        return arrays
+
+    def total_particles(self) -> int:
+        n = C.c_uint64()
+        check(lib().lp_batch_total_particles(self._h, C.byref(n)))
+        return int(n.value)
+
+    def set_warm_start(self, weights: np.ndarray | None) -> None:
+        if weights is None:
+            check(lib().lp_batch_set_warm_start(self._h, None, 0, 0))
+            return
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        check(lib().lp_batch_set_warm_start(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size, 1))
+
+
+__all__ = ["Simulation", "Batch", "LPError"]

@@ -1,0 +1,71 @@
+"""C-ABI boundary checks that need no GPU: the library builds, loads, exports every function
+the header declares, and its struct layouts match the ctypes mirrors."""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import pytest
+
+
+@pytest.fixture(scope="module")
+def L():
+    from litter_physics_b200 import _lib
+
+    _lib.build()
+    return _lib
+
+
+def test_library_exports_every_declared_symbol(L):
+    names = L.declared_functions()
+    assert len(names) > 40
+    missing = [n for n in names if not hasattr(L.lib(), n)]
+    assert missing == []
+
+
+def test_struct_layouts_match(L):
+    from litter_physics_b200 import _abi
+
+    sizes = L.struct_sizes()
+    assert sizes == {
+        "material": C.sizeof(_abi.Material),
+        "fixture_spec": C.sizeof(_abi.FixtureSpec),
+        "ledger": C.sizeof(_abi.Ledger),
+        "counters": C.sizeof(_abi.Counters),
+        "particles": C.sizeof(_abi.Particles),
+        "pellet": C.sizeof(_abi.Pellet),
+    }
+    assert L.lib().lp_abi_version() == 1
+
+
+def test_material_helpers_match_reference_formulas(L, oracle_mod):
+    """constitutive.rs:146-243 on both sides of the boundary (host arithmetic only)."""
+    lib = L.lib()
+    for args in [(1000.0, 1e5, 0.3, 20.0, 5.0, 0.6), (1200.0, 56250.0, 0.40625, 50.0, 5.0, 0.5)]:
+        a = lib.lp_material_paste_from_shear_rheology(*args)
+        b = oracle_mod.material_paste_shear(*args)
+        for f in ("shear_modulus", "lame_lambda", "bulk_modulus", "yield_stress", "consistency", "flow_index"):
+            assert getattr(a, f) == getattr(b, f), f
+        assert lib.lp_material_wave_speed(C.byref(a)) > 0
+    liq = lib.lp_material_liquid(1000.0, 1e5, 0.2, 1e-3)
+    assert liq.bulk_modulus == oracle_mod.material_liquid(1000.0, 1e5, 0.2, 1e-3).bulk_modulus
+    assert lib.lp_material_diffusivity(C.byref(liq)) == pytest.approx(1e-6)
+
+
+def test_hb_features_are_finite(L):
+    out = (C.c_float * 6)()
+    L.lib().lp_hb_features(100.0, 86.6, 11.4, 0.5, 2e4, 1e-4, out)
+    assert all(abs(v) < 1e3 for v in out)
+
+
+def test_compute_entry_points_fail_loudly_without_device(L):
+    """No host fallback: without a CUDA device, creation returns LP_DEVICE."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from litter_physics_b200 import _abi, configs, sim
+
+    with pytest.raises(sim.LPError) as e:
+        sim.Simulation(configs.slump(16, (4, 4, 8)))
+    assert e.value.status == _abi.LP_DEVICE

@@ -1,0 +1,253 @@
+"""GPU parity against the FP64 oracle, through the C ABI.
+
+Bars (north-star parity contract):
+  * particle positions: max_p |x_gpu - x_ref| / L_domain <= 1e-5 after 100 substeps;
+  * particle velocities: ||v_gpu - v_ref||_2 / ||v_ref||_2 <= 1e-5 after 100 substeps
+    (particles matched by id, since both sides reorder them);
+  * grid mass and momentum after P2G equal the particle totals to 1e-10 relative;
+  * ledger totals: relative agreement stated per field below (FP32 device arithmetic against
+    FP64 reference arithmetic).
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import load_request
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-5
+VEL_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def lib_built():
+    from litter_physics_b200 import _lib
+
+    _lib.build()
+    return _lib
+
+
+def by_id(p: dict) -> dict:
+    order = np.argsort(p["id"])
+    return {k: v[order] for k, v in p.items()}
+
+
+def compare(gpu: dict, ref: dict, length: float) -> dict:
+    g, r = by_id(gpu), by_id(ref)
+    assert np.array_equal(g["id"], r["id"])
+    x_err = float(np.max(np.abs(g["position"] - r["position"]))) / length
+    v_ref = float(np.linalg.norm(r["velocity"]))
+    v_err = float(np.linalg.norm(g["velocity"] - r["velocity"])) / max(v_ref, 1e-300)
+    return {"x": x_err, "v": v_err, "v_norm": v_ref}
+
+
+def run_pair(spec, steps: int):
+    import oracle
+    from litter_physics_b200.sim import Simulation
+
+    target = steps * spec.max_dt
+    ref = oracle.OracleSim(spec)
+    ref.advance_to(target)
+    gpu = Simulation(spec)
+    gpu.advance_to(target)
+    return gpu, ref
+
+
+def small_slump():
+    from litter_physics_b200 import configs
+
+    # config-0 material on a 32^3 grid (column 8x8x16 cells, 8192 particles)
+    return configs.slump(32, (8, 8, 16), seed=0)
+
+
+def test_initial_state_matches_oracle(lib_built):
+    import oracle
+    from litter_physics_b200.sim import Simulation
+
+    spec = small_slump()
+    gpu = Simulation(spec).particles()
+    ref = oracle.OracleSim(spec).particles()
+    d = compare(gpu, ref, 1.0)
+    assert d["x"] < 1e-7
+    assert np.allclose(by_id(gpu)["mass"], by_id(ref)["mass"], rtol=1e-7)
+
+
+@pytest.mark.parametrize("name", ["slump32", "research_slump", "research_hydrostatic_water", "dam_break",
+                                  "research_coupled_patch"])
+def test_100_substeps_match_oracle(lib_built, name):
+    from litter_physics_b200 import configs, research
+
+    if name == "slump32":
+        spec = small_slump()
+    elif name == "dam_break":
+        spec = configs.dam_break(32, (16, 8, 16), seed=1)
+    else:
+        spec = research.spec_from_request(load_request(name))
+    gpu, ref = run_pair(spec, 100)
+    length = max(spec.domain)
+    d = compare(gpu.particles(), ref.particles(), length)
+    print(name, d)
+    gc, rc = gpu.counters, ref.counters()
+    assert gc.step_count == rc.step_count and gc.rejected_steps == rc.rejected_steps
+    assert d["x"] <= POS_TOL, d
+    assert d["v"] <= VEL_TOL, d
+
+
+def test_ledgers_match_oracle(lib_built):
+    spec = small_slump()
+    gpu, ref = run_pair(spec, 100)
+    lg, lr = gpu.ledger, ref.ledger()
+    assert lg.initial_mass == pytest.approx(lr.initial_mass, rel=1e-7)
+    for f in ("gravity_impulse", "wall_impulse"):
+        a, b = np.array(getattr(lg, f)), np.array(getattr(lr, f))
+        assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(b), f
+    for f, rel in (("wall_normal_projection_energy", 1e-3), ("wall_friction_dissipation", 1e-3),
+                   ("wall_normal_traction_energy", 1e-3), ("plastic_dissipation", 1e-3)):
+        a, b = getattr(lg, f), getattr(lr, f)
+        assert abs(a - b) <= rel * max(abs(b), 1e-30), (f, a, b)
+
+
+def test_grid_conserves_mass_and_momentum(lib_built):
+    from litter_physics_b200.sim import Simulation
+
+    spec = small_slump()
+    sim = Simulation(spec)
+    sim.advance_to(30 * spec.max_dt)
+    t = sim.grid_totals(spec.max_dt)
+    assert abs(t["grid_mass"] - t["particle_mass"]) <= 1e-10 * t["particle_mass"]
+    scale = np.linalg.norm(t["particle_momentum"])
+    assert np.linalg.norm(t["grid_momentum"] - t["particle_momentum"]) <= 1e-10 * scale
+
+
+def test_runs_are_bitwise_repeatable(lib_built):
+    from litter_physics_b200.sim import Simulation
+
+    spec = small_slump()
+    out = []
+    for _ in range(2):
+        sim = Simulation(spec)
+        sim.advance_to(50 * spec.max_dt)
+        led = sim.ledger
+        p = by_id(sim.particles())
+        out.append((bytes(led), p["position"].tobytes(), p["velocity"].tobytes()))
+    assert out[0] == out[1]
+
+
+def test_rejected_trial_preserves_state(lib_built):
+    """solver.rs:1714-1740: an oversized step is rejected before any commit."""
+    from litter_physics_b200 import research
+    from litter_physics_b200.sim import Simulation
+
+    spec = research.spec_from_request(load_request("research_slump"))
+    spec.initial_velocity[:] = [1.0, 0.0, -1.0]
+    sim = Simulation(spec)
+    sim.advance_to(2e-4)
+    before = (bytes(sim.ledger), sim.particles()["position"].tobytes())
+    ok, reason = sim.try_step(5e-3)
+    assert not ok and reason
+    after = (bytes(sim.ledger), sim.particles()["position"].tobytes())
+    assert before == after
+
+
+def test_constitutive_kernels_match_oracle(lib_built):
+    import ctypes as C
+
+    import oracle
+    from litter_physics_b200 import _lib
+
+    rng = np.random.default_rng(5)
+    m = oracle.material_paste_shear(1200.0, 56250.0, 0.40625, 50.0, 5.0, 0.5)
+    n = 512
+    f = np.eye(3)[None] + rng.normal(scale=3e-3, size=(n, 3, 3))
+    f = np.ascontiguousarray(f)
+    dt = 1e-4
+    fn, tau = np.zeros((n, 9)), np.zeros((n, 9))
+    dep, diss, eq = np.zeros(n), np.zeros(n), np.zeros(n)
+    st = np.zeros(n, dtype=np.int32)
+    D = C.POINTER(C.c_double)
+    _lib.check(_lib.lib().lp_update_paste_batch(n, f.ctypes.data_as(D), C.byref(m), dt, fn.ctypes.data_as(D),
+                                                 tau.ctypes.data_as(D), dep.ctypes.data_as(D),
+                                                 diss.ctypes.data_as(D), eq.ctypes.data_as(D),
+                                                 st.ctypes.data_as(C.POINTER(C.c_int32))))
+    assert (st == 0).all()
+    yielded = 0
+    for i in range(n):
+        rs, rfn, rtau, rdep, rdiss, req = oracle.update_paste(f[i], m, dt)
+        assert rs == 0
+        scale = np.abs(rtau).max()
+        assert np.abs(tau[i].reshape(3, 3) - rtau).max() <= 1e-4 * scale + 1e-3
+        assert np.abs(fn[i].reshape(3, 3) - rfn).max() <= 2e-6
+        if rdep > 0:
+            yielded += 1
+            assert abs(eq[i] - req) <= 1e-4 * req
+    assert yielded > 50
+
+
+def test_hb_return_batch_matches_oracle(lib_built):
+    import ctypes as C
+
+    import oracle
+    from litter_physics_b200 import _lib
+
+    rng = np.random.default_rng(1)
+    n = 2000
+    ys = rng.uniform(10, 300, n)
+    trial = ys * rng.uniform(1.0001, 3.0, n)
+    k = rng.uniform(1, 40, n)
+    nn = rng.uniform(0.3, 1.5, n)
+    mu = rng.uniform(5e3, 5e4, n)
+    dt = rng.uniform(1e-5, 1e-3, n)
+    out = np.zeros((n, 3))
+    st = np.zeros(n, dtype=np.int32)
+    D = C.POINTER(C.c_double)
+    args = [a.ctypes.data_as(D) for a in (trial, ys, k, nn, mu, dt)]
+    _lib.check(_lib.lib().lp_hb_return_batch(n, *args, 1e-12, None, 0, out.ctypes.data_as(D),
+                                              st.ctypes.data_as(C.POINTER(C.c_int32))))
+    assert (st == 0).all()
+    for i in range(0, n, 7):
+        rs, sigma, dep, it = oracle.hb_return(trial[i], ys[i], k[i], nn[i], mu[i], dt[i])
+        assert rs == 0 and it == int(out[i, 2])
+        assert abs(out[i, 0] - sigma) <= 1e-12 * max(trial[i], 1.0) * 4
+
+
+def test_liquid_kernel_matches_oracle(lib_built):
+    import ctypes as C
+
+    import oracle
+    from litter_physics_b200 import _lib
+
+    m = oracle.material_liquid(1000.0, 1e5, 0.2, 0.5)
+    rng = np.random.default_rng(2)
+    n = 256
+    j = rng.uniform(0.98, 1.02, n)
+    g = rng.normal(scale=2.0, size=(n, 3, 3))
+    jn, tau, p = np.zeros(n), np.zeros((n, 9)), np.zeros(n)
+    st = np.zeros(n, dtype=np.int32)
+    D = C.POINTER(C.c_double)
+    _lib.check(_lib.lib().lp_update_liquid_batch(n, j.ctypes.data_as(D), np.ascontiguousarray(g).ctypes.data_as(D),
+                                                  C.byref(m), 1e-4, jn.ctypes.data_as(D), tau.ctypes.data_as(D),
+                                                  p.ctypes.data_as(D), st.ctypes.data_as(C.POINTER(C.c_int32))))
+    for i in range(n):
+        rs, rj, rtau, rp = oracle.update_liquid(j[i], g[i], m, 1e-4)
+        assert abs(jn[i] - rj) <= 1e-6
+        assert abs(p[i] - rp) <= 1e-4 * abs(m.bulk_modulus) * 1e-2 + 1e-3 * abs(rp)
+
+
+def test_batch_matches_single_instances(lib_built):
+    from litter_physics_b200 import configs
+    from litter_physics_b200.sim import Batch, Simulation
+
+    specs = [configs.slump(16, (4, 4, 8), seed=s) for s in (11, 12)] + [configs.slump(24, (6, 6, 12), seed=13)]
+    b = Batch(specs)
+    b.advance_to(40 * 1e-4)
+    for i, s in enumerate(specs):
+        one = Simulation(s)
+        one.advance_to(40 * 1e-4)
+        pb, ps = by_id(b.particles(i)), by_id(one.particles())
+        assert np.array_equal(pb["position"], ps["position"])
+        assert bytes(b.ledger(i)) == bytes(one.ledger)
