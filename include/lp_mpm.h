@@ -222,6 +222,11 @@ lp_status lp_sim_set_warm_start(lp_sim* sim, const float* weights, int32_t nweig
  * return out[0] = grid mass, out[1..3] = grid momentum (exact fixed-point sums over nodes),
  * out[4] = particle mass, out[5..7] = particle momentum (FP64 sums); the grid is then cleared. */
 lp_status lp_sim_grid_totals(lp_sim* sim, double dt, double out[8]);
+/* Grid probe: P2G + wall traction of the committed state with step dt; copies node mass
+ * (node_count), momentum (3*node_count, without reactions) and signed wall reactions
+ * (3*node_count) to the caller (node order of the dense padded grid), then clears the grid. */
+lp_status lp_sim_grid_dump(lp_sim* sim, double dt, double* mass, double* momentum, double* reaction,
+                           int64_t node_count);
 /* Time `steps` attempts kernel by kernel with CUDA events on the simulation's stream:
  * ms[k] = mean duration of kernel k, names = 32-char slots; *count = kernels per attempt. */
 lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* names, int32_t capacity,

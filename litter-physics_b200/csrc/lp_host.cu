@@ -1280,6 +1280,41 @@ lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* name
   return pull_ctrl(E);
 }
 
+lp_status lp_sim_grid_dump(lp_sim* sim, double dt, double* mass, double* momentum, double* reaction,
+                           int64_t node_count) {
+  Ensemble& E = sim->E;
+  const int64_t nn = (int64_t)E.desc[0].nodes[0] * E.desc[0].nodes[1] * E.desc[0].nodes[2];
+  if (node_count != nn) return set_error(LP_INVALID, "node_count does not match the grid");
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  E.ctrl_h[0].forced_dt = dt;
+  st = push_ctrl(E);
+  if (st != LP_OK) return st;
+  lp::launch_p2g_traction(E.A, E.stream);
+  CUDA_CK(cudaGetLastError());
+  std::vector<long long> acc(4 * nn), tr(6 * nn);
+  for (int k = 0; k < 4; ++k)
+    CUDA_CK(cudaMemcpyAsync(acc.data() + k * nn, E.A.acc + k * E.A.node_total, sizeof(long long) * nn,
+                            cudaMemcpyDeviceToHost, E.stream));
+  for (int k = 0; k < 6; ++k)
+    CUDA_CK(cudaMemcpyAsync(tr.data() + k * nn, E.A.trac + k * E.A.node_total, sizeof(long long) * nn,
+                            cudaMemcpyDeviceToHost, E.stream));
+  CUDA_CK(cudaMemsetAsync(E.A.acc, 0, sizeof(long long) * 4 * E.A.node_total, E.stream));
+  CUDA_CK(cudaMemsetAsync(E.A.trac, 0, sizeof(long long) * 6 * E.A.node_total, E.stream));
+  st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const double sm = E.desc[0].s_mass, sp = E.ctrl_h[0].s_mom;
+  for (int64_t g = 0; g < nn; ++g) {
+    if (mass) mass[g] = (double)acc[g] / sm;
+    for (int a = 0; a < 3; ++a) {
+      if (momentum) momentum[3 * g + a] = (double)acc[(1 + a) * nn + g] / sp;
+      if (reaction) reaction[3 * g + a] = ((double)tr[a * nn + g] - (double)tr[(a + 3) * nn + g]) / sp;
+    }
+  }
+  E.ctrl_h[0].forced_dt = 0.0;
+  return push_ctrl(E);
+}
+
 lp_status lp_sim_use_graph(lp_sim* sim, int32_t steps) {
   sim->E.invalidate_graph();
   sim->E.graph_steps = steps > 0 ? steps : 0;

@@ -46,63 +46,53 @@ __device__ __forceinline__ void weights_of(float fx, float dx, float w[3], float
   d[2] = (fx - 2.0f) * -dx;
 }
 
-// block-wide deterministic reductions (fixed tree)
+// block-wide deterministic reductions (fixed tree); NT need not be a power of two: the
+// entries above the largest power of two are folded in first.
 template <int NT>
-__device__ double block_sum_d(double v, double* sh) {
+struct Pow2Floor {
+  static constexpr int value = (NT & (NT - 1)) == 0 ? NT : Pow2Floor<NT & (NT - 1)>::value;
+};
+template <>
+struct Pow2Floor<0> {
+  static constexpr int value = 0;
+};
+
+template <int NT, typename T, typename Op>
+__device__ T block_reduce(T v, T* sh, Op op) {
+  constexpr int P = Pow2Floor<NT>::value;
   const int t = threadIdx.x;
   sh[t] = v;
   __syncthreads();
-  for (int s = NT / 2; s > 0; s >>= 1) {
-    if (t < s) sh[t] += sh[t + s];
+  if (P < NT) {
+    if (t < NT - P) sh[t] = op(sh[t], sh[t + P]);
     __syncthreads();
   }
-  double r = sh[0];
+  for (int s = P / 2; s > 0; s >>= 1) {
+    if (t < s) sh[t] = op(sh[t], sh[t + s]);
+    __syncthreads();
+  }
+  T r = sh[0];
   __syncthreads();
   return r;
 }
+struct AddOp {
+  template <typename T>
+  __device__ T operator()(T a, T b) const { return a + b; }
+};
+struct MaxFOp {
+  __device__ float operator()(float a, float b) const { return fmaxf(a, b); }
+};
+struct MaxIOp {
+  __device__ int operator()(int a, int b) const { return max(a, b); }
+};
 template <int NT>
-__device__ long long block_sum_ll(long long v, long long* sh) {
-  const int t = threadIdx.x;
-  sh[t] = v;
-  __syncthreads();
-  for (int s = NT / 2; s > 0; s >>= 1) {
-    if (t < s) sh[t] += sh[t + s];
-    __syncthreads();
-  }
-  long long r = sh[0];
-  __syncthreads();
-  return r;
-}
+__device__ double block_sum_d(double v, double* sh) { return block_reduce<NT>(v, sh, AddOp()); }
 template <int NT>
-__device__ float block_max_f(float v, float* sh) {
-  const int t = threadIdx.x;
-  sh[t] = v;
-  __syncthreads();
-  for (int s = NT / 2; s > 0; s >>= 1) {
-    if (t < s) sh[t] = fmaxf(sh[t], sh[t + s]);
-    __syncthreads();
-  }
-  float r = sh[0];
-  __syncthreads();
-  return r;
-}
+__device__ long long block_sum_ll(long long v, long long* sh) { return block_reduce<NT>(v, sh, AddOp()); }
 template <int NT>
-__device__ int block_max_i(int v, int* sh) {
-  const int t = threadIdx.x;
-  sh[t] = v;
-  __syncthreads();
-  for (int s = NT / 2; s > 0; s >>= 1) {
-    if (t < s) sh[t] = max(sh[t], sh[t + s]);
-    __syncthreads();
-  }
-  int r = sh[0];
-  __syncthreads();
-  return r;
-}
+__device__ float block_max_f(float v, float* sh) { return block_reduce<NT>(v, sh, MaxFOp()); }
 template <int NT>
-__device__ long long block_sum_i(long long v, long long* sh) {
-  return block_sum_ll<NT>(v, sh);
-}
+__device__ int block_max_i(int v, int* sh) { return block_reduce<NT>(v, sh, MaxIOp()); }
 
 // ============================================================== begin
 // One thread per instance: decides whether the instance attempts a step and with which dt.
@@ -411,10 +401,11 @@ __global__ void __launch_bounds__(P2G_THREADS, 1)
       }
     }
     if (slab == 0) {
+      // exact per-particle totals: FP64 products of the stored FP32 mass and velocity
       tm += to_fixed((double)m, s_m);
-      tq0 += to_fixed((double)q[0], s_p);
-      tq1 += to_fixed((double)q[1], s_p);
-      tq2 += to_fixed((double)q[2], s_p);
+      tq0 += to_fixed((double)m * (double)v[0], s_p);
+      tq1 += to_fixed((double)m * (double)v[1], s_p);
+      tq2 += to_fixed((double)m * (double)v[2], s_p);
     }
   }
   // mark the node blocks of this bin's stencil active for this attempt
@@ -1620,6 +1611,25 @@ __global__ void k_grid_sums(const long long* __restrict__ acc, int64_t node_tota
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < node_total; g += (int64_t)gridDim.x * blockDim.x)
     for (int k = 0; k < 4; ++k) v[k] += acc[k * node_total + g];
   for (int k = 0; k < 4; ++k) atomicAdd(out + k, (unsigned long long)v[k]);
+}
+
+int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
+  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count);
+  k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+                                                          A.keys, A.count, A.nw_list, A.nw_count);
+  k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
+  k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
+  k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
+  k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
+                                                            A.perm);
+  k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
+                                                                      A.perm, A.id[0], A.id[1]);
+  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
+                                                     A.perm, A.acc, A.node_total, A.blk_epoch);
+  k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
+                                     A.acc, A.trac, A.node_total);
+  g_launches += 9;
+  return 9;
 }
 
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {

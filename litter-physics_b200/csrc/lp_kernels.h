@@ -59,6 +59,7 @@ const char* attempt_kernel_name(int k, int any_pellet);
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s);
 // begin + binning + P2G only (conservation probe), then exact node sums into out[4] (int64)
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s);
+int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s);
 int launch_diagnostics(const DeviceArrays& A, int hydro, double h0, int dam, double* out, cudaStream_t s);
 uint64_t kernel_launch_count();
 void add_kernel_launches(uint64_t n);

@@ -94,6 +94,7 @@ def lib():
         "lp_sim_set_warm_start": ([P, F, I32, I32], I32),
         "lp_sim_use_graph": ([P, I32], I32),
         "lp_sim_grid_totals": ([P, C.c_double, D], I32),
+        "lp_sim_grid_dump": ([P, C.c_double, D, D, D, I64], I32),
         "lp_sim_kernel_times": ([P, I32, D, C.c_char_p, I32, C.POINTER(I32)], I32),
         "lp_sim_enable_newton_log": ([P, I64], I32),
         "lp_sim_read_newton_log": ([P, F, F, I64, C.POINTER(I64)], I32),
