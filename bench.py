@@ -220,8 +220,17 @@ def ours(args, ws, rank, local):
     _lib.build()
     stream = torch.cuda.Stream()
 
-    weights, train_info = train_warm_start(torch, args.log_steps, args.epochs)
-    spec = configs.config2() if args.workload == "config2" else configs.config0()
+    if args.no_warm:
+        weights, train_info = None, None
+    else:
+        weights, train_info = train_warm_start(torch, args.log_steps, args.epochs)
+    if args.workload == "config2":
+        spec = configs.config2()
+    elif args.workload == "small":
+        # profiling case: config-2 material and resolution pattern on a 128^3 grid, 64^3-cell column
+        spec = configs.slump(128, (64, 64, 64), seed=2, yield_range=(20.0, 100.0))
+    else:
+        spec = configs.config0()
     t0 = time.perf_counter()
     sim = Simulation(spec)
     sim.set_stream(stream.cuda_stream)
@@ -242,7 +251,8 @@ def ours(args, ws, rank, local):
     results = {}
     clocks = None
     launches = {}
-    for arm in ("plain", "warm"):
+    arms = ("plain",) if args.no_warm else ("plain", "warm")
+    for arm in arms:
         restore()
         sim.set_warm_start(weights if arm == "warm" else None)
         sim.use_graph(args.graph)
@@ -251,7 +261,7 @@ def ours(args, ws, rank, local):
         it0 = sim.counters.newton_iterations
         if dist is not None:
             dist.barrier()
-        sampler = ClockSampler(local) if arm == "warm" else None
+        sampler = ClockSampler(local) if arm == arms[-1] else None
         if sampler:
             sampler.start()
         l0 = _lib.kernel_launches()
@@ -266,12 +276,22 @@ def ours(args, ws, rank, local):
             ms = float(t.item())
         results[arm] = {"ms": ms, "accepted": accepted, "newton_iterations": int(it1 - it0),
                         "value": ws * n * accepted / (ms / 1e3)}
-    # per-kernel live timing (CUDA events on the same stream), warm arm
+    # per-kernel live timing (CUDA events on the same stream), last arm
     ktimes = sim.kernel_times(args.kernel_steps)
+    if args.no_e2e:
+        e2e_steps = 0
+    else:
+        e2e_steps = args.e2e_steps
+    if e2e_steps == 0:
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "particles": n,
+                              "results": results, "kernel_ms": ktimes}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     # end to end through the C ABI with host buffers: import -> advance -> export
     restore()
     sim.set_warm_start(weights)
-    e2e_steps = args.e2e_steps
     bytes_in = sum(v.nbytes for v in snap.values())
     torch.cuda.synchronize()
     te0 = time.perf_counter()
@@ -352,7 +372,9 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config0"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config0", "small"])
+    ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start (profiling)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and CPU legs (profiling)")
     ap.add_argument("--develop", type=int, default=150)
     ap.add_argument("--graph", type=int, default=0)
     ap.add_argument("--log-steps", type=int, default=300)

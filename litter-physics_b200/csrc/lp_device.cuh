@@ -88,6 +88,7 @@ struct InstDesc {
   int64_t gcta_off, gcta_cnt;  // grid-update CTAs
   int64_t slot_off, slot_cap;  // particle slots
   int64_t pcta_off, pcta_cnt;  // G2P CTAs
+  int64_t seg_off, seg_cnt, seg_cnt_g;  // reduction segments (grid segments first)
   // material (constitutive.rs:111-131), FP64 master copy
   double density, mu, lambda, bulk, yield, consistency, flow_index, tait_gamma;
   // config (solver.rs:48-62)
@@ -152,6 +153,15 @@ struct GridPartial {
   int fail;
   int pad;
 };
+// a reduction segment: [begin, end) of grid (kind 0) or particle (kind 1) partials of one instance
+struct SegDesc {
+  int64_t begin, end;
+  int inst, kind;
+};
+struct SegPartial {
+  double v[13];
+};
+constexpr int SEG_SPAN = 2048;
 // partial results of one G2P CTA
 struct ParticlePartial {
   double diss, bbound, mass;

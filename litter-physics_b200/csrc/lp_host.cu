@@ -463,12 +463,14 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   }
   E.n = count;
   E.specs.assign(specs, specs + count);
+  lp::configure_kernels();
   CUDA_CK(cudaStreamCreateWithFlags(&E.own_stream, cudaStreamNonBlocking));
   E.stream = E.own_stream;
   // geometry and offsets
   E.desc.resize(count);
   int64_t node_off = 0, tile_off = 0, key_off = 0, blk_off = 0, gcta_off = 0, slot_off = 0;
   std::vector<int> tile_inst, gcta_inst, pcta_inst, chunk_inst;
+  std::vector<lp::SegDesc> segs;
   int any_pellet = 0;
   for (int i = 0; i < count; ++i) {
     const lp_fixture_spec& s = specs[i];
@@ -531,6 +533,13 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
     double mass = 0.0;
     for (size_t p = 0; p < h.P.size(); ++p) mass += (double)(float)h.P.m[p];
     D.s_mass = std::ldexp(1.0, (int)std::floor(std::log2(4.611686018427388e18 / std::max(mass, 1e-300))));
+    D.seg_off = (int64_t)segs.size();
+    D.seg_cnt_g = (D.gcta_cnt + lp::SEG_SPAN - 1) / lp::SEG_SPAN;
+    for (int64_t b = 0; b < D.gcta_cnt; b += lp::SEG_SPAN)
+      segs.push_back(lp::SegDesc{D.gcta_off + b, D.gcta_off + std::min<int64_t>(b + lp::SEG_SPAN, D.gcta_cnt), i, 0});
+    for (int64_t b = 0; b < D.pcta_cnt; b += lp::SEG_SPAN)
+      segs.push_back(lp::SegDesc{D.pcta_off + b, D.pcta_off + std::min<int64_t>(b + lp::SEG_SPAN, D.pcta_cnt), i, 1});
+    D.seg_cnt = (int64_t)segs.size() - D.seg_off;
     E.desc[i] = D;
     for (int64_t t = 0; t < ntiles; ++t) tile_inst.push_back(i);
     for (int64_t t = 0; t < D.gcta_cnt; ++t) gcta_inst.push_back(i);
@@ -583,7 +592,11 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   ALLOC(A.vel, A.node_total);
   ALLOC(A.gpart, A.n_gcta);
   ALLOC(A.ppart, A.n_pcta);
+  A.n_seg = (int64_t)segs.size();
+  ALLOC(A.segs, A.n_seg);
+  ALLOC(A.seg, A.n_seg);
 #undef ALLOC
+  CUDA_CK(cudaMemcpyAsync(A.segs, segs.data(), sizeof(lp::SegDesc) * segs.size(), cudaMemcpyHostToDevice, E.stream));
   CUDA_CK(cudaMemcpyAsync(A.desc, E.desc.data(), sizeof(InstDesc) * count, cudaMemcpyHostToDevice, E.stream));
   CUDA_CK(cudaMemcpyAsync(A.pcta_inst, pcta_inst.data(), sizeof(int) * pcta_inst.size(), cudaMemcpyHostToDevice, E.stream));
   CUDA_CK(cudaMemcpyAsync(A.tile_inst, tile_inst.data(), sizeof(int) * tile_inst.size(), cudaMemcpyHostToDevice, E.stream));

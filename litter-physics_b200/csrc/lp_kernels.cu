@@ -94,6 +94,104 @@ __device__ float block_max_f(float v, float* sh) { return block_reduce<NT>(v, sh
 template <int NT>
 __device__ int block_max_i(int v, int* sh) { return block_reduce<NT>(v, sh, MaxIOp()); }
 
+// Multi-value block reductions with a fixed warp butterfly (__shfl_xor_sync) followed by one
+// shared-memory pass in warp 0: deterministic, two barriers.  Bit k of max_mask selects max
+// instead of sum for value k.  The results are returned to every thread.
+template <int K>
+__device__ __forceinline__ void warp_reduce_multi(double (&v)[K], unsigned max_mask) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double other = __shfl_xor_sync(0xffffffffu, v[k], o);
+      v[k] = ((max_mask >> k) & 1u) ? fmax(v[k], other) : v[k] + other;
+    }
+  }
+}
+template <int NT, int K>
+__device__ void block_reduce_multi(double (&v)[K], unsigned max_mask, double* sh /* NT/32*K + K */) {
+  constexpr int NW = NT / 32;
+  static_assert(NT % 32 == 0 && NW <= 32, "block size");
+  warp_reduce_multi<K>(v, max_mask);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) sh[w * K + k] = v[k];
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = lane < NW ? sh[lane * K + k] : (((max_mask >> k) & 1u) ? -1e300 : 0.0);
+    warp_reduce_multi<K>(v, max_mask);
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) sh[NW * K + k] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = sh[NW * K + k];
+  __syncthreads();
+}
+template <int K>
+__device__ __forceinline__ void warp_sum_ll_multi(long long (&v)[K]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+}
+template <int NT, int K>
+__device__ void block_sum_ll_multi(long long (&v)[K], long long* sh /* NT/32*K + K */) {
+  constexpr int NW = NT / 32;
+  warp_sum_ll_multi<K>(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) sh[w * K + k] = v[k];
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = lane < NW ? sh[lane * K + k] : 0;
+    warp_sum_ll_multi<K>(v);
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) sh[NW * K + k] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = sh[NW * K + k];
+  __syncthreads();
+}
+// argmax of (value, index) over the block: largest value, lowest index on ties
+template <int NT>
+__device__ int block_argmax_ll(long long value, int index, long long* shv, int* shi) {
+  constexpr int NW = NT / 32;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const long long ov = __shfl_xor_sync(0xffffffffu, value, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, index, o);
+    if (ov > value || (ov == value && oi < index)) {
+      value = ov;
+      index = oi;
+    }
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    shv[w] = value;
+    shi[w] = index;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < NW; ++k)
+      if (shv[k] > shv[0] || (shv[k] == shv[0] && shi[k] < shi[0])) {
+        shv[0] = shv[k];
+        shi[0] = shi[k];
+      }
+  }
+  __syncthreads();
+  const int r = shi[0];
+  __syncthreads();
+  return r;
+}
+
 // ============================================================== begin
 // One thread per instance: decides whether the instance attempts a step and with which dt.
 __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, int n_inst,
@@ -308,19 +406,19 @@ __global__ void k_bin_sort(const InstDesc* __restrict__ desc, const Control* __r
 // ============================================================== P2G
 // One CTA per tile of TX x TY x TZ bins; three threads per bin, one per slab a of the 3x3x3
 // stencil.  All particles of a bin share the same 27 target nodes, so each thread accumulates
-// its 9 nodes x (mass, momentum) in registers over the bin's particles, then the tile's halo is
-// combined in shared memory in 27 fixed rounds (deterministic, no atomics), converted to int64
-// fixed point with an exact-conservation correction, and flushed with one global atomic per
-// node component.
-__global__ void __launch_bounds__(P2G_THREADS, 1)
+// its 9 nodes x (mass, momentum) in registers over the bin's particles.  The partial sums go to
+// shared memory; then one thread per halo node adds its 27 contributors in a fixed order
+// (deterministic, no atomics, one barrier), converts to int64 fixed point, the tile's exact
+// particle totals are restored by a proportional correction, and each node component is
+// flushed with one global atomic.
+__global__ void __launch_bounds__(P2G_THREADS, 2)
     k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
           const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
           int64_t node_total, uint32_t* __restrict__ blk_epoch) {
-  __shared__ float h[4][HN];
-  __shared__ long long hi[4][HN];
-  __shared__ long long red[P2G_THREADS];
-  __shared__ int bestidx[P2G_THREADS];
+  extern __shared__ float4 part[];  // TB * 27 partial node sums (dynamic: 55 KB)
+  __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
+  __shared__ int redi[P2G_THREADS / 32];
 
   const int tile = blockIdx.x;
   const int inst = tile_inst[tile];
@@ -339,11 +437,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 1)
   const int lx = bin / (TY * TZ), ly = (bin / TZ) % TY, lz = bin % TZ;
   const int bx = tx * TX + lx, by = ty * TY + ly, bz = tz * TZ + lz;
 
-  for (int j = t; j < 4 * HN; j += P2G_THREADS) (&h[0][0])[j] = 0.0f;
-
   const float* cur = c.parity ? st1 : st0;
   const float dx = (float)D.dx;
-  const float dt = (float)c.dt;
   const float stress_scale = (float)(c.dt * 4.0 / (D.dx * D.dx));
   const double s_m = D.s_mass, s_p = c.s_mom;
 
@@ -354,7 +449,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 1)
     for (int q = 0; q < 3; ++q)
 #pragma unroll
       for (int k = 0; k < 4; ++k) acc9[b][q][k] = 0.0f;
-  long long tm = 0, tq0 = 0, tq1 = 0, tq2 = 0;
+  long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // tile totals (particles) then halo sums (nodes)
 
   const uint32_t s = start[key0 + bin], e = start[key0 + bin + 1];
   const float basef[3] = {(float)(bx - 1), (float)(by - 1), (float)(bz - 1)};
@@ -402,14 +497,14 @@ __global__ void __launch_bounds__(P2G_THREADS, 1)
     }
     if (slab == 0) {
       // exact per-particle totals: FP64 products of the stored FP32 mass and velocity
-      tm += to_fixed((double)m, s_m);
-      tq0 += to_fixed((double)m * (double)v[0], s_p);
-      tq1 += to_fixed((double)m * (double)v[1], s_p);
-      tq2 += to_fixed((double)m * (double)v[2], s_p);
+      tot[0] += to_fixed((double)m, s_m);
+      tot[1] += to_fixed((double)m * (double)v[0], s_p);
+      tot[2] += to_fixed((double)m * (double)v[1], s_p);
+      tot[3] += to_fixed((double)m * (double)v[2], s_p);
     }
   }
-  // mark the node blocks of this bin's stencil active for this attempt
   if (e > s) {
+    // mark the node blocks of this bin's stencil active for this attempt
     for (int b = 0; b < 3; ++b)
       for (int cc = 0; cc < 3; ++cc) {
         const int nx = bx + slab, ny = by + b, nz = bz + cc;
@@ -417,100 +512,85 @@ __global__ void __launch_bounds__(P2G_THREADS, 1)
         blk_epoch[blk] = (uint32_t)c.epoch;
       }
   }
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc)
+      part[bin * 27 + slab * 9 + b * 3 + cc] =
+          make_float4(acc9[b][cc][0], acc9[b][cc][1], acc9[b][cc][2], acc9[b][cc][3]);
   __syncthreads();
-  // halo combine: 27 rounds, each conflict-free
+  // one thread per halo node: sum the 27 contributing (bin, slab) partials in a fixed order
+  long long nv[4] = {0, 0, 0, 0};
+  int hx = 0, hy = 0, hz = 0;
+  const bool has_node = t < HN;
+  if (has_node) {
+    hz = t % HZ;
+    hy = (t / HZ) % HY;
+    hx = t / (HZ * HY);
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
-  for (int a = 0; a < 3; ++a)
+    for (int a = 0; a < 3; ++a) {
+      const int lbx = hx - a;
+      if (lbx < 0 || lbx >= TX) continue;
 #pragma unroll
-    for (int b = 0; b < 3; ++b)
+      for (int b = 0; b < 3; ++b) {
+        const int lby = hy - b;
+        if (lby < 0 || lby >= TY) continue;
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        if (slab == a) {
-          const int n = ((lx + a) * HY + (ly + b)) * HZ + (lz + cc);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) h[k][n] += acc9[b][cc][k];
+        for (int cc = 0; cc < 3; ++cc) {
+          const int lbz = hz - cc;
+          if (lbz < 0 || lbz >= TZ) continue;
+          const float4 q = part[((lbx * TY + lby) * TZ + lbz) * 27 + a * 9 + b * 3 + cc];
+          s0 += q.x;
+          s1 += q.y;
+          s2 += q.z;
+          s3 += q.w;
         }
-        __syncthreads();
       }
-  // exact per-tile totals
-  tm = block_sum_ll<P2G_THREADS>(tm, red);
-  tq0 = block_sum_ll<P2G_THREADS>(tq0, red);
-  tq1 = block_sum_ll<P2G_THREADS>(tq1, red);
-  tq2 = block_sum_ll<P2G_THREADS>(tq2, red);
-  // convert halo to fixed point
-  long long sm = 0, sp0 = 0, sp1 = 0, sp2 = 0;
-  for (int n = t; n < HN; n += P2G_THREADS) {
-    hi[0][n] = to_fixed((double)h[0][n], s_m);
-    hi[1][n] = to_fixed((double)h[1][n], s_p);
-    hi[2][n] = to_fixed((double)h[2][n], s_p);
-    hi[3][n] = to_fixed((double)h[3][n], s_p);
-    sm += hi[0][n];
-    sp0 += hi[1][n];
-    sp1 += hi[2][n];
-    sp2 += hi[3][n];
+    }
+    nv[0] = to_fixed((double)s0, s_m);
+    nv[1] = to_fixed((double)s1, s_p);
+    nv[2] = to_fixed((double)s2, s_p);
+    nv[3] = to_fixed((double)s3, s_p);
+    tot[4] = nv[0];
+    tot[5] = nv[1];
+    tot[6] = nv[2];
+    tot[7] = nv[3];
   }
-  sm = block_sum_ll<P2G_THREADS>(sm, red);
-  sp0 = block_sum_ll<P2G_THREADS>(sp0, red);
-  sp1 = block_sum_ll<P2G_THREADS>(sp1, red);
-  sp2 = block_sum_ll<P2G_THREADS>(sp2, red);
-  const long long Dm = tm - sm, D0 = tq0 - sp0, D1 = tq1 - sp1, D2 = tq2 - sp2;
+  block_sum_ll_multi<P2G_THREADS, 8>(tot, red);
+  const long long Dm = tot[0] - tot[4], D0 = tot[1] - tot[5], D1 = tot[2] - tot[6], D2 = tot[3] - tot[7];
   if (Dm != 0 || D0 != 0 || D1 != 0 || D2 != 0) {
     // distribute the discrepancy in proportion to node mass, remainder to the heaviest node
-    long long cm = 0, c0 = 0, c1 = 0, c2 = 0;
-    long long bestv = LLONG_MIN;
-    int bestn = HN;
-    const double inv = sm > 0 ? 1.0 / (double)sm : 0.0;
-    for (int n = t; n < HN; n += P2G_THREADS) {
-      const double f = (double)hi[0][n] * inv;
-      if (hi[0][n] > bestv) {
-        bestv = hi[0][n];
-        bestn = n;
-      }
-      const long long a0 = __double2ll_rn((double)Dm * f), a1 = __double2ll_rn((double)D0 * f),
-                      a2 = __double2ll_rn((double)D1 * f), a3 = __double2ll_rn((double)D2 * f);
-      hi[0][n] += a0;
-      hi[1][n] += a1;
-      hi[2][n] += a2;
-      hi[3][n] += a3;
-      cm += a0;
-      c0 += a1;
-      c1 += a2;
-      c2 += a3;
+    long long cs[4] = {0, 0, 0, 0};
+    if (has_node) {
+      const double f = tot[4] > 0 ? (double)nv[0] / (double)tot[4] : 0.0;
+      cs[0] = __double2ll_rn((double)Dm * f);
+      cs[1] = __double2ll_rn((double)D0 * f);
+      cs[2] = __double2ll_rn((double)D1 * f);
+      cs[3] = __double2ll_rn((double)D2 * f);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) nv[k] += cs[k];
     }
-    cm = block_sum_ll<P2G_THREADS>(cm, red);
-    c0 = block_sum_ll<P2G_THREADS>(c0, red);
-    c1 = block_sum_ll<P2G_THREADS>(c1, red);
-    c2 = block_sum_ll<P2G_THREADS>(c2, red);
-    red[t] = bestv;
-    bestidx[t] = bestn;
-    __syncthreads();
-    if (t == 0) {
-      long long bv = LLONG_MIN;
-      int bn = 0;
-      for (int k = 0; k < P2G_THREADS; ++k)
-        if (red[k] > bv || (red[k] == bv && bestidx[k] < bn)) {
-          bv = red[k];
-          bn = bestidx[k];
-        }
-      hi[0][bn] += Dm - cm;
-      hi[1][bn] += D0 - c0;
-      hi[2][bn] += D1 - c1;
-      hi[3][bn] += D2 - c2;
+    const long long heavy = has_node ? nv[0] : LLONG_MIN;
+    const int best = block_argmax_ll<P2G_THREADS>(heavy, t, red, redi);
+    block_sum_ll_multi<P2G_THREADS, 4>(cs, red);
+    if (t == best) {
+      nv[0] += Dm - cs[0];
+      nv[1] += D0 - cs[1];
+      nv[2] += D1 - cs[2];
+      nv[3] += D2 - cs[3];
     }
-    __syncthreads();
   }
   // flush to the global grid
-  for (int n = t; n < HN; n += P2G_THREADS) {
-    const long long vm = hi[0][n], v0 = hi[1][n], v1 = hi[2][n], v2 = hi[3][n];
-    if ((vm | v0 | v1 | v2) == 0) continue;
-    const int hz = n % HZ, hy = (n / HZ) % HY, hx = n / (HZ * HY);
+  if (has_node && (nv[0] | nv[1] | nv[2] | nv[3]) != 0) {
     const int nx = tx * TX + hx, ny = ty * TY + hy, nz = tz * TZ + hz;
-    if (nx >= D.nodes[0] || ny >= D.nodes[1] || nz >= D.nodes[2]) continue;
-    const int64_t g = node_index(D, nx, ny, nz);
-    atomic_add_ll(acc + g, vm);
-    atomic_add_ll(acc + node_total + g, v0);
-    atomic_add_ll(acc + 2 * node_total + g, v1);
-    atomic_add_ll(acc + 3 * node_total + g, v2);
+    if (nx < D.nodes[0] && ny < D.nodes[1] && nz < D.nodes[2]) {
+      const int64_t g = node_index(D, nx, ny, nz);
+      atomic_add_ll(acc + g, nv[0]);
+      atomic_add_ll(acc + node_total + g, nv[1]);
+      atomic_add_ll(acc + 2 * node_total + g, nv[2]);
+      atomic_add_ll(acc + 3 * node_total + g, nv[3]);
+    }
   }
 }
 
@@ -626,8 +706,7 @@ __global__ void __launch_bounds__(GU_THREADS)
                   const int* __restrict__ gcta_inst, long long* __restrict__ acc, long long* __restrict__ trac,
                   int64_t node_total, const uint32_t* __restrict__ blk_epoch, float4* __restrict__ vel,
                   GridPartial* __restrict__ part) {
-  __shared__ double shd[GU_THREADS];
-  __shared__ int shi[GU_THREADS];
+  __shared__ double shd[(GU_THREADS / 32) * 7 + 7];
   const int inst = gcta_inst[blockIdx.x];
   const Control& c = ctrl[inst];
   if (!c.active) return;
@@ -647,6 +726,15 @@ __global__ void __launch_bounds__(GU_THREADS)
     nj = bj * NB + (l / 4) % 4;
     nk = bk * NB + l % 4;
     live = ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2];
+  }
+  if (!__syncthreads_or(live ? 1 : 0)) {
+    if (t == 0) {
+      GridPartial& P = part[blockIdx.x];
+      P.wall_impulse[0] = P.wall_impulse[1] = P.wall_impulse[2] = 0.0;
+      P.proj = P.fric = P.trac = 0.0;
+      P.fail = F_OK;
+    }
+    return;
   }
   if (live) {
     const int64_t g = node_index(D, ni, nj, nk);
@@ -751,13 +839,15 @@ __global__ void __launch_bounds__(GU_THREADS)
       }
     }
   }
-  wi0 = block_sum_d<GU_THREADS>(wi0, shd);
-  wi1 = block_sum_d<GU_THREADS>(wi1, shd);
-  wi2 = block_sum_d<GU_THREADS>(wi2, shd);
-  proj = block_sum_d<GU_THREADS>(proj, shd);
-  fric = block_sum_d<GU_THREADS>(fric, shd);
-  tren = block_sum_d<GU_THREADS>(tren, shd);
-  fail = block_max_i<GU_THREADS>(fail, shi);
+  double rv[7] = {wi0, wi1, wi2, proj, fric, tren, (double)fail};
+  block_reduce_multi<GU_THREADS, 7>(rv, 1u << 6, shd);
+  wi0 = rv[0];
+  wi1 = rv[1];
+  wi2 = rv[2];
+  proj = rv[3];
+  fric = rv[4];
+  tren = rv[5];
+  fail = (int)rv[6];
   if (t == 0) {
     GridPartial& P = part[blockIdx.x];
     P.wall_impulse[0] = wi0;
@@ -1029,16 +1119,13 @@ __global__ void k_couple(const InstDesc* __restrict__ desc, Control* __restrict_
 }
 
 // ============================================================== G2P + constitutive
-__global__ void __launch_bounds__(G2P_THREADS)
+__global__ void __launch_bounds__(G2P_THREADS, 2)
     k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ pcta_inst,
           float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
           int64_t cap, const uint32_t* __restrict__ perm, const float4* __restrict__ vel,
           ParticlePartial* __restrict__ part, const float* __restrict__ mlp, float* __restrict__ log_x,
           float* __restrict__ log_y, unsigned long long* __restrict__ log_n, long long log_cap) {
-  __shared__ double shd[G2P_THREADS];
-  __shared__ float shf[G2P_THREADS];
-  __shared__ int shi[G2P_THREADS];
-  __shared__ long long shl[G2P_THREADS];
+  __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
   const int inst = pcta_inst[blockIdx.x];
   const Control& c = ctrl[inst];
   if (!c.active) return;
@@ -1190,14 +1277,18 @@ __global__ void __launch_bounds__(G2P_THREADS)
     max_speed = speed;
     max_disp = disp;
   }
-  diss = block_sum_d<G2P_THREADS>(diss, shd);
-  bb = block_sum_d<G2P_THREADS>(bb, shd);
-  mass_sum = block_sum_d<G2P_THREADS>(mass_sum, shd);
-  max_speed = block_max_f<G2P_THREADS>(max_speed, shf);
-  max_disp = block_max_f<G2P_THREADS>(max_disp, shf);
-  const int fail_all = block_max_i<G2P_THREADS>(fail, shi);
-  const long long it_all = block_sum_ll<G2P_THREADS>(iters, shl);
-  const long long y_all = block_sum_ll<G2P_THREADS>(yielded, shl);
+  double rv[9] = {diss, bb, mass_sum, (double)max_speed, (double)max_disp, (double)fail, (double)iters,
+                  (double)yielded, fail_value};
+  block_reduce_multi<G2P_THREADS, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
+  diss = rv[0];
+  bb = rv[1];
+  mass_sum = rv[2];
+  max_speed = (float)rv[3];
+  max_disp = (float)rv[4];
+  const int fail_all = (int)rv[5];
+  const long long it_all = (long long)rv[6];
+  const long long y_all = (long long)rv[7];
+  fail_value = rv[8];
   if (threadIdx.x == 0) {
     ParticlePartial& P = part[blockIdx.x];
     P.diss = diss;
@@ -1213,58 +1304,73 @@ __global__ void __launch_bounds__(G2P_THREADS)
 }
 
 // ============================================================== end of attempt
+// Level 1: one CTA per segment of at most SEG_SPAN grid or particle partials of one instance,
+// reduced in a fixed order.  Level 2 (k_end): the instance's segments in order.
+__global__ void k_segments(const Control* __restrict__ ctrl, const SegDesc* __restrict__ segs,
+                           const GridPartial* __restrict__ gpart, const ParticlePartial* __restrict__ ppart,
+                           SegPartial* __restrict__ out) {
+  __shared__ double shd[(256 / 32) * 13 + 13];
+  const SegDesc sd = segs[blockIdx.x];
+  if (!ctrl[sd.inst].active) return;
+  const int t = threadIdx.x;
+  // sums: wi0 wi1 wi2 proj fric trac diss bb its yl; max: ms md fail
+  double v[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (sd.kind == 0) {
+    for (int64_t j = sd.begin + t; j < sd.end; j += 256) {
+      const GridPartial& P = gpart[j];
+      v[0] += P.wall_impulse[0];
+      v[1] += P.wall_impulse[1];
+      v[2] += P.wall_impulse[2];
+      v[3] += P.proj;
+      v[4] += P.fric;
+      v[5] += P.trac;
+      v[12] = fmax(v[12], (double)P.fail);
+    }
+  } else {
+    for (int64_t j = sd.begin + t; j < sd.end; j += 256) {
+      const ParticlePartial& P = ppart[j];
+      v[6] += P.diss;
+      v[7] += P.bbound;
+      v[8] += (double)P.iterations;
+      v[9] += (double)P.yielded;
+      v[10] = fmax(v[10], (double)P.max_speed);
+      v[11] = fmax(v[11], (double)P.max_disp);
+      v[12] = fmax(v[12], (double)P.fail);
+    }
+  }
+  block_reduce_multi<256, 13>(v, (1u << 10) | (1u << 11) | (1u << 12), shd);
+  if (t == 0) {
+    SegPartial& o = out[blockIdx.x];
+    for (int k = 0; k < 13; ++k) o.v[k] = v[k];
+  }
+}
+
 __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
-                      const GridPartial* __restrict__ gpart, const ParticlePartial* __restrict__ ppart) {
-  __shared__ double shd[256];
-  __shared__ float shf[256];
-  __shared__ int shi[256];
-  __shared__ long long shl[256];
+                      const SegPartial* __restrict__ seg) {
+  __shared__ double shd[(256 / 32) * 15 + 15];
   const int inst = blockIdx.x;
   Control& c = ctrl[inst];
   if (!c.active) return;
   const InstDesc& D = desc[inst];
   const int t = threadIdx.x;
-  // fixed-order reductions
-  double wi[3] = {0, 0, 0}, proj = 0, fric = 0, trac = 0;
-  int fail = F_OK;
-  for (int64_t j = t; j < D.gcta_cnt; j += 256) {
-    const GridPartial& P = gpart[D.gcta_off + j];
-    // CTAs with no live block did not write; their entries were zeroed by the host at creation
-    wi[0] += P.wall_impulse[0];
-    wi[1] += P.wall_impulse[1];
-    wi[2] += P.wall_impulse[2];
-    proj += P.proj;
-    fric += P.fric;
-    trac += P.trac;
-    fail = max(fail, P.fail);
+  // v: wi0 wi1 wi2 proj fric trac diss bb its yl | ms md | grid fail, particle fail (max)
+  double v[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t j = t; j < D.seg_cnt; j += 256) {
+    const SegPartial& P = seg[D.seg_off + j];
+    const bool grid = j < D.seg_cnt_g;
+    for (int k = 0; k < 10; ++k) v[k] += P.v[k];
+    v[10] = fmax(v[10], P.v[10]);
+    v[11] = fmax(v[11], P.v[11]);
+    if (grid) v[12] = fmax(v[12], P.v[12]);
+    else v[13] = fmax(v[13], P.v[12]);
   }
-  double diss = 0, bb = 0;
-  float ms = 0.f, md = 0.f;
-  long long its = 0, yl = 0;
-  int pfail = F_OK;
-  for (int64_t j = t; j < D.pcta_cnt; j += 256) {
-    const ParticlePartial& P = ppart[D.pcta_off + j];
-    diss += P.diss;
-    bb += P.bbound;
-    ms = fmaxf(ms, P.max_speed);
-    md = fmaxf(md, P.max_disp);
-    pfail = max(pfail, P.fail);
-    its += P.iterations;
-    yl += P.yielded;
-  }
-  for (int a = 0; a < 3; ++a) wi[a] = block_sum_d<256>(wi[a], shd);
-  proj = block_sum_d<256>(proj, shd);
-  fric = block_sum_d<256>(fric, shd);
-  trac = block_sum_d<256>(trac, shd);
-  diss = block_sum_d<256>(diss, shd);
-  bb = block_sum_d<256>(bb, shd);
-  ms = block_max_f<256>(ms, shf);
-  md = block_max_f<256>(md, shf);
-  fail = block_max_i<256>(fail, shi);
-  pfail = block_max_i<256>(pfail, shi);
-  its = block_sum_ll<256>(its, shl);
-  yl = block_sum_ll<256>(yl, shl);
+  block_reduce_multi<256, 14>(v, (1u << 10) | (1u << 11) | (1u << 12) | (1u << 13), shd);
   if (t != 0) return;
+  const double wi[3] = {v[0], v[1], v[2]};
+  const double proj = v[3], fric = v[4], trac = v[5], diss = v[6], bb = v[7];
+  const long long its = (long long)v[8], yl = (long long)v[9];
+  const float ms = (float)v[10], md = (float)v[11];
+  const int fail = (int)v[12], pfail = (int)v[13];
   int f = F_OK;
   if (!isfinite(trac) || !isfinite(c.ledger.trac + trac)) f = F_TRACTION_NONFINITE;
   else if (fail != F_OK) f = fail;
@@ -1545,6 +1651,11 @@ __global__ void k_liquid_batch(int64_t n, const double* j, const double* grad, d
 
 // ============================================================== launchers
 static uint64_t g_launches = 0;
+constexpr size_t P2G_SMEM = sizeof(float4) * TB * 27;
+
+void configure_kernels() {
+  cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM);
+}
 uint64_t kernel_launch_count() { return g_launches; }
 void add_kernel_launches(uint64_t n) { g_launches += n; }
 
@@ -1577,7 +1688,7 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
                                                                       A.perm, A.id[0], A.id[1]);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
+  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
                                                      A.perm, A.acc, A.node_total, A.blk_epoch);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
@@ -1599,7 +1710,10 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
                                                     A.log_cap);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_end<<<A.n_inst, 256, 0, s>>>(A.desc, A.ctrl, A.gpart, A.ppart);
+  k_segments<<<(unsigned)A.n_seg, 256, 0, s>>>(A.ctrl, A.segs, A.gpart, A.ppart, A.seg);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_end<<<A.n_inst, 256, 0, s>>>(A.desc, A.ctrl, A.seg);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   g_launches += (uint64_t)n;
@@ -1624,7 +1738,7 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
                                                             A.perm);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
                                                                       A.perm, A.id[0], A.id[1]);
-  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
+  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
                                                      A.perm, A.acc, A.node_total, A.blk_epoch);
   k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
                                      A.acc, A.trac, A.node_total);
@@ -1643,7 +1757,7 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
                                                             A.perm);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
                                                                       A.perm, A.id[0], A.id[1]);
-  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
+  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
                                                      A.perm, A.acc, A.node_total, A.blk_epoch);
   k_grid_sums<<<148 * 4, 256, 0, s>>>(A.acc, A.node_total, (unsigned long long*)out);
   g_launches += 9;
@@ -1655,9 +1769,9 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return launch_attemp
 const char* attempt_kernel_name(int k, int any_pellet) {
   static const char* a[] = {"k_begin", "k_bin_count", "k_scan_chunks", "k_scan_instances", "k_scan_apply",
                             "k_bin_scatter", "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple",
-                            "k_g2p", "k_end"};
+                            "k_g2p", "k_segments", "k_end"};
   if (!any_pellet && k >= 10) ++k;
-  return k < 13 ? a[k] : "?";
+  return k < 14 ? a[k] : "?";
 }
 
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s) {

@@ -43,6 +43,9 @@ struct DeviceArrays {
   float4* vel = nullptr;
   GridPartial* gpart = nullptr;
   ParticlePartial* ppart = nullptr;
+  SegDesc* segs = nullptr;  // reduction segments
+  SegPartial* seg = nullptr;
+  int64_t n_seg = 0;
   float* mlp = nullptr;  // warm-start weights (device) or null
   float* log_x = nullptr;
   float* log_y = nullptr;
@@ -62,6 +65,7 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s);
 int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s);
 int launch_diagnostics(const DeviceArrays& A, int hydro, double h0, int dam, double* out, cudaStream_t s);
 uint64_t kernel_launch_count();
+void configure_kernels();  // one-time function attributes (dynamic shared memory)
 void add_kernel_launches(uint64_t n);
 
 // constitutive unit kernels on device arrays
