@@ -960,6 +960,8 @@ lp_status observables(Ensemble& E, int i, std::map<std::string, double>& out) {
 
 }  // namespace
 
+void lp::set_last_error(const char* msg) { g_err = msg; }
+
 // ================================================================ C ABI
 struct lp_sim {
   Ensemble E;

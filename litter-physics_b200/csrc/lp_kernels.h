@@ -65,7 +65,8 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s);
 int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s);
 int launch_diagnostics(const DeviceArrays& A, int hydro, double h0, int dam, double* out, cudaStream_t s);
 uint64_t kernel_launch_count();
-void configure_kernels();  // one-time function attributes (dynamic shared memory)
+void configure_kernels();              // one-time function attributes (dynamic shared memory)
+void set_last_error(const char* msg);  // message returned by lp_last_error()
 void add_kernel_launches(uint64_t n);
 
 // constitutive unit kernels on device arrays

@@ -147,7 +147,7 @@ namespace {
 thread_local std::string g_mlp_err;
 lp_status mlp_fail(lp_status s, const std::string& m) {
   g_mlp_err = m;
-  std::fprintf(stderr, "lp_mlp: %s\n", m.c_str());
+  lp::set_last_error(m.c_str());
   return s;
 }
 #define MCK(expr)                                                                                 \

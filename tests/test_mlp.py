@@ -1,0 +1,104 @@
+"""Learned warm start: CPU checks of the oracle network and the feature map, GPU checks of the
+device forward/backward kernels against the FP64 oracle, training, and the gain of the trained
+network over the midpoint start at equal tolerance."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+def test_oracle_gradient_matches_finite_differences():
+    import mlp_oracle as M
+
+    rng = np.random.default_rng(0)
+    w = rng.normal(scale=0.3, size=M.NW)
+    x = rng.normal(size=(64, 6))
+    y = rng.normal(size=64)
+    _, g = M.loss_grad(w, x, y)
+    idx = [0, 5, M.B1 + 3, M.W2 + 100, M.W2 + 4000, M.B2 + 7, M.W3 + 10, M.B3]
+    fd = M.finite_difference(w, x, y, idx)
+    assert np.allclose(g[idx], fd, rtol=1e-5, atol=1e-9)
+
+
+def test_feature_map_matches_device_definition():
+    import ctypes as C
+
+    from litter_physics_b200 import _lib, warmstart
+
+    _lib.build()
+    raw = np.array([[120.0, 86.6, 11.4, 0.5, 2e4, 1e-4], [300.0, 40.0, 3.0, 0.9, 5e3, 1e-3]])
+    f = warmstart.features(raw)
+    for i in range(len(raw)):
+        out = (C.c_float * 6)()
+        _lib.lib().lp_hb_features(*[float(v) for v in raw[i]], out)
+        assert np.allclose(np.array(out), f[i], rtol=1e-6, atol=1e-7)
+
+
+def test_targets_invert_to_the_root():
+    from litter_physics_b200 import warmstart
+
+    raw = np.array([[120.0, 86.6, 11.4, 0.5, 2e4, 1e-4]])
+    sigma = np.array([100.0])
+    t = 1.0 / (1.0 + np.exp(-warmstart.targets(raw, sigma).astype(np.float64)))
+    assert abs(86.6 + t[0] * (120.0 - 86.6) - 100.0) < 1e-3
+
+
+@pytest.mark.gpu
+def test_device_gradient_matches_fp64_oracle():
+    import mlp_oracle as M
+
+    from litter_physics_b200 import _lib, warmstart
+
+    _lib.build()
+    rng = np.random.default_rng(1)
+    w = warmstart.init_weights(seed=7)
+    x = rng.normal(size=(2048, 6)).astype(np.float32)
+    y = rng.normal(size=2048).astype(np.float32)
+    loss, g = warmstart.loss_grad(w, x, y)
+    rloss, rg = M.loss_grad(w.astype(np.float64), x, y)
+    assert abs(loss - rloss) <= 1e-5 * abs(rloss)
+    assert np.abs(g - rg).max() <= 1e-4 * np.abs(rg).max()
+    yp = warmstart.predict(w, x[:100])
+    assert np.allclose(yp, M.forward(w, x[:100]), rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.gpu
+def test_trained_network_cuts_newton_iterations_at_equal_tolerance():
+    """Train on pairs the plain Newton logs during a slump, then solve fresh return problems
+    with and without the warm start: same residual tolerance, fewer iterations."""
+    import ctypes as C
+
+    from litter_physics_b200 import _lib, configs, warmstart
+    from litter_physics_b200.sim import Simulation
+
+    _lib.build()
+    sim = Simulation(configs.slump(32, (8, 8, 16), seed=3, yield_range=(20.0, 100.0)))
+    raw, sigma = warmstart.collect(sim, 150, capacity=1_000_000)
+    x, y = warmstart.dataset(raw, sigma)
+    assert len(y) > 1000
+    w, loss = warmstart.train(x, y, epochs=20, batch=1024, lr=2e-3)
+    assert loss < 0.05
+    # fresh problems from a different slump
+    sim2 = Simulation(configs.slump(32, (8, 8, 16), seed=9, yield_range=(20.0, 100.0)))
+    raw2, _ = warmstart.collect(sim2, 120, capacity=200_000)
+    r = raw2.astype(np.float64)
+    n = len(r)
+    D = C.POINTER(C.c_double)
+    cols = [np.ascontiguousarray(r[:, i]) for i in range(6)]
+    res = {}
+    for name, weights in (("plain", None), ("warm", w)):
+        out = np.zeros((n, 3))
+        st = np.zeros(n, dtype=np.int32)
+        wp = weights.ctypes.data_as(C.POINTER(C.c_float)) if weights is not None else None
+        _lib.check(_lib.lib().lp_hb_return_batch(n, *[c.ctypes.data_as(D) for c in cols], 1e-10, wp,
+                                                  warmstart.NW if weights is not None else 0,
+                                                  out.ctypes.data_as(D), st.ctypes.data_as(C.POINTER(C.c_int32))))
+        assert (st == 0).all()
+        res[name] = out
+    # equal residual tolerance: both meet the stopping rule; the returned stress agrees to it
+    tol = 1e-10 * np.maximum(r[:, 0], 1.0)
+    assert np.all(np.abs(res["plain"][:, 0] - res["warm"][:, 0]) <= 10 * tol + 1e-9 * r[:, 0])
+    it_plain, it_warm = res["plain"][:, 2].mean(), res["warm"][:, 2].mean()
+    print(f"mean Newton iterations: plain {it_plain:.3f}, warm {it_warm:.3f}")
+    assert it_warm < 0.8 * it_plain
