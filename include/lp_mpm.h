@@ -278,6 +278,21 @@ lp_status lp_mlp_forward(const float* weights, int32_t nweights, const float* x,
 /* Loss and gradient of mean squared error over n samples (FP32), for gradient checks. */
 lp_status lp_mlp_loss_grad(const float* weights, int32_t nweights, const float* x, const float* y,
                            int64_t n, float* loss, float* grad);
+/* Loss and gradient of the warm-start network without allocating any device memory.
+ * No counterpart in the reference.  Meant for callers that cannot call cudaMalloc, such as a
+ * host framework that owns all device memory through its own pool, or code running while
+ * allocation is forbidden.  Inputs and outputs are caller-owned DEVICE pointers:
+ * weights[lp_mlp_weight_count()], x[6*n], y[n] in; loss[1], grad[lp_mlp_weight_count()] out.
+ * Work space is a fixed static device array of the library sized for at most
+ * LP_MLP_NOALLOC_MAX_SAMPLES samples (about 4.5 MB per GPU that loads the library, held until
+ * exit); larger n returns LP_INVALID.  The first call on each device looks up that array's
+ * device address, so make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.  stream is a cudaStream_t (NULL = default stream); the call
+ * returns after queueing the work. */
+#define LP_MLP_NOALLOC_MAX_SAMPLES 4096
+lp_status lp_mlp_loss_grad_noalloc(const float* weights, const float* x, const float* y, int64_t n, float* loss,
+                                   float* grad, void* stream);
 /* Feature map of one return problem: trial stress, yield, consistency, flow index, mu, dt. */
 void lp_hb_features(double trial, double yield, double consistency, double flow_index, double mu,
                     double dt, float out[6]);

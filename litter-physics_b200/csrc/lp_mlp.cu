@@ -133,6 +133,13 @@ __global__ void k_mlp_adam(float* __restrict__ W, const float* __restrict__ grad
   W[w] -= lr * ah / (sqrtf(bh) + 1e-8f);
 }
 
+__global__ void k_mlp_loss_final(const float* __restrict__ part, int nparts, int64_t n, float* __restrict__ loss) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double s = 0.0;
+  for (int i = 0; i < nparts; ++i) s += part[i];
+  loss[0] = (float)(s / (double)n);
+}
+
 __global__ void k_mlp_infer(const float* __restrict__ W, const float* __restrict__ X, int64_t n, float* __restrict__ Y) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
@@ -212,9 +219,57 @@ uint64_t splitmix(uint64_t& s) {
 }
 }  // namespace
 
+// Work space of lp_mlp_loss_grad_noalloc: a fixed static device array, so that callers who
+// cannot allocate device memory can still evaluate the loss and gradient.  Layout (floats):
+// H1, H2, dZ1, dZ2 [NOALLOC_MAX * 64 each], G3 [NOALLOC_MAX], loss partials, gradient partials.
+namespace {
+constexpr int64_t NOALLOC_MAX = LP_MLP_NOALLOC_MAX_SAMPLES;
+constexpr int64_t NA_H1 = 0;
+constexpr int64_t NA_H2 = NA_H1 + NOALLOC_MAX * lp::MLP_H;
+constexpr int64_t NA_DZ1 = NA_H2 + NOALLOC_MAX * lp::MLP_H;
+constexpr int64_t NA_DZ2 = NA_DZ1 + NOALLOC_MAX * lp::MLP_H;
+constexpr int64_t NA_G3 = NA_DZ2 + NOALLOC_MAX * lp::MLP_H;
+constexpr int64_t NA_LOSS = NA_G3 + NOALLOC_MAX;
+constexpr int64_t NA_PART = NA_LOSS + (NOALLOC_MAX + 255) / 256;
+constexpr int64_t NA_TOTAL = NA_PART + (int64_t)lp::MLP_SPLIT * lp::MLP_NW;
+constexpr int kMaxDevices = 64;
+float* g_noalloc_ptr[kMaxDevices] = {nullptr};
+}  // namespace
+
+static __device__ __align__(256) float g_noalloc_scratch[NA_TOTAL];
+
 extern "C" {
 
 int32_t lp_mlp_weight_count(void) { return lp::MLP_NW; }
+
+lp_status lp_mlp_loss_grad_noalloc(const float* w, const float* x, const float* y, int64_t n, float* loss,
+                                   float* grad, void* stream) {
+  if (!w || !x || !y || !loss || !grad) return mlp_fail(LP_INVALID, "null argument");
+  if (n <= 0 || n > NOALLOC_MAX)
+    return mlp_fail(LP_INVALID, "n=" + std::to_string(n) + " is outside 1.." + std::to_string(NOALLOC_MAX) +
+                                    " (the fixed work space of lp_mlp_loss_grad_noalloc)");
+  int dev = 0;
+  MCK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return mlp_fail(LP_DEVICE, "device index out of range");
+  if (g_noalloc_ptr[dev] == nullptr) {
+    // one-time set-up on this device: the host-side name is not a device address
+    void* ptr = nullptr;
+    MCK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<float*>(ptr);
+  }
+  float* S = g_noalloc_ptr[dev];
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  lp::k_mlp_sample<<<nb, 256, 0, st>>>(w, x, y, n, S + NA_H1, S + NA_H2, S + NA_DZ1, S + NA_DZ2, S + NA_G3,
+                                       S + NA_LOSS);
+  dim3 g((lp::MLP_NW + 255) / 256, lp::MLP_SPLIT);
+  lp::k_mlp_wgrad<<<g, 256, 0, st>>>(x, S + NA_H1, S + NA_H2, S + NA_DZ1, S + NA_DZ2, S + NA_G3, n, S + NA_PART);
+  lp::k_mlp_gsum<<<(lp::MLP_NW + 255) / 256, 256, 0, st>>>(S + NA_PART, grad);
+  lp::k_mlp_loss_final<<<1, 1, 0, st>>>(S + NA_LOSS, (int)nb, n, loss);
+  lp::add_kernel_launches(4);
+  MCK(cudaGetLastError());
+  return LP_OK;
+}
 
 lp_status lp_mlp_init(float* w, int32_t nw, uint64_t seed) {
   if (!w || nw != lp::MLP_NW) return mlp_fail(LP_INVALID, "weight count mismatch");
