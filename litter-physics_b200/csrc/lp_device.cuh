@@ -207,8 +207,11 @@ __device__ inline int hb_return_d(double trial, double ys, double k, double n, d
   double lower = ys, upper = trial;
   double sigma = (sigma0 > lower && sigma0 < upper) ? sigma0 : 0.5 * (lower + upper);
   const double tolerance = tol_rel * fmax(trial, 1.0);
+  // over^(1/n) is evaluated once per iterate as exp(log(over)/n) and reused by the derivative
+  // (over^(1/n - 1) = over^(1/n) / over)
   double over = fmax((sigma - ys) / k, 0.0);
-  double last = sigma - trial + viscous_scale * pow(over, exponent);
+  double pw = over > 0.0 ? exp(exponent * log(over)) : 0.0;
+  double last = sigma - trial + viscous_scale * pw;
   for (int it = 1; it <= 200; ++it) {
     if (fabs(last) <= tolerance || (upper - lower) <= tolerance) {
       *sigma_out = sigma;
@@ -218,17 +221,17 @@ __device__ inline int hb_return_d(double trial, double ys, double k, double n, d
     }
     if (last > 0.0) upper = sigma;
     else lower = sigma;
-    over = fmax((sigma - ys) / k, 0.0);
     double newton;
     if (over > 0.0) {
-      double derivative = 1.0 + viscous_scale * exponent * pow(over, exponent - 1.0) / k;
+      const double derivative = 1.0 + viscous_scale * exponent * (pw / over) / k;
       newton = sigma - last / derivative;
     } else {
       newton = sigma;  // infinite derivative: the reference's Newton step is a no-op here
     }
     sigma = (isfinite(newton) && newton > lower && newton < upper) ? newton : 0.5 * (lower + upper);
     over = fmax((sigma - ys) / k, 0.0);
-    last = sigma - trial + viscous_scale * pow(over, exponent);
+    pw = over > 0.0 ? exp(exponent * log(over)) : 0.0;
+    last = sigma - trial + viscous_scale * pw;
     if (!isfinite(last)) {
       *iters = it;
       return F_CONST_NONFINITE;
@@ -302,9 +305,11 @@ struct PasteOut {
   int yielded;
 };
 
-// warm_w: learned warm-start weights (null: the reference's midpoint start)
-__device__ inline void paste_update(const float Htr[9], float mu, float lambda, double mu_d, double ys, double k,
-                                    double n, double dt, double tol, const float* warm_w, PasteOut& o) {
+// Eigen-decomposition path (any strain size); warm_w: learned warm-start weights (null: the
+// reference's midpoint start).
+static __device__ __noinline__ void paste_update_jacobi(const float Htr[9], float mu, float lambda, double mu_d, double ys,
+                                           double k, double n, double dt, double tol, const float* warm_w,
+                                           PasteOut& o) {
   o.fail = F_OK;
   o.iters = 0;
   o.yielded = 0;
@@ -436,6 +441,167 @@ __device__ inline void paste_update(const float Htr[9], float mu, float lambda, 
       for (int j = 0; j < 3; ++j) {
         float s = M[i][j] + (M[i][0] * Htr[0 * 3 + j] + M[i][1] * Htr[1 * 3 + j] + M[i][2] * Htr[2 * 3 + j]);
         o.H[3 * i + j] = Htr[3 * i + j] + s;
+      }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) o.H[i] = Htr[i];
+  }
+  o.diss_density = o.eq * o.dep;
+}
+
+// ---------------------------------------------------------------- paste update, series path
+// For ||B||_F <= 0.25 the isotropic tensor functions of update_paste need no eigenvectors:
+//   E = log(I + B) / 2                    (Hencky strain tensor, Horner series in B)
+//   tau = 2 mu (mean I + s dev E) + lambda tr(E) I,  s = sigma / sigma_tr
+//   F_new = exp((s - 1) dev E) F_tr  ->  H_new = H_tr + G (I + H_tr),  G = exp((s-1) dev E) - I
+// These are the same functions of the same matrix as U diag(.) U^T in constitutive.rs:456-531;
+// all the polynomials in B commute, so their products stay symmetric (6 stored entries).
+struct Sym {
+  float xx, yy, zz, xy, xz, yz;
+};
+// product of two commuting symmetric matrices
+__device__ __forceinline__ Sym sym_mul(const Sym& p, const Sym& q) {
+  Sym r;
+  r.xx = p.xx * q.xx + p.xy * q.xy + p.xz * q.xz;
+  r.yy = p.xy * q.xy + p.yy * q.yy + p.yz * q.yz;
+  r.zz = p.xz * q.xz + p.yz * q.yz + p.zz * q.zz;
+  r.xy = p.xx * q.xy + p.xy * q.yy + p.xz * q.yz;
+  r.xz = p.xx * q.xz + p.xy * q.yz + p.xz * q.zz;
+  r.yz = p.xy * q.xz + p.yy * q.yz + p.yz * q.zz;
+  return r;
+}
+__device__ __forceinline__ float sym_norm(const Sym& a) {
+  return sqrtf(a.xx * a.xx + a.yy * a.yy + a.zz * a.zz + 2.f * (a.xy * a.xy + a.xz * a.xz + a.yz * a.yz));
+}
+
+__device__ inline void paste_update(const float Htr[9], float mu, float lambda, double mu_d, double ys, double k,
+                                    double n, double dt, double tol, const float* warm_w, PasteOut& o) {
+  Sym B;
+  B.xx = 2.f * Htr[0] + (Htr[0] * Htr[0] + Htr[1] * Htr[1] + Htr[2] * Htr[2]);
+  B.yy = 2.f * Htr[4] + (Htr[3] * Htr[3] + Htr[4] * Htr[4] + Htr[5] * Htr[5]);
+  B.zz = 2.f * Htr[8] + (Htr[6] * Htr[6] + Htr[7] * Htr[7] + Htr[8] * Htr[8]);
+  B.xy = Htr[1] + Htr[3] + (Htr[0] * Htr[3] + Htr[1] * Htr[4] + Htr[2] * Htr[5]);
+  B.xz = Htr[2] + Htr[6] + (Htr[0] * Htr[6] + Htr[1] * Htr[7] + Htr[2] * Htr[8]);
+  B.yz = Htr[5] + Htr[7] + (Htr[3] * Htr[6] + Htr[4] * Htr[7] + Htr[5] * Htr[8]);
+  const float r = sym_norm(B);
+  if (!(r <= 0.25f)) {  // large or non-finite strain: eigen-decomposition path
+    paste_update_jacobi(Htr, mu, lambda, mu_d, ys, k, n, dt, tol, warm_w, o);
+    return;
+  }
+  o.fail = F_OK;
+  o.iters = 0;
+  o.yielded = 0;
+  o.dep = 0.0;
+  o.diss_density = 0.0;
+  const float f00 = 1.f + Htr[0], f01 = Htr[1], f02 = Htr[2];
+  const float f10 = Htr[3], f11 = 1.f + Htr[4], f12 = Htr[5];
+  const float f20 = Htr[6], f21 = Htr[7], f22 = 1.f + Htr[8];
+  const float det = f00 * (f11 * f22 - f21 * f12) - f01 * (f10 * f22 - f20 * f12) + f02 * (f10 * f21 - f20 * f11);
+  if (!(det > 0.f)) {
+    o.fail = isfinite(det) ? F_CONST_INVERTED : F_CONST_NONFINITE;
+    return;
+  }
+  // log(I + B) = B (c1 I + B (c2 I + ... + B cK)), c_j = (-1)^(j+1) / j; K from the truncation
+  // bound r^(K+1) / ((K+1)(1-r)) <= 2e-8 r
+  const int K = r <= 0.01f ? 4 : (r <= 0.05f ? 6 : (r <= 0.1f ? 7 : (r <= 0.18f ? 10 : 12)));
+  Sym P;
+  {
+    const float cK = ((K & 1) ? 1.f : -1.f) / (float)K;
+    P.xx = P.yy = P.zz = cK;
+    P.xy = P.xz = P.yz = 0.f;
+    for (int j = K - 1; j >= 1; --j) {
+      Sym q = sym_mul(B, P);
+      const float cj = ((j & 1) ? 1.f : -1.f) / (float)j;
+      q.xx += cj;
+      q.yy += cj;
+      q.zz += cj;
+      P = q;
+    }
+  }
+  Sym E = sym_mul(B, P);
+  E.xx *= 0.5f;
+  E.yy *= 0.5f;
+  E.zz *= 0.5f;
+  E.xy *= 0.5f;
+  E.xz *= 0.5f;
+  E.yz *= 0.5f;
+  const float vol = E.xx + E.yy + E.zz;
+  const float mean = vol / 3.f;
+  Sym dev = E;
+  dev.xx -= mean;
+  dev.yy -= mean;
+  dev.zz -= mean;
+  const float dnorm = sym_norm(dev);
+  const double trial_eq = 1.2247448713915890 * 2.0 * mu_d * (double)dnorm;  // sqrt(3/2) 2 mu |dev|
+  double scale = 1.0;
+  o.eq = trial_eq;
+  o.trial = trial_eq;
+  if (trial_eq > ys && dnorm > 0.f) {
+    double sigma, dep;
+    int iters;
+    double sigma0 = -1.0;
+    if (warm_w != nullptr) {
+      const double frac = warm_fraction(warm_w, trial_eq, ys, k, n, mu_d, dt);
+      if (frac > 0.0) sigma0 = ys + frac * (trial_eq - ys);
+    }
+    const int e = hb_return_d(trial_eq, ys, k, n, mu_d, dt, tol, sigma0, &sigma, &dep, &iters);
+    o.iters = iters;
+    if (e != F_OK) {
+      o.fail = e;
+      return;
+    }
+    scale = sigma / trial_eq;
+    o.dep = dep;
+    o.eq = sigma;
+    o.yielded = 1;
+  }
+  const float sc = (float)scale;
+  const float lv = lambda * vol;
+  o.tau[0] = 2.f * mu * (dev.xx * sc + mean) + lv;
+  o.tau[1] = 2.f * mu * (dev.yy * sc + mean) + lv;
+  o.tau[2] = 2.f * mu * (dev.zz * sc + mean) + lv;
+  o.tau[3] = 2.f * mu * dev.xy * sc;
+  o.tau[4] = 2.f * mu * dev.xz * sc;
+  o.tau[5] = 2.f * mu * dev.yz * sc;
+  for (int i = 0; i < 6; ++i)
+    if (!isfinite(o.tau[i])) {
+      o.fail = F_CONST_NONFINITE;
+      return;
+    }
+  if (o.yielded) {
+    // G = exp(M) - I, M = (s - 1) dev E, Horner: M (I + M/2 (I + M/3 (I + ...)))
+    Sym M = dev;
+    const float a = sc - 1.f;
+    M.xx *= a;
+    M.yy *= a;
+    M.zz *= a;
+    M.xy *= a;
+    M.xz *= a;
+    M.yz *= a;
+    const float mn = sym_norm(M);
+    const int T = mn <= 0.02f ? 4 : (mn <= 0.1f ? 6 : 9);
+    Sym Q;
+    Q.xx = Q.yy = Q.zz = 1.f;
+    Q.xy = Q.xz = Q.yz = 0.f;
+    for (int j = T; j >= 2; --j) {
+      Sym q = sym_mul(M, Q);
+      const float inv = 1.f / (float)j;
+      Q.xx = 1.f + q.xx * inv;
+      Q.yy = 1.f + q.yy * inv;
+      Q.zz = 1.f + q.zz * inv;
+      Q.xy = q.xy * inv;
+      Q.xz = q.xz * inv;
+      Q.yz = q.yz * inv;
+    }
+    const Sym G = sym_mul(M, Q);
+    const float Gm[9] = {G.xx, G.xy, G.xz, G.xy, G.yy, G.yz, G.xz, G.yz, G.zz};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const float s2 = Gm[3 * i + j] + (Gm[3 * i + 0] * Htr[0 * 3 + j] + Gm[3 * i + 1] * Htr[1 * 3 + j] +
+                                          Gm[3 * i + 2] * Htr[2 * 3 + j]);
+        o.H[3 * i + j] = Htr[3 * i + j] + s2;
       }
   } else {
 #pragma unroll

@@ -537,8 +537,8 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
     D.seg_cnt_g = (D.gcta_cnt + lp::SEG_SPAN - 1) / lp::SEG_SPAN;
     for (int64_t b = 0; b < D.gcta_cnt; b += lp::SEG_SPAN)
       segs.push_back(lp::SegDesc{D.gcta_off + b, D.gcta_off + std::min<int64_t>(b + lp::SEG_SPAN, D.gcta_cnt), i, 0});
-    for (int64_t b = 0; b < D.pcta_cnt; b += lp::SEG_SPAN)
-      segs.push_back(lp::SegDesc{D.pcta_off + b, D.pcta_off + std::min<int64_t>(b + lp::SEG_SPAN, D.pcta_cnt), i, 1});
+    for (int64_t b = 0; b < ntiles; b += lp::SEG_SPAN)
+      segs.push_back(lp::SegDesc{D.tile_off + b, D.tile_off + std::min<int64_t>(b + lp::SEG_SPAN, ntiles), i, 1});
     D.seg_cnt = (int64_t)segs.size() - D.seg_off;
     E.desc[i] = D;
     for (int64_t t = 0; t < ntiles; ++t) tile_inst.push_back(i);
@@ -592,6 +592,7 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   ALLOC(A.vel, A.node_total);
   ALLOC(A.gpart, A.n_gcta);
   ALLOC(A.ppart, A.n_pcta);
+  ALLOC(A.tpart, A.n_tiles);
   A.n_seg = (int64_t)segs.size();
   ALLOC(A.segs, A.n_seg);
   ALLOC(A.seg, A.n_seg);

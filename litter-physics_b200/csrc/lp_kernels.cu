@@ -1119,24 +1119,56 @@ __global__ void k_couple(const InstDesc* __restrict__ desc, Control* __restrict_
 }
 
 // ============================================================== G2P + constitutive
+// One CTA per P2G tile: the tile's (TX+2)(TY+2)(TZ+2) node velocities are staged in shared
+// memory once, then the CTA walks the tile's particles (contiguous in sorted slot order),
+// gathers from shared memory, advects, runs the constitutive update and writes the trial state
+// in sorted slot order.
 __global__ void __launch_bounds__(G2P_THREADS, 2)
-    k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ pcta_inst,
+    k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
-          int64_t cap, const uint32_t* __restrict__ perm, const float4* __restrict__ vel,
-          ParticlePartial* __restrict__ part, const float* __restrict__ mlp, float* __restrict__ log_x,
-          float* __restrict__ log_y, unsigned long long* __restrict__ log_n, long long log_cap) {
+          int64_t cap, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
+          const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const float* __restrict__ mlp,
+          float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
+          long long log_cap) {
+  __shared__ float4 hv[HN];
   __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
-  const int inst = pcta_inst[blockIdx.x];
+  const int tile = blockIdx.x;
+  const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
   if (!c.active) return;
   const InstDesc& D = desc[inst];
-  const int64_t k = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
-  const int64_t valid_n = c.count - c.outflow;
+  const int64_t ltile = tile - D.tile_off;
+  const int64_t key0 = D.key_off + ltile * TB;
+  const uint32_t s0 = start[key0], e0 = start[key0 + TB];
+  if (s0 == e0) {
+    if (threadIdx.x == 0) {
+      ParticlePartial& P = part[blockIdx.x];
+      P.diss = P.bbound = P.mass = 0.0;
+      P.max_speed = P.max_disp = 0.f;
+      P.fail = F_OK;
+      P.iterations = P.yielded = 0;
+      P.fail_value = 0.0;
+    }
+    return;
+  }
+  const int tz = (int)(ltile % D.tiles[2]);
+  const int ty = (int)((ltile / D.tiles[2]) % D.tiles[1]);
+  const int tx = (int)(ltile / ((int64_t)D.tiles[2] * D.tiles[1]));
+  const int ox = tx * TX, oy = ty * TY, oz = tz * TZ;
+  for (int n = threadIdx.x; n < HN; n += G2P_THREADS) {
+    const int hz = n % HZ, hy = (n / HZ) % HY, hx = n / (HZ * HY);
+    const int gi = ox + hx, gj = oy + hy, gk = oz + hz;
+    hv[n] = (gi < D.nodes[0] && gj < D.nodes[1] && gk < D.nodes[2]) ? __ldg(&vel[node_index(D, gi, gj, gk)])
+                                                                    : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
   double diss = 0.0, bb = 0.0, mass_sum = 0.0;
   float max_speed = 0.0f, max_disp = 0.0f;
   int fail = F_OK, iters = 0, yielded = 0;
   double fail_value = 0.0;
-  if (k - D.slot_off < valid_n) {
+  for (uint32_t base0 = s0; base0 < e0; base0 += G2P_THREADS) {
+    const int64_t k = (int64_t)base0 + threadIdx.x;
+    if (k >= (int64_t)e0) continue;
     const int64_t src = perm[k];
     const float* cur = c.parity ? st1 : st0;
     float* nxt = c.parity ? st0 : st1;
@@ -1159,15 +1191,16 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
     float Cm[9];
 #pragma unroll
     for (int a = 0; a < 9; ++a) Cm[a] = 0.0f;
+    const int lbx = base[0] - ox, lby = base[1] - oy, lbz = base[2] - oz;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
-        const int64_t row = node_index(D, base[0] + a, base[1] + b, base[2]);
+        const int row = ((lbx + a) * HY + (lby + b)) * HZ + lbz;
         const float wab = w[0][a] * w[1][b];
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
-          const float4 nv = __ldg(&vel[row + cc]);
+          const float4 nv = hv[row + cc];
           const float ww = wab * w[2][cc];
           const float vx = nv.x * ww, vy = nv.y * ww, vz = nv.z * ww;
           v[0] += vx;
@@ -1210,7 +1243,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
       paste_update(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, D.consistency, D.flow_index, c.dt, D.tol,
                    c.warm_start ? mlp : nullptr, o);
       if (o.fail != F_OK) {
-        fail = o.fail;
+        fail = max(fail, o.fail);
         fail_value = o.eq;
       }
 #pragma unroll
@@ -1218,9 +1251,9 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
 #pragma unroll
       for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
       ep += (float)o.dep;
-      diss = o.diss_density * (double)v0;
-      iters = o.iters;
-      yielded = o.yielded;
+      diss += o.diss_density * (double)v0;
+      iters += o.iters;
+      yielded += o.yielded;
       if (log_n != nullptr && o.yielded && o.fail == F_OK) {
         const unsigned long long slot = atomicAdd(log_n, 1ull);
         if ((long long)slot < log_cap) {
@@ -1238,7 +1271,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
       const float jm1 = cur[C_JM1 * cap + src];
       LiquidOut o;
       liquid_update(jm1, Cm, (float)D.bulk, (float)D.consistency, (float)D.tait_gamma, dt, o);
-      if (o.fail != F_OK) fail = o.fail;
+      if (o.fail != F_OK) fail = max(fail, o.fail);
 #pragma unroll
       for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
       jm1n = o.jm1;
@@ -1271,35 +1304,26 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
     const double tn = sqrt((double)(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]) +
                            2.0 * (double)(tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]));
     const double gn = sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]);
-    bb = mm * (double)speed + (cn * mm + tn * D.max_dt * 4.0 * (double)v0 / (D.dx * D.dx)) * 2.6 * D.dx +
-         6.0 * mm * gn * D.max_dt;
-    mass_sum = mm;
-    max_speed = speed;
-    max_disp = disp;
+    bb += mm * (double)speed + (cn * mm + tn * D.max_dt * 4.0 * (double)v0 / (D.dx * D.dx)) * 2.6 * D.dx +
+          6.0 * mm * gn * D.max_dt;
+    mass_sum += mm;
+    max_speed = fmaxf(max_speed, speed);
+    max_disp = fmaxf(max_disp, disp);
   }
   double rv[9] = {diss, bb, mass_sum, (double)max_speed, (double)max_disp, (double)fail, (double)iters,
                   (double)yielded, fail_value};
   block_reduce_multi<G2P_THREADS, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
-  diss = rv[0];
-  bb = rv[1];
-  mass_sum = rv[2];
-  max_speed = (float)rv[3];
-  max_disp = (float)rv[4];
-  const int fail_all = (int)rv[5];
-  const long long it_all = (long long)rv[6];
-  const long long y_all = (long long)rv[7];
-  fail_value = rv[8];
   if (threadIdx.x == 0) {
     ParticlePartial& P = part[blockIdx.x];
-    P.diss = diss;
-    P.bbound = bb;
-    P.mass = mass_sum;
-    P.max_speed = max_speed;
-    P.max_disp = max_disp;
-    P.fail = fail_all;
-    P.iterations = (int)it_all;
-    P.yielded = (int)y_all;
-    P.fail_value = fail_value;
+    P.diss = rv[0];
+    P.bbound = rv[1];
+    P.mass = rv[2];
+    P.max_speed = (float)rv[3];
+    P.max_disp = (float)rv[4];
+    P.fail = (int)rv[5];
+    P.iterations = (int)rv[6];
+    P.yielded = (int)rv[7];
+    P.fail_value = rv[8];
   }
 }
 
@@ -1705,12 +1729,12 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
     ++n;
     if (ev) cudaEventRecord(ev[n], s);
   }
-  k_g2p<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.id[0], A.id[1],
-                                                    A.cap, A.perm, A.vel, A.ppart, A.mlp, A.log_x, A.log_y, A.log_n,
-                                                    A.log_cap);
+  k_g2p<<<(unsigned)A.n_tiles, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
+                                                     A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, A.mlp, A.log_x,
+                                                     A.log_y, A.log_n, A.log_cap);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_segments<<<(unsigned)A.n_seg, 256, 0, s>>>(A.ctrl, A.segs, A.gpart, A.ppart, A.seg);
+  k_segments<<<(unsigned)A.n_seg, 256, 0, s>>>(A.ctrl, A.segs, A.gpart, A.tpart, A.seg);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_end<<<A.n_inst, 256, 0, s>>>(A.desc, A.ctrl, A.seg);

@@ -42,7 +42,8 @@ struct DeviceArrays {
   int64_t n_blk = 0;
   float4* vel = nullptr;
   GridPartial* gpart = nullptr;
-  ParticlePartial* ppart = nullptr;
+  ParticlePartial* ppart = nullptr;  // per slot-CTA (state statistics)
+  ParticlePartial* tpart = nullptr;  // per tile (G2P)
   SegDesc* segs = nullptr;  // reduction segments
   SegPartial* seg = nullptr;
   int64_t n_seg = 0;

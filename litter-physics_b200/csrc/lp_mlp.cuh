@@ -63,7 +63,7 @@ __device__ inline float mlp_forward(const float* __restrict__ W, const float f[6
 }
 
 // Warm-start fraction in (0, 1) for the Newton start, from the network output.
-__device__ __forceinline__ double warm_fraction(const float* __restrict__ W, double trial, double ys, double k,
+static __device__ __noinline__ double warm_fraction(const float* __restrict__ W, double trial, double ys, double k,
                                                 double n, double mu, double dt) {
   if (W == nullptr || !(trial > ys) || !(k > 0.0)) return -1.0;
   float f[6];

@@ -168,7 +168,9 @@ def test_constitutive_kernels_match_oracle(lib_built):
     rng = np.random.default_rng(5)
     m = oracle.material_paste_shear(1200.0, 56250.0, 0.40625, 50.0, 5.0, 0.5)
     n = 512
+    # small strains (series path) and large stretches (||F F^T - I|| > 0.25: eigen path)
     f = np.eye(3)[None] + rng.normal(scale=3e-3, size=(n, 3, 3))
+    f[n // 2:] = np.diag([0.8, 1.15, 0.95])[None] + rng.normal(scale=2e-2, size=(n - n // 2, 3, 3))
     f = np.ascontiguousarray(f)
     dt = 1e-4
     fn, tau = np.zeros((n, 9)), np.zeros((n, 9))
@@ -186,7 +188,7 @@ def test_constitutive_kernels_match_oracle(lib_built):
         assert rs == 0
         scale = np.abs(rtau).max()
         assert np.abs(tau[i].reshape(3, 3) - rtau).max() <= 1e-4 * scale + 1e-3
-        assert np.abs(fn[i].reshape(3, 3) - rfn).max() <= 2e-6
+        assert np.abs(fn[i].reshape(3, 3) - rfn).max() <= 2e-6 * max(1.0, np.abs(rfn).max())
         if rdep > 0:
             yielded += 1
             assert abs(eq[i] - req) <= 1e-4 * req
