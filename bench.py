@@ -276,8 +276,9 @@ def ours(args, ws, rank, local):
             ms = float(t.item())
         results[arm] = {"ms": ms, "accepted": accepted, "newton_iterations": int(it1 - it0),
                         "value": ws * n * accepted / (ms / 1e3)}
-    # per-kernel live timing (CUDA events on the same stream), last arm
-    ktimes = sim.kernel_times(args.kernel_steps)
+        # per-kernel live timing (CUDA events on the same stream) of this arm
+        results[arm]["kernel_ms"] = sim.kernel_times(args.kernel_steps)
+    ktimes = results[arms[-1]]["kernel_ms"]
     if args.no_e2e:
         e2e_steps = 0
     else:
@@ -341,7 +342,8 @@ def ours(args, ws, rank, local):
             "precision": "f32 particle/grid arithmetic, f64 HB Newton and ledgers, int64 fixed-point grid sums",
         },
         "plain": {"value": plain["value"], "ms_per_step": plain["ms"] / args.steps,
-                  "newton_iterations_per_step": plain["newton_iterations"] / max(plain["accepted"], 1)},
+                  "newton_iterations_per_step": plain["newton_iterations"] / max(plain["accepted"], 1),
+                  "kernel_ms": {k: round(v, 5) for k, v in plain["kernel_ms"].items()}},
         "warm": {"newton_iterations_per_step": warm["newton_iterations"] / max(warm["accepted"], 1),
                  "mlp": train_info},
         "warm_over_plain": warm["value"] / plain["value"],

@@ -274,7 +274,12 @@ lp_status lp_mlp_init(float* weights, int32_t nweights, uint64_t seed);
 /* Features x[6*n] (see lp_hb_features), targets y[n]; runs `epochs` passes of minibatch Adam. */
 lp_status lp_mlp_train(float* weights, int32_t nweights, const float* x, const float* y, int64_t n,
                        int32_t epochs, int32_t batch, float lr, float* final_loss);
+/* FP32 forward pass (the training kernels' arithmetic). */
 lp_status lp_mlp_forward(const float* weights, int32_t nweights, const float* x, int64_t n, float* y);
+/* Forward pass the solver uses for the warm start: one warp per 32 rows on the tensor cores
+ * (mma.sync m16n8k16, BF16 weights and activations, inputs as BF16 hi + lo pairs, FP32
+ * accumulation, hardware tanh in SiLU). */
+lp_status lp_mlp_forward_mma(const float* weights, int32_t nweights, const float* x, int64_t n, float* y);
 /* Loss and gradient of mean squared error over n samples (FP32), for gradient checks. */
 lp_status lp_mlp_loss_grad(const float* weights, int32_t nweights, const float* x, const float* y,
                            int64_t n, float* loss, float* grad);

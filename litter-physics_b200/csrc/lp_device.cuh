@@ -305,11 +305,11 @@ struct PasteOut {
   int yielded;
 };
 
-// Eigen-decomposition path (any strain size); warm_w: learned warm-start weights (null: the
-// reference's midpoint start).
+// Eigen-decomposition path (any strain size).  sigma0: Newton start in (yield, trial), or -1 for
+// the reference's midpoint start.  trial_only: stop after the trial equivalent stress (o.trial).
 static __device__ __noinline__ void paste_update_jacobi(const float Htr[9], float mu, float lambda, double mu_d, double ys,
-                                           double k, double n, double dt, double tol, const float* warm_w,
-                                           PasteOut& o) {
+                                           double k, double n, double dt, double tol, double sigma0,
+                                           bool trial_only, PasteOut& o) {
   o.fail = F_OK;
   o.iters = 0;
   o.yielded = 0;
@@ -382,14 +382,10 @@ static __device__ __noinline__ void paste_update_jacobi(const float Htr[9], floa
   double scale = 1.0;
   o.eq = trial_eq;
   o.trial = trial_eq;
+  if (trial_only) return;
   if (trial_eq > ys && dnorm > 0.f) {
     double sigma, dep;
     int iters;
-    double sigma0 = -1.0;
-    if (warm_w != nullptr) {
-      const double frac = warm_fraction(warm_w, trial_eq, ys, k, n, mu_d, dt);
-      if (frac > 0.0) sigma0 = ys + frac * (trial_eq - ys);
-    }
     int e = hb_return_d(trial_eq, ys, k, n, mu_d, dt, tol, sigma0, &sigma, &dep, &iters);
     o.iters = iters;
     if (e != F_OK) {
@@ -474,8 +470,23 @@ __device__ __forceinline__ float sym_norm(const Sym& a) {
   return sqrtf(a.xx * a.xx + a.yy * a.yy + a.zz * a.zz + 2.f * (a.xy * a.xy + a.xz * a.xz + a.yz * a.yz));
 }
 
-__device__ inline void paste_update(const float Htr[9], float mu, float lambda, double mu_d, double ys, double k,
-                                    double n, double dt, double tol, const float* warm_w, PasteOut& o) {
+// Trial part of the paste update: the Hencky strain of H_tr and its equivalent stress.  The
+// Newton start (the learned warm start) is chosen from t.trial_eq between paste_trial and
+// paste_finish, which lets a warp evaluate the network for all its lanes at one call site.
+enum { PT_SERIES = 0, PT_JACOBI = 1, PT_DONE = 2 };
+struct PasteTrial {
+  Sym dev;
+  float mean, vol, dnorm;
+  double trial_eq;
+  int path;
+};
+
+__device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& t, PasteOut& o) {
+  o.fail = F_OK;
+  o.iters = 0;
+  o.yielded = 0;
+  o.dep = 0.0;
+  o.diss_density = 0.0;
   Sym B;
   B.xx = 2.f * Htr[0] + (Htr[0] * Htr[0] + Htr[1] * Htr[1] + Htr[2] * Htr[2]);
   B.yy = 2.f * Htr[4] + (Htr[3] * Htr[3] + Htr[4] * Htr[4] + Htr[5] * Htr[5]);
@@ -485,20 +496,19 @@ __device__ inline void paste_update(const float Htr[9], float mu, float lambda, 
   B.yz = Htr[5] + Htr[7] + (Htr[3] * Htr[6] + Htr[4] * Htr[7] + Htr[5] * Htr[8]);
   const float r = sym_norm(B);
   if (!(r <= 0.25f)) {  // large or non-finite strain: eigen-decomposition path
-    paste_update_jacobi(Htr, mu, lambda, mu_d, ys, k, n, dt, tol, warm_w, o);
+    paste_update_jacobi(Htr, 0.f, 0.f, mu_d, 0.0, 0.0, 0.0, 0.0, 0.0, -1.0, true, o);
+    t.path = o.fail == F_OK ? PT_JACOBI : PT_DONE;
+    t.trial_eq = o.trial;
     return;
   }
-  o.fail = F_OK;
-  o.iters = 0;
-  o.yielded = 0;
-  o.dep = 0.0;
-  o.diss_density = 0.0;
   const float f00 = 1.f + Htr[0], f01 = Htr[1], f02 = Htr[2];
   const float f10 = Htr[3], f11 = 1.f + Htr[4], f12 = Htr[5];
   const float f20 = Htr[6], f21 = Htr[7], f22 = 1.f + Htr[8];
   const float det = f00 * (f11 * f22 - f21 * f12) - f01 * (f10 * f22 - f20 * f12) + f02 * (f10 * f21 - f20 * f11);
   if (!(det > 0.f)) {
     o.fail = isfinite(det) ? F_CONST_INVERTED : F_CONST_NONFINITE;
+    t.path = PT_DONE;
+    t.trial_eq = 0.0;
     return;
   }
   // log(I + B) = B (c1 I + B (c2 I + ... + B cK)), c_j = (-1)^(j+1) / j; K from the truncation
@@ -527,23 +537,37 @@ __device__ inline void paste_update(const float Htr[9], float mu, float lambda, 
   E.yz *= 0.5f;
   const float vol = E.xx + E.yy + E.zz;
   const float mean = vol / 3.f;
-  Sym dev = E;
+  t.vol = vol;
+  t.mean = mean;
+  Sym& dev = t.dev;
+  dev = E;
   dev.xx -= mean;
   dev.yy -= mean;
   dev.zz -= mean;
-  const float dnorm = sym_norm(dev);
-  const double trial_eq = 1.2247448713915890 * 2.0 * mu_d * (double)dnorm;  // sqrt(3/2) 2 mu |dev|
-  double scale = 1.0;
+  t.dnorm = sym_norm(dev);
+  t.trial_eq = 1.2247448713915890 * 2.0 * mu_d * (double)t.dnorm;  // sqrt(3/2) 2 mu |dev|
+  t.path = PT_SERIES;
+}
+
+// Rest of the paste update after paste_trial: the Herschel-Bulkley return started at sigma0
+// (in (yield, trial), or -1 for the midpoint), the stress and the plastic correction of H.
+__device__ inline void paste_finish(const float Htr[9], float mu, float lambda, double mu_d, double ys, double k,
+                                    double n, double dt, double tol, double sigma0, const PasteTrial& t,
+                                    PasteOut& o) {
+  if (t.path == PT_DONE) return;
+  if (t.path == PT_JACOBI) {
+    paste_update_jacobi(Htr, mu, lambda, mu_d, ys, k, n, dt, tol, sigma0, false, o);
+    return;
+  }
+  const Sym& dev = t.dev;
+  const float vol = t.vol, mean = t.mean;
+  const double trial_eq = t.trial_eq;
   o.eq = trial_eq;
   o.trial = trial_eq;
-  if (trial_eq > ys && dnorm > 0.f) {
+  double scale = 1.0;
+  if (trial_eq > ys && t.dnorm > 0.f) {
     double sigma, dep;
     int iters;
-    double sigma0 = -1.0;
-    if (warm_w != nullptr) {
-      const double frac = warm_fraction(warm_w, trial_eq, ys, k, n, mu_d, dt);
-      if (frac > 0.0) sigma0 = ys + frac * (trial_eq - ys);
-    }
     const int e = hb_return_d(trial_eq, ys, k, n, mu_d, dt, tol, sigma0, &sigma, &dep, &iters);
     o.iters = iters;
     if (e != F_OK) {
@@ -608,6 +632,14 @@ __device__ inline void paste_update(const float Htr[9], float mu, float lambda, 
     for (int i = 0; i < 9; ++i) o.H[i] = Htr[i];
   }
   o.diss_density = o.eq * o.dep;
+}
+
+// whole paste update (constitutive.rs:456-531) with the reference's midpoint Newton start
+__device__ inline void paste_update(const float Htr[9], float mu, float lambda, double mu_d, double ys, double k,
+                                    double n, double dt, double tol, PasteOut& o) {
+  PasteTrial t;
+  paste_trial(Htr, mu_d, t, o);
+  paste_finish(Htr, mu, lambda, mu_d, ys, k, n, dt, tol, -1.0, t, o);
 }
 
 // ---------------------------------------------------------------- liquid update (J - 1)

@@ -271,6 +271,7 @@ struct Ensemble {
   std::vector<Control> ctrl_h;
   double* d_diag = nullptr;
   float* d_mlp = nullptr;
+  lp::MlpPacked* d_mlp_pk = nullptr;
   int warm = 0;
 
   ~Ensemble() { release(); }
@@ -1220,13 +1221,20 @@ static lp_status set_warm(Ensemble& E, const float* w, int32_t nw, int32_t enabl
       lp_status st = E.alloc(&E.d_mlp, lp::MLP_NW);
       if (st != LP_OK) return st;
     }
+    if (!E.d_mlp_pk) {
+      lp_status st = E.alloc(&E.d_mlp_pk, 1);
+      if (st != LP_OK) return st;
+    }
     CUDA_CK(cudaMemcpyAsync(E.d_mlp, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice, E.stream));
-    E.A.mlp = E.d_mlp;
+    lp::launch_mlp_pack(E.d_mlp, E.d_mlp_pk, E.stream);
+    CUDA_CK(cudaGetLastError());
+    E.A.mlp = E.d_mlp_pk;
   }
   E.invalidate_graph();
   lp_status st = pull_ctrl(E);
   if (st != LP_OK) return st;
   for (auto& c : E.ctrl_h) c.warm_start = enable ? 1 : 0;
+  E.A.warm = enable ? 1 : 0;
   return push_ctrl(E);
 }
 lp_status lp_sim_set_warm_start(lp_sim* sim, const float* w, int32_t nw, int32_t enable) {
@@ -1493,17 +1501,20 @@ lp_status lp_hb_return_batch(int64_t n, const double* trial, const double* yield
   if (mlp_weights && nweights != lp::MLP_NW) return set_error(LP_INVALID, "MLP weight count mismatch");
   double* d = nullptr;
   float* w = nullptr;
+  lp::MlpPacked* pk = nullptr;
   int* s = nullptr;
   const size_t nb = sizeof(double) * (size_t)n;
   CUDA_CK(cudaMalloc(&d, nb * 9));
   CUDA_CK(cudaMalloc(&s, sizeof(int) * n));
   if (mlp_weights) {
     CUDA_CK(cudaMalloc(&w, sizeof(float) * lp::MLP_NW));
+    CUDA_CK(cudaMalloc(&pk, sizeof(lp::MlpPacked)));
     CUDA_CK(cudaMemcpy(w, mlp_weights, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
+    lp::launch_mlp_pack(w, pk, 0);
   }
   const double* src[6] = {trial, yield, consistency, flow_index, mu, dt};
   for (int k = 0; k < 6; ++k) CUDA_CK(cudaMemcpy(d + k * n, src[k], nb, cudaMemcpyHostToDevice));
-  lp::launch_hb_return_batch(n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, tol_rel > 0 ? tol_rel : 1e-12, w,
+  lp::launch_hb_return_batch(n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, tol_rel > 0 ? tol_rel : 1e-12, pk,
                              d + 6 * n, s, 0);
   CUDA_CK(cudaGetLastError());
   CUDA_CK(cudaMemcpy(out, d + 6 * n, nb * 3, cudaMemcpyDeviceToHost));
@@ -1511,6 +1522,7 @@ lp_status lp_hb_return_batch(int64_t n, const double* trial, const double* yield
   cudaFree(d);
   cudaFree(s);
   if (w) cudaFree(w);
+  if (pk) cudaFree(pk);
   return LP_OK;
 }
 

@@ -1123,15 +1123,33 @@ __global__ void k_couple(const InstDesc* __restrict__ desc, Control* __restrict_
 // memory once, then the CTA walks the tile's particles (contiguous in sorted slot order),
 // gathers from shared memory, advects, runs the constitutive update and writes the trial state
 // in sorted slot order.
+struct G2pMlpShared {
+  MlpPacked w;
+  uint32_t xs[(G2P_THREADS / 32) * MLP_XS_WORDS];
+};
+template <bool WARM>
+struct G2pWarmShared {
+  struct type {
+    int unused;
+  };
+};
+template <>
+struct G2pWarmShared<true> {
+  using type = G2pMlpShared;
+};
+
+template <bool WARM>
 __global__ void __launch_bounds__(G2P_THREADS, 2)
     k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
           int64_t cap, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
-          const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const float* __restrict__ mlp,
+          const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const MlpPacked* __restrict__ mlp,
           float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
           long long log_cap) {
   __shared__ float4 hv[HN];
   __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
+  // network weights and per-warp feature rows (the WARM instantiation only)
+  __shared__ typename G2pWarmShared<WARM>::type wsh;
   const int tile = blockIdx.x;
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
@@ -1161,14 +1179,21 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
     hv[n] = (gi < D.nodes[0] && gj < D.nodes[1] && gk < D.nodes[2]) ? __ldg(&vel[node_index(D, gi, gj, gk)])
                                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
   }
+  const bool use_mlp = WARM && D.kind == 0 && c.warm_start && mlp != nullptr;  // CTA-uniform
+  if constexpr (WARM) {
+    if (use_mlp) mlp_stage(mlp, wsh.w);
+  }
   __syncthreads();
   double diss = 0.0, bb = 0.0, mass_sum = 0.0;
   float max_speed = 0.0f, max_disp = 0.0f;
   int fail = F_OK, iters = 0, yielded = 0;
   double fail_value = 0.0;
   for (uint32_t base0 = s0; base0 < e0; base0 += G2P_THREADS) {
-    const int64_t k = (int64_t)base0 + threadIdx.x;
-    if (k >= (int64_t)e0) continue;
+    // warp-uniform exit; lanes past the end of a partly filled warp redo the tile's last
+    // particle and store nothing, so the warp reaches the network call converged
+    if (base0 + (threadIdx.x & ~31u) >= e0) break;
+    const bool valid = base0 + threadIdx.x < e0;
+    const int64_t k = valid ? (int64_t)base0 + threadIdx.x : (int64_t)e0 - 1;
     const int64_t src = perm[k];
     const float* cur = c.parity ? st1 : st0;
     float* nxt = c.parity ? st0 : st1;
@@ -1222,9 +1247,23 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
     const float disp = speed * dt / dx;
     const float m = cur[C_M * cap + src];
     const float v0 = cur[C_V0 * cap + src];
+    // kinematic part of the trial state, stored before the constitutive update (sorted slot order)
+    if (valid) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        nxt[(C_X + a) * cap + k] = x[a] + v[a] * dt;
+        nxt[(C_V + a) * cap + k] = v[a];
+      }
+#pragma unroll
+      for (int a = 0; a < 9; ++a) nxt[(C_C + a) * cap + k] = Cm[a];
+      nxt[C_M * cap + k] = m;
+      nxt[C_V0 * cap + k] = v0;
+      if (D.per_particle_yield) nxt[C_YS * cap + k] = cur[C_YS * cap + src];
+      idn[k] = idc[src];
+    }
+    const double cn = sqrt((double)(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] +
+                                    Cm[5] * Cm[5] + Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]));
     float tau[6];
-    float Hn[9];
-    float jm1n = 0.0f;
     float ep = cur[C_EP * cap + src];
     if (D.kind == 0) {
       float H[9], Htr[9];
@@ -1240,67 +1279,69 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
         }
       const double ys = D.per_particle_yield ? (double)cur[C_YS * cap + src] : D.yield;
       PasteOut o;
-      paste_update(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, D.consistency, D.flow_index, c.dt, D.tol,
-                   c.warm_start ? mlp : nullptr, o);
-      if (o.fail != F_OK) {
-        fail = max(fail, o.fail);
-        fail_value = o.eq;
+      PasteTrial pt;
+      paste_trial(Htr, D.mu, pt, o);
+      double sigma0 = -1.0;
+      if constexpr (WARM) {
+        if (use_mlp) {
+          // learned warm start: one tensor-core network pass per warp that has a yielding lane
+          const bool need =
+              valid && pt.path != PT_DONE && pt.trial_eq > ys && pt.trial_eq > 0.0 && D.consistency > 0.0;
+          if (__any_sync(0xffffffffu, need)) {
+            float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (need) hb_features(pt.trial_eq, ys, D.consistency, D.flow_index, D.mu, c.dt, f);
+            const float y = warp_mlp_logit(wsh.w, wsh.xs + (threadIdx.x >> 5) * MLP_XS_WORDS, f);
+            const double frac = warm_fraction_of(y);
+            if (need && frac > 0.0) sigma0 = ys + frac * (pt.trial_eq - ys);
+          }
+        }
       }
-#pragma unroll
-      for (int a = 0; a < 9; ++a) Hn[a] = o.H[a];
+      paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, D.consistency, D.flow_index, c.dt, D.tol, sigma0, pt,
+                   o);
 #pragma unroll
       for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
-      ep += (float)o.dep;
-      diss += o.diss_density * (double)v0;
-      iters += o.iters;
-      yielded += o.yielded;
-      if (log_n != nullptr && o.yielded && o.fail == F_OK) {
-        const unsigned long long slot = atomicAdd(log_n, 1ull);
-        if ((long long)slot < log_cap) {
-          // (trial stress, yield, consistency, flow index, mu, dt) -> returned stress
-          log_x[6 * slot + 0] = (float)o.trial;
-          log_x[6 * slot + 1] = (float)ys;
-          log_x[6 * slot + 2] = (float)D.consistency;
-          log_x[6 * slot + 3] = (float)D.flow_index;
-          log_x[6 * slot + 4] = (float)D.mu;
-          log_x[6 * slot + 5] = (float)c.dt;
-          log_y[slot] = (float)o.eq;
+      if (valid) {
+        if (o.fail != F_OK) {
+          fail = max(fail, o.fail);
+          fail_value = o.eq;
+        }
+#pragma unroll
+        for (int a = 0; a < 9; ++a) nxt[(C_H + a) * cap + k] = o.H[a];
+        ep += (float)o.dep;
+        diss += o.diss_density * (double)v0;
+        iters += o.iters;
+        yielded += o.yielded;
+        if (log_n != nullptr && o.yielded && o.fail == F_OK) {
+          const unsigned long long slot = atomicAdd(log_n, 1ull);
+          if ((long long)slot < log_cap) {
+            // (trial stress, yield, consistency, flow index, mu, dt) -> returned stress
+            log_x[6 * slot + 0] = (float)o.trial;
+            log_x[6 * slot + 1] = (float)ys;
+            log_x[6 * slot + 2] = (float)D.consistency;
+            log_x[6 * slot + 3] = (float)D.flow_index;
+            log_x[6 * slot + 4] = (float)D.mu;
+            log_x[6 * slot + 5] = (float)c.dt;
+            log_y[slot] = (float)o.eq;
+          }
         }
       }
     } else {
       const float jm1 = cur[C_JM1 * cap + src];
       LiquidOut o;
       liquid_update(jm1, Cm, (float)D.bulk, (float)D.consistency, (float)D.tait_gamma, dt, o);
-      if (o.fail != F_OK) fail = max(fail, o.fail);
 #pragma unroll
       for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
-      jm1n = o.jm1;
+      if (valid) {
+        if (o.fail != F_OK) fail = max(fail, o.fail);
+        nxt[C_JM1 * cap + k] = o.jm1;
+      }
     }
-    // write the trial state in sorted slot order
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      nxt[(C_X + a) * cap + k] = x[a] + v[a] * dt;
-      nxt[(C_V + a) * cap + k] = v[a];
-    }
-#pragma unroll
-    for (int a = 0; a < 9; ++a) nxt[(C_C + a) * cap + k] = Cm[a];
-    if (D.kind == 0) {
-#pragma unroll
-      for (int a = 0; a < 9; ++a) nxt[(C_H + a) * cap + k] = Hn[a];
-    } else {
-      nxt[C_JM1 * cap + k] = jm1n;
-    }
+    if (!valid) continue;
 #pragma unroll
     for (int a = 0; a < 6; ++a) nxt[(C_TAU + a) * cap + k] = tau[a];
     nxt[C_EP * cap + k] = ep;
-    nxt[C_M * cap + k] = m;
-    nxt[C_V0 * cap + k] = v0;
-    if (D.per_particle_yield) nxt[C_YS * cap + k] = cur[C_YS * cap + src];
-    idn[k] = idc[src];
     // momentum bound of the new state for the next attempt's fixed-point scale
     const double mm = m;
-    const double cn = sqrt((double)(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] +
-                                    Cm[5] * Cm[5] + Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]));
     const double tn = sqrt((double)(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]) +
                            2.0 * (double)(tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]));
     const double gn = sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]);
@@ -1623,16 +1664,31 @@ __global__ void k_diagnostics(const InstDesc* __restrict__ desc, const Control* 
 
 
 // ============================================================== unit kernels (host arrays API)
-__global__ void k_hb_batch(int64_t n, const double* trial, const double* ys, const double* k, const double* nn,
-                           const double* mu, const double* dt, double tol, const float* mlp, double* out,
-                           int* status) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// One return problem per lane; with weights, each warp starts its lanes' Newton solves from one
+// tensor-core network pass (the same call as in k_g2p).
+__global__ void __launch_bounds__(128) k_hb_batch(int64_t n, const double* trial, const double* ys, const double* k,
+                                                  const double* nn, const double* mu, const double* dt, double tol,
+                                                  const MlpPacked* mlp, double* out, int* status) {
+  __shared__ MlpPacked mlp_s;
+  __shared__ uint32_t mlp_xs[4 * MLP_XS_WORDS];
+  if (mlp != nullptr) mlp_stage(mlp, mlp_s);
+  __syncthreads();
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u) >= n) return;  // warp-uniform
+  const bool valid = i0 < n;
+  const int64_t i = valid ? i0 : n - 1;
   double sigma0 = -1.0;
   if (mlp != nullptr) {
-    const double frac = warm_fraction(mlp, trial[i], ys[i], k[i], nn[i], mu[i], dt[i]);
-    if (frac > 0.0) sigma0 = ys[i] + frac * (trial[i] - ys[i]);
+    const bool need = valid && trial[i] > ys[i] && k[i] > 0.0;
+    if (__any_sync(0xffffffffu, need)) {
+      float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (need) hb_features(trial[i], ys[i], k[i], nn[i], mu[i], dt[i], f);
+      const float y = warp_mlp_logit(mlp_s, mlp_xs + (threadIdx.x >> 5) * MLP_XS_WORDS, f);
+      const double frac = warm_fraction_of(y);
+      if (need && frac > 0.0) sigma0 = ys[i] + frac * (trial[i] - ys[i]);
+    }
   }
+  if (!valid) return;
   double sigma = 0.0, dep = 0.0;
   int it = 0;
   status[i] = hb_return_d(trial[i], ys[i], k[i], nn[i], mu[i], dt[i], tol, sigma0, &sigma, &dep, &it);
@@ -1647,7 +1703,7 @@ __global__ void k_paste_batch(int64_t n, const double* f, double mu, double lamb
   float Htr[9];
   for (int a = 0; a < 9; ++a) Htr[a] = (float)(f[9 * i + a] - ((a % 4) == 0 ? 1.0 : 0.0));
   PasteOut o;
-  paste_update(Htr, (float)mu, (float)lambda, mu, ys, k, nn, dt, tol, nullptr, o);
+  paste_update(Htr, (float)mu, (float)lambda, mu, ys, k, nn, dt, tol, o);
   status[i] = o.fail;
   if (o.fail != F_OK) return;
   for (int a = 0; a < 9; ++a) fnew[9 * i + a] = (double)o.H[a] + ((a % 4) == 0 ? 1.0 : 0.0);
@@ -1729,7 +1785,7 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
     ++n;
     if (ev) cudaEventRecord(ev[n], s);
   }
-  k_g2p<<<(unsigned)A.n_tiles, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
+  (A.mlp != nullptr && A.warm ? k_g2p<true> : k_g2p<false>)<<<(unsigned)A.n_tiles, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
                                                      A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, A.mlp, A.log_x,
                                                      A.log_y, A.log_n, A.log_cap);
   ++n;
@@ -1813,8 +1869,8 @@ int launch_diagnostics(const DeviceArrays& A, int hydro, double h0, int dam, dou
 }
 
 int launch_hb_return_batch(int64_t n, const double* trial, const double* ys, const double* k, const double* nn,
-                           const double* mu, const double* dt, double tol, const float* mlp, double* out, int* status,
-                           cudaStream_t s) {
+                           const double* mu, const double* dt, double tol, const MlpPacked* mlp, double* out,
+                           int* status, cudaStream_t s) {
   k_hb_batch<<<grid_of(n, 128), 128, 0, s>>>(n, trial, ys, k, nn, mu, dt, tol, mlp, out, status);
   g_launches += 1;
   return 1;

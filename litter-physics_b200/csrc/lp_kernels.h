@@ -47,7 +47,8 @@ struct DeviceArrays {
   SegDesc* segs = nullptr;  // reduction segments
   SegPartial* seg = nullptr;
   int64_t n_seg = 0;
-  float* mlp = nullptr;  // warm-start weights (device) or null
+  const MlpPacked* mlp = nullptr;  // packed warm-start weights (device) or null
+  int warm = 0;                     // some instance has the warm start on: launch the WARM G2P
   float* log_x = nullptr;
   float* log_y = nullptr;
   unsigned long long* log_n = nullptr;
@@ -70,9 +71,12 @@ void configure_kernels();              // one-time function attributes (dynamic 
 void set_last_error(const char* msg);  // message returned by lp_last_error()
 void add_kernel_launches(uint64_t n);
 
+// FP32 warm-start weights -> packed BF16 layout of the tensor-core inference
+void launch_mlp_pack(const float* W, MlpPacked* P, cudaStream_t s);
+
 // constitutive unit kernels on device arrays
 int launch_hb_return_batch(int64_t n, const double* trial, const double* ys, const double* k, const double* nn,
-                           const double* mu, const double* dt, double tol, const float* mlp, double* out, int* status,
+                           const double* mu, const double* dt, double tol, const MlpPacked* mlp, double* out, int* status,
                            cudaStream_t s);
 int launch_update_paste_batch(int64_t n, const double* f, double mu, double lambda, double ys, double k, double nn,
                               double dt, double tol, double* fnew, double* tau, double* scal, int* status,

@@ -148,6 +148,32 @@ __global__ void k_mlp_infer(const float* __restrict__ W, const float* __restrict
   Y[s] = mlp_forward(W, f);
 }
 
+__global__ void k_mlp_pack(const float* __restrict__ W, MlpPacked* __restrict__ P) {
+  mlp_pack_words(W, *P, (int)(blockIdx.x * blockDim.x + threadIdx.x), (int)(gridDim.x * blockDim.x));
+}
+
+void launch_mlp_pack(const float* W, MlpPacked* P, cudaStream_t s) {
+  k_mlp_pack<<<8, 256, 0, s>>>(W, P);
+  add_kernel_launches(1);
+}
+
+// tensor-core inference of the network (the path the solver uses), on feature rows
+__global__ void __launch_bounds__(128) k_mlp_infer_mma(const MlpPacked* __restrict__ P, const float* __restrict__ X,
+                                                       int64_t n, float* __restrict__ Y) {
+  __shared__ MlpPacked S;
+  __shared__ uint32_t xs[4 * MLP_XS_WORDS];
+  mlp_stage(P, S);
+  __syncthreads();
+  if ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u) >= n) return;  // warp-uniform
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = i0 < n ? i0 : n - 1;
+  float f[MLP_IN];
+#pragma unroll
+  for (int j = 0; j < MLP_IN; ++j) f[j] = X[i * MLP_IN + j];
+  const float y = warp_mlp_logit(S, xs + (threadIdx.x >> 5) * MLP_XS_WORDS, f);
+  if (i0 < n) Y[i0] = y;
+}
+
 }  // namespace lp
 
 namespace {
@@ -369,6 +395,30 @@ lp_status lp_mlp_forward(const float* w, int32_t nw, const float* x, int64_t n, 
   MCK(cudaGetLastError());
   MCK(cudaMemcpy(y, Y, sizeof(float) * n, cudaMemcpyDeviceToHost));
   cudaFree(W);
+  cudaFree(X);
+  cudaFree(Y);
+  return LP_OK;
+}
+
+lp_status lp_mlp_forward_mma(const float* w, int32_t nw, const float* x, int64_t n, float* y) {
+  if (!w || nw != lp::MLP_NW || n <= 0) return mlp_fail(LP_INVALID, "bad arguments");
+  int dc = 0;
+  if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return mlp_fail(LP_DEVICE, "no CUDA device");
+  float *W = nullptr, *X = nullptr, *Y = nullptr;
+  lp::MlpPacked* P = nullptr;
+  MCK(cudaMalloc(&W, sizeof(float) * lp::MLP_NW));
+  MCK(cudaMalloc(&P, sizeof(lp::MlpPacked)));
+  MCK(cudaMalloc(&X, sizeof(float) * n * lp::MLP_IN));
+  MCK(cudaMalloc(&Y, sizeof(float) * n));
+  MCK(cudaMemcpy(W, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(X, x, sizeof(float) * n * lp::MLP_IN, cudaMemcpyHostToDevice));
+  lp::launch_mlp_pack(W, P, 0);
+  lp::k_mlp_infer_mma<<<(unsigned)((n + 127) / 128), 128>>>(P, X, n, Y);
+  lp::add_kernel_launches(1);
+  MCK(cudaGetLastError());
+  MCK(cudaMemcpy(y, Y, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  cudaFree(W);
+  cudaFree(P);
   cudaFree(X);
   cudaFree(Y);
   return LP_OK;

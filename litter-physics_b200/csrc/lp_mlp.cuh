@@ -13,7 +13,9 @@
 // Network: 6 -> 64 -> 64 -> 1, SiLU, FP32 weights, flat layout below.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cstdint>
 
 namespace lp {
 
@@ -62,15 +64,149 @@ __device__ inline float mlp_forward(const float* __restrict__ W, const float f[6
   return out;
 }
 
-// Warm-start fraction in (0, 1) for the Newton start, from the network output.
-static __device__ __noinline__ double warm_fraction(const float* __restrict__ W, double trial, double ys, double k,
-                                                double n, double mu, double dt) {
-  if (W == nullptr || !(trial > ys) || !(k > 0.0)) return -1.0;
-  float f[6];
-  hb_features(trial, ys, k, n, mu, dt, f);
-  const float y = mlp_forward(W, f);
-  const double t = 1.0 / (1.0 + exp(-(double)y));
-  return (t > 0.0 && t < 1.0) ? t : -1.0;
+// ---------------------------------------------------------------- warp-cooperative inference
+// One warp evaluates the network for its 32 lanes at once on the tensor cores with
+// mma.sync.m16n8k16 (BF16 operands, FP32 accumulation); rows are lanes:
+//   layer 1: [32 x 16] x [16 x 64].  Each FP32 feature enters as a BF16 pair hi + lo (columns
+//            k and k + 6, both multiplying the same W1 column), so the inputs keep ~16 bits;
+//   layer 2: [32 x 64] x [64 x 64], A fragments are the layer-1 accumulators after bias + SiLU,
+//            re-packed to BF16 in registers (the C layout of one n-tile pair is the A layout of
+//            one k-step);
+//   layer 3: 64-wide FP32 dot product, reduced across each lane quad.
+// SiLU uses the hardware tanh: silu(z) = z/2 (1 + tanh(z/2)).
+// Packed weights (MlpPacked, built once per weight upload by k_mlp_pack) are BF16 pairs with
+// padded row strides of 12 and 36 words, so that fragment loads are free of bank conflicts.
+constexpr int MLP_S1 = 12, MLP_S2 = 36;
+struct __align__(16) MlpPacked {
+  uint32_t w1[MLP_H * MLP_S1];  // [n][k/2]: words 0-2 W1[n][0..5], 3-5 the same again, rest 0
+  uint32_t w2[MLP_H * MLP_S2];  // [n][k/2], k < 64
+  float b1[MLP_H], b2[MLP_H], w3[MLP_H], b3[4];
+};
+static_assert(sizeof(MlpPacked) % 16 == 0, "MlpPacked is staged with 16-byte copies");
+constexpr int MLP_XS_WORDS = 32 * MLP_S1;  // per-warp feature rows (BF16 pairs, 12-word stride)
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float silu_hw(float z) {
+  const float h = 0.5f * z;
+  return fmaf(h, tanh_hw(h), h);
+}
+
+// FP32 weights -> packed BF16 layout (any grid; grid-stride over the words)
+__device__ inline void mlp_pack_words(const float* __restrict__ W, MlpPacked& P, int tid, int stride) {
+  for (int i = tid; i < MLP_H * MLP_S1; i += stride) {
+    const int n = i / MLP_S1, w = i % MLP_S1, k = 2 * (w < 3 ? w : w - 3);
+    P.w1[i] = w < 6 ? pack_bf16(W[MLP_W1 + n * MLP_IN + k], W[MLP_W1 + n * MLP_IN + k + 1]) : 0u;
+  }
+  for (int i = tid; i < MLP_H * MLP_S2; i += stride) {
+    const int n = i / MLP_S2, w = i % MLP_S2;
+    P.w2[i] = w < 32 ? pack_bf16(W[MLP_W2 + n * MLP_H + 2 * w], W[MLP_W2 + n * MLP_H + 2 * w + 1]) : 0u;
+  }
+  for (int i = tid; i < MLP_H; i += stride) {
+    P.b1[i] = W[MLP_B1 + i];
+    P.b2[i] = W[MLP_B2 + i];
+    P.w3[i] = W[MLP_W3 + i];
+  }
+  if (tid < 4) P.b3[tid] = tid == 0 ? W[MLP_B3] : 0.f;
+}
+
+// copy of the packed weights into shared memory by all threads of the CTA (caller syncs)
+__device__ inline void mlp_stage(const MlpPacked* __restrict__ g, MlpPacked& s) {
+  const uint4* src = reinterpret_cast<const uint4*>(g);
+  uint4* dst = reinterpret_cast<uint4*>(&s);
+  for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) dst[i] = __ldg(src + i);
+}
+
+// Network output (logit of the root fraction) for this lane's features.  Every lane of the warp
+// calls it, converged; xs is this warp's MLP_XS_WORDS-word scratch in shared memory.
+__device__ __forceinline__ float warp_mlp_logit(const MlpPacked& S, uint32_t* xs, const float (&f)[6]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  {
+    float hi[6], lo[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      hi[i] = __bfloat162float(__float2bfloat16_rn(f[i]));
+      lo[i] = f[i] - hi[i];
+    }
+    uint32_t* row = xs + lane * MLP_S1;
+    row[0] = pack_bf16(hi[0], hi[1]);
+    row[1] = pack_bf16(hi[2], hi[3]);
+    row[2] = pack_bf16(hi[4], hi[5]);
+    row[3] = pack_bf16(lo[0], lo[1]);
+    row[4] = pack_bf16(lo[2], lo[3]);
+    row[5] = pack_bf16(lo[4], lo[5]);
+    row[6] = 0u;
+    row[7] = 0u;
+  }
+  __syncwarp();
+  float part[2][2];
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const int r0 = mt * 16 + g, r1 = r0 + 8;
+    const uint32_t a[4] = {xs[r0 * MLP_S1 + t], xs[r1 * MLP_S1 + t], xs[r0 * MLP_S1 + t + 4],
+                           xs[r1 * MLP_S1 + t + 4]};
+    uint32_t a2[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        const int nn = 2 * kk + half;
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        mma_bf16_16816(c, a, S.w1[(nn * 8 + g) * MLP_S1 + t], S.w1[(nn * 8 + g) * MLP_S1 + t + 4]);
+        const int col = nn * 8 + 2 * t;
+        const float bb0 = S.b1[col], bb1 = S.b1[col + 1];
+        a2[kk][2 * half + 0] = pack_bf16(silu_hw(c[0] + bb0), silu_hw(c[1] + bb1));
+        a2[kk][2 * half + 1] = pack_bf16(silu_hw(c[2] + bb0), silu_hw(c[3] + bb1));
+      }
+    float p0 = 0.f, p1 = 0.f;
+#pragma unroll
+    for (int nn = 0; nn < 8; ++nn) {
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+        mma_bf16_16816(c, a2[kk], S.w2[(nn * 8 + g) * MLP_S2 + kk * 8 + t],
+                       S.w2[(nn * 8 + g) * MLP_S2 + kk * 8 + t + 4]);
+      const int col = nn * 8 + 2 * t;
+      const float bb0 = S.b2[col], bb1 = S.b2[col + 1], u0 = S.w3[col], u1 = S.w3[col + 1];
+      p0 = fmaf(silu_hw(c[0] + bb0), u0, fmaf(silu_hw(c[1] + bb1), u1, p0));
+      p1 = fmaf(silu_hw(c[2] + bb0), u0, fmaf(silu_hw(c[3] + bb1), u1, p1));
+    }
+    p0 += __shfl_xor_sync(0xffffffffu, p0, 1);
+    p0 += __shfl_xor_sync(0xffffffffu, p0, 2);
+    p1 += __shfl_xor_sync(0xffffffffu, p1, 1);
+    p1 += __shfl_xor_sync(0xffffffffu, p1, 2);
+    part[mt][0] = p0;
+    part[mt][1] = p1;
+  }
+  __syncwarp();  // xs may be rewritten by the next call
+  // row r of m-tile mt sits in lane quad (r % 8) as p0 (r < 8) or p1
+  const int src = (lane & 7) * 4;
+  const float v00 = __shfl_sync(0xffffffffu, part[0][0], src), v01 = __shfl_sync(0xffffffffu, part[0][1], src);
+  const float v10 = __shfl_sync(0xffffffffu, part[1][0], src), v11 = __shfl_sync(0xffffffffu, part[1][1], src);
+  const float out = lane < 16 ? ((lane & 8) ? v01 : v00) : ((lane & 8) ? v11 : v10);
+  return out + S.b3[0];
+}
+
+// warm-start fraction in (0, 1) from the network output, or -1 (midpoint start)
+__device__ __forceinline__ double warm_fraction_of(float logit) {
+  const float t = 1.0f / (1.0f + __expf(-logit));
+  return (t > 0.f && t < 1.f) ? (double)t : -1.0;
 }
 
 }  // namespace lp

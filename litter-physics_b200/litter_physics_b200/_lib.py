@@ -118,6 +118,7 @@ def lib():
         "lp_mlp_init": ([F, I32, U64], I32),
         "lp_mlp_train": ([F, I32, F, F, I64, I32, I32, C.c_float, F], I32),
         "lp_mlp_forward": ([F, I32, F, I64, F], I32),
+        "lp_mlp_forward_mma": ([F, I32, F, I64, F], I32),
         "lp_mlp_loss_grad": ([F, I32, F, F, I64, F, F], I32),
         "lp_mlp_loss_grad_noalloc": ([P, P, P, I64, P, P, P], I32),
         "lp_hb_features": ([C.c_double] * 6 + [F], None),

@@ -66,12 +66,15 @@ def train(x: np.ndarray, y: np.ndarray, epochs: int = 8, batch: int = 4096, lr: 
     return w, float(loss.value)
 
 
-def predict(w: np.ndarray, x: np.ndarray) -> np.ndarray:
+def predict(w: np.ndarray, x: np.ndarray, tensor_cores: bool = False) -> np.ndarray:
+    """Network output per feature row: the FP32 training arithmetic, or (tensor_cores) the BF16
+    tensor-core inference the solver's warm start runs."""
     x = np.ascontiguousarray(x, dtype=np.float32)
     y = np.zeros(len(x), dtype=np.float32)
     F = C.POINTER(C.c_float)
-    check(lib().lp_mlp_forward(np.ascontiguousarray(w, dtype=np.float32).ctypes.data_as(F), NW, x.ctypes.data_as(F),
-                               len(x), y.ctypes.data_as(F)))
+    fn = lib().lp_mlp_forward_mma if tensor_cores else lib().lp_mlp_forward
+    check(fn(np.ascontiguousarray(w, dtype=np.float32).ctypes.data_as(F), NW, x.ctypes.data_as(F), len(x),
+             y.ctypes.data_as(F)))
     return y
 
 

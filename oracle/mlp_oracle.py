@@ -39,6 +39,31 @@ def forward(w: np.ndarray, x: np.ndarray) -> np.ndarray:
     return h2 @ w3 + b3
 
 
+def bf16(a) -> np.ndarray:
+    """Round FP32 values to the nearest BF16 (ties to even), returned as FP32."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def forward_bf16(w: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """The tensor-core inference of lp_mlp.cuh with its roundings made explicit and the rest in
+    FP64: inputs split into BF16 hi + lo, W1 and W2 in BF16, the first hidden layer rounded to
+    BF16 after SiLU, the second hidden layer and the output layer unrounded."""
+    w32 = np.asarray(w, dtype=np.float32)
+    x32 = np.asarray(x, dtype=np.float32)
+    hi = bf16(x32)
+    lo = bf16(x32 - hi)
+    w1 = bf16(w32[W1:B1]).astype(np.float64).reshape(H, IN)
+    w2 = bf16(w32[W2:B2]).astype(np.float64).reshape(H, H)
+    b1, b2 = w32[B1:W2].astype(np.float64), w32[B2:W3].astype(np.float64)
+    w3, b3 = w32[W3:B3].astype(np.float64), float(w32[B3])
+    z1 = hi.astype(np.float64) @ w1.T + lo.astype(np.float64) @ w1.T + b1
+    h1 = bf16(silu(z1).astype(np.float32)).astype(np.float64)
+    h2 = silu(h1 @ w2.T + b2)
+    return h2 @ w3 + b3
+
+
 def loss_grad(w: np.ndarray, x: np.ndarray, y: np.ndarray) -> tuple[float, np.ndarray]:
     x = np.asarray(x, dtype=np.float64)
     y = np.asarray(y, dtype=np.float64)

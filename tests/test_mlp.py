@@ -63,12 +63,9 @@ def test_device_gradient_matches_fp64_oracle():
     assert np.allclose(yp, M.forward(w, x[:100]), rtol=1e-4, atol=1e-5)
 
 
-@pytest.mark.gpu
-def test_trained_network_cuts_newton_iterations_at_equal_tolerance():
-    """Train on pairs the plain Newton logs during a slump, then solve fresh return problems
-    with and without the warm start: same residual tolerance, fewer iterations."""
-    import ctypes as C
-
+@pytest.fixture(scope="module")
+def trained():
+    """Network trained by the device kernels on the pairs the plain Newton logs in a slump."""
     from litter_physics_b200 import _lib, configs, warmstart
     from litter_physics_b200.sim import Simulation
 
@@ -79,6 +76,81 @@ def test_trained_network_cuts_newton_iterations_at_equal_tolerance():
     assert len(y) > 1000
     w, loss = warmstart.train(x, y, epochs=20, batch=1024, lr=2e-3)
     assert loss < 0.05
+    return w, x
+
+
+@pytest.mark.gpu
+def test_tensor_core_inference_matches_oracle(trained):
+    """The solver's BF16 mma.sync forward pass against the FP64 oracle: error within the BF16
+    budget (1% of the output scale), and closer to the oracle's explicit-BF16-rounding forward
+    than to the unrounded one (the gap is rounding, not a fragment-layout error)."""
+    import mlp_oracle as M
+
+    from litter_physics_b200 import warmstart
+
+    w, x_train = trained
+    rng = np.random.default_rng(5)
+    x = np.concatenate([x_train[rng.choice(len(x_train), 3000, replace=False)],
+                        rng.normal(size=(997, 6)).astype(np.float32)])  # 3997 rows: a ragged last warp
+    y = warmstart.predict(w, x, tensor_cores=True).astype(np.float64)
+    y64 = M.forward(w.astype(np.float64), x)
+    yb = M.forward_bf16(w, x)
+    scale = max(1.0, float(np.abs(y64).max()))
+    err64 = np.abs(y - y64)
+    errb = np.abs(y - yb)
+    print(f"max |mma - fp64| {err64.max():.3e}, mean {err64.mean():.3e}; mean |mma - bf16 oracle| {errb.mean():.3e}")
+    assert err64.max() <= 1e-2 * scale
+    assert errb.mean() <= 0.5 * err64.mean()
+    # rows are independent of their warp neighbours
+    y_sub = warmstart.predict(w, x[7:40], tensor_cores=True).astype(np.float64)
+    assert np.array_equal(y_sub, y[7:40])
+
+
+@pytest.mark.gpu
+def test_warm_started_slump_matches_oracle(trained):
+    """Warm start inside the solver (G2P's tensor-core network pass): the slump after 100
+    substeps stays within the parity bars of the plain solver against the FP64 oracle, with
+    fewer Newton iterations."""
+    import oracle
+    from litter_physics_b200 import configs
+    from litter_physics_b200.sim import Simulation
+
+    w, _ = trained
+    spec = configs.slump(32, (8, 8, 16), seed=11, yield_range=(20.0, 100.0))
+    steps = 100
+    ref = oracle.OracleSim(spec)
+    ref.advance_to(steps * spec.max_dt)
+    r = ref.particles()
+    order_r = np.argsort(r["id"])
+    out = {}
+    for name, weights in (("plain", None), ("warm", w)):
+        sim = Simulation(spec)
+        sim.set_warm_start(weights)
+        sim.advance_to(steps * spec.max_dt)
+        p = sim.particles()
+        o = np.argsort(p["id"])
+        assert np.array_equal(p["id"][o], r["id"][order_r])
+        dx = float(np.abs(p["position"][o] - r["position"][order_r]).max()) / max(spec.domain)
+        dv = float(np.linalg.norm(p["velocity"][o] - r["velocity"][order_r])) / float(
+            np.linalg.norm(r["velocity"]))
+        out[name] = (dx, dv, sim.counters.newton_iterations, sim.counters.yielded_particles)
+    print(out)
+    for name in out:
+        assert out[name][0] <= 1e-5 and out[name][1] <= 1e-5, (name, out[name])
+    assert out["warm"][3] > 0
+    assert out["warm"][2] < 0.8 * out["plain"][2]
+
+
+@pytest.mark.gpu
+def test_trained_network_cuts_newton_iterations_at_equal_tolerance(trained):
+    """Solve fresh return problems with and without the warm start (tensor-core inference):
+    same residual tolerance, fewer iterations."""
+    import ctypes as C
+
+    from litter_physics_b200 import _lib, configs, warmstart
+    from litter_physics_b200.sim import Simulation
+
+    w, _ = trained
     # fresh problems from a different slump
     sim2 = Simulation(configs.slump(32, (8, 8, 16), seed=9, yield_range=(20.0, 100.0)))
     raw2, _ = warmstart.collect(sim2, 120, capacity=200_000)
