@@ -1123,9 +1123,16 @@ __global__ void k_couple(const InstDesc* __restrict__ desc, Control* __restrict_
 // memory once, then the CTA walks the tile's particles (contiguous in sorted slot order),
 // gathers from shared memory, advects, runs the constitutive update and writes the trial state
 // in sorted slot order.
+// Warm start (WARM instantiation): after the trial phase of each round of G2P_THREADS
+// particles, the yielding lanes of the whole CTA are compacted (ballot + warp prefix) into
+// feature rows in shared memory, ceil(count / 32) warps run the tensor-core network on full
+// 32-row blocks, and each lane reads its start value back.  The weights are staged on the
+// first round that has a yielding particle, so tiles with none never load them.
 struct G2pMlpShared {
   MlpPacked w;
-  uint32_t xs[(G2P_THREADS / 32) * MLP_XS_WORDS];
+  uint32_t xs[G2P_THREADS * MLP_S1];  // compacted feature rows
+  float out[G2P_THREADS];             // network output per row
+  int cnt[G2P_THREADS / 32];          // yielding lanes per warp
 };
 template <bool WARM>
 struct G2pWarmShared {
@@ -1138,6 +1145,36 @@ struct G2pWarmShared<true> {
   using type = G2pMlpShared;
 };
 
+// CTA-wide network pass of one round; every thread of the CTA calls it.  Returns the network
+// output for lanes with `need`, NaN otherwise.
+__device__ __forceinline__ float cta_warm_logit(G2pMlpShared& sh, const MlpPacked* __restrict__ mlp, bool& staged,
+                                                bool need, const float (&f)[6]) {
+  const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned bal = __ballot_sync(0xffffffffu, need);
+  if (lane == 0) sh.cnt[wid] = __popc(bal);
+  __syncthreads();
+  int before = 0, total = 0;
+#pragma unroll
+  for (int i = 0; i < G2P_THREADS / 32; ++i) {
+    const int ci = sh.cnt[i];
+    before += i < (int)wid ? ci : 0;
+    total += ci;
+  }
+  if (total == 0) return __int_as_float(0x7fc00000);  // CTA-uniform
+  const int q = before + __popc(bal & ((1u << lane) - 1u));
+  if (need) mlp_write_row(sh.xs + q * MLP_S1, f);
+  const int rows = (total + 31) & ~31;
+  if ((int)threadIdx.x >= total && (int)threadIdx.x < rows) mlp_zero_row(sh.xs + threadIdx.x * MLP_S1);
+  if (!staged) {  // CTA-uniform
+    mlp_stage(mlp, sh.w);
+    staged = true;
+  }
+  __syncthreads();
+  if ((int)(wid * 32) < total) sh.out[wid * 32 + lane] = warp_mlp_rows(sh.w, sh.xs + wid * 32 * MLP_S1);
+  __syncthreads();
+  return need ? sh.out[q] : __int_as_float(0x7fc00000);
+}
+
 template <bool WARM>
 __global__ void __launch_bounds__(G2P_THREADS, 2)
     k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
@@ -1148,7 +1185,6 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
           long long log_cap) {
   __shared__ float4 hv[HN];
   __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
-  // network weights and per-warp feature rows (the WARM instantiation only)
   __shared__ typename G2pWarmShared<WARM>::type wsh;
   const int tile = blockIdx.x;
   const int inst = tile_inst[tile];
@@ -1179,123 +1215,146 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
     hv[n] = (gi < D.nodes[0] && gj < D.nodes[1] && gk < D.nodes[2]) ? __ldg(&vel[node_index(D, gi, gj, gk)])
                                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
   }
-  const bool use_mlp = WARM && D.kind == 0 && c.warm_start && mlp != nullptr;  // CTA-uniform
-  if constexpr (WARM) {
-    if (use_mlp) mlp_stage(mlp, wsh.w);
-  }
   __syncthreads();
+  const bool use_mlp = WARM && D.kind == 0 && c.warm_start && mlp != nullptr;  // CTA-uniform
+  HbFeatureConst hfc;
+  if (use_mlp) hfc = hb_feature_const(D.consistency, D.flow_index, D.mu, c.dt);
+  bool staged = false;
+  const float* cur = c.parity ? st1 : st0;
+  float* nxt = c.parity ? st0 : st1;
+  const uint32_t* idc = c.parity ? id1 : id0;
+  uint32_t* idn = c.parity ? id0 : id1;
+  const float dx = (float)D.dx;
+  const float dt = (float)c.dt;
   double diss = 0.0, bb = 0.0, mass_sum = 0.0;
   float max_speed = 0.0f, max_disp = 0.0f;
   int fail = F_OK, iters = 0, yielded = 0;
   double fail_value = 0.0;
   for (uint32_t base0 = s0; base0 < e0; base0 += G2P_THREADS) {
-    // warp-uniform exit; lanes past the end of a partly filled warp redo the tile's last
-    // particle and store nothing, so the warp reaches the network call converged
-    if (base0 + (threadIdx.x & ~31u) >= e0) break;
+    // Without the network, a warp leaves once its slots are past the tile.  With it, the rounds
+    // stay CTA-uniform (the network pass synchronises the CTA); lanes past the end redo the
+    // tile's last particle and store nothing.
+    const bool warp_live = base0 + (threadIdx.x & ~31u) < e0;
+    if (!use_mlp && !warp_live) break;
     const bool valid = base0 + threadIdx.x < e0;
     const int64_t k = valid ? (int64_t)base0 + threadIdx.x : (int64_t)e0 - 1;
-    const int64_t src = perm[k];
-    const float* cur = c.parity ? st1 : st0;
-    float* nxt = c.parity ? st0 : st1;
-    const uint32_t* idc = c.parity ? id1 : id0;
-    uint32_t* idn = c.parity ? id0 : id1;
-    const float dx = (float)D.dx;
-    const float dt = (float)c.dt;
-    float x[3];
-    int base[3];
-    float w[3][3], d[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      x[a] = cur[(C_X + a) * cap + src];
-      const float sc = scaled_of(x[a], dx);
-      const float bf = floorf(sc - 0.5f);
-      base[a] = (int)(bf + 1.0f);
-      weights_of(sc - bf, dx, w[a], d[a]);
-    }
-    float v[3] = {0.f, 0.f, 0.f};
-    float Cm[9];
-#pragma unroll
-    for (int a = 0; a < 9; ++a) Cm[a] = 0.0f;
-    const int lbx = base[0] - ox, lby = base[1] - oy, lbz = base[2] - oz;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        const int row = ((lbx + a) * HY + (lby + b)) * HZ + lbz;
-        const float wab = w[0][a] * w[1][b];
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          const float4 nv = hv[row + cc];
-          const float ww = wab * w[2][cc];
-          const float vx = nv.x * ww, vy = nv.y * ww, vz = nv.z * ww;
-          v[0] += vx;
-          v[1] += vy;
-          v[2] += vz;
-          const float dd[3] = {d[0][a], d[1][b], d[2][cc]};
-#pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            Cm[0 * 3 + j] += vx * dd[j];
-            Cm[1 * 3 + j] += vy * dd[j];
-            Cm[2 * 3 + j] += vz * dd[j];
-          }
-        }
-      }
-    const float dx2_inv = 4.0f / (dx * dx);
-#pragma unroll
-    for (int a = 0; a < 9; ++a) Cm[a] *= dx2_inv;
-    const float speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    const float disp = speed * dt / dx;
-    const float m = cur[C_M * cap + src];
-    const float v0 = cur[C_V0 * cap + src];
-    // kinematic part of the trial state, stored before the constitutive update (sorted slot order)
-    if (valid) {
+    float Htr[9];
+    float tau[6];
+    float ep = 0.f, speed = 0.f, disp = 0.f, m = 0.f, v0 = 0.f;
+    double cn = 0.0, ys = 0.0;
+    int64_t src = 0;
+    PasteTrial pt;
+    PasteOut o;
+    pt.path = PT_DONE;
+    pt.trial_eq = 0.0;
+    if (warp_live) {
+      src = perm[k];
+      float x[3];
+      int base[3];
+      float w[3][3], d[3][3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        nxt[(C_X + a) * cap + k] = x[a] + v[a] * dt;
-        nxt[(C_V + a) * cap + k] = v[a];
+        x[a] = cur[(C_X + a) * cap + src];
+        const float sc = scaled_of(x[a], dx);
+        const float bf = floorf(sc - 0.5f);
+        base[a] = (int)(bf + 1.0f);
+        weights_of(sc - bf, dx, w[a], d[a]);
       }
+      float v[3] = {0.f, 0.f, 0.f};
+      float Cm[9];
 #pragma unroll
-      for (int a = 0; a < 9; ++a) nxt[(C_C + a) * cap + k] = Cm[a];
-      nxt[C_M * cap + k] = m;
-      nxt[C_V0 * cap + k] = v0;
-      if (D.per_particle_yield) nxt[C_YS * cap + k] = cur[C_YS * cap + src];
-      idn[k] = idc[src];
-    }
-    const double cn = sqrt((double)(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] +
-                                    Cm[5] * Cm[5] + Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]));
-    float tau[6];
-    float ep = cur[C_EP * cap + src];
-    if (D.kind == 0) {
-      float H[9], Htr[9];
+      for (int a = 0; a < 9; ++a) Cm[a] = 0.0f;
+      const int lbx = base[0] - ox, lby = base[1] - oy, lbz = base[2] - oz;
 #pragma unroll
-      for (int a = 0; a < 9; ++a) H[a] = cur[(C_H + a) * cap + src];
-      // H_tr = H + dt C + dt C H
+      for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
+        for (int b = 0; b < 3; ++b) {
+          const int row = ((lbx + a) * HY + (lby + b)) * HZ + lbz;
+          const float wab = w[0][a] * w[1][b];
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const float ch = Cm[3 * i + 0] * H[0 * 3 + j] + Cm[3 * i + 1] * H[1 * 3 + j] + Cm[3 * i + 2] * H[2 * 3 + j];
-          Htr[3 * i + j] = H[3 * i + j] + dt * (Cm[3 * i + j] + ch);
-        }
-      const double ys = D.per_particle_yield ? (double)cur[C_YS * cap + src] : D.yield;
-      PasteOut o;
-      PasteTrial pt;
-      paste_trial(Htr, D.mu, pt, o);
-      double sigma0 = -1.0;
-      if constexpr (WARM) {
-        if (use_mlp) {
-          // learned warm start: one tensor-core network pass per warp that has a yielding lane
-          const bool need =
-              valid && pt.path != PT_DONE && pt.trial_eq > ys && pt.trial_eq > 0.0 && D.consistency > 0.0;
-          if (__any_sync(0xffffffffu, need)) {
-            float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            if (need) hb_features(pt.trial_eq, ys, D.consistency, D.flow_index, D.mu, c.dt, f);
-            const float y = warp_mlp_logit(wsh.w, wsh.xs + (threadIdx.x >> 5) * MLP_XS_WORDS, f);
-            const double frac = warm_fraction_of(y);
-            if (need && frac > 0.0) sigma0 = ys + frac * (pt.trial_eq - ys);
+          for (int cc = 0; cc < 3; ++cc) {
+            const float4 nv = hv[row + cc];
+            const float ww = wab * w[2][cc];
+            const float vx = nv.x * ww, vy = nv.y * ww, vz = nv.z * ww;
+            v[0] += vx;
+            v[1] += vy;
+            v[2] += vz;
+            const float dd[3] = {d[0][a], d[1][b], d[2][cc]};
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              Cm[0 * 3 + j] += vx * dd[j];
+              Cm[1 * 3 + j] += vy * dd[j];
+              Cm[2 * 3 + j] += vz * dd[j];
+            }
           }
         }
+      const float dx2_inv = 4.0f / (dx * dx);
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Cm[a] *= dx2_inv;
+      speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      disp = speed * dt / dx;
+      m = cur[C_M * cap + src];
+      v0 = cur[C_V0 * cap + src];
+      ep = cur[C_EP * cap + src];
+      // kinematic part of the trial state, stored before the constitutive update (sorted slot order)
+      if (valid) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          nxt[(C_X + a) * cap + k] = x[a] + v[a] * dt;
+          nxt[(C_V + a) * cap + k] = v[a];
+        }
+#pragma unroll
+        for (int a = 0; a < 9; ++a) nxt[(C_C + a) * cap + k] = Cm[a];
+        nxt[C_M * cap + k] = m;
+        nxt[C_V0 * cap + k] = v0;
+        if (D.per_particle_yield) nxt[C_YS * cap + k] = cur[C_YS * cap + src];
+        idn[k] = idc[src];
       }
+      cn = sqrt((double)(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] +
+                         Cm[5] * Cm[5] + Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]));
+      if (D.kind == 0) {
+        float H[9];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) H[a] = cur[(C_H + a) * cap + src];
+        // H_tr = H + dt C + dt C H
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const float ch =
+                Cm[3 * i + 0] * H[0 * 3 + j] + Cm[3 * i + 1] * H[1 * 3 + j] + Cm[3 * i + 2] * H[2 * 3 + j];
+            Htr[3 * i + j] = H[3 * i + j] + dt * (Cm[3 * i + j] + ch);
+          }
+        ys = D.per_particle_yield ? (double)cur[C_YS * cap + src] : D.yield;
+        paste_trial(Htr, D.mu, pt, o);
+      } else {
+        const float jm1 = cur[C_JM1 * cap + src];
+        LiquidOut lo;
+        liquid_update(jm1, Cm, (float)D.bulk, (float)D.consistency, (float)D.tait_gamma, dt, lo);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) tau[a] = lo.tau[a];
+        if (valid) {
+          if (lo.fail != F_OK) fail = max(fail, lo.fail);
+          nxt[C_JM1 * cap + k] = lo.jm1;
+        }
+      }
+    }
+    double sigma0 = -1.0;
+    if constexpr (WARM) {
+      if (use_mlp) {
+        // learned warm start for the yielding lanes of this round
+        const bool need = valid && pt.path != PT_DONE && pt.trial_eq > ys && pt.trial_eq > 0.0;
+        float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (need) hb_features_f(hfc, pt.trial_eq, ys, f);
+        const float y = cta_warm_logit(wsh, mlp, staged, need, f);
+        if (need) {
+          const double frac = warm_fraction_of(y);
+          if (frac > 0.0) sigma0 = ys + frac * (pt.trial_eq - ys);
+        }
+      }
+    }
+    if (!warp_live) continue;
+    if (D.kind == 0) {
       paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, D.consistency, D.flow_index, c.dt, D.tol, sigma0, pt,
                    o);
 #pragma unroll
@@ -1324,16 +1383,6 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
             log_y[slot] = (float)o.eq;
           }
         }
-      }
-    } else {
-      const float jm1 = cur[C_JM1 * cap + src];
-      LiquidOut o;
-      liquid_update(jm1, Cm, (float)D.bulk, (float)D.consistency, (float)D.tait_gamma, dt, o);
-#pragma unroll
-      for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
-      if (valid) {
-        if (o.fail != F_OK) fail = max(fail, o.fail);
-        nxt[C_JM1 * cap + k] = o.jm1;
       }
     }
     if (!valid) continue;

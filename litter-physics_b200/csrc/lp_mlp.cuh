@@ -133,28 +133,33 @@ __device__ inline void mlp_stage(const MlpPacked* __restrict__ g, MlpPacked& s) 
   for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 16); i += blockDim.x) dst[i] = __ldg(src + i);
 }
 
-// Network output (logit of the root fraction) for this lane's features.  Every lane of the warp
-// calls it, converged; xs is this warp's MLP_XS_WORDS-word scratch in shared memory.
-__device__ __forceinline__ float warp_mlp_logit(const MlpPacked& S, uint32_t* xs, const float (&f)[6]) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  {
-    float hi[6], lo[6];
+// One feature row in the BF16 hi + lo layout of the first layer's A operand.
+__device__ __forceinline__ void mlp_write_row(uint32_t* row, const float (&f)[6]) {
+  float hi[6], lo[6];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      hi[i] = __bfloat162float(__float2bfloat16_rn(f[i]));
-      lo[i] = f[i] - hi[i];
-    }
-    uint32_t* row = xs + lane * MLP_S1;
-    row[0] = pack_bf16(hi[0], hi[1]);
-    row[1] = pack_bf16(hi[2], hi[3]);
-    row[2] = pack_bf16(hi[4], hi[5]);
-    row[3] = pack_bf16(lo[0], lo[1]);
-    row[4] = pack_bf16(lo[2], lo[3]);
-    row[5] = pack_bf16(lo[4], lo[5]);
-    row[6] = 0u;
-    row[7] = 0u;
+  for (int i = 0; i < 6; ++i) {
+    hi[i] = __bfloat162float(__float2bfloat16_rn(f[i]));
+    lo[i] = f[i] - hi[i];
   }
-  __syncwarp();
+  row[0] = pack_bf16(hi[0], hi[1]);
+  row[1] = pack_bf16(hi[2], hi[3]);
+  row[2] = pack_bf16(hi[4], hi[5]);
+  row[3] = pack_bf16(lo[0], lo[1]);
+  row[4] = pack_bf16(lo[2], lo[3]);
+  row[5] = pack_bf16(lo[4], lo[5]);
+  row[6] = 0u;
+  row[7] = 0u;
+}
+__device__ __forceinline__ void mlp_zero_row(uint32_t* row) {
+#pragma unroll
+  for (int w = 0; w < 8; ++w) row[w] = 0u;
+}
+
+// Network output (logit of the root fraction) of the 32 feature rows at xs (row stride MLP_S1
+// words) for the lane's own row.  Every lane of the warp calls it, converged, after the rows
+// are visible to the warp.
+__device__ __forceinline__ float warp_mlp_rows(const MlpPacked& S, const uint32_t* xs) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   float part[2][2];
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt) {
@@ -194,13 +199,50 @@ __device__ __forceinline__ float warp_mlp_logit(const MlpPacked& S, uint32_t* xs
     part[mt][0] = p0;
     part[mt][1] = p1;
   }
-  __syncwarp();  // xs may be rewritten by the next call
   // row r of m-tile mt sits in lane quad (r % 8) as p0 (r < 8) or p1
   const int src = (lane & 7) * 4;
   const float v00 = __shfl_sync(0xffffffffu, part[0][0], src), v01 = __shfl_sync(0xffffffffu, part[0][1], src);
   const float v10 = __shfl_sync(0xffffffffu, part[1][0], src), v11 = __shfl_sync(0xffffffffu, part[1][1], src);
   const float out = lane < 16 ? ((lane & 8) ? v01 : v00) : ((lane & 8) ? v11 : v10);
   return out + S.b3[0];
+}
+
+// Network output for this lane's features, rows staged in this warp's scratch xs
+// (MLP_XS_WORDS words); every lane of the warp calls it, converged.
+__device__ __forceinline__ float warp_mlp_logit(const MlpPacked& S, uint32_t* xs, const float (&f)[6]) {
+  const int lane = threadIdx.x & 31;
+  mlp_write_row(xs + lane * MLP_S1, f);
+  __syncwarp();
+  const float y = warp_mlp_rows(S, xs);
+  __syncwarp();  // xs may be rewritten by the next call
+  return y;
+}
+
+// Features of many return problems that share consistency, flow index, mu and dt (one
+// material, one attempt): the per-problem part is log a only.  FP32 restatement of hb_features.
+struct HbFeatureConst {
+  float lb8, n, inv_n_m1, f4, f5, inv_k;
+};
+__device__ inline HbFeatureConst hb_feature_const(double k, double n, double mu, double dt) {
+  HbFeatureConst h;
+  const double b = fmax(3.0 * mu * dt / k, 1e-300);
+  h.lb8 = (float)(log(b) / 8.0);
+  h.n = (float)n;
+  h.inv_n_m1 = (float)(1.0 / n - 1.0);
+  h.f4 = (float)(1.0 / (3.0 * n));
+  h.f5 = (float)log(n);
+  h.inv_k = (float)(1.0 / k);
+  return h;
+}
+__device__ __forceinline__ void hb_features_f(const HbFeatureConst& h, double trial, double ys, float (&f)[6]) {
+  const float a = fmaxf((float)(trial - ys) * h.inv_k, 1e-37f);
+  const float la8 = logf(a) * 0.125f;
+  f[0] = la8;
+  f[1] = h.lb8;
+  f[2] = h.n;
+  f[3] = h.lb8 + h.inv_n_m1 * la8;
+  f[4] = h.f4;
+  f[5] = h.f5;
 }
 
 // warm-start fraction in (0, 1) from the network output, or -1 (midpoint start)
