@@ -1123,6 +1123,51 @@ __global__ void k_couple(const InstDesc* __restrict__ desc, Control* __restrict_
 // memory once, then the CTA walks the tile's particles (contiguous in sorted slot order),
 // gathers from shared memory, advects, runs the constitutive update and writes the trial state
 // in sorted slot order.
+// Asynchronous 4-byte global -> shared copies (cp.async), used to prefetch the next round's
+// particle inputs while the current round computes.
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// G2P input slots per particle, [slot][thread] in shared memory, two rounds in flight
+enum {
+  PF_X = 0,    // 3: position
+  PF_H = 3,    // 9: F - I (paste)
+  PF_JM1 = 3,  // 1: J - 1 (liquid)
+  PF_EP = 12,
+  PF_M = 13,
+  PF_V0 = 14,
+  PF_YS = 15,  // per-particle yield stress
+  PF_ID = 16,
+  PF_SLOTS = 17
+};
+constexpr size_t G2P_SMEM = sizeof(float) * 2 * PF_SLOTS * G2P_THREADS;
+
+__device__ __forceinline__ void g2p_prefetch(float* __restrict__ buf, const float* __restrict__ cur,
+                                             const uint32_t* __restrict__ idc, int64_t cap, int64_t src, bool paste,
+                                             bool pyield) {
+  float* b = buf + threadIdx.x;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) cp_async4(b + (PF_X + a) * G2P_THREADS, cur + (C_X + a) * cap + src);
+  if (paste) {
+#pragma unroll
+    for (int a = 0; a < 9; ++a) cp_async4(b + (PF_H + a) * G2P_THREADS, cur + (C_H + a) * cap + src);
+    if (pyield) cp_async4(b + PF_YS * G2P_THREADS, cur + C_YS * cap + src);
+  } else {
+    cp_async4(b + PF_JM1 * G2P_THREADS, cur + C_JM1 * cap + src);
+  }
+  cp_async4(b + PF_EP * G2P_THREADS, cur + C_EP * cap + src);
+  cp_async4(b + PF_M * G2P_THREADS, cur + C_M * cap + src);
+  cp_async4(b + PF_V0 * G2P_THREADS, cur + C_V0 * cap + src);
+  cp_async4(b + PF_ID * G2P_THREADS, idc + src);
+}
+
 // Warm start (WARM instantiation): after the trial phase of each round of G2P_THREADS
 // particles, the yielding lanes of the whole CTA are compacted (ballot + warp prefix) into
 // feature rows in shared memory, ceil(count / 32) warps run the tensor-core network on full
@@ -1186,6 +1231,8 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
   __shared__ float4 hv[HN];
   __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
   __shared__ typename G2pWarmShared<WARM>::type wsh;
+  extern __shared__ float4 g2p_dyn[];  // G2P_SMEM bytes: prefetched inputs of two rounds
+  float* pf = reinterpret_cast<float*>(g2p_dyn);
   const int tile = blockIdx.x;
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
@@ -1230,31 +1277,56 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
   float max_speed = 0.0f, max_disp = 0.0f;
   int fail = F_OK, iters = 0, yielded = 0;
   double fail_value = 0.0;
-  for (uint32_t base0 = s0; base0 < e0; base0 += G2P_THREADS) {
+  const bool paste = D.kind == 0, pyield = paste && D.per_particle_yield;
+  const int nround = (int)((e0 - s0 + G2P_THREADS - 1) / G2P_THREADS);
+  // slot of this thread in round r (clamped to the tile's last particle) and warp liveness
+  auto slot_of = [&](int r) -> int64_t {
+    const int64_t kk = (int64_t)s0 + (int64_t)r * G2P_THREADS + threadIdx.x;
+    return kk < (int64_t)e0 ? kk : (int64_t)e0 - 1;
+  };
+  auto live_of = [&](int r) -> bool {
+    return (int64_t)s0 + (int64_t)r * G2P_THREADS + (threadIdx.x & ~31u) < (int64_t)e0;
+  };
+  // pipeline: copies of round r+1 are in flight while round r computes; perm of round r+2 is
+  // loaded a round ahead of its copies
+  int64_t src_next = 0;
+  if (live_of(0)) g2p_prefetch(pf, cur, idc, cap, perm[slot_of(0)], paste, pyield);
+  cp_async_commit();
+  if (nround > 1 && live_of(1)) src_next = perm[slot_of(1)];
+  const float c_tau = (float)(D.max_dt * 4.0 / (D.dx * D.dx));
+  const float c_dx = (float)(2.6 * D.dx);
+  const float c_g =
+      (float)(6.0 * sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]) *
+              D.max_dt);
+  for (int r = 0; r < nround; ++r) {
     // Without the network, a warp leaves once its slots are past the tile.  With it, the rounds
     // stay CTA-uniform (the network pass synchronises the CTA); lanes past the end redo the
     // tile's last particle and store nothing.
-    const bool warp_live = base0 + (threadIdx.x & ~31u) < e0;
+    const bool warp_live = live_of(r);
     if (!use_mlp && !warp_live) break;
-    const bool valid = base0 + threadIdx.x < e0;
-    const int64_t k = valid ? (int64_t)base0 + threadIdx.x : (int64_t)e0 - 1;
+    if (r + 1 < nround && live_of(r + 1))
+      g2p_prefetch(pf + ((r + 1) & 1) * PF_SLOTS * G2P_THREADS, cur, idc, cap, src_next, paste, pyield);
+    cp_async_commit();
+    if (r + 2 < nround && live_of(r + 2)) src_next = perm[slot_of(r + 2)];
+    cp_async_wait<1>();  // this thread's copies of round r have landed
+    const float* in = pf + (r & 1) * PF_SLOTS * G2P_THREADS + threadIdx.x;
+    const bool valid = (int64_t)s0 + (int64_t)r * G2P_THREADS + threadIdx.x < (int64_t)e0;
+    const int64_t k = slot_of(r);
     float Htr[9];
     float tau[6];
-    float ep = 0.f, speed = 0.f, disp = 0.f, m = 0.f, v0 = 0.f;
-    double cn = 0.0, ys = 0.0;
-    int64_t src = 0;
+    float ep = 0.f, speed = 0.f, disp = 0.f, m = 0.f, v0 = 0.f, cn = 0.f;
+    double ys = 0.0;
     PasteTrial pt;
     PasteOut o;
     pt.path = PT_DONE;
     pt.trial_eq = 0.0;
     if (warp_live) {
-      src = perm[k];
       float x[3];
       int base[3];
       float w[3][3], d[3][3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        x[a] = cur[(C_X + a) * cap + src];
+        x[a] = in[(PF_X + a) * G2P_THREADS];
         const float sc = scaled_of(x[a], dx);
         const float bf = floorf(sc - 0.5f);
         base[a] = (int)(bf + 1.0f);
@@ -1293,9 +1365,9 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
       for (int a = 0; a < 9; ++a) Cm[a] *= dx2_inv;
       speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
       disp = speed * dt / dx;
-      m = cur[C_M * cap + src];
-      v0 = cur[C_V0 * cap + src];
-      ep = cur[C_EP * cap + src];
+      m = in[PF_M * G2P_THREADS];
+      v0 = in[PF_V0 * G2P_THREADS];
+      ep = in[PF_EP * G2P_THREADS];
       // kinematic part of the trial state, stored before the constitutive update (sorted slot order)
       if (valid) {
 #pragma unroll
@@ -1307,15 +1379,15 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
         for (int a = 0; a < 9; ++a) nxt[(C_C + a) * cap + k] = Cm[a];
         nxt[C_M * cap + k] = m;
         nxt[C_V0 * cap + k] = v0;
-        if (D.per_particle_yield) nxt[C_YS * cap + k] = cur[C_YS * cap + src];
-        idn[k] = idc[src];
+        if (pyield) nxt[C_YS * cap + k] = in[PF_YS * G2P_THREADS];
+        idn[k] = __float_as_uint(in[PF_ID * G2P_THREADS]);
       }
-      cn = sqrt((double)(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] +
-                         Cm[5] * Cm[5] + Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]));
-      if (D.kind == 0) {
+      cn = sqrtf(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] + Cm[5] * Cm[5] +
+                 Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]);
+      if (paste) {
         float H[9];
 #pragma unroll
-        for (int a = 0; a < 9; ++a) H[a] = cur[(C_H + a) * cap + src];
+        for (int a = 0; a < 9; ++a) H[a] = in[(PF_H + a) * G2P_THREADS];
         // H_tr = H + dt C + dt C H
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -1325,10 +1397,10 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
                 Cm[3 * i + 0] * H[0 * 3 + j] + Cm[3 * i + 1] * H[1 * 3 + j] + Cm[3 * i + 2] * H[2 * 3 + j];
             Htr[3 * i + j] = H[3 * i + j] + dt * (Cm[3 * i + j] + ch);
           }
-        ys = D.per_particle_yield ? (double)cur[C_YS * cap + src] : D.yield;
+        ys = pyield ? (double)in[PF_YS * G2P_THREADS] : D.yield;
         paste_trial(Htr, D.mu, pt, o);
       } else {
-        const float jm1 = cur[C_JM1 * cap + src];
+        const float jm1 = in[PF_JM1 * G2P_THREADS];
         LiquidOut lo;
         liquid_update(jm1, Cm, (float)D.bulk, (float)D.consistency, (float)D.tait_gamma, dt, lo);
 #pragma unroll
@@ -1354,7 +1426,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
       }
     }
     if (!warp_live) continue;
-    if (D.kind == 0) {
+    if (paste) {
       paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, D.consistency, D.flow_index, c.dt, D.tol, sigma0, pt,
                    o);
 #pragma unroll
@@ -1389,17 +1461,16 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
 #pragma unroll
     for (int a = 0; a < 6; ++a) nxt[(C_TAU + a) * cap + k] = tau[a];
     nxt[C_EP * cap + k] = ep;
-    // momentum bound of the new state for the next attempt's fixed-point scale
-    const double mm = m;
-    const double tn = sqrt((double)(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]) +
-                           2.0 * (double)(tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]));
-    const double gn = sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]);
-    bb += mm * (double)speed + (cn * mm + tn * D.max_dt * 4.0 * (double)v0 / (D.dx * D.dx)) * 2.6 * D.dx +
-          6.0 * mm * gn * D.max_dt;
-    mass_sum += mm;
+    // momentum bound of the new state for the next attempt's fixed-point scale (its factors of
+    // 2.6 and 6 leave ample room for the FP32 rounding of the terms)
+    const float tn = sqrtf(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2] +
+                           2.f * (tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]));
+    bb += (double)(m * speed + (cn * m + tn * c_tau * v0) * c_dx + m * c_g);
+    mass_sum += (double)m;
     max_speed = fmaxf(max_speed, speed);
     max_disp = fmaxf(max_disp, disp);
   }
+  cp_async_wait<0>();  // no copy may land after the CTA's shared memory is released
   double rv[9] = {diss, bb, mass_sum, (double)max_speed, (double)max_disp, (double)fail, (double)iters,
                   (double)yielded, fail_value};
   block_reduce_multi<G2P_THREADS, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
@@ -1784,6 +1855,8 @@ constexpr size_t P2G_SMEM = sizeof(float4) * TB * 27;
 
 void configure_kernels() {
   cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM);
+  cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G2P_SMEM);
+  cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G2P_SMEM);
 }
 uint64_t kernel_launch_count() { return g_launches; }
 void add_kernel_launches(uint64_t n) { g_launches += n; }
@@ -1834,7 +1907,7 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
     ++n;
     if (ev) cudaEventRecord(ev[n], s);
   }
-  (A.mlp != nullptr && A.warm ? k_g2p<true> : k_g2p<false>)<<<(unsigned)A.n_tiles, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
+  (A.mlp != nullptr && A.warm ? k_g2p<true> : k_g2p<false>)<<<(unsigned)A.n_tiles, G2P_THREADS, G2P_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
                                                      A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, A.mlp, A.log_x,
                                                      A.log_y, A.log_n, A.log_cap);
   ++n;
