@@ -404,21 +404,34 @@ __global__ void k_bin_sort(const InstDesc* __restrict__ desc, const Control* __r
 }
 
 // ============================================================== P2G
-// One CTA per tile of TX x TY x TZ bins; three threads per bin, one per slab a of the 3x3x3
-// stencil.  All particles of a bin share the same 27 target nodes, so each thread accumulates
-// its 9 nodes x (mass, momentum) in registers over the bin's particles.  The partial sums go to
-// shared memory; then one thread per halo node adds its 27 contributors in a fixed order
-// (deterministic, no atomics, one barrier), converts to int64 fixed point, the tile's exact
-// particle totals are restored by a proportional correction, and each node component is
-// flushed with one global atomic.
+// One CTA per tile of TX x TY x TZ bins.  The tile's particles (contiguous in sorted slot order)
+// are taken in chunks of P2G_CHUNK:
+//   phase 1: the CTA loads each particle once (coalesced in slot order) and writes a 16-float
+//            record to shared memory: mass, momentum m v, the affine matrix
+//            A = C m - tau (dt 4/dx^2 V0), and the position relative to its stencil base;
+//   phase 2: three threads per bin, one per slab a of the 3x3x3 stencil, accumulate their 9
+//            nodes x (mass, momentum) in registers over the bin's records in sorted order.
+// All particles of a bin share the same 27 target nodes.  The partial sums then go to shared
+// memory (aliasing the records); one thread per halo node adds its 27 contributors in a fixed
+// order (deterministic, no atomics), converts to int64 fixed point, the tile's exact particle
+// totals are restored by a proportional correction, and each node component is flushed with
+// one global atomic.
+constexpr int P2G_CHUNK = 768;
+constexpr int P2G_REC = 16;  // m, q[3], A[9], f[3]
+constexpr size_t P2G_PART_BYTES = sizeof(float4) * TB * 27;
+constexpr size_t P2G_REC_BYTES = sizeof(float) * P2G_REC * P2G_CHUNK;
+constexpr size_t P2G_SMEM = P2G_PART_BYTES > P2G_REC_BYTES ? P2G_PART_BYTES : P2G_REC_BYTES;
+
 __global__ void __launch_bounds__(P2G_THREADS, 2)
     k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
           const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
           int64_t node_total, uint32_t* __restrict__ blk_epoch) {
-  extern __shared__ float4 part[];  // TB * 27 partial node sums (dynamic: 55 KB)
+  extern __shared__ float4 part[];  // particle records during the chunks, then TB * 27 partial node sums
+  float* rec = reinterpret_cast<float*>(part);  // [P2G_REC][P2G_CHUNK]
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
   __shared__ int redi[P2G_THREADS / 32];
+  __shared__ uint32_t bstart[TB + 1];
 
   const int tile = blockIdx.x;
   const int inst = tile_inst[tile];
@@ -427,12 +440,15 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
   const InstDesc& D = desc[inst];
   const int64_t ltile = tile - D.tile_off;
   const int64_t key0 = D.key_off + ltile * TB;
-  if (start[key0] == start[key0 + TB]) return;  // empty tile (uniform across the CTA)
+  const uint32_t ts = start[key0], te = start[key0 + TB];
+  if (ts == te) return;  // empty tile (uniform across the CTA)
 
   const int tz = (int)(ltile % D.tiles[2]);
   const int ty = (int)((ltile / D.tiles[2]) % D.tiles[1]);
   const int tx = (int)(ltile / ((int64_t)D.tiles[2] * D.tiles[1]));
   const int t = threadIdx.x;
+  if (t <= TB) bstart[t] = start[key0 + t];
+  __syncthreads();
   const int bin = t / 3, slab = t % 3;
   const int lx = bin / (TY * TZ), ly = (bin / TZ) % TY, lz = bin % TZ;
   const int bx = tx * TX + lx, by = ty * TY + ly, bz = tz * TZ + lz;
@@ -451,56 +467,77 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
       for (int k = 0; k < 4; ++k) acc9[b][q][k] = 0.0f;
   long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // tile totals (particles) then halo sums (nodes)
 
-  const uint32_t s = start[key0 + bin], e = start[key0 + bin + 1];
-  const float basef[3] = {(float)(bx - 1), (float)(by - 1), (float)(bz - 1)};
-  for (uint32_t j = s; j < e; ++j) {
-    const int64_t src = perm[j];
-    float x[3], v[3], Cm[9], tau[6];
+  const uint32_t s = bstart[bin], e = bstart[bin + 1];
+  for (uint32_t c0 = ts; c0 < te; c0 += P2G_CHUNK) {
+    const uint32_t cn = min((uint32_t)P2G_CHUNK, te - c0);
+    if (c0 != ts) __syncthreads();  // the previous chunk's records are consumed
+    // phase 1: one thread per particle
+    for (uint32_t i = t; i < cn; i += P2G_THREADS) {
+      const int64_t src = perm[c0 + i];
+      float x[3], v[3], Cm[9], tau[6];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      x[a] = cur[(C_X + a) * cap + src];
-      v[a] = cur[(C_V + a) * cap + src];
-    }
-#pragma unroll
-    for (int a = 0; a < 9; ++a) Cm[a] = cur[(C_C + a) * cap + src];
-#pragma unroll
-    for (int a = 0; a < 6; ++a) tau[a] = cur[(C_TAU + a) * cap + src];
-    const float m = cur[C_M * cap + src];
-    const float v0 = cur[C_V0 * cap + src];
-    float w[3][3], d[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) weights_of(scaled_of(x[a], dx) - basef[a], dx, w[a], d[a]);
-    // A = C m - tau (dt 4/dx^2 V0)
-    const float sv = stress_scale * v0;
-    const float T[9] = {tau[0], tau[3], tau[4], tau[3], tau[1], tau[5], tau[4], tau[5], tau[2]};
-    float A[9];
-#pragma unroll
-    for (int a = 0; a < 9; ++a) A[a] = Cm[a] * m - T[a] * sv;
-    const float q[3] = {v[0] * m, v[1] * m, v[2] * m};
-    const float wa = w[0][slab], da = d[0][slab];
-    float u[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) u[r] = q[r] + A[3 * r + 0] * da;
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      const float wab = wa * w[1][b];
-      float ub[3];
-#pragma unroll
-      for (int r = 0; r < 3; ++r) ub[r] = u[r] + A[3 * r + 1] * d[1][b];
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        const float ww = wab * w[2][cc];
-        acc9[b][cc][0] += ww * m;
-#pragma unroll
-        for (int r = 0; r < 3; ++r) acc9[b][cc][1 + r] += ww * (ub[r] + A[3 * r + 2] * d[2][cc]);
+      for (int a = 0; a < 3; ++a) {
+        x[a] = cur[(C_X + a) * cap + src];
+        v[a] = cur[(C_V + a) * cap + src];
       }
-    }
-    if (slab == 0) {
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Cm[a] = cur[(C_C + a) * cap + src];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) tau[a] = cur[(C_TAU + a) * cap + src];
+      const float m = cur[C_M * cap + src];
+      const float v0 = cur[C_V0 * cap + src];
+      // A = C m - tau (dt 4/dx^2 V0)
+      const float sv = stress_scale * v0;
+      const float T[9] = {tau[0], tau[3], tau[4], tau[3], tau[1], tau[5], tau[4], tau[5], tau[2]};
+      float* r = rec + i;
+      r[0] = m;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) r[(1 + a) * P2G_CHUNK] = v[a] * m;
+#pragma unroll
+      for (int a = 0; a < 9; ++a) r[(4 + a) * P2G_CHUNK] = Cm[a] * m - T[a] * sv;
+      // position relative to the particle's stencil base (its bin's base: floor(x/dx - 0.5))
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float sc = scaled_of(x[a], dx);
+        r[(13 + a) * P2G_CHUNK] = sc - floorf(sc - 0.5f);
+      }
       // exact per-particle totals: FP64 products of the stored FP32 mass and velocity
       tot[0] += to_fixed((double)m, s_m);
       tot[1] += to_fixed((double)m * (double)v[0], s_p);
       tot[2] += to_fixed((double)m * (double)v[1], s_p);
       tot[3] += to_fixed((double)m * (double)v[2], s_p);
+    }
+    __syncthreads();
+    // phase 2: this bin's particles inside the chunk, in sorted order
+    const uint32_t j0 = max(s, c0), j1 = min(e, c0 + cn);
+    for (uint32_t j = j0; j < j1; ++j) {
+      const float* r = rec + (j - c0);
+      const float m = r[0];
+      const float q[3] = {r[P2G_CHUNK], r[2 * P2G_CHUNK], r[3 * P2G_CHUNK]};
+      float A[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) A[a] = r[(4 + a) * P2G_CHUNK];
+      float w[3][3], d[3][3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) weights_of(r[(13 + a) * P2G_CHUNK], dx, w[a], d[a]);
+      const float wa = w[0][slab], da = d[0][slab];
+      float u[3];
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr) u[rr] = q[rr] + A[3 * rr + 0] * da;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float wab = wa * w[1][b];
+        float ub[3];
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr) ub[rr] = u[rr] + A[3 * rr + 1] * d[1][b];
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const float ww = wab * w[2][cc];
+          acc9[b][cc][0] += ww * m;
+#pragma unroll
+          for (int rr = 0; rr < 3; ++rr) acc9[b][cc][1 + rr] += ww * (ub[rr] + A[3 * rr + 2] * d[2][cc]);
+        }
+      }
     }
   }
   if (e > s) {
@@ -512,6 +549,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
         blk_epoch[blk] = (uint32_t)c.epoch;
       }
   }
+  __syncthreads();  // the last chunk's records (aliasing part[]) are consumed
 #pragma unroll
   for (int b = 0; b < 3; ++b)
 #pragma unroll
@@ -1851,7 +1889,6 @@ __global__ void k_liquid_batch(int64_t n, const double* j, const double* grad, d
 
 // ============================================================== launchers
 static uint64_t g_launches = 0;
-constexpr size_t P2G_SMEM = sizeof(float4) * TB * 27;
 
 void configure_kernels() {
   cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM);
