@@ -1211,22 +1211,21 @@ __device__ __forceinline__ void g2p_prefetch(float* __restrict__ buf, const floa
 // feature rows in shared memory, ceil(count / 32) warps run the tensor-core network on full
 // 32-row blocks, and each lane reads its start value back.  The weights are staged on the
 // first round that has a yielding particle, so tiles with none never load them.
+// The round's per-particle state (stress trial, kinematics) is parked in shared memory across
+// the network pass, whose fragments need the registers.
+constexpr int G2P_STASH = 28;
 struct G2pMlpShared {
   MlpPacked w;
-  uint32_t xs[G2P_THREADS * MLP_S1];  // compacted feature rows
-  float out[G2P_THREADS];             // network output per row
-  int cnt[G2P_THREADS / 32];          // yielding lanes per warp
+  uint32_t xs[G2P_THREADS * MLP_S1];     // compacted feature rows
+  float out[G2P_THREADS];                // network output per row
+  int cnt[G2P_THREADS / 32];             // yielding lanes per warp
+  float stash[G2P_STASH * G2P_THREADS];  // [slot][thread]
 };
+// dynamic shared memory of the G2P instantiations: prefetch slots, then (WARM) the network state
 template <bool WARM>
-struct G2pWarmShared {
-  struct type {
-    int unused;
-  };
-};
-template <>
-struct G2pWarmShared<true> {
-  using type = G2pMlpShared;
-};
+constexpr size_t g2p_smem_bytes() {
+  return G2P_SMEM + (WARM ? sizeof(G2pMlpShared) : 0);
+}
 
 // CTA-wide network pass of one round; every thread of the CTA calls it.  Returns the network
 // output for lanes with `need`, NaN otherwise.
@@ -1268,9 +1267,9 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
           long long log_cap) {
   __shared__ float4 hv[HN];
   __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
-  __shared__ typename G2pWarmShared<WARM>::type wsh;
-  extern __shared__ float4 g2p_dyn[];  // G2P_SMEM bytes: prefetched inputs of two rounds
+  extern __shared__ float4 g2p_dyn[];  // prefetched inputs of two rounds, then the network state
   float* pf = reinterpret_cast<float*>(g2p_dyn);
+  G2pMlpShared& wsh = *reinterpret_cast<G2pMlpShared*>(reinterpret_cast<char*>(g2p_dyn) + G2P_SMEM);
   const int tile = blockIdx.x;
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
@@ -1456,7 +1455,46 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
         const bool need = valid && pt.path != PT_DONE && pt.trial_eq > ys && pt.trial_eq > 0.0;
         float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (need) hb_features_f(hfc, pt.trial_eq, ys, f);
+        float* sp = wsh.stash + threadIdx.x;
+        {
+          const float park[G2P_STASH] = {Htr[0], Htr[1], Htr[2], Htr[3], Htr[4], Htr[5], Htr[6], Htr[7], Htr[8],
+                                         pt.dev.xx, pt.dev.yy, pt.dev.zz, pt.dev.xy, pt.dev.xz, pt.dev.yz,
+                                         pt.mean, pt.vol, pt.dnorm,
+                                         __int_as_float(__double2loint(pt.trial_eq)),
+                                         __int_as_float(__double2hiint(pt.trial_eq)),
+                                         __int_as_float(__double2loint(ys)), __int_as_float(__double2hiint(ys)),
+                                         ep, speed, disp, m, v0, cn};
+#pragma unroll
+          for (int i = 0; i < G2P_STASH; ++i) sp[i * G2P_THREADS] = park[i];
+        }
+        const int path = pt.path, ofail = o.fail;
         const float y = cta_warm_logit(wsh, mlp, staged, need, f);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Htr[i] = sp[i * G2P_THREADS];
+        pt.dev.xx = sp[9 * G2P_THREADS];
+        pt.dev.yy = sp[10 * G2P_THREADS];
+        pt.dev.zz = sp[11 * G2P_THREADS];
+        pt.dev.xy = sp[12 * G2P_THREADS];
+        pt.dev.xz = sp[13 * G2P_THREADS];
+        pt.dev.yz = sp[14 * G2P_THREADS];
+        pt.mean = sp[15 * G2P_THREADS];
+        pt.vol = sp[16 * G2P_THREADS];
+        pt.dnorm = sp[17 * G2P_THREADS];
+        pt.trial_eq = __hiloint2double(__float_as_int(sp[19 * G2P_THREADS]), __float_as_int(sp[18 * G2P_THREADS]));
+        ys = __hiloint2double(__float_as_int(sp[21 * G2P_THREADS]), __float_as_int(sp[20 * G2P_THREADS]));
+        ep = sp[22 * G2P_THREADS];
+        speed = sp[23 * G2P_THREADS];
+        disp = sp[24 * G2P_THREADS];
+        m = sp[25 * G2P_THREADS];
+        v0 = sp[26 * G2P_THREADS];
+        cn = sp[27 * G2P_THREADS];
+        pt.path = path;
+        o.fail = ofail;
+        o.iters = 0;
+        o.yielded = 0;
+        o.dep = 0.0;
+        o.diss_density = 0.0;
+        o.trial = o.eq = pt.trial_eq;
         if (need) {
           const double frac = warm_fraction_of(y);
           if (frac > 0.0) sigma0 = ys + frac * (pt.trial_eq - ys);
@@ -1892,8 +1930,8 @@ static uint64_t g_launches = 0;
 
 void configure_kernels() {
   cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM);
-  cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G2P_SMEM);
-  cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G2P_SMEM);
+  cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes<false>());
+  cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes<true>());
 }
 uint64_t kernel_launch_count() { return g_launches; }
 void add_kernel_launches(uint64_t n) { g_launches += n; }
@@ -1944,7 +1982,9 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
     ++n;
     if (ev) cudaEventRecord(ev[n], s);
   }
-  (A.mlp != nullptr && A.warm ? k_g2p<true> : k_g2p<false>)<<<(unsigned)A.n_tiles, G2P_THREADS, G2P_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
+  const bool warm_g2p = A.mlp != nullptr && A.warm;
+  (warm_g2p ? k_g2p<true> : k_g2p<false>)<<<(unsigned)A.n_tiles, G2P_THREADS,
+                                            warm_g2p ? g2p_smem_bytes<true>() : g2p_smem_bytes<false>(), s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
                                                      A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, A.mlp, A.log_x,
                                                      A.log_y, A.log_n, A.log_cap);
   ++n;
