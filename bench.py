@@ -177,6 +177,41 @@ def cpu_baseline_run(spec_fn, steps: int, threads: int) -> dict:
     return {"value": n * steps / dt, "particles": n, "steps": steps, "seconds": dt}
 
 
+def batch_measurement(args, stream, torch) -> dict:
+    """Config 3: 256 independent slumps of uneven size in one launch sequence per attempt.
+
+    Plain Newton; the autotuner picks the CUDA-graph length on the live batch; after W warm-up
+    attempts, K attempts of the whole batch are timed with CUDA events on the batch's stream."""
+    from litter_physics_b200 import configs
+    from litter_physics_b200.sim import Batch
+
+    t0 = time.perf_counter()
+    specs = configs.config3()
+    batch = Batch(specs)
+    batch.set_stream(stream.cuda_stream)
+    n = batch.total_particles()
+    setup = time.perf_counter() - t0
+    choice = batch.autotune(16)
+    batch.run_substeps(args.warmup)
+    batch.sync()
+    c0 = [batch.counters(i).step_count for i in range(len(specs))]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    batch.run_substeps(args.steps)
+    end.record(stream)
+    end.synchronize()
+    batch.sync()
+    ms = start.elapsed_time(end)
+    accepted = sum(int(batch.counters(i).step_count - c0[i]) * int(batch.counters(i).particle_count)
+                   for i in range(len(specs)))
+    batch.close()
+    return {"workload": "config 3: 256 HB slumps, particle counts log-uniform 8k-260k, seeds 100-355, "
+                        "parameters per instance as specified, plain Newton, tol 1e-10",
+            "instances": len(specs), "particles": n, "value": accepted / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / args.steps, "autotune": choice, "setup_s": round(setup, 2)}
+
+
 def reference_arm(args, ws, rank):
     if rank != 0:
         return
@@ -315,6 +350,7 @@ def ours(args, ws, rank, local):
         if dist is not None:
             dist.destroy_process_group()
         return
+    batch_info = None if args.no_batch else batch_measurement(args, stream, torch)
     peaks = measured_peaks()
     g2p_ms = ktimes.get("k_g2p", float("nan"))
     achieved = G2P_BYTES_PER_PARTICLE * n / (g2p_ms / 1e3) / 1e9
@@ -370,6 +406,7 @@ def ours(args, ws, rank, local):
                 "d2h_bytes_per_step": bytes_out / steps_done,
                 "path": "lp_sim_import_particles -> lp_sim_advance -> lp_sim_export_particles (host FP64 buffers)",
                 "steps": steps_done},
+        "batch_config3": batch_info,
         "gpu_launches": int(launches["warm"]),
         "clocks": clocks,
     }
@@ -387,6 +424,7 @@ def main():
     ap.add_argument("--workload", default="config2", choices=["config2", "config0", "small"])
     ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start (profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and CPU legs (profiling)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the config-3 batched measurement")
     ap.add_argument("--develop", type=int, default=150)
     ap.add_argument("--graph", type=int, default=0)
     ap.add_argument("--log-steps", type=int, default=300)

@@ -1714,18 +1714,22 @@ __global__ void k_state_stats(const InstDesc* __restrict__ desc, const Control* 
     for (int a = 0; a < 3; ++a) v[a] = cur[(C_V + a) * cap + k];
     for (int a = 0; a < 9; ++a) Cm[a] = cur[(C_C + a) * cap + k];
     for (int a = 0; a < 6; ++a) tau[a] = cur[(C_TAU + a) * cap + k];
-    const double m = cur[C_M * cap + k], v0 = cur[C_V0 * cap + k];
-    // speed in FP64 from the FP32 components
-    const double speed = sqrt((double)v[0] * v[0] + (double)v[1] * v[1] + (double)v[2] * v[2]);
-    double cn = 0, tn = 0;
-    for (int a = 0; a < 9; ++a) cn += (double)Cm[a] * Cm[a];
-    for (int a = 0; a < 3; ++a) tn += (double)tau[a] * tau[a];
-    for (int a = 3; a < 6; ++a) tn += 2.0 * (double)tau[a] * tau[a];
-    const double gn = sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]);
-    bb = m * speed + (sqrt(cn) * m + sqrt(tn) * D.max_dt * 4.0 * v0 / (D.dx * D.dx)) * 2.6 * D.dx +
-         6.0 * m * gn * D.max_dt;
-    sp = (float)speed;
-    ms = m;
+    const float m = cur[C_M * cap + k], v0 = cur[C_V0 * cap + k];
+    // the same FP32 expressions as the end of k_g2p, so that a state imported from a
+    // checkpoint gets the same speed and per-particle bound as the run that wrote it
+    const float speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const float cn = sqrtf(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] +
+                           Cm[5] * Cm[5] + Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]);
+    const float tn = sqrtf(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2] +
+                           2.f * (tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]));
+    const float c_tau = (float)(D.max_dt * 4.0 / (D.dx * D.dx));
+    const float c_dx = (float)(2.6 * D.dx);
+    const float c_g =
+        (float)(6.0 * sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]) *
+                D.max_dt);
+    bb = (double)(m * speed + (cn * m + tn * c_tau * v0) * c_dx + m * c_g);
+    sp = speed;
+    ms = (double)m;
   }
   bb = block_sum_d<G2P_THREADS>(bb, shd);
   ms = block_sum_d<G2P_THREADS>(ms, shd);
