@@ -96,6 +96,14 @@ typedef struct lp_fixture_spec {
   int32_t yield_random;       /* 1: per-particle sigma_y ~ U(yield_min, yield_max) (von Mises) */
   int32_t _pad2;
   double yield_min, yield_max;
+  /* pellet bed (config 4): bed_count >= 2 pellets of the geometry above (has_pellet = 1, fixture
+   * slump), centres and orientations drawn from bed_seed inside [bed_lo, bed_hi] without overlap,
+   * Hertz-Mindlin sphere contact between pellets; bed_count < 2 keeps the reference */
+  int32_t bed_count;
+  int32_t _pad3;
+  uint64_t bed_seed;
+  double bed_lo[3], bed_hi[3];
+  double hm_young, hm_poisson, hm_friction, hm_restitution;
 } lp_fixture_spec;
 
 /* Mirror of Ledger (solver.rs:65-124), FP64. */
@@ -209,6 +217,12 @@ lp_status lp_sim_export_particles(lp_sim* sim, lp_particles* out);
 lp_status lp_sim_import_particles(lp_sim* sim, const lp_particles* in);
 lp_status lp_sim_get_pellet(lp_sim* sim, lp_pellet* out, int32_t* has_pellet);
 lp_status lp_sim_set_pellet(lp_sim* sim, const lp_pellet* in);
+/* Pellet bed (extension, no reference counterpart): the committed state of every pellet, in
+ * pellet index order; *count = number of pellets (0 without a bed), at most cap written. */
+lp_status lp_sim_get_pellets(lp_sim* sim, lp_pellet* out, int32_t cap, int32_t* count);
+/* Pellet bed: replace the pose, velocity and angular momentum of every pellet (geometry must
+ * match); the sphere-contact histories restart empty. */
+lp_status lp_sim_set_pellets(lp_sim* sim, const lp_pellet* in, int32_t count);
 /* Observables as sorted name/value pairs (fixtures.rs:369-461).  names is a buffer of
  * `capacity` entries of 64 chars each; *count receives the number written. */
 lp_status lp_sim_observables(lp_sim* sim, char* names, double* values, int32_t capacity,

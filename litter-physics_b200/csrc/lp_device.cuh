@@ -100,6 +100,12 @@ struct InstDesc {
   double contact_k, contact_e, contact_mu;
   double extent[3];
   double s_mass;  // fixed-point scale of node mass
+  // pellet bed (extension): bed_np >= 2 pellets of one geometry, Hertz-Mindlin sphere contact
+  int bed_np;
+  int bed_nc[3];             // coarse cells per axis (cell edge bed_h = two bounding radii)
+  int64_t bed_off;           // first pellet of this instance in the global bed arrays
+  double bed_h, bed_rb;      // coarse cell edge, pellet bounding radius
+  double hm_estar, hm_gstar, hm_mu, hm_beta;  // effective moduli, friction, damping parameter
 };
 
 // pellet state (rigid.rs:30-49), FP64
@@ -144,6 +150,30 @@ struct Control {
   // pellet-step results of the current attempt
   double c_impulse[3], c_angular[3], c_grid_energy, c_pellet_energy, pw_impulse[3], pw_work;
   int pellet_fail, warm_start;
+  // pellet bed: committed buffer parity, cumulative sphere-contact work, last accepted step's
+  // contact count and history overflows
+  int bed_parity, bed_contacts;
+  double bed_contact_work;
+  uint64_t bed_overflow;
+};
+
+// pellet bed: tangential spring of one sphere pair (pellet-local sphere a, other pellet's b)
+constexpr int HM_SLOTS = 24;
+constexpr int BED_MAX = 4096;  // pellets per instance
+struct HmContact {
+  int other, a, b, pad;
+  double xi[3];
+};
+// pellet bed: double-buffered device arrays (index = buffer parity), passed to kernels by value
+struct BedPtrs {
+  PelletState* state[2];  // [pellet]
+  HmContact* hist[2];     // [pellet * HM_SLOTS]
+  int* hist_n[2];         // [pellet]
+};
+// pellet bed: per-pellet results of one attempt
+struct BedStep {
+  double imp[3], ang[3], cgrid, cpellet, wimp[3], wwork, ppwork;
+  int contacts, overflow, fail, pad;
 };
 
 // partial results of one grid-update CTA
@@ -172,6 +202,22 @@ struct ParticlePartial {
   int pad;
   double fail_value;
 };
+
+// Pellet-bed step limit: per pellet the reference's wall-contact and pellet-CFL limits
+// (solver.rs:477-498), plus 0.2 sqrt(m*/k_c) for the Hertz stiffness at an overlap of 5 % of
+// the sphere radius, k_c = 2 E* sqrt(R* 0.05 r).
+__host__ __device__ inline double bed_limit(const InstDesc& D, const PelletState* S) {
+  double limit = 1e300;
+  for (int p = 0; p < D.bed_np; ++p) {
+    const PelletState& P = S[p];
+    limit = fmin(limit, 0.2 * sqrt(P.mass / D.contact_k));
+    const double ps = sqrt(P.vel[0] * P.vel[0] + P.vel[1] * P.vel[1] + P.vel[2] * P.vel[2]);
+    if (ps > 0.0) limit = fmin(limit, D.cfl * D.dx / ps);
+    const double kc = 2.0 * D.hm_estar * sqrt(0.5 * P.radius * 0.05 * P.radius);
+    limit = fmin(limit, 0.2 * sqrt(0.5 * P.mass / kc));
+  }
+  return limit;
+}
 
 // ---------------------------------------------------------------- small helpers
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }

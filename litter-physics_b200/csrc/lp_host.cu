@@ -66,6 +66,7 @@ struct HostInstance {
   HostParticles P;
   bool has_pellet = false;
   lp::PelletState pellet;
+  std::vector<lp::PelletState> bed;  // pellet bed (extension)
 };
 
 int64_t axis_count(double size, double spacing) {
@@ -133,11 +134,118 @@ lp_status validate_spec(const lp_fixture_spec& s) {
     }
     case LP_SLUMP:
     case LP_DAM_BREAK:
-      if (s.has_pellet)
+      if (s.has_pellet && !(s.fixture == LP_SLUMP && s.bed_count >= 2))
         return set_error(LP_INVALID, "fixture does not accept boxes; only `coupled_patch` uses pellet geometry");
       break;
     default:
       return set_error(LP_INVALID, "unknown fixture");
+  }
+  if (s.bed_count >= 2) {
+    if (s.fixture != LP_SLUMP || !s.has_pellet)
+      return set_error(LP_UNSUPPORTED, "a pellet bed needs the slump fixture and a pellet geometry");
+    if (s.bed_count > lp::BED_MAX) return set_error(LP_INVALID, "pellet bed exceeds 4096 pellets per simulation");
+    for (int a = 0; a < 3; ++a)
+      if (!(std::isfinite(s.bed_lo[a]) && std::isfinite(s.bed_hi[a]) && s.bed_lo[a] <= s.bed_hi[a] &&
+            s.bed_lo[a] >= 0.0 && s.bed_hi[a] <= s.domain[a]))
+        return set_error(LP_INVALID, "pellet bed region must lie inside `domain_m`");
+    if (!(std::isfinite(s.hm_young) && s.hm_young > 0.0) || !(s.hm_poisson >= 0.0 && s.hm_poisson < 0.5) ||
+        !(std::isfinite(s.hm_friction) && s.hm_friction >= 0.0) ||
+        !(s.hm_restitution > 0.0 && s.hm_restitution <= 1.0))
+      return set_error(LP_INVALID, "invalid Hertz-Mindlin parameters (young > 0, 0 <= poisson < 0.5, "
+                                   "friction >= 0, 0 < restitution <= 1)");
+  }
+  return LP_OK;
+}
+
+// Damping of the Hertz-Mindlin normal force, F = (4/3) E* sqrt(R*) d^1.5 - gamma v_n with
+// gamma = -2 sqrt(5/6) beta sqrt(2 E* sqrt(R* d) m*), calibrated so that a head-on impact
+// rebounds with the requested restitution e.  In scaled units the overlap obeys
+// x'' = -max(x^1.5 + c x^0.25 x', 0), c = -sqrt(5) beta, x(0) = 0, x'(0) = 1, whatever the
+// impact speed, masses and moduli (the damping scales with the contact stiffness), and
+// e = -x' when the spheres separate.  The closed form beta = ln e / sqrt(ln^2 e + pi^2) of the
+// linear spring-dashpot would give e = 0.40 for a requested 0.3 under Hertz contact.
+static double hm_restitution_of(double beta) {
+  const double c = -std::sqrt(5.0) * beta, h = 2e-4;
+  auto acc = [c](double x, double v) {
+    if (x <= 0.0) return 0.0;
+    const double f = std::pow(x, 1.5) + c * std::pow(x, 0.25) * v;
+    return f > 0.0 ? -f : 0.0;
+  };
+  double x = 0.0, v = 1.0;
+  for (int n = 1; n <= 1000000; ++n) {
+    const double k1x = v, k1v = acc(x, v);
+    const double k2x = v + 0.5 * h * k1v, k2v = acc(x + 0.5 * h * k1x, v + 0.5 * h * k1v);
+    const double k3x = v + 0.5 * h * k2v, k3v = acc(x + 0.5 * h * k2x, v + 0.5 * h * k2v);
+    const double k4x = v + h * k3v, k4v = acc(x + h * k3x, v + h * k3v);
+    x += h / 6.0 * (k1x + 2.0 * k2x + 2.0 * k3x + k4x);
+    v += h / 6.0 * (k1v + 2.0 * k2v + 2.0 * k3v + k4v);
+    if (x <= 0.0) break;
+  }
+  return -v;
+}
+static double hm_beta_for(double e) {
+  if (e >= 1.0) return 0.0;
+  double lo = -20.0, hi = 0.0;  // restitution rises from lo to hi
+  for (int it = 0; it < 60; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (hm_restitution_of(mid) < e) lo = mid;
+    else hi = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+lp_status make_pellet(double r, double len, double rho, const double pos[3], lp::PelletState& p);
+void q_matrix(const double* q, double R[3][3]);
+
+// Pellet bed placement (extension).  Pellet p draws its centre (three uniforms, x y z) and then
+// its orientation (three uniforms, Shoemake's uniform random rotation: q = (sqrt(1-u1) sin 2pi u2,
+// sqrt(1-u1) cos 2pi u2, sqrt(u1) sin 2pi u3, sqrt(u1) cos 2pi u3) as (i, j, k, w)) from one
+// SplitMix64 stream seeded with bed_seed, and redraws until every sphere lies at least one
+// radius inside the walls and at least 2.02 radii from every sphere of the pellets placed so far.
+lp_status make_bed(const lp_fixture_spec& s, const double extent[3], std::vector<lp::PelletState>& bed) {
+  SplitMix64 rng{s.bed_seed};
+  bed.clear();
+  const double zero[3] = {0.0, 0.0, 0.0};
+  lp::PelletState proto;
+  lp_status st = make_pellet(s.pellet_radius, s.pellet_length, s.pellet_density, zero, proto);
+  if (st != LP_OK) return st;
+  const double r = proto.radius;
+  std::vector<double> centres;  // 3 per placed sphere
+  for (int p = 0; p < s.bed_count; ++p) {
+    bool placed = false;
+    for (int attempt = 0; attempt < 10000 && !placed; ++attempt) {
+      lp::PelletState P = proto;
+      for (int a = 0; a < 3; ++a) P.pos[a] = s.bed_lo[a] + (s.bed_hi[a] - s.bed_lo[a]) * rng.next_unit();
+      const double u1 = rng.next_unit(), u2 = rng.next_unit(), u3 = rng.next_unit();
+      const double s1 = std::sqrt(1.0 - u1), s2 = std::sqrt(u1), t1 = 2.0 * kPi * u2, t2 = 2.0 * kPi * u3;
+      P.q[0] = s1 * std::sin(t1);
+      P.q[1] = s1 * std::cos(t1);
+      P.q[2] = s2 * std::sin(t2);
+      P.q[3] = s2 * std::cos(t2);
+      double R[3][3];
+      q_matrix(P.q, R);
+      std::vector<double> mine;
+      bool ok = true;
+      for (int k = 0; k < P.nsph && ok; ++k) {
+        double c[3];
+        for (int a = 0; a < 3; ++a) {
+          c[a] = P.pos[a] + R[a][0] * P.off[k];
+          if (c[a] < r || c[a] > extent[a] - r) ok = false;
+        }
+        for (size_t o = 0; o < centres.size() && ok; o += 3) {
+          const double dx = c[0] - centres[o], dy = c[1] - centres[o + 1], dz = c[2] - centres[o + 2];
+          if (dx * dx + dy * dy + dz * dz < (2.02 * r) * (2.02 * r)) ok = false;
+        }
+        mine.insert(mine.end(), c, c + 3);
+      }
+      if (!ok) continue;
+      centres.insert(centres.end(), mine.begin(), mine.end());
+      bed.push_back(P);
+      placed = true;
+    }
+    if (!placed)
+      return set_error(LP_INVALID, "pellet bed: pellet " + std::to_string(p) +
+                                       " does not fit in the region without overlap after 10000 draws");
   }
   return LP_OK;
 }
@@ -240,6 +348,13 @@ lp_status build_instance(const lp_fixture_spec& s, HostInstance& h) {
   if (s.yield_random)
     for (size_t p = 0; p < n; ++p) P.ys[p] = s.yield_min + (s.yield_max - s.yield_min) * rng.next_unit();
   h.has_pellet = false;
+  h.bed.clear();
+  if (s.bed_count >= 2) {
+    const double extent[3] = {(double)h.cells[0] * s.grid_spacing, (double)h.cells[1] * s.grid_spacing,
+                              (double)h.cells[2] * s.grid_spacing};
+    st = make_bed(s, extent, h.bed);
+    if (st != LP_OK) return st;
+  }
   if (s.fixture == LP_COUPLED_PATCH && s.has_pellet) {
     const double center[3] = {0.5 * s.domain[0], 0.5 * s.domain[1],
                               s.initial_size[2] + 2.0 * s.grid_spacing + s.pellet_radius};
@@ -426,6 +541,18 @@ struct Energies {
   double ke, pe, ee, mech, mass_res, mom_res[3], e_res;
 };
 
+// committed pellet-bed states of instance i (host copy)
+std::vector<lp::PelletState> bed_pull(const Ensemble& E, int i) {
+  const InstDesc& D = E.desc[i];
+  std::vector<lp::PelletState> out((size_t)std::max(D.bed_np, 0));
+  if (D.bed_np < 2) return out;
+  const int par = E.ctrl_h[i].bed_parity;
+  cudaStreamSynchronize(E.stream);
+  cudaMemcpy(out.data(), E.A.bed.state[par] + D.bed_off, sizeof(lp::PelletState) * out.size(),
+             cudaMemcpyDeviceToHost);
+  return out;
+}
+
 Energies energies_of(const Ensemble& E, int i, const Diag& d) {
   const Control& c = E.ctrl_h[i];
   const InstDesc& D = E.desc[i];
@@ -439,13 +566,22 @@ Energies energies_of(const Ensemble& E, int i, const Diag& d) {
     r.pe -= c.pellet.mass * (D.gravity[0] * c.pellet.pos[0] + D.gravity[1] * c.pellet.pos[1] + D.gravity[2] * c.pellet.pos[2]);
     for (int a = 0; a < 3; ++a) mom[a] += c.pellet.vel[a] * c.pellet.mass;
   }
+  if (D.bed_np >= 2)
+    for (const lp::PelletState& P : bed_pull(E, i)) {
+      r.ke += pellet_ke_h(P);
+      r.pe -= P.mass * (D.gravity[0] * P.pos[0] + D.gravity[1] * P.pos[1] + D.gravity[2] * P.pos[2]);
+      for (int a = 0; a < 3; ++a) mom[a] += P.vel[a] * P.mass;
+    }
   r.mech = r.ke + r.pe + r.ee;
   const lp::LedgerD& L = c.ledger;
   r.mass_res = d.mass + L.outflow_mass - L.initial_mass;
   for (int a = 0; a < 3; ++a)
     r.mom_res[a] = mom[a] - L.initial_momentum[a] - L.gravity_impulse[a] + L.outflow_momentum[a] - L.wall_impulse[a] -
                    L.pellet_wall_impulse[a];
-  const double ledgered = L.proj - L.fric + L.trac + L.pellet_work + L.cgrid + L.cpellet - L.plastic;
+  // the pellet bed's sphere-contact work (dissipation plus energy stored in the contacts) is
+  // ledgered beside the reference channels
+  const double ledgered =
+      L.proj - L.fric + L.trac + L.pellet_work + L.cgrid + L.cpellet - L.plastic + c.bed_contact_work;
   r.e_res = r.mech - L.initial_mech - ledgered;
   return r;
 }
@@ -472,7 +608,9 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   int64_t node_off = 0, tile_off = 0, key_off = 0, blk_off = 0, gcta_off = 0, slot_off = 0;
   std::vector<int> tile_inst, gcta_inst, pcta_inst, chunk_inst;
   std::vector<lp::SegDesc> segs;
-  int any_pellet = 0;
+  int any_pellet = 0, any_bed = 0;
+  int64_t bed_off = 0;
+  std::vector<int> bed_inst;
   for (int i = 0; i < count; ++i) {
     const lp_fixture_spec& s = specs[i];
     HostInstance& h = H[i];
@@ -495,6 +633,25 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
     D.face_mode = s.face_mode_enabled ? 1 : 0;
     D.has_pellet = h.has_pellet ? 1 : 0;
     any_pellet |= D.has_pellet;
+    D.bed_np = (int)h.bed.size();
+    D.bed_off = bed_off;
+    if (D.bed_np >= 2) {
+      any_bed = 1;
+      const lp::PelletState& P0 = h.bed[0];
+      double hs = 0.0;
+      for (int k = 0; k < P0.nsph; ++k) hs = std::fmax(hs, std::fabs(P0.off[k]));
+      D.bed_rb = hs + P0.radius;
+      D.bed_h = 2.0 * D.bed_rb;
+      for (int a = 0; a < 3; ++a)
+        D.bed_nc[a] = std::max(1, (int)std::ceil((double)h.cells[a] * s.grid_spacing / D.bed_h));
+      const double nu = s.hm_poisson, E = s.hm_young, G = E / (2.0 * (1.0 + nu));
+      D.hm_estar = E / (2.0 * (1.0 - nu * nu));
+      D.hm_gstar = G / (2.0 * (2.0 - nu));
+      D.hm_mu = s.hm_friction;
+      D.hm_beta = hm_beta_for(s.hm_restitution);
+      for (int p = 0; p < D.bed_np; ++p) bed_inst.push_back(i);
+      bed_off += D.bed_np;
+    }
     const int64_t ntiles = (int64_t)D.tiles[0] * D.tiles[1] * D.tiles[2];
     const int64_t nnodes = (int64_t)D.nodes[0] * D.nodes[1] * D.nodes[2];
     const int64_t nblk = (int64_t)D.nblk[0] * D.nblk[1] * D.nblk[2];
@@ -558,6 +715,8 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   lp::DeviceArrays& A = E.A;
   A.n_inst = count;
   A.any_pellet = any_pellet;
+  A.any_bed = any_bed;
+  A.n_bed = bed_off;
   A.cap = slot_off;
   A.n_pcta = (int64_t)pcta_inst.size();
   A.n_tiles = (int64_t)tile_inst.size();
@@ -597,7 +756,25 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   A.n_seg = (int64_t)segs.size();
   ALLOC(A.segs, A.n_seg);
   ALLOC(A.seg, A.n_seg);
+  for (int b = 0; b < 2; ++b) {
+    ALLOC(A.bed.state[b], A.n_bed);
+    ALLOC(A.bed.hist[b], A.n_bed * lp::HM_SLOTS);
+    ALLOC(A.bed.hist_n[b], A.n_bed);
+  }
+  ALLOC(A.bed_step, A.n_bed);
+  ALLOC(A.bed_key, A.n_bed);
+  ALLOC(A.bed_idx, A.n_bed);
+  ALLOC(A.bed_inst, A.n_bed);
 #undef ALLOC
+  if (any_bed) {
+    std::vector<lp::PelletState> all;
+    for (int i = 0; i < count; ++i) all.insert(all.end(), H[i].bed.begin(), H[i].bed.end());
+    CUDA_CK(cudaMemcpyAsync(A.bed.state[0], all.data(), sizeof(lp::PelletState) * all.size(), cudaMemcpyHostToDevice,
+                            E.stream));
+    CUDA_CK(cudaMemcpyAsync(A.bed_inst, bed_inst.data(), sizeof(int) * bed_inst.size(), cudaMemcpyHostToDevice,
+                            E.stream));
+    CUDA_CK(cudaStreamSynchronize(E.stream));
+  }
   CUDA_CK(cudaMemcpyAsync(A.segs, segs.data(), sizeof(lp::SegDesc) * segs.size(), cudaMemcpyHostToDevice, E.stream));
   CUDA_CK(cudaMemcpyAsync(A.desc, E.desc.data(), sizeof(InstDesc) * count, cudaMemcpyHostToDevice, E.stream));
   CUDA_CK(cudaMemcpyAsync(A.pcta_inst, pcta_inst.data(), sizeof(int) * pcta_inst.size(), cudaMemcpyHostToDevice, E.stream));
@@ -663,6 +840,8 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
     c.ledger.initial_mass = d[i].mass;
     for (int a = 0; a < 3; ++a)
       c.ledger.initial_momentum[a] = d[i].mom[a] + (E.desc[i].has_pellet ? c.pellet.vel[a] * c.pellet.mass : 0.0);
+    for (const lp::PelletState& P : H[i].bed)
+      for (int a = 0; a < 3; ++a) c.ledger.initial_momentum[a] += P.vel[a] * P.mass;
     c.ledger.initial_mech = en.mech;
   }
   return push_ctrl(E);
@@ -957,6 +1136,28 @@ lp_status observables(Ensemble& E, int i, std::map<std::string, double>& out) {
     out["coupling_grid_energy_j"] = L.cgrid;
     out["coupling_pellet_energy_j"] = L.cpellet;
   }
+  if (D.bed_np >= 2) {
+    const std::vector<lp::PelletState> B = bed_pull(E, i);
+    double zs = 0.0, zmin = 1e300, vmax = 0.0, ke = 0.0;
+    for (const lp::PelletState& P : B) {
+      zs += P.pos[2];
+      zmin = std::min(zmin, P.pos[2]);
+      vmax = std::max(vmax, std::sqrt(P.vel[0] * P.vel[0] + P.vel[1] * P.vel[1] + P.vel[2] * P.vel[2]));
+      ke += pellet_ke_h(P);
+    }
+    out["pellet_count"] = (double)B.size();
+    out["pellet_mean_z_m"] = zs / (double)B.size();
+    out["pellet_min_z_m"] = zmin;
+    out["pellet_max_speed_m_s"] = vmax;
+    out["pellet_kinetic_energy_j"] = ke;
+    out["pellet_contact_work_j"] = c.bed_contact_work;
+    out["pellet_contacts"] = (double)c.bed_contacts;
+    out["pellet_history_overflow"] = (double)c.bed_overflow;
+    out["pellet_wall_work_j"] = L.pellet_work;
+    out["coupling_grid_energy_j"] = L.cgrid;
+    out["coupling_pellet_energy_j"] = L.cpellet;
+    out["coupling_impulse_z_kg_m_s"] = L.coupling_impulse[2];
+  }
   return LP_OK;
 }
 
@@ -1091,6 +1292,10 @@ lp_status lp_sim_stability_limit(lp_sim* sim, double* out) {
     const double ps = std::sqrt(c.pellet.vel[0] * c.pellet.vel[0] + c.pellet.vel[1] * c.pellet.vel[1] + c.pellet.vel[2] * c.pellet.vel[2]);
     if (ps > 0.0) limit = std::fmin(limit, D.cfl * D.dx / ps);
   }
+  if (D.bed_np >= 2) {
+    const std::vector<lp::PelletState> B = bed_pull(sim->E, 0);
+    limit = std::fmin(limit, lp::bed_limit(D, B.data()));
+  }
   *out = limit;
   return LP_OK;
 }
@@ -1138,6 +1343,55 @@ lp_status lp_sim_particle_count(lp_sim* sim, uint64_t* out) {
 lp_status lp_sim_export_particles(lp_sim* sim, lp_particles* out) { return export_particles(sim->E, 0, out); }
 lp_status lp_sim_import_particles(lp_sim* sim, const lp_particles* in) { return import_particles(sim->E, 0, in); }
 
+static void pellet_out(const lp::PelletState& P, lp_pellet* out) {
+  std::memset(out, 0, sizeof(*out));
+  out->radius = P.radius;
+  out->length = P.length;
+  out->mass = P.mass;
+  for (int a = 0; a < 3; ++a) {
+    out->inertia_body[a] = P.inertia[a];
+    out->position[a] = P.pos[a];
+    out->velocity[a] = P.vel[a];
+    out->angular_momentum[a] = P.L[a];
+  }
+  for (int a = 0; a < 4; ++a) out->orientation[a] = P.q[a];
+  out->sphere_count = P.nsph;
+  for (int k = 0; k < P.nsph; ++k) out->sphere_offsets[k] = P.off[k];
+}
+lp_status lp_sim_get_pellets(lp_sim* sim, lp_pellet* out, int32_t cap, int32_t* count) {
+  if (!count) return set_error(LP_INVALID, "null count");
+  lp_status st = pull_ctrl(sim->E);
+  if (st != LP_OK) return st;
+  const std::vector<lp::PelletState> B = bed_pull(sim->E, 0);
+  *count = (int32_t)B.size();
+  for (int32_t p = 0; p < std::min<int32_t>(cap, (int32_t)B.size()); ++p) pellet_out(B[p], out + p);
+  return LP_OK;
+}
+lp_status lp_sim_set_pellets(lp_sim* sim, const lp_pellet* in, int32_t count) {
+  Ensemble& E = sim->E;
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const InstDesc& D = E.desc[0];
+  if (D.bed_np < 2 || count != D.bed_np || !in) return set_error(LP_INVALID, "pellet count differs from the bed's");
+  std::vector<lp::PelletState> B = bed_pull(E, 0);
+  for (int32_t p = 0; p < count; ++p) {
+    const lp_pellet& q = in[p];
+    if (q.sphere_count != B[p].nsph || q.radius != B[p].radius || q.mass != B[p].mass)
+      return set_error(LP_INVALID, "pellet geometry differs from the bed's");
+    for (int a = 0; a < 3; ++a) {
+      B[p].pos[a] = q.position[a];
+      B[p].vel[a] = q.velocity[a];
+      B[p].L[a] = q.angular_momentum[a];
+    }
+    for (int a = 0; a < 4; ++a) B[p].q[a] = q.orientation[a];
+  }
+  E.invalidate_graph();
+  const int par = E.ctrl_h[0].bed_parity;
+  CUDA_CK(cudaMemcpy(E.A.bed.state[par] + D.bed_off, B.data(), sizeof(lp::PelletState) * B.size(),
+                     cudaMemcpyHostToDevice));
+  CUDA_CK(cudaMemset(E.A.bed.hist_n[par] + D.bed_off, 0, sizeof(int) * B.size()));
+  return LP_OK;
+}
 lp_status lp_sim_get_pellet(lp_sim* sim, lp_pellet* out, int32_t* has) {
   lp_status st = pull_ctrl(sim->E);
   if (st != LP_OK) return st;
@@ -1280,9 +1534,9 @@ lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* name
     lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
     if (st != LP_OK) return st;
   }
-  cudaEvent_t ev[16];
-  for (int k = 0; k < 16; ++k) CUDA_CK(cudaEventCreate(&ev[k]));
-  std::vector<double> acc(16, 0.0);
+  cudaEvent_t ev[24];
+  for (int k = 0; k < 24; ++k) CUDA_CK(cudaEventCreate(&ev[k]));
+  std::vector<double> acc(24, 0.0);
   int nk = 0;
   for (int s = 0; s < steps; ++s) {
     nk = lp::launch_attempt(E.A, E.stream, ev);
@@ -1294,11 +1548,11 @@ lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* name
       acc[k] += t;
     }
   }
-  for (int k = 0; k < 16; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < 24; ++k) cudaEventDestroy(ev[k]);
   const int n = std::min(nk, (int)capacity);
   for (int k = 0; k < n; ++k) {
     ms[k] = acc[k] / std::max(steps, 1);
-    std::snprintf(names + 32 * k, 32, "%s", lp::attempt_kernel_name(k, E.A.any_pellet));
+    std::snprintf(names + 32 * k, 32, "%s", lp::attempt_kernel_name(k, E.A.any_pellet, E.A.any_bed));
   }
   *count = n;
   return pull_ctrl(E);

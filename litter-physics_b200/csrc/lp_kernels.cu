@@ -195,7 +195,7 @@ __device__ int block_argmax_ll(long long value, int index, long long* shv, int* 
 // ============================================================== begin
 // One thread per instance: decides whether the instance attempts a step and with which dt.
 __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, int n_inst,
-                        uint32_t* __restrict__ nw_count) {
+                        uint32_t* __restrict__ nw_count, BedPtrs bed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *nw_count = 0u;
   if (i >= n_inst) return;
@@ -234,6 +234,7 @@ __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__
                            c.pellet.vel[2] * c.pellet.vel[2]);
     if (ps > 0.0) limit = fmin(limit, D.cfl * dx / ps);
   }
+  if (D.bed_np >= 2) limit = fmin(limit, bed_limit(D, bed.state[c.bed_parity] + D.bed_off));
   // advance_while dt choice (solver.rs:424-441)
   const double remaining = c.target - c.time;
   const double scaled = c.dt_scale * limit;
@@ -946,8 +947,11 @@ __device__ inline double pellet_ke(const PelletState& P) {
          0.5 * (om[0] * P.L[0] + om[1] * P.L[1] + om[2] * P.L[2]);
 }
 // rigid.rs:279-334
+// ef / et: extra force and torque (pellet-bed sphere contacts) or null (the reference's single
+// pellet); impulse_out and work_out book the wall contacts only.
 __device__ inline void pellet_integrate(PelletState& P, double dt, const double* g, const double* ext, double k,
-                                        double e, double mu, double* impulse_out, double* work_out) {
+                                        double e, double mu, double* impulse_out, double* work_out,
+                                        const double* ef = nullptr, const double* et = nullptr) {
   double zeta;
   if (e <= 0.0) zeta = 1.0;
   else if (e >= 1.0) zeta = 0.0;
@@ -999,9 +1003,10 @@ __device__ inline void pellet_integrate(PelletState& P, double dt, const double*
   }
   for (int a = 0; a < 3; ++a) {
     impulse_out[a] = force[a] * dt;
-    P.vel[a] = P.vel[a] + (g[a] * dt + impulse_out[a] / P.mass);
+    const double applied = ef ? (force[a] + ef[a]) * dt : impulse_out[a];
+    P.vel[a] = P.vel[a] + (g[a] * dt + applied / P.mass);
   }
-  for (int a = 0; a < 3; ++a) P.L[a] += torque[a] * dt;
+  for (int a = 0; a < 3; ++a) P.L[a] += (et ? torque[a] + et[a] : torque[a]) * dt;
   for (int a = 0; a < 3; ++a) P.pos[a] += P.vel[a] * dt;
   double on[3];
   pellet_omega(P, on);
@@ -1154,6 +1159,397 @@ __global__ void k_couple(const InstDesc* __restrict__ desc, Control* __restrict_
     c.pw_work = work;
     c.pellet_fail = finite ? 0 : 1;
   }
+}
+
+// ============================================================== pellet bed (extension)
+// Many pellets of one multisphere geometry (rigid.rs:115-182 per pellet).  Per attempt:
+//   k_bed_bin    : pellets sorted by coarse cell (edge = two bounding radii), ties by index;
+//   k_bed_couple : one CTA per pellet applies couple_grid (rigid.rs:385-438) to the grid nodes it
+//                  owns: a node inside several proxies belongs to the pellet of smallest signed
+//                  distance (ties: lower index), so every node is constrained at most once;
+//   k_bed_step   : one thread per pellet: Hertz-Mindlin sphere contact with the other pellets
+//                  (start-of-step states, tangential spring history per sphere pair), then
+//                  apply_impulse and integrate (rigid.rs:251-334) with the contact force added.
+// The two sides of a contact evaluate mirrored expressions (d -> -d, v_rel -> -v_rel, the
+// contact point is the sphere midpoint), so their forces are exact negatives.
+__device__ inline double pellet_phi(const PelletState& P, const double ax[3], const double y[3], double nrm[3]) {
+  double best = 1e300;
+  nrm[0] = 0.0;
+  nrm[1] = 0.0;
+  nrm[2] = 1.0;
+  for (int s = 0; s < P.nsph; ++s) {
+    double d[3];
+    for (int a = 0; a < 3; ++a) d[a] = y[a] - (P.pos[a] + ax[a] * P.off[s]);
+    const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    const double phi = dist - P.radius;
+    if (phi < best) {
+      best = phi;
+      if (dist > 1e-12) {
+        nrm[0] = d[0] / dist;
+        nrm[1] = d[1] / dist;
+        nrm[2] = d[2] / dist;
+      } else {
+        nrm[0] = 0;
+        nrm[1] = 0;
+        nrm[2] = 1;
+      }
+    }
+  }
+  return best;
+}
+__device__ inline void bed_cell(const InstDesc& D, const double x[3], int cc[3]) {
+  for (int a = 0; a < 3; ++a) {
+    const double f = floor(x[a] / D.bed_h);
+    cc[a] = f < 0.0 ? 0 : (f > (double)(D.bed_nc[a] - 1) ? D.bed_nc[a] - 1 : (int)f);
+  }
+}
+__device__ inline long long bed_key_of(const InstDesc& D, const int cc[3]) {
+  return ((long long)cc[0] * D.bed_nc[1] + cc[1]) * D.bed_nc[2] + cc[2];
+}
+// [lo, hi) of sorted entries with this key
+__device__ inline void bed_range(const long long* __restrict__ keys, int np, long long key, int& lo, int& hi) {
+  int a = 0, b = np;
+  while (a < b) {
+    const int m = (a + b) >> 1;
+    if (keys[m] < key) a = m + 1;
+    else b = m;
+  }
+  lo = a;
+  b = np;
+  while (a < b) {
+    const int m = (a + b) >> 1;
+    if (keys[m] <= key) a = m + 1;
+    else b = m;
+  }
+  hi = a;
+}
+
+__global__ void __launch_bounds__(1024) k_bed_bin(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                                                  BedPtrs bed, long long* __restrict__ key, int* __restrict__ idx) {
+  __shared__ long long sk[BED_MAX];
+  const int inst = blockIdx.x;
+  const InstDesc& D = desc[inst];
+  const Control& c = ctrl[inst];
+  if (D.bed_np < 2 || !c.active) return;
+  const PelletState* S = bed.state[c.bed_parity] + D.bed_off;
+  const int np = D.bed_np;
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    int cc[3];
+    bed_cell(D, S[p].pos, cc);
+    sk[p] = bed_key_of(D, cc);
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    const long long kp = sk[p];
+    int rank = 0;
+    for (int q = 0; q < np; ++q) {
+      const long long kq = sk[q];
+      rank += (kq < kp) || (kq == kp && q < p);
+    }
+    key[D.bed_off + rank] = kp;
+    idx[D.bed_off + rank] = p;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_bed_couple(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
+                                                    const int* __restrict__ bed_inst, BedPtrs bed,
+                                                    const long long* __restrict__ key, const int* __restrict__ idx,
+                                                    BedStep* __restrict__ step, const uint32_t* __restrict__ blk_epoch,
+                                                    float4* __restrict__ vel) {
+  __shared__ double shd[128];
+  const int64_t gp = blockIdx.x;
+  const int inst = bed_inst[gp];
+  const Control& c = ctrl[inst];
+  const InstDesc& D = desc[inst];
+  if (!c.active) return;
+  const int p = (int)(gp - D.bed_off);
+  const PelletState* S = bed.state[c.bed_parity] + D.bed_off;
+  const long long* K = key + D.bed_off;
+  const int* I = idx + D.bed_off;
+  const PelletState& P = S[p];
+  double ax[3];
+  const double ex[3] = {1.0, 0.0, 0.0};
+  qrotv(P.q, ex, ax);
+  double hs = 0.0;
+  for (int s = 0; s < P.nsph; ++s) hs = fmax(hs, fabs(P.off[s]));
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    const double reach = fabs(ax[a]) * hs + P.radius;
+    lo[a] = P.pos[a] - reach;
+    hi[a] = P.pos[a] + reach;
+  }
+  int i0[3], n[3];
+  for (int a = 0; a < 3; ++a) {
+    int a0 = (int)floor(lo[a] / D.dx + 1.0) - 1, a1 = (int)ceil(hi[a] / D.dx + 1.0) + 1;
+    a0 = a0 < 0 ? 0 : a0;
+    a1 = a1 > D.nodes[a] - 1 ? D.nodes[a] - 1 : a1;
+    i0[a] = a0;
+    n[a] = a1 >= a0 ? a1 - a0 + 1 : 0;
+  }
+  double om[3];
+  pellet_omega(P, om);
+  double imp[3] = {0, 0, 0}, ang[3] = {0, 0, 0}, energy = 0.0;
+  const int64_t total = (int64_t)n[0] * n[1] * n[2];
+  for (int64_t l = threadIdx.x; l < total; l += blockDim.x) {
+    const int k = i0[2] + (int)(l % n[2]);
+    const int j = i0[1] + (int)((l / n[2]) % n[1]);
+    const int i = i0[0] + (int)(l / ((int64_t)n[2] * n[1]));
+    const int64_t blk = D.blk_off + ((int64_t)(i / NB) * D.nblk[1] + j / NB) * D.nblk[2] + k / NB;
+    if (blk_epoch[blk] != (uint32_t)c.epoch) continue;
+    const int64_t g = node_index(D, i, j, k);
+    const float4 nv = vel[g];
+    const double mass = nv.w;
+    if (!(mass > 0.0)) continue;
+    const double node[3] = {((double)i - 1.0) * D.dx, ((double)j - 1.0) * D.dx, ((double)k - 1.0) * D.dx};
+    bool outside = false;
+    for (int a = 0; a < 3; ++a)
+      if (node[a] < lo[a] || node[a] > hi[a]) outside = true;
+    if (outside) continue;
+    double normal[3];
+    const double best = pellet_phi(P, ax, node, normal);
+    if (best > 0.0) continue;
+    // ownership: the pellet of smallest signed distance, ties to the lower index
+    bool own = true;
+    int cc[3];
+    bed_cell(D, node, cc);
+    for (int di = -1; di <= 1 && own; ++di)
+      for (int dj = -1; dj <= 1 && own; ++dj)
+        for (int dk = -1; dk <= 1 && own; ++dk) {
+          const int c3[3] = {cc[0] + di, cc[1] + dj, cc[2] + dk};
+          if (c3[0] < 0 || c3[1] < 0 || c3[2] < 0 || c3[0] >= D.bed_nc[0] || c3[1] >= D.bed_nc[1] ||
+              c3[2] >= D.bed_nc[2])
+            continue;
+          int r0, r1;
+          bed_range(K, D.bed_np, bed_key_of(D, c3), r0, r1);
+          for (int r = r0; r < r1 && own; ++r) {
+            const int q = I[r];
+            if (q == p) continue;
+            const PelletState& Q = S[q];
+            const double dq[3] = {node[0] - Q.pos[0], node[1] - Q.pos[1], node[2] - Q.pos[2]};
+            if (dq[0] * dq[0] + dq[1] * dq[1] + dq[2] * dq[2] > D.bed_rb * D.bed_rb) continue;
+            double axq[3], nq[3];
+            qrotv(Q.q, ex, axq);
+            const double phq = pellet_phi(Q, axq, node, nq);
+            if (phq < best || (phq == best && q < p)) own = false;
+          }
+        }
+    if (!own) continue;
+    double lever[3], tmp[3], bv[3];
+    for (int a = 0; a < 3; ++a) lever[a] = node[a] - P.pos[a];
+    cross3(om, lever, tmp);
+    for (int a = 0; a < 3; ++a) bv[a] = P.vel[a] + tmp[a];
+    const double v[3] = {nv.x, nv.y, nv.z};
+    double rel[3];
+    for (int a = 0; a < 3; ++a) rel[a] = v[a] - bv[a];
+    const double nsp = rel[0] * normal[0] + rel[1] * normal[1] + rel[2] * normal[2];
+    if (nsp >= 0.0) continue;
+    double tg[3];
+    for (int a = 0; a < 3; ++a) tg[a] = rel[a] - normal[a] * nsp;
+    const double ts = sqrt(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]);
+    const double fr = D.friction * (-nsp);
+    double tn[3] = {0, 0, 0};
+    if (!(ts <= fr || ts < 1e-14))
+      for (int a = 0; a < 3; ++a) tn[a] = tg[a] * ((ts - fr) / ts);
+    double nvv[3], dp[3];
+    for (int a = 0; a < 3; ++a) {
+      nvv[a] = bv[a] + tn[a];
+      dp[a] = (nvv[a] - v[a]) * mass;
+    }
+    energy += 0.5 * mass * ((nvv[0] * nvv[0] + nvv[1] * nvv[1] + nvv[2] * nvv[2]) - (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    double lx[3];
+    cross3(lever, dp, lx);
+    for (int a = 0; a < 3; ++a) {
+      imp[a] -= dp[a];
+      ang[a] -= lx[a];
+    }
+    vel[g] = make_float4((float)nvv[0], (float)nvv[1], (float)nvv[2], nv.w);
+  }
+  for (int a = 0; a < 3; ++a) imp[a] = block_sum_d<128>(imp[a], shd);
+  for (int a = 0; a < 3; ++a) ang[a] = block_sum_d<128>(ang[a], shd);
+  energy = block_sum_d<128>(energy, shd);
+  if (threadIdx.x == 0) {
+    BedStep& st = step[gp];
+    for (int a = 0; a < 3; ++a) {
+      st.imp[a] = imp[a];
+      st.ang[a] = ang[a];
+    }
+    st.cgrid = energy;
+  }
+}
+
+constexpr int BED_CAND = 64;  // neighbour pellets examined per pellet
+
+__global__ void __launch_bounds__(64) k_bed_step(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
+                                                 const int* __restrict__ bed_inst, int64_t n_bed, BedPtrs bed,
+                                                 const long long* __restrict__ key, const int* __restrict__ idx,
+                                                 BedStep* __restrict__ step) {
+  const int64_t gp = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gp >= n_bed) return;
+  const int inst = bed_inst[gp];
+  const Control& c = ctrl[inst];
+  const InstDesc& D = desc[inst];
+  if (!c.active) return;
+  const int par = c.bed_parity;
+  const int p = (int)(gp - D.bed_off);
+  const PelletState* S = bed.state[par] + D.bed_off;
+  PelletState* T = bed.state[par ^ 1] + D.bed_off;
+  const HmContact* hold = bed.hist[par] + gp * HM_SLOTS;
+  const int nold = bed.hist_n[par][gp];
+  HmContact* hnew = bed.hist[par ^ 1] + gp * HM_SLOTS;
+  const long long* K = key + D.bed_off;
+  const int* I = idx + D.bed_off;
+  const PelletState& P = S[p];
+  const double dt = c.dt;
+  const double ex[3] = {1.0, 0.0, 0.0};
+  double axp[3], omp[3];
+  qrotv(P.q, ex, axp);
+  pellet_omega(P, omp);
+  BedStep& st = step[gp];
+  int fail = 0, overflow = 0, contacts = 0, nnew = 0;
+  // neighbours within two bounding radii, in increasing index
+  int cand[BED_CAND];
+  int nc = 0;
+  int cc[3];
+  bed_cell(D, P.pos, cc);
+  for (int di = -1; di <= 1; ++di)
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int dk = -1; dk <= 1; ++dk) {
+        const int c3[3] = {cc[0] + di, cc[1] + dj, cc[2] + dk};
+        if (c3[0] < 0 || c3[1] < 0 || c3[2] < 0 || c3[0] >= D.bed_nc[0] || c3[1] >= D.bed_nc[1] ||
+            c3[2] >= D.bed_nc[2])
+          continue;
+        int r0, r1;
+        bed_range(K, D.bed_np, bed_key_of(D, c3), r0, r1);
+        for (int r = r0; r < r1; ++r) {
+          const int q = I[r];
+          if (q == p) continue;
+          const double dq[3] = {S[q].pos[0] - P.pos[0], S[q].pos[1] - P.pos[1], S[q].pos[2] - P.pos[2]};
+          if (dq[0] * dq[0] + dq[1] * dq[1] + dq[2] * dq[2] > 4.0 * D.bed_rb * D.bed_rb) continue;
+          if (nc == BED_CAND) {
+            fail = 1;
+            continue;
+          }
+          int w = nc++;
+          while (w > 0 && cand[w - 1] > q) {
+            cand[w] = cand[w - 1];
+            --w;
+          }
+          cand[w] = q;
+        }
+      }
+  const double rs = 0.5 * P.radius;       // effective radius of two equal spheres
+  const double k56 = 1.8257418583505538;  // 2 sqrt(5/6)
+  double F[3] = {0, 0, 0}, Tq[3] = {0, 0, 0}, W = 0.0;
+  for (int ci = 0; ci < nc; ++ci) {
+    const int q = cand[ci];
+    const PelletState& Q = S[q];
+    double axq[3], omq[3];
+    qrotv(Q.q, ex, axq);
+    pellet_omega(Q, omq);
+    const double mstar = P.mass * Q.mass / (P.mass + Q.mass);
+    for (int a = 0; a < P.nsph; ++a) {
+      double ca[3];
+      for (int k = 0; k < 3; ++k) ca[k] = P.pos[k] + axp[k] * P.off[a];
+      for (int b = 0; b < Q.nsph; ++b) {
+        double cb[3], d[3];
+        for (int k = 0; k < 3; ++k) {
+          cb[k] = Q.pos[k] + axq[k] * Q.off[b];
+          d[k] = cb[k] - ca[k];
+        }
+        const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        const double delta = (P.radius + Q.radius) - dist;
+        if (!(delta > 0.0) || !(dist > 1e-12)) continue;
+        double nn[3], cp[3], lp[3], lq[3], t1[3], t2[3], vp[3], vrel[3];
+        for (int k = 0; k < 3; ++k) {
+          nn[k] = d[k] / dist;
+          cp[k] = 0.5 * (ca[k] + cb[k]);
+          lp[k] = cp[k] - P.pos[k];
+          lq[k] = cp[k] - Q.pos[k];
+        }
+        cross3(omp, lp, t1);
+        cross3(omq, lq, t2);
+        for (int k = 0; k < 3; ++k) {
+          vp[k] = P.vel[k] + t1[k];
+          vrel[k] = (Q.vel[k] + t2[k]) - vp[k];
+        }
+        const double vn = vrel[0] * nn[0] + vrel[1] * nn[1] + vrel[2] * nn[2];
+        double vt[3];
+        for (int k = 0; k < 3; ++k) vt[k] = vrel[k] - vn * nn[k];
+        const double sq = sqrt(rs * delta);
+        const double sn = 2.0 * D.hm_estar * sq, stf = 8.0 * D.hm_gstar * sq;
+        const double gn = -k56 * D.hm_beta * sqrt(sn * mstar), gt = -k56 * D.hm_beta * sqrt(stf * mstar);
+        const double fn = fmax((4.0 / 3.0) * D.hm_estar * sqrt(rs) * (delta * sqrt(delta)) - gn * vn, 0.0);
+        double xi[3] = {0.0, 0.0, 0.0};
+        for (int h = 0; h < nold; ++h)
+          if (hold[h].other == q && hold[h].a == a && hold[h].b == b) {
+            xi[0] = hold[h].xi[0];
+            xi[1] = hold[h].xi[1];
+            xi[2] = hold[h].xi[2];
+            break;
+          }
+        const double xn = xi[0] * nn[0] + xi[1] * nn[1] + xi[2] * nn[2];
+        double ft[3];
+        for (int k = 0; k < 3; ++k) {
+          xi[k] = (xi[k] - xn * nn[k]) + vt[k] * dt;
+          ft[k] = stf * xi[k] + gt * vt[k];
+        }
+        const double ftn = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+        const double lim = D.hm_mu * fn;
+        if (ftn > lim) {
+          const double sc = lim / ftn;
+          for (int k = 0; k < 3; ++k) {
+            ft[k] *= sc;
+            xi[k] = (ft[k] - gt * vt[k]) / stf;
+          }
+        }
+        double f[3], tq[3];
+        for (int k = 0; k < 3; ++k) f[k] = ft[k] - fn * nn[k];
+        cross3(lp, f, tq);
+        for (int k = 0; k < 3; ++k) {
+          F[k] += f[k];
+          Tq[k] += tq[k];
+        }
+        ++contacts;
+        if (nnew < HM_SLOTS) {
+          HmContact& hc = hnew[nnew++];
+          hc.other = q;
+          hc.a = a;
+          hc.b = b;
+          hc.pad = 0;
+          for (int k = 0; k < 3; ++k) hc.xi[k] = xi[k];
+        } else {
+          ++overflow;
+        }
+      }
+    }
+  }
+  bed.hist_n[par ^ 1][gp] = nnew;
+  // coupling impulse, then the rigid step with the contact force (rigid.rs:251-334)
+  PelletState Tp = P;
+  const double kb = pellet_ke(Tp);
+  for (int a = 0; a < 3; ++a) {
+    Tp.vel[a] += st.imp[a] / Tp.mass;
+    Tp.L[a] += st.ang[a];
+  }
+  const double pe = pellet_ke(Tp) - kb;
+  double wimp[3], work;
+  pellet_integrate(Tp, dt, D.gravity, D.extent, D.contact_k, D.contact_e, D.contact_mu, wimp, &work, F, Tq);
+  // contact work over the step at the step's mean linear and angular velocity: for the
+  // explicit update this is the kinetic-energy change the contact force causes
+  double ome[3];
+  pellet_omega(Tp, ome);
+  for (int k = 0; k < 3; ++k) W += (F[k] * (0.5 * (P.vel[k] + Tp.vel[k])) + Tq[k] * (0.5 * (omp[k] + ome[k]))) * dt;
+  bool finite = isfinite(pe) && isfinite(W);
+  for (int a = 0; a < 3; ++a) finite = finite && isfinite(Tp.pos[a]) && isfinite(Tp.vel[a]) && isfinite(Tp.L[a]);
+  for (int a = 0; a < 4; ++a) finite = finite && isfinite(Tp.q[a]);
+  T[p] = Tp;
+  st.cpellet = pe;
+  for (int a = 0; a < 3; ++a) st.wimp[a] = wimp[a];
+  st.wwork = work;
+  st.ppwork = W;
+  st.contacts = contacts;
+  st.overflow = overflow;
+  st.fail = (fail || !finite) ? 1 : 0;
 }
 
 // ============================================================== G2P + constitutive
@@ -1607,8 +2003,8 @@ __global__ void k_segments(const Control* __restrict__ ctrl, const SegDesc* __re
 }
 
 __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
-                      const SegPartial* __restrict__ seg) {
-  __shared__ double shd[(256 / 32) * 15 + 15];
+                      const SegPartial* __restrict__ seg, const BedStep* __restrict__ bed_step, BedPtrs bed) {
+  __shared__ double shd[(256 / 32) * 18 + 18];
   const int inst = blockIdx.x;
   Control& c = ctrl[inst];
   if (!c.active) return;
@@ -1626,6 +2022,28 @@ __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ c
     else v[13] = fmax(v[13], P.v[12]);
   }
   block_reduce_multi<256, 14>(v, (1u << 10) | (1u << 11) | (1u << 12) | (1u << 13), shd);
+  // pellet bed: imp3 ang3 cgrid cpellet wimp3 wwork ppwork contacts overflow mass | fail (max)
+  double bv[18] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (D.bed_np >= 2) {
+    const PelletState* S = bed.state[c.bed_parity] + D.bed_off;
+    for (int p = t; p < D.bed_np; p += 256) {
+      const BedStep& B = bed_step[D.bed_off + p];
+      for (int a = 0; a < 3; ++a) {
+        bv[a] += B.imp[a];
+        bv[3 + a] += B.ang[a];
+        bv[8 + a] += B.wimp[a];
+      }
+      bv[6] += B.cgrid;
+      bv[7] += B.cpellet;
+      bv[11] += B.wwork;
+      bv[12] += B.ppwork;
+      bv[13] += (double)B.contacts;
+      bv[14] += (double)B.overflow;
+      bv[15] += S[p].mass;
+      bv[16] = fmax(bv[16], (double)B.fail);
+    }
+    block_reduce_multi<256, 18>(bv, 1u << 16, shd);
+  }
   if (t != 0) return;
   const double wi[3] = {v[0], v[1], v[2]};
   const double proj = v[3], fric = v[4], trac = v[5], diss = v[6], bb = v[7];
@@ -1636,6 +2054,7 @@ __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ c
   if (!isfinite(trac) || !isfinite(c.ledger.trac + trac)) f = F_TRACTION_NONFINITE;
   else if (fail != F_OK) f = fail;
   else if (D.has_pellet && c.pellet_fail) f = F_PELLET_NONFINITE;
+  else if (D.bed_np >= 2 && bv[16] > 0.0) f = F_PELLET_NONFINITE;
   else if (pfail != F_OK) f = pfail;
   else if (md > 1.0f) f = F_DISPLACEMENT;
   else if (c.outflow > 0) f = F_OUTFLOW;
@@ -1676,6 +2095,21 @@ __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ c
     L.cgrid += c.c_grid_energy;
     L.cpellet += c.c_pellet_energy;
     c.pellet = c.pellet_trial;
+  }
+  if (D.bed_np >= 2) {
+    for (int a = 0; a < 3; ++a) {
+      L.gravity_impulse[a] += D.gravity[a] * (bv[15] * dt);
+      L.pellet_wall_impulse[a] += bv[8 + a];
+      L.coupling_impulse[a] += bv[a];
+      L.coupling_angular[a] += bv[3 + a];
+    }
+    L.pellet_work += bv[11];
+    L.cgrid += bv[6];
+    L.cpellet += bv[7];
+    c.bed_contact_work += bv[12];
+    c.bed_contacts = (int)bv[13];
+    c.bed_overflow += (uint64_t)bv[14];
+    c.bed_parity ^= 1;
   }
   c.max_speed = ms;
   c.bbound = bb;
@@ -1945,7 +2379,7 @@ static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1)
 int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
   int n = 0;
   if (ev) cudaEventRecord(ev[0], s);
-  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count);
+  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
@@ -1986,6 +2420,19 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
     ++n;
     if (ev) cudaEventRecord(ev[n], s);
   }
+  if (A.any_bed) {
+    k_bed_bin<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.bed, A.bed_key, A.bed_idx);
+    ++n;
+    if (ev) cudaEventRecord(ev[n], s);
+    k_bed_couple<<<(unsigned)A.n_bed, 128, 0, s>>>(A.desc, A.ctrl, A.bed_inst, A.bed, A.bed_key, A.bed_idx,
+                                                   A.bed_step, A.blk_epoch, A.vel);
+    ++n;
+    if (ev) cudaEventRecord(ev[n], s);
+    k_bed_step<<<grid_of(A.n_bed, 64), 64, 0, s>>>(A.desc, A.ctrl, A.bed_inst, A.n_bed, A.bed, A.bed_key,
+                                                   A.bed_idx, A.bed_step);
+    ++n;
+    if (ev) cudaEventRecord(ev[n], s);
+  }
   const bool warm_g2p = A.mlp != nullptr && A.warm;
   (warm_g2p ? k_g2p<true> : k_g2p<false>)<<<(unsigned)A.n_tiles, G2P_THREADS,
                                             warm_g2p ? g2p_smem_bytes<true>() : g2p_smem_bytes<false>(), s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
@@ -1996,7 +2443,7 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
   k_segments<<<(unsigned)A.n_seg, 256, 0, s>>>(A.ctrl, A.segs, A.gpart, A.tpart, A.seg);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_end<<<A.n_inst, 256, 0, s>>>(A.desc, A.ctrl, A.seg);
+  k_end<<<A.n_inst, 256, 0, s>>>(A.desc, A.ctrl, A.seg, A.bed_step, A.bed);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   g_launches += (uint64_t)n;
@@ -2011,7 +2458,7 @@ __global__ void k_grid_sums(const long long* __restrict__ acc, int64_t node_tota
 }
 
 int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
-  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count);
+  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.nw_list, A.nw_count);
   k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
@@ -2030,7 +2477,7 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
 }
 
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
-  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count);
+  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.nw_list, A.nw_count);
   k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
@@ -2049,12 +2496,13 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
 
 int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return launch_attempt(A, s, nullptr); }
 
-const char* attempt_kernel_name(int k, int any_pellet) {
+const char* attempt_kernel_name(int k, int any_pellet, int any_bed) {
   static const char* a[] = {"k_begin", "k_bin_count", "k_scan_chunks", "k_scan_instances", "k_scan_apply",
                             "k_bin_scatter", "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple",
-                            "k_g2p", "k_segments", "k_end"};
+                            "k_bed_bin", "k_bed_couple", "k_bed_step", "k_g2p", "k_segments", "k_end"};
   if (!any_pellet && k >= 10) ++k;
-  return k < 14 ? a[k] : "?";
+  if (!any_bed && k >= 11) k += 3;
+  return k < 17 ? a[k] : "?";
 }
 
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s) {

@@ -54,13 +54,21 @@ struct DeviceArrays {
   unsigned long long* log_n = nullptr;
   long long log_cap = 0;
   int p2g_variant = 0;  // autotuner choice (reserved)
+  // pellet bed (instances with InstDesc::bed_np >= 2)
+  int any_bed = 0;
+  int64_t n_bed = 0;                                 // pellets of all instances
+  int* bed_inst = nullptr;                           // pellet -> instance
+  BedPtrs bed = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+  BedStep* bed_step = nullptr;                       // [pellet]
+  long long* bed_key = nullptr;                      // coarse-cell keys sorted per instance
+  int* bed_idx = nullptr;                            // instance-local pellet index per sorted key
 };
 
 // One substep attempt for every active instance; returns the number of kernels launched.
 int launch_attempt(const DeviceArrays& A, cudaStream_t s);
 // same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 14 events)
 int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev);
-const char* attempt_kernel_name(int k, int any_pellet);
+const char* attempt_kernel_name(int k, int any_pellet, int any_bed);
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s);
 // begin + binning + P2G only (conservation probe), then exact node sums into out[4] (int64)
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s);

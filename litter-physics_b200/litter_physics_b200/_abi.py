@@ -73,6 +73,15 @@ class FixtureSpec(C.Structure):
         ("_pad2", C.c_int32),
         ("yield_min", C.c_double),
         ("yield_max", C.c_double),
+        ("bed_count", C.c_int32),
+        ("_pad3", C.c_int32),
+        ("bed_seed", C.c_uint64),
+        ("bed_lo", C.c_double * 3),
+        ("bed_hi", C.c_double * 3),
+        ("hm_young", C.c_double),
+        ("hm_poisson", C.c_double),
+        ("hm_friction", C.c_double),
+        ("hm_restitution", C.c_double),
     ]
 
 

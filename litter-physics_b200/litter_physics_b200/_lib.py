@@ -89,6 +89,8 @@ def lib():
         "lp_sim_import_particles": ([P, C.POINTER(_abi.Particles)], I32),
         "lp_sim_get_pellet": ([P, C.POINTER(_abi.Pellet), C.POINTER(I32)], I32),
         "lp_sim_set_pellet": ([P, C.POINTER(_abi.Pellet)], I32),
+        "lp_sim_get_pellets": ([P, C.POINTER(_abi.Pellet), I32, C.POINTER(I32)], I32),
+        "lp_sim_set_pellets": ([P, C.POINTER(_abi.Pellet), I32], I32),
         "lp_sim_observables": ([P, C.c_char_p, D, I32, C.POINTER(I32)], I32),
         "lp_sim_energies": ([P, D], I32),
         "lp_sim_set_warm_start": ([P, F, I32, I32], I32),

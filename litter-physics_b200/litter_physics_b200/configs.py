@@ -110,3 +110,47 @@ def config3(count: int = 256, seed: int = 2024) -> list[_abi.FixtureSpec]:
 
     rng = random.Random(seed)
     return [sweep_instance(k, rng) for k in range(count)]
+
+
+def pellet_bed(cells: int = 128, layer_cells: int = 8, pellets: int = 512, seed: int = 7, dt: float = 5e-5,
+               domain_m: float = 1.0, young: float = 5e6, region=None, gravity: float = -9.81) -> _abi.FixtureSpec:
+    """Config 4 (extension): an HB paste layer with config-0 material under a bed of rigid pine pellets.
+
+    Paste: a full-width layer `layer_cells` cells thick at 8 particles per cell (128 x 128 x 8
+    cells = 1,048,576 particles at the defaults), sticky floor and slip walls.  Pellets: radius
+    3 mm, length 20 mm, density 650 kg/m^3 -- 6 spheres by the reference's count rule
+    (rigid.rs:147-160), where the config text says 5 -- with random orientations and
+    non-overlapping centres drawn from `seed` in the slab 1-6 cm above the layer.  Pellet-pellet
+    contact is Hertz-Mindlin with friction 0.5, restitution 0.3, Poisson 0.3 and a softened
+    Young's modulus (5 MPa: the contact time stays above ten steps of 5e-5 s); pellet-wall
+    contact is the reference's spring-dashpot.  The config's 3 mm radius is below the
+    reference's 1.5 dx resolution rule for the coupled patch (dx = 7.8 mm), which the bed does
+    not apply.
+    """
+    dx = domain_m / cells
+    e, nu = young_poisson(2e4, 1e5)
+    top = layer_cells * dx
+    s = base_spec(fixture=_abi.LP_SLUMP, grid_spacing=dx, domain=[domain_m] * 3,
+                  initial_size=[domain_m, domain_m, top], initial_velocity=[0, 0, 0], seed=seed,
+                  wall_friction=0.0, max_dt=dt, min_dt=1e-12, contact_stiffness=1000.0,
+                  contact_restitution=0.2, contact_friction=0.4, max_particles=2**31 - 1, max_nodes=2**40)
+    s.gravity[:] = [0.0, 0.0, gravity]
+    s.material = material_paste_shear(1200.0, e, nu, 50.0, 5.0, 0.5)
+    _sticky_floor_slip_walls(s)
+    s.newton_tolerance = 1e-10
+    s.has_pellet = 1
+    s.pellet_radius, s.pellet_length, s.pellet_density = 0.003, 0.020, 650.0
+    s.bed_count = pellets
+    s.bed_seed = seed
+    lo, hi = region if region is not None else ([0.02, 0.02, top + 0.01], [domain_m - 0.02, domain_m - 0.02,
+                                                                              top + 0.06])
+    s.bed_lo[:] = list(lo)
+    s.bed_hi[:] = list(hi)
+    s.hm_young, s.hm_poisson, s.hm_friction, s.hm_restitution = young, 0.3, 0.5, 0.3
+    return s
+
+
+def config4() -> _abi.FixtureSpec:
+    """Coupled pellet bed: 128^3 grid, ~1M paste particles, 512 pellets, seed 7, dt 5e-5 s."""
+    return pellet_bed()
+

@@ -205,7 +205,8 @@ def base_spec(**kw: Any) -> _abi.FixtureSpec:
     s.max_particles = MAX_PARTICLES
     s.max_nodes = MAX_NODES
     for key, value in kw.items():
-        if key in ("domain", "initial_size", "initial_velocity", "gravity", "face_friction", "face_sticky"):
+        if key in ("domain", "initial_size", "initial_velocity", "gravity", "face_friction", "face_sticky", "bed_lo",
+                   "bed_hi"):
             getattr(s, key)[:] = list(value)
         else:
             setattr(s, key, value)

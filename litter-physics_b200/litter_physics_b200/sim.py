@@ -133,6 +133,19 @@ class Simulation:
     def set_pellet(self, p: _abi.Pellet) -> None:
         check(lib().lp_sim_set_pellet(self._h, C.byref(p)))
 
+    def pellets(self) -> list:
+        """Pellet bed (extension): committed state of every pellet, in index order."""
+        n = C.c_int32()
+        check(lib().lp_sim_get_pellets(self._h, None, 0, C.byref(n)))
+        arr = (_abi.Pellet * max(n.value, 1))()
+        check(lib().lp_sim_get_pellets(self._h, arr, n.value, C.byref(n)))
+        return list(arr)[: n.value]
+
+    def set_pellets(self, pellets: list) -> None:
+        """Pellet bed: replace every pellet's pose and momenta (contact histories restart)."""
+        arr = (_abi.Pellet * len(pellets))(*pellets)
+        check(lib().lp_sim_set_pellets(self._h, arr, len(pellets)))
+
     def observables(self) -> dict:
         cap = 128
         names = C.create_string_buffer(64 * cap)

@@ -741,8 +741,9 @@ struct Pellet {
     return finite3(position) && finite3(velocity) && finite3(L) && std::isfinite(q.i) && std::isfinite(q.j) &&
            std::isfinite(q.k) && std::isfinite(q.w);
   }
-  // rigid.rs:279-334
-  WallContact integrate(double dt, const V3& g, const V3& ext, const Contact& c) {
+  // rigid.rs:279-334; ef / et: pellet-bed sphere-contact force and torque (extension)
+  WallContact integrate(double dt, const V3& g, const V3& ext, const Contact& c, const V3* ef = nullptr,
+                        const V3* et = nullptr) {
     double damping = c.damping(mass);
     V3 force = zero3(), torque = zero3();
     WallContact led{zero3(), 0.0, 0};
@@ -778,8 +779,9 @@ struct Pellet {
     }
     V3 impulse = mul(force, dt);
     led.impulse = impulse;
-    velocity = add(velocity, add(mul(g, dt), divs(impulse, mass)));
-    L = add(L, mul(torque, dt));
+    V3 applied = ef ? mul(add(force, *ef), dt) : impulse;
+    velocity = add(velocity, add(mul(g, dt), divs(applied, mass)));
+    L = add(L, mul(et ? add(torque, *et) : torque, dt));
     position = add(position, mul(velocity, dt));
     V3 on = angular_velocity();
     Quat inc = q_from_scaled_axis(mul(on, dt));
@@ -877,12 +879,26 @@ struct NodeTrial {
 
 enum StepFail { SF_OK = 0, SF_CONST, SF_GRID, SF_DISP, SF_PELLET, SF_TRACTION };
 
+// pellet bed (extension): tangential spring of one sphere pair
+struct HmEntry {
+  int other, a, b;
+  V3 xi;
+};
+constexpr int HM_SLOTS = 24, BED_CAND = 64;
+
 struct Simulation {
   Material mat;
   Particles P;
   Grid grid;
   bool has_pellet = false;
   Pellet pellet;
+  // pellet bed (extension)
+  std::vector<Pellet> bed;
+  std::vector<std::vector<HmEntry>> hist;
+  double hm_estar = 0, hm_gstar = 0, hm_mu = 0, hm_beta = 0, bed_rb = 0;
+  double bed_contact_work = 0.0;
+  int bed_contacts = 0;
+  uint64_t bed_overflow = 0;
   Config cfg;
   Ledger ledger;
   double time = 0.0;
@@ -905,6 +921,7 @@ struct Simulation {
   V3 total_momentum() const {
     V3 m = P.linear_momentum();
     if (has_pellet) m = add(m, mul(pellet.velocity, pellet.mass));
+    for (const Pellet& b : bed) m = add(m, mul(b.velocity, b.mass));
     return m;
   }
   // solver.rs:1013-1020
@@ -920,6 +937,7 @@ struct Simulation {
     double e = 0.0;
     for (size_t p = 0; p < P.size(); ++p) e += -P.m[p] * dot(g, P.x[p]);
     if (has_pellet) e -= pellet.mass * dot(g, pellet.position);
+    for (const Pellet& b : bed) e -= b.mass * dot(g, b.position);
     return e;
   }
   double elastic_energy() const {
@@ -946,9 +964,15 @@ struct Simulation {
     }
     return s;
   }
-  double kinetic_energy() const { return P.kinetic_energy() + (has_pellet ? pellet.kinetic_energy() : 0.0); }
+  double kinetic_energy() const {
+    double k = P.kinetic_energy() + (has_pellet ? pellet.kinetic_energy() : 0.0);
+    for (const Pellet& b : bed) k += b.kinetic_energy();
+    return k;
+  }
   double mechanical_energy() const { return kinetic_energy() + potential_energy() + elastic_energy(); }
-  double energy_residual() const { return mechanical_energy() - ledger.initial_mech - ledger.ledgered(); }
+  double energy_residual() const {
+    return mechanical_energy() - ledger.initial_mech - (ledger.ledgered() + bed_contact_work);
+  }
 
   // solver.rs:477-498
   double stability_limit() const {
@@ -963,6 +987,15 @@ struct Simulation {
       limit = std::fmin(limit, cfg.contact.stable_dt(pellet.mass));
       double ps = norm(pellet.velocity);
       if (ps > 0.0) limit = std::fmin(limit, cfg.cfl * dx / ps);
+    }
+    // pellet bed: per pellet as above, plus 0.2 sqrt(m*/k_c) for the Hertz stiffness at an
+    // overlap of 5 % of the radius, k_c = 2 E* sqrt(R* 0.05 r)
+    for (const Pellet& b : bed) {
+      limit = std::fmin(limit, cfg.contact.stable_dt(b.mass));
+      double ps = norm(b.velocity);
+      if (ps > 0.0) limit = std::fmin(limit, cfg.cfl * dx / ps);
+      double kc = 2.0 * hm_estar * std::sqrt(0.5 * b.radius * 0.05 * b.radius);
+      limit = std::fmin(limit, 0.2 * std::sqrt(0.5 * b.mass / kc));
     }
     return limit;
   }
@@ -1145,6 +1178,153 @@ struct Simulation {
     return true;
   }
 
+  // Pellet bed coupling: couple_grid (rigid.rs:385-438) over all pellets, each node constrained
+  // by the pellet of smallest signed distance (ties: lower index); per-pellet sums in node order.
+  std::vector<Coupling> couple_bed(const std::vector<Pellet>& pels, double friction) {
+    const Layout& L = grid.layout;
+    const size_t na = grid.active.size();
+    const size_t np = pels.size();
+    std::vector<V3> lo(np), hi(np);
+    for (size_t q = 0; q < np; ++q) pels[q].bounding_box(lo[q], hi[q]);
+    struct Upd {
+      int owner;
+      V3 nv, dp, lever;
+      double energy;
+    };
+    std::vector<Upd> upd(na);
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < (int64_t)na; ++s) {
+      int64_t index = grid.active[s];
+      Upd u;
+      u.owner = -1;
+      double mass = grid.mass[index];
+      if (mass > 0.0) {
+        int64_t i, j, k;
+        L.coords(index, i, j, k);
+        V3 node = L.node_position(i, j, k);
+        int best_q = -1;
+        double best = 0.0;
+        V3 best_n = zero3();
+        for (size_t q = 0; q < np; ++q) {
+          bool outside = false;
+          for (int a = 0; a < 3; ++a)
+            if (node[a] < lo[q][a] || node[a] > hi[q][a]) outside = true;
+          if (outside) continue;
+          V3 n;
+          double phi = pels[q].signed_distance(node, n);
+          if (phi > 0.0) continue;
+          if (best_q < 0 || phi < best) {
+            best_q = (int)q;
+            best = phi;
+            best_n = n;
+          }
+        }
+        if (best_q >= 0) {
+          const Pellet& pel = pels[best_q];
+          V3 vel = grid.momentum[index];
+          V3 bv = pel.point_velocity(node);
+          V3 rel = sub(vel, bv);
+          double nsp = dot(rel, best_n);
+          if (nsp < 0.0) {
+            V3 tang = sub(rel, mul(best_n, nsp));
+            double ts = norm(tang);
+            double fr = friction * (-nsp);
+            V3 tn = (ts <= fr || ts < 1e-14) ? zero3() : mul(tang, (ts - fr) / ts);
+            V3 nv = add(bv, tn);
+            V3 dp = mul(sub(nv, vel), mass);
+            double energy = 0.5 * mass * (norm2(nv) - norm2(vel));
+            u = Upd{best_q, nv, dp, sub(node, pel.position), energy};
+          }
+        }
+      }
+      upd[s] = u;
+    }
+    std::vector<Coupling> r(np, Coupling{zero3(), zero3(), 0.0, 0});
+    for (size_t s = 0; s < na; ++s) {
+      if (upd[s].owner < 0) continue;
+      grid.momentum[grid.active[s]] = upd[s].nv;
+      Coupling& c = r[upd[s].owner];
+      c.impulse = sub(c.impulse, upd[s].dp);
+      c.angular = sub(c.angular, cross(upd[s].lever, upd[s].dp));
+      c.grid_energy += upd[s].energy;
+      c.constrained += 1;
+    }
+    return r;
+  }
+
+  // Hertz-Mindlin sphere contact on pellet p from the start-of-step states of all pellets:
+  // force and torque on p and its new tangential-spring list.  Returns false when more than
+  // BED_CAND pellets lie within two bounding radii.
+  bool bed_contact(size_t p, double dt, V3& F, V3& T, int& contacts, int& overflow,
+                   std::vector<HmEntry>& next) const {
+    const Pellet& P = bed[p];
+    F = zero3();
+    T = zero3();
+    contacts = 0;
+    overflow = 0;
+    next.clear();
+    const V3 axp = P.axis(), omp = P.angular_velocity();
+    const double rs = 0.5 * P.radius, k56 = 1.8257418583505538;
+    int cand = 0;
+    for (size_t q = 0; q < bed.size(); ++q) {
+      if (q == p) continue;
+      const Pellet& Q = bed[q];
+      V3 dq = sub(Q.position, P.position);
+      if (norm2(dq) > 4.0 * bed_rb * bed_rb) continue;
+      if (++cand > BED_CAND) return false;
+      const V3 axq = Q.axis(), omq = Q.angular_velocity();
+      const double mstar = P.mass * Q.mass / (P.mass + Q.mass);
+      for (size_t a = 0; a < P.offsets.size(); ++a) {
+        V3 ca = add(P.position, mul(axp, P.offsets[a]));
+        for (size_t b = 0; b < Q.offsets.size(); ++b) {
+          V3 cb = add(Q.position, mul(axq, Q.offsets[b]));
+          V3 d = sub(cb, ca);
+          double dist = norm(d);
+          double delta = (P.radius + Q.radius) - dist;
+          if (!(delta > 0.0) || !(dist > 1e-12)) continue;
+          V3 nn = divs(d, dist);
+          V3 cp = mul(add(ca, cb), 0.5);
+          V3 lp = sub(cp, P.position), lq = sub(cp, Q.position);
+          V3 vp = add(P.velocity, cross(omp, lp));
+          V3 vrel = sub(add(Q.velocity, cross(omq, lq)), vp);
+          double vn = dot(vrel, nn);
+          V3 vt = sub(vrel, mul(nn, vn));
+          double sq = std::sqrt(rs * delta);
+          double sn = 2.0 * hm_estar * sq, stf = 8.0 * hm_gstar * sq;
+          double gn = -k56 * hm_beta * std::sqrt(sn * mstar), gt = -k56 * hm_beta * std::sqrt(stf * mstar);
+          double fn = std::fmax((4.0 / 3.0) * hm_estar * std::sqrt(rs) * (delta * std::sqrt(delta)) - gn * vn, 0.0);
+          V3 xi = zero3();
+          for (const HmEntry& h : hist[p])
+            if (h.other == (int)q && h.a == (int)a && h.b == (int)b) {
+              xi = h.xi;
+              break;
+            }
+          double xn = dot(xi, nn);
+          V3 ft;
+          for (int k = 0; k < 3; ++k) {
+            xi[k] = (xi[k] - xn * nn[k]) + vt[k] * dt;
+            ft[k] = stf * xi[k] + gt * vt[k];
+          }
+          double ftn = norm(ft), lim = hm_mu * fn;
+          if (ftn > lim) {
+            double sc = lim / ftn;
+            for (int k = 0; k < 3; ++k) {
+              ft[k] *= sc;
+              xi[k] = (ft[k] - gt * vt[k]) / stf;
+            }
+          }
+          V3 f = sub(ft, mul(nn, fn));
+          F = add(F, f);
+          T = add(T, cross(lp, f));
+          ++contacts;
+          if ((int)next.size() < HM_SLOTS) next.push_back(HmEntry{(int)q, (int)a, (int)b, xi});
+          else ++overflow;
+        }
+      }
+    }
+    return true;
+  }
+
   // rigid.rs:385-438
   Coupling couple_grid(const Pellet& pel, double friction) {
     V3 lo, hi;
@@ -1305,6 +1485,43 @@ struct Simulation {
         return SF_PELLET;
       }
     }
+    // pellet bed (extension): coupling, sphere contacts from the start-of-step states, rigid step
+    std::vector<Pellet> btrial = bed;
+    std::vector<std::vector<HmEntry>> htrial(bed.size());
+    std::vector<Coupling> bcoup;
+    std::vector<double> bpe(bed.size(), 0.0), bwork(bed.size(), 0.0);
+    std::vector<WallContact> bwall(bed.size(), WallContact{zero3(), 0.0, 0});
+    int bcontacts = 0;
+    uint64_t boverflow = 0;
+    if (!bed.empty()) {
+      bcoup = couple_bed(bed, cfg.friction);
+      V3 ext = grid.layout.extents();
+      for (size_t p = 0; p < bed.size(); ++p) {
+        V3 F, T;
+        int nc, ov;
+        if (!bed_contact(p, dt, F, T, nc, ov, htrial[p])) {
+          last_failure = "pellet state became non-finite";
+          return SF_PELLET;
+        }
+        bcontacts += nc;
+        boverflow += (uint64_t)ov;
+        Pellet& b = btrial[p];
+        double kb = b.kinetic_energy();
+        b.apply_impulse(bcoup[p].impulse, bcoup[p].angular);
+        bpe[p] = b.kinetic_energy() - kb;
+        bwall[p] = b.integrate(dt, cfg.gravity, ext, cfg.contact, &F, &T);
+        // contact work at the step's mean linear and angular velocity
+        const V3 om0 = bed[p].angular_velocity(), om1 = b.angular_velocity();
+        double W = 0.0;
+        for (int k = 0; k < 3; ++k)
+          W += (F[k] * (0.5 * (bed[p].velocity[k] + b.velocity[k])) + T[k] * (0.5 * (om0[k] + om1[k]))) * dt;
+        bwork[p] = W;
+        if (!b.finite() || !std::isfinite(bpe[p]) || !std::isfinite(W)) {
+          last_failure = "pellet state became non-finite";
+          return SF_PELLET;
+        }
+      }
+    }
     const size_t np = P.size();
     std::vector<ParticleTrial> tr(np);
     std::vector<int> err(np, CE_OK);
@@ -1355,6 +1572,24 @@ struct Simulation {
       ledger.cgrid += coup.grid_energy;
       ledger.cpellet += pellet_energy;
       pellet = ptrial;
+    }
+    if (!bed.empty()) {
+      double bm = 0.0;
+      for (size_t p = 0; p < bed.size(); ++p) {
+        bm += btrial[p].mass;
+        ledger.pellet_wall_impulse = add(ledger.pellet_wall_impulse, bwall[p].impulse);
+        ledger.pellet_work += bwall[p].work;
+        ledger.coupling_impulse = add(ledger.coupling_impulse, bcoup[p].impulse);
+        ledger.coupling_angular = add(ledger.coupling_angular, bcoup[p].angular);
+        ledger.cgrid += bcoup[p].grid_energy;
+        ledger.cpellet += bpe[p];
+        bed_contact_work += bwork[p];
+      }
+      ledger.gravity_impulse = add(ledger.gravity_impulse, mul(cfg.gravity, bm * dt));
+      bed_contacts = bcontacts;
+      bed_overflow += boverflow;
+      bed = btrial;
+      hist = htrial;
     }
     return SF_OK;
   }
@@ -1470,10 +1705,101 @@ bool validate_spec(const lp_fixture_spec& s, std::string& err) {
       break;
     }
     default:
-      if (s.has_pellet) {
+      if (s.has_pellet && !(s.fixture == LP_SLUMP && s.bed_count >= 2)) {
         err = "fixture does not accept boxes; only `coupled_patch` uses pellet geometry";
         return false;
       }
+  }
+  if (s.bed_count >= 2) {
+    if (s.fixture != LP_SLUMP || !s.has_pellet || s.bed_count > 4096) {
+      err = "a pellet bed needs the slump fixture, a pellet geometry and at most 4096 pellets";
+      return false;
+    }
+    if (!(s.hm_young > 0.0) || !(s.hm_poisson >= 0.0 && s.hm_poisson < 0.5) || !(s.hm_friction >= 0.0) ||
+        !(s.hm_restitution > 0.0 && s.hm_restitution <= 1.0)) {
+      err = "invalid Hertz-Mindlin parameters (young > 0, 0 <= poisson < 0.5, friction >= 0, 0 < restitution <= 1)";
+      return false;
+    }
+  }
+  return true;
+}
+
+// Damping parameter of the Hertz-Mindlin normal force, calibrated so that a head-on impact
+// rebounds with restitution e: in scaled units the overlap obeys
+// x'' = -max(x^1.5 + c x^0.25 x', 0), c = -sqrt(5) beta, x(0) = 0, x'(0) = 1, independent of
+// speed, masses and moduli; e = -x' at separation (RK4, step 2e-4), bisection on beta.
+static double hm_restitution_of(double beta) {
+  const double c = -std::sqrt(5.0) * beta, h = 2e-4;
+  auto acc = [c](double x, double v) {
+    if (x <= 0.0) return 0.0;
+    const double f = std::pow(x, 1.5) + c * std::pow(x, 0.25) * v;
+    return f > 0.0 ? -f : 0.0;
+  };
+  double x = 0.0, v = 1.0;
+  for (int n = 1; n <= 1000000; ++n) {
+    const double k1x = v, k1v = acc(x, v);
+    const double k2x = v + 0.5 * h * k1v, k2v = acc(x + 0.5 * h * k1x, v + 0.5 * h * k1v);
+    const double k3x = v + 0.5 * h * k2v, k3v = acc(x + 0.5 * h * k2x, v + 0.5 * h * k2v);
+    const double k4x = v + h * k3v, k4v = acc(x + h * k3x, v + h * k3v);
+    x += h / 6.0 * (k1x + 2.0 * k2x + 2.0 * k3x + k4x);
+    v += h / 6.0 * (k1v + 2.0 * k2v + 2.0 * k3v + k4v);
+    if (x <= 0.0) break;
+  }
+  return -v;
+}
+static double hm_beta_for(double e) {
+  if (e >= 1.0) return 0.0;
+  double lo = -20.0, hi = 0.0;
+  for (int it = 0; it < 60; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (hm_restitution_of(mid) < e) lo = mid;
+    else hi = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// Pellet bed placement (extension): per pellet, centre (x y z uniforms in [bed_lo, bed_hi]) then
+// orientation (Shoemake: three uniforms) from one SplitMix64 stream seeded with bed_seed,
+// redrawn until every sphere is a radius inside the walls and 2.02 radii from placed spheres.
+bool make_bed(const lp_fixture_spec& s, const V3& extent, std::vector<Pellet>& bed, std::string& err) {
+  SplitMix64 rng{s.bed_seed};
+  Pellet proto;
+  if (!make_pellet(s.pellet_radius, s.pellet_length, s.pellet_density, zero3(), proto, err)) return false;
+  const double r = proto.radius;
+  std::vector<V3> centres;
+  bed.clear();
+  for (int p = 0; p < s.bed_count; ++p) {
+    bool placed = false;
+    for (int attempt = 0; attempt < 10000 && !placed; ++attempt) {
+      Pellet P = proto;
+      for (int a = 0; a < 3; ++a) P.position[a] = s.bed_lo[a] + (s.bed_hi[a] - s.bed_lo[a]) * rng.next_unit();
+      double u1 = rng.next_unit(), u2 = rng.next_unit(), u3 = rng.next_unit();
+      double s1 = std::sqrt(1.0 - u1), s2 = std::sqrt(u1), t1 = 2.0 * kPi * u2, t2 = 2.0 * kPi * u3;
+      P.q = Quat{s1 * std::sin(t1), s1 * std::cos(t1), s2 * std::sin(t2), s2 * std::cos(t2)};
+      M3 R = qmatrix(P.q);
+      std::vector<V3> mine;
+      bool ok = true;
+      for (size_t k = 0; k < P.offsets.size() && ok; ++k) {
+        V3 c;
+        for (int a = 0; a < 3; ++a) {
+          c[a] = P.position[a] + R.a[a][0] * P.offsets[k];
+          if (c[a] < r || c[a] > extent[a] - r) ok = false;
+        }
+        for (const V3& o : centres) {
+          double dx = c[0] - o[0], dy = c[1] - o[1], dz = c[2] - o[2];
+          if (dx * dx + dy * dy + dz * dz < (2.02 * r) * (2.02 * r)) ok = false;
+        }
+        mine.push_back(c);
+      }
+      if (!ok) continue;
+      centres.insert(centres.end(), mine.begin(), mine.end());
+      bed.push_back(P);
+      placed = true;
+    }
+    if (!placed) {
+      err = "pellet bed: pellet " + std::to_string(p) + " does not fit in the region without overlap after 10000 draws";
+      return false;
+    }
   }
   return true;
 }
@@ -1534,6 +1860,20 @@ bool build(const lp_fixture_spec& s, Simulation& sim, std::string& err) {
   sim.mat = mat;
   sim.grid.init(L);
   sim.has_pellet = false;
+  sim.bed.clear();
+  sim.hist.clear();
+  if (s.bed_count >= 2) {
+    if (!make_bed(s, L.extents(), sim.bed, err)) return false;
+    sim.hist.assign(sim.bed.size(), std::vector<HmEntry>());
+    const double nu = s.hm_poisson, E = s.hm_young, G = E / (2.0 * (1.0 + nu));
+    sim.hm_estar = E / (2.0 * (1.0 - nu * nu));
+    sim.hm_gstar = G / (2.0 * (2.0 - nu));
+    sim.hm_mu = s.hm_friction;
+    sim.hm_beta = hm_beta_for(s.hm_restitution);
+    double hs = 0.0;
+    for (double o : sim.bed[0].offsets) hs = std::fmax(hs, std::fabs(o));
+    sim.bed_rb = hs + sim.bed[0].radius;
+  }
   if (s.fixture == LP_COUPLED_PATCH && s.has_pellet) {
     V3 center = v3(0.5 * s.domain[0], 0.5 * s.domain[1], s.initial_size[2] + 2.0 * s.grid_spacing + s.pellet_radius);
     if (!make_pellet(s.pellet_radius, s.pellet_length, s.pellet_density, center, sim.pellet, err)) return false;
@@ -1555,6 +1895,7 @@ bool build(const lp_fixture_spec& s, Simulation& sim, std::string& err) {
   // Simulation::new (solver.rs:357-394)
   V3 mom = P.linear_momentum();
   if (sim.has_pellet) mom = add(mom, mul(sim.pellet.velocity, sim.pellet.mass));
+  for (const Pellet& b : sim.bed) mom = add(mom, mul(b.velocity, b.mass));
   sim.ledger = Ledger();
   sim.ledger.initial_mass = P.total_mass();
   sim.ledger.initial_momentum = mom;
@@ -1675,6 +2016,28 @@ std::map<std::string, double> observables(const Fixture& fx, const Simulation& s
     out["pellet_wall_work_j"] = l.pellet_work;
     out["coupling_grid_energy_j"] = l.cgrid;
     out["coupling_pellet_energy_j"] = l.cpellet;
+  }
+  if (!sim.bed.empty()) {
+    double zs = 0.0, zmin = 1e300, vmax = 0.0, ke = 0.0;
+    for (const Pellet& b : sim.bed) {
+      zs += b.position[2];
+      zmin = std::fmin(zmin, b.position[2]);
+      vmax = std::fmax(vmax, norm(b.velocity));
+      ke += b.kinetic_energy();
+    }
+    const Ledger& l = sim.ledger;
+    out["pellet_count"] = (double)sim.bed.size();
+    out["pellet_mean_z_m"] = zs / (double)sim.bed.size();
+    out["pellet_min_z_m"] = zmin;
+    out["pellet_max_speed_m_s"] = vmax;
+    out["pellet_kinetic_energy_j"] = ke;
+    out["pellet_contact_work_j"] = sim.bed_contact_work;
+    out["pellet_contacts"] = (double)sim.bed_contacts;
+    out["pellet_history_overflow"] = (double)sim.bed_overflow;
+    out["pellet_wall_work_j"] = l.pellet_work;
+    out["coupling_grid_energy_j"] = l.cgrid;
+    out["coupling_pellet_energy_j"] = l.cpellet;
+    out["coupling_impulse_z_kg_m_s"] = l.coupling_impulse[2];
   }
   return out;
 }
@@ -1875,6 +2238,42 @@ void ora_sim_set_pellet(ora_sim* s, const lp_pellet* o) {
   p.L = v3_in(o->angular_momentum);
   p.offsets.assign(o->sphere_offsets, o->sphere_offsets + o->sphere_count);
   s->sim.has_pellet = true;
+}
+
+int32_t ora_sim_get_pellets(ora_sim* s, lp_pellet* out, int32_t cap) {
+  const std::vector<Pellet>& B = s->sim.bed;
+  for (int32_t i = 0; i < std::min<int32_t>(cap, (int32_t)B.size()); ++i) {
+    const Pellet& p = B[i];
+    lp_pellet* o = out + i;
+    std::memset(o, 0, sizeof(*o));
+    o->radius = p.radius;
+    o->length = p.length;
+    o->mass = p.mass;
+    v3_out(p.inertia, o->inertia_body);
+    v3_out(p.position, o->position);
+    o->orientation[0] = p.q.i;
+    o->orientation[1] = p.q.j;
+    o->orientation[2] = p.q.k;
+    o->orientation[3] = p.q.w;
+    v3_out(p.velocity, o->velocity);
+    v3_out(p.L, o->angular_momentum);
+    o->sphere_count = (int32_t)p.offsets.size();
+    for (size_t k = 0; k < p.offsets.size(); ++k) o->sphere_offsets[k] = p.offsets[k];
+  }
+  return (int32_t)B.size();
+}
+
+int32_t ora_sim_set_pellets(ora_sim* s, const lp_pellet* in, int32_t count) {
+  std::vector<Pellet>& B = s->sim.bed;
+  if (count != (int32_t)B.size()) return LP_INVALID;
+  for (int32_t i = 0; i < count; ++i) {
+    B[i].position = v3_in(in[i].position);
+    B[i].velocity = v3_in(in[i].velocity);
+    B[i].L = v3_in(in[i].angular_momentum);
+    B[i].q = Quat{in[i].orientation[0], in[i].orientation[1], in[i].orientation[2], in[i].orientation[3]};
+  }
+  s->sim.hist.assign(B.size(), std::vector<HmEntry>());
+  return LP_OK;
 }
 
 int32_t ora_sim_observables(ora_sim* s, char* names, double* values, int32_t capacity) {

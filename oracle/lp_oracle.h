@@ -37,6 +37,9 @@ void ora_sim_export_particles(ora_sim* s, lp_particles* out);
 int32_t ora_sim_import_particles(ora_sim* s, const lp_particles* in);
 int32_t ora_sim_get_pellet(ora_sim* s, lp_pellet* out);
 void ora_sim_set_pellet(ora_sim* s, const lp_pellet* in);
+/* pellet bed (extension): committed pellets in index order (returns the count); replace poses */
+int32_t ora_sim_get_pellets(ora_sim* s, lp_pellet* out, int32_t cap);
+int32_t ora_sim_set_pellets(ora_sim* s, const lp_pellet* in, int32_t count);
 int32_t ora_sim_observables(ora_sim* s, char* names, double* values, int32_t capacity);
 void ora_sim_energies(ora_sim* s, double out[9]);
 /* Threads used by the node/particle-parallel loops (0 = OpenMP default). */

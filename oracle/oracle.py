@@ -57,6 +57,10 @@ def lib():
         L.ora_sim_get_pellet.argtypes = [P, C.POINTER(_abi.Pellet)]
         L.ora_sim_get_pellet.restype = C.c_int32
         L.ora_sim_set_pellet.argtypes = [P, C.POINTER(_abi.Pellet)]
+        L.ora_sim_get_pellets.argtypes = [P, C.POINTER(_abi.Pellet), C.c_int32]
+        L.ora_sim_get_pellets.restype = C.c_int32
+        L.ora_sim_set_pellets.argtypes = [P, C.POINTER(_abi.Pellet), C.c_int32]
+        L.ora_sim_set_pellets.restype = C.c_int32
         L.ora_sim_observables.argtypes = [P, C.c_char_p, C.POINTER(C.c_double), C.c_int32]
         L.ora_sim_observables.restype = C.c_int32
         L.ora_sim_energies.argtypes = [P, C.POINTER(C.c_double)]
@@ -169,6 +173,18 @@ class OracleSim:
 
     def set_pellet(self, p: _abi.Pellet) -> None:
         lib().ora_sim_set_pellet(self._h, C.byref(p))
+
+    def pellets(self) -> list:
+        """Pellet bed (extension): committed pellets in index order."""
+        n = lib().ora_sim_get_pellets(self._h, None, 0)
+        arr = (_abi.Pellet * max(n, 1))()
+        lib().ora_sim_get_pellets(self._h, arr, n)
+        return list(arr)[:n]
+
+    def set_pellets(self, pellets: list) -> None:
+        arr = (_abi.Pellet * len(pellets))(*pellets)
+        if lib().ora_sim_set_pellets(self._h, arr, len(pellets)) != 0:
+            raise ValueError("pellet count differs from the bed's")
 
     def observables(self) -> dict:
         cap = 128
