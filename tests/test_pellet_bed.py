@@ -162,8 +162,9 @@ def test_gpu_collision_matches_oracle(built):
 @pytest.mark.gpu
 def test_gpu_bed_falling_on_paste_matches_oracle(built):
     """24 pellets dropped onto a 2-cell paste layer for 0.04 s (800 substeps): pellet and paste
-    positions within 1e-5 of the domain, and the coupling and contact energies within 1e-3 of
-    the pellets' kinetic-energy scale (FP32 paste state on the device against FP64)."""
+    positions within 1e-5 of the domain, the coupling and contact energies within 1e-3 of the
+    pellets' kinetic-energy scale (FP32 paste state on the device against FP64), and momentum
+    closed to 1e-6 of the gravity impulse."""
     import oracle
 
     from litter_physics_b200.sim import Simulation
@@ -194,4 +195,6 @@ def test_gpu_bed_falling_on_paste_matches_oracle(built):
     assert not bad, bad
     assert ro["pellet_contact_work_j"] < 0.0  # contacts happened
     assert go["step_count"] == ro["step_count"] and go["rejected_steps"] == ro["rejected_steps"]
-    assert abs(go["momentum_residual_kg_m_s"]) <= 1e-12
+    # momentum closes to FP32 rounding of the particle velocities (1e-6 of the gravity impulse)
+    impulse = (sum(p.mass for p in gpu.pellets()) + float(pg["mass"].sum())) * 9.81 * t
+    assert abs(go["momentum_residual_kg_m_s"]) <= 1e-6 * impulse
