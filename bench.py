@@ -212,6 +212,33 @@ def batch_measurement(args, stream, torch) -> dict:
             "ms_per_step": ms / args.steps, "autotune": choice, "setup_s": round(setup, 2)}
 
 
+def bed_measurement(args, stream, torch) -> dict:
+    """Config 4 (extension): 1M-particle paste layer under 512 Hertz-Mindlin pellets.
+
+    The bed is first advanced 2000 substeps (0.1 s) so that pellets land on the layer and touch
+    each other; then W warm-up and K timed substeps, CUDA events on the simulation's stream."""
+    from litter_physics_b200 import configs
+    from litter_physics_b200.sim import Simulation
+
+    spec = configs.config4()
+    sim = Simulation(spec)
+    sim.set_stream(stream.cuda_stream)
+    n = sim.particle_count()
+    sim.run_substeps(2000)
+    sim.run_substeps(args.warmup)
+    sim.sync()
+    ms, accepted = time_steps(sim, args.steps, stream, torch)
+    obs = sim.observables()
+    kt = sim.kernel_times(args.kernel_steps)
+    out = {"workload": "config 4: 128^3 grid, 128x128x8-cell paste layer (config-0 material), 512 pellets "
+                       "(r 3 mm, L 20 mm, rho 650, seed 7), Hertz-Mindlin e 0.3 mu 0.5, dt 5e-5 s, after 0.1 s",
+           "particles": n, "pellets": int(obs["pellet_count"]), "value": n * accepted / (ms / 1e3), "unit": UNIT,
+           "ms_per_step": ms / args.steps, "pellet_contacts": int(obs["pellet_contacts"]),
+           "kernel_ms": {k: round(v, 5) for k, v in kt.items()}}
+    sim.close()
+    return out
+
+
 def reference_arm(args, ws, rank):
     if rank != 0:
         return
@@ -351,6 +378,7 @@ def ours(args, ws, rank, local):
             dist.destroy_process_group()
         return
     batch_info = None if args.no_batch else batch_measurement(args, stream, torch)
+    bed_info = None if args.no_batch else bed_measurement(args, stream, torch)
     peaks = measured_peaks()
     g2p_ms = ktimes.get("k_g2p", float("nan"))
     achieved = G2P_BYTES_PER_PARTICLE * n / (g2p_ms / 1e3) / 1e9
@@ -407,6 +435,7 @@ def ours(args, ws, rank, local):
                 "path": "lp_sim_import_particles -> lp_sim_advance -> lp_sim_export_particles (host FP64 buffers)",
                 "steps": steps_done},
         "batch_config3": batch_info,
+        "pellet_bed_config4": bed_info,
         "gpu_launches": int(launches["warm"]),
         "clocks": clocks,
     }
@@ -424,7 +453,7 @@ def main():
     ap.add_argument("--workload", default="config2", choices=["config2", "config0", "small"])
     ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start (profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and CPU legs (profiling)")
-    ap.add_argument("--no-batch", action="store_true", help="skip the config-3 batched measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the config-3 and config-4 measurements")
     ap.add_argument("--develop", type=int, default=150)
     ap.add_argument("--graph", type=int, default=0)
     ap.add_argument("--log-steps", type=int, default=300)

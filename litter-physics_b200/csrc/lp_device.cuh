@@ -155,6 +155,7 @@ struct Control {
   int bed_parity, bed_contacts;
   double bed_contact_work;
   uint64_t bed_overflow;
+  double bed_limit;  // step limit of the committed pellets (set on commit and by the host)
 };
 
 // pellet bed: tangential spring of one sphere pair (pellet-local sphere a, other pellet's b)
@@ -172,7 +173,7 @@ struct BedPtrs {
 };
 // pellet bed: per-pellet results of one attempt
 struct BedStep {
-  double imp[3], ang[3], cgrid, cpellet, wimp[3], wwork, ppwork;
+  double imp[3], ang[3], cgrid, cpellet, wimp[3], wwork, ppwork, limit;
   int contacts, overflow, fail, pad;
 };
 
@@ -206,16 +207,16 @@ struct ParticlePartial {
 // Pellet-bed step limit: per pellet the reference's wall-contact and pellet-CFL limits
 // (solver.rs:477-498), plus 0.2 sqrt(m*/k_c) for the Hertz stiffness at an overlap of 5 % of
 // the sphere radius, k_c = 2 E* sqrt(R* 0.05 r).
+__host__ __device__ inline double pellet_bed_limit(const InstDesc& D, const PelletState& P) {
+  double limit = 0.2 * sqrt(P.mass / D.contact_k);
+  const double ps = sqrt(P.vel[0] * P.vel[0] + P.vel[1] * P.vel[1] + P.vel[2] * P.vel[2]);
+  if (ps > 0.0) limit = fmin(limit, D.cfl * D.dx / ps);
+  const double kc = 2.0 * D.hm_estar * sqrt(0.5 * P.radius * 0.05 * P.radius);
+  return fmin(limit, 0.2 * sqrt(0.5 * P.mass / kc));
+}
 __host__ __device__ inline double bed_limit(const InstDesc& D, const PelletState* S) {
   double limit = 1e300;
-  for (int p = 0; p < D.bed_np; ++p) {
-    const PelletState& P = S[p];
-    limit = fmin(limit, 0.2 * sqrt(P.mass / D.contact_k));
-    const double ps = sqrt(P.vel[0] * P.vel[0] + P.vel[1] * P.vel[1] + P.vel[2] * P.vel[2]);
-    if (ps > 0.0) limit = fmin(limit, D.cfl * D.dx / ps);
-    const double kc = 2.0 * D.hm_estar * sqrt(0.5 * P.radius * 0.05 * P.radius);
-    limit = fmin(limit, 0.2 * sqrt(0.5 * P.mass / kc));
-  }
+  for (int p = 0; p < D.bed_np; ++p) limit = fmin(limit, pellet_bed_limit(D, S[p]));
   return limit;
 }
 

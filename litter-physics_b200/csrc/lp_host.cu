@@ -825,6 +825,7 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
     c.count = (int64_t)H[i].P.size();
     c.status = lp::S_RUNNING;
     if (H[i].has_pellet) c.pellet = H[i].pellet;
+    if (E.desc[i].bed_np >= 2) c.bed_limit = lp::bed_limit(E.desc[i], H[i].bed.data());
   }
   lp_status s2 = push_ctrl(E);
   if (s2 != LP_OK) return s2;
@@ -1390,7 +1391,8 @@ lp_status lp_sim_set_pellets(lp_sim* sim, const lp_pellet* in, int32_t count) {
   CUDA_CK(cudaMemcpy(E.A.bed.state[par] + D.bed_off, B.data(), sizeof(lp::PelletState) * B.size(),
                      cudaMemcpyHostToDevice));
   CUDA_CK(cudaMemset(E.A.bed.hist_n[par] + D.bed_off, 0, sizeof(int) * B.size()));
-  return LP_OK;
+  E.ctrl_h[0].bed_limit = lp::bed_limit(D, B.data());
+  return push_ctrl(E);
 }
 lp_status lp_sim_get_pellet(lp_sim* sim, lp_pellet* out, int32_t* has) {
   lp_status st = pull_ctrl(sim->E);

@@ -234,7 +234,7 @@ __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__
                            c.pellet.vel[2] * c.pellet.vel[2]);
     if (ps > 0.0) limit = fmin(limit, D.cfl * dx / ps);
   }
-  if (D.bed_np >= 2) limit = fmin(limit, bed_limit(D, bed.state[c.bed_parity] + D.bed_off));
+  if (D.bed_np >= 2) limit = fmin(limit, c.bed_limit);
   // advance_while dt choice (solver.rs:424-441)
   const double remaining = c.target - c.time;
   const double scaled = c.dt_scale * limit;
@@ -1549,6 +1549,7 @@ __global__ void __launch_bounds__(64) k_bed_step(const InstDesc* __restrict__ de
   st.ppwork = W;
   st.contacts = contacts;
   st.overflow = overflow;
+  st.limit = pellet_bed_limit(D, Tp);
   st.fail = (fail || !finite) ? 1 : 0;
 }
 
@@ -2023,7 +2024,7 @@ __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ c
   }
   block_reduce_multi<256, 14>(v, (1u << 10) | (1u << 11) | (1u << 12) | (1u << 13), shd);
   // pellet bed: imp3 ang3 cgrid cpellet wimp3 wwork ppwork contacts overflow mass | fail (max)
-  double bv[18] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double bv[18] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, -1e300};
   if (D.bed_np >= 2) {
     const PelletState* S = bed.state[c.bed_parity] + D.bed_off;
     for (int p = t; p < D.bed_np; p += 256) {
@@ -2041,8 +2042,9 @@ __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ c
       bv[14] += (double)B.overflow;
       bv[15] += S[p].mass;
       bv[16] = fmax(bv[16], (double)B.fail);
+      bv[17] = fmax(bv[17], -B.limit);  // smallest step limit of the trial pellets
     }
-    block_reduce_multi<256, 18>(bv, 1u << 16, shd);
+    block_reduce_multi<256, 18>(bv, (1u << 16) | (1u << 17), shd);
   }
   if (t != 0) return;
   const double wi[3] = {v[0], v[1], v[2]};
@@ -2109,6 +2111,7 @@ __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ c
     c.bed_contact_work += bv[12];
     c.bed_contacts = (int)bv[13];
     c.bed_overflow += (uint64_t)bv[14];
+    c.bed_limit = -bv[17];
     c.bed_parity ^= 1;
   }
   c.max_speed = ms;
