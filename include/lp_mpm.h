@@ -166,6 +166,26 @@ typedef struct lp_pellet {
   double sphere_offsets[64];
 } lp_pellet;
 
+/* Energy audit of one trial step (audit.rs:254-271), all energies in J.  before / after:
+ * EnergyState (translation, APIC affine norm h^2/8 sum m |C|^2, elastic, potential, pellet).
+ * stages: grid_transport, grid_after_stress, grid_after_traction, grid_after_gravity,
+ * grid_after_walls, grid_after_coupling, pellet_after_coupling, plastic_dissipation.
+ * increments: ledger differences of plastic dissipation, wall friction, wall normal projection,
+ * wall normal traction, coupling grid, coupling pellet, pellet wall work.
+ * terms: p2g transfer loss, g2p transfer loss, stress/storage/plastic mismatch, uncoupled
+ * gravity/potential mismatch (NaN when coupled), coupled grid-gravity plus potential change
+ * (NaN when uncoupled), pellet integrator change, traction change, walls change, coupling
+ * change, augmented energy change, telescoping sum, telescoping error. */
+typedef struct lp_energy_audit {
+  double time, dt;
+  double before[5], after[5];
+  double stages[8];
+  double increments[7];
+  double terms[12];
+  int32_t coupled;
+  int32_t _pad;
+} lp_energy_audit;
+
 typedef struct lp_sim lp_sim;
 typedef struct lp_batch lp_batch;
 

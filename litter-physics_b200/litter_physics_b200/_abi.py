@@ -152,6 +152,49 @@ class Particles(C.Structure):
     ]
 
 
+class EnergyAudit(C.Structure):
+    """Mirror of `lp_energy_audit` (audit.rs:254-271 EnergyAudit)."""
+
+    _fields_ = [
+        ("time", C.c_double),
+        ("dt", C.c_double),
+        ("before", C.c_double * 5),
+        ("after", C.c_double * 5),
+        ("stages", C.c_double * 8),
+        ("increments", C.c_double * 7),
+        ("terms", C.c_double * 12),
+        ("coupled", C.c_int32),
+        ("_pad", C.c_int32),
+    ]
+
+    STATE = ("translation", "affine", "elastic", "potential", "pellet")
+    STAGES = ("grid_transport", "grid_after_stress", "grid_after_traction", "grid_after_gravity",
+              "grid_after_walls", "grid_after_coupling", "pellet_after_coupling", "plastic_dissipation")
+    INCREMENTS = ("plastic_dissipation", "wall_friction_dissipation", "wall_normal_projection_energy",
+                  "wall_normal_traction_energy", "coupling_grid_energy", "coupling_pellet_energy", "pellet_wall_work")
+    TERMS = ("p2g_transfer_loss", "g2p_transfer_loss", "stress_storage_plastic_mismatch",
+             "uncoupled_gravity_potential_mismatch", "coupled_grid_gravity_total_potential_change",
+             "pellet_integrator_combined_change", "traction_change", "walls_change", "coupling_change",
+             "augmented_energy_change", "telescoping_sum", "telescoping_error")
+
+    def as_dict(self) -> dict:
+        """The reference's `EnergyAudit` JSON shape; the optional gravity term of the other
+        scope is None, like the reference's `Option`."""
+        terms = {}
+        for k, name in enumerate(self.TERMS):
+            v = float(self.terms[k])
+            optional = (k == 3 and self.coupled) or (k == 4 and not self.coupled)
+            terms[name] = None if optional else v
+        return {
+            "time": self.time, "dt": self.dt,
+            "before": dict(zip(self.STATE, map(float, self.before))),
+            "after": dict(zip(self.STATE, map(float, self.after))),
+            "stages": dict(zip(self.STAGES, map(float, self.stages))),
+            "increments": dict(zip(self.INCREMENTS, map(float, self.increments))),
+            "terms": terms,
+        }
+
+
 class Pellet(C.Structure):
     """Mirror of `Pellet` (core/src/mpm/rigid.rs:30-49)."""
 

@@ -879,6 +879,12 @@ struct NodeTrial {
 
 enum StepFail { SF_OK = 0, SF_CONST, SF_GRID, SF_DISP, SF_PELLET, SF_TRACTION };
 
+// audit.rs:72-90: kinetic snapshots of one trial
+struct AuditStages {
+  double transport = 0, stress = 0, traction = 0, gravity = 0, walls = 0, coupling = 0, pellet_after = 0,
+         plastic = 0;
+};
+
 // pellet bed (extension): tangential spring of one sphere pair
 struct HmEntry {
   int other, a, b;
@@ -906,6 +912,63 @@ struct Simulation {
   double dt_scale = 1.0, min_dt_used = std::numeric_limits<double>::infinity(), max_dt_used = 0.0;
   uint64_t newton_iterations = 0, yielded = 0;
   std::string last_failure;
+  AuditStages* audit = nullptr;  // set while an audit trial records its stages
+
+  // audit.rs:360-378 grid_kinetic: active nodes, momentum (or velocity after the walls) plus kick
+  double grid_kinetic(bool velocities, const V3& kick) const {
+    double e = 0.0;
+    for (int64_t i : grid.active) {
+      const double m = grid.mass[i];
+      if (!(m > 0.0)) continue;
+      V3 v = velocities ? grid.momentum[i] : divs(grid.momentum[i], m);
+      e += 0.5 * m * norm2(add(v, kick));
+    }
+    return e;
+  }
+  // audit.rs:381-398: independent APIC-only deposition on a shadow grid
+  double transport_energy() const {
+    Grid shadow;
+    shadow.init(grid.layout);
+    const Layout& L = grid.layout;
+    for (size_t p = 0; p < P.size(); ++p) {
+      Stencil s;
+      if (!stencil_of(L, P.x[p], s)) return std::numeric_limits<double>::quiet_NaN();
+      const double mass = P.m[p];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+          for (int c = 0; c < 3; ++c) {
+            const double w = s.weight(a, b, c);
+            V3 vel = add(P.v[p], mvec(P.C[p], s.distance(a, b, c)));
+            int64_t index = L.index(s.base[0] + a, s.base[1] + b, s.base[2] + c);
+            shadow.deposit(index, w * mass, mul(vel, w * mass));
+          }
+    }
+    double e = 0.0;
+    for (int64_t i : shadow.active) {
+      const double m = shadow.mass[i];
+      if (!(m > 0.0)) continue;
+      e += 0.5 * m * norm2(divs(shadow.momentum[i], m));
+    }
+    return e;
+  }
+  // audit.rs:38-53 EnergyState::measure: translation, affine norm, elastic, potential, pellet
+  void energy_state(double out[5]) const {
+    const double h = grid.layout.spacing;
+    double aff = 0.0;
+    for (size_t p = 0; p < P.size(); ++p) {
+      double n2 = 0.0;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) n2 += P.C[p].a[i][j] * P.C[p].a[i][j];
+      aff += P.m[p] * n2;
+    }
+    out[0] = P.kinetic_energy();
+    out[1] = h * h / 8.0 * aff;
+    out[2] = elastic_energy();
+    out[3] = potential_energy();
+    double pk = has_pellet ? pellet.kinetic_energy() : 0.0;
+    for (const Pellet& b : bed) pk += b.kinetic_energy();
+    out[4] = pk;
+  }
 
   double ys_of(size_t p) const { return P.ys[p]; }
 
@@ -1444,9 +1507,14 @@ struct Simulation {
   int try_step(double dt) {
     sweep_outflow();
     deposit_particles(dt);
+    if (audit) audit->stress = grid_kinetic(false, zero3());
     V3 timp;
     double tenergy;
     wall_traction(dt, timp, tenergy);
+    if (audit) {
+      audit->traction = grid_kinetic(false, zero3());
+      audit->gravity = grid_kinetic(false, mul(cfg.gravity, dt));
+    }
     if (!std::isfinite(tenergy) || !std::isfinite(ledger.trac + tenergy)) {
       last_failure = "wall traction kinetic-energy jump became non-finite";
       return SF_TRACTION;
@@ -1469,6 +1537,7 @@ struct Simulation {
       wproj += nt[s].proj;
       wfric += nt[s].fric;
     }
+    if (audit) audit->walls = grid_kinetic(true, zero3());
     Pellet ptrial = pellet;
     Coupling coup{zero3(), zero3(), 0.0, 0};
     double pellet_energy = 0.0;
@@ -1478,6 +1547,7 @@ struct Simulation {
       double kb = ptrial.kinetic_energy();
       ptrial.apply_impulse(coup.impulse, coup.angular);
       pellet_energy = ptrial.kinetic_energy() - kb;
+      if (audit) audit->pellet_after = ptrial.kinetic_energy();
       V3 ext = grid.layout.extents();
       pwall = ptrial.integrate(dt, cfg.gravity, ext, cfg.contact);
       if (!ptrial.finite() || !std::isfinite(pellet_energy)) {
@@ -1509,6 +1579,7 @@ struct Simulation {
         double kb = b.kinetic_energy();
         b.apply_impulse(bcoup[p].impulse, bcoup[p].angular);
         bpe[p] = b.kinetic_energy() - kb;
+        if (audit) audit->pellet_after += b.kinetic_energy();
         bwall[p] = b.integrate(dt, cfg.gravity, ext, cfg.contact, &F, &T);
         // contact work at the step's mean linear and angular velocity
         const V3 om0 = bed[p].angular_velocity(), om1 = b.angular_velocity();
@@ -1522,6 +1593,7 @@ struct Simulation {
         }
       }
     }
+    if (audit) audit->coupling = grid_kinetic(true, zero3());
     const size_t np = P.size();
     std::vector<ParticleTrial> tr(np);
     std::vector<int> err(np, CE_OK);
@@ -1532,6 +1604,11 @@ struct Simulation {
         last_failure = std::string("constitutive update failed: ") + const_err_name(err[p]);
         return SF_CONST;
       }
+    if (audit) {
+      double d = 0.0;
+      for (size_t p = 0; p < np; ++p) d += tr[p].diss;
+      audit->plastic = d;
+    }
     double max_cells = 0.0;
     for (size_t p = 0; p < np; ++p) max_cells = std::fmax(max_cells, tr[p].disp);
     if (max_cells > 1.0) {
@@ -1903,6 +1980,88 @@ bool build(const lp_fixture_spec& s, Simulation& sim, std::string& err) {
   return true;
 }
 
+// audit.rs:214-243 EnergyTerms::measure
+void audit_terms(lp_energy_audit& a) {
+  const double* b = a.before;
+  const double* f = a.after;
+  const double* s = a.stages;
+  const double p2g = b[0] + b[1] - s[0];
+  const double g2p = s[5] - f[0] - f[1];
+  const double stress = s[1] - s[0] + f[2] - b[2] + s[7];
+  const double gravity = s[3] - s[2] + f[3] - b[3];
+  const double integrator = f[4] - s[6];
+  const double traction = s[2] - s[1];
+  const double walls = s[4] - s[3];
+  const double coupling = s[5] - s[4] + s[6] - b[4];
+  const double change = (f[0] + f[1] + f[2] + f[3] + f[4]) - (b[0] + b[1] + b[2] + b[3] + b[4]);
+  const double sum = -p2g - g2p + stress - s[7] + gravity + integrator + traction + walls + coupling;
+  const double nan = std::numeric_limits<double>::quiet_NaN();
+  const double t[12] = {p2g,      g2p,       stress, a.coupled ? nan : gravity, a.coupled ? gravity : nan,
+                        integrator, traction, walls,  coupling, change, sum, change - sum};
+  for (int k = 0; k < 12; ++k) a.terms[k] = t[k];
+}
+
+// audit.rs:284-353 Simulation::audit_step on a copy of the simulation
+bool audit_step(const Simulation& sim, double dt, lp_energy_audit& out, std::string& err) {
+  std::memset(&out, 0, sizeof(out));
+  const Config& c = sim.cfg;
+  const double stability = sim.stability_limit();
+  if (!finite3(c.gravity) || !std::isfinite(c.cfl) || c.cfl <= 0.0 || !std::isfinite(c.friction) || c.friction < 0.0 ||
+      !std::isfinite(c.min_dt) || c.min_dt <= 0.0 || !std::isfinite(c.max_dt) || c.max_dt < c.min_dt ||
+      !std::isfinite(stability) || stability <= 0.0) {
+    err = "invalid solver state: invalid audit step configuration or stability limit";
+    return false;
+  }
+  const double limit = std::fmin(sim.dt_scale * stability, c.max_dt);
+  if (!std::isfinite(dt) || dt <= 0.0 || dt < c.min_dt || !std::isfinite(limit) || dt > limit) {
+    char buf[200];
+    std::snprintf(buf, sizeof(buf), "invalid solver state: audit `dt`='%.17g' outside finite accepted range ending at '%.17g'",
+                  dt, limit);
+    err = buf;
+    return false;
+  }
+  out.time = sim.time;
+  out.dt = dt;
+  out.coupled = (sim.has_pellet || !sim.bed.empty()) ? 1 : 0;
+  sim.energy_state(out.before);
+  for (double v : out.before)
+    if (!std::isfinite(v)) {
+      err = "invalid solver state: nonfinite initial audit energy";
+      return false;
+    }
+  AuditStages st;
+  st.transport = sim.transport_energy();
+  Simulation trial = sim;
+  trial.audit = &st;
+  const int f = trial.try_step(dt);
+  trial.audit = nullptr;
+  if (f != SF_OK) {
+    err = "invalid solver state: audit trial rejected: " + trial.last_failure;
+    return false;
+  }
+  trial.energy_state(out.after);
+  const double stg[8] = {st.transport, st.stress, st.traction, st.gravity, st.walls, st.coupling, st.pellet_after,
+                         st.plastic};
+  for (int k = 0; k < 8; ++k) out.stages[k] = stg[k];
+  const Ledger& l0 = sim.ledger;
+  const Ledger& l1 = trial.ledger;
+  const double inc[7] = {l1.plastic - l0.plastic, l1.fric - l0.fric, l1.proj - l0.proj, l1.trac - l0.trac,
+                         l1.cgrid - l0.cgrid, l1.cpellet - l0.cpellet, l1.pellet_work - l0.pellet_work};
+  for (int k = 0; k < 7; ++k) out.increments[k] = inc[k];
+  audit_terms(out);
+  bool finite = true;
+  for (double v : out.after) finite = finite && std::isfinite(v);
+  for (double v : out.stages) finite = finite && std::isfinite(v);
+  for (double v : out.increments) finite = finite && std::isfinite(v);
+  for (int k = 0; k < 12; ++k)
+    if (!((k == 3 && out.coupled) || (k == 4 && !out.coupled))) finite = finite && std::isfinite(out.terms[k]);
+  if (!finite) {
+    err = "invalid solver state: audit energy became nonfinite";
+    return false;
+  }
+  return true;
+}
+
 // fixtures.rs:354-364
 double hydrostatic_reference(const Simulation& sim, double depth) {
   double g = norm(sim.cfg.gravity);
@@ -2103,6 +2262,15 @@ int32_t ora_sim_try_step(ora_sim* s, double dt, int32_t* accepted, char* reason,
 
 double ora_sim_stability_limit(ora_sim* s) { return s->sim.stability_limit(); }
 
+int32_t ora_sim_audit_step(ora_sim* s, double dt, lp_energy_audit* out, char* err, int32_t errlen) {
+  std::string e;
+  if (!audit_step(s->sim, dt, *out, e)) {
+    set_err(err, errlen, e);
+    return LP_INVALID;
+  }
+  return LP_OK;
+}
+
 void ora_sim_counters(ora_sim* s, lp_counters* out) {
   const Simulation& m = s->sim;
   out->time = m.time;
@@ -2115,6 +2283,19 @@ void ora_sim_counters(ora_sim* s, lp_counters* out) {
   out->particle_count = m.P.size();
   out->newton_iterations = m.newton_iterations;
   out->yielded_particles = m.yielded;
+}
+
+int32_t ora_sim_set_counters(ora_sim* s, const lp_counters* in) {
+  Simulation& m = s->sim;
+  if (!(in->dt_scale > 0.0 && in->dt_scale <= 1.0) || !std::isfinite(in->time) || in->time < 0.0) return LP_INVALID;
+  m.time = in->time;
+  m.step_count = in->step_count;
+  m.limited_steps = in->limited_steps;
+  m.rejected_steps = in->rejected_steps;
+  m.dt_scale = in->dt_scale;
+  m.min_dt_used = in->min_dt_used;
+  m.max_dt_used = in->max_dt_used;
+  return LP_OK;
 }
 
 static void v3_out(const V3& v, double* d) {

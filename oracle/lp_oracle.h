@@ -29,7 +29,11 @@ int32_t ora_sim_advance(ora_sim* s, double target, int64_t max_accepted, int32_t
                         int32_t errlen);
 int32_t ora_sim_try_step(ora_sim* s, double dt, int32_t* accepted, char* reason, int32_t len);
 double ora_sim_stability_limit(ora_sim* s);
+/* Energy audit of one trial step on a copy (audit.rs:284-353); the simulation is unchanged. */
+int32_t ora_sim_audit_step(ora_sim* s, double dt, lp_energy_audit* out, char* err, int32_t errlen);
 void ora_sim_counters(ora_sim* s, lp_counters* out);
+/* counters as lp_sim_set_counters takes them (time, step counts, dt_scale in (0, 1]) */
+int32_t ora_sim_set_counters(ora_sim* s, const lp_counters* in);
 void ora_sim_ledger(ora_sim* s, lp_ledger* out);
 void ora_sim_set_ledger(ora_sim* s, const lp_ledger* in);
 uint64_t ora_sim_particle_count(ora_sim* s);

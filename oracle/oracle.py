@@ -57,6 +57,10 @@ def lib():
         L.ora_sim_get_pellet.argtypes = [P, C.POINTER(_abi.Pellet)]
         L.ora_sim_get_pellet.restype = C.c_int32
         L.ora_sim_set_pellet.argtypes = [P, C.POINTER(_abi.Pellet)]
+        L.ora_sim_audit_step.argtypes = [P, C.c_double, C.POINTER(_abi.EnergyAudit), C.c_char_p, C.c_int32]
+        L.ora_sim_audit_step.restype = C.c_int32
+        L.ora_sim_set_counters.argtypes = [P, C.POINTER(_abi.Counters)]
+        L.ora_sim_set_counters.restype = C.c_int32
         L.ora_sim_get_pellets.argtypes = [P, C.POINTER(_abi.Pellet), C.c_int32]
         L.ora_sim_get_pellets.restype = C.c_int32
         L.ora_sim_set_pellets.argtypes = [P, C.POINTER(_abi.Pellet), C.c_int32]
@@ -149,6 +153,10 @@ class OracleSim:
         lib().ora_sim_counters(self._h, C.byref(c))
         return c
 
+    def set_counters(self, c: _abi.Counters) -> None:
+        if lib().ora_sim_set_counters(self._h, C.byref(c)) != 0:
+            raise ValueError("invalid counters")
+
     def ledger(self) -> _abi.Ledger:
         led = _abi.Ledger()
         lib().ora_sim_ledger(self._h, C.byref(led))
@@ -173,6 +181,14 @@ class OracleSim:
 
     def set_pellet(self, p: _abi.Pellet) -> None:
         lib().ora_sim_set_pellet(self._h, C.byref(p))
+
+    def audit_step(self, dt: float) -> dict:
+        """audit.rs:284-353: energy audit of one trial step on a copy; raises ValueError."""
+        out = _abi.EnergyAudit()
+        err = C.create_string_buffer(512)
+        if lib().ora_sim_audit_step(self._h, float(dt), C.byref(out), err, 512) != 0:
+            raise ValueError(err.value.decode())
+        return out.as_dict()
 
     def pellets(self) -> list:
         """Pellet bed (extension): committed pellets in index order."""
