@@ -226,6 +226,11 @@ lp_status lp_sim_try_step(lp_sim* sim, double dt, int32_t* accepted, char* reaso
 lp_status lp_sim_run_substeps(lp_sim* sim, int32_t steps);
 lp_status lp_sim_sync(lp_sim* sim);
 lp_status lp_sim_stability_limit(lp_sim* sim, double* out);
+/* Energy audit of one trial step of exactly dt (replaces Simulation::audit_step,
+ * core/src/mpm/audit.rs:284-353).  dt must lie in [min_dt, min(dt_scale * stability limit,
+ * max_dt)]; a refused or rejected trial returns LP_INVALID with the reason in lp_last_error().
+ * The simulation's committed state is unchanged. */
+lp_status lp_sim_audit_step(lp_sim* sim, double dt, lp_energy_audit* out);
 lp_status lp_sim_get_ledger(lp_sim* sim, lp_ledger* out);
 lp_status lp_sim_set_ledger(lp_sim* sim, const lp_ledger* in);
 lp_status lp_sim_get_counters(lp_sim* sim, lp_counters* out);

@@ -156,6 +156,7 @@ struct Control {
   double bed_contact_work;
   uint64_t bed_overflow;
   double bed_limit;  // step limit of the committed pellets (set on commit and by the host)
+  double step_diss;  // plastic work of the last attempt, accepted or not (energy audit)
 };
 
 // pellet bed: tangential spring of one sphere pair (pellet-local sphere a, other pellet's b)

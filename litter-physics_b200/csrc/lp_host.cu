@@ -385,6 +385,7 @@ struct Ensemble {
   int graph_kernels = 0;
   std::vector<Control> ctrl_h;
   double* d_diag = nullptr;
+  double* d_audit = nullptr;  // energy-audit partials, 6 per grid-update CTA
   float* d_mlp = nullptr;
   lp::MlpPacked* d_mlp_pk = nullptr;
   int warm = 0;
@@ -458,7 +459,8 @@ lp_status refresh_stats(Ensemble& E) {
 }
 
 struct Diag {
-  double ke, pe, ee, mass, mom[3], max_speed, max_ep, yielded, min_x, max_x, min_y, max_y, max_z, hsq, hmax, column;
+  double ke, pe, ee, mass, mom[3], max_speed, max_ep, yielded, min_x, max_x, min_y, max_y, max_z, hsq, hmax, column,
+      cnorm;
 };
 
 lp_status diagnostics(Ensemble& E, std::vector<Diag>& out) {
@@ -501,6 +503,7 @@ lp_status diagnostics(Ensemble& E, std::vector<Diag>& out) {
       d.hsq += v[15];
       d.hmax = std::max(d.hmax, v[16]);
       d.column = std::max(d.column, v[17]);
+      d.cnorm += v[18];
     }
     out[i] = d;
   }
@@ -1467,6 +1470,156 @@ lp_status lp_sim_energies(lp_sim* sim, double out[9]) {
   out[6] = en.mom_res[1];
   out[7] = en.mom_res[2];
   out[8] = en.e_res;
+  return LP_OK;
+}
+
+// ---------------------------------------------------------------- energy audit (audit.rs)
+// EnergyState::measure (audit.rs:38-53) of the committed state of instance 0: translation,
+// APIC affine norm h^2/8 sum m |C|^2, elastic, potential (material and pellets), pellet kinetic.
+static lp_status audit_state(Ensemble& E, double out[5]) {
+  std::vector<Diag> d;
+  lp_status st = diagnostics(E, d);
+  if (st != LP_OK) return st;
+  st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const Energies en = energies_of(E, 0, d[0]);
+  const InstDesc& D = E.desc[0];
+  double pellet = 0.0;
+  if (D.has_pellet) pellet += pellet_ke_h(E.ctrl_h[0].pellet);
+  if (D.bed_np >= 2)
+    for (const lp::PelletState& P : bed_pull(E, 0)) pellet += pellet_ke_h(P);
+  out[0] = d[0].ke;
+  out[1] = D.dx * D.dx / 8.0 * d[0].cnorm;
+  out[2] = d[0].ee;
+  out[3] = en.pe;
+  out[4] = pellet;
+  return LP_OK;
+}
+
+// EnergyTerms::measure (audit.rs:214-243)
+static void audit_terms(lp_energy_audit& a) {
+  const double* b = a.before;
+  const double* f = a.after;
+  const double* s = a.stages;
+  const double p2g = b[0] + b[1] - s[0];
+  const double g2p = s[5] - f[0] - f[1];
+  const double stress = s[1] - s[0] + f[2] - b[2] + s[7];
+  const double gravity = s[3] - s[2] + f[3] - b[3];
+  const double integrator = f[4] - s[6];
+  const double traction = s[2] - s[1];
+  const double walls = s[4] - s[3];
+  const double coupling = s[5] - s[4] + s[6] - b[4];
+  const double change = (f[0] + f[1] + f[2] + f[3] + f[4]) - (b[0] + b[1] + b[2] + b[3] + b[4]);
+  const double sum = -p2g - g2p + stress - s[7] + gravity + integrator + traction + walls + coupling;
+  const double nan = std::numeric_limits<double>::quiet_NaN();
+  const double t[12] = {p2g,        g2p,      stress, a.coupled ? nan : gravity, a.coupled ? gravity : nan,
+                        integrator, traction, walls,  coupling,                  change, sum, change - sum};
+  for (int k = 0; k < 12; ++k) a.terms[k] = t[k];
+}
+
+// Simulation::audit_step (audit.rs:284-353): one trial step of exactly dt with its stage energies;
+// the committed state (particles, pellets, ledger, counters) is left as it was.
+lp_status lp_sim_audit_step(lp_sim* sim, double dt, lp_energy_audit* out) {
+  if (!sim || !out) return set_error(LP_INVALID, "null argument");
+  Ensemble& E = sim->E;
+  std::memset(out, 0, sizeof(*out));
+  double stability = 0.0;
+  lp_status st = lp_sim_stability_limit(sim, &stability);
+  if (st != LP_OK) return st;
+  const Control saved = E.ctrl_h[0];
+  const InstDesc& D = E.desc[0];
+  const lp_fixture_spec& S = E.specs[0];
+  if (!(std::isfinite(S.gravity[0]) && std::isfinite(S.gravity[1]) && std::isfinite(S.gravity[2])) ||
+      !std::isfinite(S.cfl) || S.cfl <= 0.0 || !std::isfinite(S.wall_friction) || S.wall_friction < 0.0 ||
+      !std::isfinite(S.min_dt) || S.min_dt <= 0.0 || !std::isfinite(S.max_dt) || S.max_dt < S.min_dt ||
+      !std::isfinite(stability) || stability <= 0.0)
+    return set_error(LP_INVALID, "invalid solver state: invalid audit step configuration or stability limit");
+  const double limit = std::fmin(saved.dt_scale * stability, D.max_dt);
+  if (!std::isfinite(dt) || dt <= 0.0 || dt < D.min_dt || !std::isfinite(limit) || dt > limit) {
+    char buf[200];
+    std::snprintf(buf, sizeof(buf),
+                  "invalid solver state: audit `dt`='%.17g' outside finite accepted range ending at '%.17g'", dt, limit);
+    return set_error(LP_INVALID, buf);
+  }
+  if (saved.status != lp::S_RUNNING && saved.status != lp::S_REACHED)
+    return set_error(LP_INVALID, "invalid solver state: the simulation has stopped");
+  out->time = saved.time;
+  out->dt = dt;
+  out->coupled = (D.has_pellet || D.bed_np >= 2) ? 1 : 0;
+  st = audit_state(E, out->before);
+  if (st != LP_OK) return st;
+  for (double v : out->before)
+    if (!std::isfinite(v)) return set_error(LP_INVALID, "invalid solver state: nonfinite initial audit energy");
+  if (!E.d_audit) {
+    st = E.alloc(&E.d_audit, (size_t)6 * E.A.n_gcta);
+    if (st != LP_OK) return st;
+  }
+  CUDA_CK(cudaMemsetAsync(E.d_audit, 0, sizeof(double) * 6 * E.A.n_gcta, E.stream));
+  E.ctrl_h[0].forced_dt = dt;
+  st = push_ctrl(E);
+  if (st != LP_OK) return st;
+  lp::launch_audit(E.A, E.d_audit, E.stream);
+  CUDA_CK(cudaGetLastError());
+  std::vector<double> raw((size_t)6 * E.A.n_gcta);
+  CUDA_CK(cudaMemcpyAsync(raw.data(), E.d_audit, sizeof(double) * raw.size(), cudaMemcpyDeviceToHost, E.stream));
+  std::vector<lp::BedStep> bstep((size_t)std::max(D.bed_np, 0));
+  if (D.bed_np >= 2)
+    CUDA_CK(cudaMemcpyAsync(bstep.data(), E.A.bed_step + D.bed_off, sizeof(lp::BedStep) * bstep.size(),
+                            cudaMemcpyDeviceToHost, E.stream));
+  st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const Control trial = E.ctrl_h[0];
+  // put the committed state back; the trial wrote only the other particle and bed buffers.
+  // The attempt epoch stays advanced so that node blocks marked by the trial never look active.
+  auto restore = [&]() {
+    Control r = saved;
+    r.epoch = trial.epoch;
+    r.forced_dt = 0.0;
+    E.ctrl_h[0] = r;
+    return push_ctrl(E);
+  };
+  if (trial.fail != lp::F_OK || trial.status == lp::S_ERROR) {
+    const int f = trial.fail != lp::F_OK ? trial.fail : lp::F_OUTFLOW;
+    st = restore();
+    if (st != LP_OK) return st;
+    return set_error(LP_INVALID, std::string("invalid solver state: audit trial rejected: ") + fail_text(f));
+  }
+  st = audit_state(E, out->after);
+  if (st != LP_OK) {
+    restore();
+    return st;
+  }
+  const int64_t g0 = D.gcta_off, g1 = D.gcta_off + D.gcta_cnt, ng = E.A.n_gcta;
+  double stage[5] = {0, 0, 0, 0, 0}, transport = 0.0;
+  for (int64_t c = g0; c < g1; ++c) {
+    for (int k = 0; k < 4; ++k) stage[k] += raw[(size_t)(4 * c + k)];
+    stage[4] += raw[(size_t)(4 * ng + c)];
+    transport += raw[(size_t)(5 * ng + c)];
+  }
+  double pellet_after = 0.0;
+  if (D.has_pellet) pellet_after += pellet_ke_h(saved.pellet) + trial.c_pellet_energy;
+  if (D.bed_np >= 2) {
+    E.ctrl_h[0].bed_parity = saved.bed_parity;
+    const std::vector<lp::PelletState> B0 = bed_pull(E, 0);
+    for (size_t p = 0; p < B0.size(); ++p) pellet_after += pellet_ke_h(B0[p]) + bstep[p].cpellet;
+  }
+  const double stg[8] = {transport, stage[0], stage[1], stage[2], stage[3], stage[4], pellet_after, trial.step_diss};
+  for (int k = 0; k < 8; ++k) out->stages[k] = stg[k];
+  const lp::LedgerD& l0 = saved.ledger;
+  const lp::LedgerD& l1 = trial.ledger;
+  const double inc[7] = {l1.plastic - l0.plastic, l1.fric - l0.fric, l1.proj - l0.proj, l1.trac - l0.trac,
+                         l1.cgrid - l0.cgrid, l1.cpellet - l0.cpellet, l1.pellet_work - l0.pellet_work};
+  for (int k = 0; k < 7; ++k) out->increments[k] = inc[k];
+  audit_terms(*out);
+  st = restore();
+  if (st != LP_OK) return st;
+  bool finite = true;
+  for (double v : out->after) finite = finite && std::isfinite(v);
+  for (double v : out->stages) finite = finite && std::isfinite(v);
+  for (double v : out->increments) finite = finite && std::isfinite(v);
+  for (int k = 0; k < 12; ++k)
+    if (!((k == 3 && out->coupled) || (k == 4 && !out->coupled))) finite = finite && std::isfinite(out->terms[k]);
+  if (!finite) return set_error(LP_INVALID, "invalid solver state: audit energy became nonfinite");
   return LP_OK;
 }
 

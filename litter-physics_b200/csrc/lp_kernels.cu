@@ -192,6 +192,23 @@ __device__ int block_argmax_ll(long long value, int index, long long* shv, int* 
   return r;
 }
 
+// Per-particle bound of the node momentum one particle can deposit (mass times speed, affine and
+// stress terms over the stencil, one gravity kick), in FP64 from the FP32 state, so that no
+// magnitude a finite FP32 state holds overflows it.  k_g2p and k_state_stats evaluate these
+// same expressions, so an imported state gets the bound of the run that wrote it.
+__device__ __forceinline__ float affine_norm(const float Cm[9]) {
+  double c2 = 0.0;
+#pragma unroll
+  for (int a = 0; a < 9; ++a) c2 += (double)Cm[a] * Cm[a];
+  return (float)sqrt(c2);
+}
+__device__ __forceinline__ double momentum_bound(float m, float speed, float cn, const float tau[6], float v0,
+                                                 float c_tau, float c_dx, float c_g) {
+  const double t2 = (double)tau[0] * tau[0] + (double)tau[1] * tau[1] + (double)tau[2] * tau[2] +
+                    2.0 * ((double)tau[3] * tau[3] + (double)tau[4] * tau[4] + (double)tau[5] * tau[5]);
+  return (double)m * speed + ((double)m * cn + sqrt(t2) * c_tau * v0) * c_dx + (double)m * c_g;
+}
+
 // ============================================================== begin
 // One thread per instance: decides whether the instance attempts a step and with which dt.
 __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, int n_inst,
@@ -207,7 +224,8 @@ __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__
   c.epoch += 1;
   // fixed-point momentum scale from the committed state's momentum bound
   {
-    double b = c.bbound > 0.0 ? c.bbound : 1e-300;
+    // a non-finite bound (non-finite state) fails the attempt in k_end; any scale does meanwhile
+    double b = c.bbound > 0.0 ? fmin(c.bbound, 1e300) : 1e-300;
     int e = (int)floor(log2(2.305843009213694e18 / b));  // 2^61 / b
     e = e > 200 ? 200 : (e < -200 ? -200 : e);
     c.s_mom = ldexp(1.0, e);
@@ -427,7 +445,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
     k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
           const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
-          int64_t node_total, uint32_t* __restrict__ blk_epoch) {
+          int64_t node_total, uint32_t* __restrict__ blk_epoch, int transport_only) {
   extern __shared__ float4 part[];  // particle records during the chunks, then TB * 27 partial node sums
   float* rec = reinterpret_cast<float*>(part);  // [P2G_REC][P2G_CHUNK]
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
@@ -456,7 +474,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
 
   const float* cur = c.parity ? st1 : st0;
   const float dx = (float)D.dx;
-  const float stress_scale = (float)(c.dt * 4.0 / (D.dx * D.dx));
+  // the energy audit's transport pass deposits APIC momentum only (audit.rs:381-398)
+  const float stress_scale = transport_only ? 0.0f : (float)(c.dt * 4.0 / (D.dx * D.dx));
   const double s_m = D.s_mass, s_p = c.s_mom;
 
   float acc9[3][3][4];
@@ -740,12 +759,17 @@ __device__ __forceinline__ void reduce_tangential(float t[3], float reduction) {
   }
 }
 
+// AUDIT (energy audit, audit.rs:72-90): each CTA also sums the grid kinetic energy after the
+// stress deposit, after wall traction, with the gravity kick, and after the wall projection and
+// friction, into audit[4 * CTA + 0..3].
+template <bool AUDIT>
 __global__ void __launch_bounds__(GU_THREADS)
     k_grid_update(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
                   const int* __restrict__ gcta_inst, long long* __restrict__ acc, long long* __restrict__ trac,
                   int64_t node_total, const uint32_t* __restrict__ blk_epoch, float4* __restrict__ vel,
-                  GridPartial* __restrict__ part) {
-  __shared__ double shd[(GU_THREADS / 32) * 7 + 7];
+                  GridPartial* __restrict__ part, double* __restrict__ audit) {
+  constexpr int RK = AUDIT ? 11 : 7;
+  __shared__ double shd[(GU_THREADS / 32) * RK + RK];
   const int inst = gcta_inst[blockIdx.x];
   const Control& c = ctrl[inst];
   if (!c.active) return;
@@ -754,6 +778,7 @@ __global__ void __launch_bounds__(GU_THREADS)
   const int64_t lblk = (blockIdx.x - D.gcta_off) * GU_BLOCKS_PER_CTA + t / 64;
   const int64_t nblk = (int64_t)D.nblk[0] * D.nblk[1] * D.nblk[2];
   double wi0 = 0, wi1 = 0, wi2 = 0, proj = 0, fric = 0, tren = 0;
+  double e_stress = 0, e_trac = 0, e_grav = 0, e_walls = 0;
   int fail = F_OK;
   bool live = lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch;
   int ni = 0, nj = 0, nk = 0;
@@ -772,6 +797,8 @@ __global__ void __launch_bounds__(GU_THREADS)
       P.wall_impulse[0] = P.wall_impulse[1] = P.wall_impulse[2] = 0.0;
       P.proj = P.fric = P.trac = 0.0;
       P.fail = F_OK;
+      if (AUDIT)
+        for (int k = 0; k < 4; ++k) audit[4 * (int64_t)blockIdx.x + k] = 0.0;
     }
     return;
   }
@@ -793,6 +820,7 @@ __global__ void __launch_bounds__(GU_THREADS)
       acc[node_total + g] = 0;
       acc[2 * node_total + g] = 0;
       acc[3 * node_total + g] = 0;
+      if (AUDIT) e_stress = 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / md;
       const int co[3] = {ni, nj, nk};
       float Tl[3] = {0.f, 0.f, 0.f}, Th[3] = {0.f, 0.f, 0.f};
       bool shell = false;
@@ -818,6 +846,15 @@ __global__ void __launch_bounds__(GU_THREADS)
             Th[a] = (float)dh;
           }
         }
+      }
+      if (AUDIT) {
+        e_trac = 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / md;
+        double k2 = 0.0;
+        for (int a = 0; a < 3; ++a) {
+          const double u = p[a] / md + D.gravity[a] * c.dt;
+          k2 += u * u;
+        }
+        e_grav = 0.5 * md * k2;
       }
       const float m = (float)md;
       const float dt = (float)c.dt;
@@ -875,11 +912,26 @@ __global__ void __launch_bounds__(GU_THREADS)
         wi1 += (double)(v[1] - before[1]) * (double)m;
         wi2 += (double)(v[2] - before[2]) * (double)m;
         vel[g] = make_float4(v[0], v[1], v[2], m);
+        if (AUDIT)
+          e_walls = 0.5 * (double)m * ((double)v[0] * v[0] + (double)v[1] * v[1] + (double)v[2] * v[2]);
       }
     }
   }
-  double rv[7] = {wi0, wi1, wi2, proj, fric, tren, (double)fail};
-  block_reduce_multi<GU_THREADS, 7>(rv, 1u << 6, shd);
+  double rv[RK];
+  rv[0] = wi0;
+  rv[1] = wi1;
+  rv[2] = wi2;
+  rv[3] = proj;
+  rv[4] = fric;
+  rv[5] = tren;
+  rv[6] = (double)fail;
+  if (AUDIT) {
+    rv[RK - 4] = e_stress;
+    rv[RK - 3] = e_trac;
+    rv[RK - 2] = e_grav;
+    rv[RK - 1] = e_walls;
+  }
+  block_reduce_multi<GU_THREADS, RK>(rv, 1u << 6, shd);
   wi0 = rv[0];
   wi1 = rv[1];
   wi2 = rv[2];
@@ -896,7 +948,56 @@ __global__ void __launch_bounds__(GU_THREADS)
     P.fric = fric;
     P.trac = tren;
     P.fail = fail;
+    if (AUDIT)
+      for (int k = 0; k < 4; ++k) audit[4 * (int64_t)blockIdx.x + k] = rv[RK - 4 + k];
   }
+}
+
+// Energy audit: grid kinetic energy of the nodes that hold mass in this attempt, one partial per
+// grid-update CTA (audit.rs:360-378 grid_kinetic).  from_acc: from the deposited momentum of the
+// transport pass, clearing the accumulators as the grid update does; otherwise from the node
+// velocities and masses of vel[].
+__global__ void __launch_bounds__(GU_THREADS)
+    k_audit_kinetic(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                    const int* __restrict__ gcta_inst, long long* __restrict__ acc, const float4* __restrict__ vel,
+                    int64_t node_total, const uint32_t* __restrict__ blk_epoch, int from_acc,
+                    double* __restrict__ out) {
+  __shared__ double shd[(GU_THREADS / 32) + 1];
+  const int inst = gcta_inst[blockIdx.x];
+  const Control& c = ctrl[inst];
+  const InstDesc& D = desc[inst];
+  const int t = threadIdx.x;
+  double e = 0.0;
+  const int64_t lblk = (blockIdx.x - D.gcta_off) * GU_BLOCKS_PER_CTA + t / 64;
+  const int64_t nblk = (int64_t)D.nblk[0] * D.nblk[1] * D.nblk[2];
+  if (c.active && lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch) {
+    const int bk = (int)(lblk % D.nblk[2]), bj = (int)((lblk / D.nblk[2]) % D.nblk[1]),
+              bi = (int)(lblk / ((int64_t)D.nblk[2] * D.nblk[1]));
+    const int l = t % 64;
+    const int ni = bi * NB + l / 16, nj = bj * NB + (l / 4) % 4, nk = bk * NB + l % 4;
+    if (ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2]) {
+      const int64_t g = node_index(D, ni, nj, nk);
+      if (from_acc) {
+        const long long mf = acc[g];
+        if (mf > 0) {
+          const double md = (double)mf / D.s_mass;
+          double p2 = 0.0;
+          for (int a = 1; a <= 3; ++a) {
+            const double pa = (double)acc[a * node_total + g] / c.s_mom;
+            p2 += pa * pa;
+          }
+          e = 0.5 * p2 / md;
+        }
+        for (int a = 0; a < 4; ++a) acc[a * node_total + g] = 0;
+      } else {
+        const float4 v = vel[g];
+        if (v.w > 0.0f) e = 0.5 * (double)v.w * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+      }
+    }
+  }
+  double r[1] = {e};
+  block_reduce_multi<GU_THREADS, 1>(r, 0u, shd);
+  if (t == 0) out[blockIdx.x] = r[0];
 }
 
 // ============================================================== pellet (FP64 rigid body)
@@ -1816,8 +1917,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
         if (pyield) nxt[C_YS * cap + k] = in[PF_YS * G2P_THREADS];
         idn[k] = __float_as_uint(in[PF_ID * G2P_THREADS]);
       }
-      cn = sqrtf(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] + Cm[5] * Cm[5] +
-                 Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]);
+      cn = affine_norm(Cm);
       if (paste) {
         float H[9];
 #pragma unroll
@@ -1935,10 +2035,8 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
     for (int a = 0; a < 6; ++a) nxt[(C_TAU + a) * cap + k] = tau[a];
     nxt[C_EP * cap + k] = ep;
     // momentum bound of the new state for the next attempt's fixed-point scale (its factors of
-    // 2.6 and 6 leave ample room for the FP32 rounding of the terms)
-    const float tn = sqrtf(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2] +
-                           2.f * (tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]));
-    bb += (double)(m * speed + (cn * m + tn * c_tau * v0) * c_dx + m * c_g);
+    // 2.6 and 6 leave ample room for rounding)
+    bb += momentum_bound(m, speed, cn, tau, v0, c_tau, c_dx, c_g);
     mass_sum += (double)m;
     max_speed = fmaxf(max_speed, speed);
     max_disp = fmaxf(max_disp, disp);
@@ -2052,8 +2150,10 @@ __global__ void k_end(const InstDesc* __restrict__ desc, Control* __restrict__ c
   const long long its = (long long)v[8], yl = (long long)v[9];
   const float ms = (float)v[10], md = (float)v[11];
   const int fail = (int)v[12], pfail = (int)v[13];
+  c.step_diss = diss;
   int f = F_OK;
   if (!isfinite(trac) || !isfinite(c.ledger.trac + trac)) f = F_TRACTION_NONFINITE;
+  else if (!isfinite(c.bbound)) f = F_GRID_NONFINITE;  // the deposit could not be represented
   else if (fail != F_OK) f = fail;
   else if (D.has_pellet && c.pellet_fail) f = F_PELLET_NONFINITE;
   else if (D.bed_np >= 2 && bv[16] > 0.0) f = F_PELLET_NONFINITE;
@@ -2155,16 +2255,12 @@ __global__ void k_state_stats(const InstDesc* __restrict__ desc, const Control* 
     // the same FP32 expressions as the end of k_g2p, so that a state imported from a
     // checkpoint gets the same speed and per-particle bound as the run that wrote it
     const float speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    const float cn = sqrtf(Cm[0] * Cm[0] + Cm[1] * Cm[1] + Cm[2] * Cm[2] + Cm[3] * Cm[3] + Cm[4] * Cm[4] +
-                           Cm[5] * Cm[5] + Cm[6] * Cm[6] + Cm[7] * Cm[7] + Cm[8] * Cm[8]);
-    const float tn = sqrtf(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2] +
-                           2.f * (tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]));
     const float c_tau = (float)(D.max_dt * 4.0 / (D.dx * D.dx));
     const float c_dx = (float)(2.6 * D.dx);
     const float c_g =
         (float)(6.0 * sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]) *
                 D.max_dt);
-    bb = (double)(m * speed + (cn * m + tn * c_tau * v0) * c_dx + m * c_g);
+    bb = momentum_bound(m, speed, affine_norm(Cm), tau, v0, c_tau, c_dx, c_g);
     sp = speed;
     ms = (double)m;
   }
@@ -2186,7 +2282,8 @@ __global__ void k_state_stats(const InstDesc* __restrict__ desc, const Control* 
 
 // Energies and observables of the committed state (FP64 partials per CTA).
 // out per CTA (DIAG_N doubles): ke, pe, ee, mass, mom xyz, max speed, max ep, yielded count,
-// min x, max x, min y, max y, max z, hydro sum sq, hydro max, column height (dam break)
+// min x, max x, min y, max y, max z, hydro sum sq, hydro max, column height (dam break),
+// sum of m |C|^2 (the APIC affine norm before its h^2/8 factor)
 __global__ void k_diagnostics(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
                               const int* __restrict__ pcta_inst, const float* __restrict__ st0,
                               const float* __restrict__ st1, int64_t cap, int fixture_hydro, double h0,
@@ -2275,10 +2372,16 @@ __global__ void k_diagnostics(const InstDesc* __restrict__ desc, const Control* 
     }
     if (fixture_dam && x[0] < D.dx) vals[17] = x[2];
     else vals[17] = -1e300;
+    double c2 = 0.0;
+    for (int a = 0; a < 9; ++a) {
+      const double ca = cur[(C_C + a) * cap + k];
+      c2 += ca * ca;
+    }
+    vals[18] = m * c2;
   } else {
     vals[17] = -1e300;
   }
-  // reduce: sums 0-6, 14, 15; max 7, 8, 10, 12, 13, 16, 17; min 9, 11
+  // reduce: sums 0-6, 14, 15, 18; max 7, 8, 10, 12, 13, 16, 17; min 9, 11
   for (int j = 0; j < DIAG_N; ++j) {
     const int t = threadIdx.x;
     shd[t] = vals[j];
@@ -2287,7 +2390,7 @@ __global__ void k_diagnostics(const InstDesc* __restrict__ desc, const Control* 
       if (t < s) {
         const double a = shd[t], b = shd[t + s];
         double r;
-        if (j <= 6 || j == 14 || j == 15) r = a + b;
+        if (j <= 6 || j == 14 || j == 15 || j == 18) r = a + b;
         else if (j == 9 || j == 11) r = fmin(a, b);
         else r = fmax(a, b);
         shd[t] = r;
@@ -2379,7 +2482,9 @@ void add_kernel_launches(uint64_t n) { g_launches += n; }
 
 static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
+// audit (energy audit) or null: the grid-update stage energies go to audit[4 * CTA + k] and the
+// kinetic energy after the pellet coupling to audit[4 * n_gcta + CTA].
+static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev, double* audit) {
   int n = 0;
   if (ev) cudaEventRecord(ev[0], s);
   k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
@@ -2407,15 +2512,19 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
-                                                     A.perm, A.acc, A.node_total, A.blk_epoch);
+                                                     A.perm, A.acc, A.node_total, A.blk_epoch, 0);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
                                      A.acc, A.trac, A.node_total);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_grid_update<<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.trac,
-                                                           A.node_total, A.blk_epoch, A.vel, A.gpart);
+  if (audit)
+    k_grid_update<true><<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.trac,
+                                                                 A.node_total, A.blk_epoch, A.vel, A.gpart, audit);
+  else
+    k_grid_update<false><<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.trac,
+                                                                  A.node_total, A.blk_epoch, A.vel, A.gpart, nullptr);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   if (A.any_pellet) {
@@ -2436,6 +2545,11 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
     ++n;
     if (ev) cudaEventRecord(ev[n], s);
   }
+  if (audit) {
+    k_audit_kinetic<<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.vel, A.node_total,
+                                                             A.blk_epoch, 0, audit + 4 * A.n_gcta);
+    ++n;
+  }
   const bool warm_g2p = A.mlp != nullptr && A.warm;
   (warm_g2p ? k_g2p<true> : k_g2p<false>)<<<(unsigned)A.n_tiles, G2P_THREADS,
                                             warm_g2p ? g2p_smem_bytes<true>() : g2p_smem_bytes<false>(), s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
@@ -2451,6 +2565,31 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[n], s);
   g_launches += (uint64_t)n;
   return n;
+}
+
+int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) { return attempt_sequence(A, s, ev, nullptr); }
+
+int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s) {
+  // transport pass: binning and an APIC-only deposit, its grid kinetic energy to buf[5 n_gcta + CTA]
+  k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
+  k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+                                                          A.keys, A.count, A.nw_list, A.nw_count);
+  k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
+  k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
+  k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
+  k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
+                                                            A.perm);
+  k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
+                                                                      A.perm, A.id[0], A.id[1]);
+  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap,
+                                                           A.start, A.perm, A.acc, A.node_total, A.blk_epoch, 1);
+  k_audit_kinetic<<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.vel, A.node_total,
+                                                           A.blk_epoch, 1, buf + 5 * A.n_gcta);
+  g_launches += 9;
+  // the audited trial step, without the Newton log
+  DeviceArrays B = A;
+  B.log_cap = 0;
+  return 9 + attempt_sequence(B, s, nullptr, buf);
 }
 
 __global__ void k_grid_sums(const long long* __restrict__ acc, int64_t node_total, unsigned long long* __restrict__ out) {
@@ -2472,7 +2611,7 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
                                                                       A.perm, A.id[0], A.id[1]);
   k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
-                                                     A.perm, A.acc, A.node_total, A.blk_epoch);
+                                                     A.perm, A.acc, A.node_total, A.blk_epoch, 0);
   k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
                                      A.acc, A.trac, A.node_total);
   g_launches += 9;
@@ -2491,13 +2630,13 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
                                                                       A.perm, A.id[0], A.id[1]);
   k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
-                                                     A.perm, A.acc, A.node_total, A.blk_epoch);
+                                                     A.perm, A.acc, A.node_total, A.blk_epoch, 0);
   k_grid_sums<<<148 * 4, 256, 0, s>>>(A.acc, A.node_total, (unsigned long long*)out);
   g_launches += 9;
   return 9;
 }
 
-int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return launch_attempt(A, s, nullptr); }
+int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return attempt_sequence(A, s, nullptr, nullptr); }
 
 const char* attempt_kernel_name(int k, int any_pellet, int any_bed) {
   static const char* a[] = {"k_begin", "k_bin_count", "k_scan_chunks", "k_scan_instances", "k_scan_apply",

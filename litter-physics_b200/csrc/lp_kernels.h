@@ -8,7 +8,7 @@
 
 namespace lp {
 
-constexpr int DIAG_N = 18;
+constexpr int DIAG_N = 19;
 
 // All device buffers of one ensemble (owned by the host runtime).
 struct DeviceArrays {
@@ -69,6 +69,11 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s);
 // same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 14 events)
 int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev);
 const char* attempt_kernel_name(int k, int any_pellet, int any_bed);
+// Energy audit of one forced-dt trial: a transport pass (binning + APIC-only deposit) and the
+// attempt with stage energies.  buf holds 6 * n_gcta doubles: [0, 4 n_gcta) the grid-update
+// stages per CTA (stress, traction, gravity kick, walls), [4 n_gcta, 5 n_gcta) the kinetic energy
+// after the pellet coupling, [5 n_gcta, 6 n_gcta) the transport pass.
+int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s);
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s);
 // begin + binning + P2G only (conservation probe), then exact node sums into out[4] (int64)
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s);

@@ -80,6 +80,7 @@ def lib():
         "lp_sim_run_substeps": ([P, I32], I32),
         "lp_sim_sync": ([P], I32),
         "lp_sim_stability_limit": ([P, D], I32),
+        "lp_sim_audit_step": ([P, C.c_double, C.POINTER(_abi.EnergyAudit)], I32),
         "lp_sim_get_ledger": ([P, C.POINTER(_abi.Ledger)], I32),
         "lp_sim_set_ledger": ([P, C.POINTER(_abi.Ledger)], I32),
         "lp_sim_get_counters": ([P, C.POINTER(_abi.Counters)], I32),

@@ -86,6 +86,17 @@ class Simulation:
         check(lib().lp_sim_stability_limit(self._h, C.byref(out)))
         return out.value
 
+    def audit_step(self, dt: float) -> dict:
+        """Energy audit of one trial step of exactly `dt` (audit.rs:284-353): endpoint energies,
+        stage grid energies, ledger increments and the stage telescope terms.  The committed
+        state is unchanged.  A refused `dt` or a rejected trial raises ValueError."""
+        out = _abi.EnergyAudit()
+        status = lib().lp_sim_audit_step(self._h, float(dt), C.byref(out))
+        if status == _abi.LP_INVALID:
+            raise ValueError(lib().lp_last_error().decode(errors="replace"))
+        check(status)
+        return out.as_dict()
+
     # ------------------------------------------------------------------ state
     @property
     def ledger(self) -> _abi.Ledger:

@@ -101,11 +101,17 @@ def isolated(factory, rows=None, pellet=False, gravity=0.0, material=None):
     return sim
 
 
+def _get(sim, name):
+    """`ledger` and `counters` are methods of the oracle and properties of the device simulation."""
+    v = getattr(sim, name)
+    return v() if callable(v) else v
+
+
 def snapshot(sim) -> tuple:
     """Everything `audit_step` must leave untouched."""
     p = sim.particles()
-    c = sim.counters()
-    led = sim.ledger()
+    c = _get(sim, "counters")
+    led = _get(sim, "ledger")
     pel = sim.pellet()
     key = (c.time, c.step_count, c.rejected_steps, c.limited_steps, c.dt_scale)
     ledger = bytes(memoryview(led))
@@ -292,7 +298,7 @@ def test_invalid_unstable_escaped_and_rejected_trials_do_not_mutate():
             sim.audit_step(dt)
         assert same_snapshot(before, snapshot(sim))
     limited = isolated(oracle_factory)
-    c = limited.counters()
+    c = _get(limited, "counters")
     c.dt_scale = 0.001
     limited.set_counters(c)
     with pytest.raises(ValueError):
@@ -324,7 +330,7 @@ def plastic_sim(factory, ledger_plastic):
     aff[0, 1] = 50.0
     sim = isolated(factory, [([0.47, 0.52, 0.55], [0.0, 0.0, 0.0], 2.0, 0.002, aff)],
                    material=research.material_paste(1000.0, 1000.0, 0.3, 0.1, 0.0, 1.0))
-    led = sim.ledger()
+    led = _get(sim, "ledger")
     led.plastic_dissipation = ledger_plastic
     sim.set_ledger(led)
     return sim
@@ -336,7 +342,7 @@ def test_plastic_increment_is_history_difference():
     a = sim.audit_step(1e-3)
     sim.advance_to(1e-3)
     assert a["increments"]["plastic_dissipation"] > 0.0
-    close(a["increments"]["plastic_dissipation"], sim.ledger().plastic_dissipation - 3.0)
+    close(a["increments"]["plastic_dissipation"], _get(sim, "ledger").plastic_dissipation - 3.0)
     s = a["stages"]
     expected = (s["grid_after_stress"] - s["grid_transport"] + a["after"]["elastic"] - a["before"]["elastic"]
                 + s["plastic_dissipation"])
@@ -386,7 +392,7 @@ def test_audit_matches_actual_advance_endpoint_and_existing_histories():
     close(a["after"]["translation"], e["kinetic"])
     close(a["after"]["elastic"], e["elastic"])
     close(a["after"]["potential"], e["potential"])
-    close(a["increments"]["plastic_dissipation"], sim.ledger().plastic_dissipation)
+    close(a["increments"]["plastic_dissipation"], _get(sim, "ledger").plastic_dissipation)
 
 
 # Published first-step figures of the light-body probe, docs/energy-audit.md:155-160.
@@ -431,6 +437,21 @@ def test_light_body_probe_reproduces_published_figures():
 
 
 # -------------------------------------------------------------------------- GPU
+def sinking_bed(factory):
+    """A 24-pellet bed (config-4 model at 7.8 mm cells) lowered 6 mm into its 2-cell paste layer
+    and moving down at 0.3 m/s, so that many pellets couple to the grid in the audited step."""
+    from test_pellet_bed import small_bed
+
+    sim = factory(small_bed())
+    moved = []
+    for p in sim.pellets():
+        p.position[2] -= 0.006
+        p.velocity[:] = [0.0, 0.0, -0.3]
+        moved.append(p)
+    sim.set_pellets(moved)
+    return sim
+
+
 GPU_CASES = {
     "translation_affine": lambda f: isolated(f, [([0.47, 0.52, 0.55], [1.0, -2.0, 0.5], 2.0, 0.002,
                                                  np.array([[0.2, 0.3, -0.1], [0.5, -0.4, 0.7], [0.1, 0.2, 0.4]]))]),
@@ -441,8 +462,21 @@ GPU_CASES = {
     "plastic": lambda f: plastic_sim(f, 3.0),
     "light_body": light_body_sim,
     "tilted_pellet": tilted_pellet_sim,
+    "pellet_bed": sinking_bed,
 }
-GPU_DT = {"freefall": 1e-3, "plastic": 1e-3, "light_body": 1e-5}
+GPU_DT = {"freefall": 1e-3, "plastic": 1e-3, "light_body": 1e-5, "pellet_bed": 2e-5}
+
+
+def test_sinking_bed_audit_couples_and_telescopes():
+    """The pellet-bed extension inside the audit: every pellet's impulse is one coupling stage,
+    and the stage telescope closes."""
+    a = sinking_bed(oracle_factory).audit_step(2e-5)
+    assert a["increments"]["coupling_grid_energy"] != 0.0
+    assert a["increments"]["coupling_pellet_energy"] != 0.0
+    close(a["terms"]["coupling_change"],
+          a["increments"]["coupling_grid_energy"] + a["increments"]["coupling_pellet_energy"], 1e-12)
+    close(a["terms"]["telescoping_error"], 0.0)
+    assert a["terms"]["coupled_grid_gravity_total_potential_change"] is not None
 
 
 @pytest.fixture(scope="module")
@@ -510,4 +544,4 @@ def test_gpu_audit_refuses_invalid_steps_without_mutation(built):
     bad2 = isolated(gpu_factory)
     bad2.audit_step(1e-4)
     bad2.advance_to(2e-4)
-    assert bad2.counters().step_count >= 1
+    assert _get(bad2, "counters").step_count >= 1
