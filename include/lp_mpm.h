@@ -104,7 +104,16 @@ typedef struct lp_fixture_spec {
   uint64_t bed_seed;
   double bed_lo[3], bed_hi[3];
   double hm_young, hm_poisson, hm_friction, hm_restitution;
+  /* contact law between bed pellets: LP_BED_HERTZ_MINDLIN (hm_* above) or LP_BED_LINEAR, the
+   * household DEM's linear spring-dashpot with a tangential spring and rolling resistance
+   * (replaces World::contact_force, core/src/dem.rs:789-834): normal stiffness dem_stiffness
+   * N/m, rolling friction dem_rolling, friction hm_friction, restitution hm_restitution */
+  int32_t bed_law;
+  int32_t _pad4;
+  double dem_stiffness, dem_rolling;
 } lp_fixture_spec;
+
+enum { LP_BED_HERTZ_MINDLIN = 0, LP_BED_LINEAR = 1 };
 
 /* Mirror of Ledger (solver.rs:65-124), FP64. */
 typedef struct lp_ledger {

@@ -106,6 +106,10 @@ struct InstDesc {
   int64_t bed_off;           // first pellet of this instance in the global bed arrays
   double bed_h, bed_rb;      // coarse cell edge, pellet bounding radius
   double hm_estar, hm_gstar, hm_mu, hm_beta;  // effective moduli, friction, damping parameter
+  // contact law: 0 Hertz-Mindlin, 1 linear spring-dashpot (stiffness, damping ratio, rolling
+  // friction; friction is hm_mu)
+  int bed_law;
+  double dem_kn, dem_zeta, dem_mur;
 };
 
 // pellet state (rigid.rs:30-49), FP64
@@ -206,14 +210,25 @@ struct ParticlePartial {
 };
 
 // Pellet-bed step limit: per pellet the reference's wall-contact and pellet-CFL limits
-// (solver.rs:477-498), plus 0.2 sqrt(m*/k_c) for the Hertz stiffness at an overlap of 5 % of
-// the sphere radius, k_c = 2 E* sqrt(R* 0.05 r).
+// (solver.rs:477-498), plus for Hertz-Mindlin 0.2 sqrt(m*/k_c) at the stiffness of an overlap
+// of 5 % of the sphere radius, k_c = 2 E* sqrt(R* 0.05 r), and for the linear law the household
+// DEM's 0.1 sqrt(m/k_n) (World::stable_dt, dem.rs:509-520).
 __host__ __device__ inline double pellet_bed_limit(const InstDesc& D, const PelletState& P) {
   double limit = 0.2 * sqrt(P.mass / D.contact_k);
   const double ps = sqrt(P.vel[0] * P.vel[0] + P.vel[1] * P.vel[1] + P.vel[2] * P.vel[2]);
   if (ps > 0.0) limit = fmin(limit, D.cfl * D.dx / ps);
+  if (D.bed_law == 1) return fmin(limit, 0.1 * sqrt(P.mass / D.dem_kn));
   const double kc = 2.0 * D.hm_estar * sqrt(0.5 * P.radius * 0.05 * P.radius);
   return fmin(limit, 0.2 * sqrt(0.5 * P.mass / kc));
+}
+
+// Damping ratio of a linear dashpot for restitution e (ContactParams::damping_ratio,
+// dem.rs:112-120): e clamped to [0, 1], critical damping at e = 0.
+__host__ __device__ inline double dem_damping_ratio(double e) {
+  e = fmin(fmax(e, 0.0), 1.0);
+  if (e <= 2.220446049250313e-16) return 1.0;
+  const double l = log(e);
+  return fmin(-l / sqrt(3.14159265358979323846 * 3.14159265358979323846 + l * l), 1.0);
 }
 __host__ __device__ inline double bed_limit(const InstDesc& D, const PelletState* S) {
   double limit = 1e300;

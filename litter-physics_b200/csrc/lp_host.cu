@@ -148,11 +148,20 @@ lp_status validate_spec(const lp_fixture_spec& s) {
       if (!(std::isfinite(s.bed_lo[a]) && std::isfinite(s.bed_hi[a]) && s.bed_lo[a] <= s.bed_hi[a] &&
             s.bed_lo[a] >= 0.0 && s.bed_hi[a] <= s.domain[a]))
         return set_error(LP_INVALID, "pellet bed region must lie inside `domain_m`");
-    if (!(std::isfinite(s.hm_young) && s.hm_young > 0.0) || !(s.hm_poisson >= 0.0 && s.hm_poisson < 0.5) ||
-        !(std::isfinite(s.hm_friction) && s.hm_friction >= 0.0) ||
-        !(s.hm_restitution > 0.0 && s.hm_restitution <= 1.0))
+    if (s.bed_law == LP_BED_LINEAR) {
+      if (!(std::isfinite(s.dem_stiffness) && s.dem_stiffness > 0.0) ||
+          !(std::isfinite(s.dem_rolling) && s.dem_rolling >= 0.0) ||
+          !(std::isfinite(s.hm_friction) && s.hm_friction >= 0.0) || !std::isfinite(s.hm_restitution))
+        return set_error(LP_INVALID, "invalid linear contact parameters (stiffness > 0, rolling friction >= 0, "
+                                     "friction >= 0, finite restitution)");
+    } else if (s.bed_law != LP_BED_HERTZ_MINDLIN) {
+      return set_error(LP_INVALID, "unknown pellet-bed contact law");
+    } else if (!(std::isfinite(s.hm_young) && s.hm_young > 0.0) || !(s.hm_poisson >= 0.0 && s.hm_poisson < 0.5) ||
+               !(std::isfinite(s.hm_friction) && s.hm_friction >= 0.0) ||
+               !(s.hm_restitution > 0.0 && s.hm_restitution <= 1.0)) {
       return set_error(LP_INVALID, "invalid Hertz-Mindlin parameters (young > 0, 0 <= poisson < 0.5, "
                                    "friction >= 0, 0 < restitution <= 1)");
+    }
   }
   return LP_OK;
 }
@@ -647,11 +656,18 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
       D.bed_h = 2.0 * D.bed_rb;
       for (int a = 0; a < 3; ++a)
         D.bed_nc[a] = std::max(1, (int)std::ceil((double)h.cells[a] * s.grid_spacing / D.bed_h));
-      const double nu = s.hm_poisson, E = s.hm_young, G = E / (2.0 * (1.0 + nu));
-      D.hm_estar = E / (2.0 * (1.0 - nu * nu));
-      D.hm_gstar = G / (2.0 * (2.0 - nu));
       D.hm_mu = s.hm_friction;
-      D.hm_beta = hm_beta_for(s.hm_restitution);
+      D.bed_law = s.bed_law;
+      if (s.bed_law == LP_BED_LINEAR) {
+        D.dem_kn = s.dem_stiffness;
+        D.dem_zeta = lp::dem_damping_ratio(s.hm_restitution);
+        D.dem_mur = s.dem_rolling;
+      } else {
+        const double nu = s.hm_poisson, E = s.hm_young, G = E / (2.0 * (1.0 + nu));
+        D.hm_estar = E / (2.0 * (1.0 - nu * nu));
+        D.hm_gstar = G / (2.0 * (2.0 - nu));
+        D.hm_beta = hm_beta_for(s.hm_restitution);
+      }
       for (int p = 0; p < D.bed_np; ++p) bed_inst.push_back(i);
       bed_off += D.bed_np;
     }

@@ -1268,7 +1268,7 @@ __global__ void k_couple(const InstDesc* __restrict__ desc, Control* __restrict_
 //   k_bed_couple : one CTA per pellet applies couple_grid (rigid.rs:385-438) to the grid nodes it
 //                  owns: a node inside several proxies belongs to the pellet of smallest signed
 //                  distance (ties: lower index), so every node is constrained at most once;
-//   k_bed_step   : one thread per pellet: Hertz-Mindlin sphere contact with the other pellets
+//   k_bed_step   : one thread per pellet: sphere contact (Hertz-Mindlin or the linear law) with the other pellets
 //                  (start-of-step states, tangential spring history per sphere pair), then
 //                  apply_impulse and integrate (rigid.rs:251-334) with the contact force added.
 // The two sides of a contact evaluate mirrored expressions (d -> -d, v_rel -> -v_rel, the
@@ -1576,10 +1576,6 @@ __global__ void __launch_bounds__(64) k_bed_step(const InstDesc* __restrict__ de
         const double vn = vrel[0] * nn[0] + vrel[1] * nn[1] + vrel[2] * nn[2];
         double vt[3];
         for (int k = 0; k < 3; ++k) vt[k] = vrel[k] - vn * nn[k];
-        const double sq = sqrt(rs * delta);
-        const double sn = 2.0 * D.hm_estar * sq, stf = 8.0 * D.hm_gstar * sq;
-        const double gn = -k56 * D.hm_beta * sqrt(sn * mstar), gt = -k56 * D.hm_beta * sqrt(stf * mstar);
-        const double fn = fmax((4.0 / 3.0) * D.hm_estar * sqrt(rs) * (delta * sqrt(delta)) - gn * vn, 0.0);
         double xi[3] = {0.0, 0.0, 0.0};
         for (int h = 0; h < nold; ++h)
           if (hold[h].other == q && hold[h].a == a && hold[h].b == b) {
@@ -1589,18 +1585,49 @@ __global__ void __launch_bounds__(64) k_bed_step(const InstDesc* __restrict__ de
             break;
           }
         const double xn = xi[0] * nn[0] + xi[1] * nn[1] + xi[2] * nn[2];
-        double ft[3];
-        for (int k = 0; k < 3; ++k) {
-          xi[k] = (xi[k] - xn * nn[k]) + vt[k] * dt;
-          ft[k] = stf * xi[k] + gt * vt[k];
-        }
-        const double ftn = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
-        const double lim = D.hm_mu * fn;
-        if (ftn > lim) {
-          const double sc = lim / ftn;
+        double fn, ft[3], roll[3] = {0.0, 0.0, 0.0};
+        if (D.bed_law == 1) {
+          // linear spring-dashpot, tangential spring with Coulomb sliding and constant rolling
+          // resistance (dem.rs:789-834).  xi follows the reference's first-body convention (this
+          // pellet first, contact normal pointing at it), in which the tangential velocity is -vt.
+          const double cn = 2.0 * D.dem_zeta * sqrt(D.dem_kn * mstar);
+          const double kt = (2.0 / 7.0) * D.dem_kn, ct = 0.5345224838248488 * cn;  // sqrt(2/7) cn
+          fn = fmax(D.dem_kn * delta - cn * vn, 0.0);
           for (int k = 0; k < 3; ++k) {
-            ft[k] *= sc;
-            xi[k] = (ft[k] - gt * vt[k]) / stf;
+            xi[k] = (xi[k] - xn * nn[k]) - vt[k] * dt;
+            ft[k] = -(xi[k] * kt) + vt[k] * ct;
+          }
+          const double ftn = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+          const double lim = D.hm_mu * fn;
+          if (ftn > lim) {
+            const double sc = ftn > 2.220446049250313e-16 ? lim / ftn : 0.0;
+            for (int k = 0; k < 3; ++k) {
+              ft[k] *= sc;
+              xi[k] = -ft[k] / kt;
+            }
+          }
+          double wr[3];
+          for (int k = 0; k < 3; ++k) wr[k] = omp[k] - omq[k];
+          const double wn = sqrt(wr[0] * wr[0] + wr[1] * wr[1] + wr[2] * wr[2]);
+          if (wn > 2.220446049250313e-16)
+            for (int k = 0; k < 3; ++k) roll[k] = -wr[k] / wn * (D.dem_mur * rs * fn);
+        } else {
+          const double sq = sqrt(rs * delta);
+          const double sn = 2.0 * D.hm_estar * sq, stf = 8.0 * D.hm_gstar * sq;
+          const double gn = -k56 * D.hm_beta * sqrt(sn * mstar), gt = -k56 * D.hm_beta * sqrt(stf * mstar);
+          fn = fmax((4.0 / 3.0) * D.hm_estar * sqrt(rs) * (delta * sqrt(delta)) - gn * vn, 0.0);
+          for (int k = 0; k < 3; ++k) {
+            xi[k] = (xi[k] - xn * nn[k]) + vt[k] * dt;
+            ft[k] = stf * xi[k] + gt * vt[k];
+          }
+          const double ftn = sqrt(ft[0] * ft[0] + ft[1] * ft[1] + ft[2] * ft[2]);
+          const double lim = D.hm_mu * fn;
+          if (ftn > lim) {
+            const double sc = lim / ftn;
+            for (int k = 0; k < 3; ++k) {
+              ft[k] *= sc;
+              xi[k] = (ft[k] - gt * vt[k]) / stf;
+            }
           }
         }
         double f[3], tq[3];
@@ -1608,7 +1635,7 @@ __global__ void __launch_bounds__(64) k_bed_step(const InstDesc* __restrict__ de
         cross3(lp, f, tq);
         for (int k = 0; k < 3; ++k) {
           F[k] += f[k];
-          Tq[k] += tq[k];
+          Tq[k] += tq[k] + roll[k];
         }
         ++contacts;
         if (nnew < HM_SLOTS) {

@@ -18,6 +18,7 @@ STATUS_NAMES = {
     LP_UNSUPPORTED: "unsupported",
 }
 LP_SLUMP, LP_HYDROSTATIC, LP_DAM_BREAK, LP_COUPLED_PATCH = range(4)
+LP_BED_HERTZ_MINDLIN, LP_BED_LINEAR = range(2)
 LP_PASTE, LP_LIQUID = range(2)
 FIXTURES = {"slump": LP_SLUMP, "hydrostatic": LP_HYDROSTATIC, "dam_break": LP_DAM_BREAK,
             "coupled_patch": LP_COUPLED_PATCH}
@@ -82,6 +83,10 @@ class FixtureSpec(C.Structure):
         ("hm_poisson", C.c_double),
         ("hm_friction", C.c_double),
         ("hm_restitution", C.c_double),
+        ("bed_law", C.c_int32),
+        ("_pad4", C.c_int32),
+        ("dem_stiffness", C.c_double),
+        ("dem_rolling", C.c_double),
     ]
 
 

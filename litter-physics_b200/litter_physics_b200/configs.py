@@ -113,7 +113,8 @@ def config3(count: int = 256, seed: int = 2024) -> list[_abi.FixtureSpec]:
 
 
 def pellet_bed(cells: int = 128, layer_cells: int = 8, pellets: int = 512, seed: int = 7, dt: float = 5e-5,
-               domain_m: float = 1.0, young: float = 5e6, region=None, gravity: float = -9.81) -> _abi.FixtureSpec:
+               domain_m: float = 1.0, young: float = 5e6, region=None, gravity: float = -9.81,
+               law: str = "hertz_mindlin", dem_stiffness: float = 1000.0, dem_rolling: float = 0.05) -> _abi.FixtureSpec:
     """Config 4 (extension): an HB paste layer with config-0 material under a bed of rigid pine pellets.
 
     Paste: a full-width layer `layer_cells` cells thick at 8 particles per cell (128 x 128 x 8
@@ -126,6 +127,11 @@ def pellet_bed(cells: int = 128, layer_cells: int = 8, pellets: int = 512, seed:
     contact is the reference's spring-dashpot.  The config's 3 mm radius is below the
     reference's 1.5 dx resolution rule for the coupled patch (dx = 7.8 mm), which the bed does
     not apply.
+
+    `law="linear"` replaces Hertz-Mindlin by the household DEM's contact law (dem.rs:789-834):
+    a linear spring-dashpot of `dem_stiffness` N/m (1000 N/m keeps the reference's stable step
+    0.1 sqrt(m/k) above 5e-5 s), a tangential spring of 2/7 of it with Coulomb sliding, and
+    rolling resistance `dem_rolling`, with the same friction and restitution.
     """
     dx = domain_m / cells
     e, nu = young_poisson(2e4, 1e5)
@@ -147,6 +153,10 @@ def pellet_bed(cells: int = 128, layer_cells: int = 8, pellets: int = 512, seed:
     s.bed_lo[:] = list(lo)
     s.bed_hi[:] = list(hi)
     s.hm_young, s.hm_poisson, s.hm_friction, s.hm_restitution = young, 0.3, 0.5, 0.3
+    if law == "linear":
+        s.bed_law, s.dem_stiffness, s.dem_rolling = _abi.LP_BED_LINEAR, dem_stiffness, dem_rolling
+    elif law != "hertz_mindlin":
+        raise ValueError(f"unknown contact law '{law}'")
     return s
 
 

@@ -902,6 +902,9 @@ struct Simulation {
   std::vector<Pellet> bed;
   std::vector<std::vector<HmEntry>> hist;
   double hm_estar = 0, hm_gstar = 0, hm_mu = 0, hm_beta = 0, bed_rb = 0;
+  // linear contact law of the household DEM (dem.rs:95-127): stiffness, damping ratio, rolling
+  int bed_law = 0;
+  double dem_kn = 0, dem_zeta = 0, dem_mur = 0;
   double bed_contact_work = 0.0;
   int bed_contacts = 0;
   uint64_t bed_overflow = 0;
@@ -1057,8 +1060,13 @@ struct Simulation {
       limit = std::fmin(limit, cfg.contact.stable_dt(b.mass));
       double ps = norm(b.velocity);
       if (ps > 0.0) limit = std::fmin(limit, cfg.cfl * dx / ps);
-      double kc = 2.0 * hm_estar * std::sqrt(0.5 * b.radius * 0.05 * b.radius);
-      limit = std::fmin(limit, 0.2 * std::sqrt(0.5 * b.mass / kc));
+      if (bed_law == LP_BED_LINEAR) {
+        // World::stable_dt (dem.rs:509-520)
+        limit = std::fmin(limit, 0.1 * std::sqrt(b.mass / dem_kn));
+      } else {
+        double kc = 2.0 * hm_estar * std::sqrt(0.5 * b.radius * 0.05 * b.radius);
+        limit = std::fmin(limit, 0.2 * std::sqrt(0.5 * b.mass / kc));
+      }
     }
     return limit;
   }
@@ -1352,10 +1360,6 @@ struct Simulation {
           V3 vrel = sub(add(Q.velocity, cross(omq, lq)), vp);
           double vn = dot(vrel, nn);
           V3 vt = sub(vrel, mul(nn, vn));
-          double sq = std::sqrt(rs * delta);
-          double sn = 2.0 * hm_estar * sq, stf = 8.0 * hm_gstar * sq;
-          double gn = -k56 * hm_beta * std::sqrt(sn * mstar), gt = -k56 * hm_beta * std::sqrt(stf * mstar);
-          double fn = std::fmax((4.0 / 3.0) * hm_estar * std::sqrt(rs) * (delta * std::sqrt(delta)) - gn * vn, 0.0);
           V3 xi = zero3();
           for (const HmEntry& h : hist[p])
             if (h.other == (int)q && h.a == (int)a && h.b == (int)b) {
@@ -1363,22 +1367,51 @@ struct Simulation {
               break;
             }
           double xn = dot(xi, nn);
-          V3 ft;
-          for (int k = 0; k < 3; ++k) {
-            xi[k] = (xi[k] - xn * nn[k]) + vt[k] * dt;
-            ft[k] = stf * xi[k] + gt * vt[k];
-          }
-          double ftn = norm(ft), lim = hm_mu * fn;
-          if (ftn > lim) {
-            double sc = lim / ftn;
+          V3 ft, roll = zero3();
+          double fn;
+          if (bed_law == LP_BED_LINEAR) {
+            // World::contact_force (dem.rs:789-834) with P as the first body: the reference's
+            // normal points at P (-nn) and its relative velocity is v_P - v_Q (-vrel), so its
+            // tangential velocity is -vt while v_n keeps its sign
+            const double cn = 2.0 * dem_zeta * std::sqrt(dem_kn * mstar);
+            const double kt = (2.0 / 7.0) * dem_kn, ct = std::sqrt(2.0 / 7.0) * cn;
+            fn = std::fmax(dem_kn * delta - cn * vn, 0.0);
             for (int k = 0; k < 3; ++k) {
-              ft[k] *= sc;
-              xi[k] = (ft[k] - gt * vt[k]) / stf;
+              xi[k] = (xi[k] - xn * nn[k]) - vt[k] * dt;
+              ft[k] = -(xi[k] * kt) + vt[k] * ct;
+            }
+            double ftn = norm(ft), lim = hm_mu * fn;
+            if (ftn > lim) {
+              double sc = ftn > std::numeric_limits<double>::epsilon() ? lim / ftn : 0.0;
+              for (int k = 0; k < 3; ++k) {
+                ft[k] *= sc;
+                xi[k] = -ft[k] / kt;
+              }
+            }
+            V3 wr = sub(omp, omq);
+            double wn = norm(wr);
+            if (wn > std::numeric_limits<double>::epsilon()) roll = mul(divs(wr, -wn), dem_mur * rs * fn);
+          } else {
+            double sq = std::sqrt(rs * delta);
+            double sn = 2.0 * hm_estar * sq, stf = 8.0 * hm_gstar * sq;
+            double gn = -k56 * hm_beta * std::sqrt(sn * mstar), gt = -k56 * hm_beta * std::sqrt(stf * mstar);
+            fn = std::fmax((4.0 / 3.0) * hm_estar * std::sqrt(rs) * (delta * std::sqrt(delta)) - gn * vn, 0.0);
+            for (int k = 0; k < 3; ++k) {
+              xi[k] = (xi[k] - xn * nn[k]) + vt[k] * dt;
+              ft[k] = stf * xi[k] + gt * vt[k];
+            }
+            double ftn = norm(ft), lim = hm_mu * fn;
+            if (ftn > lim) {
+              double sc = lim / ftn;
+              for (int k = 0; k < 3; ++k) {
+                ft[k] *= sc;
+                xi[k] = (ft[k] - gt * vt[k]) / stf;
+              }
             }
           }
           V3 f = sub(ft, mul(nn, fn));
           F = add(F, f);
-          T = add(T, cross(lp, f));
+          T = add(add(T, cross(lp, f)), roll);
           ++contacts;
           if ((int)next.size() < HM_SLOTS) next.push_back(HmEntry{(int)q, (int)a, (int)b, xi});
           else ++overflow;
@@ -1792,8 +1825,18 @@ bool validate_spec(const lp_fixture_spec& s, std::string& err) {
       err = "a pellet bed needs the slump fixture, a pellet geometry and at most 4096 pellets";
       return false;
     }
-    if (!(s.hm_young > 0.0) || !(s.hm_poisson >= 0.0 && s.hm_poisson < 0.5) || !(s.hm_friction >= 0.0) ||
-        !(s.hm_restitution > 0.0 && s.hm_restitution <= 1.0)) {
+    if (s.bed_law == LP_BED_LINEAR) {
+      if (!(std::isfinite(s.dem_stiffness) && s.dem_stiffness > 0.0) ||
+          !(std::isfinite(s.dem_rolling) && s.dem_rolling >= 0.0) || !(s.hm_friction >= 0.0) ||
+          !std::isfinite(s.hm_restitution)) {
+        err = "invalid linear contact parameters (stiffness > 0, rolling friction >= 0, friction >= 0, finite restitution)";
+        return false;
+      }
+    } else if (s.bed_law != LP_BED_HERTZ_MINDLIN) {
+      err = "unknown pellet-bed contact law";
+      return false;
+    } else if (!(s.hm_young > 0.0) || !(s.hm_poisson >= 0.0 && s.hm_poisson < 0.5) || !(s.hm_friction >= 0.0) ||
+               !(s.hm_restitution > 0.0 && s.hm_restitution <= 1.0)) {
       err = "invalid Hertz-Mindlin parameters (young > 0, 0 <= poisson < 0.5, friction >= 0, 0 < restitution <= 1)";
       return false;
     }
@@ -1805,6 +1848,14 @@ bool validate_spec(const lp_fixture_spec& s, std::string& err) {
 // rebounds with restitution e: in scaled units the overlap obeys
 // x'' = -max(x^1.5 + c x^0.25 x', 0), c = -sqrt(5) beta, x(0) = 0, x'(0) = 1, independent of
 // speed, masses and moduli; e = -x' at separation (RK4, step 2e-4), bisection on beta.
+// ContactParams::damping_ratio (dem.rs:112-120)
+static double dem_damping_ratio(double e) {
+  e = std::fmin(std::fmax(e, 0.0), 1.0);
+  if (e <= std::numeric_limits<double>::epsilon()) return 1.0;
+  const double l = std::log(e);
+  return std::fmin(-l / std::sqrt(M_PI * M_PI + l * l), 1.0);
+}
+
 static double hm_restitution_of(double beta) {
   const double c = -std::sqrt(5.0) * beta, h = 2e-4;
   auto acc = [c](double x, double v) {
@@ -1942,11 +1993,18 @@ bool build(const lp_fixture_spec& s, Simulation& sim, std::string& err) {
   if (s.bed_count >= 2) {
     if (!make_bed(s, L.extents(), sim.bed, err)) return false;
     sim.hist.assign(sim.bed.size(), std::vector<HmEntry>());
-    const double nu = s.hm_poisson, E = s.hm_young, G = E / (2.0 * (1.0 + nu));
-    sim.hm_estar = E / (2.0 * (1.0 - nu * nu));
-    sim.hm_gstar = G / (2.0 * (2.0 - nu));
     sim.hm_mu = s.hm_friction;
-    sim.hm_beta = hm_beta_for(s.hm_restitution);
+    sim.bed_law = s.bed_law;
+    if (s.bed_law == LP_BED_LINEAR) {
+      sim.dem_kn = s.dem_stiffness;
+      sim.dem_zeta = dem_damping_ratio(s.hm_restitution);
+      sim.dem_mur = s.dem_rolling;
+    } else {
+      const double nu = s.hm_poisson, E = s.hm_young, G = E / (2.0 * (1.0 + nu));
+      sim.hm_estar = E / (2.0 * (1.0 - nu * nu));
+      sim.hm_gstar = G / (2.0 * (2.0 - nu));
+      sim.hm_beta = hm_beta_for(s.hm_restitution);
+    }
     double hs = 0.0;
     for (double o : sim.bed[0].offsets) hs = std::fmax(hs, std::fabs(o));
     sim.bed_rb = hs + sim.bed[0].radius;
