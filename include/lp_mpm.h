@@ -296,6 +296,16 @@ lp_status lp_batch_export_particles(lp_batch* b, int32_t index, lp_particles* ou
 lp_status lp_batch_total_particles(lp_batch* b, uint64_t* out);
 lp_status lp_batch_set_warm_start(lp_batch* b, const float* weights, int32_t nweights, int32_t enable);
 lp_status lp_batch_use_graph(lp_batch* b, int32_t steps);
+/* Per-instance views, so that each instance of a batched sweep reports what the reference's
+ * sweep (python/litter_physics/sweep.py:206-262) gets from running that job alone. */
+lp_status lp_batch_get_pellet(lp_batch* b, int32_t index, lp_pellet* out, int32_t* has_pellet);
+lp_status lp_batch_observables(lp_batch* b, int32_t index, char* names, double* values, int32_t capacity,
+                               int32_t* count);
+lp_status lp_batch_energies(lp_batch* b, int32_t index, double out[9]);
+/* *state: 0 running, 1 reached its target, 2 aborted below the minimum step, 3 leaked particles
+ * beyond the padded grid; a stopped instance's reason goes to `message`.  Stopped instances
+ * stay stopped while the others advance. */
+lp_status lp_batch_instance_state(lp_batch* b, int32_t index, int32_t* state, char* message, size_t message_len);
 /* Autotuner: times the candidate tile/block shapes on the live batch and keeps the fastest. */
 lp_status lp_batch_autotune(lp_batch* b, int32_t trial_steps, char* report, size_t report_len);
 

@@ -1413,12 +1413,12 @@ lp_status lp_sim_set_pellets(lp_sim* sim, const lp_pellet* in, int32_t count) {
   E.ctrl_h[0].bed_limit = lp::bed_limit(D, B.data());
   return push_ctrl(E);
 }
-lp_status lp_sim_get_pellet(lp_sim* sim, lp_pellet* out, int32_t* has) {
-  lp_status st = pull_ctrl(sim->E);
+static lp_status get_pellet(Ensemble& E, int i, lp_pellet* out, int32_t* has) {
+  lp_status st = pull_ctrl(E);
   if (st != LP_OK) return st;
-  *has = sim->E.desc[0].has_pellet;
+  *has = E.desc[i].has_pellet;
   if (!*has) return LP_OK;
-  const lp::PelletState& P = sim->E.ctrl_h[0].pellet;
+  const lp::PelletState& P = E.ctrl_h[i].pellet;
   std::memset(out, 0, sizeof(*out));
   out->radius = P.radius;
   out->length = P.length;
@@ -1434,6 +1434,7 @@ lp_status lp_sim_get_pellet(lp_sim* sim, lp_pellet* out, int32_t* has) {
   for (int k = 0; k < P.nsph; ++k) out->sphere_offsets[k] = P.off[k];
   return LP_OK;
 }
+lp_status lp_sim_get_pellet(lp_sim* sim, lp_pellet* out, int32_t* has) { return get_pellet(sim->E, 0, out, has); }
 lp_status lp_sim_set_pellet(lp_sim* sim, const lp_pellet* in) {
   lp_status st = pull_ctrl(sim->E);
   if (st != LP_OK) return st;
@@ -1853,6 +1854,61 @@ lp_status lp_batch_get_ledger(lp_batch* b, int32_t i, lp_ledger* out) {
 lp_status lp_batch_export_particles(lp_batch* b, int32_t i, lp_particles* out) {
   if (i < 0 || i >= b->E.n) return set_error(LP_INVALID, "instance index out of range");
   return export_particles(b->E, i, out);
+}
+lp_status lp_batch_get_pellet(lp_batch* b, int32_t i, lp_pellet* out, int32_t* has) {
+  if (i < 0 || i >= b->E.n) return set_error(LP_INVALID, "instance index out of range");
+  return get_pellet(b->E, i, out, has);
+}
+lp_status lp_batch_observables(lp_batch* b, int32_t i, char* names, double* values, int32_t capacity, int32_t* count) {
+  if (i < 0 || i >= b->E.n) return set_error(LP_INVALID, "instance index out of range");
+  std::map<std::string, double> obs;
+  lp_status st = observables(b->E, i, obs);
+  if (st != LP_OK) return st;
+  int32_t n = 0;
+  for (auto& kv : obs) {
+    if (n >= capacity) break;
+    std::snprintf(names + 64 * n, 64, "%s", kv.first.c_str());
+    values[n] = kv.second;
+    ++n;
+  }
+  *count = n;
+  return LP_OK;
+}
+lp_status lp_batch_energies(lp_batch* b, int32_t i, double out[9]) {
+  if (i < 0 || i >= b->E.n) return set_error(LP_INVALID, "instance index out of range");
+  std::vector<Diag> d;
+  lp_status st = diagnostics(b->E, d);
+  if (st != LP_OK) return st;
+  st = pull_ctrl(b->E);
+  if (st != LP_OK) return st;
+  const Energies en = energies_of(b->E, i, d[i]);
+  const double v[9] = {en.ke, en.pe, en.ee, en.mech, en.mass_res, en.mom_res[0], en.mom_res[1], en.mom_res[2],
+                       en.e_res};
+  for (int k = 0; k < 9; ++k) out[k] = v[k];
+  return LP_OK;
+}
+lp_status lp_batch_instance_state(lp_batch* b, int32_t i, int32_t* state, char* message, size_t message_len) {
+  if (i < 0 || i >= b->E.n) return set_error(LP_INVALID, "instance index out of range");
+  lp_status st = pull_ctrl(b->E);
+  if (st != LP_OK) return st;
+  const Control& c = b->E.ctrl_h[i];
+  char buf[256] = "";
+  switch (c.status) {
+    case lp::S_RUNNING: *state = 0; break;
+    case lp::S_REACHED: *state = 1; break;
+    case lp::S_MIN_STEP:
+      *state = 2;
+      std::snprintf(buf, sizeof(buf),
+                    "solver aborted at t='%.17g' s: step '%.17g' s below minimum after '%llu' rejections; last failure code %d",
+                    c.time, c.dt, (unsigned long long)c.rejected_steps, c.last_fail);
+      break;
+    default:
+      *state = 3;
+      std::snprintf(buf, sizeof(buf), "closed fixture leaked particles beyond the padded grid (outflow)");
+      break;
+  }
+  if (message && message_len) std::snprintf(message, message_len, "%s", buf);
+  return LP_OK;
 }
 lp_status lp_batch_total_particles(lp_batch* b, uint64_t* out) {
   lp_status st = pull_ctrl(b->E);

@@ -114,6 +114,10 @@ def lib():
         "lp_batch_set_warm_start": ([P, F, I32, I32], I32),
         "lp_batch_use_graph": ([P, I32], I32),
         "lp_batch_autotune": ([P, I32, C.c_char_p, C.c_size_t], I32),
+        "lp_batch_get_pellet": ([P, I32, C.POINTER(_abi.Pellet), C.POINTER(I32)], I32),
+        "lp_batch_observables": ([P, I32, C.c_char_p, D, I32, C.POINTER(I32)], I32),
+        "lp_batch_energies": ([P, I32, D], I32),
+        "lp_batch_instance_state": ([P, I32, C.POINTER(I32), C.c_char_p, C.c_size_t], I32),
         "lp_hb_return_batch": ([I64, D, D, D, D, D, D, C.c_double, F, I32, D, C.POINTER(I32)], I32),
         "lp_update_paste_batch": ([I64, D, C.POINTER(_abi.Material), C.c_double, D, D, D, D, D, C.POINTER(I32)], I32),
         "lp_update_liquid_batch": ([I64, D, D, C.POINTER(_abi.Material), C.c_double, D, D, D, C.POINTER(I32)], I32),

@@ -778,3 +778,98 @@ def run(req: dict, resume=None) -> dict:
         if _time.monotonic() - started >= budget:
             output["status"] = "budget_exhausted"
         return output
+
+
+def run_batch(reqs: list, clock=None) -> list:
+    """`research::run` for several requests in one batched launch (extension).
+
+    The requests must share `duration_s`, `record_interval_s` and the fixture kind.  Entry k of
+    the result is what `run(reqs[k])` returns for that request alone -- batched instances step
+    exactly like single simulations -- or the RunError it would raise.  The wall budget is the
+    smallest `max_wall_time_s` of the group.  Invalid requests raise SpecError before anything
+    runs."""
+    import time as _time
+
+    from ._lib import LPError
+    from .sim import Batch
+
+    clock = clock or _time.monotonic
+    started = clock()
+    if not reqs:
+        return []
+    specs = [spec_from_request(r) for r in reqs]
+    duration = float(reqs[0]["duration_s"])
+    interval = float(reqs[0]["record_interval_s"])
+    if any(float(r["duration_s"]) != duration or float(r["record_interval_s"]) != interval for r in reqs):
+        raise SpecError("batched requests must share `duration_s` and `record_interval_s`")
+    budget = min(float(r["max_wall_time_s"]) for r in reqs)
+    try:
+        batch = Batch(specs)
+    except LPError as e:
+        raise RunError(e.message) from e
+    n = len(reqs)
+    members = [batch.member(i) for i in range(n)]
+    frames: list = [[] for _ in range(n)]
+    metrics: list = [[] for _ in range(n)]
+    errors: list = [None] * n
+
+    def alive() -> list:
+        return [i for i in range(n) if errors[i] is None]
+
+    try:
+        for i in range(n):
+            record(members[i], specs[i], frames[i], metrics[i])
+        next_record = 1
+        completed = batch.counters(0).time >= duration
+        while not completed and alive():
+            target = min(float(next_record) * interval, duration)
+            try:
+                res = batch.advance_while(target, lambda: clock() - started < budget)
+            except LPError as e:
+                raise RunError(e.message) from e
+            if res == "budget":
+                break
+            for i in alive():
+                state, why = batch.state(i)
+                if state in ("min_step", "outflow"):
+                    errors[i] = RunError(why)
+                    continue
+                try:
+                    parts = members[i].particles()
+                    check_closed_state(members[i], specs[i], parts)
+                    record(members[i], specs[i], frames[i], metrics[i], parts)
+                except RunError as e:
+                    errors[i] = e
+            next_record += 1
+            live = alive()
+            completed = bool(live) and members[live[0]].time >= duration
+        out: list = []
+        for i in range(n):
+            if errors[i] is not None:
+                out.append(errors[i])
+                continue
+            m = members[i]
+            try:
+                check_closed_state(m, specs[i])
+                checkpoint = {"schema_version": SCHEMA_VERSION, "mode": "research", "request": reqs[i],
+                              "time_s": m.time, "state": snapshot(m, next_record)}
+                observables = m.observables()
+                if any(not math.isfinite(v) for v in observables.values()):
+                    raise RunError("research observables became nonfinite")
+            except RunError as e:
+                out.append(e)
+                continue
+            done = m.time >= duration
+            output = {
+                "schema_version": SCHEMA_VERSION, "mode": "research",
+                "status": "completed" if done else "budget_exhausted",
+                "fidelity": "research_unvalidated", "time_s": m.time,
+                "frames": frames[i], "metrics": metrics[i], "observables": observables,
+                "checkpoint": checkpoint, "diagnostics": list(_DIAGNOSTICS),
+            }
+            if clock() - started >= budget:
+                output["status"] = "budget_exhausted"
+            out.append(output)
+        return out
+    finally:
+        batch.close()

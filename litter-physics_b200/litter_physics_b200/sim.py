@@ -245,6 +245,54 @@ class Batch:
         check(lib().lp_batch_advance(self._h, float(target_time), _abi.KEEP_GOING_FN(0), None, C.byref(reached)))
         return bool(reached.value)
 
+    def advance_while(self, target_time: float, should_continue: Callable[[], bool] | None = None) -> str:
+        """Advance every running instance toward `target_time`.  Returns "budget" at a resumable
+        budget stop, else "done"; instances that stop on their own (min step, outflow) stay
+        stopped and are reported by `state(i)`, not raised."""
+        reached = C.c_int32()
+        cb = _abi.KEEP_GOING_FN(lambda _ctx: 1 if should_continue() else 0) if should_continue else \
+            _abi.KEEP_GOING_FN(0)
+        st = lib().lp_batch_advance(self._h, float(target_time), cb, None, C.byref(reached))
+        if st == _abi.LP_BUDGET:
+            return "budget"
+        if st in (_abi.LP_OK, _abi.LP_MIN_STEP) or (st == _abi.LP_INVALID and "outflow" in
+                                                   lib().lp_last_error().decode(errors="replace")):
+            return "done"
+        check(st)
+        return "done"
+
+    def state(self, i: int) -> tuple[str, str]:
+        """("running" | "reached" | "min_step" | "outflow", reason) of instance i."""
+        st = C.c_int32()
+        msg = C.create_string_buffer(256)
+        check(lib().lp_batch_instance_state(self._h, i, C.byref(st), msg, 256))
+        return ("running", "reached", "min_step", "outflow")[st.value], msg.value.decode()
+
+    def pellet(self, i: int) -> _abi.Pellet | None:
+        p = _abi.Pellet()
+        has = C.c_int32()
+        check(lib().lp_batch_get_pellet(self._h, i, C.byref(p), C.byref(has)))
+        return p if has.value else None
+
+    def observables(self, i: int) -> dict:
+        cap = 128
+        names = C.create_string_buffer(64 * cap)
+        values = (C.c_double * cap)()
+        n = C.c_int32()
+        check(lib().lp_batch_observables(self._h, i, names, values, cap, C.byref(n)))
+        raw = names.raw
+        return {raw[64 * k:64 * k + 64].split(b"\0", 1)[0].decode(): values[k] for k in range(n.value)}
+
+    def energies(self, i: int) -> dict:
+        out = (C.c_double * 9)()
+        check(lib().lp_batch_energies(self._h, i, out))
+        keys = ["kinetic", "potential", "elastic", "mechanical", "mass_residual", "momentum_residual_x",
+                "momentum_residual_y", "momentum_residual_z", "energy_residual"]
+        return dict(zip(keys, list(out)))
+
+    def member(self, i: int) -> "BatchMember":
+        return BatchMember(self, i)
+
     def run_substeps(self, steps: int) -> None:
         check(lib().lp_batch_run_substeps(self._h, int(steps)))
 
@@ -291,4 +339,39 @@ class Batch:
         check(lib().lp_batch_set_warm_start(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size, 1))
 
 
-__all__ = ["Simulation", "Batch", "LPError"]
+class BatchMember:
+    """Read-only view of one batch instance with the `Simulation` accessors the research driver
+    uses (particles, ledger, counters, time, pellet, observables, residuals)."""
+
+    def __init__(self, batch: Batch, index: int):
+        self.batch, self.index = batch, index
+
+    def particles(self) -> dict:
+        return self.batch.particles(self.index)
+
+    @property
+    def ledger(self) -> _abi.Ledger:
+        return self.batch.ledger(self.index)
+
+    @property
+    def counters(self) -> _abi.Counters:
+        return self.batch.counters(self.index)
+
+    @property
+    def time(self) -> float:
+        return self.counters.time
+
+    def pellet(self) -> _abi.Pellet | None:
+        return self.batch.pellet(self.index)
+
+    def observables(self) -> dict:
+        return self.batch.observables(self.index)
+
+    def energies(self) -> dict:
+        return self.batch.energies(self.index)
+
+    def mass_residual(self) -> float:
+        return self.energies()["mass_residual"]
+
+
+__all__ = ["Simulation", "Batch", "BatchMember", "LPError"]
