@@ -395,6 +395,10 @@ struct Ensemble {
   std::vector<Control> ctrl_h;
   double* d_diag = nullptr;
   double* d_audit = nullptr;  // energy-audit partials, 6 per grid-update CTA
+  // staging of host-layout particle chunks for import / export (38 doubles + 1 id per particle)
+  double* d_stage = nullptr;
+  int64_t stage_particles = 0;
+  unsigned long long* d_bad = nullptr;
   float* d_mlp = nullptr;
   lp::MlpPacked* d_mlp_pk = nullptr;
   int warm = 0;
@@ -962,6 +966,45 @@ const char* fail_text(int f) {
 }
 
 // ---------------------------------------------------------------- export / import
+// Particles per staging chunk of import and export: 2^21 x 308 B = 646 MB of device memory.
+static const int64_t STAGE_CHUNK = (int64_t)1 << 21;
+
+// Device staging for `count` particles; carves the host-layout arrays out of it.
+static lp_status stage_chunk(Ensemble& E, int64_t count, lp::HostParticleChunk& h) {
+  const int64_t want = std::min<int64_t>(std::max<int64_t>(count, 1), STAGE_CHUNK);
+  if (E.stage_particles < want) {
+    if (E.d_stage) {
+      cudaStreamSynchronize(E.stream);
+      cudaFree(E.d_stage);
+      E.allocs.erase(std::remove(E.allocs.begin(), E.allocs.end(), (void*)E.d_stage), E.allocs.end());
+      E.d_stage = nullptr;
+    }
+    lp_status st = E.alloc(&E.d_stage, (size_t)want * 39);
+    if (st != LP_OK) return st;
+    E.stage_particles = want;
+  }
+  if (!E.d_bad) {
+    lp_status st = E.alloc(&E.d_bad, 1);
+    if (st != LP_OK) return st;
+  }
+  const int64_t c = E.stage_particles;
+  double* b = E.d_stage;
+  h.position = b;
+  h.velocity = b + 3 * c;
+  h.affine = b + 6 * c;
+  h.deformation = b + 15 * c;
+  h.kirchhoff = b + 24 * c;
+  h.volume_ratio = b + 33 * c;
+  h.plastic_strain = b + 34 * c;
+  h.mass = b + 35 * c;
+  h.volume0 = b + 36 * c;
+  h.yield_stress = b + 37 * c;
+  h.id = reinterpret_cast<uint32_t*>(b + 38 * c);
+  return LP_OK;
+}
+
+// Export instance i's committed particles into the caller's FP64 arrays (null fields are
+// skipped): chunks are converted on the device and copied back one array at a time.
 lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
   lp_status st = pull_ctrl(E);
   if (st != LP_OK) return st;
@@ -969,41 +1012,41 @@ lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
   const InstDesc& D = E.desc[i];
   const int64_t n = c.count;
   if ((int64_t)out->count < n) return set_error(LP_INVALID, "particle buffer too small");
-  const float* cur = E.A.st[c.parity];
-  std::vector<float> buf((size_t)lp::NCOMP * n);
-  for (int comp = 0; comp < lp::NCOMP; ++comp)
-    CUDA_CK(cudaMemcpyAsync(buf.data() + (size_t)comp * n, cur + (size_t)comp * E.A.cap + D.slot_off, sizeof(float) * n,
-                            cudaMemcpyDeviceToHost, E.stream));
-  std::vector<uint32_t> ids(n);
-  CUDA_CK(cudaMemcpyAsync(ids.data(), E.A.id[c.parity] + D.slot_off, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost,
-                          E.stream));
-  CUDA_CK(cudaStreamSynchronize(E.stream));
-  auto g = [&](int comp, int64_t p) { return (double)buf[(size_t)comp * n + p]; };
-  for (int64_t p = 0; p < n; ++p) {
-    if (out->id) out->id[p] = ids[p];
-    for (int a = 0; a < 3; ++a) {
-      if (out->position) out->position[3 * p + a] = g(lp::C_X + a, p);
-      if (out->velocity) out->velocity[3 * p + a] = g(lp::C_V + a, p);
-    }
-    for (int a = 0; a < 9; ++a) {
-      if (out->affine) out->affine[9 * p + a] = g(lp::C_C + a, p);
-      if (out->deformation)
-        out->deformation[9 * p + a] = D.kind == 0 ? g(lp::C_H + a, p) + ((a % 4) == 0 ? 1.0 : 0.0) : ((a % 4) == 0 ? 1.0 : 0.0);
-    }
-    if (out->kirchhoff) {
-      const int map[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
-      for (int a = 0; a < 9; ++a) out->kirchhoff[9 * p + a] = g(lp::C_TAU + map[a], p);
-    }
-    if (out->volume_ratio) out->volume_ratio[p] = D.kind == 1 ? 1.0 + g(lp::C_JM1, p) : 1.0;
-    if (out->plastic_strain) out->plastic_strain[p] = g(lp::C_EP, p);
-    if (out->mass) out->mass[p] = g(lp::C_M, p);
-    if (out->volume0) out->volume0[p] = g(lp::C_V0, p);
-    if (out->yield_stress) out->yield_stress[p] = D.per_particle_yield ? g(lp::C_YS, p) : D.yield;
+  lp::HostParticleChunk h;
+  st = stage_chunk(E, n, h);
+  if (st != LP_OK) return st;
+  for (int64_t first = 0; first < n; first += E.stage_particles) {
+    const int64_t m = std::min(E.stage_particles, n - first);
+    lp::launch_export(h, m, first, E.A.st[c.parity], E.A.id[c.parity], E.A.cap, D.slot_off, D.kind == 0,
+                      D.per_particle_yield, D.yield, E.stream);
+    CUDA_CK(cudaGetLastError());
+    auto back = [&](void* dst, const void* src, size_t bytes) -> lp_status {
+      if (dst) CUDA_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, E.stream));
+      return LP_OK;
+    };
+    const size_t d1 = sizeof(double) * (size_t)m;
+    if (back(out->id ? out->id + first : nullptr, h.id, sizeof(uint32_t) * (size_t)m) != LP_OK ||
+        back(out->position ? out->position + 3 * first : nullptr, h.position, 3 * d1) != LP_OK ||
+        back(out->velocity ? out->velocity + 3 * first : nullptr, h.velocity, 3 * d1) != LP_OK ||
+        back(out->affine ? out->affine + 9 * first : nullptr, h.affine, 9 * d1) != LP_OK ||
+        back(out->deformation ? out->deformation + 9 * first : nullptr, h.deformation, 9 * d1) != LP_OK ||
+        back(out->kirchhoff ? out->kirchhoff + 9 * first : nullptr, h.kirchhoff, 9 * d1) != LP_OK ||
+        back(out->volume_ratio ? out->volume_ratio + first : nullptr, h.volume_ratio, d1) != LP_OK ||
+        back(out->plastic_strain ? out->plastic_strain + first : nullptr, h.plastic_strain, d1) != LP_OK ||
+        back(out->mass ? out->mass + first : nullptr, h.mass, d1) != LP_OK ||
+        back(out->volume0 ? out->volume0 + first : nullptr, h.volume0, d1) != LP_OK ||
+        back(out->yield_stress ? out->yield_stress + first : nullptr, h.yield_stress, d1) != LP_OK)
+      return LP_DEVICE;
+    CUDA_CK(cudaStreamSynchronize(E.stream));
   }
   out->count = (uint64_t)n;
   return LP_OK;
 }
 
+// Import the caller's FP64 arrays as instance i's committed particles.  They are converted on
+// the device into the instance's scratch (other-parity) buffers, which become the committed
+// ones only when every particle has finite positive mass and volume and finite kinematics, so a
+// refused import leaves the simulation as it was.
 lp_status import_particles(Ensemble& E, int i, const lp_particles* in) {
   lp_status st = pull_ctrl(E);
   if (st != LP_OK) return st;
@@ -1011,41 +1054,44 @@ lp_status import_particles(Ensemble& E, int i, const lp_particles* in) {
   const InstDesc& D = E.desc[i];
   const int64_t n = (int64_t)in->count;
   if (n > D.slot_cap) return set_error(LP_INVALID, "imported particle count exceeds the instance capacity");
-  for (int64_t p = 0; p < n; ++p) {
-    bool ok = std::isfinite(in->mass[p]) && in->mass[p] > 0.0 && std::isfinite(in->volume0[p]) && in->volume0[p] > 0.0;
-    for (int a = 0; a < 3 && ok; ++a) ok = std::isfinite(in->position[3 * p + a]) && std::isfinite(in->velocity[3 * p + a]);
-    if (!ok) return set_error(LP_INVALID, "particle id '" + std::to_string(in->id[p]) + "' has non-finite state");
+  if (n > 0 && (!in->id || !in->position || !in->velocity || !in->affine || !in->deformation || !in->kirchhoff ||
+                !in->volume_ratio || !in->plastic_strain || !in->mass || !in->volume0))
+    return set_error(LP_INVALID, "imported particles need every array but yield_stress");
+  lp::HostParticleChunk h;
+  st = stage_chunk(E, n, h);
+  if (st != LP_OK) return st;
+  const int par = c.parity ^ 1;
+  const unsigned long long none = ~0ull;
+  CUDA_CK(cudaMemcpyAsync(E.d_bad, &none, sizeof(none), cudaMemcpyHostToDevice, E.stream));
+  for (int64_t first = 0; first < n; first += E.stage_particles) {
+    const int64_t m = std::min(E.stage_particles, n - first);
+    const size_t d1 = sizeof(double) * (size_t)m;
+    CUDA_CK(cudaMemcpyAsync(h.id, in->id + first, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.position, in->position + 3 * first, 3 * d1, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.velocity, in->velocity + 3 * first, 3 * d1, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.affine, in->affine + 9 * first, 9 * d1, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.deformation, in->deformation + 9 * first, 9 * d1, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.kirchhoff, in->kirchhoff + 9 * first, 9 * d1, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.volume_ratio, in->volume_ratio + first, d1, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.plastic_strain, in->plastic_strain + first, d1, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.mass, in->mass + first, d1, cudaMemcpyHostToDevice, E.stream));
+    CUDA_CK(cudaMemcpyAsync(h.volume0, in->volume0 + first, d1, cudaMemcpyHostToDevice, E.stream));
+    lp::HostParticleChunk hc = h;
+    if (in->yield_stress)
+      CUDA_CK(cudaMemcpyAsync(h.yield_stress, in->yield_stress + first, d1, cudaMemcpyHostToDevice, E.stream));
+    else
+      hc.yield_stress = nullptr;
+    lp::launch_import(hc, m, first, E.A.st[par], E.A.id[par], E.A.cap, D.slot_off, D.yield, E.d_bad, E.stream);
+    CUDA_CK(cudaGetLastError());
+    // the staging arrays are reused by the next chunk's copies
+    CUDA_CK(cudaStreamSynchronize(E.stream));
   }
-  std::vector<float> buf((size_t)lp::NCOMP * n, 0.0f);
-  auto put = [&](int comp, int64_t p, double v) { buf[(size_t)comp * n + p] = (float)v; };
-  for (int64_t p = 0; p < n; ++p) {
-    for (int a = 0; a < 3; ++a) {
-      put(lp::C_X + a, p, in->position[3 * p + a]);
-      put(lp::C_V + a, p, in->velocity[3 * p + a]);
-    }
-    for (int a = 0; a < 9; ++a) {
-      put(lp::C_C + a, p, in->affine[9 * p + a]);
-      put(lp::C_H + a, p, in->deformation[9 * p + a] - ((a % 4) == 0 ? 1.0 : 0.0));
-    }
-    const double* T = in->kirchhoff + 9 * p;
-    put(lp::C_TAU + 0, p, T[0]);
-    put(lp::C_TAU + 1, p, T[4]);
-    put(lp::C_TAU + 2, p, T[8]);
-    put(lp::C_TAU + 3, p, 0.5 * (T[1] + T[3]));
-    put(lp::C_TAU + 4, p, 0.5 * (T[2] + T[6]));
-    put(lp::C_TAU + 5, p, 0.5 * (T[5] + T[7]));
-    put(lp::C_EP, p, in->plastic_strain[p]);
-    put(lp::C_M, p, in->mass[p]);
-    put(lp::C_V0, p, in->volume0[p]);
-    put(lp::C_YS, p, in->yield_stress ? in->yield_stress[p] : D.yield);
-    put(lp::C_JM1, p, in->volume_ratio[p] - 1.0);
-  }
-  float* cur = E.A.st[c.parity];
-  for (int comp = 0; comp < lp::NCOMP; ++comp)
-    CUDA_CK(cudaMemcpyAsync(cur + (size_t)comp * E.A.cap + D.slot_off, buf.data() + (size_t)comp * n, sizeof(float) * n,
-                            cudaMemcpyHostToDevice, E.stream));
-  CUDA_CK(cudaMemcpyAsync(E.A.id[c.parity] + D.slot_off, in->id, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, E.stream));
+  unsigned long long bad = none;
+  CUDA_CK(cudaMemcpyAsync(&bad, E.d_bad, sizeof(bad), cudaMemcpyDeviceToHost, E.stream));
   CUDA_CK(cudaStreamSynchronize(E.stream));
+  if (bad != none)
+    return set_error(LP_INVALID, "particle id '" + std::to_string(in->id[bad]) + "' has non-finite state");
+  c.parity = par;
   c.count = n;
   st = push_ctrl(E);
   if (st != LP_OK) return st;

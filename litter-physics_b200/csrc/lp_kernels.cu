@@ -2430,6 +2430,74 @@ __global__ void k_diagnostics(const InstDesc* __restrict__ desc, const Control* 
 }
 
 
+// ============================================================== host-layout import / export
+// Conversion between the reference's FP64 particle arrays (ParticleSet layout, matrices
+// row-major) staged in device memory and the FP32 component-major state, one thread per
+// particle of a chunk.  The FP64 -> FP32 roundings are those of a host-side cast.
+__global__ void k_import(HostParticleChunk h, int64_t n, int64_t first, float* __restrict__ dst,
+                         uint32_t* __restrict__ ids, int64_t cap, int64_t slot_off, double yield_default,
+                         unsigned long long* __restrict__ bad) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int64_t k = slot_off + first + p;
+  bool ok = isfinite(h.mass[p]) && h.mass[p] > 0.0 && isfinite(h.volume0[p]) && h.volume0[p] > 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double x = h.position[3 * p + a], v = h.velocity[3 * p + a];
+    ok = ok && isfinite(x) && isfinite(v);
+    dst[(C_X + a) * cap + k] = (float)x;
+    dst[(C_V + a) * cap + k] = (float)v;
+  }
+  if (!ok) atomicMin(bad, (unsigned long long)(first + p));
+#pragma unroll
+  for (int a = 0; a < 9; ++a) {
+    dst[(C_C + a) * cap + k] = (float)h.affine[9 * p + a];
+    dst[(C_H + a) * cap + k] = (float)(h.deformation[9 * p + a] - ((a % 4) == 0 ? 1.0 : 0.0));
+  }
+  const double* T = h.kirchhoff + 9 * p;
+  dst[(C_TAU + 0) * cap + k] = (float)T[0];
+  dst[(C_TAU + 1) * cap + k] = (float)T[4];
+  dst[(C_TAU + 2) * cap + k] = (float)T[8];
+  dst[(C_TAU + 3) * cap + k] = (float)(0.5 * (T[1] + T[3]));
+  dst[(C_TAU + 4) * cap + k] = (float)(0.5 * (T[2] + T[6]));
+  dst[(C_TAU + 5) * cap + k] = (float)(0.5 * (T[5] + T[7]));
+  dst[C_EP * cap + k] = (float)h.plastic_strain[p];
+  dst[C_M * cap + k] = (float)h.mass[p];
+  dst[C_V0 * cap + k] = (float)h.volume0[p];
+  dst[C_YS * cap + k] = (float)(h.yield_stress ? h.yield_stress[p] : yield_default);
+  dst[C_JM1 * cap + k] = (float)(h.volume_ratio[p] - 1.0);
+  ids[k] = h.id[p];
+}
+
+__global__ void k_export(HostParticleChunk h, int64_t n, int64_t first, const float* __restrict__ src,
+                         const uint32_t* __restrict__ ids, int64_t cap, int64_t slot_off, int paste,
+                         int per_particle_yield, double yield_default) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int64_t k = slot_off + first + p;
+  auto g = [&](int comp) { return (double)src[comp * cap + k]; };
+  h.id[p] = ids[k];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    h.position[3 * p + a] = g(C_X + a);
+    h.velocity[3 * p + a] = g(C_V + a);
+  }
+#pragma unroll
+  for (int a = 0; a < 9; ++a) {
+    const double eye = (a % 4) == 0 ? 1.0 : 0.0;
+    h.affine[9 * p + a] = g(C_C + a);
+    h.deformation[9 * p + a] = paste ? g(C_H + a) + eye : eye;
+  }
+  const int map[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+#pragma unroll
+  for (int a = 0; a < 9; ++a) h.kirchhoff[9 * p + a] = g(C_TAU + map[a]);
+  h.volume_ratio[p] = paste ? 1.0 : 1.0 + g(C_JM1);
+  h.plastic_strain[p] = g(C_EP);
+  h.mass[p] = g(C_M);
+  h.volume0[p] = g(C_V0);
+  h.yield_stress[p] = per_particle_yield ? g(C_YS) : yield_default;
+}
+
 // ============================================================== unit kernels (host arrays API)
 // One return problem per lane; with weights, each warp starts its lanes' Newton solves from one
 // tensor-core network pass (the same call as in k_g2p).
@@ -2705,6 +2773,21 @@ int launch_update_paste_batch(int64_t n, const double* f, double mu, double lamb
 int launch_update_liquid_batch(int64_t n, const double* j, const double* grad, double bulk, double visc, double gamma,
                                double dt, double* jnew, double* tau, double* p, int* status, cudaStream_t s) {
   k_liquid_batch<<<grid_of(n, 128), 128, 0, s>>>(n, j, grad, bulk, visc, gamma, dt, jnew, tau, p, status);
+  g_launches += 1;
+  return 1;
+}
+
+int launch_import(const HostParticleChunk& h, int64_t n, int64_t first, float* dst, uint32_t* ids, int64_t cap,
+                  int64_t slot_off, double yield_default, unsigned long long* bad, cudaStream_t s) {
+  k_import<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h, n, first, dst, ids, cap, slot_off, yield_default, bad);
+  g_launches += 1;
+  return 1;
+}
+int launch_export(const HostParticleChunk& h, int64_t n, int64_t first, const float* src, const uint32_t* ids,
+                  int64_t cap, int64_t slot_off, int paste, int per_particle_yield, double yield_default,
+                  cudaStream_t s) {
+  k_export<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h, n, first, src, ids, cap, slot_off, paste, per_particle_yield,
+                                           yield_default);
   g_launches += 1;
   return 1;
 }

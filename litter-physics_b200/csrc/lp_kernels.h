@@ -79,6 +79,20 @@ int launch_state_stats(const DeviceArrays& A, cudaStream_t s);
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s);
 int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s);
 int launch_diagnostics(const DeviceArrays& A, int hydro, double h0, int dam, double* out, cudaStream_t s);
+// FP64 particle arrays of one chunk in the reference's host layout (device pointers)
+struct HostParticleChunk {
+  uint32_t* id;
+  double *position, *velocity, *affine, *deformation, *volume_ratio, *kirchhoff, *plastic_strain, *mass, *volume0,
+      *yield_stress;  // yield_stress may be null on import (instance default)
+};
+// FP64 host-layout chunk [first, first + n) of an instance <-> its FP32 component-major state.
+// Import writes dst/ids and records the smallest index whose mass, volume or kinematics are not
+// finite and positive in *bad.
+int launch_import(const HostParticleChunk& h, int64_t n, int64_t first, float* dst, uint32_t* ids, int64_t cap,
+                  int64_t slot_off, double yield_default, unsigned long long* bad, cudaStream_t s);
+int launch_export(const HostParticleChunk& h, int64_t n, int64_t first, const float* src, const uint32_t* ids,
+                  int64_t cap, int64_t slot_off, int paste, int per_particle_yield, double yield_default,
+                  cudaStream_t s);
 uint64_t kernel_launch_count();
 void configure_kernels();              // one-time function attributes (dynamic shared memory)
 void set_last_error(const char* msg);  // message returned by lp_last_error()
