@@ -435,7 +435,7 @@ __global__ void k_bin_sort(const InstDesc* __restrict__ desc, const Control* __r
 // order (deterministic, no atomics), converts to int64 fixed point, the tile's exact particle
 // totals are restored by a proportional correction, and each node component is flushed with
 // one global atomic.
-constexpr int P2G_CHUNK = 768;
+constexpr int P2G_CHUNK = 1024;
 constexpr int P2G_REC = 16;  // m, q[3], A[9], f[3]
 constexpr size_t P2G_PART_BYTES = sizeof(float4) * TB * 27;
 constexpr size_t P2G_REC_BYTES = sizeof(float) * P2G_REC * P2G_CHUNK;
