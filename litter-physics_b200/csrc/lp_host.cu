@@ -14,6 +14,7 @@
 #include <limits>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lp_mpm.h"
@@ -397,6 +398,7 @@ struct Ensemble {
   double* d_audit = nullptr;  // energy-audit partials, 6 per grid-update CTA
   // staging of host-layout particle chunks for import / export (38 doubles + 1 id per particle)
   double* d_stage = nullptr;
+  double* h_stage = nullptr;  // pinned host twin of d_stage
   int64_t stage_particles = 0;
   unsigned long long* d_bad = nullptr;
   float* d_mlp = nullptr;
@@ -411,6 +413,8 @@ struct Ensemble {
     graph = nullptr;
     for (void* p : allocs) cudaFree(p);
     allocs.clear();
+    if (h_stage) cudaFreeHost(h_stage);
+    h_stage = nullptr;
     if (own_stream) cudaStreamDestroy(own_stream);
     own_stream = nullptr;
   }
@@ -969,18 +973,26 @@ const char* fail_text(int f) {
 // Particles per staging chunk of import and export: 2^21 x 308 B = 646 MB of device memory.
 static const int64_t STAGE_CHUNK = (int64_t)1 << 21;
 
-// Device staging for `count` particles; carves the host-layout arrays out of it.
+// Device staging for `count` particles and its pinned host twin; carves the host-layout arrays
+// out of the device one.
 static lp_status stage_chunk(Ensemble& E, int64_t count, lp::HostParticleChunk& h) {
   const int64_t want = std::min<int64_t>(std::max<int64_t>(count, 1), STAGE_CHUNK);
   if (E.stage_particles < want) {
+    cudaStreamSynchronize(E.stream);
     if (E.d_stage) {
-      cudaStreamSynchronize(E.stream);
       cudaFree(E.d_stage);
       E.allocs.erase(std::remove(E.allocs.begin(), E.allocs.end(), (void*)E.d_stage), E.allocs.end());
       E.d_stage = nullptr;
     }
+    if (E.h_stage) cudaFreeHost(E.h_stage);
+    E.h_stage = nullptr;
+    E.stage_particles = 0;
     lp_status st = E.alloc(&E.d_stage, (size_t)want * 39);
     if (st != LP_OK) return st;
+    if (cudaHostAlloc((void**)&E.h_stage, sizeof(double) * 39 * (size_t)want, cudaHostAllocDefault) != cudaSuccess) {
+      E.h_stage = nullptr;
+      return set_error(LP_DEVICE, "cudaHostAlloc of the particle staging buffer failed");
+    }
     E.stage_particles = want;
   }
   if (!E.d_bad) {
@@ -1003,6 +1015,42 @@ static lp_status stage_chunk(Ensemble& E, int64_t count, lp::HostParticleChunk& 
   return LP_OK;
 }
 
+// memcpy of the listed (destination, source, bytes) spans over a few host threads
+struct CopySpan {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+static void parallel_copy(const std::vector<CopySpan>& spans) {
+  size_t total = 0;
+  for (const CopySpan& c : spans) total += c.bytes;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = (unsigned)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total >> 24));
+  auto run = [&](unsigned k) {
+    // thread k copies bytes [k total / nt, (k + 1) total / nt) of the concatenated spans
+    const size_t lo = total * k / nt, hi = total * (k + 1) / nt;
+    size_t base = 0;
+    for (const CopySpan& c : spans) {
+      const size_t a = std::max(lo, base), b = std::min(hi, base + c.bytes);
+      if (a < b) std::memcpy((char*)c.dst + (a - base), (const char*)c.src + (a - base), b - a);
+      base += c.bytes;
+    }
+  };
+  if (nt == 1) {
+    run(0);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (unsigned k = 1; k < nt; ++k) pool.emplace_back(run, k);
+  run(0);
+  for (std::thread& t : pool) t.join();
+}
+
+// the host twin of a device staging pointer
+static inline void* host_twin(const Ensemble& E, const void* dev) {
+  return (char*)E.h_stage + ((const char*)dev - (const char*)E.d_stage);
+}
+
 // Export instance i's committed particles into the caller's FP64 arrays (null fields are
 // skipped): chunks are converted on the device and copied back one array at a time.
 lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
@@ -1020,8 +1068,13 @@ lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
     lp::launch_export(h, m, first, E.A.st[c.parity], E.A.id[c.parity], E.A.cap, D.slot_off, D.kind == 0,
                       D.per_particle_yield, D.yield, E.stream);
     CUDA_CK(cudaGetLastError());
+    // device staging -> pinned twin (one copy per requested field) -> caller arrays (host threads)
+    std::vector<CopySpan> spans;
     auto back = [&](void* dst, const void* src, size_t bytes) -> lp_status {
-      if (dst) CUDA_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, E.stream));
+      if (!dst) return LP_OK;
+      void* pinned = host_twin(E, src);
+      CUDA_CK(cudaMemcpyAsync(pinned, src, bytes, cudaMemcpyDeviceToHost, E.stream));
+      spans.push_back({dst, pinned, bytes});
       return LP_OK;
     };
     const size_t d1 = sizeof(double) * (size_t)m;
@@ -1038,6 +1091,7 @@ lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
         back(out->yield_stress ? out->yield_stress + first : nullptr, h.yield_stress, d1) != LP_OK)
       return LP_DEVICE;
     CUDA_CK(cudaStreamSynchronize(E.stream));
+    parallel_copy(spans);
   }
   out->count = (uint64_t)n;
   return LP_OK;
@@ -1066,21 +1120,25 @@ lp_status import_particles(Ensemble& E, int i, const lp_particles* in) {
   for (int64_t first = 0; first < n; first += E.stage_particles) {
     const int64_t m = std::min(E.stage_particles, n - first);
     const size_t d1 = sizeof(double) * (size_t)m;
-    CUDA_CK(cudaMemcpyAsync(h.id, in->id + first, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.position, in->position + 3 * first, 3 * d1, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.velocity, in->velocity + 3 * first, 3 * d1, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.affine, in->affine + 9 * first, 9 * d1, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.deformation, in->deformation + 9 * first, 9 * d1, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.kirchhoff, in->kirchhoff + 9 * first, 9 * d1, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.volume_ratio, in->volume_ratio + first, d1, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.plastic_strain, in->plastic_strain + first, d1, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.mass, in->mass + first, d1, cudaMemcpyHostToDevice, E.stream));
-    CUDA_CK(cudaMemcpyAsync(h.volume0, in->volume0 + first, d1, cudaMemcpyHostToDevice, E.stream));
+    // caller arrays -> pinned twin (host threads) -> device staging (one copy per field)
+    std::vector<CopySpan> spans = {
+        {host_twin(E, h.id), in->id + first, sizeof(uint32_t) * (size_t)m},
+        {host_twin(E, h.position), in->position + 3 * first, 3 * d1},
+        {host_twin(E, h.velocity), in->velocity + 3 * first, 3 * d1},
+        {host_twin(E, h.affine), in->affine + 9 * first, 9 * d1},
+        {host_twin(E, h.deformation), in->deformation + 9 * first, 9 * d1},
+        {host_twin(E, h.kirchhoff), in->kirchhoff + 9 * first, 9 * d1},
+        {host_twin(E, h.volume_ratio), in->volume_ratio + first, d1},
+        {host_twin(E, h.plastic_strain), in->plastic_strain + first, d1},
+        {host_twin(E, h.mass), in->mass + first, d1},
+        {host_twin(E, h.volume0), in->volume0 + first, d1}};
     lp::HostParticleChunk hc = h;
-    if (in->yield_stress)
-      CUDA_CK(cudaMemcpyAsync(h.yield_stress, in->yield_stress + first, d1, cudaMemcpyHostToDevice, E.stream));
-    else
-      hc.yield_stress = nullptr;
+    if (in->yield_stress) spans.push_back({host_twin(E, h.yield_stress), in->yield_stress + first, d1});
+    else hc.yield_stress = nullptr;
+    parallel_copy(spans);
+    for (const CopySpan& c : spans)
+      CUDA_CK(cudaMemcpyAsync((char*)E.d_stage + ((const char*)c.dst - (const char*)E.h_stage), c.dst, c.bytes,
+                              cudaMemcpyHostToDevice, E.stream));
     lp::launch_import(hc, m, first, E.A.st[par], E.A.id[par], E.A.cap, D.slot_off, D.yield, E.d_bad, E.stream);
     CUDA_CK(cudaGetLastError());
     // the staging arrays are reused by the next chunk's copies
