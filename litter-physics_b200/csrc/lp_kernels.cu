@@ -560,15 +560,6 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
       }
     }
   }
-  if (e > s) {
-    // mark the node blocks of this bin's stencil active for this attempt
-    for (int b = 0; b < 3; ++b)
-      for (int cc = 0; cc < 3; ++cc) {
-        const int nx = bx + slab, ny = by + b, nz = bz + cc;
-        const int64_t blk = D.blk_off + ((int64_t)(nx / NB) * D.nblk[1] + ny / NB) * D.nblk[2] + nz / NB;
-        blk_epoch[blk] = (uint32_t)c.epoch;
-      }
-  }
   __syncthreads();  // the last chunk's records (aliasing part[]) are consumed
 #pragma unroll
   for (int b = 0; b < 3; ++b)
@@ -644,6 +635,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
     const int nx = tx * TX + hx, ny = ty * TY + hy, nz = tz * TZ + hz;
     if (nx < D.nodes[0] && ny < D.nodes[1] && nz < D.nodes[2]) {
       const int64_t g = node_index(D, nx, ny, nz);
+      // the node's block takes part in this attempt's grid update
+      blk_epoch[D.blk_off + ((int64_t)(nx / NB) * D.nblk[1] + ny / NB) * D.nblk[2] + nz / NB] = (uint32_t)c.epoch;
       atomic_add_ll(acc + g, nv[0]);
       atomic_add_ll(acc + node_total + g, nv[1]);
       atomic_add_ll(acc + 2 * node_total + g, nv[2]);
@@ -1899,27 +1892,33 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
 #pragma unroll
       for (int a = 0; a < 9; ++a) Cm[a] = 0.0f;
       const int lbx = base[0] - ox, lby = base[1] - oy, lbz = base[2] - oz;
+      // separable gather: per (a, b) row, z sums S0 = sum_c w_c v and S1 = sum_c w_c d_c v, then
+      // v += w_ab S0, C[:,0] += w_ab d_a S0, C[:,1] += w_ab d_b S0, C[:,2] += w_ab S1
+      const float wdz[3] = {w[2][0] * d[2][0], w[2][1] * d[2][1], w[2][2] * d[2][2]};
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
           const int row = ((lbx + a) * HY + (lby + b)) * HZ + lbz;
-          const float wab = w[0][a] * w[1][b];
+          float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f};
 #pragma unroll
           for (int cc = 0; cc < 3; ++cc) {
             const float4 nv = hv[row + cc];
-            const float ww = wab * w[2][cc];
-            const float vx = nv.x * ww, vy = nv.y * ww, vz = nv.z * ww;
-            v[0] += vx;
-            v[1] += vy;
-            v[2] += vz;
-            const float dd[3] = {d[0][a], d[1][b], d[2][cc]};
+            const float nvv[3] = {nv.x, nv.y, nv.z};
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-              Cm[0 * 3 + j] += vx * dd[j];
-              Cm[1 * 3 + j] += vy * dd[j];
-              Cm[2 * 3 + j] += vz * dd[j];
+            for (int i = 0; i < 3; ++i) {
+              s0[i] += w[2][cc] * nvv[i];
+              s1[i] += wdz[cc] * nvv[i];
             }
+          }
+          const float wab = w[0][a] * w[1][b];
+          const float wa0 = wab * d[0][a], wa1 = wab * d[1][b];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            v[i] += wab * s0[i];
+            Cm[3 * i + 0] += wa0 * s0[i];
+            Cm[3 * i + 1] += wa1 * s0[i];
+            Cm[3 * i + 2] += wab * s1[i];
           }
         }
       const float dx2_inv = 4.0f / (dx * dx);
