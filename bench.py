@@ -66,7 +66,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -77,6 +77,13 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def begin_region(self, timeout: float = 3.0) -> None:
+        """Wait for the sampler's first line, then keep only samples taken from now on."""
+        t0 = time.perf_counter()
+        while self.proc is not None and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
+        self.first = len(self.lines)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -90,7 +97,7 @@ class ClockSampler:
             self.thread.join(timeout=2)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for line in self.lines[getattr(self, "first", 0):]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -326,6 +333,7 @@ def ours(args, ws, rank, local):
         sampler = ClockSampler(local) if arm == arms[-1] else None
         if sampler:
             sampler.start()
+            sampler.begin_region()
         l0 = _lib.kernel_launches()
         torch.cuda.nvtx.range_push(f"timed_{arm}")  # ncu --nvtx-include "timed_warm/" selects these launches
         ms, accepted = time_steps(sim, args.steps, stream, torch)
@@ -447,7 +455,7 @@ def ours(args, ws, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config2", choices=["config2", "config0", "small"])
