@@ -559,7 +559,13 @@ __device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& 
   B.yz = Htr[5] + Htr[7] + (Htr[3] * Htr[6] + Htr[4] * Htr[7] + Htr[5] * Htr[8]);
   const float r = sym_norm(B);
   if (!(r <= 0.25f)) {  // large or non-finite strain: eigen-decomposition path
-    paste_update_jacobi(Htr, 0.f, 0.f, mu_d, 0.0, 0.0, 0.0, 0.0, 0.0, -1.0, true, o);
+    // the out-of-line call works on copies, so that the caller's arrays need no stack home
+    float Hj[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Hj[i] = Htr[i];
+    PasteOut oj = o;
+    paste_update_jacobi(Hj, 0.f, 0.f, mu_d, 0.0, 0.0, 0.0, 0.0, 0.0, -1.0, true, oj);
+    o = oj;
     t.path = o.fail == F_OK ? PT_JACOBI : PT_DONE;
     t.trial_eq = o.trial;
     return;
@@ -619,7 +625,12 @@ __device__ inline void paste_finish(const float Htr[9], float mu, float lambda, 
                                     PasteOut& o) {
   if (t.path == PT_DONE) return;
   if (t.path == PT_JACOBI) {
-    paste_update_jacobi(Htr, mu, lambda, mu_d, ys, k, n, dt, tol, sigma0, false, o);
+    float Hj[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Hj[i] = Htr[i];
+    PasteOut oj = o;
+    paste_update_jacobi(Hj, mu, lambda, mu_d, ys, k, n, dt, tol, sigma0, false, oj);
+    o = oj;
     return;
   }
   const Sym& dev = t.dev;

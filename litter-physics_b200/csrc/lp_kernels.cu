@@ -539,8 +539,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
       for (int a = 0; a < 9; ++a) A[a] = r[(4 + a) * P2G_CHUNK];
       float w[3][3], d[3][3];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) weights_of(r[(13 + a) * P2G_CHUNK], dx, w[a], d[a]);
-      const float wa = w[0][slab], da = d[0][slab];
+      for (int a = 1; a < 3; ++a) weights_of(r[(13 + a) * P2G_CHUNK], dx, w[a], d[a]);
+      // x weight of this thread's slab only (the expressions of weights_of for offset `slab`)
+      const float fx = r[13 * P2G_CHUNK];
+      const float ao = slab == 0 ? 1.5f - fx : (slab == 1 ? fx - 1.0f : fx - 0.5f);
+      const float wa = slab == 1 ? 0.75f - ao * ao : 0.5f * (ao * ao);
+      const float da = (fx - (float)slab) * -dx;
       float u[3];
 #pragma unroll
       for (int rr = 0; rr < 3; ++rr) u[rr] = q[rr] + A[3 * rr + 0] * da;
