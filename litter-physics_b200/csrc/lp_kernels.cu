@@ -366,17 +366,28 @@ __global__ void k_scan_apply(const uint32_t* __restrict__ count, const uint32_t*
   const int64_t chunk = blockIdx.x;
   if (!ctrl[chunk_inst[chunk]].active) return;
   const int64_t base = chunk * KEY_CHUNK;
-  // 1024 threads, one key each
+  // 1024 threads, one key each: inclusive warp scans, then a scan of the 32 warp totals
   const uint32_t v = count[base + threadIdx.x];
-  sh[threadIdx.x] = v;
-  __syncthreads();
-  for (int off = 1; off < KEY_CHUNK; off <<= 1) {
-    uint32_t add = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
-    __syncthreads();
-    sh[threadIdx.x] += add;
-    __syncthreads();
+  const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= (unsigned)off) x += y;
   }
-  start[base + threadIdx.x] = chunk_base[chunk] + sh[threadIdx.x] - v;
+  if (lane == 31) sh[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t t = sh[lane];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, t, off);
+      if (lane >= (unsigned)off) t += y;
+    }
+    sh[32 + lane] = t - sh[lane];  // exclusive prefix of the warp totals
+  }
+  __syncthreads();
+  start[base + threadIdx.x] = chunk_base[chunk] + sh[32 + wid] + x - v;
 }
 
 __global__ void k_bin_scatter(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
@@ -394,11 +405,31 @@ __global__ void k_bin_scatter(const InstDesc* __restrict__ desc, const Control* 
   perm[start[key] + r] = (uint32_t)slot;
 }
 
-// order each bin by particle id (the reference's sort key ties), making the order deterministic
+// sort n <= R slot indices in registers (unrolled insertion network; unused entries sort last)
+template <int R>
+__device__ __forceinline__ void bin_sort_small(uint32_t* __restrict__ p, int n) {
+  uint32_t v[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) v[i] = i < n ? p[i] : 0xffffffffu;
+#pragma unroll
+  for (int i = 1; i < R; ++i)
+#pragma unroll
+    for (int j = i; j > 0; --j) {
+      const uint32_t a = v[j - 1], b = v[j];
+      v[j - 1] = min(a, b);
+      v[j] = max(a, b);
+    }
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+    if (i < n) p[i] = v[i];
+}
+
+// Order each bin by slot, that is by the particles' order in the committed state, which makes the
+// binned order deterministic after the atomic scatter.  The committed state is itself in binned
+// order, so a particle keeps its place relative to the others of its bin from step to step.
 __global__ void k_bin_sort(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
                            const int* __restrict__ chunk_inst, const uint32_t* __restrict__ start,
-                           uint32_t* __restrict__ perm, const uint32_t* __restrict__ id0,
-                           const uint32_t* __restrict__ id1) {
+                           uint32_t* __restrict__ perm) {
   const int64_t key = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int inst = chunk_inst[key / KEY_CHUNK];
   const Control& c = ctrl[inst];
@@ -409,12 +440,18 @@ __global__ void k_bin_sort(const InstDesc* __restrict__ desc, const Control* __r
   const uint32_t s = start[key];
   const uint32_t e = (lk == D.nkeys - 1) ? (uint32_t)(D.slot_off + c.count) : start[key + 1];
   if (e <= s + 1) return;
-  const uint32_t* ids = c.parity ? id1 : id0;
+  if (e - s <= 8u) {  // the common case at 8 particles per cell
+    bin_sort_small<8>(perm + s, (int)(e - s));
+    return;
+  }
+  if (e - s <= 16u) {
+    bin_sort_small<16>(perm + s, (int)(e - s));
+    return;
+  }
   for (uint32_t j = s + 1; j < e; ++j) {
     const uint32_t pj = perm[j];
-    const uint32_t ij = ids[pj];
     uint32_t k = j;
-    while (k > s && ids[perm[k - 1]] > ij) {
+    while (k > s && perm[k - 1] > pj) {
       perm[k] = perm[k - 1];
       --k;
     }
@@ -2606,7 +2643,7 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
-                                                                      A.perm, A.id[0], A.id[1]);
+                                                                      A.perm);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
@@ -2678,7 +2715,7 @@ int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s) {
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
-                                                                      A.perm, A.id[0], A.id[1]);
+                                                                      A.perm);
   k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap,
                                                            A.start, A.perm, A.acc, A.node_total, A.blk_epoch, 1);
   k_audit_kinetic<<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.vel, A.node_total,
@@ -2707,7 +2744,7 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
-                                                                      A.perm, A.id[0], A.id[1]);
+                                                                      A.perm);
   k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
                                                      A.perm, A.acc, A.node_total, A.blk_epoch, 0);
   k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
@@ -2726,7 +2763,7 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
-                                                                      A.perm, A.id[0], A.id[1]);
+                                                                      A.perm);
   k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
                                                      A.perm, A.acc, A.node_total, A.blk_epoch, 0);
   k_grid_sums<<<148 * 4, 256, 0, s>>>(A.acc, A.node_total, (unsigned long long*)out);
