@@ -273,11 +273,22 @@ __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__
 }
 
 // ============================================================== binning
+// Runs of equal values among the active lanes (a prefix of the warp): the first lane of each run
+// gets the run's length, the others 0.
+__device__ __forceinline__ uint32_t run_length(unsigned am, unsigned lane, uint32_t v) {
+  const uint32_t prev = __shfl_up_sync(am, v, 1);
+  const unsigned heads = __ballot_sync(am, lane == 0 || prev != v) | ~am;
+  if (!((heads >> lane) & 1u) || !((am >> lane) & 1u)) return 0u;
+  const unsigned later = heads & ~((2u << lane) - 1u);  // heads after this lane (lane 31: none)
+  const unsigned next = later ? (unsigned)(__ffs(later) - 1) : 32u;
+  return next - lane;
+}
+
 __global__ void k_bin_count(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
                             const int* __restrict__ pcta_inst, const float* __restrict__ st0,
                             const float* __restrict__ st1, int64_t cap, uint32_t* __restrict__ keys,
-                            uint32_t* __restrict__ count, uint32_t* __restrict__ nw_list,
-                            uint32_t* __restrict__ nw_count) {
+                            uint32_t* __restrict__ count, uint32_t* __restrict__ chunk_sum,
+                            uint32_t* __restrict__ nw_list, uint32_t* __restrict__ nw_count) {
   const int inst = pcta_inst[blockIdx.x];
   const Control& c = ctrl[inst];
   if (!c.active) return;
@@ -315,25 +326,20 @@ __global__ void k_bin_count(const InstDesc* __restrict__ desc, Control* __restri
     }
   }
   keys[slot] = key;
-  atomicAdd(&count[key], 1u);
+  // particles arrive in binned order, so a warp's keys come in runs: one atomic per run of
+  // equal keys, and one per run of equal key chunks
+  const unsigned am = __activemask(), lane = threadIdx.x & 31;
+  uint32_t len = run_length(am, lane, key);
+  if (len) atomicAdd(&count[key], len);
+  const uint32_t ch = key / KEY_CHUNK;
+  len = run_length(am, lane, ch);
+  if (len) atomicAdd(&chunk_sum[ch], len);
 }
 
-// chunk sums of the key counts
-__global__ void k_scan_chunks(const uint32_t* __restrict__ count, uint32_t* __restrict__ chunk_sum,
-                              const int* __restrict__ chunk_inst, const Control* __restrict__ ctrl) {
-  __shared__ long long sh[256];
-  const int64_t chunk = blockIdx.x;
-  if (!ctrl[chunk_inst[chunk]].active) return;
-  long long s = 0;
-  const int64_t base = chunk * KEY_CHUNK;
-  for (int j = threadIdx.x; j < KEY_CHUNK; j += 256) s += count[base + j];
-  s = block_sum_ll<256>(s, sh);
-  if (threadIdx.x == 0) chunk_sum[chunk] = (uint32_t)s;
-}
-
-// per instance: exclusive scan of its chunk sums, offset by the instance's first slot
+// per instance: exclusive scan of its key-chunk sums (accumulated by k_bin_count), offset by the
+// instance's first slot
 __global__ void k_scan_instances(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
-                                 const uint32_t* __restrict__ chunk_sum, uint32_t* __restrict__ chunk_base) {
+                                 uint32_t* __restrict__ chunk_sum, uint32_t* __restrict__ chunk_base) {
   __shared__ uint32_t sh[1024];
   const int inst = blockIdx.x;
   if (!ctrl[inst].active) return;
@@ -342,7 +348,11 @@ __global__ void k_scan_instances(const InstDesc* __restrict__ desc, const Contro
   uint32_t carry = (uint32_t)D.slot_off;
   for (int64_t base = 0; base < nc; base += 1024) {
     const int64_t j = base + threadIdx.x;
-    uint32_t v = j < nc ? chunk_sum[c0 + j] : 0u;
+    uint32_t v = 0u;
+    if (j < nc) {
+      v = chunk_sum[c0 + j];
+      chunk_sum[c0 + j] = 0u;  // k_bin_count of the next attempt accumulates from zero
+    }
     sh[threadIdx.x] = v;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {
@@ -401,8 +411,16 @@ __global__ void k_bin_scatter(const InstDesc* __restrict__ desc, const Control* 
   const int64_t slot = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
   if (slot - D.slot_off >= c.count) return;
   const uint32_t key = keys[slot];
-  const uint32_t r = atomicSub(&count[key], 1u) - 1u;  // leaves count at zero for the next attempt
-  perm[start[key] + r] = (uint32_t)slot;
+  // one atomic per run of lanes with equal keys; leaves count at zero for the next attempt
+  const unsigned am = __activemask(), lane = threadIdx.x & 31;
+  const uint32_t len = run_length(am, lane, key);
+  const unsigned prev = __shfl_up_sync(am, key, 1);
+  const unsigned heads = __ballot_sync(am, lane == 0 || prev != key);
+  const unsigned leader = 31u - __clz(heads & ((2u << lane) - 1u));  // first lane of this run
+  uint32_t top = 0u;
+  if (len) top = atomicSub(&count[key], len);
+  top = __shfl_sync(am, top, leader);
+  perm[start[key] + top - 1u - (lane - leader)] = (uint32_t)slot;
 }
 
 // sort n <= R slot indices in registers (unrolled insertion network; unused entries sort last)
@@ -2626,10 +2644,7 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
-                                                          A.keys, A.count, A.nw_list, A.nw_count);
-  ++n;
-  if (ev) cudaEventRecord(ev[n], s);
-  k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
+                                                          A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
@@ -2708,8 +2723,7 @@ int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s) {
   // transport pass: binning and an APIC-only deposit, its grid kinetic energy to buf[5 n_gcta + CTA]
   k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
-                                                          A.keys, A.count, A.nw_list, A.nw_count);
-  k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
+                                                          A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
   k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
@@ -2720,11 +2734,11 @@ int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s) {
                                                            A.start, A.perm, A.acc, A.node_total, A.blk_epoch, 1);
   k_audit_kinetic<<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.vel, A.node_total,
                                                            A.blk_epoch, 1, buf + 5 * A.n_gcta);
-  g_launches += 9;
+  g_launches += 8;
   // the audited trial step, without the Newton log
   DeviceArrays B = A;
   B.log_cap = 0;
-  return 9 + attempt_sequence(B, s, nullptr, buf);
+  return 8 + attempt_sequence(B, s, nullptr, buf);
 }
 
 __global__ void k_grid_sums(const long long* __restrict__ acc, int64_t node_total, unsigned long long* __restrict__ out) {
@@ -2737,8 +2751,7 @@ __global__ void k_grid_sums(const long long* __restrict__ acc, int64_t node_tota
 int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
   k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
-                                                          A.keys, A.count, A.nw_list, A.nw_count);
-  k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
+                                                          A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
   k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
@@ -2749,15 +2762,14 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
                                                      A.perm, A.acc, A.node_total, A.blk_epoch, 0);
   k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
                                      A.acc, A.trac, A.node_total);
-  g_launches += 9;
-  return 9;
+  g_launches += 8;
+  return 8;
 }
 
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
   k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
-                                                          A.keys, A.count, A.nw_list, A.nw_count);
-  k_scan_chunks<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_sum, A.chunk_inst, A.ctrl);
+                                                          A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
   k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
@@ -2767,19 +2779,19 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
   k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
                                                      A.perm, A.acc, A.node_total, A.blk_epoch, 0);
   k_grid_sums<<<148 * 4, 256, 0, s>>>(A.acc, A.node_total, (unsigned long long*)out);
-  g_launches += 9;
-  return 9;
+  g_launches += 8;
+  return 8;
 }
 
 int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return attempt_sequence(A, s, nullptr, nullptr); }
 
 const char* attempt_kernel_name(int k, int any_pellet, int any_bed) {
-  static const char* a[] = {"k_begin", "k_bin_count", "k_scan_chunks", "k_scan_instances", "k_scan_apply",
-                            "k_bin_scatter", "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple",
-                            "k_bed_bin", "k_bed_couple", "k_bed_step", "k_g2p", "k_segments", "k_end"};
-  if (!any_pellet && k >= 10) ++k;
-  if (!any_bed && k >= 11) k += 3;
-  return k < 17 ? a[k] : "?";
+  static const char* a[] = {"k_begin", "k_bin_count", "k_scan_instances", "k_scan_apply", "k_bin_scatter",
+                            "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple", "k_bed_bin",
+                            "k_bed_couple", "k_bed_step", "k_g2p", "k_segments", "k_end"};
+  if (!any_pellet && k >= 9) ++k;
+  if (!any_bed && k >= 10) k += 3;
+  return k < 16 ? a[k] : "?";
 }
 
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s) {
