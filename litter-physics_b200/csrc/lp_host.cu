@@ -688,7 +688,7 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
     D.nkeys = round_up(ntiles * lp::TB + 1, lp::KEY_CHUNK);
     D.blk_off = blk_off;
     D.gcta_off = gcta_off;
-    D.gcta_cnt = (nblk + lp::GU_BLOCKS_PER_CTA - 1) / lp::GU_BLOCKS_PER_CTA;
+    D.gcta_cnt = (nblk + lp::GU_BLOCKS_PER_CTA * lp::GU_PASSES - 1) / (lp::GU_BLOCKS_PER_CTA * lp::GU_PASSES);
     D.slot_off = slot_off;
     D.slot_cap = round_up(std::max<int64_t>((int64_t)h.P.size(), 1), lp::SLOT_ALIGN);
     D.pcta_off = slot_off / lp::G2P_THREADS;

@@ -827,23 +827,144 @@ __global__ void __launch_bounds__(GU_THREADS)
   if (!c.active) return;
   const InstDesc& D = desc[inst];
   const int t = threadIdx.x;
-  const int64_t lblk = (blockIdx.x - D.gcta_off) * GU_BLOCKS_PER_CTA + t / 64;
   const int64_t nblk = (int64_t)D.nblk[0] * D.nblk[1] * D.nblk[2];
   double wi0 = 0, wi1 = 0, wi2 = 0, proj = 0, fric = 0, tren = 0;
   double e_stress = 0, e_trac = 0, e_grav = 0, e_walls = 0;
   int fail = F_OK;
-  bool live = lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch;
-  int ni = 0, nj = 0, nk = 0;
-  if (live) {
-    const int bk = (int)(lblk % D.nblk[2]), bj = (int)((lblk / D.nblk[2]) % D.nblk[1]),
-              bi = (int)(lblk / ((int64_t)D.nblk[2] * D.nblk[1]));
-    const int l = t % 64;
-    ni = bi * NB + l / 16;
-    nj = bj * NB + (l / 4) % 4;
-    nk = bk * NB + l % 4;
-    live = ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2];
+  bool any_live = false;
+  // GU_PASSES passes of GU_BLOCKS_PER_CTA node blocks each; passes without a live block are skipped
+  for (int pass = 0; pass < GU_PASSES; ++pass) {
+    const int64_t lblk = ((blockIdx.x - D.gcta_off) * GU_PASSES + pass) * GU_BLOCKS_PER_CTA + t / 64;
+    bool live = lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch;
+    int ni = 0, nj = 0, nk = 0;
+    if (live) {
+      const int bk = (int)(lblk % D.nblk[2]), bj = (int)((lblk / D.nblk[2]) % D.nblk[1]),
+                bi = (int)(lblk / ((int64_t)D.nblk[2] * D.nblk[1]));
+      const int l = t % 64;
+      ni = bi * NB + l / 16;
+      nj = bj * NB + (l / 4) % 4;
+      nk = bk * NB + l % 4;
+      live = ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2];
+    }
+    if (!__syncthreads_or(live ? 1 : 0)) continue;  // CTA-uniform
+    any_live = true;
+    if (live) {
+      const int64_t g = node_index(D, ni, nj, nk);
+      const long long mf = acc[g];
+      if (mf <= 0) {
+        vel[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        acc[g] = 0;
+        acc[node_total + g] = 0;
+        acc[2 * node_total + g] = 0;
+        acc[3 * node_total + g] = 0;
+      } else {
+        const double s_m = D.s_mass, s_p = c.s_mom;
+        const double md = (double)mf / s_m;
+        double p[3] = {(double)acc[node_total + g] / s_p, (double)acc[2 * node_total + g] / s_p,
+                       (double)acc[3 * node_total + g] / s_p};
+        acc[g] = 0;
+        acc[node_total + g] = 0;
+        acc[2 * node_total + g] = 0;
+        acc[3 * node_total + g] = 0;
+        if (AUDIT) e_stress += 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / md;
+        const int co[3] = {ni, nj, nk};
+        float Tl[3] = {0.f, 0.f, 0.f}, Th[3] = {0.f, 0.f, 0.f};
+        bool shell = false;
+  #pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (co[a] == 2 || co[a] == 3 || co[a] == D.cells[a] - 1 || co[a] == D.cells[a]) shell = true;
+        if (shell) {
+  #pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const long long l = trac[(int64_t)a * node_total + g], h = trac[(int64_t)(a + 3) * node_total + g];
+            if (l | h) {
+              trac[(int64_t)a * node_total + g] = 0;
+              trac[(int64_t)(a + 3) * node_total + g] = 0;
+              const double dl = (double)l / s_p, dh = (double)h / s_p;
+              const double S = dl - dh;
+              // telescoped kinetic-energy jump of the reaction deposits (grid.rs:279-295)
+              tren += S * (p[a] / md + S / (2.0 * md));
+              if (a == 0) wi0 += S;
+              if (a == 1) wi1 += S;
+              if (a == 2) wi2 += S;
+              p[a] += S;
+              Tl[a] = (float)dl;
+              Th[a] = (float)dh;
+            }
+          }
+        }
+        if (AUDIT) {
+          e_trac += 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / md;
+          double k2 = 0.0;
+          for (int a = 0; a < 3; ++a) {
+            const double u = p[a] / md + D.gravity[a] * c.dt;
+            k2 += u * u;
+          }
+          e_grav += 0.5 * md * k2;
+        }
+        const float m = (float)md;
+        const float dt = (float)c.dt;
+        float v[3];
+  #pragma unroll
+        for (int a = 0; a < 3; ++a) v[a] = (float)p[a] / m + (float)D.gravity[a] * dt;
+        if (!(isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]))) {
+          fail = F_GRID_NONFINITE;
+          vel[g] = make_float4(0.f, 0.f, 0.f, m);
+        } else {
+          const float before[3] = {v[0], v[1], v[2]};
+  #pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            float sign = 0.0f;
+            if (co[a] <= 1) sign = 1.0f;
+            else if (co[a] > D.cells[a]) sign = -1.0f;
+            if (sign == 0.0f) continue;
+            const float nsp = v[a] * sign;
+            if (nsp >= 0.0f) continue;
+            proj -= 0.5 * (double)m * (double)nsp * (double)nsp;
+            v[a] = 0.0f;
+            const float t0 = v[0], t1 = v[1], t2 = v[2];
+            const int face = 2 * a + (sign > 0.f ? 0 : 1);
+            if (D.face_mode && D.face_sticky[face]) {
+              v[0] = v[1] = v[2] = 0.0f;
+            } else {
+              const float mu = D.face_mode ? (float)D.face_mu[face] : (float)D.friction;
+              reduce_tangential(v, mu * (-nsp));
+            }
+            fric += 0.5 * (double)m *
+                    ((double)(t0 * t0 + t1 * t1 + t2 * t2) - (double)(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+          }
+  #pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float R = Tl[a] + Th[a];
+            if (!(R > 0.0f)) continue;
+            const float normal = v[a];
+            float tg[3] = {v[0], v[1], v[2]};
+            tg[a] = 0.0f;
+            const double t2b = (double)(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]);
+            if (D.face_mode) {
+              const bool stick = (Tl[a] > 0.f && D.face_sticky[2 * a]) || (Th[a] > 0.f && D.face_sticky[2 * a + 1]);
+              if (stick) tg[0] = tg[1] = tg[2] = 0.0f;
+              else reduce_tangential(tg, ((float)D.face_mu[2 * a] * Tl[a] + (float)D.face_mu[2 * a + 1] * Th[a]) / m);
+            } else {
+              reduce_tangential(tg, (float)D.friction * R / m);
+            }
+            fric += 0.5 * (double)m * (t2b - (double)(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]));
+            v[0] = tg[0];
+            v[1] = tg[1];
+            v[2] = tg[2];
+            v[a] = normal;
+          }
+          wi0 += (double)(v[0] - before[0]) * (double)m;
+          wi1 += (double)(v[1] - before[1]) * (double)m;
+          wi2 += (double)(v[2] - before[2]) * (double)m;
+          vel[g] = make_float4(v[0], v[1], v[2], m);
+          if (AUDIT)
+            e_walls += 0.5 * (double)m * ((double)v[0] * v[0] + (double)v[1] * v[1] + (double)v[2] * v[2]);
+        }
+      }
+    }
   }
-  if (!__syncthreads_or(live ? 1 : 0)) {
+  if (!any_live) {  // CTA-uniform
     if (t == 0) {
       GridPartial& P = part[blockIdx.x];
       P.wall_impulse[0] = P.wall_impulse[1] = P.wall_impulse[2] = 0.0;
@@ -853,121 +974,6 @@ __global__ void __launch_bounds__(GU_THREADS)
         for (int k = 0; k < 4; ++k) audit[4 * (int64_t)blockIdx.x + k] = 0.0;
     }
     return;
-  }
-  if (live) {
-    const int64_t g = node_index(D, ni, nj, nk);
-    const long long mf = acc[g];
-    if (mf <= 0) {
-      vel[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-      acc[g] = 0;
-      acc[node_total + g] = 0;
-      acc[2 * node_total + g] = 0;
-      acc[3 * node_total + g] = 0;
-    } else {
-      const double s_m = D.s_mass, s_p = c.s_mom;
-      const double md = (double)mf / s_m;
-      double p[3] = {(double)acc[node_total + g] / s_p, (double)acc[2 * node_total + g] / s_p,
-                     (double)acc[3 * node_total + g] / s_p};
-      acc[g] = 0;
-      acc[node_total + g] = 0;
-      acc[2 * node_total + g] = 0;
-      acc[3 * node_total + g] = 0;
-      if (AUDIT) e_stress = 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / md;
-      const int co[3] = {ni, nj, nk};
-      float Tl[3] = {0.f, 0.f, 0.f}, Th[3] = {0.f, 0.f, 0.f};
-      bool shell = false;
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-        if (co[a] == 2 || co[a] == 3 || co[a] == D.cells[a] - 1 || co[a] == D.cells[a]) shell = true;
-      if (shell) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const long long l = trac[(int64_t)a * node_total + g], h = trac[(int64_t)(a + 3) * node_total + g];
-          if (l | h) {
-            trac[(int64_t)a * node_total + g] = 0;
-            trac[(int64_t)(a + 3) * node_total + g] = 0;
-            const double dl = (double)l / s_p, dh = (double)h / s_p;
-            const double S = dl - dh;
-            // telescoped kinetic-energy jump of the reaction deposits (grid.rs:279-295)
-            tren += S * (p[a] / md + S / (2.0 * md));
-            if (a == 0) wi0 += S;
-            if (a == 1) wi1 += S;
-            if (a == 2) wi2 += S;
-            p[a] += S;
-            Tl[a] = (float)dl;
-            Th[a] = (float)dh;
-          }
-        }
-      }
-      if (AUDIT) {
-        e_trac = 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / md;
-        double k2 = 0.0;
-        for (int a = 0; a < 3; ++a) {
-          const double u = p[a] / md + D.gravity[a] * c.dt;
-          k2 += u * u;
-        }
-        e_grav = 0.5 * md * k2;
-      }
-      const float m = (float)md;
-      const float dt = (float)c.dt;
-      float v[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) v[a] = (float)p[a] / m + (float)D.gravity[a] * dt;
-      if (!(isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]))) {
-        fail = F_GRID_NONFINITE;
-        vel[g] = make_float4(0.f, 0.f, 0.f, m);
-      } else {
-        const float before[3] = {v[0], v[1], v[2]};
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          float sign = 0.0f;
-          if (co[a] <= 1) sign = 1.0f;
-          else if (co[a] > D.cells[a]) sign = -1.0f;
-          if (sign == 0.0f) continue;
-          const float nsp = v[a] * sign;
-          if (nsp >= 0.0f) continue;
-          proj -= 0.5 * (double)m * (double)nsp * (double)nsp;
-          v[a] = 0.0f;
-          const float t0 = v[0], t1 = v[1], t2 = v[2];
-          const int face = 2 * a + (sign > 0.f ? 0 : 1);
-          if (D.face_mode && D.face_sticky[face]) {
-            v[0] = v[1] = v[2] = 0.0f;
-          } else {
-            const float mu = D.face_mode ? (float)D.face_mu[face] : (float)D.friction;
-            reduce_tangential(v, mu * (-nsp));
-          }
-          fric += 0.5 * (double)m *
-                  ((double)(t0 * t0 + t1 * t1 + t2 * t2) - (double)(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
-        }
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const float R = Tl[a] + Th[a];
-          if (!(R > 0.0f)) continue;
-          const float normal = v[a];
-          float tg[3] = {v[0], v[1], v[2]};
-          tg[a] = 0.0f;
-          const double t2b = (double)(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]);
-          if (D.face_mode) {
-            const bool stick = (Tl[a] > 0.f && D.face_sticky[2 * a]) || (Th[a] > 0.f && D.face_sticky[2 * a + 1]);
-            if (stick) tg[0] = tg[1] = tg[2] = 0.0f;
-            else reduce_tangential(tg, ((float)D.face_mu[2 * a] * Tl[a] + (float)D.face_mu[2 * a + 1] * Th[a]) / m);
-          } else {
-            reduce_tangential(tg, (float)D.friction * R / m);
-          }
-          fric += 0.5 * (double)m * (t2b - (double)(tg[0] * tg[0] + tg[1] * tg[1] + tg[2] * tg[2]));
-          v[0] = tg[0];
-          v[1] = tg[1];
-          v[2] = tg[2];
-          v[a] = normal;
-        }
-        wi0 += (double)(v[0] - before[0]) * (double)m;
-        wi1 += (double)(v[1] - before[1]) * (double)m;
-        wi2 += (double)(v[2] - before[2]) * (double)m;
-        vel[g] = make_float4(v[0], v[1], v[2], m);
-        if (AUDIT)
-          e_walls = 0.5 * (double)m * ((double)v[0] * v[0] + (double)v[1] * v[1] + (double)v[2] * v[2]);
-      }
-    }
   }
   double rv[RK];
   rv[0] = wi0;
@@ -1020,30 +1026,32 @@ __global__ void __launch_bounds__(GU_THREADS)
   const InstDesc& D = desc[inst];
   const int t = threadIdx.x;
   double e = 0.0;
-  const int64_t lblk = (blockIdx.x - D.gcta_off) * GU_BLOCKS_PER_CTA + t / 64;
   const int64_t nblk = (int64_t)D.nblk[0] * D.nblk[1] * D.nblk[2];
-  if (c.active && lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch) {
-    const int bk = (int)(lblk % D.nblk[2]), bj = (int)((lblk / D.nblk[2]) % D.nblk[1]),
-              bi = (int)(lblk / ((int64_t)D.nblk[2] * D.nblk[1]));
-    const int l = t % 64;
-    const int ni = bi * NB + l / 16, nj = bj * NB + (l / 4) % 4, nk = bk * NB + l % 4;
-    if (ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2]) {
-      const int64_t g = node_index(D, ni, nj, nk);
-      if (from_acc) {
-        const long long mf = acc[g];
-        if (mf > 0) {
-          const double md = (double)mf / D.s_mass;
-          double p2 = 0.0;
-          for (int a = 1; a <= 3; ++a) {
-            const double pa = (double)acc[a * node_total + g] / c.s_mom;
-            p2 += pa * pa;
+  for (int pass = 0; pass < GU_PASSES; ++pass) {
+    const int64_t lblk = ((blockIdx.x - D.gcta_off) * GU_PASSES + pass) * GU_BLOCKS_PER_CTA + t / 64;
+    if (c.active && lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch) {
+      const int bk = (int)(lblk % D.nblk[2]), bj = (int)((lblk / D.nblk[2]) % D.nblk[1]),
+                bi = (int)(lblk / ((int64_t)D.nblk[2] * D.nblk[1]));
+      const int l = t % 64;
+      const int ni = bi * NB + l / 16, nj = bj * NB + (l / 4) % 4, nk = bk * NB + l % 4;
+      if (ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2]) {
+        const int64_t g = node_index(D, ni, nj, nk);
+        if (from_acc) {
+          const long long mf = acc[g];
+          if (mf > 0) {
+            const double md = (double)mf / D.s_mass;
+            double p2 = 0.0;
+            for (int a = 1; a <= 3; ++a) {
+              const double pa = (double)acc[a * node_total + g] / c.s_mom;
+              p2 += pa * pa;
+            }
+            e += 0.5 * p2 / md;
           }
-          e = 0.5 * p2 / md;
+          for (int a = 0; a < 4; ++a) acc[a * node_total + g] = 0;
+        } else {
+          const float4 v = vel[g];
+          if (v.w > 0.0f) e += 0.5 * (double)v.w * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
         }
-        for (int a = 0; a < 4; ++a) acc[a * node_total + g] = 0;
-      } else {
-        const float4 v = vel[g];
-        if (v.w > 0.0f) e = 0.5 * (double)v.w * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
       }
     }
   }
