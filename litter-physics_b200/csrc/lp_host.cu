@@ -772,7 +772,9 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   ALLOC(A.chunk_base, A.n_chunks);
   ALLOC(A.perm, A.cap);
   ALLOC(A.nw_list, A.cap);
-  ALLOC(A.nw_count, 1);
+  ALLOC(A.nw_count, 2);
+  A.tile_count = A.nw_count + 1;
+  ALLOC(A.tile_list, A.n_tiles);
   ALLOC(A.acc, 4 * A.node_total);
   ALLOC(A.trac, 6 * A.node_total);
   ALLOC(A.blk_epoch, A.n_blk);

@@ -214,7 +214,10 @@ __device__ __forceinline__ double momentum_bound(float m, float speed, float cn,
 __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, int n_inst,
                         uint32_t* __restrict__ nw_count, BedPtrs bed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *nw_count = 0u;
+  if (i == 0) {
+    nw_count[0] = 0u;  // near-wall particle list of this attempt
+    nw_count[1] = 0u;  // occupied-tile list of this attempt
+  }
   if (i >= n_inst) return;
   const InstDesc& D = desc[i];
   Control& c = ctrl[i];
@@ -477,6 +480,39 @@ __global__ void k_bin_sort(const InstDesc* __restrict__ desc, const Control* __r
   }
 }
 
+// The attempt's occupied tiles of the active instances, for the persistent P2G and G2P CTAs (the
+// list order does not matter: their results are per tile).  Empty tiles get zero G2P partials.
+__global__ void k_tiles(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                        const int* __restrict__ tile_inst, int64_t n_tiles, const uint32_t* __restrict__ start,
+                        uint32_t* __restrict__ tile_list, uint32_t* __restrict__ tile_count,
+                        ParticlePartial* __restrict__ tpart) {
+  const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool busy = false;
+  if (tile < n_tiles) {
+    const int inst = tile_inst[tile];
+    const Control& c = ctrl[inst];
+    if (c.active) {
+      const InstDesc& D = desc[inst];
+      const int64_t key0 = D.key_off + (tile - D.tile_off) * TB;
+      busy = start[key0 + TB] > start[key0];
+      if (!busy) {
+        ParticlePartial& P = tpart[tile];
+        P.diss = P.bbound = P.mass = 0.0;
+        P.max_speed = P.max_disp = 0.f;
+        P.fail = F_OK;
+        P.iterations = P.yielded = 0;
+        P.fail_value = 0.0;
+      }
+    }
+  }
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned bal = __ballot_sync(0xffffffffu, busy);
+  uint32_t base = 0u;
+  if (lane == 0 && bal) base = atomicAdd(tile_count, (uint32_t)__popc(bal));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (busy) tile_list[base + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)tile;
+}
+
 // ============================================================== P2G
 // One CTA per tile of TX x TY x TZ bins.  The tile's particles (contiguous in sorted slot order)
 // are taken in chunks of P2G_CHUNK:
@@ -496,18 +532,19 @@ constexpr size_t P2G_PART_BYTES = sizeof(float4) * TB * 27;
 constexpr size_t P2G_REC_BYTES = sizeof(float) * P2G_REC * P2G_CHUNK;
 constexpr size_t P2G_SMEM = P2G_PART_BYTES > P2G_REC_BYTES ? P2G_PART_BYTES : P2G_REC_BYTES;
 
-__global__ void __launch_bounds__(P2G_THREADS, 2)
-    k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
-          const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
-          const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
-          int64_t node_total, uint32_t* __restrict__ blk_epoch, int transport_only) {
+// one tile of k_p2g
+__device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restrict__ desc,
+                                         const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
+                                         const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
+                                         const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
+                                         long long* __restrict__ acc, int64_t node_total,
+                                         uint32_t* __restrict__ blk_epoch, int transport_only) {
   extern __shared__ float4 part[];  // particle records during the chunks, then TB * 27 partial node sums
   float* rec = reinterpret_cast<float*>(part);  // [P2G_REC][P2G_CHUNK]
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
   __shared__ int redi[P2G_THREADS / 32];
   __shared__ uint32_t bstart[TB + 1];
 
-  const int tile = blockIdx.x;
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
   if (!c.active) return;
@@ -701,6 +738,21 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
       atomic_add_ll(acc + 2 * node_total + g, nv[2]);
       atomic_add_ll(acc + 3 * node_total + g, nv[3]);
     }
+  }
+}
+
+// Persistent CTAs (as many as fit the GPU at once) walk the attempt's list of occupied tiles.
+__global__ void __launch_bounds__(P2G_THREADS, 2)
+    k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
+          const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
+          const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
+          int64_t node_total, uint32_t* __restrict__ blk_epoch, int transport_only,
+          const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count) {
+  const uint32_t n = *tile_count;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    p2g_tile((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm, acc, node_total, blk_epoch,
+             transport_only);
+    __syncthreads();  // the next tile reuses the shared memory
   }
 }
 
@@ -1842,20 +1894,22 @@ __device__ __forceinline__ float cta_warm_logit(G2pMlpShared& sh, const MlpPacke
   return need ? sh.out[q] : __int_as_float(0x7fc00000);
 }
 
+// one tile of k_g2p; `staged` tells whether the CTA already holds the network weights
 template <bool WARM>
-__global__ void __launch_bounds__(G2P_THREADS, 2)
-    k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
-          float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
-          int64_t cap, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
-          const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const MlpPacked* __restrict__ mlp,
-          float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
-          long long log_cap) {
+__device__ __forceinline__ void g2p_tile(const int tile, bool& staged, const InstDesc* __restrict__ desc,
+                                         const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
+                                         float* __restrict__ st0, float* __restrict__ st1,
+                                         uint32_t* __restrict__ id0, uint32_t* __restrict__ id1, int64_t cap,
+                                         const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
+                                         const float4* __restrict__ vel, ParticlePartial* __restrict__ part,
+                                         const MlpPacked* __restrict__ mlp, float* __restrict__ log_x,
+                                         float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
+                                         long long log_cap) {
   __shared__ float4 hv[HN];
   __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
   extern __shared__ float4 g2p_dyn[];  // prefetched inputs of two rounds, then the network state
   float* pf = reinterpret_cast<float*>(g2p_dyn);
   G2pMlpShared& wsh = *reinterpret_cast<G2pMlpShared*>(reinterpret_cast<char*>(g2p_dyn) + G2P_SMEM);
-  const int tile = blockIdx.x;
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
   if (!c.active) return;
@@ -1865,7 +1919,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
   const uint32_t s0 = start[key0], e0 = start[key0 + TB];
   if (s0 == e0) {
     if (threadIdx.x == 0) {
-      ParticlePartial& P = part[blockIdx.x];
+      ParticlePartial& P = part[tile];
       P.diss = P.bbound = P.mass = 0.0;
       P.max_speed = P.max_disp = 0.f;
       P.fail = F_OK;
@@ -1888,7 +1942,6 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
   const bool use_mlp = WARM && D.kind == 0 && c.warm_start && mlp != nullptr;  // CTA-uniform
   HbFeatureConst hfc;
   if (use_mlp) hfc = hb_feature_const(D.consistency, D.flow_index, D.mu, c.dt);
-  bool staged = false;
   const float* cur = c.parity ? st1 : st0;
   float* nxt = c.parity ? st0 : st1;
   const uint32_t* idc = c.parity ? id1 : id0;
@@ -2139,7 +2192,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
                   (double)yielded, fail_value};
   block_reduce_multi<G2P_THREADS, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
   if (threadIdx.x == 0) {
-    ParticlePartial& P = part[blockIdx.x];
+    ParticlePartial& P = part[tile];
     P.diss = rv[0];
     P.bbound = rv[1];
     P.mass = rv[2];
@@ -2149,6 +2202,25 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
     P.iterations = (int)rv[6];
     P.yielded = (int)rv[7];
     P.fail_value = rv[8];
+  }
+}
+
+// Persistent CTAs (as many as fit the GPU at once) walk the attempt's list of occupied tiles;
+// the partial results are per tile, so they do not depend on which CTA took which tile.
+template <bool WARM>
+__global__ void __launch_bounds__(G2P_THREADS, 2)
+    k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
+          float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
+          int64_t cap, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
+          const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const MlpPacked* __restrict__ mlp,
+          float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
+          long long log_cap, const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count) {
+  bool staged = false;
+  const uint32_t n = *tile_count;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    g2p_tile<WARM>((int)tile_list[i], staged, desc, ctrl, tile_inst, st0, st1, id0, id1, cap, start, perm, vel, part,
+                   mlp, log_x, log_y, log_n, log_cap);
+    __syncthreads();  // the next tile reuses the shared memory
   }
 }
 
@@ -2633,15 +2705,45 @@ __global__ void k_liquid_batch(int64_t n, const double* j, const double* grad, d
 // ============================================================== launchers
 static uint64_t g_launches = 0;
 
+static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// persistent grid sizes of P2G and the two G2P instantiations: resident CTAs per SM times SMs
+static int g_p2g_ctas = 296, g_g2p_ctas[2] = {296, 296};
+
 void configure_kernels() {
   cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM);
   cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes<false>());
   cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes<true>());
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return;
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2g, P2G_THREADS, P2G_SMEM) == cudaSuccess && per > 0)
+    g_p2g_ctas = per * sms;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<false>, G2P_THREADS, g2p_smem_bytes<false>()) ==
+          cudaSuccess && per > 0)
+    g_g2p_ctas[0] = per * sms;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<true>, G2P_THREADS, g2p_smem_bytes<true>()) ==
+          cudaSuccess && per > 0)
+    g_g2p_ctas[1] = per * sms;
+}
+
+// the occupied-tile list, then P2G over it
+static int launch_tiles_p2g(const DeviceArrays& A, cudaStream_t s, int transport_only, cudaEvent_t* ev, int& n) {
+  k_tiles<<<grid_of(A.n_tiles, 256), 256, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.n_tiles, A.start, A.tile_list,
+                                                   A.tile_count, A.tpart);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  k_p2g<<<(unsigned)g_p2g_ctas, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap,
+                                                             A.start, A.perm, A.acc, A.node_total, A.blk_epoch,
+                                                             transport_only, A.tile_list, A.tile_count);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  return 2;
 }
 uint64_t kernel_launch_count() { return g_launches; }
 void add_kernel_launches(uint64_t n) { g_launches += n; }
 
-static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // audit (energy audit) or null: the grid-update stage energies go to audit[4 * CTA + k] and the
 // kinetic energy after the pellet coupling to audit[4 * n_gcta + CTA].
@@ -2669,10 +2771,7 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
                                                                       A.perm);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
-                                                     A.perm, A.acc, A.node_total, A.blk_epoch, 0);
-  ++n;
-  if (ev) cudaEventRecord(ev[n], s);
+  launch_tiles_p2g(A, s, 0, ev, n);
   k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
                                      A.acc, A.trac, A.node_total);
   ++n;
@@ -2709,10 +2808,10 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
     ++n;
   }
   const bool warm_g2p = A.mlp != nullptr && A.warm;
-  (warm_g2p ? k_g2p<true> : k_g2p<false>)<<<(unsigned)A.n_tiles, G2P_THREADS,
-                                            warm_g2p ? g2p_smem_bytes<true>() : g2p_smem_bytes<false>(), s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0],
-                                                     A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, A.mlp, A.log_x,
-                                                     A.log_y, A.log_n, A.log_cap);
+  (warm_g2p ? k_g2p<true> : k_g2p<false>)<<<(unsigned)g_g2p_ctas[warm_g2p ? 1 : 0], G2P_THREADS,
+                                            warm_g2p ? g2p_smem_bytes<true>() : g2p_smem_bytes<false>(), s>>>(
+      A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, A.mlp,
+      A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_segments<<<(unsigned)A.n_seg, 256, 0, s>>>(A.ctrl, A.segs, A.gpart, A.tpart, A.seg);
@@ -2738,15 +2837,15 @@ int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s) {
                                                             A.perm);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
                                                                       A.perm);
-  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap,
-                                                           A.start, A.perm, A.acc, A.node_total, A.blk_epoch, 1);
+  int nt = 0;
+  launch_tiles_p2g(A, s, 1, nullptr, nt);
   k_audit_kinetic<<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.vel, A.node_total,
                                                            A.blk_epoch, 1, buf + 5 * A.n_gcta);
-  g_launches += 8;
+  g_launches += 9;
   // the audited trial step, without the Newton log
   DeviceArrays B = A;
   B.log_cap = 0;
-  return 8 + attempt_sequence(B, s, nullptr, buf);
+  return 9 + attempt_sequence(B, s, nullptr, buf);
 }
 
 __global__ void k_grid_sums(const long long* __restrict__ acc, int64_t node_total, unsigned long long* __restrict__ out) {
@@ -2766,12 +2865,14 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
                                                             A.perm);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
                                                                       A.perm);
-  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
-                                                     A.perm, A.acc, A.node_total, A.blk_epoch, 0);
+  {
+    int nt = 0;
+    launch_tiles_p2g(A, s, 0, nullptr, nt);
+  }
   k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
                                      A.acc, A.trac, A.node_total);
-  g_launches += 8;
-  return 8;
+  g_launches += 9;
+  return 9;
 }
 
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
@@ -2784,22 +2885,24 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
                                                             A.perm);
   k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
                                                                       A.perm);
-  k_p2g<<<(unsigned)A.n_tiles, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start,
-                                                     A.perm, A.acc, A.node_total, A.blk_epoch, 0);
+  {
+    int nt = 0;
+    launch_tiles_p2g(A, s, 0, nullptr, nt);
+  }
   k_grid_sums<<<148 * 4, 256, 0, s>>>(A.acc, A.node_total, (unsigned long long*)out);
-  g_launches += 8;
-  return 8;
+  g_launches += 9;
+  return 9;
 }
 
 int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return attempt_sequence(A, s, nullptr, nullptr); }
 
 const char* attempt_kernel_name(int k, int any_pellet, int any_bed) {
   static const char* a[] = {"k_begin", "k_bin_count", "k_scan_instances", "k_scan_apply", "k_bin_scatter",
-                            "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple", "k_bed_bin",
-                            "k_bed_couple", "k_bed_step", "k_g2p", "k_segments", "k_end"};
-  if (!any_pellet && k >= 9) ++k;
-  if (!any_bed && k >= 10) k += 3;
-  return k < 16 ? a[k] : "?";
+                            "k_bin_sort", "k_tiles", "k_p2g", "k_traction", "k_grid_update", "k_couple",
+                            "k_bed_bin", "k_bed_couple", "k_bed_step", "k_g2p", "k_segments", "k_end"};
+  if (!any_pellet && k >= 10) ++k;
+  if (!any_bed && k >= 11) k += 3;
+  return k < 17 ? a[k] : "?";
 }
 
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s) {

@@ -34,7 +34,9 @@ struct DeviceArrays {
   uint32_t* chunk_base = nullptr;
   uint32_t* perm = nullptr;
   uint32_t* nw_list = nullptr;
-  uint32_t* nw_count = nullptr;
+  uint32_t* nw_count = nullptr;    // [0] near-wall particles, [1] occupied tiles of the attempt
+  uint32_t* tile_count = nullptr;  // = nw_count + 1
+  uint32_t* tile_list = nullptr;   // occupied tiles of the attempt (n_tiles capacity)
   long long* acc = nullptr;   // 4 x node_total: mass, momentum xyz (int64 fixed point)
   long long* trac = nullptr;  // 6 x node_total: reactions per axis, low faces then high faces
   int64_t node_total = 0;
@@ -66,7 +68,7 @@ struct DeviceArrays {
 
 // One substep attempt for every active instance; returns the number of kernels launched.
 int launch_attempt(const DeviceArrays& A, cudaStream_t s);
-// same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 14 events)
+// same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 18 events)
 int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev);
 const char* attempt_kernel_name(int k, int any_pellet, int any_bed);
 // Energy audit of one forced-dt trial: a transport pass (binning + APIC-only deposit) and the

@@ -192,7 +192,7 @@ class Simulation:
 
     def kernel_times(self, steps: int) -> dict:
         """Mean per-kernel duration (ms) over `steps` attempts, CUDA events on the stream."""
-        cap = 16
+        cap = 24
         ms = (C.c_double * cap)()
         names = C.create_string_buffer(32 * cap)
         n = C.c_int32()
