@@ -381,6 +381,10 @@ __global__ void k_scan_apply(const uint32_t* __restrict__ count, const uint32_t*
   const int64_t base = chunk * KEY_CHUNK;
   // 1024 threads, one key each: inclusive warp scans, then a scan of the 32 warp totals
   const uint32_t v = count[base + threadIdx.x];
+  if (!__syncthreads_or(v != 0u)) {  // no particle in this chunk (CTA-uniform)
+    start[base + threadIdx.x] = chunk_base[chunk];
+    return;
+  }
   const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint32_t x = v;
 #pragma unroll
@@ -448,35 +452,36 @@ __device__ __forceinline__ void bin_sort_small(uint32_t* __restrict__ p, int n) 
 // Order each bin by slot, that is by the particles' order in the committed state, which makes the
 // binned order deterministic after the atomic scatter.  The committed state is itself in binned
 // order, so a particle keeps its place relative to the others of its bin from step to step.
-__global__ void k_bin_sort(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
-                           const int* __restrict__ chunk_inst, const uint32_t* __restrict__ start,
-                           uint32_t* __restrict__ perm) {
-  const int64_t key = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int inst = chunk_inst[key / KEY_CHUNK];
-  const Control& c = ctrl[inst];
-  if (!c.active) return;
-  const InstDesc& D = desc[inst];
-  const int64_t lk = key - D.key_off;
-  if (lk >= D.nkeys) return;
-  const uint32_t s = start[key];
-  const uint32_t e = (lk == D.nkeys - 1) ? (uint32_t)(D.slot_off + c.count) : start[key + 1];
-  if (e <= s + 1) return;
-  if (e - s <= 8u) {  // the common case at 8 particles per cell
-    bin_sort_small<8>(perm + s, (int)(e - s));
-    return;
-  }
-  if (e - s <= 16u) {
-    bin_sort_small<16>(perm + s, (int)(e - s));
-    return;
-  }
-  for (uint32_t j = s + 1; j < e; ++j) {
-    const uint32_t pj = perm[j];
-    uint32_t k = j;
-    while (k > s && perm[k - 1] > pj) {
-      perm[k] = perm[k - 1];
-      --k;
+// Persistent CTAs of TB threads walk the occupied-tile list, one thread per bin.
+__global__ void __launch_bounds__(TB) k_bin_sort(const InstDesc* __restrict__ desc, const int* __restrict__ tile_inst,
+                                                 const uint32_t* __restrict__ start, uint32_t* __restrict__ perm,
+                                                 const uint32_t* __restrict__ tile_list,
+                                                 const uint32_t* __restrict__ tile_count) {
+  const uint32_t n = *tile_count;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const int tile = (int)tile_list[i];
+    const InstDesc& D = desc[tile_inst[tile]];
+    // a tile's keys are followed by at least the instance's outflow key, so key + 1 is valid
+    const int64_t key = D.key_off + (int64_t)(tile - D.tile_off) * TB + threadIdx.x;
+    const uint32_t s = start[key], e = start[key + 1];
+    if (e <= s + 1) continue;
+    if (e - s <= 8u) {  // the common case at 8 particles per cell
+      bin_sort_small<8>(perm + s, (int)(e - s));
+      continue;
     }
-    perm[k] = pj;
+    if (e - s <= 16u) {
+      bin_sort_small<16>(perm + s, (int)(e - s));
+      continue;
+    }
+    for (uint32_t j = s + 1; j < e; ++j) {
+      const uint32_t pj = perm[j];
+      uint32_t k = j;
+      while (k > s && perm[k - 1] > pj) {
+        perm[k] = perm[k - 1];
+        --k;
+      }
+      perm[k] = pj;
+    }
   }
 }
 
@@ -2708,7 +2713,7 @@ static uint64_t g_launches = 0;
 static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // persistent grid sizes of P2G and the two G2P instantiations: resident CTAs per SM times SMs
-static int g_p2g_ctas = 296, g_g2p_ctas[2] = {296, 296};
+static int g_p2g_ctas = 296, g_g2p_ctas[2] = {296, 296}, g_sort_ctas = 148 * 16;
 
 void configure_kernels() {
   cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM);
@@ -2718,6 +2723,8 @@ void configure_kernels() {
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return;
   int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bin_sort, TB, 0) == cudaSuccess && per > 0)
+    g_sort_ctas = per * sms;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2g, P2G_THREADS, P2G_SMEM) == cudaSuccess && per > 0)
     g_p2g_ctas = per * sms;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<false>, G2P_THREADS, g2p_smem_bytes<false>()) ==
@@ -2734,12 +2741,15 @@ static int launch_tiles_p2g(const DeviceArrays& A, cudaStream_t s, int transport
                                                    A.tile_count, A.tpart);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
+  k_bin_sort<<<(unsigned)g_sort_ctas, TB, 0, s>>>(A.desc, A.tile_inst, A.start, A.perm, A.tile_list, A.tile_count);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
   k_p2g<<<(unsigned)g_p2g_ctas, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap,
                                                              A.start, A.perm, A.acc, A.node_total, A.blk_epoch,
                                                              transport_only, A.tile_list, A.tile_count);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  return 2;
+  return 3;
 }
 uint64_t kernel_launch_count() { return g_launches; }
 void add_kernel_launches(uint64_t n) { g_launches += n; }
@@ -2765,10 +2775,6 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
   if (ev) cudaEventRecord(ev[n], s);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
-  ++n;
-  if (ev) cudaEventRecord(ev[n], s);
-  k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
-                                                                      A.perm);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   launch_tiles_p2g(A, s, 0, ev, n);
@@ -2835,8 +2841,6 @@ int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s) {
   k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
-  k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
-                                                                      A.perm);
   int nt = 0;
   launch_tiles_p2g(A, s, 1, nullptr, nt);
   k_audit_kinetic<<<(unsigned)A.n_gcta, GU_THREADS, 0, s>>>(A.desc, A.ctrl, A.gcta_inst, A.acc, A.vel, A.node_total,
@@ -2863,8 +2867,6 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
   k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
-  k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
-                                                                      A.perm);
   {
     int nt = 0;
     launch_tiles_p2g(A, s, 0, nullptr, nt);
@@ -2883,8 +2885,6 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
   k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
-  k_bin_sort<<<(unsigned)(A.n_chunks * KEY_CHUNK / 256), 256, 0, s>>>(A.desc, A.ctrl, A.chunk_inst, A.start,
-                                                                      A.perm);
   {
     int nt = 0;
     launch_tiles_p2g(A, s, 0, nullptr, nt);
@@ -2898,7 +2898,7 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return attempt_seque
 
 const char* attempt_kernel_name(int k, int any_pellet, int any_bed) {
   static const char* a[] = {"k_begin", "k_bin_count", "k_scan_instances", "k_scan_apply", "k_bin_scatter",
-                            "k_bin_sort", "k_tiles", "k_p2g", "k_traction", "k_grid_update", "k_couple",
+                            "k_tiles", "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple",
                             "k_bed_bin", "k_bed_couple", "k_bed_step", "k_g2p", "k_segments", "k_end"};
   if (!any_pellet && k >= 10) ++k;
   if (!any_bed && k >= 11) k += 3;
