@@ -33,7 +33,7 @@ constexpr int HN = HX * HY * HZ;                 // 360 halo nodes per tile
 constexpr int P2G_THREADS = 3 * TB;              // 3 slab threads per bin
 constexpr int NB = 4;                            // node block edge (grid update / activity)
 constexpr int GU_BLOCKS_PER_CTA = 4;             // node blocks per grid-update CTA pass
-constexpr int GU_PASSES = 4;                     // passes per grid-update CTA
+constexpr int GU_PASSES = 8;                     // passes per grid-update CTA
 constexpr int GU_THREADS = NB * NB * NB * GU_BLOCKS_PER_CTA;  // 256
 constexpr int G2P_THREADS = 256;
 constexpr int SLOT_ALIGN = G2P_THREADS;          // instance slot ranges are aligned to this

@@ -323,15 +323,20 @@ __global__ void k_bin_count(const InstDesc* __restrict__ desc, Control* __restri
     const int lx = b[0] % TX, ly = b[1] % TY, lz = b[2] % TZ;
     const int64_t tile = ((int64_t)tx * D.tiles[1] + ty) * D.tiles[2] + tz;
     key = (uint32_t)(D.key_off + tile * TB + (lx * TY + ly) * TZ + lz);
-    if (near) {
-      const uint32_t w = atomicAdd(nw_count, 1u);
-      nw_list[w] = (uint32_t)slot;
-    }
   }
   keys[slot] = key;
+  const unsigned am = __activemask(), lane = threadIdx.x & 31;
+  // near-wall particles go to the traction list: one atomic per warp on the shared counter
+  const unsigned nb = __ballot_sync(am, ok && near);
+  if (nb) {
+    const unsigned first = (unsigned)(__ffs(nb) - 1);
+    uint32_t w = 0u;
+    if (lane == first) w = atomicAdd(nw_count, (uint32_t)__popc(nb));
+    w = __shfl_sync(am, w, first);
+    if (ok && near) nw_list[w + __popc(nb & ((1u << lane) - 1u))] = (uint32_t)slot;
+  }
   // particles arrive in binned order, so a warp's keys come in runs: one atomic per run of
   // equal keys, and one per run of equal key chunks
-  const unsigned am = __activemask(), lane = threadIdx.x & 31;
   uint32_t len = run_length(am, lane, key);
   if (len) atomicAdd(&count[key], len);
   const uint32_t ch = key / KEY_CHUNK;
@@ -371,22 +376,24 @@ __global__ void k_scan_instances(const InstDesc* __restrict__ desc, const Contro
   }
 }
 
-// per chunk: exclusive scan of counts -> bin start slots
-__global__ void k_scan_apply(const uint32_t* __restrict__ count, const uint32_t* __restrict__ chunk_base,
-                             uint32_t* __restrict__ start, const int* __restrict__ chunk_inst,
-                             const Control* __restrict__ ctrl) {
-  __shared__ uint32_t sh[KEY_CHUNK];
+// per chunk: exclusive scan of counts -> bin start slots; 256 threads, four keys each
+__global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* __restrict__ count,
+                                                   const uint32_t* __restrict__ chunk_base,
+                                                   uint32_t* __restrict__ start, const int* __restrict__ chunk_inst,
+                                                   const Control* __restrict__ ctrl) {
+  __shared__ uint32_t sh[16];
   const int64_t chunk = blockIdx.x;
   if (!ctrl[chunk_inst[chunk]].active) return;
   const int64_t base = chunk * KEY_CHUNK;
-  // 1024 threads, one key each: inclusive warp scans, then a scan of the 32 warp totals
-  const uint32_t v = count[base + threadIdx.x];
-  if (!__syncthreads_or(v != 0u)) {  // no particle in this chunk (CTA-uniform)
-    start[base + threadIdx.x] = chunk_base[chunk];
+  const uint4 c4 = reinterpret_cast<const uint4*>(count + base)[threadIdx.x];
+  const uint32_t tsum = c4.x + c4.y + c4.z + c4.w;
+  const uint32_t cb = chunk_base[chunk];
+  if (!__syncthreads_or(tsum != 0u)) {  // no particle in this chunk (CTA-uniform)
+    reinterpret_cast<uint4*>(start + base)[threadIdx.x] = make_uint4(cb, cb, cb, cb);
     return;
   }
   const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  uint32_t x = v;
+  uint32_t x = tsum;
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
     const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
@@ -395,16 +402,19 @@ __global__ void k_scan_apply(const uint32_t* __restrict__ count, const uint32_t*
   if (lane == 31) sh[wid] = x;
   __syncthreads();
   if (wid == 0) {
-    uint32_t t = sh[lane];
+    const uint32_t w = lane < 8 ? sh[lane] : 0u;
+    uint32_t t = w;
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
+    for (int off = 1; off < 8; off <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, t, off);
       if (lane >= (unsigned)off) t += y;
     }
-    sh[32 + lane] = t - sh[lane];  // exclusive prefix of the warp totals
+    if (lane < 8) sh[8 + lane] = t - w;  // exclusive prefix of the warp totals
   }
   __syncthreads();
-  start[base + threadIdx.x] = chunk_base[chunk] + sh[32 + wid] + x - v;
+  const uint32_t e0 = cb + sh[8 + wid] + x - tsum;
+  reinterpret_cast<uint4*>(start + base)[threadIdx.x] =
+      make_uint4(e0, e0 + c4.x, e0 + c4.x + c4.y, e0 + c4.x + c4.y + c4.z);
 }
 
 __global__ void k_bin_scatter(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
@@ -2770,7 +2780,7 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
+  k_scan_apply<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
@@ -2838,7 +2848,7 @@ int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s) {
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
-  k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
+  k_scan_apply<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   int nt = 0;
@@ -2864,7 +2874,7 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
-  k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
+  k_scan_apply<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   {
@@ -2882,7 +2892,7 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
   k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
-  k_scan_apply<<<(unsigned)A.n_chunks, KEY_CHUNK, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
+  k_scan_apply<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   {
