@@ -529,8 +529,8 @@ __global__ void k_tiles(const InstDesc* __restrict__ desc, const Control* __rest
 }
 
 // ============================================================== P2G
-// One CTA per tile of TX x TY x TZ bins.  The tile's particles (contiguous in sorted slot order)
-// are taken in chunks of P2G_CHUNK:
+// Persistent CTAs take the occupied tiles of TX x TY x TZ bins from the attempt's tile list.  A
+// tile's particles (contiguous in sorted slot order) are taken in chunks of P2G_CHUNK:
 //   phase 1: the CTA loads each particle once (coalesced in slot order) and writes a 16-float
 //            record to shared memory: mass, momentum m v, the affine matrix
 //            A = C m - tau (dt 4/dx^2 V0), and the position relative to its stencil base;
@@ -1809,8 +1809,9 @@ __global__ void __launch_bounds__(64) k_bed_step(const InstDesc* __restrict__ de
 }
 
 // ============================================================== G2P + constitutive
-// One CTA per P2G tile: the tile's (TX+2)(TY+2)(TZ+2) node velocities are staged in shared
-// memory once, then the CTA walks the tile's particles (contiguous in sorted slot order),
+// Persistent CTAs take the occupied P2G tiles from the attempt's tile list.  Per tile, the
+// (TX+2)(TY+2)(TZ+2) node velocities are staged in shared memory once, then the CTA walks the
+// tile's particles (contiguous in sorted slot order),
 // gathers from shared memory, advects, runs the constitutive update and writes the trial state
 // in sorted slot order.
 // Asynchronous 4-byte global -> shared copies (cp.async), used to prefetch the next round's
