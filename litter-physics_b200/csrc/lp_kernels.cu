@@ -546,6 +546,10 @@ constexpr int P2G_REC = 16;  // m, q[3], A[9], f[3]
 constexpr size_t P2G_PART_BYTES = sizeof(float4) * TB * 27;
 constexpr size_t P2G_REC_BYTES = sizeof(float) * P2G_REC * P2G_CHUNK;
 constexpr size_t P2G_SMEM = P2G_PART_BYTES > P2G_REC_BYTES ? P2G_PART_BYTES : P2G_REC_BYTES;
+// Slot of chunk particle i in each record row: within each 32-word segment the slots rotate by
+// the segment number, so bins whose particles start 32 apart (8 per bin in a lattice fill) read
+// different shared-memory banks in the per-bin pass; consecutive i still fill a segment.
+__device__ __forceinline__ uint32_t rec_slot(uint32_t i) { return (i & ~31u) | ((i + (i >> 5)) & 31u); }
 
 // one tile of k_p2g
 __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restrict__ desc,
@@ -616,7 +620,7 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
       // A = C m - tau (dt 4/dx^2 V0)
       const float sv = stress_scale * v0;
       const float T[9] = {tau[0], tau[3], tau[4], tau[3], tau[1], tau[5], tau[4], tau[5], tau[2]};
-      float* r = rec + i;
+      float* r = rec + rec_slot(i);
       r[0] = m;
 #pragma unroll
       for (int a = 0; a < 3; ++a) r[(1 + a) * P2G_CHUNK] = v[a] * m;
@@ -638,7 +642,7 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
     // phase 2: this bin's particles inside the chunk, in sorted order
     const uint32_t j0 = max(s, c0), j1 = min(e, c0 + cn);
     for (uint32_t j = j0; j < j1; ++j) {
-      const float* r = rec + (j - c0);
+      const float* r = rec + rec_slot(j - c0);
       const float m = r[0];
       const float q[3] = {r[P2G_CHUNK], r[2 * P2G_CHUNK], r[3 * P2G_CHUNK]};
       float A[9];
