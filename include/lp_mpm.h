@@ -266,6 +266,17 @@ lp_status lp_sim_observables(lp_sim* sim, char* names, double* values, int32_t c
 lp_status lp_sim_energies(lp_sim* sim, double out[9]);
 /* Enable the learned Newton warm start (weights from lp_mlp_*); 0 disables. */
 lp_status lp_sim_set_warm_start(lp_sim* sim, const float* weights, int32_t nweights, int32_t enable);
+/* Logit table of the warm start.  Within one instance and one dt the network's six features
+ * depend on la8 = log((trial - yield) / K) / 8 alone, so the solver evaluates the network
+ * (the lp_mlp_forward_mma pass) once per instance and dt at the nodes
+ * la8_j = LP_MLP_TAB_LO + j * LP_MLP_TAB_H, j < LP_MLP_TAB_N, which cover every finite FP32
+ * la8, and interpolates linearly between them.  Copies the table of instance `instance`
+ * (0 for a simulation) to out[LP_MLP_TAB_N]; *dt = the dt it was built for, or NaN (out
+ * untouched) while none is built.  No counterpart in the reference. */
+#define LP_MLP_TAB_N 2049
+#define LP_MLP_TAB_LO (-10.75f)
+#define LP_MLP_TAB_H (11.0f / 1024.0f)
+lp_status lp_sim_warm_table(lp_sim* sim, float* out, int32_t capacity, double* dt);
 /* Conservation probe: scatter the committed state to the grid with step dt (P2G only) and
  * return out[0] = grid mass, out[1..3] = grid momentum (exact fixed-point sums over nodes),
  * out[4] = particle mass, out[5..7] = particle momentum (FP64 sums); the grid is then cleared. */
@@ -295,6 +306,8 @@ lp_status lp_batch_get_ledger(lp_batch* b, int32_t index, lp_ledger* out);
 lp_status lp_batch_export_particles(lp_batch* b, int32_t index, lp_particles* out);
 lp_status lp_batch_total_particles(lp_batch* b, uint64_t* out);
 lp_status lp_batch_set_warm_start(lp_batch* b, const float* weights, int32_t nweights, int32_t enable);
+/* lp_sim_warm_table for member `instance` of a batch. */
+lp_status lp_batch_warm_table(lp_batch* b, int32_t instance, float* out, int32_t capacity, double* dt);
 lp_status lp_batch_use_graph(lp_batch* b, int32_t steps);
 /* Per-instance views, so that each instance of a batched sweep reports what the reference's
  * sweep (python/litter_physics/sweep.py:206-262) gets from running that job alone. */

@@ -268,13 +268,16 @@ __device__ inline int hb_return_d(double trial, double ys, double k, double n, d
     return F_OK;
   }
   const double exponent = 1.0 / n;
+  const double log_k = log(k), c1 = viscous_scale * exponent;
   double lower = ys, upper = trial;
   double sigma = (sigma0 > lower && sigma0 < upper) ? sigma0 : 0.5 * (lower + upper);
   const double tolerance = tol_rel * fmax(trial, 1.0);
-  // over^(1/n) is evaluated once per iterate as exp(log(over)/n) and reused by the derivative
-  // (over^(1/n - 1) = over^(1/n) / over)
-  double over = fmax((sigma - ys) / k, 0.0);
-  double pw = over > 0.0 ? exp(exponent * log(over)) : 0.0;
+  // With over = sigma - yield, the flow term is (over / K)^(1/n) = exp((log(over) - log K) / n),
+  // evaluated once per iterate, and the Newton step
+  //   sigma - f / f',  f' = 1 + 3 mu dt (1/n) (over/K)^(1/n) / over
+  // is written sigma - f over / (over + 3 mu dt (1/n) (over/K)^(1/n)): one division per iterate.
+  double over = fmax(sigma - ys, 0.0);
+  double pw = over > 0.0 ? exp(exponent * (log(over) - log_k)) : 0.0;
   double last = sigma - trial + viscous_scale * pw;
   for (int it = 1; it <= 200; ++it) {
     if (fabs(last) <= tolerance || (upper - lower) <= tolerance) {
@@ -287,14 +290,13 @@ __device__ inline int hb_return_d(double trial, double ys, double k, double n, d
     else lower = sigma;
     double newton;
     if (over > 0.0) {
-      const double derivative = 1.0 + viscous_scale * exponent * (pw / over) / k;
-      newton = sigma - last / derivative;
+      newton = sigma - last * over / (over + c1 * pw);
     } else {
       newton = sigma;  // infinite derivative: the reference's Newton step is a no-op here
     }
     sigma = (isfinite(newton) && newton > lower && newton < upper) ? newton : 0.5 * (lower + upper);
-    over = fmax((sigma - ys) / k, 0.0);
-    pw = over > 0.0 ? exp(exponent * log(over)) : 0.0;
+    over = fmax(sigma - ys, 0.0);
+    pw = over > 0.0 ? exp(exponent * (log(over) - log_k)) : 0.0;
     last = sigma - trial + viscous_scale * pw;
     if (!isfinite(last)) {
       *iters = it;

@@ -1757,9 +1757,17 @@ static lp_status set_warm(Ensemble& E, const float* w, int32_t nw, int32_t enabl
       lp_status st = E.alloc(&E.d_mlp_pk, 1);
       if (st != LP_OK) return st;
     }
+    if (!E.A.mlp_tab) {
+      lp_status st = E.alloc(&E.A.mlp_tab, (size_t)E.A.n_inst * lp::MLP_TAB_FLOATS);
+      if (st != LP_OK) return st;
+      st = E.alloc(&E.A.mlp_tab_dt, (size_t)E.A.n_inst);
+      if (st != LP_OK) return st;
+    }
     CUDA_CK(cudaMemcpyAsync(E.d_mlp, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice, E.stream));
     lp::launch_mlp_pack(E.d_mlp, E.d_mlp_pk, E.stream);
     CUDA_CK(cudaGetLastError());
+    // new weights: every instance's logit table is rebuilt on its next attempt (NaN never equals dt)
+    CUDA_CK(cudaMemsetAsync(E.A.mlp_tab_dt, 0xff, sizeof(double) * (size_t)E.A.n_inst, E.stream));
     E.A.mlp = E.d_mlp_pk;
   }
   E.invalidate_graph();
@@ -1771,6 +1779,26 @@ static lp_status set_warm(Ensemble& E, const float* w, int32_t nw, int32_t enabl
 }
 lp_status lp_sim_set_warm_start(lp_sim* sim, const float* w, int32_t nw, int32_t enable) {
   return set_warm(sim->E, w, nw, enable);
+}
+static_assert(LP_MLP_TAB_N == lp::MLP_TAB_N, "table size of the C header");
+static lp_status warm_table(Ensemble& E, int32_t inst, float* out, int32_t capacity, double* dt) {
+  if (!out || !dt) return set_error(LP_INVALID, "null output");
+  if (inst < 0 || inst >= E.A.n_inst) return set_error(LP_INVALID, "instance out of range");
+  if (capacity < lp::MLP_TAB_N) return set_error(LP_INVALID, "capacity below LP_MLP_TAB_N");
+  *dt = std::numeric_limits<double>::quiet_NaN();
+  if (!E.A.mlp_tab) return LP_OK;
+  double built = 0.0;
+  CUDA_CK(cudaMemcpyAsync(&built, E.A.mlp_tab_dt + inst, sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  if (!(built > 0.0)) return LP_OK;  // never built (0) or stale (NaN)
+  CUDA_CK(cudaMemcpyAsync(out, E.A.mlp_tab + (size_t)inst * lp::MLP_TAB_FLOATS, sizeof(float) * lp::MLP_TAB_N,
+                          cudaMemcpyDeviceToHost, E.stream));
+  CUDA_CK(cudaStreamSynchronize(E.stream));
+  *dt = built;
+  return LP_OK;
+}
+lp_status lp_sim_warm_table(lp_sim* sim, float* out, int32_t capacity, double* dt) {
+  return warm_table(sim->E, 0, out, capacity, dt);
 }
 lp_status lp_sim_grid_totals(lp_sim* sim, double dt, double out[8]) {
   Ensemble& E = sim->E;
@@ -1830,7 +1858,8 @@ lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* name
   const int n = std::min(nk, (int)capacity);
   for (int k = 0; k < n; ++k) {
     ms[k] = acc[k] / std::max(steps, 1);
-    std::snprintf(names + 32 * k, 32, "%s", lp::attempt_kernel_name(k, E.A.any_pellet, E.A.any_bed));
+    std::snprintf(names + 32 * k, 32, "%s", lp::attempt_kernel_name(k, E.A.any_pellet, E.A.any_bed,
+                                                                    E.A.mlp && E.A.mlp_tab && E.A.warm));
   }
   *count = n;
   return pull_ctrl(E);
@@ -2026,6 +2055,9 @@ lp_status lp_batch_total_particles(lp_batch* b, uint64_t* out) {
 }
 lp_status lp_batch_set_warm_start(lp_batch* b, const float* w, int32_t nw, int32_t enable) {
   return set_warm(b->E, w, nw, enable);
+}
+lp_status lp_batch_warm_table(lp_batch* b, int32_t instance, float* out, int32_t capacity, double* dt) {
+  return warm_table(b->E, instance, out, capacity, dt);
 }
 lp_status lp_batch_use_graph(lp_batch* b, int32_t steps) {
   b->E.invalidate_graph();

@@ -580,8 +580,6 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
   if (t <= TB) bstart[t] = start[key0 + t];
   __syncthreads();
   const int bin = t / 3, slab = t % 3;
-  const int lx = bin / (TY * TZ), ly = (bin / TZ) % TY, lz = bin % TZ;
-  const int bx = tx * TX + lx, by = ty * TY + ly, bz = tz * TZ + lz;
 
   const float* cur = c.parity ? st1 : st0;
   const float dx = (float)D.dx;
@@ -1863,73 +1861,23 @@ __device__ __forceinline__ void g2p_prefetch(float* __restrict__ buf, const floa
   cp_async4(b + PF_ID * G2P_THREADS, idc + src);
 }
 
-// Warm start (WARM instantiation): after the trial phase of each round of G2P_THREADS
-// particles, the yielding lanes of the whole CTA are compacted (ballot + warp prefix) into
-// feature rows in shared memory, ceil(count / 32) warps run the tensor-core network on full
-// 32-row blocks, and each lane reads its start value back.  The weights are staged on the
-// first round that has a yielding particle, so tiles with none never load them.
-// The round's per-particle state (stress trial, kinematics) is parked in shared memory across
-// the network pass, whose fragments need the registers.
-constexpr int G2P_STASH = 28;
-struct G2pMlpShared {
-  MlpPacked w;
-  uint32_t xs[G2P_THREADS * MLP_S1];     // compacted feature rows
-  float out[G2P_THREADS];                // network output per row
-  int cnt[G2P_THREADS / 32];             // yielding lanes per warp
-  float stash[G2P_STASH * G2P_THREADS];  // [slot][thread]
-};
-// dynamic shared memory of the G2P instantiations: prefetch slots, then (WARM) the network state
+// Warm start (WARM instantiation): each yielding lane reads the network's logit at its la8 from
+// its instance's table (k_mlp_table), interpolated between the two neighbouring nodes.
+// one tile of k_g2p
 template <bool WARM>
-constexpr size_t g2p_smem_bytes() {
-  return G2P_SMEM + (WARM ? sizeof(G2pMlpShared) : 0);
-}
-
-// CTA-wide network pass of one round; every thread of the CTA calls it.  Returns the network
-// output for lanes with `need`, NaN otherwise.
-__device__ __forceinline__ float cta_warm_logit(G2pMlpShared& sh, const MlpPacked* __restrict__ mlp, bool& staged,
-                                                bool need, const float (&f)[6]) {
-  const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const unsigned bal = __ballot_sync(0xffffffffu, need);
-  if (lane == 0) sh.cnt[wid] = __popc(bal);
-  __syncthreads();
-  int before = 0, total = 0;
-#pragma unroll
-  for (int i = 0; i < G2P_THREADS / 32; ++i) {
-    const int ci = sh.cnt[i];
-    before += i < (int)wid ? ci : 0;
-    total += ci;
-  }
-  if (total == 0) return __int_as_float(0x7fc00000);  // CTA-uniform
-  const int q = before + __popc(bal & ((1u << lane) - 1u));
-  if (need) mlp_write_row(sh.xs + q * MLP_S1, f);
-  const int rows = (total + 31) & ~31;
-  if ((int)threadIdx.x >= total && (int)threadIdx.x < rows) mlp_zero_row(sh.xs + threadIdx.x * MLP_S1);
-  if (!staged) {  // CTA-uniform
-    mlp_stage(mlp, sh.w);
-    staged = true;
-  }
-  __syncthreads();
-  if ((int)(wid * 32) < total) sh.out[wid * 32 + lane] = warp_mlp_rows(sh.w, sh.xs + wid * 32 * MLP_S1);
-  __syncthreads();
-  return need ? sh.out[q] : __int_as_float(0x7fc00000);
-}
-
-// one tile of k_g2p; `staged` tells whether the CTA already holds the network weights
-template <bool WARM>
-__device__ __forceinline__ void g2p_tile(const int tile, bool& staged, const InstDesc* __restrict__ desc,
+__device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restrict__ desc,
                                          const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
                                          float* __restrict__ st0, float* __restrict__ st1,
                                          uint32_t* __restrict__ id0, uint32_t* __restrict__ id1, int64_t cap,
                                          const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
                                          const float4* __restrict__ vel, ParticlePartial* __restrict__ part,
-                                         const MlpPacked* __restrict__ mlp, float* __restrict__ log_x,
+                                         const float* __restrict__ mlp_tab, float* __restrict__ log_x,
                                          float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
                                          long long log_cap) {
   __shared__ float4 hv[HN];
   __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
-  extern __shared__ float4 g2p_dyn[];  // prefetched inputs of two rounds, then the network state
+  extern __shared__ float4 g2p_dyn[];  // prefetched inputs of two rounds
   float* pf = reinterpret_cast<float*>(g2p_dyn);
-  G2pMlpShared& wsh = *reinterpret_cast<G2pMlpShared*>(reinterpret_cast<char*>(g2p_dyn) + G2P_SMEM);
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
   if (!c.active) return;
@@ -1959,9 +1907,10 @@ __device__ __forceinline__ void g2p_tile(const int tile, bool& staged, const Ins
                                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
-  const bool use_mlp = WARM && D.kind == 0 && c.warm_start && mlp != nullptr;  // CTA-uniform
-  HbFeatureConst hfc;
-  if (use_mlp) hfc = hb_feature_const(D.consistency, D.flow_index, D.mu, c.dt);
+  const bool use_mlp = WARM && D.kind == 0 && c.warm_start && mlp_tab != nullptr;  // CTA-uniform
+  const float2* tab =
+      use_mlp ? reinterpret_cast<const float2*>(mlp_tab + (int64_t)inst * MLP_TAB_FLOATS + MLP_TAB_STRIDE) : nullptr;
+  const float inv_k = (float)(1.0 / D.consistency);
   const float* cur = c.parity ? st1 : st0;
   float* nxt = c.parity ? st0 : st1;
   const uint32_t* idc = c.parity ? id1 : id0;
@@ -1994,11 +1943,10 @@ __device__ __forceinline__ void g2p_tile(const int tile, bool& staged, const Ins
       (float)(6.0 * sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]) *
               D.max_dt);
   for (int r = 0; r < nround; ++r) {
-    // Without the network, a warp leaves once its slots are past the tile.  With it, the rounds
-    // stay CTA-uniform (the network pass synchronises the CTA); lanes past the end redo the
-    // tile's last particle and store nothing.
+    // a warp leaves once its slots are past the tile; lanes past the end of a live warp redo the
+    // tile's last particle and store nothing
     const bool warp_live = live_of(r);
-    if (!use_mlp && !warp_live) break;
+    if (!warp_live) break;
     if (r + 1 < nround && live_of(r + 1))
       g2p_prefetch(pf + ((r + 1) & 1) * PF_SLOTS * G2P_THREADS, cur, idc, cap, src_next, paste, pyield);
     cp_async_commit();
@@ -2113,58 +2061,12 @@ __device__ __forceinline__ void g2p_tile(const int tile, bool& staged, const Ins
     }
     double sigma0 = -1.0;
     if constexpr (WARM) {
-      if (use_mlp) {
-        // learned warm start for the yielding lanes of this round
-        const bool need = valid && pt.path != PT_DONE && pt.trial_eq > ys && pt.trial_eq > 0.0;
-        float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (need) hb_features_f(hfc, pt.trial_eq, ys, f);
-        float* sp = wsh.stash + threadIdx.x;
-        {
-          const float park[G2P_STASH] = {Htr[0], Htr[1], Htr[2], Htr[3], Htr[4], Htr[5], Htr[6], Htr[7], Htr[8],
-                                         pt.dev.xx, pt.dev.yy, pt.dev.zz, pt.dev.xy, pt.dev.xz, pt.dev.yz,
-                                         pt.mean, pt.vol, pt.dnorm,
-                                         __int_as_float(__double2loint(pt.trial_eq)),
-                                         __int_as_float(__double2hiint(pt.trial_eq)),
-                                         __int_as_float(__double2loint(ys)), __int_as_float(__double2hiint(ys)),
-                                         ep, speed, disp, m, v0, cn};
-#pragma unroll
-          for (int i = 0; i < G2P_STASH; ++i) sp[i * G2P_THREADS] = park[i];
-        }
-        const int path = pt.path, ofail = o.fail;
-        const float y = cta_warm_logit(wsh, mlp, staged, need, f);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) Htr[i] = sp[i * G2P_THREADS];
-        pt.dev.xx = sp[9 * G2P_THREADS];
-        pt.dev.yy = sp[10 * G2P_THREADS];
-        pt.dev.zz = sp[11 * G2P_THREADS];
-        pt.dev.xy = sp[12 * G2P_THREADS];
-        pt.dev.xz = sp[13 * G2P_THREADS];
-        pt.dev.yz = sp[14 * G2P_THREADS];
-        pt.mean = sp[15 * G2P_THREADS];
-        pt.vol = sp[16 * G2P_THREADS];
-        pt.dnorm = sp[17 * G2P_THREADS];
-        pt.trial_eq = __hiloint2double(__float_as_int(sp[19 * G2P_THREADS]), __float_as_int(sp[18 * G2P_THREADS]));
-        ys = __hiloint2double(__float_as_int(sp[21 * G2P_THREADS]), __float_as_int(sp[20 * G2P_THREADS]));
-        ep = sp[22 * G2P_THREADS];
-        speed = sp[23 * G2P_THREADS];
-        disp = sp[24 * G2P_THREADS];
-        m = sp[25 * G2P_THREADS];
-        v0 = sp[26 * G2P_THREADS];
-        cn = sp[27 * G2P_THREADS];
-        pt.path = path;
-        o.fail = ofail;
-        o.iters = 0;
-        o.yielded = 0;
-        o.dep = 0.0;
-        o.diss_density = 0.0;
-        o.trial = o.eq = pt.trial_eq;
-        if (need) {
-          const double frac = warm_fraction_of(y);
-          if (frac > 0.0) sigma0 = ys + frac * (pt.trial_eq - ys);
-        }
+      // learned warm start of the yielding lanes (the network's root fraction from the table)
+      if (use_mlp && valid && pt.path != PT_DONE && pt.trial_eq > ys && pt.trial_eq > 0.0) {
+        const float t = mlp_table_fraction(tab, hb_la8(inv_k, pt.trial_eq, ys));
+        if (t > 0.0f && t < 1.0f) sigma0 = ys + (double)t * (pt.trial_eq - ys);
       }
     }
-    if (!warp_live) continue;
     if (paste) {
       paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, D.consistency, D.flow_index, c.dt, D.tol, sigma0, pt,
                    o);
@@ -2232,16 +2134,54 @@ __global__ void __launch_bounds__(G2P_THREADS, 2)
     k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
           int64_t cap, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
-          const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const MlpPacked* __restrict__ mlp,
+          const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const float* __restrict__ mlp_tab,
           float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
           long long log_cap, const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count) {
-  bool staged = false;
   const uint32_t n = *tile_count;
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-    g2p_tile<WARM>((int)tile_list[i], staged, desc, ctrl, tile_inst, st0, st1, id0, id1, cap, start, perm, vel, part,
-                   mlp, log_x, log_y, log_n, log_cap);
+    g2p_tile<WARM>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, id0, id1, cap, start, perm, vel, part, mlp_tab,
+                   log_x, log_y, log_n, log_cap);
     __syncthreads();  // the next tile reuses the shared memory
   }
+}
+
+// Warm-start table, one CTA per instance: the tensor-core network pass at the MLP_TAB_N nodes
+// of la8 with the instance's material constants and this attempt's dt, then the root fractions.  A
+// table built for the same dt is kept (tab_dt holds the dt of each built table; the host sets it
+// to NaN when the weights change).
+constexpr int MLP_TAB_THREADS = 256;
+__global__ void __launch_bounds__(MLP_TAB_THREADS) k_mlp_table(const InstDesc* __restrict__ desc,
+                                                               const Control* __restrict__ ctrl,
+                                                               const MlpPacked* __restrict__ mlp,
+                                                               float* __restrict__ tab, double* __restrict__ tab_dt) {
+  __shared__ MlpPacked w;
+  __shared__ uint32_t xs[(MLP_TAB_THREADS / 32) * MLP_XS_WORDS];
+  const int inst = blockIdx.x;
+  const Control& c = ctrl[inst];
+  const InstDesc& D = desc[inst];
+  if (!c.active || !c.warm_start || D.kind != 0 || tab_dt[inst] == c.dt) return;  // CTA-uniform
+  mlp_stage(mlp, w);
+  const HbFeatureConst h = hb_feature_const(D.consistency, D.flow_index, D.mu, c.dt);
+  __syncthreads();
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* out = tab + (int64_t)inst * MLP_TAB_FLOATS;
+  for (int r0 = wid * 32; r0 < MLP_TAB_N; r0 += MLP_TAB_THREADS) {  // warp-uniform
+    const int r = r0 + lane;
+    float f[6];
+    hb_features_la8(h, mlp_table_node(min(r, MLP_TAB_N - 1)), f);
+    const float y = warp_mlp_logit(w, xs + wid * MLP_XS_WORDS, f);
+    if (r < MLP_TAB_N) out[r] = y;
+  }
+  __syncthreads();
+  // root fractions and their node differences (the sigmoid of warm_fraction_of)
+  float2* pairs = reinterpret_cast<float2*>(out + MLP_TAB_STRIDE);
+  for (int r = threadIdx.x; r < MLP_TAB_N; r += MLP_TAB_THREADS) {
+    const float t0 = 1.0f / (1.0f + __expf(-out[r]));
+    const float t1 = r + 1 < MLP_TAB_N ? 1.0f / (1.0f + __expf(-out[r + 1])) : t0;
+    pairs[r] = make_float2(t0, t1 - t0);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) tab_dt[inst] = c.dt;
 }
 
 // ============================================================== end of attempt
@@ -2732,8 +2672,8 @@ static int g_p2g_ctas = 296, g_g2p_ctas[2] = {296, 296}, g_sort_ctas = 148 * 16;
 
 void configure_kernels() {
   cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM);
-  cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes<false>());
-  cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes<true>());
+  cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G2P_SMEM);
+  cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G2P_SMEM);
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return;
@@ -2742,10 +2682,10 @@ void configure_kernels() {
     g_sort_ctas = per * sms;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2g, P2G_THREADS, P2G_SMEM) == cudaSuccess && per > 0)
     g_p2g_ctas = per * sms;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<false>, G2P_THREADS, g2p_smem_bytes<false>()) ==
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<false>, G2P_THREADS, G2P_SMEM) ==
           cudaSuccess && per > 0)
     g_g2p_ctas[0] = per * sms;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<true>, G2P_THREADS, g2p_smem_bytes<true>()) ==
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<true>, G2P_THREADS, G2P_SMEM) ==
           cudaSuccess && per > 0)
     g_g2p_ctas[1] = per * sms;
 }
@@ -2828,11 +2768,15 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
                                                              A.blk_epoch, 0, audit + 4 * A.n_gcta);
     ++n;
   }
-  const bool warm_g2p = A.mlp != nullptr && A.warm;
-  (warm_g2p ? k_g2p<true> : k_g2p<false>)<<<(unsigned)g_g2p_ctas[warm_g2p ? 1 : 0], G2P_THREADS,
-                                            warm_g2p ? g2p_smem_bytes<true>() : g2p_smem_bytes<false>(), s>>>(
-      A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, A.mlp,
-      A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count);
+  const bool warm_g2p = A.mlp != nullptr && A.mlp_tab != nullptr && A.warm;
+  if (warm_g2p) {
+    k_mlp_table<<<A.n_inst, MLP_TAB_THREADS, 0, s>>>(A.desc, A.ctrl, A.mlp, A.mlp_tab, A.mlp_tab_dt);
+    ++n;
+    if (ev) cudaEventRecord(ev[n], s);
+  }
+  (warm_g2p ? k_g2p<true> : k_g2p<false>)<<<(unsigned)g_g2p_ctas[warm_g2p ? 1 : 0], G2P_THREADS, G2P_SMEM, s>>>(
+      A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart,
+      warm_g2p ? A.mlp_tab : nullptr, A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_segments<<<(unsigned)A.n_seg, 256, 0, s>>>(A.ctrl, A.segs, A.gpart, A.tpart, A.seg);
@@ -2911,13 +2855,15 @@ int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
 
 int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return attempt_sequence(A, s, nullptr, nullptr); }
 
-const char* attempt_kernel_name(int k, int any_pellet, int any_bed) {
+const char* attempt_kernel_name(int k, int any_pellet, int any_bed, int warm) {
   static const char* a[] = {"k_begin", "k_bin_count", "k_scan_instances", "k_scan_apply", "k_bin_scatter",
                             "k_tiles", "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple",
-                            "k_bed_bin", "k_bed_couple", "k_bed_step", "k_g2p", "k_segments", "k_end"};
+                            "k_bed_bin", "k_bed_couple", "k_bed_step", "k_mlp_table", "k_g2p", "k_segments",
+                            "k_end"};
   if (!any_pellet && k >= 10) ++k;
   if (!any_bed && k >= 11) k += 3;
-  return k < 17 ? a[k] : "?";
+  if (!warm && k >= 14) ++k;
+  return k < 18 ? a[k] : "?";
 }
 
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s) {

@@ -50,6 +50,8 @@ struct DeviceArrays {
   SegPartial* seg = nullptr;
   int64_t n_seg = 0;
   const MlpPacked* mlp = nullptr;  // packed warm-start weights (device) or null
+  float* mlp_tab = nullptr;         // [n_inst][MLP_TAB_FLOATS] warm-start tables (logits, fractions)
+  double* mlp_tab_dt = nullptr;     // [n_inst] dt each table was built for (NaN: stale)
   int warm = 0;                     // some instance has the warm start on: launch the WARM G2P
   float* log_x = nullptr;
   float* log_y = nullptr;
@@ -68,9 +70,9 @@ struct DeviceArrays {
 
 // One substep attempt for every active instance; returns the number of kernels launched.
 int launch_attempt(const DeviceArrays& A, cudaStream_t s);
-// same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 18 events)
+// same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 19 events)
 int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev);
-const char* attempt_kernel_name(int k, int any_pellet, int any_bed);
+const char* attempt_kernel_name(int k, int any_pellet, int any_bed, int warm);
 // Energy audit of one forced-dt trial: a transport pass (binning + APIC-only deposit) and the
 // attempt with stage energies.  buf holds 6 * n_gcta doubles: [0, 4 n_gcta) the grid-update
 // stages per CTA (stress, traction, gravity kick, walls), [4 n_gcta, 5 n_gcta) the kinetic energy

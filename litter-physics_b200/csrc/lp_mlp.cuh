@@ -221,7 +221,7 @@ __device__ __forceinline__ float warp_mlp_logit(const MlpPacked& S, uint32_t* xs
 // Features of many return problems that share consistency, flow index, mu and dt (one
 // material, one attempt): the per-problem part is log a only.  FP32 restatement of hb_features.
 struct HbFeatureConst {
-  float lb8, n, inv_n_m1, f4, f5, inv_k;
+  float lb8, n, inv_n_m1, f4, f5;
 };
 __device__ inline HbFeatureConst hb_feature_const(double k, double n, double mu, double dt) {
   HbFeatureConst h;
@@ -231,18 +231,42 @@ __device__ inline HbFeatureConst hb_feature_const(double k, double n, double mu,
   h.inv_n_m1 = (float)(1.0 / n - 1.0);
   h.f4 = (float)(1.0 / (3.0 * n));
   h.f5 = (float)log(n);
-  h.inv_k = (float)(1.0 / k);
   return h;
 }
-__device__ __forceinline__ void hb_features_f(const HbFeatureConst& h, double trial, double ys, float (&f)[6]) {
-  const float a = fmaxf((float)(trial - ys) * h.inv_k, 1e-37f);
-  const float la8 = logf(a) * 0.125f;
+// log(a) / 8 of one return problem, a = (trial - yield) / K floored at 1e-37; the hardware
+// logarithm suffices, since la8 only places the problem between table nodes 0.011 apart
+__device__ __forceinline__ float hb_la8(float inv_k, double trial, double ys) {
+  const float a = fmaxf((float)(trial - ys) * inv_k, 1e-37f);
+  return __logf(a) * 0.125f;
+}
+__device__ __forceinline__ void hb_features_la8(const HbFeatureConst& h, float la8, float (&f)[6]) {
   f[0] = la8;
   f[1] = h.lb8;
   f[2] = h.n;
   f[3] = h.lb8 + h.inv_n_m1 * la8;
   f[4] = h.f4;
   f[5] = h.f5;
+}
+
+// Warm-start table of one instance.  For one material and one dt, four of the six features are
+// constants, the first is la8 = log(a)/8 and the fourth is affine in it, so the network is a
+// smooth function of la8 alone.  It is evaluated (the same tensor-core pass) at MLP_TAB_N nodes
+// la8_j = MLP_TAB_LO + j MLP_TAB_H, which cover every finite FP32 a >= 1e-37
+// (la8 in [-10.66, 11.10]); the node spacing is exact in FP32.  Per instance the table holds the
+// logits (MLP_TAB_STRIDE floats), then one float2 per node: the root fraction
+// t_j = 1 / (1 + exp(-logit_j)) and t_(j+1) - t_j, which the solver interpolates linearly.
+constexpr int MLP_TAB_N = 2049, MLP_TAB_STRIDE = 2056;
+constexpr int MLP_TAB_FLOATS = 3 * MLP_TAB_STRIDE;  // per instance: logits, then (t, dt) pairs
+constexpr float MLP_TAB_LO = -10.75f, MLP_TAB_H = 11.0f / 1024.0f, MLP_TAB_INV_H = 1024.0f / 11.0f;
+__device__ __forceinline__ float mlp_table_node(int j) { return MLP_TAB_LO + (float)j * MLP_TAB_H; }
+// interpolated root fraction at la8 of the instance's (t, dt) pairs; NaN outside the table (a
+// non-finite la8 included)
+__device__ __forceinline__ float mlp_table_fraction(const float2* __restrict__ pairs, float la8) {
+  const float u = (la8 - MLP_TAB_LO) * MLP_TAB_INV_H;
+  if (!(u >= 0.0f && u <= (float)(MLP_TAB_N - 1))) return __int_as_float(0x7fc00000);
+  const int i = min((int)u, MLP_TAB_N - 2);
+  const float2 p = __ldg(pairs + i);
+  return fmaf(u - (float)i, p.y, p.x);
 }
 
 // warm-start fraction in (0, 1) from the network output, or -1 (midpoint start)

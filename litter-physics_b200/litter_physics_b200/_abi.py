@@ -19,6 +19,8 @@ STATUS_NAMES = {
 }
 LP_SLUMP, LP_HYDROSTATIC, LP_DAM_BREAK, LP_COUPLED_PATCH = range(4)
 LP_BED_HERTZ_MINDLIN, LP_BED_LINEAR = range(2)
+# warm-start logit table: node j at la8 = MLP_TAB_LO + j * MLP_TAB_H (LP_MLP_TAB_* of lp_mpm.h)
+MLP_TAB_N, MLP_TAB_LO, MLP_TAB_H = 2049, -10.75, 11.0 / 1024.0
 LP_PASTE, LP_LIQUID = range(2)
 FIXTURES = {"slump": LP_SLUMP, "hydrostatic": LP_HYDROSTATIC, "dam_break": LP_DAM_BREAK,
             "coupled_patch": LP_COUPLED_PATCH}

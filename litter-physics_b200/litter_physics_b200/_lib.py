@@ -95,6 +95,7 @@ def lib():
         "lp_sim_observables": ([P, C.c_char_p, D, I32, C.POINTER(I32)], I32),
         "lp_sim_energies": ([P, D], I32),
         "lp_sim_set_warm_start": ([P, F, I32, I32], I32),
+        "lp_sim_warm_table": ([P, F, I32, D], I32),
         "lp_sim_use_graph": ([P, I32], I32),
         "lp_sim_grid_totals": ([P, C.c_double, D], I32),
         "lp_sim_grid_dump": ([P, C.c_double, D, D, D, I64], I32),
@@ -112,6 +113,7 @@ def lib():
         "lp_batch_export_particles": ([P, I32, C.POINTER(_abi.Particles)], I32),
         "lp_batch_total_particles": ([P, C.POINTER(U64)], I32),
         "lp_batch_set_warm_start": ([P, F, I32, I32], I32),
+        "lp_batch_warm_table": ([P, I32, F, I32, D], I32),
         "lp_batch_use_graph": ([P, I32], I32),
         "lp_batch_autotune": ([P, I32, C.c_char_p, C.c_size_t], I32),
         "lp_batch_get_pellet": ([P, I32, C.POINTER(_abi.Pellet), C.POINTER(I32)], I32),

@@ -208,6 +208,14 @@ class Simulation:
         w = np.ascontiguousarray(weights, dtype=np.float32)
         check(lib().lp_sim_set_warm_start(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size, 1))
 
+    def warm_table(self) -> tuple[np.ndarray | None, float]:
+        """The warm start's logit table (network logits at the la8 nodes of `_abi.MLP_TAB_*`)
+        and the dt it was built for; (None, nan) before the first warm-started attempt."""
+        out = np.zeros(_abi.MLP_TAB_N, dtype=np.float32)
+        dt = C.c_double()
+        check(lib().lp_sim_warm_table(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size, C.byref(dt)))
+        return (out if np.isfinite(dt.value) else None), dt.value
+
     def enable_newton_log(self, capacity: int) -> None:
         check(lib().lp_sim_enable_newton_log(self._h, int(capacity)))
 
@@ -337,6 +345,14 @@ class Batch:
             return
         w = np.ascontiguousarray(weights, dtype=np.float32)
         check(lib().lp_batch_set_warm_start(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size, 1))
+
+    def warm_table(self, i: int) -> tuple[np.ndarray | None, float]:
+        """`Simulation.warm_table` of member i."""
+        out = np.zeros(_abi.MLP_TAB_N, dtype=np.float32)
+        dt = C.c_double()
+        check(lib().lp_batch_warm_table(self._h, int(i), out.ctypes.data_as(C.POINTER(C.c_float)), out.size,
+                                        C.byref(dt)))
+        return (out if np.isfinite(dt.value) else None), dt.value
 
 
 class BatchMember:

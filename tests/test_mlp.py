@@ -107,6 +107,53 @@ def test_tensor_core_inference_matches_oracle(trained):
 
 
 @pytest.mark.gpu
+def test_warm_table_matches_network(trained):
+    """The solver's logit table (one tensor-core pass per instance and dt over the la8 nodes)
+    against the network evaluated directly: equal at the nodes up to feature rounding, and the
+    linear interpolation half-way between nodes within the BF16 budget of the FP64 network."""
+    import mlp_oracle as M
+
+    from litter_physics_b200 import _abi, configs, warmstart
+    from litter_physics_b200.sim import Simulation
+
+    w, _ = trained
+    spec = configs.slump(32, (8, 8, 16), seed=11, yield_range=(20.0, 100.0))
+    sim = Simulation(spec)
+    assert sim.warm_table()[0] is None
+    sim.set_warm_start(w)
+    sim.run_substeps(2)
+    tab, dt = sim.warm_table()
+    assert tab is not None and 0.0 < dt <= spec.max_dt
+    mat = spec.material
+    k, n, mu = mat.consistency, mat.flow_index, mat.shear_modulus
+
+    def rows(la8):
+        # return problems whose log(a)/8 is la8: trial - yield = K exp(8 la8)
+        la8 = np.asarray(la8, dtype=np.float64)
+        ys = np.zeros(la8.shape)  # a yield of 0 keeps trial - yield exact down to a = 1e-37
+        raw = np.stack([k * np.exp(8.0 * la8), ys, np.full(la8.shape, k), np.full(la8.shape, n),
+                        np.full(la8.shape, mu), np.full(la8.shape, dt)], axis=1)
+        return warmstart.features(raw).astype(np.float32)
+
+    j = np.arange(_abi.MLP_TAB_N)
+    nodes = (np.float32(_abi.MLP_TAB_LO) + j.astype(np.float32) * np.float32(_abi.MLP_TAB_H)).astype(np.float64)
+    assert nodes[0] < np.log(1e-37) / 8 and nodes[-1] > np.log(np.finfo(np.float32).max) / 8
+    # the la8 range of real problems (a from 1e-6 to 1e4) and a spread over the whole table
+    sel = np.unique(np.concatenate([np.flatnonzero((nodes > -1.8) & (nodes < 1.2)), j[::16]]))
+    sel = sel[sel < _abi.MLP_TAB_N - 1]
+    direct = warmstart.predict(w, rows(nodes[sel]), tensor_cores=True).astype(np.float64)
+    scale = max(1.0, float(np.abs(direct).max()))
+    assert np.abs(tab[sel] - direct).max() <= 1e-3 * scale
+    mid = 0.5 * (nodes[sel] + nodes[sel + 1])
+    interp = 0.5 * (tab[sel].astype(np.float64) + tab[sel + 1])
+    y64 = M.forward(w.astype(np.float64), rows(mid))
+    err = np.abs(interp - y64)
+    print(f"table: max |node - mma| {np.abs(tab[sel] - direct).max():.3e}; "
+          f"mid-node |interp - fp64| max {err.max():.3e}, mean {err.mean():.3e}")
+    assert err.max() <= 1e-2 * scale
+
+
+@pytest.mark.gpu
 def test_warm_started_slump_matches_oracle(trained):
     """Warm start inside the solver (G2P's tensor-core network pass): the slump after 100
     substeps stays within the parity bars of the plain solver against the FP64 oracle, with
