@@ -536,6 +536,14 @@ __device__ __forceinline__ float sym_norm(const Sym& a) {
   return sqrtf(a.xx * a.xx + a.yy * a.yy + a.zz * a.zz + 2.f * (a.xy * a.xy + a.xz * a.xz + a.yz * a.yz));
 }
 
+// Series coefficients, correctly rounded like the FP32 divisions they replace:
+// kLogSeries[j] = (-1)^(j+1) / j (log(I + B)), kInverse[j] = 1 / j (exp(M) by Horner).
+__constant__ const float kLogSeries[13] = {0.0f,         1.0f,         -1.0f / 2.0f,  1.0f / 3.0f,  -1.0f / 4.0f,
+                                           1.0f / 5.0f,  -1.0f / 6.0f, 1.0f / 7.0f,   -1.0f / 8.0f, 1.0f / 9.0f,
+                                           -1.0f / 10.0f, 1.0f / 11.0f, -1.0f / 12.0f};
+__constant__ const float kInverse[10] = {0.0f,        1.0f,        1.0f / 2.0f, 1.0f / 3.0f, 1.0f / 4.0f,
+                                         1.0f / 5.0f, 1.0f / 6.0f, 1.0f / 7.0f, 1.0f / 8.0f, 1.0f / 9.0f};
+
 // Trial part of the paste update: the Hencky strain of H_tr and its equivalent stress.  The
 // Newton start (the learned warm start) is chosen from t.trial_eq between paste_trial and
 // paste_finish, which lets a warp evaluate the network for all its lanes at one call site.
@@ -588,12 +596,12 @@ __device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& 
   const int K = r <= 0.01f ? 4 : (r <= 0.05f ? 6 : (r <= 0.1f ? 7 : (r <= 0.18f ? 10 : 12)));
   Sym P;
   {
-    const float cK = ((K & 1) ? 1.f : -1.f) / (float)K;
+    const float cK = kLogSeries[K];
     P.xx = P.yy = P.zz = cK;
     P.xy = P.xz = P.yz = 0.f;
     for (int j = K - 1; j >= 1; --j) {
       Sym q = sym_mul(B, P);
-      const float cj = ((j & 1) ? 1.f : -1.f) / (float)j;
+      const float cj = kLogSeries[j];
       q.xx += cj;
       q.yy += cj;
       q.zz += cj;
@@ -686,7 +694,7 @@ __device__ inline void paste_finish(const float Htr[9], float mu, float lambda, 
     Q.xy = Q.xz = Q.yz = 0.f;
     for (int j = T; j >= 2; --j) {
       Sym q = sym_mul(M, Q);
-      const float inv = 1.f / (float)j;
+      const float inv = kInverse[j];
       Q.xx = 1.f + q.xx * inv;
       Q.yy = 1.f + q.yy * inv;
       Q.zz = 1.f + q.zz * inv;

@@ -287,92 +287,147 @@ __device__ __forceinline__ uint32_t run_length(unsigned am, unsigned lane, uint3
   return next - lane;
 }
 
-__global__ void k_bin_count(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl,
-                            const int* __restrict__ pcta_inst, const float* __restrict__ st0,
-                            const float* __restrict__ st1, int64_t cap, uint32_t* __restrict__ keys,
-                            uint32_t* __restrict__ count, uint32_t* __restrict__ chunk_sum,
-                            uint32_t* __restrict__ nw_list, uint32_t* __restrict__ nw_count) {
-  const int inst = pcta_inst[blockIdx.x];
-  const Control& c = ctrl[inst];
-  if (!c.active) return;
-  const InstDesc& D = desc[inst];
-  const int64_t slot = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
-  if (slot - D.slot_off >= c.count) return;
-  const float* cur = c.parity ? st1 : st0;
-  const float dx = (float)D.dx;
+// The binning passes run 2 warps per block of G2P_THREADS slots; each warp takes 4 rounds of 32
+// consecutive slots and issues the loads (and, in the scatter, the atomics) of all its rounds
+// before using them, so that each warp keeps several memory requests in flight.
+constexpr int BIN_THREADS = 64, BIN_ROUNDS = 4;
+static_assert(BIN_THREADS * BIN_ROUNDS == G2P_THREADS, "a binning CTA covers one slot block");
+
+// stencil-cell key of a particle at x (the instance's outflow key when the stencil leaves the
+// grid) and whether it lies within dx/2 of a wall
+__device__ __forceinline__ uint32_t bin_key(const InstDesc& D, const float (&x)[3], float dx, bool& ok, bool& near) {
   int b[3];
-  bool ok = true;
-  bool near = false;
+  ok = true;
+  near = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const float x = cur[(int64_t)(C_X + a) * cap + slot];
-    const float s = scaled_of(x, dx);
+    const float s = scaled_of(x[a], dx);
     const float bf = floorf(s - 0.5f);
     const float padded = bf + 1.0f;
     if (!(padded >= 0.0f) || padded + 2.0f >= (float)D.nodes[a]) ok = false;
     b[a] = ok ? (int)padded : 0;
     const float half = 0.5f * dx;
-    if (x < half || x > (float)D.extent[a] - half) near = true;
+    if (x[a] < half || x[a] > (float)D.extent[a] - half) near = true;
   }
-  uint32_t key;
-  if (!ok) {
-    key = (uint32_t)(D.key_off + D.nkeys - 1);
-    atomicAdd((unsigned long long*)&ctrl[inst].outflow, 1ull);
-  } else {
-    const int tx = b[0] / TX, ty = b[1] / TY, tz = b[2] / TZ;
-    const int lx = b[0] % TX, ly = b[1] % TY, lz = b[2] % TZ;
-    const int64_t tile = ((int64_t)tx * D.tiles[1] + ty) * D.tiles[2] + tz;
-    key = (uint32_t)(D.key_off + tile * TB + (lx * TY + ly) * TZ + lz);
+  if (!ok) return (uint32_t)(D.key_off + D.nkeys - 1);
+  const int tx = b[0] / TX, ty = b[1] / TY, tz = b[2] / TZ;
+  const int lx = b[0] % TX, ly = b[1] % TY, lz = b[2] % TZ;
+  const int64_t tile = ((int64_t)tx * D.tiles[1] + ty) * D.tiles[2] + tz;
+  return (uint32_t)(D.key_off + tile * TB + (lx * TY + ly) * TZ + lz);
+}
+
+__global__ void __launch_bounds__(BIN_THREADS)
+    k_bin_count(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, const int* __restrict__ pcta_inst,
+                const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
+                uint32_t* __restrict__ keys, uint32_t* __restrict__ count, uint32_t* __restrict__ chunk_sum,
+                uint32_t* __restrict__ nw_list, uint32_t* __restrict__ nw_count) {
+  const int inst = pcta_inst[blockIdx.x];
+  const Control& c = ctrl[inst];
+  if (!c.active) return;
+  const InstDesc& D = desc[inst];
+  const unsigned lane = threadIdx.x & 31;
+  const int64_t base = (int64_t)blockIdx.x * G2P_THREADS + (threadIdx.x >> 5) * (32 * BIN_ROUNDS) + lane;
+  const int64_t lim = D.slot_off + c.count;  // slots below lim hold particles
+  const float* cur = c.parity ? st1 : st0;
+  float xs[BIN_ROUNDS][3];
+#pragma unroll
+  for (int q = 0; q < BIN_ROUNDS; ++q)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int64_t slot = base + 32 * q;
+      xs[q][a] = slot < lim ? cur[(int64_t)(C_X + a) * cap + slot] : 0.f;
+    }
+  // lanes holding a particle in each round (a prefix of the warp), taken while the warp is converged
+  unsigned amq[BIN_ROUNDS];
+#pragma unroll
+  for (int q = 0; q < BIN_ROUNDS; ++q) amq[q] = __ballot_sync(0xffffffffu, base + 32 * q < lim);
+  const float dx = (float)D.dx;
+#pragma unroll
+  for (int q = 0; q < BIN_ROUNDS; ++q) {
+    const unsigned am = amq[q];
+    if (!am) break;  // warp-uniform
+    const int64_t slot = base + 32 * q;
+    if (slot < lim) {
+      bool ok, near;
+      const uint32_t key = bin_key(D, xs[q], dx, ok, near);
+      if (!ok) atomicAdd((unsigned long long*)&ctrl[inst].outflow, 1ull);
+      keys[slot] = key;
+      // near-wall particles go to the traction list: one atomic per warp on the shared counter
+      const unsigned nb = __ballot_sync(am, ok && near);
+      if (nb) {
+        const unsigned first = (unsigned)(__ffs(nb) - 1);
+        uint32_t w = 0u;
+        if (lane == first) w = atomicAdd(nw_count, (uint32_t)__popc(nb));
+        w = __shfl_sync(am, w, first);
+        if (ok && near) nw_list[w + __popc(nb & ((1u << lane) - 1u))] = (uint32_t)slot;
+      }
+      // particles arrive in binned order, so a warp's keys come in runs: one atomic per run of
+      // equal keys, and one per run of equal key chunks
+      uint32_t len = run_length(am, lane, key);
+      if (len) atomicAdd(&count[key], len);
+      const uint32_t ch = key / KEY_CHUNK;
+      len = run_length(am, lane, ch);
+      if (len) atomicAdd(&chunk_sum[ch], len);
+    }
+    __syncwarp();  // the warp reconverges before the next round's masked collectives
   }
-  keys[slot] = key;
-  const unsigned am = __activemask(), lane = threadIdx.x & 31;
-  // near-wall particles go to the traction list: one atomic per warp on the shared counter
-  const unsigned nb = __ballot_sync(am, ok && near);
-  if (nb) {
-    const unsigned first = (unsigned)(__ffs(nb) - 1);
-    uint32_t w = 0u;
-    if (lane == first) w = atomicAdd(nw_count, (uint32_t)__popc(nb));
-    w = __shfl_sync(am, w, first);
-    if (ok && near) nw_list[w + __popc(nb & ((1u << lane) - 1u))] = (uint32_t)slot;
-  }
-  // particles arrive in binned order, so a warp's keys come in runs: one atomic per run of
-  // equal keys, and one per run of equal key chunks
-  uint32_t len = run_length(am, lane, key);
-  if (len) atomicAdd(&count[key], len);
-  const uint32_t ch = key / KEY_CHUNK;
-  len = run_length(am, lane, ch);
-  if (len) atomicAdd(&chunk_sum[ch], len);
 }
 
 // per instance: exclusive scan of its key-chunk sums (accumulated by k_bin_count), offset by the
-// instance's first slot
-__global__ void k_scan_instances(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
-                                 uint32_t* __restrict__ chunk_sum, uint32_t* __restrict__ chunk_base) {
-  __shared__ uint32_t sh[1024];
+// instance's first slot.  1024 threads take 4 consecutive chunks each per pass: warp shuffles scan
+// the thread sums, one warp scans the 32 warp totals.
+__global__ void __launch_bounds__(1024) k_scan_instances(const InstDesc* __restrict__ desc,
+                                                         const Control* __restrict__ ctrl,
+                                                         uint32_t* __restrict__ chunk_sum,
+                                                         uint32_t* __restrict__ chunk_base) {
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t pass_total;
   const int inst = blockIdx.x;
   if (!ctrl[inst].active) return;
   const InstDesc& D = desc[inst];
   const int64_t c0 = D.key_off / KEY_CHUNK, nc = D.nkeys / KEY_CHUNK;
+  const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint32_t carry = (uint32_t)D.slot_off;
-  for (int64_t base = 0; base < nc; base += 1024) {
-    const int64_t j = base + threadIdx.x;
-    uint32_t v = 0u;
-    if (j < nc) {
-      v = chunk_sum[c0 + j];
-      chunk_sum[c0 + j] = 0u;  // k_bin_count of the next attempt accumulates from zero
+  for (int64_t base = 0; base < nc; base += 4 * 1024) {
+    const int64_t j0 = base + 4 * (int64_t)threadIdx.x;
+    uint32_t v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      v[q] = 0u;
+      if (j0 + q < nc) {
+        v[q] = chunk_sum[c0 + j0 + q];
+        chunk_sum[c0 + j0 + q] = 0u;  // k_bin_count of the next attempt accumulates from zero
+      }
     }
-    sh[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-      uint32_t add = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
-      __syncthreads();
-      sh[threadIdx.x] += add;
-      __syncthreads();
+    const uint32_t tsum = v[0] + v[1] + v[2] + v[3];
+    uint32_t x = tsum;  // inclusive scan of the thread sums within the warp
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= (unsigned)off) x += y;
     }
-    if (j < nc) chunk_base[c0 + j] = carry + sh[threadIdx.x] - v;
-    const uint32_t total = sh[1023];
+    if (lane == 31) wsum[wid] = x;
     __syncthreads();
-    carry += total;
+    if (wid == 0) {
+      const uint32_t w = wsum[lane];
+      uint32_t t = w;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, t, off);
+        if (lane >= (unsigned)off) t += y;
+      }
+      wsum[lane] = t - w;  // exclusive prefix of the warp totals
+      if (lane == 31) pass_total = t;
+    }
+    __syncthreads();
+    uint32_t e = carry + wsum[wid] + x - tsum;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (j0 + q < nc) chunk_base[c0 + j0 + q] = e;
+      e += v[q];
+    }
+    carry += pass_total;
+    __syncthreads();  // wsum and pass_total are rewritten by the next pass
   }
 }
 
@@ -417,27 +472,51 @@ __global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* __restrict__
       make_uint4(e0, e0 + c4.x, e0 + c4.x + c4.y, e0 + c4.x + c4.y + c4.z);
 }
 
-__global__ void k_bin_scatter(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
-                              const int* __restrict__ pcta_inst, const uint32_t* __restrict__ keys,
-                              uint32_t* __restrict__ count, const uint32_t* __restrict__ start,
-                              uint32_t* __restrict__ perm) {
+// Each particle takes a place in its bin: one atomicSub per run of equal keys in a round, which
+// also leaves count at zero for the next attempt.  The order inside a bin follows the atomics and
+// is made deterministic by k_bin_sort.
+__global__ void __launch_bounds__(BIN_THREADS)
+    k_bin_scatter(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+                  const int* __restrict__ pcta_inst, const uint32_t* __restrict__ keys, uint32_t* __restrict__ count,
+                  const uint32_t* __restrict__ start, uint32_t* __restrict__ perm) {
   const int inst = pcta_inst[blockIdx.x];
   const Control& c = ctrl[inst];
   if (!c.active) return;
   const InstDesc& D = desc[inst];
-  const int64_t slot = (int64_t)blockIdx.x * G2P_THREADS + threadIdx.x;
-  if (slot - D.slot_off >= c.count) return;
-  const uint32_t key = keys[slot];
-  // one atomic per run of lanes with equal keys; leaves count at zero for the next attempt
-  const unsigned am = __activemask(), lane = threadIdx.x & 31;
-  const uint32_t len = run_length(am, lane, key);
-  const unsigned prev = __shfl_up_sync(am, key, 1);
-  const unsigned heads = __ballot_sync(am, lane == 0 || prev != key);
-  const unsigned leader = 31u - __clz(heads & ((2u << lane) - 1u));  // first lane of this run
-  uint32_t top = 0u;
-  if (len) top = atomicSub(&count[key], len);
-  top = __shfl_sync(am, top, leader);
-  perm[start[key] + top - 1u - (lane - leader)] = (uint32_t)slot;
+  const unsigned lane = threadIdx.x & 31;
+  const int64_t base = (int64_t)blockIdx.x * G2P_THREADS + (threadIdx.x >> 5) * (32 * BIN_ROUNDS) + lane;
+  const int64_t lim = D.slot_off + c.count;
+  uint32_t key[BIN_ROUNDS], top[BIN_ROUNDS], lead[BIN_ROUNDS], st[BIN_ROUNDS];
+  unsigned am[BIN_ROUNDS];
+#pragma unroll
+  for (int q = 0; q < BIN_ROUNDS; ++q) key[q] = base + 32 * q < lim ? keys[base + 32 * q] : 0u;
+#pragma unroll
+  for (int q = 0; q < BIN_ROUNDS; ++q) {
+    am[q] = __ballot_sync(0xffffffffu, base + 32 * q < lim);
+    top[q] = lead[q] = st[q] = 0u;
+  }
+#pragma unroll
+  for (int q = 0; q < BIN_ROUNDS; ++q) {
+    if (base + 32 * q < lim) {
+      const uint32_t len = run_length(am[q], lane, key[q]);
+      const unsigned prev = __shfl_up_sync(am[q], key[q], 1);
+      const unsigned heads = __ballot_sync(am[q], lane == 0 || prev != key[q]);
+      lead[q] = 31u - __clz(heads & ((2u << lane) - 1u));  // first lane of this lane's run
+      if (len) top[q] = atomicSub(&count[key[q]], len);
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int q = 0; q < BIN_ROUNDS; ++q) {
+    if (base + 32 * q < lim) {
+      top[q] = __shfl_sync(am[q], top[q], lead[q]);
+      st[q] = start[key[q]];
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int q = 0; q < BIN_ROUNDS; ++q)
+    if (base + 32 * q < lim) perm[st[q] + top[q] - 1u - (lane - lead[q])] = (uint32_t)(base + 32 * q);
 }
 
 // sort n <= R slot indices in registers (unrolled insertion network; unused entries sort last)
@@ -2718,7 +2797,7 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
   k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+  k_bin_count<<<(unsigned)A.n_pcta, BIN_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
@@ -2728,7 +2807,7 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
   k_scan_apply<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
+  k_bin_scatter<<<(unsigned)A.n_pcta, BIN_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
@@ -2794,11 +2873,11 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev) { ret
 int launch_audit(const DeviceArrays& A, double* buf, cudaStream_t s) {
   // transport pass: binning and an APIC-only deposit, its grid kinetic energy to buf[5 n_gcta + CTA]
   k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
-  k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+  k_bin_count<<<(unsigned)A.n_pcta, BIN_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
   k_scan_apply<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
-  k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
+  k_bin_scatter<<<(unsigned)A.n_pcta, BIN_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   int nt = 0;
   launch_tiles_p2g(A, s, 1, nullptr, nt);
@@ -2820,11 +2899,11 @@ __global__ void k_grid_sums(const long long* __restrict__ acc, int64_t node_tota
 
 int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
   k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
-  k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+  k_bin_count<<<(unsigned)A.n_pcta, BIN_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
   k_scan_apply<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
-  k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
+  k_bin_scatter<<<(unsigned)A.n_pcta, BIN_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   {
     int nt = 0;
@@ -2838,11 +2917,11 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
 
 int launch_grid_totals(const DeviceArrays& A, long long* out, cudaStream_t s) {
   k_begin<<<grid_of(A.n_inst, 64), 64, 0, s>>>(A.desc, A.ctrl, A.n_inst, A.nw_count, A.bed);
-  k_bin_count<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
+  k_bin_count<<<(unsigned)A.n_pcta, BIN_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap,
                                                           A.keys, A.count, A.chunk_sum, A.nw_list, A.nw_count);
   k_scan_instances<<<A.n_inst, 1024, 0, s>>>(A.desc, A.ctrl, A.chunk_sum, A.chunk_base);
   k_scan_apply<<<(unsigned)A.n_chunks, 256, 0, s>>>(A.count, A.chunk_base, A.start, A.chunk_inst, A.ctrl);
-  k_bin_scatter<<<(unsigned)A.n_pcta, G2P_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
+  k_bin_scatter<<<(unsigned)A.n_pcta, BIN_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.keys, A.count, A.start,
                                                             A.perm);
   {
     int nt = 0;
