@@ -622,6 +622,7 @@ __global__ void k_tiles(const InstDesc* __restrict__ desc, const Control* __rest
 // one global atomic.
 constexpr int P2G_CHUNK = 1024;
 constexpr int P2G_REC = 16;  // m, q[3], A[9], f[3]
+constexpr int P2G_PER_THREAD = (P2G_CHUNK + P2G_THREADS - 1) / P2G_THREADS;  // phase-1 particles per thread
 constexpr size_t P2G_PART_BYTES = sizeof(float4) * TB * 27;
 constexpr size_t P2G_REC_BYTES = sizeof(float) * P2G_REC * P2G_CHUNK;
 constexpr size_t P2G_SMEM = P2G_PART_BYTES > P2G_REC_BYTES ? P2G_PART_BYTES : P2G_REC_BYTES;
@@ -679,9 +680,17 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
   for (uint32_t c0 = ts; c0 < te; c0 += P2G_CHUNK) {
     const uint32_t cn = min((uint32_t)P2G_CHUNK, te - c0);
     if (c0 != ts) __syncthreads();  // the previous chunk's records are consumed
-    // phase 1: one thread per particle
-    for (uint32_t i = t; i < cn; i += P2G_THREADS) {
-      const int64_t src = perm[c0 + i];
+    // phase 1: one thread per particle.  The thread's permutation entries of the chunk are loaded
+    // first, so that each particle's state loads issue without waiting for its entry.
+    uint32_t srcs[P2G_PER_THREAD];
+#pragma unroll
+    for (int q = 0; q < P2G_PER_THREAD; ++q)
+      srcs[q] = t + q * P2G_THREADS < cn ? perm[c0 + t + q * P2G_THREADS] : 0u;
+#pragma unroll
+    for (int q = 0; q < P2G_PER_THREAD; ++q) {
+      const uint32_t i = t + q * P2G_THREADS;
+      if (i >= cn) break;
+      const int64_t src = srcs[q];
       float x[3], v[3], Cm[9], tau[6];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
