@@ -1,18 +1,22 @@
 // lp_kernels.cu - CUDA kernels of one MLS-MPM substep attempt (sm_100a).
 //
-// Attempt = begin -> bin (count, scan, scatter, id-sort) -> P2G -> wall traction -> grid update
-//           -> pellet coupling -> G2P + constitutive -> end (reduce, accept / reject, commit).
+// Attempt = begin -> bin (count, scan, scatter, slot sort) -> P2G -> wall traction -> grid update
+//           -> pellet coupling -> (warm-start table) -> G2P + constitutive -> end (reduce,
+//           accept / reject, commit).
 // Every kernel reads dt, the fixed-point scales and the buffer parity of its instance from the
 // device control block, so one attempt is a fixed launch sequence that a CUDA graph can replay.
 //
 // Reference mapping (nredd/litter-physics):
 //   k_begin        solver.rs:418-441 (dt selection of advance_while), 477-498 (stability_limit)
 //   k_bin_*        replaces sort_particles (solver.rs:501-517): a counting sort by stencil cell
-//                  every attempt; ties ordered by id, so the order is deterministic
+//                  every attempt; ties ordered by slot in the committed state, so the order is
+//                  deterministic
 //   k_p2g          deposit_particles (solver.rs:632-661), Grid::deposit (grid.rs:254-263)
 //   k_traction     wall_traction_to_grid (solver.rs:725-819), Grid::deposit_reaction (grid.rs:279-295)
 //   k_grid_update  grid_update (solver.rs:822-892), reduce_tangential_velocity (solver.rs:1145-1155)
 //   k_couple       couple_grid (rigid.rs:385-438), apply_impulse / integrate (rigid.rs:251-334)
+//   k_mlp_table    learned warm start of the HB return: the network tabulated per instance and dt
+//                  (no reference counterpart)
 //   k_g2p          grid_to_particle (solver.rs:895-977) + update_paste / update_liquid
 //   k_end          try_step_captured's accept/reject and commit (solver.rs:540-611, 980-998),
 //                  advance_while's bookkeeping (solver.rs:442-468)

@@ -150,10 +150,6 @@ __device__ __forceinline__ void mlp_write_row(uint32_t* row, const float (&f)[6]
   row[6] = 0u;
   row[7] = 0u;
 }
-__device__ __forceinline__ void mlp_zero_row(uint32_t* row) {
-#pragma unroll
-  for (int w = 0; w < 8; ++w) row[w] = 0u;
-}
 
 // Network output (logit of the root fraction) of the 32 feature rows at xs (row stride MLP_S1
 // words) for the lane's own row.  Every lane of the warp calls it, converged, after the rows
