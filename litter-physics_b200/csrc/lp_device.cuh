@@ -74,6 +74,7 @@ enum Status : int { S_RUNNING = 0, S_REACHED = 1, S_MIN_STEP = 2, S_ERROR = 3 };
 // per-instance constants (set at creation)
 struct InstDesc {
   double dx, inv_dx;
+  float pow2_inv_dx;  // 1 / (float)dx when (float)dx is a power of two (then x * it == x / dx), else 0
   int cells[3], nodes[3];
   int bins[3], tiles[3];
   int nblk[3];

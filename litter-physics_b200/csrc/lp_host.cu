@@ -638,6 +638,11 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
     std::memset(&D, 0, sizeof(D));
     D.dx = s.grid_spacing;
     D.inv_dx = 1.0 / s.grid_spacing;
+    {
+      const float f = (float)s.grid_spacing;
+      int e = 0;
+      D.pow2_inv_dx = (std::isfinite(f) && f > 0.f && std::frexp(f, &e) == 0.5f) ? 1.0f / f : 0.0f;
+    }
     for (int a = 0; a < 3; ++a) {
       D.cells[a] = (int)h.cells[a];
       D.nodes[a] = (int)h.nodes[a];

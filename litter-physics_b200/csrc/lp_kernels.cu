@@ -38,7 +38,11 @@ __device__ __forceinline__ int64_t node_index(const InstDesc& D, int i, int j, i
 }
 
 // Stencil base (padded) of a coordinate: floor(x/dx - 0.5) + 1 (grid.rs:151-182).
-__device__ __forceinline__ float scaled_of(float x, float dx) { return x / dx; }
+// x / dx in grid units.  For a power-of-two dx (pow2_inv_dx != 0) the product with its exact
+// reciprocal is the same correctly rounded quotient, without the division.
+__device__ __forceinline__ float scaled_of(float x, float dx, float pow2_inv_dx) {
+  return pow2_inv_dx != 0.0f ? x * pow2_inv_dx : x / dx;
+}
 
 __device__ __forceinline__ void weights_of(float fx, float dx, float w[3], float d[3]) {
   const float a0 = 1.5f - fx, a1 = fx - 1.0f, a2 = fx - 0.5f;
@@ -305,7 +309,7 @@ __device__ __forceinline__ uint32_t bin_key(const InstDesc& D, const float (&x)[
   near = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const float s = scaled_of(x[a], dx);
+    const float s = scaled_of(x[a], dx, D.pow2_inv_dx);
     const float bf = floorf(s - 0.5f);
     const float padded = bf + 1.0f;
     if (!(padded >= 0.0f) || padded + 2.0f >= (float)D.nodes[a]) ok = false;
@@ -719,7 +723,7 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
       // position relative to the particle's stencil base (its bin's base: floor(x/dx - 0.5))
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        const float sc = scaled_of(x[a], dx);
+        const float sc = scaled_of(x[a], dx, D.pow2_inv_dx);
         r[(13 + a) * P2G_CHUNK] = sc - floorf(sc - 0.5f);
       }
       // exact per-particle totals: FP64 products of the stored FP32 mass and velocity
@@ -914,7 +918,7 @@ __device__ void traction_particle(const InstDesc* __restrict__ desc, const Contr
     bool ok = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float sc = scaled_of(img[a], dx);
+      const float sc = scaled_of(img[a], dx, D.pow2_inv_dx);
       const float bf = floorf(sc - 0.5f);
       const float padded = bf + 1.0f;
       if (!(padded >= 0.0f) || padded + 2.0f >= (float)D.nodes[a]) ok = false;
@@ -2062,7 +2066,7 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         x[a] = in[(PF_X + a) * G2P_THREADS];
-        const float sc = scaled_of(x[a], dx);
+        const float sc = scaled_of(x[a], dx, D.pow2_inv_dx);
         const float bf = floorf(sc - 0.5f);
         base[a] = (int)(bf + 1.0f);
         weights_of(sc - bf, dx, w[a], d[a]);
@@ -2105,7 +2109,7 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
 #pragma unroll
       for (int a = 0; a < 9; ++a) Cm[a] *= dx2_inv;
       speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-      disp = speed * dt / dx;
+      disp = scaled_of(speed * dt, dx, D.pow2_inv_dx);
       m = in[PF_M * G2P_THREADS];
       v0 = in[PF_V0 * G2P_THREADS];
       ep = in[PF_EP * G2P_THREADS];
