@@ -154,6 +154,42 @@ def test_warm_table_matches_network(trained):
 
 
 @pytest.mark.gpu
+def test_batch_warm_tables_per_member(trained):
+    """Each batch member's warm-start table comes from its own material and dt: it equals the
+    table of a single simulation of the same spec, members with different flow indices get
+    different tables, and a weight upload marks every table stale until the next attempt."""
+    from litter_physics_b200 import configs
+    from litter_physics_b200.sim import Batch, Simulation
+
+    w, _ = trained
+    spec_a = configs.slump(16, (4, 4, 8), seed=1, yield_range=(20.0, 100.0))
+    spec_b = configs.slump(16, (4, 4, 8), seed=2, yield_range=(20.0, 100.0))
+    spec_b.material.flow_index = 0.8
+    batch = Batch([spec_a, spec_b])
+    batch.set_warm_start(w)
+    batch.run_substeps(2)
+    batch.sync()
+    ta, dta = batch.warm_table(0)
+    tb, dtb = batch.warm_table(1)
+    assert ta is not None and tb is not None and dta > 0.0 and dtb > 0.0
+    assert not np.array_equal(ta, tb)
+    one = Simulation(spec_a)
+    one.set_warm_start(w)
+    one.run_substeps(2)
+    one.sync()
+    t1, dt1 = one.warm_table()
+    assert dt1 == dta and np.array_equal(t1, ta)
+    batch.set_warm_start(w)  # a new upload: every table is rebuilt on the next attempt
+    assert batch.warm_table(0)[0] is None and batch.warm_table(1)[0] is None
+    batch.run_substeps(1)
+    batch.sync()
+    ta2, dta2 = batch.warm_table(0)
+    assert ta2 is not None and (dta2 != dta or np.array_equal(ta2, ta))
+    with pytest.raises(Exception):
+        batch.warm_table(2)
+
+
+@pytest.mark.gpu
 def test_warm_started_slump_matches_oracle(trained):
     """Warm start inside the solver (G2P's tensor-core network pass): the slump after 100
     substeps stays within the parity bars of the plain solver against the FP64 oracle, with
