@@ -168,36 +168,56 @@ __device__ void block_sum_ll_multi(long long (&v)[K], long long* sh /* NT/32*K +
   for (int k = 0; k < K; ++k) v[k] = sh[NW * K + k];
   __syncthreads();
 }
-// argmax of (value, index) over the block: largest value, lowest index on ties
-template <int NT>
-__device__ int block_argmax_ll(long long value, int index, long long* shv, int* shi) {
+// Sums of K int64 values over the block and, in the same pass, the argmax of (value, index):
+// largest value, lowest index on ties.  sh holds NW K + NW + K values and shi NW + 1 ints (NW
+// warps).  Two barriers; the caller must not rewrite sh or shi before another barrier.
+template <int NT, int K>
+__device__ int block_sum_argmax_ll(long long (&v)[K], long long value, int index, long long* sh, int* shi) {
   constexpr int NW = NT / 32;
+  warp_sum_ll_multi<K>(v);
+  auto better = [](long long ov, int oi, long long bv, int bi) { return ov > bv || (ov == bv && oi < bi); };
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const long long ov = __shfl_xor_sync(0xffffffffu, value, o);
     const int oi = __shfl_xor_sync(0xffffffffu, index, o);
-    if (ov > value || (ov == value && oi < index)) {
+    if (better(ov, oi, value, index)) {
       value = ov;
       index = oi;
     }
   }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) {
-    shv[w] = value;
+#pragma unroll
+    for (int k = 0; k < K; ++k) sh[w * K + k] = v[k];
+    sh[NW * K + w] = value;
     shi[w] = index;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 1; k < NW; ++k)
-      if (shv[k] > shv[0] || (shv[k] == shv[0] && shi[k] < shi[0])) {
-        shv[0] = shv[k];
-        shi[0] = shi[k];
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = lane < NW ? sh[lane * K + k] : 0;
+    warp_sum_ll_multi<K>(v);
+    long long bv = lane < NW ? sh[NW * K + lane] : LLONG_MIN;
+    int bi = lane < NW ? shi[lane] : INT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const long long ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (better(ov, oi, bv, bi)) {
+        bv = ov;
+        bi = oi;
       }
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) sh[NW * K + NW + k] = v[k];
+      shi[NW] = bi;
+    }
   }
   __syncthreads();
-  const int r = shi[0];
-  __syncthreads();
-  return r;
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = sh[NW * K + NW + k];
+  return shi[NW];
 }
 
 // Per-particle bound of the node momentum one particle can deposit (mass times speed, affine and
@@ -649,7 +669,7 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
   extern __shared__ float4 part[];  // particle records during the chunks, then TB * 27 partial node sums
   float* rec = reinterpret_cast<float*>(part);  // [P2G_REC][P2G_CHUNK]
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
-  __shared__ int redi[P2G_THREADS / 32];
+  __shared__ int redi[P2G_THREADS / 32 + 1];
   __shared__ uint32_t bstart[TB + 1];
 
   const int inst = tile_inst[tile];
@@ -830,8 +850,9 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
       for (int k = 0; k < 4; ++k) nv[k] += cs[k];
     }
     const long long heavy = has_node ? nv[0] : LLONG_MIN;
-    const int best = block_argmax_ll<P2G_THREADS>(heavy, t, red, redi);
-    block_sum_ll_multi<P2G_THREADS, 4>(cs, red);
+    // the sum of the shares and the heaviest node in one pass; red and redi are not written
+    // again before the barrier that ends the tile
+    const int best = block_sum_argmax_ll<P2G_THREADS, 4>(cs, heavy, t, red, redi);
     if (t == best) {
       nv[0] += Dm - cs[0];
       nv[1] += D0 - cs[1];
