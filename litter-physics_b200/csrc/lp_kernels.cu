@@ -146,7 +146,9 @@ __device__ __forceinline__ void warp_sum_ll_multi(long long (&v)[K]) {
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
 }
-template <int NT, int K>
+// TRAIL = false leaves out the closing barrier: the caller must not rewrite sh[NW K .. NW K + K)
+// before another barrier (the partial sums below it may be rewritten at once)
+template <int NT, int K, bool TRAIL = true>
 __device__ void block_sum_ll_multi(long long (&v)[K], long long* sh /* NT/32*K + K */) {
   constexpr int NW = NT / 32;
   warp_sum_ll_multi<K>(v);
@@ -166,7 +168,7 @@ __device__ void block_sum_ll_multi(long long (&v)[K], long long* sh /* NT/32*K +
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < K; ++k) v[k] = sh[NW * K + k];
-  __syncthreads();
+  if (TRAIL) __syncthreads();
 }
 // Sums of K int64 values over the block and, in the same pass, the argmax of (value, index):
 // largest value, lowest index on ties.  sh holds NW K + NW + K values and shi NW + 1 ints (NW
@@ -670,7 +672,6 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
   float* rec = reinterpret_cast<float*>(part);  // [P2G_REC][P2G_CHUNK]
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
   __shared__ int redi[P2G_THREADS / 32 + 1];
-  __shared__ uint32_t bstart[TB + 1];
 
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
@@ -685,8 +686,6 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
   const int ty = (int)((ltile / D.tiles[2]) % D.tiles[1]);
   const int tx = (int)(ltile / ((int64_t)D.tiles[2] * D.tiles[1]));
   const int t = threadIdx.x;
-  if (t <= TB) bstart[t] = start[key0 + t];
-  __syncthreads();
   const int bin = t / 3, slab = t % 3;
 
   const float* cur = c.parity ? st1 : st0;
@@ -704,7 +703,7 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
       for (int k = 0; k < 4; ++k) acc9[b][q][k] = 0.0f;
   long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // tile totals (particles) then halo sums (nodes)
 
-  const uint32_t s = bstart[bin], e = bstart[bin + 1];
+  const uint32_t s = start[key0 + bin], e = start[key0 + bin + 1];  // this bin's sorted range
   for (uint32_t c0 = ts; c0 < te; c0 += P2G_CHUNK) {
     const uint32_t cn = min((uint32_t)P2G_CHUNK, te - c0);
     if (c0 != ts) __syncthreads();  // the previous chunk's records are consumed
@@ -835,7 +834,8 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
     tot[6] = nv[2];
     tot[7] = nv[3];
   }
-  block_sum_ll_multi<P2G_THREADS, 8>(tot, red);
+  // no closing barrier: the pass below writes only red[0, 64), below the totals at red[96, 104)
+  block_sum_ll_multi<P2G_THREADS, 8, false>(tot, red);
   const long long Dm = tot[0] - tot[4], D0 = tot[1] - tot[5], D1 = tot[2] - tot[6], D2 = tot[3] - tot[7];
   if (Dm != 0 || D0 != 0 || D1 != 0 || D2 != 0) {
     // distribute the discrepancy in proportion to node mass, remainder to the heaviest node
