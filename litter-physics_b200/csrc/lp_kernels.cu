@@ -139,6 +139,24 @@ __device__ void block_reduce_multi(double (&v)[K], unsigned max_mask, double* sh
   for (int k = 0; k < K; ++k) v[k] = sh[NW * K + k];
   __syncthreads();
 }
+// block_reduce_multi for a caller that reads the result in thread 0 only: one barrier, the
+// totals end in warp 0, and sh must not be rewritten before the caller's next barrier
+template <int NT, int K>
+__device__ void block_reduce_multi_to0(double (&v)[K], unsigned max_mask, double* sh /* NT/32*K */) {
+  constexpr int NW = NT / 32;
+  static_assert(NT % 32 == 0 && NW <= 32, "block size");
+  warp_reduce_multi<K>(v, max_mask);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) sh[w * K + k] = v[k];
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = lane < NW ? sh[lane * K + k] : (((max_mask >> k) & 1u) ? -1e300 : 0.0);
+    warp_reduce_multi<K>(v, max_mask);
+  }
+}
 template <int K>
 __device__ __forceinline__ void warp_sum_ll_multi(long long (&v)[K]) {
 #pragma unroll
@@ -1175,7 +1193,7 @@ __global__ void __launch_bounds__(GU_THREADS)
     rv[RK - 2] = e_grav;
     rv[RK - 1] = e_walls;
   }
-  block_reduce_multi<GU_THREADS, RK>(rv, 1u << 6, shd);
+  block_reduce_multi_to0<GU_THREADS, RK>(rv, 1u << 6, shd);  // kernel end: thread 0 writes
   wi0 = rv[0];
   wi1 = rv[1];
   wi2 = rv[2];
@@ -1242,7 +1260,7 @@ __global__ void __launch_bounds__(GU_THREADS)
     }
   }
   double r[1] = {e};
-  block_reduce_multi<GU_THREADS, 1>(r, 0u, shd);
+  block_reduce_multi_to0<GU_THREADS, 1>(r, 0u, shd);
   if (t == 0) out[blockIdx.x] = r[0];
 }
 
@@ -2229,7 +2247,8 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
   cp_async_wait<0>();  // no copy may land after the CTA's shared memory is released
   double rv[9] = {diss, bb, mass_sum, (double)max_speed, (double)max_disp, (double)fail, (double)iters,
                   (double)yielded, fail_value};
-  block_reduce_multi<G2P_THREADS, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
+  // thread 0 writes the tile's partial; shd is next written after the tile-end barrier
+  block_reduce_multi_to0<G2P_THREADS, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
   if (threadIdx.x == 0) {
     ParticlePartial& P = part[tile];
     P.diss = rv[0];
@@ -2336,7 +2355,7 @@ __global__ void k_segments(const Control* __restrict__ ctrl, const SegDesc* __re
       v[12] = fmax(v[12], (double)P.fail);
     }
   }
-  block_reduce_multi<256, 13>(v, (1u << 10) | (1u << 11) | (1u << 12), shd);
+  block_reduce_multi_to0<256, 13>(v, (1u << 10) | (1u << 11) | (1u << 12), shd);
   if (t == 0) {
     SegPartial& o = out[blockIdx.x];
     for (int k = 0; k < 13; ++k) o.v[k] = v[k];
