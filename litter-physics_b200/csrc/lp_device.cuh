@@ -134,6 +134,16 @@ struct LedgerD {
       cpellet, plastic, outflow_momentum[3];
 };
 
+// Constants of the HB return (hb_return_d) that depend on the material (consistency K, flow
+// index n, shear modulus mu) and dt only: hb_const computes them once per instance and attempt
+// (k_begin) instead of per particle, with the expressions of the per-particle form, so the
+// results are the same.
+struct HbConst {
+  double k, mu3, viscous_scale, exponent, log_k, c1;  // K, 3 mu, 3 mu dt, 1/n, log K, 3 mu dt / n
+  int finite;                                         // K, n, mu and dt are finite
+  int pad;
+};
+
 // per-instance mutable control block (device resident)
 struct Control {
   double time, target;
@@ -163,6 +173,7 @@ struct Control {
   uint64_t bed_overflow;
   double bed_limit;  // step limit of the committed pellets (set on commit and by the host)
   double step_diss;  // plastic work of the last attempt, accepted or not (energy audit)
+  HbConst hb;        // HB return constants of the current attempt's dt (set by k_begin)
 };
 
 // pellet bed: tangential spring of one sphere pair (pellet-local sphere a, other pellet's b)
@@ -249,27 +260,38 @@ __device__ __forceinline__ void atomic_add_ll(long long* p, long long v) {
 }
 
 // ---------------------------------------------------------------- HB scalar return (FP64)
+__device__ inline HbConst hb_const(double k, double n, double mu, double dt) {
+  HbConst h;
+  h.finite = (isfinite(k) && isfinite(n) && isfinite(mu) && isfinite(dt)) ? 1 : 0;
+  h.k = k;
+  h.mu3 = 3.0 * mu;
+  h.viscous_scale = 3.0 * mu * dt;
+  h.exponent = 1.0 / n;
+  h.log_k = log(k);
+  h.c1 = h.viscous_scale * h.exponent;
+  h.pad = 0;
+  return h;
+}
+
 // Bracketed Newton of constitutive.rs:280-362, with an optional start value sigma0 in
 // (yield, trial) (the learned warm start); the plain solver starts at the midpoint.
 // Returns failure code; iterations through *iters.
-__device__ inline int hb_return_d(double trial, double ys, double k, double n, double mu, double dt, double tol_rel,
-                                  double sigma0, double* sigma_out, double* dep_out, int* iters) {
+__device__ inline int hb_return_d(double trial, double ys, const HbConst& h, double tol_rel, double sigma0,
+                                  double* sigma_out, double* dep_out, int* iters) {
   *iters = 0;
-  if (!(isfinite(trial) && isfinite(ys) && isfinite(k) && isfinite(n) && isfinite(mu) && isfinite(dt)))
-    return F_CONST_NONFINITE;
-  const double viscous_scale = 3.0 * mu * dt;
+  if (!(isfinite(trial) && isfinite(ys) && h.finite)) return F_CONST_NONFINITE;
+  const double viscous_scale = h.viscous_scale;
   if (trial <= ys) {
     *sigma_out = trial;
     *dep_out = 0.0;
     return F_OK;
   }
-  if (k <= 0.0) {
+  if (h.k <= 0.0) {
     *sigma_out = ys;
-    *dep_out = (trial - ys) / (3.0 * mu);
+    *dep_out = (trial - ys) / h.mu3;
     return F_OK;
   }
-  const double exponent = 1.0 / n;
-  const double log_k = log(k), c1 = viscous_scale * exponent;
+  const double exponent = h.exponent, log_k = h.log_k, c1 = h.c1;
   double lower = ys, upper = trial;
   double sigma = (sigma0 > lower && sigma0 < upper) ? sigma0 : 0.5 * (lower + upper);
   const double tolerance = tol_rel * fmax(trial, 1.0);
@@ -283,7 +305,7 @@ __device__ inline int hb_return_d(double trial, double ys, double k, double n, d
   for (int it = 1; it <= 200; ++it) {
     if (fabs(last) <= tolerance || (upper - lower) <= tolerance) {
       *sigma_out = sigma;
-      *dep_out = (trial - sigma) / (3.0 * mu);
+      *dep_out = (trial - sigma) / h.mu3;
       *iters = it;
       return F_OK;
     }
@@ -306,6 +328,11 @@ __device__ inline int hb_return_d(double trial, double ys, double k, double n, d
   }
   *iters = 200;
   return F_CONST_NOT_CONVERGED;
+}
+// the same with the constants computed here (one return problem per material)
+__device__ inline int hb_return_d(double trial, double ys, double k, double n, double mu, double dt, double tol_rel,
+                                  double sigma0, double* sigma_out, double* dep_out, int* iters) {
+  return hb_return_d(trial, ys, hb_const(k, n, mu, dt), tol_rel, sigma0, sigma_out, dep_out, iters);
 }
 
 // ---------------------------------------------------------------- symmetric 3x3 eigen (Jacobi)
@@ -375,8 +402,8 @@ struct PasteOut {
 // Eigen-decomposition path (any strain size).  sigma0: Newton start in (yield, trial), or -1 for
 // the reference's midpoint start.  trial_only: stop after the trial equivalent stress (o.trial).
 static __device__ __noinline__ void paste_update_jacobi(const float Htr[9], float mu, float lambda, double mu_d, double ys,
-                                           double k, double n, double dt, double tol, double sigma0,
-                                           bool trial_only, PasteOut& o) {
+                                                        const HbConst& h, double tol, double sigma0, bool trial_only,
+                                                        PasteOut& o) {
   o.fail = F_OK;
   o.iters = 0;
   o.yielded = 0;
@@ -453,7 +480,7 @@ static __device__ __noinline__ void paste_update_jacobi(const float Htr[9], floa
   if (trial_eq > ys && dnorm > 0.f) {
     double sigma, dep;
     int iters;
-    int e = hb_return_d(trial_eq, ys, k, n, mu_d, dt, tol, sigma0, &sigma, &dep, &iters);
+    int e = hb_return_d(trial_eq, ys, h, tol, sigma0, &sigma, &dep, &iters);
     o.iters = iters;
     if (e != F_OK) {
       o.fail = e;
@@ -576,7 +603,8 @@ __device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& 
 #pragma unroll
     for (int i = 0; i < 9; ++i) Hj[i] = Htr[i];
     PasteOut oj = o;
-    paste_update_jacobi(Hj, 0.f, 0.f, mu_d, 0.0, 0.0, 0.0, 0.0, 0.0, -1.0, true, oj);
+    const HbConst none = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0};  // the trial stops before the return
+    paste_update_jacobi(Hj, 0.f, 0.f, mu_d, 0.0, none, 0.0, -1.0, true, oj);
     o = oj;
     t.path = o.fail == F_OK ? PT_JACOBI : PT_DONE;
     t.trial_eq = o.trial;
@@ -632,16 +660,15 @@ __device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& 
 
 // Rest of the paste update after paste_trial: the Herschel-Bulkley return started at sigma0
 // (in (yield, trial), or -1 for the midpoint), the stress and the plastic correction of H.
-__device__ inline void paste_finish(const float Htr[9], float mu, float lambda, double mu_d, double ys, double k,
-                                    double n, double dt, double tol, double sigma0, const PasteTrial& t,
-                                    PasteOut& o) {
+__device__ inline void paste_finish(const float Htr[9], float mu, float lambda, double mu_d, double ys, const HbConst& h,
+                                    double tol, double sigma0, const PasteTrial& t, PasteOut& o) {
   if (t.path == PT_DONE) return;
   if (t.path == PT_JACOBI) {
     float Hj[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) Hj[i] = Htr[i];
     PasteOut oj = o;
-    paste_update_jacobi(Hj, mu, lambda, mu_d, ys, k, n, dt, tol, sigma0, false, oj);
+    paste_update_jacobi(Hj, mu, lambda, mu_d, ys, h, tol, sigma0, false, oj);
     o = oj;
     return;
   }
@@ -654,7 +681,7 @@ __device__ inline void paste_finish(const float Htr[9], float mu, float lambda, 
   if (trial_eq > ys && t.dnorm > 0.f) {
     double sigma, dep;
     int iters;
-    const int e = hb_return_d(trial_eq, ys, k, n, mu_d, dt, tol, sigma0, &sigma, &dep, &iters);
+    const int e = hb_return_d(trial_eq, ys, h, tol, sigma0, &sigma, &dep, &iters);
     o.iters = iters;
     if (e != F_OK) {
       o.fail = e;
@@ -725,7 +752,7 @@ __device__ inline void paste_update(const float Htr[9], float mu, float lambda, 
                                     double n, double dt, double tol, PasteOut& o) {
   PasteTrial t;
   paste_trial(Htr, mu_d, t, o);
-  paste_finish(Htr, mu, lambda, mu_d, ys, k, n, dt, tol, -1.0, t, o);
+  paste_finish(Htr, mu, lambda, mu_d, ys, hb_const(k, n, mu_d, dt), tol, -1.0, t, o);
 }
 
 // ---------------------------------------------------------------- liquid update (J - 1)

@@ -284,6 +284,7 @@ __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__
   if (c.forced_dt > 0.0) {
     c.active = (c.status == S_RUNNING || c.status == S_REACHED) ? 1 : 0;
     c.dt = c.forced_dt;
+    c.hb = hb_const(D.consistency, D.flow_index, D.mu, c.dt);
     c.limited = 0;
     return;
   }
@@ -319,6 +320,7 @@ __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__
   }
   c.limit = limit;
   c.dt = dt;
+  c.hb = hb_const(D.consistency, D.flow_index, D.mu, dt);
   c.limited = limited;
   c.active = 1;
 }
@@ -2203,8 +2205,7 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
       }
     }
     if (paste) {
-      paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, D.consistency, D.flow_index, c.dt, D.tol, sigma0, pt,
-                   o);
+      paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, c.hb, D.tol, sigma0, pt, o);
 #pragma unroll
       for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
       if (valid) {
