@@ -1,8 +1,8 @@
 """Drop-in for the reference's compiled extension `litter_physics._core` (core/src/lib.rs:11-57,
 python/litter_physics/_core.pyi): `protocol_version()` and `run_json(request_json, resume_json)`.
 
-Research mode runs on the GPU through `research.run`; household mode is outside this build's
-scope and is refused with ValueError, as the reference refuses any request it cannot run.
+Research mode runs on the GPU through `research.run`; household mode (the DEM litter model) is
+not part of the GPU substep and is refused with ValueError, as the reference refuses any request it cannot run.
 Every failure surfaces as ValueError, like the PyO3 binding's `PyValueError`.
 """
 
