@@ -38,6 +38,27 @@ def test_struct_layouts_match(L):
     assert L.lib().lp_abi_version() == 1
 
 
+def test_warm_table_constants_match_header(L):
+    """The warm-start table's node layout in the C header equals the Python mirror, and its nodes
+    cover every finite FP32 log(a)/8 the solver can form (a >= 1e-37)."""
+    import re
+
+    import numpy as np
+
+    from litter_physics_b200 import _abi
+
+    text = L.HEADER.read_text()
+    defs = dict(re.findall(r"#define (LP_MLP_TAB_\w+) (.+)", text))
+    assert int(defs["LP_MLP_TAB_N"]) == _abi.MLP_TAB_N
+    nums = {k: [float(x) for x in re.findall(r"-?\d+\.\d+", v)] for k, v in defs.items()}
+    lo = nums["LP_MLP_TAB_LO"][0]
+    h = nums["LP_MLP_TAB_H"][0] / nums["LP_MLP_TAB_H"][1]  # written as a quotient
+    assert lo == _abi.MLP_TAB_LO and h == _abi.MLP_TAB_H
+    nodes = np.float32(lo) + np.arange(_abi.MLP_TAB_N, dtype=np.float32) * np.float32(h)
+    assert np.array_equal(nodes.astype(np.float64), lo + np.arange(_abi.MLP_TAB_N) * h)  # exact in FP32
+    assert nodes[0] < np.log(1e-37) / 8 and nodes[-1] > np.log(np.finfo(np.float32).max) / 8
+
+
 def test_material_helpers_match_reference_formulas(L, oracle_mod):
     """constitutive.rs:146-243 on both sides of the boundary (host arithmetic only)."""
     lib = L.lib()
