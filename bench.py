@@ -35,8 +35,11 @@ sys.path.insert(0, str(ROOT / "litter-physics_b200"))
 
 METRIC = "particle-substeps/s, warm-started vs plain HB MPM on 1 B200 at equal residual"
 UNIT = "particle-substeps/s"
-G2P_BYTES_PER_PARTICLE = 176.0  # algorithmic: 52 B read + 124 B written per particle-substep
+G2P_BYTES_PER_PARTICLE = 176.0  # algorithmic: 52 B read (x, F-I, eps_p) + 124 B written (x v C F-I eps_p tau)
 P2G_BYTES_PER_PARTICLE = 92.0   # algorithmic: x, v, C, tau(sym), m, V0 read
+G2P_BYTES_LIQUID = 104.0        # algorithmic: 16 B read (x, J) + 88 B written (x v C J tau)
+STEP_BYTES_PASTE = 215.0        # whole substep, paste: state read + written once, m V0, grid share
+STEP_BYTES_LIQUID = 143.0       # whole substep, liquid: x v C J read + written, m V0, grid share
 
 
 def log(*a):
@@ -246,28 +249,123 @@ def bed_measurement(args, stream, torch) -> dict:
     return out
 
 
-def reference_arm(args, ws, rank):
-    if rank != 0:
-        return
+def large_slump_sample():
+    """The large slump's grid spacing (1/256 m), material and per-particle yield stress on a
+    32^3-cell column: 262,144 particles, a bounded CPU sample of the 16.8M-particle column."""
     from litter_physics_b200 import configs
 
+    return configs.slump(256, (32, 32, 32), seed=2, yield_range=(20.0, 100.0))
+
+
+def reference_arm(args, ws, rank):
+    """The reference algorithm (FP64 oracle restatement, all host threads) on the large-slump
+    sample: W untimed warm-up substeps, then exactly K timed substeps."""
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
     threads = len(os.sched_getaffinity(0))
-    sample = configs.slump(256, (32, 32, 32), seed=2, yield_range=(20.0, 100.0))
-    spec_fn = lambda: sample  # noqa: E731
-    for _ in range(args.warmup):
-        pass  # each oracle run builds its own state; the first substep inside is untimed
-    res = cpu_baseline_run(spec_fn, max(1, args.steps // 10), threads)
+    spec = large_slump_sample()
+    sim = oracle.OracleSim(spec, threads=threads)
+    n = int(oracle.lib().ora_sim_particle_count(sim._h))
+    sim.advance_to(args.warmup * spec.max_dt)
+    t0 = time.perf_counter()
+    sim.advance_to((args.warmup + args.steps) * spec.max_dt)
+    seconds = time.perf_counter() - t0
+    steps = int(sim.counters().step_count) - args.warmup
+    value = n * steps / seconds
     line = {
-        "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / res["steps"],
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * seconds / max(steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "large HB slump sample: config-2 grid spacing and material, 32^3-cell column "
                                "(262,144 particles), FP64 oracle restatement of the reference step"},
-        "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{res['steps']} substeps x {res['particles']} particles after 1 untimed"},
-        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{steps} timed substeps x {n} particles after {args.warmup} untimed"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    sim.close()
     print(json.dumps(line), flush=True)
+
+
+def parity_measurement(weights, steps: int = 100) -> dict:
+    """Error of the headline path against the reference algorithm on identical seeded inputs:
+    the large-slump sample (262,144 particles, per-particle yield stress) warm-started on the
+    GPU and in the FP64 oracle for `steps` substeps; particles matched by id.  Runs outside
+    every timed region."""
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    from litter_physics_b200.sim import Simulation
+
+    spec = large_slump_sample()
+    t0 = time.perf_counter()
+    ref = oracle.OracleSim(spec, threads=len(os.sched_getaffinity(0)))
+    ref.advance_to(steps * spec.max_dt)
+    sim = Simulation(spec)
+    sim.set_warm_start(weights)
+    sim.advance_to(steps * spec.max_dt)
+    g, r = sim.particles(), ref.particles()
+    og, orr = np.argsort(g["id"]), np.argsort(r["id"])
+    assert np.array_equal(g["id"][og], r["id"][orr])
+    dx = float(np.abs(g["position"][og] - r["position"][orr]).max()) / max(spec.domain)
+    dv = float(np.linalg.norm(g["velocity"][og] - r["velocity"][orr]) / np.linalg.norm(r["velocity"]))
+    lg, lr = sim.ledger, ref.ledger()
+    led = {}
+    for f in ("gravity_impulse", "wall_impulse"):
+        a, b = np.array(getattr(lg, f)), np.array(getattr(lr, f))
+        led[f] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    for f in ("wall_normal_projection_energy", "wall_friction_dissipation", "wall_normal_traction_energy",
+              "plastic_dissipation"):
+        a, b = getattr(lg, f), getattr(lr, f)
+        if b != 0.0:
+            led[f] = abs(a - b) / abs(b)
+    gc, rc = sim.counters, ref.counters()
+    out = {"workload": "large-slump sample (262,144 particles, 256^3 grid spacing, yield U(20,100) Pa), "
+                       f"warm-started, {steps} substeps against the FP64 oracle",
+           "max_dx_over_L": dx, "dv_rel": dv, "ledger_rel": max(led.values()), "ledger_rel_by_field": led,
+           "steps_equal": bool(gc.step_count == rc.step_count and gc.rejected_steps == rc.rejected_steps),
+           "bars": {"max_dx_over_L": 1e-5, "dv_rel": 1e-5}, "seconds": round(time.perf_counter() - t0, 1)}
+    sim.close()
+    ref.close()
+    return out
+
+
+def config_measurement(name: str, spec, args, stream, torch, develop: int) -> dict:
+    """A single-simulation configuration timed like the headline arm: `develop` untimed
+    substeps, W warm-up and K timed substeps on the library's stream, kernel times by CUDA
+    events, and the whole-step and per-kernel rooflines."""
+    from litter_physics_b200.sim import Simulation
+
+    sim = Simulation(spec)
+    sim.set_stream(stream.cuda_stream)
+    n = sim.particle_count()
+    sim.run_substeps(develop + args.warmup)
+    sim.sync()
+    ms, accepted = time_steps(sim, args.steps, stream, torch)
+    kt = sim.kernel_times(args.kernel_steps)
+    liquid = spec.material.kind == 1
+    step_bytes = STEP_BYTES_LIQUID if liquid else STEP_BYTES_PASTE
+    g2p_bytes = G2P_BYTES_LIQUID if liquid else G2P_BYTES_PER_PARTICLE
+    peaks = measured_peaks()
+
+    def roof(kernel, bytes_per_particle, seconds):
+        a = bytes_per_particle * n / seconds / 1e9
+        return {"kernel": kernel, "bound": "hbm", "achieved": a, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": a / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                "algorithmic_bytes_per_particle": bytes_per_particle}
+
+    ms_step = ms / max(accepted, 1)
+    out = {"workload": name, "particles": n, "value": n * accepted / (ms / 1e3), "unit": UNIT,
+           "ms_per_step": ms_step, "accepted": accepted, "develop_substeps": develop,
+           "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
+           "roofline_step": roof("whole substep", step_bytes, ms_step / 1e3),
+           "roofline_g2p": roof("k_g2p", g2p_bytes, kt["k_g2p"] / 1e3),
+           "roofline_p2g": roof("k_p2g", P2G_BYTES_PER_PARTICLE, kt["k_p2g"] / 1e3)}
+    sim.close()
+    return out
 
 
 def ours(args, ws, rank, local):
@@ -387,6 +485,16 @@ def ours(args, ws, rank, local):
         return
     batch_info = None if args.no_batch else batch_measurement(args, stream, torch)
     bed_info = None if args.no_batch else bed_measurement(args, stream, torch)
+    if args.no_batch:
+        config0_info = config1_info = None
+    else:
+        config0_info = config_measurement(
+            "config 0: plain HB slump, 64^3 grid, 16x16x32-cell column, 65,536 particles, seed 0, dt 1e-4, "
+            "plain Newton tol 1e-10", configs.config0(), args, stream, torch, develop=150)
+        config1_info = config_measurement(
+            "config 1: Tait dam break, 128^3 grid, 64x32x64-cell block, 1,048,576 particles, seed 1, gamma 7, "
+            "dt <= 5e-5", configs.config1(), args, stream, torch, develop=150)
+    parity = None if args.no_parity else parity_measurement(weights)
     peaks = measured_peaks()
     g2p_ms = ktimes.get("k_g2p", float("nan"))
     achieved = G2P_BYTES_PER_PARTICLE * n / (g2p_ms / 1e3) / 1e9
@@ -395,7 +503,7 @@ def ours(args, ws, rank, local):
     p2g_achieved = P2G_BYTES_PER_PARTICLE * n / (p2g_ms / 1e3) / 1e9
     p2g_traffic = committed_traffic("k_p2g")
     threads = len(os.sched_getaffinity(0))
-    cpu = cpu_baseline_run(lambda: configs.slump(256, (32, 32, 32), seed=2, yield_range=(20.0, 100.0)), 2, threads)
+    cpu = cpu_baseline_run(large_slump_sample, 10, threads)
     warm, plain = results["warm"], results["plain"]
     line = {
         "metric": METRIC,
@@ -442,6 +550,9 @@ def ours(args, ws, rank, local):
                 "d2h_bytes_per_step": bytes_out / steps_done,
                 "path": "lp_sim_import_particles -> lp_sim_advance -> lp_sim_export_particles (host FP64 buffers)",
                 "steps": steps_done},
+        "parity": parity,
+        "config0": config0_info,
+        "config1": config1_info,
         "batch_config3": batch_info,
         "pellet_bed_config4": bed_info,
         "gpu_launches": int(launches["warm"]),
@@ -461,7 +572,9 @@ def main():
     ap.add_argument("--workload", default="config2", choices=["config2", "config0", "small"])
     ap.add_argument("--no-warm", action="store_true", help="skip the learned warm start (profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and CPU legs (profiling)")
-    ap.add_argument("--no-batch", action="store_true", help="skip the config-3 and config-4 measurements")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the config-0, config-1, config-3 and config-4 measurements")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity check of the headline path")
     ap.add_argument("--develop", type=int, default=150)
     ap.add_argument("--graph", type=int, default=0)
     ap.add_argument("--log-steps", type=int, default=300)

@@ -190,6 +190,20 @@ class Simulation:
         return {"grid_mass": out[0], "grid_momentum": np.array(out[1:4]), "particle_mass": out[4],
                 "particle_momentum": np.array(out[5:8])}
 
+    def grid_dump(self, dt: float) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """P2G and wall traction of the committed state with step `dt`: (node mass, node
+        momentum before the wall reactions, signed wall reaction impulse), dense padded node
+        order ((n+3)^3 nodes, grid.rs:71-109).  The simulation state is unchanged."""
+        nodes = [int(round(d / self.spec.grid_spacing)) + 3 for d in self.spec.domain]
+        nn = nodes[0] * nodes[1] * nodes[2]
+        mass = np.zeros(nn)
+        mom = np.zeros((nn, 3))
+        reaction = np.zeros((nn, 3))
+        D = C.POINTER(C.c_double)
+        check(lib().lp_sim_grid_dump(self._h, float(dt), mass.ctypes.data_as(D), mom.ctypes.data_as(D),
+                                     reaction.ctypes.data_as(D), nn))
+        return mass, mom, reaction
+
     def kernel_times(self, steps: int) -> dict:
         """Mean per-kernel duration (ms) over `steps` attempts, CUDA events on the stream."""
         cap = 24

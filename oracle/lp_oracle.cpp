@@ -2549,6 +2549,28 @@ void ora_set_threads(int32_t threads) {
 #endif
 }
 
+// deposit_particles (solver.rs:632-661) then wall_traction_to_grid (solver.rs:725-819) on a copy:
+// node mass, node momentum without the wall reactions, and the signed reaction impulse each node
+// received (Grid::deposit_reaction, grid.rs:279-295: impulse = inward_impulse * inward, so the
+// reference's post-traction momentum is momentum + reaction).
+int64_t ora_sim_probe_grid(ora_sim* s, double dt, double* mass, double* momentum, double* reaction) {
+  Simulation copy = s->sim;
+  copy.sweep_outflow();
+  copy.deposit_particles(dt);
+  const int64_t n = copy.grid.layout.node_count();
+  if (momentum)
+    for (int64_t i = 0; i < n; ++i) v3_out(copy.grid.momentum[i], momentum + 3 * i);
+  V3 imp;
+  double e;
+  copy.wall_traction(dt, imp, e);
+  if (mass)
+    for (int64_t i = 0; i < n; ++i) mass[i] = copy.grid.mass[i];
+  if (reaction)
+    for (int64_t i = 0; i < n; ++i)
+      v3_out(sub(copy.grid.traction_low[i], copy.grid.traction_high[i]), reaction + 3 * i);
+  return (int64_t)copy.grid.active.size();
+}
+
 int64_t ora_sim_probe_p2g(ora_sim* s, double dt, double* mass, double* momentum, double* traction_energy,
                           double traction_impulse[3]) {
   Simulation copy = s->sim;

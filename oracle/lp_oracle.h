@@ -54,6 +54,11 @@ void ora_set_threads(int32_t threads);
 int64_t ora_sim_probe_p2g(ora_sim* s, double dt, double* mass, double* momentum, double* traction_energy,
                           double traction_impulse[3]);
 
+/* Grid probe of one step's scatter (solver.rs:632-661 then 725-819) on a copy: node mass,
+ * node momentum before the wall reactions, and the signed reaction impulse of each node
+ * (3 per node), in dense padded node order; returns the active node count. */
+int64_t ora_sim_probe_grid(ora_sim* s, double dt, double* mass, double* momentum, double* reaction);
+
 /* constitutive.rs functions on scalars */
 int32_t ora_hb_return(double trial, double yield, double consistency, double flow_index, double mu,
                       double dt, double tol_rel, double out[3]);

@@ -72,6 +72,8 @@ def lib():
         D = C.POINTER(C.c_double)
         L.ora_sim_probe_p2g.argtypes = [P, C.c_double, D, D, D, D]
         L.ora_sim_probe_p2g.restype = C.c_int64
+        L.ora_sim_probe_grid.argtypes = [P, C.c_double, D, D, D]
+        L.ora_sim_probe_grid.restype = C.c_int64
         L.ora_hb_return.argtypes = [C.c_double] * 7 + [D]
         L.ora_hb_return.restype = C.c_int32
         L.ora_update_paste.argtypes = [D, C.POINTER(_abi.Material), C.c_double, C.c_double, C.c_double, D, D, D]
@@ -224,6 +226,16 @@ class OracleSim:
         imp = np.zeros(3)
         active = lib().ora_sim_probe_p2g(self._h, dt, _dptr(mass), _dptr(mom), C.byref(e), _dptr(imp))
         return mass, mom, e.value, imp, active
+
+
+    def probe_grid(self, dt: float, node_count: int):
+        """One step's P2G deposit and wall traction on a copy: (node mass, node momentum before
+        the reactions, signed reaction impulse per node), dense padded node order."""
+        mass = np.zeros(node_count)
+        mom = np.zeros((node_count, 3))
+        reaction = np.zeros((node_count, 3))
+        lib().ora_sim_probe_grid(self._h, dt, _dptr(mass), _dptr(mom), _dptr(reaction))
+        return mass, mom, reaction
 
 
 def hb_return(trial, yield_stress, consistency, flow_index, mu, dt, tol=1e-12):

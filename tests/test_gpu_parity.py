@@ -2,11 +2,13 @@
 
 Bars (north-star parity contract):
   * particle positions: max_p |x_gpu - x_ref| / L_domain <= 1e-5 after 100 substeps;
-  * particle velocities: ||v_gpu - v_ref||_2 / max(||v_ref||_2, sqrt(N) g t) <= 1e-5 after 100
-    substeps (particles matched by id, since both sides reorder them).  The gravity scale
-    sqrt(N) g t only matters for a column at rest (hydrostatic fixture), whose reference
-    velocities are discretisation noise five orders of magnitude below g t;
-  * grid mass and momentum after P2G equal the particle totals to 1e-10 relative;
+  * particle velocities: ||v_gpu - v_ref||_2 / ||v_ref||_2 <= 1e-5 after 100 substeps
+    (particles matched by id, since both sides reorder them).  The hydrostatic column at rest
+    has reference velocities that are discretisation noise, not a velocity scale; there the
+    bar is absolute, per particle, in m/s (see the test);
+  * grid mass and momentum after P2G equal the particle totals to 1e-10 relative (the P2G
+    tile totals are exact by construction), and node by node the deposit and the wall
+    reactions agree with the oracle's FP64 grid to 1e-6 of the grid's scale;
   * ledger totals: relative agreement stated per field below (FP32 device arithmetic against
     FP64 reference arithmetic).
 """
@@ -39,14 +41,13 @@ def by_id(p: dict) -> dict:
     return {k: v[order] for k, v in p.items()}
 
 
-def compare(gpu: dict, ref: dict, length: float, v_floor: float = 0.0) -> dict:
+def compare(gpu: dict, ref: dict, length: float) -> dict:
     g, r = by_id(gpu), by_id(ref)
     assert np.array_equal(g["id"], r["id"])
     x_err = float(np.max(np.abs(g["position"] - r["position"]))) / length
     v_ref = float(np.linalg.norm(r["velocity"]))
     dv = float(np.linalg.norm(g["velocity"] - r["velocity"]))
-    return {"x": x_err, "v": dv / max(v_ref, v_floor, 1e-300), "v_rel_ref": dv / max(v_ref, 1e-300),
-            "v_norm": v_ref}
+    return {"x": x_err, "v": dv / max(v_ref, 1e-300), "v_norm": v_ref}
 
 
 def run_pair(spec, steps: int):
@@ -93,14 +94,28 @@ def test_100_substeps_match_oracle(lib_built, name):
         spec = research.spec_from_request(load_request(name))
     gpu, ref = run_pair(spec, 100)
     length = max(spec.domain)
-    pg = gpu.particles()
-    g_t = math.sqrt(sum(v * v for v in spec.gravity)) * gpu.time
-    d = compare(pg, ref.particles(), length, v_floor=math.sqrt(len(pg["id"])) * g_t)
-    print(name, d)
+    pg, pr = gpu.particles(), ref.particles()
+    d = compare(pg, pr, length)
     gc, rc = gpu.counters, ref.counters()
     assert gc.step_count == rc.step_count and gc.rejected_steps == rc.rejected_steps
     assert d["x"] <= POS_TOL, d
-    assert d["v"] <= VEL_TOL, d
+    if name == "research_hydrostatic_water":
+        # A column at rest: the reference velocities are the residual of gravity against the
+        # pressure gradient, not a physical velocity scale, so the bar is absolute.  Per step,
+        # FP32 rounding of positions and stress (relative 2^-23) perturbs each particle's
+        # acceleration by about (h / dx) 2^-23 |g|, the pressure-gradient cancellation of a
+        # column of h / dx cells; over n steps that is n (h / dx) 2^-23 |g| dt.  The bar is 8
+        # times that bound, per particle.
+        g = math.sqrt(sum(v * v for v in spec.gravity))
+        cells_high = spec.initial_size[2] / spec.grid_spacing
+        bar = 8.0 * gc.step_count * cells_high * 2.0**-23 * g * spec.max_dt
+        gv, rv = by_id(pg)["velocity"], by_id(pr)["velocity"]
+        err = np.linalg.norm(gv - rv, axis=1)
+        print(name, d, f"max |dv| {err.max():.3e} m/s, rms {np.sqrt(np.mean(err**2)):.3e} m/s, bar {bar:.3e} m/s")
+        assert err.max() <= bar, (err.max(), bar)
+    else:
+        print(name, d)
+        assert d["v"] <= VEL_TOL, d
 
 
 def test_ledgers_match_oracle(lib_built):
@@ -127,6 +142,58 @@ def test_grid_conserves_mass_and_momentum(lib_built):
     assert abs(t["grid_mass"] - t["particle_mass"]) <= 1e-10 * t["particle_mass"]
     scale = np.linalg.norm(t["particle_momentum"])
     assert np.linalg.norm(t["grid_momentum"] - t["particle_momentum"]) <= 1e-10 * scale
+
+
+def random_state(p: dict, spec, rng) -> dict:
+    """A developed state made generic: positions jittered by up to 0.3 cells (kept inside the
+    domain), random velocities, affine fields and symmetric Kirchhoff stresses, every value
+    rounded to FP32 so that the device and the oracle start from the same numbers."""
+    q = {k: v.copy() for k, v in p.items()}
+    n = len(q["id"])
+    dx = spec.grid_spacing
+    lo, hi = 0.25 * dx, np.array(spec.domain) - 0.25 * dx
+    q["position"] = np.clip(q["position"] + rng.uniform(-0.3 * dx, 0.3 * dx, (n, 3)), lo, hi)
+    q["velocity"] = q["velocity"] + rng.normal(scale=0.05, size=(n, 3))
+    q["affine"] = q["affine"] + rng.normal(scale=2.0, size=(n, 3, 3))
+    s = rng.normal(scale=200.0, size=(n, 3, 3))
+    q["kirchhoff"] = q["kirchhoff"] + 0.5 * (s + s.transpose(0, 2, 1))
+    for k in ("position", "velocity", "affine", "kirchhoff"):
+        q[k] = np.ascontiguousarray(q[k].astype(np.float32).astype(np.float64))
+    return q
+
+
+@pytest.mark.parametrize("name", ["slump32", "dam_break"])
+def test_p2g_and_traction_match_oracle_node_by_node(lib_built, name):
+    """P2G (solver.rs:632-661, grid.rs:254-263) and the wall traction (solver.rs:725-819,
+    grid.rs:279-295) of one generic state, node by node against the oracle's FP64 grid: mass,
+    momentum before the reactions and the signed reaction impulses, including the wall shell."""
+    import oracle
+    from litter_physics_b200 import configs
+    from litter_physics_b200.sim import Simulation
+
+    spec = small_slump() if name == "slump32" else configs.dam_break(32, (16, 8, 16), seed=1)
+    sim = Simulation(spec)
+    sim.advance_to(30 * spec.max_dt)
+    state = random_state(sim.particles(), spec, np.random.default_rng(3))
+    sim.set_particles(state)
+    ref = oracle.OracleSim(spec)
+    ref.set_particles(state)
+    dt = spec.max_dt
+    gm, gp, gr = sim.grid_dump(dt)
+    rm, rp, rr = ref.probe_grid(dt, len(gm))
+    m_scale, p_scale = rm.max(), np.abs(rp).max()
+    r_scale = np.abs(rr).max()
+    assert m_scale > 0 and p_scale > 0 and r_scale > 0  # the case has deposits and wall reactions
+    m_err = np.abs(gm - rm).max() / m_scale
+    p_err = np.abs(gp - rp).max() / p_scale
+    r_err = np.abs(gr - rr).max() / r_scale
+    walls = np.count_nonzero(np.any(rr != 0.0, axis=1))
+    print(name, f"nodes {np.count_nonzero(rm)}, wall nodes {walls}, mass {m_err:.2e}, momentum {p_err:.2e}, "
+          f"reaction {r_err:.2e}")
+    assert m_err <= 1e-6 and p_err <= 1e-6 and r_err <= 1e-6
+    # the probe leaves the committed state untouched
+    after = sim.particles()
+    assert np.array_equal(by_id(after)["position"], by_id(state)["position"])
 
 
 def test_runs_are_bitwise_repeatable(lib_built):
