@@ -361,11 +361,15 @@ lp_status lp_mlp_loss_grad(const float* weights, int32_t nweights, const float* 
  * weights[lp_mlp_weight_count()], x[6*n], y[n] in; loss[1], grad[lp_mlp_weight_count()] out.
  * Work space is a fixed static device array of the library sized for at most
  * LP_MLP_NOALLOC_MAX_SAMPLES samples (about 4.5 MB per GPU that loads the library, held until
- * exit); larger n returns LP_INVALID.  The first call on each device looks up that array's
- * device address, so make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU (other streams, other host threads) race and must be
- * serialised by the caller.  stream is a cudaStream_t (NULL = default stream); the call
- * returns after queueing the work. */
+ * exit); larger n returns LP_INVALID.  With CUDA's lazy module loading the driver reserves
+ * that array when the library's device code is first used on a device, by this call or by any
+ * earlier library call: a caller whose memory pool takes all free device memory makes one
+ * library call first.  The first call on each device looks up that array's device address,
+ * so make that first call before any stream capture; the address stays valid until the
+ * device's primary context is reset (cudaDeviceReset), after which the library must be
+ * reloaded.  All calls share the array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller.  stream is a cudaStream_t
+ * (NULL = default stream); the call returns after queueing the work. */
 #define LP_MLP_NOALLOC_MAX_SAMPLES 4096
 lp_status lp_mlp_loss_grad_noalloc(const float* weights, const float* x, const float* y, int64_t n, float* loss,
                                    float* grad, void* stream);

@@ -855,6 +855,9 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
     tot[7] = nv[3];
   }
   // no closing barrier: the pass below writes only red[0, 64), below the totals at red[96, 104)
+  constexpr int P2G_NW = P2G_THREADS / 32;
+  static_assert(P2G_NW * 4 + P2G_NW + 4 <= P2G_NW * 8,
+                "the argmax pass's scratch must stay below the totals that block_sum_ll_multi leaves in red");
   block_sum_ll_multi<P2G_THREADS, 8, false>(tot, red);
   const long long Dm = tot[0] - tot[4], D0 = tot[1] - tot[5], D1 = tot[2] - tot[6], D2 = tot[3] - tot[7];
   if (Dm != 0 || D0 != 0 || D1 != 0 || D2 != 0) {

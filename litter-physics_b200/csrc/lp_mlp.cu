@@ -8,6 +8,7 @@
 //                  partials are summed in slice order (deterministic);
 //   k_mlp_adam   : Adam update.
 // Loss = mean over the batch of (out - y)^2, with y = logit of the root fraction.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -259,7 +260,28 @@ constexpr int64_t NA_LOSS = NA_G3 + NOALLOC_MAX;
 constexpr int64_t NA_PART = NA_LOSS + (NOALLOC_MAX + 255) / 256;
 constexpr int64_t NA_TOTAL = NA_PART + (int64_t)lp::MLP_SPLIT * lp::MLP_NW;
 constexpr int kMaxDevices = 64;
-float* g_noalloc_ptr[kMaxDevices] = {nullptr};
+// Device address of g_noalloc_scratch per device, looked up once.  Atomic so that host threads
+// making their first call at the same time both store the same address without a data race.
+std::atomic<float*> g_noalloc_ptr[kMaxDevices];
+
+// Device buffers of one allocating call, freed on every return path.
+struct DevBufs {
+  std::vector<void*> ptrs;
+  ~DevBufs() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <typename T>
+  cudaError_t alloc(T** p, size_t bytes) {
+    *p = nullptr;
+    void* q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, bytes);
+    if (e == cudaSuccess) {
+      ptrs.push_back(q);
+      *p = static_cast<T*>(q);
+    }
+    return e;
+  }
+};
 }  // namespace
 
 static __device__ __align__(256) float g_noalloc_scratch[NA_TOTAL];
@@ -277,13 +299,14 @@ lp_status lp_mlp_loss_grad_noalloc(const float* w, const float* x, const float* 
   int dev = 0;
   MCK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return mlp_fail(LP_DEVICE, "device index out of range");
-  if (g_noalloc_ptr[dev] == nullptr) {
+  float* S = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (S == nullptr) {
     // one-time set-up on this device: the host-side name is not a device address
     void* ptr = nullptr;
     MCK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-    g_noalloc_ptr[dev] = static_cast<float*>(ptr);
+    S = static_cast<float*>(ptr);
+    g_noalloc_ptr[dev].store(S, std::memory_order_release);
   }
-  float* S = g_noalloc_ptr[dev];
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const unsigned nb = (unsigned)((n + 255) / 256);
   lp::k_mlp_sample<<<nb, 256, 0, st>>>(w, x, y, n, S + NA_H1, S + NA_H2, S + NA_DZ1, S + NA_DZ2, S + NA_G3,
@@ -321,11 +344,9 @@ lp_status lp_mlp_loss_grad(const float* w, int32_t nw, const float* x, const flo
   MlpBuffers B;
   lp_status st = B.alloc(n);
   if (st != LP_OK) return st;
-  float *X = nullptr, *Y = nullptr;
-  MCK(cudaMalloc(&X, sizeof(float) * n * lp::MLP_IN));
-  MCK(cudaMalloc(&Y, sizeof(float) * n));
-  B.X = X;
-  B.Y = Y;
+  MCK(cudaMalloc(&B.X, sizeof(float) * n * lp::MLP_IN));  // owned by B from here on
+  MCK(cudaMalloc(&B.Y, sizeof(float) * n));
+  float *X = B.X, *Y = B.Y;
   MCK(cudaMemcpy(B.W, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(X, x, sizeof(float) * n * lp::MLP_IN, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(Y, y, sizeof(float) * n, cudaMemcpyHostToDevice));
@@ -344,11 +365,9 @@ lp_status lp_mlp_train(float* w, int32_t nw, const float* x, const float* y, int
   MlpBuffers B;
   lp_status st = B.alloc(b);
   if (st != LP_OK) return st;
-  float *X = nullptr, *Y = nullptr;
-  MCK(cudaMalloc(&X, sizeof(float) * n * lp::MLP_IN));
-  MCK(cudaMalloc(&Y, sizeof(float) * n));
-  B.X = X;
-  B.Y = Y;
+  MCK(cudaMalloc(&B.X, sizeof(float) * n * lp::MLP_IN));  // owned by B from here on
+  MCK(cudaMalloc(&B.Y, sizeof(float) * n));
+  float *X = B.X, *Y = B.Y;
   MCK(cudaMemcpy(B.W, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(X, x, sizeof(float) * n * lp::MLP_IN, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(Y, y, sizeof(float) * n, cudaMemcpyHostToDevice));
@@ -384,19 +403,17 @@ lp_status lp_mlp_forward(const float* w, int32_t nw, const float* x, int64_t n, 
   if (!w || nw != lp::MLP_NW || n <= 0) return mlp_fail(LP_INVALID, "bad arguments");
   int dc = 0;
   if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return mlp_fail(LP_DEVICE, "no CUDA device");
+  DevBufs bufs;  // freed on every return path
   float *W = nullptr, *X = nullptr, *Y = nullptr;
-  MCK(cudaMalloc(&W, sizeof(float) * lp::MLP_NW));
-  MCK(cudaMalloc(&X, sizeof(float) * n * lp::MLP_IN));
-  MCK(cudaMalloc(&Y, sizeof(float) * n));
+  MCK(bufs.alloc(&W, sizeof(float) * lp::MLP_NW));
+  MCK(bufs.alloc(&X, sizeof(float) * n * lp::MLP_IN));
+  MCK(bufs.alloc(&Y, sizeof(float) * n));
   MCK(cudaMemcpy(W, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(X, x, sizeof(float) * n * lp::MLP_IN, cudaMemcpyHostToDevice));
   lp::k_mlp_infer<<<(unsigned)((n + 255) / 256), 256>>>(W, X, n, Y);
   lp::add_kernel_launches(1);
   MCK(cudaGetLastError());
   MCK(cudaMemcpy(y, Y, sizeof(float) * n, cudaMemcpyDeviceToHost));
-  cudaFree(W);
-  cudaFree(X);
-  cudaFree(Y);
   return LP_OK;
 }
 
@@ -404,12 +421,13 @@ lp_status lp_mlp_forward_mma(const float* w, int32_t nw, const float* x, int64_t
   if (!w || nw != lp::MLP_NW || n <= 0) return mlp_fail(LP_INVALID, "bad arguments");
   int dc = 0;
   if (cudaGetDeviceCount(&dc) != cudaSuccess || dc == 0) return mlp_fail(LP_DEVICE, "no CUDA device");
+  DevBufs bufs;  // freed on every return path
   float *W = nullptr, *X = nullptr, *Y = nullptr;
   lp::MlpPacked* P = nullptr;
-  MCK(cudaMalloc(&W, sizeof(float) * lp::MLP_NW));
-  MCK(cudaMalloc(&P, sizeof(lp::MlpPacked)));
-  MCK(cudaMalloc(&X, sizeof(float) * n * lp::MLP_IN));
-  MCK(cudaMalloc(&Y, sizeof(float) * n));
+  MCK(bufs.alloc(&W, sizeof(float) * lp::MLP_NW));
+  MCK(bufs.alloc(&P, sizeof(lp::MlpPacked)));
+  MCK(bufs.alloc(&X, sizeof(float) * n * lp::MLP_IN));
+  MCK(bufs.alloc(&Y, sizeof(float) * n));
   MCK(cudaMemcpy(W, w, sizeof(float) * lp::MLP_NW, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(X, x, sizeof(float) * n * lp::MLP_IN, cudaMemcpyHostToDevice));
   lp::launch_mlp_pack(W, P, 0);
@@ -417,10 +435,6 @@ lp_status lp_mlp_forward_mma(const float* w, int32_t nw, const float* x, int64_t
   lp::add_kernel_launches(1);
   MCK(cudaGetLastError());
   MCK(cudaMemcpy(y, Y, sizeof(float) * n, cudaMemcpyDeviceToHost));
-  cudaFree(W);
-  cudaFree(P);
-  cudaFree(X);
-  cudaFree(Y);
   return LP_OK;
 }
 

@@ -54,6 +54,38 @@ def test_noalloc_loss_grad_matches_allocating_entry_point():
         assert np.abs(got - ref_grad).max() <= TOL * np.abs(ref_grad).max()
 
 
+def test_noalloc_call_on_a_side_stream_allocates_nothing():
+    """After the first call has set the work space up, a call queued on another stream leaves
+    the device's free memory unchanged and still matches the allocating entry point."""
+    import torch
+
+    from litter_physics_b200 import _lib as L
+    from litter_physics_b200 import warmstart
+
+    L.build()
+    w = warmstart.init_weights(seed=5)
+    rng = np.random.default_rng(12)
+    n = 2048
+    x = rng.normal(size=(n, 6)).astype(np.float32)
+    y = rng.normal(size=n).astype(np.float32)
+    dw, dx, dy = torch.from_numpy(w).cuda(), torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    dloss = torch.zeros(1, device="cuda")
+    dgrad = torch.zeros(w.size, device="cuda")
+    side = torch.cuda.Stream()
+    args = (dw.data_ptr(), dx.data_ptr(), dy.data_ptr(), n, dloss.data_ptr(), dgrad.data_ptr(), side.cuda_stream)
+    L.check(L.lib().lp_mlp_loss_grad_noalloc(*args))  # set-up call (may be the first on this device)
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        L.check(L.lib().lp_mlp_loss_grad_noalloc(*args))
+    side.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    ref_loss, ref_grad = _host_loss_grad(L, w, x, y)
+    assert abs(dloss.item() - ref_loss) <= TOL * abs(ref_loss)
+    assert np.abs(dgrad.cpu().numpy() - ref_grad).max() <= TOL * np.abs(ref_grad).max()
+
+
 def test_noalloc_rejects_sizes_beyond_its_work_space():
     import torch
 
