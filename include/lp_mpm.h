@@ -309,6 +309,10 @@ lp_status lp_batch_set_warm_start(lp_batch* b, const float* weights, int32_t nwe
 /* lp_sim_warm_table for member `instance` of a batch. */
 lp_status lp_batch_warm_table(lp_batch* b, int32_t instance, float* out, int32_t capacity, double* dt);
 lp_status lp_batch_use_graph(lp_batch* b, int32_t steps);
+/* lp_sim_kernel_times for a whole batch: each kernel's mean duration over `steps` attempts of
+ * every instance at once.  No counterpart in the reference. */
+lp_status lp_batch_kernel_times(lp_batch* b, int32_t steps, double* ms, char* names, int32_t capacity,
+                                int32_t* count);
 /* Per-instance views, so that each instance of a batched sweep reports what the reference's
  * sweep (python/litter_physics/sweep.py:206-262) gets from running that job alone. */
 lp_status lp_batch_get_pellet(lp_batch* b, int32_t index, lp_pellet* out, int32_t* has_pellet);
@@ -319,8 +323,29 @@ lp_status lp_batch_energies(lp_batch* b, int32_t index, double out[9]);
  * beyond the padded grid; a stopped instance's reason goes to `message`.  Stopped instances
  * stay stopped while the others advance. */
 lp_status lp_batch_instance_state(lp_batch* b, int32_t index, int32_t* state, char* message, size_t message_len);
-/* Autotuner: times the candidate tile/block shapes on the live batch and keeps the fastest. */
+/* Launch shape of the persistent tile kernels (bin sort, P2G, G2P) and of the attempt loop.  No
+ * counterpart in the reference (its loops run on rayon's pool).  Every shape gives the same
+ * results; only the speed differs.
+ *   g2p_small      1: G2P CTAs of 128 threads, 0: 256 threads
+ *   g2p_per_sm     persistent G2P CTAs per SM (0, or more than fit: as many as fit)
+ *   p2g_small      1: P2G chunks of 512 particles, 0: 1024 particles
+ *   p2g_per_sm     persistent P2G CTAs per SM (0, or more than fit: as many as fit)
+ *   dynamic_tiles  1: CTAs take occupied tiles from an atomic cursor, 0: round robin
+ *   graph_attempts attempts captured per CUDA graph replay of run_substeps (0 or 1: no graph)
+ * The getter reports the CTAs per SM the launches use. */
+typedef struct lp_launch_shape {
+  int32_t g2p_small, g2p_per_sm, p2g_small, p2g_per_sm, dynamic_tiles, graph_attempts;
+} lp_launch_shape;
+lp_status lp_sim_set_launch_shape(lp_sim* sim, const lp_launch_shape* shape);
+lp_status lp_sim_get_launch_shape(lp_sim* sim, lp_launch_shape* out);
+lp_status lp_batch_set_launch_shape(lp_batch* b, const lp_launch_shape* shape);
+lp_status lp_batch_get_launch_shape(lp_batch* b, lp_launch_shape* out);
+/* Autotuner: a coordinate search over the launch shape on the live ensemble (tile scheduling,
+ * G2P block shape and CTAs per SM, P2G chunk and CTAs per SM, attempts per graph), each candidate
+ * timed over trial_steps real attempts (time advances); keeps the fastest shape and writes one
+ * line per candidate and the choice to report. */
 lp_status lp_batch_autotune(lp_batch* b, int32_t trial_steps, char* report, size_t report_len);
+lp_status lp_sim_autotune(lp_sim* sim, int32_t trial_steps, char* report, size_t report_len);
 
 /* ---------------- constitutive kernels on host arrays (unit parity) ---------------- */
 /* out[3*i] = equivalent stress, out[3*i+1] = plastic increment, out[3*i+2] = iterations;

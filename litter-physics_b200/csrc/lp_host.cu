@@ -8,6 +8,7 @@
 // layout at the boundary.  It never computes a substep on the host: without a CUDA device every
 // entry point that needs one fails with LP_DEVICE.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -396,10 +397,13 @@ struct Ensemble {
   std::vector<Control> ctrl_h;
   double* d_diag = nullptr;
   double* d_audit = nullptr;  // energy-audit partials, 6 per grid-update CTA
-  // staging of host-layout particle chunks for import / export (38 doubles + 1 id per particle)
+  // staging of host-layout particle chunks for import / export (38 doubles + 1 id per particle),
+  // two slots so that the host copies of one chunk overlap the transfer and conversion of the
+  // other; stage_ev[s] marks the end of the device work that last used slot s
   double* d_stage = nullptr;
   double* h_stage = nullptr;  // pinned host twin of d_stage
-  int64_t stage_particles = 0;
+  int64_t stage_particles = 0;  // particles per slot
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   unsigned long long* d_bad = nullptr;
   float* d_mlp = nullptr;
   lp::MlpPacked* d_mlp_pk = nullptr;
@@ -415,6 +419,10 @@ struct Ensemble {
     allocs.clear();
     if (h_stage) cudaFreeHost(h_stage);
     h_stage = nullptr;
+    for (cudaEvent_t& ev : stage_ev) {
+      if (ev) cudaEventDestroy(ev);
+      ev = nullptr;
+    }
     if (own_stream) cudaStreamDestroy(own_stream);
     own_stream = nullptr;
   }
@@ -777,7 +785,7 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   ALLOC(A.chunk_base, A.n_chunks);
   ALLOC(A.perm, A.cap);
   ALLOC(A.nw_list, A.cap);
-  ALLOC(A.nw_count, 2);
+  ALLOC(A.nw_count, 5);
   A.tile_count = A.nw_count + 1;
   ALLOC(A.tile_list, A.n_tiles);
   ALLOC(A.acc, 4 * A.node_total);
@@ -882,29 +890,159 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   return push_ctrl(E);
 }
 
+// Queue `steps` attempts: with a graph length G > 1, floor(steps / G) replays of a CUDA graph of G
+// attempts (captured on first use) and the remainder as plain launches.
 lp_status run_attempts(Ensemble& E, int steps) {
   if (steps <= 0) return LP_OK;
-  if (E.graph_steps > 0 && steps == E.graph_steps) {
+  const int G = E.graph_steps;
+  if (G > 1 && steps >= G) {
     if (!E.graph_exec) {
       cudaStream_t cs = E.stream;
       CUDA_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
       int kernels = 0;
-      for (int s = 0; s < steps; ++s) kernels += lp::launch_attempt(E.A, cs);
+      for (int s = 0; s < G; ++s) kernels += lp::launch_attempt(E.A, cs);
       cudaGraph_t g = nullptr;
       CUDA_CK(cudaStreamEndCapture(cs, &g));
       E.graph = g;
       CUDA_CK(cudaGraphInstantiate(&E.graph_exec, g, 0));
-      // kernels counted while capturing correspond to this first replay
+      // kernels counted while capturing correspond to the first replay below
       E.graph_kernels = kernels;
       CUDA_CK(cudaGraphLaunch(E.graph_exec, E.stream));
-      return LP_OK;
+      steps -= G;
     }
-    CUDA_CK(cudaGraphLaunch(E.graph_exec, E.stream));
-    lp::add_kernel_launches((uint64_t)E.graph_kernels);
-    return LP_OK;
+    for (; steps >= G; steps -= G) {
+      CUDA_CK(cudaGraphLaunch(E.graph_exec, E.stream));
+      lp::add_kernel_launches((uint64_t)E.graph_kernels);
+    }
   }
   for (int s = 0; s < steps; ++s) lp::launch_attempt(E.A, E.stream);
   CUDA_CK(cudaGetLastError());
+  return LP_OK;
+}
+
+// ---------------------------------------------------------------- launch shapes and autotuner
+lp_status set_targets(Ensemble& E, double target, bool forced_reset);
+
+static lp_status set_launch_shape(Ensemble& E, const lp_launch_shape* in) {
+  if (!in) return set_error(LP_INVALID, "null launch shape");
+  if (in->g2p_small < 0 || in->g2p_small > 1 || in->p2g_small < 0 || in->p2g_small > 1 || in->dynamic_tiles < 0 ||
+      in->dynamic_tiles > 1 || in->g2p_per_sm < 0 || in->p2g_per_sm < 0 || in->graph_attempts < 0)
+    return set_error(LP_INVALID, "launch shape fields out of range");
+  E.invalidate_graph();
+  E.A.shape.g2p_small = in->g2p_small;
+  E.A.shape.g2p_per_sm = in->g2p_per_sm;
+  E.A.shape.p2g_small = in->p2g_small;
+  E.A.shape.p2g_per_sm = in->p2g_per_sm;
+  E.A.shape.dynamic = in->dynamic_tiles;
+  E.graph_steps = in->graph_attempts > 1 ? in->graph_attempts : 0;
+  return LP_OK;
+}
+static lp_status get_launch_shape(Ensemble& E, lp_launch_shape* out) {
+  if (!out) return set_error(LP_INVALID, "null launch shape");
+  int lim[6];
+  lp::launch_shape_limits(lim);
+  const lp::LaunchShape& L = E.A.shape;
+  out->g2p_small = L.g2p_small;
+  out->p2g_small = L.p2g_small;
+  out->dynamic_tiles = L.dynamic;
+  // the CTAs per SM the launches use: the request, at most the resident limit
+  const int g2p_lim = lim[L.g2p_small ? 4 : 3], p2g_lim = lim[L.p2g_small ? 2 : 1];
+  out->g2p_per_sm = (L.g2p_per_sm > 0 && L.g2p_per_sm < g2p_lim) ? L.g2p_per_sm : g2p_lim;
+  out->p2g_per_sm = (L.p2g_per_sm > 0 && L.p2g_per_sm < p2g_lim) ? L.p2g_per_sm : p2g_lim;
+  out->graph_attempts = E.graph_steps > 1 ? E.graph_steps : 1;
+  return LP_OK;
+}
+static std::string shape_text(const lp_launch_shape& s) {
+  char b[160];
+  std::snprintf(b, sizeof(b), "g2p_threads=%d g2p_per_sm=%d p2g_chunk=%d p2g_per_sm=%d dynamic_tiles=%d graph_attempts=%d",
+                s.g2p_small ? 128 : 256, s.g2p_per_sm, s.p2g_small ? 512 : 1024, s.p2g_per_sm, s.dynamic_tiles,
+                s.graph_attempts);
+  return b;
+}
+
+// Coordinate search over the launch shape on the live ensemble: one knob at a time (tile
+// scheduling, G2P block shape and CTAs per SM, P2G chunk and CTAs per SM, attempts per graph
+// replay), each candidate timed over trial_steps attempts with CUDA events after two untimed
+// ones, keeping the fastest value before moving to the next knob.  The attempts are real steps:
+// time advances and every accepted step is a valid step of the trajectory.  Every candidate
+// gives the same results (the tile kernels' results do not depend on these choices), so only
+// the speed differs.
+static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t report_len) {
+  if (trial_steps < 1) return set_error(LP_INVALID, "trial_steps must be at least 1");
+  if (E.ctrl_h.empty() || !std::isinf(E.ctrl_h[0].target)) {
+    lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
+    if (st != LP_OK) return st;
+  }
+  int lim[6];
+  lp::launch_shape_limits(lim);
+  lp_launch_shape best;
+  lp_status st = get_launch_shape(E, &best);
+  if (st != LP_OK) return st;
+  best.g2p_per_sm = best.p2g_per_sm = 0;  // 0: as many as fit
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CUDA_CK(cudaEventCreate(&e0));
+  CUDA_CK(cudaEventCreate(&e1));
+  std::string rep;
+  auto measure = [&](const lp_launch_shape& s, float* ms_per_attempt) -> lp_status {
+    lp_status r = set_launch_shape(E, &s);
+    if (r != LP_OK) return r;
+    const int per = std::max(1, s.graph_attempts);
+    const int reps = std::max(1, trial_steps / per);
+    r = run_attempts(E, per);  // untimed (captures the graph)
+    if (r != LP_OK) return r;
+    r = run_attempts(E, per);
+    if (r != LP_OK) return r;
+    CUDA_CK(cudaEventRecord(e0, E.stream));
+    for (int k = 0; k < reps; ++k) {
+      r = run_attempts(E, per);
+      if (r != LP_OK) return r;
+    }
+    CUDA_CK(cudaEventRecord(e1, E.stream));
+    CUDA_CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CUDA_CK(cudaEventElapsedTime(&ms, e0, e1));
+    *ms_per_attempt = ms / (float)(reps * per);
+    rep += shape_text(s) + " ms_per_attempt=" + std::to_string(*ms_per_attempt) + "\n";
+    return LP_OK;
+  };
+  float best_ms = 0.f;
+  st = measure(best, &best_ms);
+  // one knob at a time; each candidate list holds complete field values for that knob
+  struct Knob {
+    std::vector<std::array<int, 2>> values;  // (small / dynamic / graph, per-SM) pairs
+    int which;                               // 0 dynamic, 1 G2P, 2 P2G, 3 graph
+  };
+  std::vector<Knob> knobs = {
+      {{{0, 0}, {1, 0}}, 0},
+      {{{0, 0}, {0, 1}, {1, 0}, {1, std::max(1, lim[4] - 1)}}, 1},
+      {{{0, 0}, {0, 1}, {1, 0}}, 2},
+      {{{1, 0}, {4, 0}, {16, 0}}, 3},
+  };
+  for (const Knob& kb : knobs) {
+    if (st != LP_OK) break;
+    for (const auto& v : kb.values) {
+      lp_launch_shape c = best;
+      if (kb.which == 0) c.dynamic_tiles = v[0];
+      else if (kb.which == 1) c.g2p_small = v[0], c.g2p_per_sm = v[1];
+      else if (kb.which == 2) c.p2g_small = v[0], c.p2g_per_sm = v[1];
+      else c.graph_attempts = v[0];
+      if (std::memcmp(&c, &best, sizeof(c)) == 0) continue;  // measured already
+      float ms = 0.f;
+      st = measure(c, &ms);
+      if (st != LP_OK) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != LP_OK) return st;
+  st = set_launch_shape(E, &best);
+  if (st != LP_OK) return st;
+  rep += "chosen: " + shape_text(best) + " ms_per_attempt=" + std::to_string(best_ms) + "\n";
+  if (report && report_len) std::snprintf(report, report_len, "%s", rep.c_str());
   return LP_OK;
 }
 
@@ -977,12 +1115,13 @@ const char* fail_text(int f) {
 }
 
 // ---------------------------------------------------------------- export / import
-// Particles per staging chunk of import and export: 2^21 x 308 B = 646 MB of device memory.
-static const int64_t STAGE_CHUNK = (int64_t)1 << 21;
+// Particles per staging slot of import and export: 2^20 x 308 B = 323 MB of device memory and
+// as much pinned host memory, twice (two slots).
+static const int64_t STAGE_CHUNK = (int64_t)1 << 20;
 
-// Device staging for `count` particles and its pinned host twin; carves the host-layout arrays
-// out of the device one.
-static lp_status stage_chunk(Ensemble& E, int64_t count, lp::HostParticleChunk& h) {
+// Two staging slots of up to STAGE_CHUNK particles on the device, their pinned host twins and
+// the slot events (allocated once, grown when a larger set arrives).
+static lp_status stage_alloc(Ensemble& E, int64_t count) {
   const int64_t want = std::min<int64_t>(std::max<int64_t>(count, 1), STAGE_CHUNK);
   if (E.stage_particles < want) {
     cudaStreamSynchronize(E.stream);
@@ -994,20 +1133,28 @@ static lp_status stage_chunk(Ensemble& E, int64_t count, lp::HostParticleChunk& 
     if (E.h_stage) cudaFreeHost(E.h_stage);
     E.h_stage = nullptr;
     E.stage_particles = 0;
-    lp_status st = E.alloc(&E.d_stage, (size_t)want * 39);
+    lp_status st = E.alloc(&E.d_stage, (size_t)want * 39 * 2);
     if (st != LP_OK) return st;
-    if (cudaHostAlloc((void**)&E.h_stage, sizeof(double) * 39 * (size_t)want, cudaHostAllocDefault) != cudaSuccess) {
+    if (cudaHostAlloc((void**)&E.h_stage, sizeof(double) * 39 * 2 * (size_t)want, cudaHostAllocDefault) !=
+        cudaSuccess) {
       E.h_stage = nullptr;
       return set_error(LP_DEVICE, "cudaHostAlloc of the particle staging buffer failed");
     }
     E.stage_particles = want;
   }
+  for (cudaEvent_t& ev : E.stage_ev)
+    if (!ev) CUDA_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   if (!E.d_bad) {
     lp_status st = E.alloc(&E.d_bad, 1);
     if (st != LP_OK) return st;
   }
+  return LP_OK;
+}
+
+// The host-layout arrays of staging slot `slot` (0 or 1), carved out of the device buffer.
+static void stage_slot(Ensemble& E, int slot, lp::HostParticleChunk& h) {
   const int64_t c = E.stage_particles;
-  double* b = E.d_stage;
+  double* b = E.d_stage + (size_t)slot * 39 * (size_t)c;
   h.position = b;
   h.velocity = b + 3 * c;
   h.affine = b + 6 * c;
@@ -1019,10 +1166,9 @@ static lp_status stage_chunk(Ensemble& E, int64_t count, lp::HostParticleChunk& 
   h.volume0 = b + 36 * c;
   h.yield_stress = b + 37 * c;
   h.id = reinterpret_cast<uint32_t*>(b + 38 * c);
-  return LP_OK;
 }
 
-// memcpy of the listed (destination, source, bytes) spans over a few host threads
+// memcpy of the listed (destination, source, bytes) spans over up to 16 host threads
 struct CopySpan {
   void* dst;
   const void* src;
@@ -1032,7 +1178,7 @@ static void parallel_copy(const std::vector<CopySpan>& spans) {
   size_t total = 0;
   for (const CopySpan& c : spans) total += c.bytes;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const unsigned nt = (unsigned)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total >> 24));
+  const unsigned nt = (unsigned)std::min<size_t>(std::min(16u, hw), std::max<size_t>(1, total >> 23));
   auto run = [&](unsigned k) {
     // thread k copies bytes [k total / nt, (k + 1) total / nt) of the concatenated spans
     const size_t lo = total * k / nt, hi = total * (k + 1) / nt;
@@ -1059,7 +1205,9 @@ static inline void* host_twin(const Ensemble& E, const void* dev) {
 }
 
 // Export instance i's committed particles into the caller's FP64 arrays (null fields are
-// skipped): chunks are converted on the device and copied back one array at a time.
+// skipped).  Chunk k is converted on the device into staging slot k % 2 and copied to its pinned
+// twin (one copy per requested field); while those run, host threads copy chunk k - 1 from the
+// other slot's pinned twin into the caller's arrays.
 lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
   lp_status st = pull_ctrl(E);
   if (st != LP_OK) return st;
@@ -1067,16 +1215,22 @@ lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
   const InstDesc& D = E.desc[i];
   const int64_t n = c.count;
   if ((int64_t)out->count < n) return set_error(LP_INVALID, "particle buffer too small");
-  lp::HostParticleChunk h;
-  st = stage_chunk(E, n, h);
+  st = stage_alloc(E, n);
   if (st != LP_OK) return st;
-  for (int64_t first = 0; first < n; first += E.stage_particles) {
+  std::vector<CopySpan> pending[2];  // host copies waiting for slot s's device-to-host copies
+  int64_t k = 0;
+  for (int64_t first = 0; first < n; first += E.stage_particles, ++k) {
+    const int slot = (int)(k & 1);
     const int64_t m = std::min(E.stage_particles, n - first);
+    lp::HostParticleChunk h;
+    stage_slot(E, slot, h);
     lp::launch_export(h, m, first, E.A.st[c.parity], E.A.id[c.parity], E.A.cap, D.slot_off, D.kind == 0,
                       D.per_particle_yield, D.yield, E.stream);
     CUDA_CK(cudaGetLastError());
-    // device staging -> pinned twin (one copy per requested field) -> caller arrays (host threads)
-    std::vector<CopySpan> spans;
+    // device staging -> pinned twin (one copy per requested field); the host copy to the caller
+    // arrays runs after the slot's event, one chunk later
+    std::vector<CopySpan>& spans = pending[slot];
+    spans.clear();
     auto back = [&](void* dst, const void* src, size_t bytes) -> lp_status {
       if (!dst) return LP_OK;
       void* pinned = host_twin(E, src);
@@ -1097,8 +1251,16 @@ lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
         back(out->volume0 ? out->volume0 + first : nullptr, h.volume0, d1) != LP_OK ||
         back(out->yield_stress ? out->yield_stress + first : nullptr, h.yield_stress, d1) != LP_OK)
       return LP_DEVICE;
-    CUDA_CK(cudaStreamSynchronize(E.stream));
-    parallel_copy(spans);
+    CUDA_CK(cudaEventRecord(E.stage_ev[slot], E.stream));
+    if (k > 0) {  // chunk k - 1: its copies have landed once the other slot's event has
+      CUDA_CK(cudaEventSynchronize(E.stage_ev[slot ^ 1]));
+      parallel_copy(pending[slot ^ 1]);
+    }
+  }
+  if (k > 0) {
+    const int last = (int)((k - 1) & 1);
+    CUDA_CK(cudaEventSynchronize(E.stage_ev[last]));
+    parallel_copy(pending[last]);
   }
   out->count = (uint64_t)n;
   return LP_OK;
@@ -1118,15 +1280,22 @@ lp_status import_particles(Ensemble& E, int i, const lp_particles* in) {
   if (n > 0 && (!in->id || !in->position || !in->velocity || !in->affine || !in->deformation || !in->kirchhoff ||
                 !in->volume_ratio || !in->plastic_strain || !in->mass || !in->volume0))
     return set_error(LP_INVALID, "imported particles need every array but yield_stress");
-  lp::HostParticleChunk h;
-  st = stage_chunk(E, n, h);
+  st = stage_alloc(E, n);
   if (st != LP_OK) return st;
   const int par = c.parity ^ 1;
   const unsigned long long none = ~0ull;
   CUDA_CK(cudaMemcpyAsync(E.d_bad, &none, sizeof(none), cudaMemcpyHostToDevice, E.stream));
-  for (int64_t first = 0; first < n; first += E.stage_particles) {
+  // Chunk k goes through staging slot k % 2: host threads fill the slot's pinned twin while the
+  // device still copies and converts chunk k - 1 from the other slot; a slot is refilled only
+  // after the event of the chunk that last used it.
+  int64_t k = 0;
+  for (int64_t first = 0; first < n; first += E.stage_particles, ++k) {
+    const int slot = (int)(k & 1);
     const int64_t m = std::min(E.stage_particles, n - first);
     const size_t d1 = sizeof(double) * (size_t)m;
+    lp::HostParticleChunk h;
+    stage_slot(E, slot, h);
+    if (k >= 2) CUDA_CK(cudaEventSynchronize(E.stage_ev[slot]));
     // caller arrays -> pinned twin (host threads) -> device staging (one copy per field)
     std::vector<CopySpan> spans = {
         {host_twin(E, h.id), in->id + first, sizeof(uint32_t) * (size_t)m},
@@ -1148,8 +1317,7 @@ lp_status import_particles(Ensemble& E, int i, const lp_particles* in) {
                               cudaMemcpyHostToDevice, E.stream));
     lp::launch_import(hc, m, first, E.A.st[par], E.A.id[par], E.A.cap, D.slot_off, D.yield, E.d_bad, E.stream);
     CUDA_CK(cudaGetLastError());
-    // the staging arrays are reused by the next chunk's copies
-    CUDA_CK(cudaStreamSynchronize(E.stream));
+    CUDA_CK(cudaEventRecord(E.stage_ev[slot], E.stream));  // the slot is free again after this
   }
   unsigned long long bad = none;
   CUDA_CK(cudaMemcpyAsync(&bad, E.d_bad, sizeof(bad), cudaMemcpyDeviceToHost, E.stream));
@@ -1838,9 +2006,10 @@ lp_status lp_sim_grid_totals(lp_sim* sim, double dt, double out[8]) {
   return push_ctrl(E);
 }
 
-lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* names, int32_t capacity,
-                              int32_t* count) {
-  Ensemble& E = sim->E;
+// Mean per-kernel duration of `steps` attempts of the whole ensemble, CUDA events between the
+// kernels on the ensemble's stream.
+static lp_status ensemble_kernel_times(Ensemble& E, int32_t steps, double* ms, char* names, int32_t capacity,
+                                       int32_t* count) {
   if (E.ctrl_h.empty() || !std::isinf(E.ctrl_h[0].target)) {
     lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
     if (st != LP_OK) return st;
@@ -1868,6 +2037,16 @@ lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* name
   }
   *count = n;
   return pull_ctrl(E);
+}
+
+lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* names, int32_t capacity,
+                              int32_t* count) {
+  return ensemble_kernel_times(sim->E, steps, ms, names, capacity, count);
+}
+
+lp_status lp_batch_kernel_times(lp_batch* b, int32_t steps, double* ms, char* names, int32_t capacity,
+                                int32_t* count) {
+  return ensemble_kernel_times(b->E, steps, ms, names, capacity, count);
 }
 
 lp_status lp_sim_grid_dump(lp_sim* sim, double dt, double* mass, double* momentum, double* reaction,
@@ -2070,50 +2249,19 @@ lp_status lp_batch_use_graph(lp_batch* b, int32_t steps) {
   return LP_OK;
 }
 lp_status lp_batch_autotune(lp_batch* b, int32_t trial_steps, char* report, size_t report_len) {
-  // Candidates: attempts per graph replay.  Each candidate runs trial_steps attempts on the live
-  // batch (time advances; the committed state stays a valid trajectory) and is timed with events.
-  Ensemble& E = b->E;
-  const int cands[4] = {1, 4, 16, 64};
-  float best_ms = 1e30f;
-  int best = 0;
-  std::string rep;
-  cudaEvent_t e0, e1;
-  CUDA_CK(cudaEventCreate(&e0));
-  CUDA_CK(cudaEventCreate(&e1));
-  for (int ci = 0; ci < 4; ++ci) {
-    E.invalidate_graph();
-    E.graph_steps = cands[ci] > 1 ? cands[ci] : 0;
-    lp_status st = lp_batch_run_substeps(b, cands[ci]);  // warm (captures the graph)
-    if (st != LP_OK) return st;
-    const int reps = std::max(1, trial_steps / cands[ci]);
-    CUDA_CK(cudaEventRecord(e0, E.stream));
-    for (int r = 0; r < reps; ++r) {
-      st = run_attempts(E, cands[ci]);
-      if (st != LP_OK) return st;
-    }
-    CUDA_CK(cudaEventRecord(e1, E.stream));
-    CUDA_CK(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    CUDA_CK(cudaEventElapsedTime(&ms, e0, e1));
-    const float per = ms / (float)(reps * cands[ci]);
-    char line[96];
-    std::snprintf(line, sizeof(line), "graph_attempts=%d ms_per_attempt=%.4f\n", cands[ci], per);
-    rep += line;
-    if (per < best_ms) {
-      best_ms = per;
-      best = cands[ci];
-    }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  E.invalidate_graph();
-  E.graph_steps = best > 1 ? best : 0;
-  char line[64];
-  std::snprintf(line, sizeof(line), "chosen=%d\n", best);
-  rep += line;
-  if (report && report_len) std::snprintf(report, report_len, "%s", rep.c_str());
-  return LP_OK;
+  return autotune(b->E, trial_steps, report, report_len);
 }
+lp_status lp_sim_autotune(lp_sim* sim, int32_t trial_steps, char* report, size_t report_len) {
+  return autotune(sim->E, trial_steps, report, report_len);
+}
+lp_status lp_batch_set_launch_shape(lp_batch* b, const lp_launch_shape* shape) {
+  return set_launch_shape(b->E, shape);
+}
+lp_status lp_batch_get_launch_shape(lp_batch* b, lp_launch_shape* out) { return get_launch_shape(b->E, out); }
+lp_status lp_sim_set_launch_shape(lp_sim* sim, const lp_launch_shape* shape) {
+  return set_launch_shape(sim->E, shape);
+}
+lp_status lp_sim_get_launch_shape(lp_sim* sim, lp_launch_shape* out) { return get_launch_shape(sim->E, out); }
 
 // ---------------- constitutive unit kernels on host arrays
 lp_status lp_hb_return_batch(int64_t n, const double* trial, const double* yield, const double* consistency,

@@ -257,6 +257,27 @@ __device__ __forceinline__ double momentum_bound(float m, float speed, float cn,
   return (double)m * speed + ((double)m * cn + sqrt(t2) * c_tau * v0) * c_dx + (double)m * c_g;
 }
 
+// Tile loop of a persistent CTA over the entries of the attempt's occupied-tile list:
+//   for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
+//     ...one tile...; __syncthreads();
+//   }
+// With a cursor the CTAs take entries from it one at a time (atomicAdd; k_begin resets it), so a
+// CTA that drew light tiles takes more of them; without one they take every gridDim.x-th entry.
+// Results are per tile, so the order and the CTA that processes a tile change nothing.  The
+// barrier that ends each tile also orders every thread's read of *slot before thread 0 writes it
+// again.
+__device__ __forceinline__ uint32_t tile_take(uint32_t* cursor, uint32_t* slot) {
+  if (threadIdx.x == 0) *slot = atomicAdd(cursor, 1u);
+  __syncthreads();
+  return *slot;
+}
+__device__ __forceinline__ uint32_t tile_first(uint32_t* cursor, uint32_t* slot) {
+  return cursor ? tile_take(cursor, slot) : blockIdx.x;
+}
+__device__ __forceinline__ uint32_t tile_next(uint32_t* cursor, uint32_t i, uint32_t* slot) {
+  return cursor ? tile_take(cursor, slot) : i + gridDim.x;
+}
+
 // ============================================================== begin
 // One thread per instance: decides whether the instance attempts a step and with which dt.
 __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, int n_inst,
@@ -265,6 +286,9 @@ __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__
   if (i == 0) {
     nw_count[0] = 0u;  // near-wall particle list of this attempt
     nw_count[1] = 0u;  // occupied-tile list of this attempt
+    nw_count[2] = 0u;  // tile cursors of the bin sort, P2G and G2P
+    nw_count[3] = 0u;
+    nw_count[4] = 0u;
   }
   if (i >= n_inst) return;
   const InstDesc& D = desc[i];
@@ -595,32 +619,33 @@ __device__ __forceinline__ void bin_sort_small(uint32_t* __restrict__ p, int n) 
 __global__ void __launch_bounds__(TB) k_bin_sort(const InstDesc* __restrict__ desc, const int* __restrict__ tile_inst,
                                                  const uint32_t* __restrict__ start, uint32_t* __restrict__ perm,
                                                  const uint32_t* __restrict__ tile_list,
-                                                 const uint32_t* __restrict__ tile_count) {
+                                                 const uint32_t* __restrict__ tile_count, uint32_t* cursor) {
+  __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
-  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+  for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
     const int tile = (int)tile_list[i];
     const InstDesc& D = desc[tile_inst[tile]];
     // a tile's keys are followed by at least the instance's outflow key, so key + 1 is valid
     const int64_t key = D.key_off + (int64_t)(tile - D.tile_off) * TB + threadIdx.x;
     const uint32_t s = start[key], e = start[key + 1];
-    if (e <= s + 1) continue;
-    if (e - s <= 8u) {  // the common case at 8 particles per cell
-      bin_sort_small<8>(perm + s, (int)(e - s));
-      continue;
-    }
-    if (e - s <= 16u) {
-      bin_sort_small<16>(perm + s, (int)(e - s));
-      continue;
-    }
-    for (uint32_t j = s + 1; j < e; ++j) {
-      const uint32_t pj = perm[j];
-      uint32_t k = j;
-      while (k > s && perm[k - 1] > pj) {
-        perm[k] = perm[k - 1];
-        --k;
+    if (e - s > 1u) {
+      if (e - s <= 8u) {  // the common case at 8 particles per cell
+        bin_sort_small<8>(perm + s, (int)(e - s));
+      } else if (e - s <= 16u) {
+        bin_sort_small<16>(perm + s, (int)(e - s));
+      } else {
+        for (uint32_t j = s + 1; j < e; ++j) {
+          const uint32_t pj = perm[j];
+          uint32_t k = j;
+          while (k > s && perm[k - 1] > pj) {
+            perm[k] = perm[k - 1];
+            --k;
+          }
+          perm[k] = pj;
+        }
       }
-      perm[k] = pj;
     }
+    if (cursor) __syncthreads();  // only the cursor's slot needs the barrier
   }
 }
 
@@ -670,26 +695,31 @@ __global__ void k_tiles(const InstDesc* __restrict__ desc, const Control* __rest
 // order (deterministic, no atomics), converts to int64 fixed point, the tile's exact particle
 // totals are restored by a proportional correction, and each node component is flushed with
 // one global atomic.
-constexpr int P2G_CHUNK = 1024;
+// Chunk sizes (particles per chunk) of the two P2G instantiations the launch shape chooses from.
+constexpr int P2G_CHUNK = 1024, P2G_CHUNK_SMALL = 512;
 constexpr int P2G_REC = 16;  // m, q[3], A[9], f[3]
-constexpr int P2G_PER_THREAD = (P2G_CHUNK + P2G_THREADS - 1) / P2G_THREADS;  // phase-1 particles per thread
 constexpr size_t P2G_PART_BYTES = sizeof(float4) * TB * 27;
-constexpr size_t P2G_REC_BYTES = sizeof(float) * P2G_REC * P2G_CHUNK;
-constexpr size_t P2G_SMEM = P2G_PART_BYTES > P2G_REC_BYTES ? P2G_PART_BYTES : P2G_REC_BYTES;
+// dynamic shared memory of a chunk size: the records, which the partial node sums alias later
+constexpr size_t p2g_smem(int chunk) {
+  return P2G_PART_BYTES > sizeof(float) * P2G_REC * chunk ? P2G_PART_BYTES : sizeof(float) * P2G_REC * chunk;
+}
 // Slot of chunk particle i in each record row: within each 32-word segment the slots rotate by
 // the segment number, so bins whose particles start 32 apart (8 per bin in a lattice fill) read
 // different shared-memory banks in the per-bin pass; consecutive i still fill a segment.
 __device__ __forceinline__ uint32_t rec_slot(uint32_t i) { return (i & ~31u) | ((i + (i >> 5)) & 31u); }
 
-// one tile of k_p2g
+// one tile of k_p2g, chunks of CHUNK particles
+template <int CHUNK>
 __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restrict__ desc,
                                          const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
                                          const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
                                          const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
                                          long long* __restrict__ acc, int64_t node_total,
                                          uint32_t* __restrict__ blk_epoch, int transport_only) {
+  constexpr int P2G_PER_THREAD = (CHUNK + P2G_THREADS - 1) / P2G_THREADS;  // phase-1 particles per thread
+  static_assert(CHUNK % 32 == 0, "record rows rotate within 32-word segments");
   extern __shared__ float4 part[];  // particle records during the chunks, then TB * 27 partial node sums
-  float* rec = reinterpret_cast<float*>(part);  // [P2G_REC][P2G_CHUNK]
+  float* rec = reinterpret_cast<float*>(part);  // [P2G_REC][CHUNK]
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
   __shared__ int redi[P2G_THREADS / 32 + 1];
 
@@ -724,8 +754,8 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
   long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // tile totals (particles) then halo sums (nodes)
 
   const uint32_t s = start[key0 + bin], e = start[key0 + bin + 1];  // this bin's sorted range
-  for (uint32_t c0 = ts; c0 < te; c0 += P2G_CHUNK) {
-    const uint32_t cn = min((uint32_t)P2G_CHUNK, te - c0);
+  for (uint32_t c0 = ts; c0 < te; c0 += CHUNK) {
+    const uint32_t cn = min((uint32_t)CHUNK, te - c0);
     if (c0 != ts) __syncthreads();  // the previous chunk's records are consumed
     // phase 1: one thread per particle.  The thread's permutation entries of the chunk are loaded
     // first, so that each particle's state loads issue without waiting for its entry.
@@ -756,14 +786,14 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
       float* r = rec + rec_slot(i);
       r[0] = m;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) r[(1 + a) * P2G_CHUNK] = v[a] * m;
+      for (int a = 0; a < 3; ++a) r[(1 + a) * CHUNK] = v[a] * m;
 #pragma unroll
-      for (int a = 0; a < 9; ++a) r[(4 + a) * P2G_CHUNK] = Cm[a] * m - T[a] * sv;
+      for (int a = 0; a < 9; ++a) r[(4 + a) * CHUNK] = Cm[a] * m - T[a] * sv;
       // position relative to the particle's stencil base (its bin's base: floor(x/dx - 0.5))
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const float sc = scaled_of(x[a], dx, D.pow2_inv_dx);
-        r[(13 + a) * P2G_CHUNK] = sc - floorf(sc - 0.5f);
+        r[(13 + a) * CHUNK] = sc - floorf(sc - 0.5f);
       }
       // exact per-particle totals: FP64 products of the stored FP32 mass and velocity
       tot[0] += to_fixed((double)m, s_m);
@@ -777,15 +807,15 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
     for (uint32_t j = j0; j < j1; ++j) {
       const float* r = rec + rec_slot(j - c0);
       const float m = r[0];
-      const float q[3] = {r[P2G_CHUNK], r[2 * P2G_CHUNK], r[3 * P2G_CHUNK]};
+      const float q[3] = {r[CHUNK], r[2 * CHUNK], r[3 * CHUNK]};
       float A[9];
 #pragma unroll
-      for (int a = 0; a < 9; ++a) A[a] = r[(4 + a) * P2G_CHUNK];
+      for (int a = 0; a < 9; ++a) A[a] = r[(4 + a) * CHUNK];
       float w[3][3], d[3][3];
 #pragma unroll
-      for (int a = 1; a < 3; ++a) weights_of(r[(13 + a) * P2G_CHUNK], dx, w[a], d[a]);
+      for (int a = 1; a < 3; ++a) weights_of(r[(13 + a) * CHUNK], dx, w[a], d[a]);
       // x weight of this thread's slab only (the expressions of weights_of for offset `slab`)
-      const float fx = r[13 * P2G_CHUNK];
+      const float fx = r[13 * CHUNK];
       const float ao = slab == 0 ? 1.5f - fx : (slab == 1 ? fx - 1.0f : fx - 0.5f);
       const float wa = slab == 1 ? 0.75f - ao * ao : 0.5f * (ao * ao);
       const float da = (fx - (float)slab) * -dx;
@@ -898,17 +928,20 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
   }
 }
 
-// Persistent CTAs (as many as fit the GPU at once) walk the attempt's list of occupied tiles.
+// Persistent CTAs (as many as the launch shape asks, at most as many as fit the GPU at once)
+// walk the attempt's list of occupied tiles.
+template <int CHUNK>
 __global__ void __launch_bounds__(P2G_THREADS, 2)
     k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
           const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
           int64_t node_total, uint32_t* __restrict__ blk_epoch, int transport_only,
-          const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count) {
+          const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count, uint32_t* cursor) {
+  __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
-  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-    p2g_tile((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm, acc, node_total, blk_epoch,
-             transport_only);
+  for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
+    p2g_tile<CHUNK>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm, acc, node_total,
+                    blk_epoch, transport_only);
     __syncthreads();  // the next tile reuses the shared memory
   }
 }
@@ -1980,31 +2013,35 @@ enum {
   PF_ID = 16,
   PF_SLOTS = 17
 };
-constexpr size_t G2P_SMEM = sizeof(float) * 2 * PF_SLOTS * G2P_THREADS;
+// dynamic shared memory of a G2P CTA of nt threads
+constexpr size_t g2p_smem(int nt) { return sizeof(float) * 2 * PF_SLOTS * nt; }
+// threads per CTA of the two G2P instantiations the launch shape chooses from
+constexpr int G2P_THREADS_SMALL = 128;
 
+template <int NT>
 __device__ __forceinline__ void g2p_prefetch(float* __restrict__ buf, const float* __restrict__ cur,
                                              const uint32_t* __restrict__ idc, int64_t cap, int64_t src, bool paste,
                                              bool pyield) {
   float* b = buf + threadIdx.x;
 #pragma unroll
-  for (int a = 0; a < 3; ++a) cp_async4(b + (PF_X + a) * G2P_THREADS, cur + (C_X + a) * cap + src);
+  for (int a = 0; a < 3; ++a) cp_async4(b + (PF_X + a) * NT, cur + (C_X + a) * cap + src);
   if (paste) {
 #pragma unroll
-    for (int a = 0; a < 9; ++a) cp_async4(b + (PF_H + a) * G2P_THREADS, cur + (C_H + a) * cap + src);
-    if (pyield) cp_async4(b + PF_YS * G2P_THREADS, cur + C_YS * cap + src);
+    for (int a = 0; a < 9; ++a) cp_async4(b + (PF_H + a) * NT, cur + (C_H + a) * cap + src);
+    if (pyield) cp_async4(b + PF_YS * NT, cur + C_YS * cap + src);
   } else {
-    cp_async4(b + PF_JM1 * G2P_THREADS, cur + C_JM1 * cap + src);
+    cp_async4(b + PF_JM1 * NT, cur + C_JM1 * cap + src);
   }
-  cp_async4(b + PF_EP * G2P_THREADS, cur + C_EP * cap + src);
-  cp_async4(b + PF_M * G2P_THREADS, cur + C_M * cap + src);
-  cp_async4(b + PF_V0 * G2P_THREADS, cur + C_V0 * cap + src);
-  cp_async4(b + PF_ID * G2P_THREADS, idc + src);
+  cp_async4(b + PF_EP * NT, cur + C_EP * cap + src);
+  cp_async4(b + PF_M * NT, cur + C_M * cap + src);
+  cp_async4(b + PF_V0 * NT, cur + C_V0 * cap + src);
+  cp_async4(b + PF_ID * NT, idc + src);
 }
 
 // Warm start (WARM instantiation): each yielding lane reads the network's logit at its la8 from
 // its instance's table (k_mlp_table), interpolated between the two neighbouring nodes.
-// one tile of k_g2p
-template <bool WARM>
+// one tile of k_g2p, CTAs of NT threads
+template <bool WARM, int NT>
 __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restrict__ desc,
                                          const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
                                          float* __restrict__ st0, float* __restrict__ st1,
@@ -2015,7 +2052,7 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
                                          float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
                                          long long log_cap) {
   __shared__ float4 hv[HN];
-  __shared__ double shd[(G2P_THREADS / 32) * 9 + 9];
+  __shared__ double shd[(NT / 32) * 9 + 9];
   extern __shared__ float4 g2p_dyn[];  // prefetched inputs of two rounds
   float* pf = reinterpret_cast<float*>(g2p_dyn);
   const int inst = tile_inst[tile];
@@ -2040,7 +2077,7 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
   const int ty = (int)((ltile / D.tiles[2]) % D.tiles[1]);
   const int tx = (int)(ltile / ((int64_t)D.tiles[2] * D.tiles[1]));
   const int ox = tx * TX, oy = ty * TY, oz = tz * TZ;
-  for (int n = threadIdx.x; n < HN; n += G2P_THREADS) {
+  for (int n = threadIdx.x; n < HN; n += NT) {
     const int hz = n % HZ, hy = (n / HZ) % HY, hx = n / (HZ * HY);
     const int gi = ox + hx, gj = oy + hy, gk = oz + hz;
     hv[n] = (gi < D.nodes[0] && gj < D.nodes[1] && gk < D.nodes[2]) ? __ldg(&vel[node_index(D, gi, gj, gk)])
@@ -2062,19 +2099,19 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
   int fail = F_OK, iters = 0, yielded = 0;
   double fail_value = 0.0;
   const bool paste = D.kind == 0, pyield = paste && D.per_particle_yield;
-  const int nround = (int)((e0 - s0 + G2P_THREADS - 1) / G2P_THREADS);
+  const int nround = (int)((e0 - s0 + NT - 1) / NT);
   // slot of this thread in round r (clamped to the tile's last particle) and warp liveness
   auto slot_of = [&](int r) -> int64_t {
-    const int64_t kk = (int64_t)s0 + (int64_t)r * G2P_THREADS + threadIdx.x;
+    const int64_t kk = (int64_t)s0 + (int64_t)r * NT + threadIdx.x;
     return kk < (int64_t)e0 ? kk : (int64_t)e0 - 1;
   };
   auto live_of = [&](int r) -> bool {
-    return (int64_t)s0 + (int64_t)r * G2P_THREADS + (threadIdx.x & ~31u) < (int64_t)e0;
+    return (int64_t)s0 + (int64_t)r * NT + (threadIdx.x & ~31u) < (int64_t)e0;
   };
   // pipeline: copies of round r+1 are in flight while round r computes; perm of round r+2 is
   // loaded a round ahead of its copies
   int64_t src_next = 0;
-  if (live_of(0)) g2p_prefetch(pf, cur, idc, cap, perm[slot_of(0)], paste, pyield);
+  if (live_of(0)) g2p_prefetch<NT>(pf, cur, idc, cap, perm[slot_of(0)], paste, pyield);
   cp_async_commit();
   if (nround > 1 && live_of(1)) src_next = perm[slot_of(1)];
   const float c_tau = (float)(D.max_dt * 4.0 / (D.dx * D.dx));
@@ -2088,12 +2125,12 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
     const bool warp_live = live_of(r);
     if (!warp_live) break;
     if (r + 1 < nround && live_of(r + 1))
-      g2p_prefetch(pf + ((r + 1) & 1) * PF_SLOTS * G2P_THREADS, cur, idc, cap, src_next, paste, pyield);
+      g2p_prefetch<NT>(pf + ((r + 1) & 1) * PF_SLOTS * NT, cur, idc, cap, src_next, paste, pyield);
     cp_async_commit();
     if (r + 2 < nround && live_of(r + 2)) src_next = perm[slot_of(r + 2)];
     cp_async_wait<1>();  // this thread's copies of round r have landed
-    const float* in = pf + (r & 1) * PF_SLOTS * G2P_THREADS + threadIdx.x;
-    const bool valid = (int64_t)s0 + (int64_t)r * G2P_THREADS + threadIdx.x < (int64_t)e0;
+    const float* in = pf + (r & 1) * PF_SLOTS * NT + threadIdx.x;
+    const bool valid = (int64_t)s0 + (int64_t)r * NT + threadIdx.x < (int64_t)e0;
     const int64_t k = slot_of(r);
     float Htr[9];
     float tau[6];
@@ -2109,7 +2146,7 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
       float w[3][3], d[3][3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        x[a] = in[(PF_X + a) * G2P_THREADS];
+        x[a] = in[(PF_X + a) * NT];
         const float sc = scaled_of(x[a], dx, D.pow2_inv_dx);
         const float bf = floorf(sc - 0.5f);
         base[a] = (int)(bf + 1.0f);
@@ -2154,9 +2191,9 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
       for (int a = 0; a < 9; ++a) Cm[a] *= dx2_inv;
       speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
       disp = scaled_of(speed * dt, dx, D.pow2_inv_dx);
-      m = in[PF_M * G2P_THREADS];
-      v0 = in[PF_V0 * G2P_THREADS];
-      ep = in[PF_EP * G2P_THREADS];
+      m = in[PF_M * NT];
+      v0 = in[PF_V0 * NT];
+      ep = in[PF_EP * NT];
       // kinematic part of the trial state, stored before the constitutive update (sorted slot order)
       if (valid) {
 #pragma unroll
@@ -2168,14 +2205,14 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
         for (int a = 0; a < 9; ++a) nxt[(C_C + a) * cap + k] = Cm[a];
         nxt[C_M * cap + k] = m;
         nxt[C_V0 * cap + k] = v0;
-        if (pyield) nxt[C_YS * cap + k] = in[PF_YS * G2P_THREADS];
-        idn[k] = __float_as_uint(in[PF_ID * G2P_THREADS]);
+        if (pyield) nxt[C_YS * cap + k] = in[PF_YS * NT];
+        idn[k] = __float_as_uint(in[PF_ID * NT]);
       }
       cn = affine_norm(Cm);
       if (paste) {
         float H[9];
 #pragma unroll
-        for (int a = 0; a < 9; ++a) H[a] = in[(PF_H + a) * G2P_THREADS];
+        for (int a = 0; a < 9; ++a) H[a] = in[(PF_H + a) * NT];
         // H_tr = H + dt C + dt C H
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -2185,10 +2222,10 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
                 Cm[3 * i + 0] * H[0 * 3 + j] + Cm[3 * i + 1] * H[1 * 3 + j] + Cm[3 * i + 2] * H[2 * 3 + j];
             Htr[3 * i + j] = H[3 * i + j] + dt * (Cm[3 * i + j] + ch);
           }
-        ys = pyield ? (double)in[PF_YS * G2P_THREADS] : D.yield;
+        ys = pyield ? (double)in[PF_YS * NT] : D.yield;
         paste_trial(Htr, D.mu, pt, o);
       } else {
-        const float jm1 = in[PF_JM1 * G2P_THREADS];
+        const float jm1 = in[PF_JM1 * NT];
         LiquidOut lo;
         liquid_update(jm1, Cm, (float)D.bulk, (float)D.consistency, (float)D.tait_gamma, dt, lo);
 #pragma unroll
@@ -2252,7 +2289,7 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
   double rv[9] = {diss, bb, mass_sum, (double)max_speed, (double)max_disp, (double)fail, (double)iters,
                   (double)yielded, fail_value};
   // thread 0 writes the tile's partial; shd is next written after the tile-end barrier
-  block_reduce_multi_to0<G2P_THREADS, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
+  block_reduce_multi_to0<NT, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
   if (threadIdx.x == 0) {
     ParticlePartial& P = part[tile];
     P.diss = rv[0];
@@ -2267,20 +2304,24 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
   }
 }
 
-// Persistent CTAs (as many as fit the GPU at once) walk the attempt's list of occupied tiles;
-// the partial results are per tile, so they do not depend on which CTA took which tile.
-template <bool WARM>
-__global__ void __launch_bounds__(G2P_THREADS, 2)
+// Persistent CTAs (as many as the launch shape asks, at most as many as fit the GPU at once)
+// walk the attempt's list of occupied tiles; the partial results are per tile, so they do not
+// depend on which CTA took which tile.  Both block shapes hold 16 warps per SM at the 128
+// registers a thread needs.
+template <bool WARM, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
     k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
           int64_t cap, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
           const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const float* __restrict__ mlp_tab,
           float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
-          long long log_cap, const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count) {
+          long long log_cap, const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count,
+          uint32_t* cursor) {
+  __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
-  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-    g2p_tile<WARM>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, id0, id1, cap, start, perm, vel, part, mlp_tab,
-                   log_x, log_y, log_n, log_cap);
+  for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
+    g2p_tile<WARM, NT>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, id0, id1, cap, start, perm, vel, part,
+                       mlp_tab, log_x, log_y, log_n, log_cap);
     __syncthreads();  // the next tile reuses the shared memory
   }
 }
@@ -2807,44 +2848,107 @@ static uint64_t g_launches = 0;
 
 static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-// persistent grid sizes of P2G and the two G2P instantiations: resident CTAs per SM times SMs
-static int g_p2g_ctas = 296, g_g2p_ctas[2] = {296, 296}, g_sort_ctas = 148 * 16;
+// Resident CTAs per SM of the persistent kernels' instantiations (from the occupancy calculator;
+// the defaults are the B200 figures) and the SM count.
+static int g_sms = 148, g_sort_per_sm = 16;
+static int g_p2g_per_sm[2] = {2, 2};                 // [p2g_small]
+static int g_g2p_per_sm[2][2] = {{2, 2}, {4, 4}};   // [g2p_small][warm]
+
+static void occupancy(int* out, const void* fn, int threads, size_t smem) {
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem) == cudaSuccess && per > 0) *out = per;
+}
 
 void configure_kernels() {
-  cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM);
-  cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G2P_SMEM);
-  cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G2P_SMEM);
+  cudaFuncSetAttribute(k_p2g<P2G_CHUNK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem(P2G_CHUNK));
+  cudaFuncSetAttribute(k_p2g<P2G_CHUNK_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)p2g_smem(P2G_CHUNK_SMALL));
+  cudaFuncSetAttribute(k_g2p<false, G2P_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)g2p_smem(G2P_THREADS));
+  cudaFuncSetAttribute(k_g2p<true, G2P_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)g2p_smem(G2P_THREADS));
+  cudaFuncSetAttribute(k_g2p<false, G2P_THREADS_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)g2p_smem(G2P_THREADS_SMALL));
+  cudaFuncSetAttribute(k_g2p<true, G2P_THREADS_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)g2p_smem(G2P_THREADS_SMALL));
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return;
-  int per = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bin_sort, TB, 0) == cudaSuccess && per > 0)
-    g_sort_ctas = per * sms;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_p2g, P2G_THREADS, P2G_SMEM) == cudaSuccess && per > 0)
-    g_p2g_ctas = per * sms;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<false>, G2P_THREADS, G2P_SMEM) ==
-          cudaSuccess && per > 0)
-    g_g2p_ctas[0] = per * sms;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_g2p<true>, G2P_THREADS, G2P_SMEM) ==
-          cudaSuccess && per > 0)
-    g_g2p_ctas[1] = per * sms;
+  g_sms = sms;
+  occupancy(&g_sort_per_sm, (const void*)k_bin_sort, TB, 0);
+  occupancy(&g_p2g_per_sm[0], (const void*)k_p2g<P2G_CHUNK>, P2G_THREADS, p2g_smem(P2G_CHUNK));
+  occupancy(&g_p2g_per_sm[1], (const void*)k_p2g<P2G_CHUNK_SMALL>, P2G_THREADS, p2g_smem(P2G_CHUNK_SMALL));
+  occupancy(&g_g2p_per_sm[0][0], (const void*)k_g2p<false, G2P_THREADS>, G2P_THREADS, g2p_smem(G2P_THREADS));
+  occupancy(&g_g2p_per_sm[0][1], (const void*)k_g2p<true, G2P_THREADS>, G2P_THREADS, g2p_smem(G2P_THREADS));
+  occupancy(&g_g2p_per_sm[1][0], (const void*)k_g2p<false, G2P_THREADS_SMALL>, G2P_THREADS_SMALL,
+            g2p_smem(G2P_THREADS_SMALL));
+  occupancy(&g_g2p_per_sm[1][1], (const void*)k_g2p<true, G2P_THREADS_SMALL>, G2P_THREADS_SMALL,
+            g2p_smem(G2P_THREADS_SMALL));
+}
+
+// persistent grid size: the requested CTAs per SM, at most the resident limit, times the SMs
+static unsigned persistent_ctas(int requested, int limit) {
+  const int per = (requested > 0 && requested < limit) ? requested : limit;
+  return (unsigned)(per * g_sms);
+}
+
+int launch_shape_limits(int out[6]) {
+  out[0] = g_sms;
+  out[1] = g_p2g_per_sm[0];
+  out[2] = g_p2g_per_sm[1];
+  out[3] = g_g2p_per_sm[0][1];
+  out[4] = g_g2p_per_sm[1][1];
+  out[5] = g_sort_per_sm;
+  return 6;
 }
 
 // the occupied-tile list, then P2G over it
 static int launch_tiles_p2g(const DeviceArrays& A, cudaStream_t s, int transport_only, cudaEvent_t* ev, int& n) {
+  const LaunchShape& L = A.shape;
+  uint32_t* cur = L.dynamic ? A.nw_count + 2 : nullptr;  // cursors: [0] bin sort, [1] P2G, [2] G2P
   k_tiles<<<grid_of(A.n_tiles, 256), 256, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.n_tiles, A.start, A.tile_list,
                                                    A.tile_count, A.tpart);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_bin_sort<<<(unsigned)g_sort_ctas, TB, 0, s>>>(A.desc, A.tile_inst, A.start, A.perm, A.tile_list, A.tile_count);
+  k_bin_sort<<<(unsigned)(g_sort_per_sm * g_sms), TB, 0, s>>>(A.desc, A.tile_inst, A.start, A.perm, A.tile_list,
+                                                               A.tile_count, cur);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_p2g<<<(unsigned)g_p2g_ctas, P2G_THREADS, P2G_SMEM, s>>>(A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap,
-                                                             A.start, A.perm, A.acc, A.node_total, A.blk_epoch,
-                                                             transport_only, A.tile_list, A.tile_count);
+  const unsigned ctas = persistent_ctas(L.p2g_per_sm, g_p2g_per_sm[L.p2g_small ? 1 : 0]);
+  uint32_t* pc = cur ? cur + 1 : nullptr;
+  if (L.p2g_small)
+    k_p2g<P2G_CHUNK_SMALL><<<ctas, P2G_THREADS, p2g_smem(P2G_CHUNK_SMALL), s>>>(
+        A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start, A.perm, A.acc, A.node_total, A.blk_epoch,
+        transport_only, A.tile_list, A.tile_count, pc);
+  else
+    k_p2g<P2G_CHUNK><<<ctas, P2G_THREADS, p2g_smem(P2G_CHUNK), s>>>(
+        A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start, A.perm, A.acc, A.node_total, A.blk_epoch,
+        transport_only, A.tile_list, A.tile_count, pc);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   return 3;
+}
+
+// G2P in the launch shape's instantiation
+static void launch_g2p(const DeviceArrays& A, bool warm, cudaStream_t s) {
+  const LaunchShape& L = A.shape;
+  uint32_t* cur = L.dynamic ? A.nw_count + 4 : nullptr;
+  const float* tab = warm ? A.mlp_tab : nullptr;
+  const int small = L.g2p_small ? 1 : 0;
+  const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[small][warm ? 1 : 0]);
+#define LP_G2P_ARGS                                                                                               \
+  A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, tab, \
+      A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count, cur
+  if (small) {
+    constexpr int T = G2P_THREADS_SMALL;
+    if (warm) k_g2p<true, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
+    else k_g2p<false, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
+  } else {
+    constexpr int T = G2P_THREADS;
+    if (warm) k_g2p<true, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
+    else k_g2p<false, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
+  }
+#undef LP_G2P_ARGS
 }
 uint64_t kernel_launch_count() { return g_launches; }
 void add_kernel_launches(uint64_t n) { g_launches += n; }
@@ -2914,9 +3018,7 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
     ++n;
     if (ev) cudaEventRecord(ev[n], s);
   }
-  (warm_g2p ? k_g2p<true> : k_g2p<false>)<<<(unsigned)g_g2p_ctas[warm_g2p ? 1 : 0], G2P_THREADS, G2P_SMEM, s>>>(
-      A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart,
-      warm_g2p ? A.mlp_tab : nullptr, A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count);
+  launch_g2p(A, warm_g2p, s);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_segments<<<(unsigned)A.n_seg, 256, 0, s>>>(A.ctrl, A.segs, A.gpart, A.tpart, A.seg);

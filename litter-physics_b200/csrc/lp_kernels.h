@@ -10,6 +10,16 @@ namespace lp {
 
 constexpr int DIAG_N = 19;
 
+// Launch shape of the persistent tile kernels, chosen per ensemble (by default, or by the
+// autotuner on the live batch).  Per-SM counts of 0, or above what fits, mean as many as fit.
+struct LaunchShape {
+  int g2p_small = 0;   // 1: G2P CTAs of G2P_THREADS_SMALL (128) threads, 0: G2P_THREADS (256)
+  int g2p_per_sm = 0;  // persistent G2P CTAs per SM
+  int p2g_small = 0;   // 1: P2G chunks of P2G_CHUNK_SMALL (512) particles, 0: P2G_CHUNK (1024)
+  int p2g_per_sm = 0;  // persistent P2G CTAs per SM
+  int dynamic = 1;     // 1: CTAs take tiles from the attempt's cursors, 0: round robin
+};
+
 // All device buffers of one ensemble (owned by the host runtime).
 struct DeviceArrays {
   InstDesc* desc = nullptr;
@@ -34,7 +44,8 @@ struct DeviceArrays {
   uint32_t* chunk_base = nullptr;
   uint32_t* perm = nullptr;
   uint32_t* nw_list = nullptr;
-  uint32_t* nw_count = nullptr;    // [0] near-wall particles, [1] occupied tiles of the attempt
+  uint32_t* nw_count = nullptr;    // [0] near-wall particles, [1] occupied tiles of the attempt,
+                                   // [2..4] tile cursors of the bin sort, P2G and G2P
   uint32_t* tile_count = nullptr;  // = nw_count + 1
   uint32_t* tile_list = nullptr;   // occupied tiles of the attempt (n_tiles capacity)
   long long* acc = nullptr;   // 4 x node_total: mass, momentum xyz (int64 fixed point)
@@ -57,7 +68,7 @@ struct DeviceArrays {
   float* log_y = nullptr;
   unsigned long long* log_n = nullptr;
   long long log_cap = 0;
-  int p2g_variant = 0;  // autotuner choice (reserved)
+  LaunchShape shape;
   // pellet bed (instances with InstDesc::bed_np >= 2)
   int any_bed = 0;
   int64_t n_bed = 0;                                 // pellets of all instances
@@ -99,6 +110,9 @@ int launch_export(const HostParticleChunk& h, int64_t n, int64_t first, const fl
                   cudaStream_t s);
 uint64_t kernel_launch_count();
 void configure_kernels();              // one-time function attributes (dynamic shared memory)
+// out = SMs, resident CTAs per SM of P2G (1024- and 512-particle chunks), of the warm G2P (256-
+// and 128-thread CTAs) and of the bin sort; returns 6
+int launch_shape_limits(int out[6]);
 void set_last_error(const char* msg);  // message returned by lp_last_error()
 void add_kernel_launches(uint64_t n);
 

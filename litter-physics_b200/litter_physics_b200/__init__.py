@@ -5,8 +5,10 @@ Modules:
   _lib      loader of the device library and status checking
   sim       Simulation / Batch: the reference's Simulation API over the device library
   research  research wire request -> fixture spec (research.rs:171-305)
-  configs   the benchmark workloads (slump, dam break, large slump, batched sweep)
-  core      drop-in `protocol_version` / `run_json` of the reference's `_core` module
+  configs   the benchmark workloads (slump, dam break, large slump, batched sweep, pellet bed)
+  _core     drop-in `protocol_version` / `run_json` of the reference's `_core` module
+  warmstart Newton-pair collection and device training of the warm-start network
+  sweep, verification  parameter sweeps and refinement studies on the batched launch
 """
 
 from ._abi import FixtureSpec, Ledger, Material  # noqa: F401

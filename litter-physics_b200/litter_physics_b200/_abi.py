@@ -220,6 +220,23 @@ class Pellet(C.Structure):
     ]
 
 
+class LaunchShape(C.Structure):
+    """Mirror of `lp_launch_shape`: launch shape of the persistent tile kernels (no reference
+    counterpart)."""
+
+    _fields_ = [
+        ("g2p_small", C.c_int32),
+        ("g2p_per_sm", C.c_int32),
+        ("p2g_small", C.c_int32),
+        ("p2g_per_sm", C.c_int32),
+        ("dynamic_tiles", C.c_int32),
+        ("graph_attempts", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
 KEEP_GOING_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
 
 PARTICLE_FIELDS = {

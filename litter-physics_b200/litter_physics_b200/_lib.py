@@ -116,6 +116,12 @@ def lib():
         "lp_batch_warm_table": ([P, I32, F, I32, D], I32),
         "lp_batch_use_graph": ([P, I32], I32),
         "lp_batch_autotune": ([P, I32, C.c_char_p, C.c_size_t], I32),
+        "lp_sim_autotune": ([P, I32, C.c_char_p, C.c_size_t], I32),
+        "lp_sim_set_launch_shape": ([P, C.POINTER(_abi.LaunchShape)], I32),
+        "lp_sim_get_launch_shape": ([P, C.POINTER(_abi.LaunchShape)], I32),
+        "lp_batch_set_launch_shape": ([P, C.POINTER(_abi.LaunchShape)], I32),
+        "lp_batch_get_launch_shape": ([P, C.POINTER(_abi.LaunchShape)], I32),
+        "lp_batch_kernel_times": ([P, I32, D, C.c_char_p, I32, C.POINTER(I32)], I32),
         "lp_batch_get_pellet": ([P, I32, C.POINTER(_abi.Pellet), C.POINTER(I32)], I32),
         "lp_batch_observables": ([P, I32, C.c_char_p, D, I32, C.POINTER(I32)], I32),
         "lp_batch_energies": ([P, I32, D], I32),

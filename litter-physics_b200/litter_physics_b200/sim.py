@@ -81,6 +81,26 @@ class Simulation:
     def use_graph(self, steps: int) -> None:
         check(lib().lp_sim_use_graph(self._h, int(steps)))
 
+    def autotune(self, trial_steps: int = 16) -> str:
+        """Pick the launch shape on the live simulation (advances it); returns the report."""
+        buf = C.create_string_buffer(8192)
+        check(lib().lp_sim_autotune(self._h, int(trial_steps), buf, 8192))
+        return buf.value.decode()
+
+    def launch_shape(self) -> dict:
+        s = _abi.LaunchShape()
+        check(lib().lp_sim_get_launch_shape(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def set_launch_shape(self, **fields) -> None:
+        """Set fields of `lp_launch_shape` (g2p_small, g2p_per_sm, p2g_small, p2g_per_sm,
+        dynamic_tiles, graph_attempts); the others keep their values."""
+        s = _abi.LaunchShape()
+        check(lib().lp_sim_get_launch_shape(self._h, C.byref(s)))
+        for k, v in fields.items():
+            setattr(s, k, int(v))
+        check(lib().lp_sim_set_launch_shape(self._h, C.byref(s)))
+
     def stability_limit(self) -> float:
         out = C.c_double()
         check(lib().lp_sim_stability_limit(self._h, C.byref(out)))
@@ -328,9 +348,32 @@ class Batch:
         check(lib().lp_batch_use_graph(self._h, int(steps)))
 
     def autotune(self, trial_steps: int = 16) -> str:
-        buf = C.create_string_buffer(2048)
-        check(lib().lp_batch_autotune(self._h, int(trial_steps), buf, 2048))
+        """Pick the launch shape on the live batch (advances it); returns the tuner's report."""
+        buf = C.create_string_buffer(8192)
+        check(lib().lp_batch_autotune(self._h, int(trial_steps), buf, 8192))
         return buf.value.decode()
+
+    def launch_shape(self) -> dict:
+        s = _abi.LaunchShape()
+        check(lib().lp_batch_get_launch_shape(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def set_launch_shape(self, **fields) -> None:
+        s = _abi.LaunchShape()
+        check(lib().lp_batch_get_launch_shape(self._h, C.byref(s)))
+        for k, v in fields.items():
+            setattr(s, k, int(v))
+        check(lib().lp_batch_set_launch_shape(self._h, C.byref(s)))
+
+    def kernel_times(self, steps: int) -> dict:
+        """Mean per-kernel duration (ms) over `steps` attempts of the whole batch."""
+        cap = 24
+        ms = (C.c_double * cap)()
+        names = C.create_string_buffer(32 * cap)
+        n = C.c_int32()
+        check(lib().lp_batch_kernel_times(self._h, int(steps), ms, names, cap, C.byref(n)))
+        raw = names.raw
+        return {raw[32 * i:32 * i + 32].split(b"\0", 1)[0].decode(): ms[i] for i in range(n.value)}
 
     def counters(self, i: int) -> _abi.Counters:
         c = _abi.Counters()

@@ -1,0 +1,103 @@
+"""Launch shapes and the autotuner: every shape of the persistent tile kernels gives the same
+particle state bit for bit (a tile's results do not depend on the CTA that takes it, on the
+order, on the G2P block size or on the P2G chunk size), and the autotuner keeps a valid
+trajectory.  The ledgers are identical too, except that the G2P block size changes which
+thread sums which particles' FP64 plastic work, so with 128-thread CTAs that one ledger entry
+agrees to rounding."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [
+    {},  # default: 256-thread G2P, 1024-particle P2G chunks, as many CTAs as fit, dynamic tiles
+    {"dynamic_tiles": 0},
+    {"g2p_small": 1},
+    {"g2p_small": 1, "g2p_per_sm": 3},
+    {"p2g_small": 1},
+    {"p2g_per_sm": 1, "g2p_per_sm": 1, "dynamic_tiles": 0},
+    {"graph_attempts": 4},
+]
+
+
+def by_id(p: dict) -> dict:
+    order = np.argsort(p["id"])
+    return {k: v[order] for k, v in p.items()}
+
+
+def run(specs_fn, shape: dict, steps: int):
+    from litter_physics_b200.sim import Batch
+
+    b = Batch(specs_fn())
+    if shape:
+        b.set_launch_shape(**shape)
+    b.run_substeps(steps)
+    b.sync()
+    out = []
+    for i in range(len(b.specs)):
+        p = by_id(b.particles(i))
+        led = b.ledger(i)
+        plastic = led.plastic_dissipation
+        led.plastic_dissipation = 0.0
+        out.append(((p["position"].tobytes(), p["velocity"].tobytes(), p["deformation"].tobytes(), bytes(led),
+                     b.counters(i).step_count), plastic))
+    b.close()
+    return out
+
+
+def uneven_batch():
+    from litter_physics_b200 import configs
+
+    return [configs.slump(16, (4, 4, 8), seed=21), configs.slump(32, (8, 8, 16), seed=22, yield_range=(20.0, 100.0)),
+            configs.dam_break(32, (16, 8, 16), seed=23)]
+
+
+def test_every_launch_shape_gives_identical_results():
+    from litter_physics_b200 import _lib
+
+    _lib.build()
+    ref = run(uneven_batch, SHAPES[0], 24)
+    for shape in SHAPES[1:]:
+        got = run(uneven_batch, shape, 24)
+        for (state, plastic), (ref_state, ref_plastic) in zip(got, ref, strict=True):
+            assert state == ref_state, shape
+            if shape.get("g2p_small"):
+                assert abs(plastic - ref_plastic) <= 1e-13 * abs(ref_plastic), shape
+            else:
+                assert plastic == ref_plastic, shape
+
+
+def test_launch_shape_round_trip_and_refusal():
+    from litter_physics_b200 import _lib, configs
+    from litter_physics_b200.sim import Simulation
+
+    _lib.build()
+    sim = Simulation(configs.slump(16, (4, 4, 8), seed=1))
+    sim.set_launch_shape(g2p_small=1, p2g_small=1, dynamic_tiles=0, graph_attempts=4)
+    s = sim.launch_shape()
+    assert (s["g2p_small"], s["p2g_small"], s["dynamic_tiles"], s["graph_attempts"]) == (1, 1, 0, 4)
+    assert s["g2p_per_sm"] >= 1 and s["p2g_per_sm"] >= 1
+    with pytest.raises(_lib.LPError):
+        sim.set_launch_shape(g2p_small=2)
+    sim.close()
+
+
+def test_autotuner_picks_a_shape_on_the_live_batch():
+    from litter_physics_b200 import _lib
+    from litter_physics_b200.sim import Batch
+
+    _lib.build()
+    b = Batch(uneven_batch())
+    t0 = [b.counters(i).time for i in range(3)]
+    report = b.autotune(4)
+    lines = report.strip().splitlines()
+    assert lines[-1].startswith("chosen: ") and len(lines) >= 8
+    chosen = b.launch_shape()
+    assert chosen["g2p_per_sm"] >= 1 and chosen["graph_attempts"] >= 1
+    # the tuning attempts were real steps of the trajectory
+    b.sync()
+    assert all(b.counters(i).time > t0[i] for i in range(3))
+    b.close()
