@@ -273,9 +273,43 @@ __device__ inline HbConst hb_const(double k, double n, double mu, double dt) {
   return h;
 }
 
+// (1 - q)^a for |q| <= 2^-7 and |a q| <= 2^-7, as exp(a log1p(-q)) from the Taylor series of
+// log1p and exp, each cut after the eighth power: log1p(-q) = -q (1 + q/2 + ... + q^7/8) and
+// exp(t) = 1 + t + ... + t^8/8!.  At these arguments the omitted terms are below 1e-19, so the
+// result is the FP64 power to rounding.
+__device__ __forceinline__ double pow_one_minus_small(double q, double a) {
+  double s = 1.0 / 8.0;
+  s = fma(s, q, 1.0 / 7.0);
+  s = fma(s, q, 1.0 / 6.0);
+  s = fma(s, q, 1.0 / 5.0);
+  s = fma(s, q, 1.0 / 4.0);
+  s = fma(s, q, 1.0 / 3.0);
+  s = fma(s, q, 1.0 / 2.0);
+  s = fma(s, q, 1.0);
+  const double t = -a * q * s;
+  double e = 1.0 / 40320.0;
+  e = fma(e, t, 1.0 / 5040.0);
+  e = fma(e, t, 1.0 / 720.0);
+  e = fma(e, t, 1.0 / 120.0);
+  e = fma(e, t, 1.0 / 24.0);
+  e = fma(e, t, 1.0 / 6.0);
+  e = fma(e, t, 1.0 / 2.0);
+  e = fma(e, t, 1.0);
+  return fma(e, t, 1.0);
+}
+
 // Bracketed Newton of constitutive.rs:280-362, with an optional start value sigma0 in
 // (yield, trial) (the learned warm start); the plain solver starts at the midpoint.
 // Returns failure code; iterations through *iters.
+//
+// The iteration runs on the excess stress x = sigma - yield over the bracket [0, trial - yield]:
+// the residual f = sigma - trial + 3 mu dt (x/K)^(1/n) = x - (trial - yield) + 3 mu dt p with
+// p = (x/K)^(1/n), and the Newton step x - f / f', f' = 1 + (3 mu dt / n) p / x, is
+// x (1 - q) with q = f / (x + (3 mu dt / n) p): one division per iterate.  The same bracket
+// updates, bisection safeguard and stopping rule as the reference's solver.  After a Newton
+// step the new power is the old one times (1 - q)^(1/n); once |q| is small (quadratic
+// convergence makes it so within a few iterates, and a good warm start from the first) that
+// factor comes from two short series instead of a logarithm and an exponential.
 __device__ inline int hb_return_d(double trial, double ys, const HbConst& h, double tol_rel, double sigma0,
                                   double* sigma_out, double* dep_out, int* iters) {
   *iters = 0;
@@ -292,35 +326,34 @@ __device__ inline int hb_return_d(double trial, double ys, const HbConst& h, dou
     return F_OK;
   }
   const double exponent = h.exponent, log_k = h.log_k, c1 = h.c1;
-  double lower = ys, upper = trial;
-  double sigma = (sigma0 > lower && sigma0 < upper) ? sigma0 : 0.5 * (lower + upper);
+  const double span = trial - ys;  // the bracket [0, span] of the excess stress
+  const double small_q = 0.0078125 / fmax(exponent, 1.0);  // |q| and |q / n| at most 2^-7
+  double lo = 0.0, hi = span;
+  double x = (sigma0 > ys && sigma0 < trial) ? sigma0 - ys : 0.5 * span;
   const double tolerance = tol_rel * fmax(trial, 1.0);
-  // With over = sigma - yield, the flow term is (over / K)^(1/n) = exp((log(over) - log K) / n),
-  // evaluated once per iterate, and the Newton step
-  //   sigma - f / f',  f' = 1 + 3 mu dt (1/n) (over/K)^(1/n) / over
-  // is written sigma - f over / (over + 3 mu dt (1/n) (over/K)^(1/n)): one division per iterate.
-  double over = fmax(sigma - ys, 0.0);
-  double pw = over > 0.0 ? exp(exponent * (log(over) - log_k)) : 0.0;
-  double last = sigma - trial + viscous_scale * pw;
+  double pw = x > 0.0 ? exp(exponent * (log(x) - log_k)) : 0.0;
+  double last = x - span + viscous_scale * pw;
   for (int it = 1; it <= 200; ++it) {
-    if (fabs(last) <= tolerance || (upper - lower) <= tolerance) {
+    if (fabs(last) <= tolerance || (hi - lo) <= tolerance) {
+      const double sigma = ys + x;
       *sigma_out = sigma;
       *dep_out = (trial - sigma) / h.mu3;
       *iters = it;
       return F_OK;
     }
-    if (last > 0.0) upper = sigma;
-    else lower = sigma;
-    double newton;
-    if (over > 0.0) {
-      newton = sigma - last * over / (over + c1 * pw);
+    if (last > 0.0) hi = x;
+    else lo = x;
+    // at x = 0 the derivative is infinite and the reference's Newton step is a no-op: bisect
+    const double q = x > 0.0 ? last / (x + c1 * pw) : 0.0;
+    const double xn = fma(-q, x, x);
+    if (x > 0.0 && isfinite(xn) && xn > lo && xn < hi) {
+      pw = fabs(q) <= small_q ? pw * pow_one_minus_small(q, exponent) : exp(exponent * (log(xn) - log_k));
+      x = xn;
     } else {
-      newton = sigma;  // infinite derivative: the reference's Newton step is a no-op here
+      x = 0.5 * (lo + hi);
+      pw = x > 0.0 ? exp(exponent * (log(x) - log_k)) : 0.0;
     }
-    sigma = (isfinite(newton) && newton > lower && newton < upper) ? newton : 0.5 * (lower + upper);
-    over = fmax(sigma - ys, 0.0);
-    pw = over > 0.0 ? exp(exponent * (log(over) - log_k)) : 0.0;
-    last = sigma - trial + viscous_scale * pw;
+    last = x - span + viscous_scale * pw;
     if (!isfinite(last)) {
       *iters = it;
       return F_CONST_NONFINITE;
