@@ -461,6 +461,14 @@ def ours(args, ws, rank, local):
         # per-kernel live timing (CUDA events on the same stream) of this arm
         results[arm]["kernel_ms"] = sim.kernel_times(args.kernel_steps)
     ktimes = results[arms[-1]]["kernel_ms"]
+    # share of G2P warp time in the FP64 return, per arm, from the same snapshot (outside the
+    # timed region; clock-instrumented G2P): the most any Newton start could save in G2P
+    return_share = {}
+    for arm in arms:
+        restore()
+        sim.set_warm_start(weights if arm == "warm" else None)
+        sim.run_substeps(args.warmup)
+        return_share[arm] = sim.g2p_return_share(args.kernel_steps)
     if args.no_e2e:
         e2e_steps = 0
     else:
@@ -545,6 +553,9 @@ def ours(args, ws, rank, local):
         "warm": {"newton_iterations_per_step": warm["newton_iterations"] / max(warm["accepted"], 1),
                  "mlp": train_info},
         "warm_over_plain": warm["value"] / plain["value"],
+        "g2p_return_share": return_share,
+        "warm_ceiling_note": "a Newton start can save at most the plain arm's g2p_return_share of G2P time, "
+                             "and G2P is kernel_ms.k_g2p of the step",
         "autotune": tune_report,
         "kernel_ms": {k: round(v, 5) for k, v in ktimes.items()},
         "roofline": {"kernel": "k_g2p", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],

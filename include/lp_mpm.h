@@ -290,6 +290,12 @@ lp_status lp_sim_grid_dump(lp_sim* sim, double dt, double* mass, double* momentu
  * ms[k] = mean duration of kernel k, names = 32-char slots; *count = kernels per attempt. */
 lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* names, int32_t capacity,
                               int32_t* count);
+/* Measurement: run `steps` attempts (real steps, time advances) with G2P's clock-instrumented
+ * instantiation and return in *share the fraction of G2P warp time spent in the FP64
+ * Herschel-Bulkley return (per round, the longest lane's time in the return, over each warp's
+ * time in its tiles).  It bounds what any Newton start, the learned warm start included, can
+ * save in G2P.  No counterpart in the reference. */
+lp_status lp_sim_g2p_return_share(lp_sim* sim, int32_t steps, double* share);
 /* Capture run_substeps into a CUDA graph of `steps` attempts (0 disables graphs). */
 lp_status lp_sim_use_graph(lp_sim* sim, int32_t steps);
 

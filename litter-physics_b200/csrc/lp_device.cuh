@@ -693,8 +693,11 @@ __device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& 
 
 // Rest of the paste update after paste_trial: the Herschel-Bulkley return started at sigma0
 // (in (yield, trial), or -1 for the midpoint), the stress and the plastic correction of H.
+// newton_cycles (measurement builds only, else null): clock64 cycles spent in the return are
+// added to it.
 __device__ inline void paste_finish(const float Htr[9], float mu, float lambda, double mu_d, double ys, const HbConst& h,
-                                    double tol, double sigma0, const PasteTrial& t, PasteOut& o) {
+                                    double tol, double sigma0, const PasteTrial& t, PasteOut& o,
+                                    long long* newton_cycles = nullptr) {
   if (t.path == PT_DONE) return;
   if (t.path == PT_JACOBI) {
     float Hj[9];
@@ -714,7 +717,9 @@ __device__ inline void paste_finish(const float Htr[9], float mu, float lambda, 
   if (trial_eq > ys && t.dnorm > 0.f) {
     double sigma, dep;
     int iters;
+    const long long c0 = newton_cycles ? clock64() : 0;
     const int e = hb_return_d(trial_eq, ys, h, tol, sigma0, &sigma, &dep, &iters);
+    if (newton_cycles) *newton_cycles += clock64() - c0;
     o.iters = iters;
     if (e != F_OK) {
       o.fail = e;

@@ -2248,6 +2248,34 @@ lp_status lp_batch_use_graph(lp_batch* b, int32_t steps) {
   b->E.graph_steps = steps > 0 ? steps : 0;
   return LP_OK;
 }
+lp_status lp_sim_g2p_return_share(lp_sim* sim, int32_t steps, double* share) {
+  Ensemble& E = sim->E;
+  if (!share || steps < 1) return set_error(LP_INVALID, "need steps >= 1 and an output");
+  if (E.ctrl_h.empty() || !std::isinf(E.ctrl_h[0].target)) {
+    lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
+    if (st != LP_OK) return st;
+  }
+  unsigned long long* d = nullptr;
+  CUDA_CK(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+  CUDA_CK(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), E.stream));
+  E.invalidate_graph();
+  E.A.g2p_clk = d;
+  lp_status st = LP_OK;
+  for (int s = 0; s < steps && st == LP_OK; ++s) {
+    lp::launch_attempt(E.A, E.stream);
+    if (cudaGetLastError() != cudaSuccess) st = set_error(LP_DEVICE, "launch failed in the return-share measurement");
+  }
+  E.A.g2p_clk = nullptr;
+  unsigned long long h[2] = {0, 0};
+  const cudaError_t e1 = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, E.stream);
+  const cudaError_t e2 = cudaStreamSynchronize(E.stream);
+  cudaFree(d);
+  if (st != LP_OK) return st;
+  if (e1 != cudaSuccess || e2 != cudaSuccess) return set_error(LP_DEVICE, "return-share measurement failed");
+  *share = h[0] > 0 ? (double)h[1] / (double)h[0] : 0.0;
+  return pull_ctrl(E);
+}
+
 lp_status lp_batch_autotune(lp_batch* b, int32_t trial_steps, char* report, size_t report_len) {
   return autotune(b->E, trial_steps, report, report_len);
 }

@@ -2040,8 +2040,11 @@ __device__ __forceinline__ void g2p_prefetch(float* __restrict__ buf, const floa
 
 // Warm start (WARM instantiation): each yielding lane reads the network's logit at its la8 from
 // its instance's table (k_mlp_table), interpolated between the two neighbouring nodes.
-// one tile of k_g2p, CTAs of NT threads
-template <bool WARM, int NT>
+// one tile of k_g2p, CTAs of NT threads.  CLOCKS (a measurement instantiation, not used by the
+// solver): every warp adds its clock64 cycles in the tile to clk[0] and, per round, the longest
+// lane time in the Herschel-Bulkley return to clk[1], so clk[1] / clk[0] is the share of warp
+// time the return takes.
+template <bool WARM, int NT, bool CLOCKS>
 __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restrict__ desc,
                                          const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
                                          float* __restrict__ st0, float* __restrict__ st1,
@@ -2050,7 +2053,7 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
                                          const float4* __restrict__ vel, ParticlePartial* __restrict__ part,
                                          const float* __restrict__ mlp_tab, float* __restrict__ log_x,
                                          float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
-                                         long long log_cap) {
+                                         long long log_cap, unsigned long long* __restrict__ clk) {
   __shared__ float4 hv[HN];
   __shared__ double shd[(NT / 32) * 9 + 9];
   extern __shared__ float4 g2p_dyn[];  // prefetched inputs of two rounds
@@ -2058,6 +2061,8 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
   if (!c.active) return;
+  const long long clk_begin = CLOCKS ? clock64() : 0;
+  unsigned long long clk_newton = 0;  // CLOCKS: this warp's return cycles in the tile
   const InstDesc& D = desc[inst];
   const int64_t ltile = tile - D.tile_off;
   const int64_t key0 = D.key_off + ltile * TB;
@@ -2245,7 +2250,9 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
       }
     }
     if (paste) {
-      paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, c.hb, D.tol, sigma0, pt, o);
+      long long nc = 0;
+      paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, c.hb, D.tol, sigma0, pt, o, CLOCKS ? &nc : nullptr);
+      if constexpr (CLOCKS) clk_newton += __reduce_max_sync(0xffffffffu, (unsigned)nc);  // the warp is converged
 #pragma unroll
       for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
       if (valid) {
@@ -2302,13 +2309,19 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
     P.yielded = (int)rv[7];
     P.fail_value = rv[8];
   }
+  if constexpr (CLOCKS) {
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(clk, (unsigned long long)(clock64() - clk_begin));
+      atomicAdd(clk + 1, clk_newton);
+    }
+  }
 }
 
 // Persistent CTAs (as many as the launch shape asks, at most as many as fit the GPU at once)
 // walk the attempt's list of occupied tiles; the partial results are per tile, so they do not
 // depend on which CTA took which tile.  Both block shapes hold 16 warps per SM at the 128
 // registers a thread needs.
-template <bool WARM, int NT>
+template <bool WARM, int NT, bool CLOCKS = false>
 __global__ void __launch_bounds__(NT, 512 / NT)
     k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
@@ -2316,12 +2329,12 @@ __global__ void __launch_bounds__(NT, 512 / NT)
           const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const float* __restrict__ mlp_tab,
           float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
           long long log_cap, const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count,
-          uint32_t* cursor) {
+          uint32_t* cursor, unsigned long long* __restrict__ clk) {
   __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
   for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
-    g2p_tile<WARM, NT>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, id0, id1, cap, start, perm, vel, part,
-                       mlp_tab, log_x, log_y, log_n, log_cap);
+    g2p_tile<WARM, NT, CLOCKS>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, id0, id1, cap, start, perm, vel,
+                               part, mlp_tab, log_x, log_y, log_n, log_cap, clk);
     __syncthreads();  // the next tile reuses the shared memory
   }
 }
@@ -2938,8 +2951,13 @@ static void launch_g2p(const DeviceArrays& A, bool warm, cudaStream_t s) {
   const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[small][warm ? 1 : 0]);
 #define LP_G2P_ARGS                                                                                               \
   A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, tab, \
-      A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count, cur
-  if (small) {
+      A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count, cur, A.g2p_clk
+  if (A.g2p_clk) {  // measurement of the return's share of G2P warp time (256-thread CTAs)
+    constexpr int T = G2P_THREADS;
+    const unsigned n2 = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[0][warm ? 1 : 0]);
+    if (warm) k_g2p<true, T, true><<<n2, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
+    else k_g2p<false, T, true><<<n2, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
+  } else if (small) {
     constexpr int T = G2P_THREADS_SMALL;
     if (warm) k_g2p<true, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
     else k_g2p<false, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);

@@ -69,6 +69,7 @@ struct DeviceArrays {
   unsigned long long* log_n = nullptr;
   long long log_cap = 0;
   LaunchShape shape;
+  unsigned long long* g2p_clk = nullptr;  // non-null: G2P runs its clock-measurement instantiation
   // pellet bed (instances with InstDesc::bed_np >= 2)
   int any_bed = 0;
   int64_t n_bed = 0;                                 // pellets of all instances

@@ -117,6 +117,7 @@ def lib():
         "lp_batch_use_graph": ([P, I32], I32),
         "lp_batch_autotune": ([P, I32, C.c_char_p, C.c_size_t], I32),
         "lp_sim_autotune": ([P, I32, C.c_char_p, C.c_size_t], I32),
+        "lp_sim_g2p_return_share": ([P, I32, D], I32),
         "lp_sim_set_launch_shape": ([P, C.POINTER(_abi.LaunchShape)], I32),
         "lp_sim_get_launch_shape": ([P, C.POINTER(_abi.LaunchShape)], I32),
         "lp_batch_set_launch_shape": ([P, C.POINTER(_abi.LaunchShape)], I32),

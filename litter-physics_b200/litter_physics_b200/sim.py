@@ -92,6 +92,13 @@ class Simulation:
         check(lib().lp_sim_get_launch_shape(self._h, C.byref(s)))
         return s.as_dict()
 
+    def g2p_return_share(self, steps: int) -> float:
+        """Share of G2P warp time in the FP64 Herschel-Bulkley return over `steps` real attempts
+        (clock-instrumented G2P): what any Newton start could save in G2P at most."""
+        out = C.c_double()
+        check(lib().lp_sim_g2p_return_share(self._h, int(steps), C.byref(out)))
+        return out.value
+
     def set_launch_shape(self, **fields) -> None:
         """Set fields of `lp_launch_shape` (g2p_small, g2p_per_sm, p2g_small, p2g_per_sm,
         dynamic_tiles, graph_attempts); the others keep their values."""

@@ -85,6 +85,27 @@ def test_launch_shape_round_trip_and_refusal():
     sim.close()
 
 
+def test_return_share_measurement_steps_like_the_solver():
+    """The clock-instrumented G2P used to measure the return's share of G2P time takes the same
+    steps as the solver's G2P, and the share is a fraction."""
+    from litter_physics_b200 import _lib, configs
+    from litter_physics_b200.sim import Simulation
+
+    _lib.build()
+    spec = configs.slump(32, (8, 8, 16), seed=4, yield_range=(20.0, 100.0))
+    a, b = Simulation(spec), Simulation(spec)
+    a.run_substeps(30)
+    b.run_substeps(20)
+    share = b.g2p_return_share(10)
+    a.sync()
+    b.sync()
+    assert 0.0 < share < 1.0
+    pa, pb = by_id(a.particles()), by_id(b.particles())
+    assert np.array_equal(pa["position"], pb["position"]) and np.array_equal(pa["deformation"], pb["deformation"])
+    liquid = Simulation(configs.dam_break(32, (16, 8, 16), seed=1))
+    assert liquid.g2p_return_share(3) == 0.0
+
+
 def test_autotuner_picks_a_shape_on_the_live_batch():
     from litter_physics_b200 import _lib
     from litter_physics_b200.sim import Batch
