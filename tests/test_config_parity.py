@@ -6,8 +6,9 @@ particles by id and checks the north-star bars:
   * velocities: ||v_gpu - v_ref||_2 / ||v_ref||_2 <= 1e-5 (every case here is in motion: a
     slumping column or a breaking dam, so ||v_ref|| is the physical velocity, not noise);
   * the same accepted and rejected step counts;
-  * ledgers: gravity and wall impulses to 1e-4, the energy channels to 1e-3 relative (FP32
-    particle arithmetic against FP64).
+  * ledgers: gravity and wall impulses to 1e-5, the energy channels (wall projection, wall
+    friction, wall traction, plastic work) to 1e-4 relative (FP32 particle arithmetic against
+    FP64; measured at most 5e-7 and 1e-5).
 
 Cases (sizes as the benchmark configurations state them):
   * the plain HB slump: 64^3 grid, 16x16x32-cell column, 65,536 particles, seed 0;
@@ -67,11 +68,11 @@ def ledger_errors(lg, lr) -> dict:
 
 def check_ledgers(err: dict, lr) -> None:
     for f in ("gravity_impulse", "wall_impulse"):
-        assert err[f] <= 1e-4, (f, err[f])
+        assert err[f] <= 1e-5, (f, err[f])
     for f in ("wall_normal_projection_energy", "wall_friction_dissipation", "wall_normal_traction_energy",
               "plastic_dissipation"):
         if getattr(lr, f) != 0.0:
-            assert err[f] <= 1e-3, (f, err[f])
+            assert err[f] <= 1e-4, (f, err[f])
 
 
 def oracle_run(spec, steps: int):

@@ -51,23 +51,31 @@ def run(specs_fn, shape: dict, steps: int):
 def uneven_batch():
     from litter_physics_b200 import configs
 
+    # one fixture kind per batch: three slumps of uneven size, one with per-particle yield stress
     return [configs.slump(16, (4, 4, 8), seed=21), configs.slump(32, (8, 8, 16), seed=22, yield_range=(20.0, 100.0)),
-            configs.dam_break(32, (16, 8, 16), seed=23)]
+            configs.slump(24, (6, 6, 12), seed=23)]
+
+
+def liquid_batch():
+    from litter_physics_b200 import configs
+
+    return [configs.dam_break(32, (16, 8, 16), seed=23), configs.dam_break(24, (12, 6, 12), seed=24)]
 
 
 def test_every_launch_shape_gives_identical_results():
     from litter_physics_b200 import _lib
 
     _lib.build()
-    ref = run(uneven_batch, SHAPES[0], 24)
-    for shape in SHAPES[1:]:
-        got = run(uneven_batch, shape, 24)
-        for (state, plastic), (ref_state, ref_plastic) in zip(got, ref, strict=True):
-            assert state == ref_state, shape
-            if shape.get("g2p_small"):
-                assert abs(plastic - ref_plastic) <= 1e-13 * abs(ref_plastic), shape
-            else:
-                assert plastic == ref_plastic, shape
+    for batch in (uneven_batch, liquid_batch):
+        ref = run(batch, SHAPES[0], 24)
+        for shape in SHAPES[1:]:
+            got = run(batch, shape, 24)
+            for (state, plastic), (ref_state, ref_plastic) in zip(got, ref, strict=True):
+                assert state == ref_state, shape
+                if shape.get("g2p_small"):
+                    assert abs(plastic - ref_plastic) <= 1e-13 * abs(ref_plastic), shape
+                else:
+                    assert plastic == ref_plastic, shape
 
 
 def test_launch_shape_round_trip_and_refusal():
