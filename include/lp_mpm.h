@@ -334,13 +334,14 @@ lp_status lp_batch_instance_state(lp_batch* b, int32_t index, int32_t* state, ch
  * results; only the speed differs.
  *   g2p_small      1: G2P CTAs of 128 threads, 0: 256 threads
  *   g2p_per_sm     persistent G2P CTAs per SM (0, or more than fit: as many as fit)
- *   p2g_small      1: P2G chunks of 512 particles, 0: 1024 particles
+ *   p2g_variant    P2G chunks of 0: 1024 particles, 1: 512 particles, 2: 512 particles whose state
+ *                  is copied into shared memory (cp.async) one chunk ahead, across tiles
  *   p2g_per_sm     persistent P2G CTAs per SM (0, or more than fit: as many as fit)
  *   dynamic_tiles  1: CTAs take occupied tiles from an atomic cursor, 0: round robin
  *   graph_attempts attempts captured per CUDA graph replay of run_substeps (0 or 1: no graph)
  * The getter reports the CTAs per SM the launches use. */
 typedef struct lp_launch_shape {
-  int32_t g2p_small, g2p_per_sm, p2g_small, p2g_per_sm, dynamic_tiles, graph_attempts;
+  int32_t g2p_small, g2p_per_sm, p2g_variant, p2g_per_sm, dynamic_tiles, graph_attempts;
 } lp_launch_shape;
 lp_status lp_sim_set_launch_shape(lp_sim* sim, const lp_launch_shape* shape);
 lp_status lp_sim_get_launch_shape(lp_sim* sim, lp_launch_shape* out);

@@ -700,7 +700,7 @@ constexpr int P2G_CHUNK = 1024, P2G_CHUNK_SMALL = 512;
 constexpr int P2G_REC = 16;  // m, q[3], A[9], f[3]
 constexpr size_t P2G_PART_BYTES = sizeof(float4) * TB * 27;
 // dynamic shared memory of a chunk size: the records, which the partial node sums alias later
-constexpr size_t p2g_smem(int chunk) {
+__host__ __device__ constexpr size_t p2g_smem(int chunk) {
   return P2G_PART_BYTES > sizeof(float) * P2G_REC * chunk ? P2G_PART_BYTES : sizeof(float) * P2G_REC * chunk;
 }
 // Slot of chunk particle i in each record row: within each 32-word segment the slots rotate by
@@ -708,29 +708,91 @@ constexpr size_t p2g_smem(int chunk) {
 // different shared-memory banks in the per-bin pass; consecutive i still fill a segment.
 __device__ __forceinline__ uint32_t rec_slot(uint32_t i) { return (i & ~31u) | ((i + (i >> 5)) & 31u); }
 
-// one tile of k_p2g, chunks of CHUNK particles
+// Asynchronous 4-byte global -> shared copies (cp.async) of this GPU's own memory, used by the
+// staged P2G and by G2P to prefetch particle inputs while the CTA computes.
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// State components P2G reads, in the order of the staged (prefetched) copies: x3 v3 C9 tau6 m V0.
+constexpr int P2G_RAW = 23;
+__device__ __forceinline__ int p2g_raw_comp(int r) {
+  return r < 15 ? C_X + r : (r < 21 ? C_TAU + (r - 15) : (r == 21 ? C_M : C_V0));
+}
+__host__ __device__ constexpr size_t p2g_raw_bytes(int chunk) { return sizeof(float) * P2G_RAW * chunk; }
+
+// Staged P2G: asynchronous copies (cp.async, 4 bytes each) of the state components of chunk
+// [c0, c0 + cn) of a tile into raw[P2G_RAW][CHUNK], particle i of the chunk copied by thread
+// i % P2G_THREADS, which is the thread that reads it back in phase 1.  The caller commits.
 template <int CHUNK>
+__device__ __forceinline__ void p2g_stage(float* __restrict__ raw, const float* __restrict__ cur,
+                                          const uint32_t* __restrict__ perm, int64_t cap, uint32_t c0, uint32_t cn) {
+  constexpr int PER = (CHUNK + P2G_THREADS - 1) / P2G_THREADS;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const uint32_t i = threadIdx.x + q * P2G_THREADS;
+    if (i < cn) {
+      const int64_t src = perm[c0 + i];
+#pragma unroll
+      for (int r = 0; r < P2G_RAW; ++r) cp_async4(raw + r * CHUNK + i, cur + (int64_t)p2g_raw_comp(r) * cap + src);
+    }
+  }
+}
+// the first chunk of occupied tile `tile` (an entry of the attempt's tile list)
+template <int CHUNK>
+__device__ __forceinline__ void p2g_stage_tile(float* __restrict__ raw, int tile, const InstDesc* __restrict__ desc,
+                                               const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
+                                               const float* __restrict__ st0, const float* __restrict__ st1,
+                                               int64_t cap, const uint32_t* __restrict__ start,
+                                               const uint32_t* __restrict__ perm) {
+  const int inst = tile_inst[tile];
+  const InstDesc& D = desc[inst];
+  const int64_t key0 = D.key_off + (int64_t)(tile - D.tile_off) * TB;
+  const uint32_t ts = start[key0], te = start[key0 + TB];
+  p2g_stage<CHUNK>(raw, ctrl[inst].parity ? st1 : st0, perm, cap, ts, min((uint32_t)CHUNK, te - ts));
+}
+
+// one tile of k_p2g, chunks of CHUNK particles.  STAGED: the particle state of each chunk
+// arrives by the asynchronous copies of p2g_stage, issued one chunk ahead: the tile's first
+// chunk by the caller (or the previous tile), each later chunk, and after the last one the
+// first chunk of next_tile (-1: none), right after the thread has read its copies of the
+// current chunk, so that the copies fly while the CTA scatters.
+template <int CHUNK, bool STAGED>
 __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restrict__ desc,
                                          const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
                                          const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
                                          const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
                                          long long* __restrict__ acc, int64_t node_total,
-                                         uint32_t* __restrict__ blk_epoch, int transport_only) {
+                                         uint32_t* __restrict__ blk_epoch, int transport_only, int next_tile) {
   constexpr int P2G_PER_THREAD = (CHUNK + P2G_THREADS - 1) / P2G_THREADS;  // phase-1 particles per thread
   static_assert(CHUNK % 32 == 0, "record rows rotate within 32-word segments");
   extern __shared__ float4 part[];  // particle records during the chunks, then TB * 27 partial node sums
   float* rec = reinterpret_cast<float*>(part);  // [P2G_REC][CHUNK]
+  // STAGED: the raw copies sit after the records / partials region
+  float* raw = reinterpret_cast<float*>(reinterpret_cast<char*>(part) + p2g_smem(CHUNK));
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
   __shared__ int redi[P2G_THREADS / 32 + 1];
 
   const int inst = tile_inst[tile];
   const Control& c = ctrl[inst];
-  if (!c.active) return;
   const InstDesc& D = desc[inst];
   const int64_t ltile = tile - D.tile_off;
   const int64_t key0 = D.key_off + ltile * TB;
   const uint32_t ts = start[key0], te = start[key0 + TB];
-  if (ts == te) return;  // empty tile (uniform across the CTA)
+  if (!c.active || ts == te) {  // inactive instance or empty tile (uniform across the CTA)
+    if constexpr (STAGED) {      // the tile list holds neither, but keep the staging chain whole
+      cp_async_wait<0>();        // this tile's copies land before the next tile's reuse the buffer
+      if (next_tile >= 0) p2g_stage_tile<CHUNK>(raw, next_tile, desc, ctrl, tile_inst, st0, st1, cap, start, perm);
+      cp_async_commit();
+    }
+    return;
+  }
 
   const int tz = (int)(ltile % D.tiles[2]);
   const int ty = (int)((ltile / D.tiles[2]) % D.tiles[1]);
@@ -760,26 +822,45 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
     // phase 1: one thread per particle.  The thread's permutation entries of the chunk are loaded
     // first, so that each particle's state loads issue without waiting for its entry.
     uint32_t srcs[P2G_PER_THREAD];
+    if constexpr (STAGED) {
+      cp_async_wait<0>();  // this thread's copies of the chunk have landed
+    } else {
 #pragma unroll
-    for (int q = 0; q < P2G_PER_THREAD; ++q)
-      srcs[q] = t + q * P2G_THREADS < cn ? perm[c0 + t + q * P2G_THREADS] : 0u;
+      for (int q = 0; q < P2G_PER_THREAD; ++q)
+        srcs[q] = t + q * P2G_THREADS < cn ? perm[c0 + t + q * P2G_THREADS] : 0u;
+    }
 #pragma unroll
     for (int q = 0; q < P2G_PER_THREAD; ++q) {
       const uint32_t i = t + q * P2G_THREADS;
       if (i >= cn) break;
-      const int64_t src = srcs[q];
-      float x[3], v[3], Cm[9], tau[6];
+      float x[3], v[3], Cm[9], tau[6], m, v0;
+      if constexpr (STAGED) {
+        const float* in = raw + i;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        x[a] = cur[(C_X + a) * cap + src];
-        v[a] = cur[(C_V + a) * cap + src];
+        for (int a = 0; a < 3; ++a) {
+          x[a] = in[a * CHUNK];
+          v[a] = in[(3 + a) * CHUNK];
+        }
+#pragma unroll
+        for (int a = 0; a < 9; ++a) Cm[a] = in[(6 + a) * CHUNK];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) tau[a] = in[(15 + a) * CHUNK];
+        m = in[21 * CHUNK];
+        v0 = in[22 * CHUNK];
+      } else {
+        const int64_t src = srcs[q];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          x[a] = cur[(C_X + a) * cap + src];
+          v[a] = cur[(C_V + a) * cap + src];
+        }
+#pragma unroll
+        for (int a = 0; a < 9; ++a) Cm[a] = cur[(C_C + a) * cap + src];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) tau[a] = cur[(C_TAU + a) * cap + src];
+        m = cur[C_M * cap + src];
+        v0 = cur[C_V0 * cap + src];
       }
-#pragma unroll
-      for (int a = 0; a < 9; ++a) Cm[a] = cur[(C_C + a) * cap + src];
-#pragma unroll
-      for (int a = 0; a < 6; ++a) tau[a] = cur[(C_TAU + a) * cap + src];
-      const float m = cur[C_M * cap + src];
-      const float v0 = cur[C_V0 * cap + src];
       // A = C m - tau (dt 4/dx^2 V0)
       const float sv = stress_scale * v0;
       const float T[9] = {tau[0], tau[3], tau[4], tau[3], tau[1], tau[5], tau[4], tau[5], tau[2]};
@@ -800,6 +881,13 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
       tot[1] += to_fixed((double)m * (double)v[0], s_p);
       tot[2] += to_fixed((double)m * (double)v[1], s_p);
       tot[3] += to_fixed((double)m * (double)v[2], s_p);
+    }
+    if constexpr (STAGED) {
+      // this thread has read its copies: the next chunk (of this tile or of the next) may land
+      if (c0 + CHUNK < te) p2g_stage<CHUNK>(raw, cur, perm, cap, c0 + CHUNK, min((uint32_t)CHUNK, te - c0 - CHUNK));
+      else if (next_tile >= 0)
+        p2g_stage_tile<CHUNK>(raw, next_tile, desc, ctrl, tile_inst, st0, st1, cap, start, perm);
+      cp_async_commit();
     }
     __syncthreads();
     // phase 2: this bin's particles inside the chunk, in sorted order
@@ -930,19 +1018,41 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
 
 // Persistent CTAs (as many as the launch shape asks, at most as many as fit the GPU at once)
 // walk the attempt's list of occupied tiles.
-template <int CHUNK>
+// STAGED: each tile's next tile is known before the tile starts (two cursor slots, used
+// alternately, so that the slot a CTA reads is not rewritten before every thread has read it),
+// and the first chunk of the next tile is copied while the current tile scatters.
+template <int CHUNK, bool STAGED>
 __global__ void __launch_bounds__(P2G_THREADS, 2)
     k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
           const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
           int64_t node_total, uint32_t* __restrict__ blk_epoch, int transport_only,
           const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count, uint32_t* cursor) {
-  __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
-  for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
-    p2g_tile<CHUNK>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm, acc, node_total,
-                    blk_epoch, transport_only);
-    __syncthreads();  // the next tile reuses the shared memory
+  if constexpr (!STAGED) {
+    __shared__ uint32_t slot;
+    for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
+      p2g_tile<CHUNK, false>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm, acc, node_total,
+                             blk_epoch, transport_only, -1);
+      __syncthreads();  // the next tile reuses the shared memory
+    }
+  } else {
+    __shared__ uint32_t slots[2];
+    extern __shared__ float4 part[];
+    float* raw = reinterpret_cast<float*>(reinterpret_cast<char*>(part) + p2g_smem(CHUNK));
+    int which = 0;
+    uint32_t i = tile_first(cursor, &slots[0]);
+    if (i < n) p2g_stage_tile<CHUNK>(raw, (int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm);
+    cp_async_commit();
+    while (i < n) {
+      which ^= 1;
+      const uint32_t nx = tile_next(cursor, i, &slots[which]);
+      p2g_tile<CHUNK, true>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm, acc, node_total,
+                            blk_epoch, transport_only, nx < n ? (int)tile_list[nx] : -1);
+      __syncthreads();  // the next tile reuses the shared memory
+      i = nx;
+    }
+    cp_async_wait<0>();  // no copy may land after the CTA's shared memory is released
   }
 }
 
@@ -1988,18 +2098,8 @@ __global__ void __launch_bounds__(64) k_bed_step(const InstDesc* __restrict__ de
 // (TX+2)(TY+2)(TZ+2) node velocities are staged in shared memory once, then the CTA walks the
 // tile's particles (contiguous in sorted slot order),
 // gathers from shared memory, advects, runs the constitutive update and writes the trial state
-// in sorted slot order.
-// Asynchronous 4-byte global -> shared copies (cp.async), used to prefetch the next round's
-// particle inputs while the current round computes.
-__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
+// in sorted slot order.  The next round's particle inputs are prefetched by cp.async while the
+// current round computes.
 
 // G2P input slots per particle, [slot][thread] in shared memory, two rounds in flight
 enum {
@@ -2864,8 +2964,13 @@ static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1)
 // Resident CTAs per SM of the persistent kernels' instantiations (from the occupancy calculator;
 // the defaults are the B200 figures) and the SM count.
 static int g_sms = 148, g_sort_per_sm = 16;
-static int g_p2g_per_sm[2] = {2, 2};                 // [p2g_small]
+static int g_p2g_per_sm[3] = {2, 2, 2};              // [p2g_variant]
 static int g_g2p_per_sm[2][2] = {{2, 2}, {4, 4}};   // [g2p_small][warm]
+
+// dynamic shared memory of each P2G variant: records / partials, plus the staged copies
+static size_t p2g_variant_smem(int v) {
+  return v == 0 ? p2g_smem(P2G_CHUNK) : p2g_smem(P2G_CHUNK_SMALL) + (v == 2 ? p2g_raw_bytes(P2G_CHUNK_SMALL) : 0);
+}
 
 static void occupancy(int* out, const void* fn, int threads, size_t smem) {
   int per = 0;
@@ -2873,9 +2978,10 @@ static void occupancy(int* out, const void* fn, int threads, size_t smem) {
 }
 
 void configure_kernels() {
-  cudaFuncSetAttribute(k_p2g<P2G_CHUNK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem(P2G_CHUNK));
-  cudaFuncSetAttribute(k_p2g<P2G_CHUNK_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)p2g_smem(P2G_CHUNK_SMALL));
+  const void* p2g[3] = {(const void*)k_p2g<P2G_CHUNK, false>, (const void*)k_p2g<P2G_CHUNK_SMALL, false>,
+                        (const void*)k_p2g<P2G_CHUNK_SMALL, true>};
+  for (int v = 0; v < 3; ++v)
+    cudaFuncSetAttribute(p2g[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_variant_smem(v));
   cudaFuncSetAttribute(k_g2p<false, G2P_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)g2p_smem(G2P_THREADS));
   cudaFuncSetAttribute(k_g2p<true, G2P_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2889,8 +2995,7 @@ void configure_kernels() {
     return;
   g_sms = sms;
   occupancy(&g_sort_per_sm, (const void*)k_bin_sort, TB, 0);
-  occupancy(&g_p2g_per_sm[0], (const void*)k_p2g<P2G_CHUNK>, P2G_THREADS, p2g_smem(P2G_CHUNK));
-  occupancy(&g_p2g_per_sm[1], (const void*)k_p2g<P2G_CHUNK_SMALL>, P2G_THREADS, p2g_smem(P2G_CHUNK_SMALL));
+  for (int v = 0; v < 3; ++v) occupancy(&g_p2g_per_sm[v], p2g[v], P2G_THREADS, p2g_variant_smem(v));
   occupancy(&g_g2p_per_sm[0][0], (const void*)k_g2p<false, G2P_THREADS>, G2P_THREADS, g2p_smem(G2P_THREADS));
   occupancy(&g_g2p_per_sm[0][1], (const void*)k_g2p<true, G2P_THREADS>, G2P_THREADS, g2p_smem(G2P_THREADS));
   occupancy(&g_g2p_per_sm[1][0], (const void*)k_g2p<false, G2P_THREADS_SMALL>, G2P_THREADS_SMALL,
@@ -2905,14 +3010,15 @@ static unsigned persistent_ctas(int requested, int limit) {
   return (unsigned)(per * g_sms);
 }
 
-int launch_shape_limits(int out[6]) {
+int launch_shape_limits(int out[7]) {
   out[0] = g_sms;
   out[1] = g_p2g_per_sm[0];
   out[2] = g_p2g_per_sm[1];
   out[3] = g_g2p_per_sm[0][1];
   out[4] = g_g2p_per_sm[1][1];
   out[5] = g_sort_per_sm;
-  return 6;
+  out[6] = g_p2g_per_sm[2];
+  return 7;
 }
 
 // the occupied-tile list, then P2G over it
@@ -2927,16 +3033,16 @@ static int launch_tiles_p2g(const DeviceArrays& A, cudaStream_t s, int transport
                                                                A.tile_count, cur);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  const unsigned ctas = persistent_ctas(L.p2g_per_sm, g_p2g_per_sm[L.p2g_small ? 1 : 0]);
+  const int v = (L.p2g_variant >= 0 && L.p2g_variant <= 2) ? L.p2g_variant : 0;
+  const unsigned ctas = persistent_ctas(L.p2g_per_sm, g_p2g_per_sm[v]);
   uint32_t* pc = cur ? cur + 1 : nullptr;
-  if (L.p2g_small)
-    k_p2g<P2G_CHUNK_SMALL><<<ctas, P2G_THREADS, p2g_smem(P2G_CHUNK_SMALL), s>>>(
-        A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start, A.perm, A.acc, A.node_total, A.blk_epoch,
-        transport_only, A.tile_list, A.tile_count, pc);
-  else
-    k_p2g<P2G_CHUNK><<<ctas, P2G_THREADS, p2g_smem(P2G_CHUNK), s>>>(
-        A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start, A.perm, A.acc, A.node_total, A.blk_epoch,
-        transport_only, A.tile_list, A.tile_count, pc);
+#define LP_P2G_ARGS                                                                                          \
+  A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start, A.perm, A.acc, A.node_total, A.blk_epoch, \
+      transport_only, A.tile_list, A.tile_count, pc
+  if (v == 2) k_p2g<P2G_CHUNK_SMALL, true><<<ctas, P2G_THREADS, p2g_variant_smem(2), s>>>(LP_P2G_ARGS);
+  else if (v == 1) k_p2g<P2G_CHUNK_SMALL, false><<<ctas, P2G_THREADS, p2g_variant_smem(1), s>>>(LP_P2G_ARGS);
+  else k_p2g<P2G_CHUNK, false><<<ctas, P2G_THREADS, p2g_variant_smem(0), s>>>(LP_P2G_ARGS);
+#undef LP_P2G_ARGS
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   return 3;

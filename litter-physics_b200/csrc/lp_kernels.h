@@ -15,7 +15,8 @@ constexpr int DIAG_N = 19;
 struct LaunchShape {
   int g2p_small = 0;   // 1: G2P CTAs of G2P_THREADS_SMALL (128) threads, 0: G2P_THREADS (256)
   int g2p_per_sm = 0;  // persistent G2P CTAs per SM
-  int p2g_small = 0;   // 1: P2G chunks of P2G_CHUNK_SMALL (512) particles, 0: P2G_CHUNK (1024)
+  int p2g_variant = 0;  // P2G chunks of 0: P2G_CHUNK (1024) particles, 1: P2G_CHUNK_SMALL (512),
+                        // 2: P2G_CHUNK_SMALL with each chunk's particle state copied one chunk ahead
   int p2g_per_sm = 0;  // persistent P2G CTAs per SM
   int dynamic = 1;     // 1: CTAs take tiles from the attempt's cursors, 0: round robin
 };
@@ -112,8 +113,8 @@ int launch_export(const HostParticleChunk& h, int64_t n, int64_t first, const fl
 uint64_t kernel_launch_count();
 void configure_kernels();              // one-time function attributes (dynamic shared memory)
 // out = SMs, resident CTAs per SM of P2G (1024- and 512-particle chunks), of the warm G2P (256-
-// and 128-thread CTAs) and of the bin sort; returns 6
-int launch_shape_limits(int out[6]);
+// and 128-thread CTAs), of the bin sort and of the staged 512-particle P2G; returns 7
+int launch_shape_limits(int out[7]);
 void set_last_error(const char* msg);  // message returned by lp_last_error()
 void add_kernel_launches(uint64_t n);
 

@@ -227,7 +227,7 @@ class LaunchShape(C.Structure):
     _fields_ = [
         ("g2p_small", C.c_int32),
         ("g2p_per_sm", C.c_int32),
-        ("p2g_small", C.c_int32),
+        ("p2g_variant", C.c_int32),
         ("p2g_per_sm", C.c_int32),
         ("dynamic_tiles", C.c_int32),
         ("graph_attempts", C.c_int32),

@@ -100,7 +100,7 @@ class Simulation:
         return out.value
 
     def set_launch_shape(self, **fields) -> None:
-        """Set fields of `lp_launch_shape` (g2p_small, g2p_per_sm, p2g_small, p2g_per_sm,
+        """Set fields of `lp_launch_shape` (g2p_small, g2p_per_sm, p2g_variant, p2g_per_sm,
         dynamic_tiles, graph_attempts); the others keep their values."""
         s = _abi.LaunchShape()
         check(lib().lp_sim_get_launch_shape(self._h, C.byref(s)))

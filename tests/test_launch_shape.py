@@ -17,7 +17,9 @@ SHAPES = [
     {"dynamic_tiles": 0},
     {"g2p_small": 1},
     {"g2p_small": 1, "g2p_per_sm": 3},
-    {"p2g_small": 1},
+    {"p2g_variant": 1},
+    {"p2g_variant": 2},
+    {"p2g_variant": 2, "dynamic_tiles": 0},
     {"p2g_per_sm": 1, "g2p_per_sm": 1, "dynamic_tiles": 0},
     {"graph_attempts": 4},
 ]
@@ -84,9 +86,9 @@ def test_launch_shape_round_trip_and_refusal():
 
     _lib.build()
     sim = Simulation(configs.slump(16, (4, 4, 8), seed=1))
-    sim.set_launch_shape(g2p_small=1, p2g_small=1, dynamic_tiles=0, graph_attempts=4)
+    sim.set_launch_shape(g2p_small=1, p2g_variant=1, dynamic_tiles=0, graph_attempts=4)
     s = sim.launch_shape()
-    assert (s["g2p_small"], s["p2g_small"], s["dynamic_tiles"], s["graph_attempts"]) == (1, 1, 0, 4)
+    assert (s["g2p_small"], s["p2g_variant"], s["dynamic_tiles"], s["graph_attempts"]) == (1, 1, 0, 4)
     assert s["g2p_per_sm"] >= 1 and s["p2g_per_sm"] >= 1
     with pytest.raises(_lib.LPError):
         sim.set_launch_shape(g2p_small=2)
