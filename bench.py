@@ -500,10 +500,13 @@ def ours(args, ws, rank, local):
     torch.cuda.synchronize()
     te0 = time.perf_counter()
     sim.set_particles(snap)
+    ti = time.perf_counter()
     t_target = sim.time + e2e_steps * spec.max_dt
     sim.advance_to(t_target)
+    ta = time.perf_counter()
     out = sim.particles()
     te1 = time.perf_counter()
+    e2e_split = {"import_s": round(ti - te0, 4), "advance_s": round(ta - ti, 4), "export_s": round(te1 - ta, 4)}
     steps_done = e2e_steps
     bytes_out = sum(v.nbytes for v in out.values())
     e2e_value = ws * n * steps_done / (te1 - te0)
@@ -587,6 +590,7 @@ def ours(args, ws, rank, local):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_in / steps_done,
                 "d2h_bytes_per_step": bytes_out / steps_done,
                 "path": "lp_sim_import_particles -> lp_sim_advance -> lp_sim_export_particles (host FP64 buffers)",
+                "split": e2e_split,
                 "steps": steps_done},
         "parity": parity,
         "config0": config0_info,

@@ -19,6 +19,21 @@ from . import _abi
 from ._lib import LPError, check, lib
 
 
+def _shape_with(read, fields: dict) -> _abi.LaunchShape:
+    """The current launch shape (read(s) fills s with the CTAs per SM in use) with `fields`
+    replaced.  A changed G2P block shape or P2G variant without its own CTAs-per-SM field gets 0
+    (as many as fit that instantiation) instead of the count that fitted the previous one."""
+    s = _abi.LaunchShape()
+    read(s)
+    if "g2p_small" in fields and "g2p_per_sm" not in fields and int(fields["g2p_small"]) != s.g2p_small:
+        s.g2p_per_sm = 0
+    if "p2g_variant" in fields and "p2g_per_sm" not in fields and int(fields["p2g_variant"]) != s.p2g_variant:
+        s.p2g_per_sm = 0
+    for k, v in fields.items():
+        setattr(s, k, int(v))
+    return s
+
+
 class Simulation:
     """One MLS-MPM simulation resident on the GPU."""
 
@@ -101,12 +116,10 @@ class Simulation:
 
     def set_launch_shape(self, **fields) -> None:
         """Set fields of `lp_launch_shape` (g2p_small, g2p_per_sm, p2g_variant, p2g_per_sm,
-        dynamic_tiles, graph_attempts); the others keep their values."""
-        s = _abi.LaunchShape()
-        check(lib().lp_sim_get_launch_shape(self._h, C.byref(s)))
-        for k, v in fields.items():
-            setattr(s, k, int(v))
-        check(lib().lp_sim_set_launch_shape(self._h, C.byref(s)))
+        dynamic_tiles, graph_attempts); the others keep their values, except that a new G2P
+        block shape or P2G variant given without its CTAs per SM gets as many as fit."""
+        check(lib().lp_sim_set_launch_shape(self._h, C.byref(_shape_with(
+            lambda s: check(lib().lp_sim_get_launch_shape(self._h, C.byref(s))), fields))))
 
     def stability_limit(self) -> float:
         out = C.c_double()
@@ -366,11 +379,9 @@ class Batch:
         return s.as_dict()
 
     def set_launch_shape(self, **fields) -> None:
-        s = _abi.LaunchShape()
-        check(lib().lp_batch_get_launch_shape(self._h, C.byref(s)))
-        for k, v in fields.items():
-            setattr(s, k, int(v))
-        check(lib().lp_batch_set_launch_shape(self._h, C.byref(s)))
+        """`Simulation.set_launch_shape` for the whole batch."""
+        check(lib().lp_batch_set_launch_shape(self._h, C.byref(_shape_with(
+            lambda s: check(lib().lp_batch_get_launch_shape(self._h, C.byref(s))), fields))))
 
     def kernel_times(self, steps: int) -> dict:
         """Mean per-kernel duration (ms) over `steps` attempts of the whole batch."""

@@ -90,6 +90,12 @@ def test_launch_shape_round_trip_and_refusal():
     s = sim.launch_shape()
     assert (s["g2p_small"], s["p2g_variant"], s["dynamic_tiles"], s["graph_attempts"]) == (1, 1, 0, 4)
     assert s["g2p_per_sm"] >= 1 and s["p2g_per_sm"] >= 1
+    # a new block shape without its CTAs per SM takes as many as fit it (4 of 128 threads on a B200)
+    wide = Simulation(configs.slump(16, (4, 4, 8), seed=1))
+    base = wide.launch_shape()["g2p_per_sm"]
+    wide.set_launch_shape(g2p_small=1)
+    assert wide.launch_shape()["g2p_per_sm"] >= 2 * base
+    wide.close()
     with pytest.raises(_lib.LPError):
         sim.set_launch_shape(g2p_small=2)
     sim.close()
