@@ -332,7 +332,8 @@ lp_status lp_batch_instance_state(lp_batch* b, int32_t index, int32_t* state, ch
 /* Launch shape of the persistent tile kernels (bin sort, P2G, G2P) and of the attempt loop.  No
  * counterpart in the reference (its loops run on rayon's pool).  Every shape gives the same
  * results; only the speed differs.
- *   g2p_small      1: G2P CTAs of 128 threads, 0: 256 threads
+ *   g2p_variant    G2P CTAs of 0: 256 threads (2 per SM), 1-3: 128 threads with registers sized
+ *                  for 4, 5 or 6 CTAs per SM (more resident warps against some spilled registers)
  *   g2p_per_sm     persistent G2P CTAs per SM (0, or more than fit: as many as fit)
  *   p2g_variant    P2G chunks of 0: 1024 particles, 1: 512 particles, 2: 512 particles whose state
  *                  is copied into shared memory (cp.async) one chunk ahead, across tiles
@@ -341,7 +342,7 @@ lp_status lp_batch_instance_state(lp_batch* b, int32_t index, int32_t* state, ch
  *   graph_attempts attempts captured per CUDA graph replay of run_substeps (0 or 1: no graph)
  * The getter reports the CTAs per SM the launches use. */
 typedef struct lp_launch_shape {
-  int32_t g2p_small, g2p_per_sm, p2g_variant, p2g_per_sm, dynamic_tiles, graph_attempts;
+  int32_t g2p_variant, g2p_per_sm, p2g_variant, p2g_per_sm, dynamic_tiles, graph_attempts;
 } lp_launch_shape;
 lp_status lp_sim_set_launch_shape(lp_sim* sim, const lp_launch_shape* shape);
 lp_status lp_sim_get_launch_shape(lp_sim* sim, lp_launch_shape* out);

@@ -925,11 +925,11 @@ lp_status set_targets(Ensemble& E, double target, bool forced_reset);
 
 static lp_status set_launch_shape(Ensemble& E, const lp_launch_shape* in) {
   if (!in) return set_error(LP_INVALID, "null launch shape");
-  if (in->g2p_small < 0 || in->g2p_small > 1 || in->p2g_variant < 0 || in->p2g_variant > 2 || in->dynamic_tiles < 0 ||
+  if (in->g2p_variant < 0 || in->g2p_variant > 3 || in->p2g_variant < 0 || in->p2g_variant > 2 || in->dynamic_tiles < 0 ||
       in->dynamic_tiles > 1 || in->g2p_per_sm < 0 || in->p2g_per_sm < 0 || in->graph_attempts < 0)
     return set_error(LP_INVALID, "launch shape fields out of range");
   E.invalidate_graph();
-  E.A.shape.g2p_small = in->g2p_small;
+  E.A.shape.g2p_variant = in->g2p_variant;
   E.A.shape.g2p_per_sm = in->g2p_per_sm;
   E.A.shape.p2g_variant = in->p2g_variant;
   E.A.shape.p2g_per_sm = in->p2g_per_sm;
@@ -939,14 +939,14 @@ static lp_status set_launch_shape(Ensemble& E, const lp_launch_shape* in) {
 }
 static lp_status get_launch_shape(Ensemble& E, lp_launch_shape* out) {
   if (!out) return set_error(LP_INVALID, "null launch shape");
-  int lim[7];
+  int lim[lp::LAUNCH_LIMITS];
   lp::launch_shape_limits(lim);
   const lp::LaunchShape& L = E.A.shape;
-  out->g2p_small = L.g2p_small;
+  out->g2p_variant = L.g2p_variant;
   out->p2g_variant = L.p2g_variant;
   out->dynamic_tiles = L.dynamic;
   // the CTAs per SM the launches use: the request, at most the resident limit
-  const int g2p_lim = lim[L.g2p_small ? 4 : 3], p2g_lim = lim[L.p2g_variant == 2 ? 6 : (L.p2g_variant ? 2 : 1)];
+  const int g2p_lim = lim[5 + L.g2p_variant], p2g_lim = lim[2 + L.p2g_variant];
   out->g2p_per_sm = (L.g2p_per_sm > 0 && L.g2p_per_sm < g2p_lim) ? L.g2p_per_sm : g2p_lim;
   out->p2g_per_sm = (L.p2g_per_sm > 0 && L.p2g_per_sm < p2g_lim) ? L.p2g_per_sm : p2g_lim;
   out->graph_attempts = E.graph_steps > 1 ? E.graph_steps : 1;
@@ -955,8 +955,9 @@ static lp_status get_launch_shape(Ensemble& E, lp_launch_shape* out) {
 static std::string shape_text(const lp_launch_shape& s) {
   char b[192];
   std::snprintf(b, sizeof(b),
-                "g2p_threads=%d g2p_per_sm=%d p2g_chunk=%d%s p2g_per_sm=%d dynamic_tiles=%d graph_attempts=%d",
-                s.g2p_small ? 128 : 256, s.g2p_per_sm, s.p2g_variant ? 512 : 1024, s.p2g_variant == 2 ? "_staged" : "",
+                "g2p_threads=%d%s g2p_per_sm=%d p2g_chunk=%d%s p2g_per_sm=%d dynamic_tiles=%d graph_attempts=%d",
+                s.g2p_variant ? 128 : 256,
+                s.g2p_variant == 2 ? "_regs_for_5" : (s.g2p_variant == 3 ? "_regs_for_6" : ""), s.g2p_per_sm, s.p2g_variant ? 512 : 1024, s.p2g_variant == 2 ? "_staged" : "",
                 s.p2g_per_sm, s.dynamic_tiles, s.graph_attempts);
   return b;
 }
@@ -974,7 +975,7 @@ static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t
     lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
     if (st != LP_OK) return st;
   }
-  int lim[7];
+  int lim[lp::LAUNCH_LIMITS];
   lp::launch_shape_limits(lim);
   lp_launch_shape best;
   lp_status st = get_launch_shape(E, &best);
@@ -1015,7 +1016,7 @@ static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t
   };
   std::vector<Knob> knobs = {
       {{{0, 0}, {1, 0}}, 0},
-      {{{0, 0}, {0, 1}, {1, 0}, {1, std::max(1, lim[4] - 1)}}, 1},
+      {{{0, 0}, {0, 1}, {1, 0}, {1, std::max(1, lim[6] - 1)}, {2, 0}, {3, 0}}, 1},
       {{{0, 0}, {0, 1}, {1, 0}, {2, 0}}, 2},
       {{{1, 0}, {4, 0}, {16, 0}}, 3},
   };
@@ -1024,7 +1025,7 @@ static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t
     for (const auto& v : kb.values) {
       lp_launch_shape c = best;
       if (kb.which == 0) c.dynamic_tiles = v[0];
-      else if (kb.which == 1) c.g2p_small = v[0], c.g2p_per_sm = v[1];
+      else if (kb.which == 1) c.g2p_variant = v[0], c.g2p_per_sm = v[1];
       else if (kb.which == 2) c.p2g_variant = v[0], c.p2g_per_sm = v[1];
       else c.graph_attempts = v[0];
       if (std::memcmp(&c, &best, sizeof(c)) == 0) continue;  // measured already

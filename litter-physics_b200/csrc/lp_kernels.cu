@@ -2117,6 +2117,9 @@ enum {
 constexpr size_t g2p_smem(int nt) { return sizeof(float) * 2 * PF_SLOTS * nt; }
 // threads per CTA of the two G2P instantiations the launch shape chooses from
 constexpr int G2P_THREADS_SMALL = 128;
+// threads per CTA of G2P variant v: 0 256 threads (2 CTAs per SM), 1-3 128 threads with registers
+// sized for 4, 5 or 6 CTAs per SM (more resident warps, some registers spilled)
+constexpr int g2p_threads(int v) { return v == 0 ? G2P_THREADS : G2P_THREADS_SMALL; }
 
 template <int NT>
 __device__ __forceinline__ void g2p_prefetch(float* __restrict__ buf, const float* __restrict__ cur,
@@ -2421,8 +2424,8 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
 // walk the attempt's list of occupied tiles; the partial results are per tile, so they do not
 // depend on which CTA took which tile.  Both block shapes hold 16 warps per SM at the 128
 // registers a thread needs.
-template <bool WARM, int NT, bool CLOCKS = false>
-__global__ void __launch_bounds__(NT, 512 / NT)
+template <bool WARM, int NT, int MINB = 512 / NT, bool CLOCKS = false>
+__global__ void __launch_bounds__(NT, MINB)
     k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
           float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
           int64_t cap, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
@@ -2965,7 +2968,7 @@ static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1)
 // the defaults are the B200 figures) and the SM count.
 static int g_sms = 148, g_sort_per_sm = 16;
 static int g_p2g_per_sm[3] = {2, 2, 2};              // [p2g_variant]
-static int g_g2p_per_sm[2][2] = {{2, 2}, {4, 4}};   // [g2p_small][warm]
+static int g_g2p_per_sm[4][2] = {{2, 2}, {4, 4}, {5, 5}, {6, 6}};  // [g2p_variant][warm]
 
 // dynamic shared memory of each P2G variant: records / partials, plus the staged copies
 static size_t p2g_variant_smem(int v) {
@@ -2982,26 +2985,21 @@ void configure_kernels() {
                         (const void*)k_p2g<P2G_CHUNK_SMALL, true>};
   for (int v = 0; v < 3; ++v)
     cudaFuncSetAttribute(p2g[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_variant_smem(v));
-  cudaFuncSetAttribute(k_g2p<false, G2P_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)g2p_smem(G2P_THREADS));
-  cudaFuncSetAttribute(k_g2p<true, G2P_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)g2p_smem(G2P_THREADS));
-  cudaFuncSetAttribute(k_g2p<false, G2P_THREADS_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)g2p_smem(G2P_THREADS_SMALL));
-  cudaFuncSetAttribute(k_g2p<true, G2P_THREADS_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)g2p_smem(G2P_THREADS_SMALL));
+  const void* g2p[4][2] = {{(const void*)k_g2p<false, G2P_THREADS>, (const void*)k_g2p<true, G2P_THREADS>},
+                           {(const void*)k_g2p<false, G2P_THREADS_SMALL>, (const void*)k_g2p<true, G2P_THREADS_SMALL>},
+                           {(const void*)k_g2p<false, G2P_THREADS_SMALL, 5>, (const void*)k_g2p<true, G2P_THREADS_SMALL, 5>},
+                           {(const void*)k_g2p<false, G2P_THREADS_SMALL, 6>, (const void*)k_g2p<true, G2P_THREADS_SMALL, 6>}};
+  for (int v = 0; v < 4; ++v)
+    for (int w = 0; w < 2; ++w)
+      cudaFuncSetAttribute(g2p[v][w], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem(g2p_threads(v)));
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return;
   g_sms = sms;
   occupancy(&g_sort_per_sm, (const void*)k_bin_sort, TB, 0);
   for (int v = 0; v < 3; ++v) occupancy(&g_p2g_per_sm[v], p2g[v], P2G_THREADS, p2g_variant_smem(v));
-  occupancy(&g_g2p_per_sm[0][0], (const void*)k_g2p<false, G2P_THREADS>, G2P_THREADS, g2p_smem(G2P_THREADS));
-  occupancy(&g_g2p_per_sm[0][1], (const void*)k_g2p<true, G2P_THREADS>, G2P_THREADS, g2p_smem(G2P_THREADS));
-  occupancy(&g_g2p_per_sm[1][0], (const void*)k_g2p<false, G2P_THREADS_SMALL>, G2P_THREADS_SMALL,
-            g2p_smem(G2P_THREADS_SMALL));
-  occupancy(&g_g2p_per_sm[1][1], (const void*)k_g2p<true, G2P_THREADS_SMALL>, G2P_THREADS_SMALL,
-            g2p_smem(G2P_THREADS_SMALL));
+  for (int v = 0; v < 4; ++v)
+    for (int w = 0; w < 2; ++w) occupancy(&g_g2p_per_sm[v][w], g2p[v][w], g2p_threads(v), g2p_smem(g2p_threads(v)));
 }
 
 // persistent grid size: the requested CTAs per SM, at most the resident limit, times the SMs
@@ -3010,15 +3008,12 @@ static unsigned persistent_ctas(int requested, int limit) {
   return (unsigned)(per * g_sms);
 }
 
-int launch_shape_limits(int out[7]) {
+int launch_shape_limits(int out[LAUNCH_LIMITS]) {
   out[0] = g_sms;
-  out[1] = g_p2g_per_sm[0];
-  out[2] = g_p2g_per_sm[1];
-  out[3] = g_g2p_per_sm[0][1];
-  out[4] = g_g2p_per_sm[1][1];
-  out[5] = g_sort_per_sm;
-  out[6] = g_p2g_per_sm[2];
-  return 7;
+  out[1] = g_sort_per_sm;
+  for (int v = 0; v < 3; ++v) out[2 + v] = g_p2g_per_sm[v];
+  for (int v = 0; v < 4; ++v) out[5 + v] = g_g2p_per_sm[v][1];
+  return LAUNCH_LIMITS;
 }
 
 // the occupied-tile list, then P2G over it
@@ -3053,25 +3048,25 @@ static void launch_g2p(const DeviceArrays& A, bool warm, cudaStream_t s) {
   const LaunchShape& L = A.shape;
   uint32_t* cur = L.dynamic ? A.nw_count + 4 : nullptr;
   const float* tab = warm ? A.mlp_tab : nullptr;
-  const int small = L.g2p_small ? 1 : 0;
-  const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[small][warm ? 1 : 0]);
+  const int v = (L.g2p_variant >= 0 && L.g2p_variant <= 3) ? L.g2p_variant : 0;
+  const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[v][warm ? 1 : 0]);
 #define LP_G2P_ARGS                                                                                               \
   A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, tab, \
       A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count, cur, A.g2p_clk
+#define LP_G2P_LAUNCH(T, MB, CLK, N) \
+  (warm ? k_g2p<true, T, MB, CLK> : k_g2p<false, T, MB, CLK>)<<<N, T, g2p_smem(T), s>>>(LP_G2P_ARGS)
   if (A.g2p_clk) {  // measurement of the return's share of G2P warp time (256-thread CTAs)
-    constexpr int T = G2P_THREADS;
-    const unsigned n2 = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[0][warm ? 1 : 0]);
-    if (warm) k_g2p<true, T, true><<<n2, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
-    else k_g2p<false, T, true><<<n2, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
-  } else if (small) {
-    constexpr int T = G2P_THREADS_SMALL;
-    if (warm) k_g2p<true, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
-    else k_g2p<false, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
+    LP_G2P_LAUNCH(G2P_THREADS, 2, true, persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[0][warm ? 1 : 0]));
+  } else if (v == 3) {
+    LP_G2P_LAUNCH(G2P_THREADS_SMALL, 6, false, ctas);
+  } else if (v == 2) {
+    LP_G2P_LAUNCH(G2P_THREADS_SMALL, 5, false, ctas);
+  } else if (v == 1) {
+    LP_G2P_LAUNCH(G2P_THREADS_SMALL, 4, false, ctas);
   } else {
-    constexpr int T = G2P_THREADS;
-    if (warm) k_g2p<true, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
-    else k_g2p<false, T><<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS);
+    LP_G2P_LAUNCH(G2P_THREADS, 2, false, ctas);
   }
+#undef LP_G2P_LAUNCH
 #undef LP_G2P_ARGS
 }
 uint64_t kernel_launch_count() { return g_launches; }

@@ -13,7 +13,8 @@ constexpr int DIAG_N = 19;
 // Launch shape of the persistent tile kernels, chosen per ensemble (by default, or by the
 // autotuner on the live batch).  Per-SM counts of 0, or above what fits, mean as many as fit.
 struct LaunchShape {
-  int g2p_small = 0;   // 1: G2P CTAs of G2P_THREADS_SMALL (128) threads, 0: G2P_THREADS (256)
+  int g2p_variant = 0;  // G2P CTAs of 0: G2P_THREADS (256) threads, 1-3: G2P_THREADS_SMALL (128)
+                        // threads with registers sized for 4, 5 or 6 CTAs per SM
   int g2p_per_sm = 0;  // persistent G2P CTAs per SM
   int p2g_variant = 0;  // P2G chunks of 0: P2G_CHUNK (1024) particles, 1: P2G_CHUNK_SMALL (512),
                         // 2: P2G_CHUNK_SMALL with each chunk's particle state copied one chunk ahead
@@ -112,9 +113,10 @@ int launch_export(const HostParticleChunk& h, int64_t n, int64_t first, const fl
                   cudaStream_t s);
 uint64_t kernel_launch_count();
 void configure_kernels();              // one-time function attributes (dynamic shared memory)
-// out = SMs, resident CTAs per SM of P2G (1024- and 512-particle chunks), of the warm G2P (256-
-// and 128-thread CTAs), of the bin sort and of the staged 512-particle P2G; returns 7
-int launch_shape_limits(int out[7]);
+// out = SMs, resident CTAs per SM of the bin sort, of P2G variants 0-2 and of the warm G2P
+// variants 0-3; returns LAUNCH_LIMITS
+constexpr int LAUNCH_LIMITS = 9;
+int launch_shape_limits(int out[LAUNCH_LIMITS]);
 void set_last_error(const char* msg);  // message returned by lp_last_error()
 void add_kernel_launches(uint64_t n);
 

@@ -225,7 +225,7 @@ class LaunchShape(C.Structure):
     counterpart)."""
 
     _fields_ = [
-        ("g2p_small", C.c_int32),
+        ("g2p_variant", C.c_int32),
         ("g2p_per_sm", C.c_int32),
         ("p2g_variant", C.c_int32),
         ("p2g_per_sm", C.c_int32),

@@ -25,7 +25,7 @@ def _shape_with(read, fields: dict) -> _abi.LaunchShape:
     (as many as fit that instantiation) instead of the count that fitted the previous one."""
     s = _abi.LaunchShape()
     read(s)
-    if "g2p_small" in fields and "g2p_per_sm" not in fields and int(fields["g2p_small"]) != s.g2p_small:
+    if "g2p_variant" in fields and "g2p_per_sm" not in fields and int(fields["g2p_variant"]) != s.g2p_variant:
         s.g2p_per_sm = 0
     if "p2g_variant" in fields and "p2g_per_sm" not in fields and int(fields["p2g_variant"]) != s.p2g_variant:
         s.p2g_per_sm = 0
@@ -115,7 +115,7 @@ class Simulation:
         return out.value
 
     def set_launch_shape(self, **fields) -> None:
-        """Set fields of `lp_launch_shape` (g2p_small, g2p_per_sm, p2g_variant, p2g_per_sm,
+        """Set fields of `lp_launch_shape` (g2p_variant, g2p_per_sm, p2g_variant, p2g_per_sm,
         dynamic_tiles, graph_attempts); the others keep their values, except that a new G2P
         block shape or P2G variant given without its CTAs per SM gets as many as fit."""
         check(lib().lp_sim_set_launch_shape(self._h, C.byref(_shape_with(

@@ -15,8 +15,10 @@ pytestmark = pytest.mark.gpu
 SHAPES = [
     {},  # default: 256-thread G2P, 1024-particle P2G chunks, as many CTAs as fit, dynamic tiles
     {"dynamic_tiles": 0},
-    {"g2p_small": 1},
-    {"g2p_small": 1, "g2p_per_sm": 3},
+    {"g2p_variant": 1},
+    {"g2p_variant": 1, "g2p_per_sm": 3},
+    {"g2p_variant": 2},
+    {"g2p_variant": 3},
     {"p2g_variant": 1},
     {"p2g_variant": 2},
     {"p2g_variant": 2, "dynamic_tiles": 0},
@@ -74,7 +76,7 @@ def test_every_launch_shape_gives_identical_results():
             got = run(batch, shape, 24)
             for (state, plastic), (ref_state, ref_plastic) in zip(got, ref, strict=True):
                 assert state == ref_state, shape
-                if shape.get("g2p_small"):
+                if shape.get("g2p_variant"):
                     assert abs(plastic - ref_plastic) <= 1e-13 * abs(ref_plastic), shape
                 else:
                     assert plastic == ref_plastic, shape
@@ -86,18 +88,18 @@ def test_launch_shape_round_trip_and_refusal():
 
     _lib.build()
     sim = Simulation(configs.slump(16, (4, 4, 8), seed=1))
-    sim.set_launch_shape(g2p_small=1, p2g_variant=1, dynamic_tiles=0, graph_attempts=4)
+    sim.set_launch_shape(g2p_variant=1, p2g_variant=1, dynamic_tiles=0, graph_attempts=4)
     s = sim.launch_shape()
-    assert (s["g2p_small"], s["p2g_variant"], s["dynamic_tiles"], s["graph_attempts"]) == (1, 1, 0, 4)
+    assert (s["g2p_variant"], s["p2g_variant"], s["dynamic_tiles"], s["graph_attempts"]) == (1, 1, 0, 4)
     assert s["g2p_per_sm"] >= 1 and s["p2g_per_sm"] >= 1
     # a new block shape without its CTAs per SM takes as many as fit it (4 of 128 threads on a B200)
     wide = Simulation(configs.slump(16, (4, 4, 8), seed=1))
     base = wide.launch_shape()["g2p_per_sm"]
-    wide.set_launch_shape(g2p_small=1)
+    wide.set_launch_shape(g2p_variant=1)
     assert wide.launch_shape()["g2p_per_sm"] >= 2 * base
     wide.close()
     with pytest.raises(_lib.LPError):
-        sim.set_launch_shape(g2p_small=2)
+        sim.set_launch_shape(g2p_variant=4)
     sim.close()
 
 
