@@ -331,9 +331,18 @@ __device__ inline int hb_return_d(double trial, double ys, const HbConst& h, dou
   double lo = 0.0, hi = span;
   double x = (sigma0 > ys && sigma0 < trial) ? sigma0 - ys : 0.5 * span;
   const double tolerance = tol_rel * fmax(trial, 1.0);
-  double pw = x > 0.0 ? exp(exponent * (log(x) - log_k)) : 0.0;
-  double last = x - span + viscous_scale * pw;
-  for (int it = 1; it <= 200; ++it) {
+  double pw = 0.0;
+  bool full = true;  // the power at x needs the logarithm and the exponential
+  // Pass `it` evaluates the residual of the iterate that pass it - 1 chose (pass 1: the start),
+  // so the FP64 logarithm and exponential have one call site and the kernels' code stays small.
+  for (int it = 1; it <= 201; ++it) {
+    if (full) pw = x > 0.0 ? exp(exponent * (log(x) - log_k)) : 0.0;
+    const double last = x - span + viscous_scale * pw;
+    if (it > 1 && !isfinite(last)) {
+      *iters = it - 1;
+      return F_CONST_NONFINITE;
+    }
+    if (it == 201) break;
     if (fabs(last) <= tolerance || (hi - lo) <= tolerance) {
       const double sigma = ys + x;
       *sigma_out = sigma;
@@ -347,16 +356,12 @@ __device__ inline int hb_return_d(double trial, double ys, const HbConst& h, dou
     const double q = x > 0.0 ? last / (x + c1 * pw) : 0.0;
     const double xn = fma(-q, x, x);
     if (x > 0.0 && isfinite(xn) && xn > lo && xn < hi) {
-      pw = fabs(q) <= small_q ? pw * pow_one_minus_small(q, exponent) : exp(exponent * (log(xn) - log_k));
+      full = fabs(q) > small_q;
+      if (!full) pw *= pow_one_minus_small(q, exponent);
       x = xn;
     } else {
       x = 0.5 * (lo + hi);
-      pw = x > 0.0 ? exp(exponent * (log(x) - log_k)) : 0.0;
-    }
-    last = x - span + viscous_scale * pw;
-    if (!isfinite(last)) {
-      *iters = it;
-      return F_CONST_NONFINITE;
+      full = true;
     }
   }
   *iters = 200;
