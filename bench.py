@@ -431,7 +431,7 @@ def ours(args, ws, rank, local):
 
     tune_report = None
     if args.launch_shape:
-        # a fixed launch shape (profiling): "g2p_small=1,p2g_variant=0,..."
+        # a fixed launch shape (profiling): "g2p_variant=1,p2g_variant=0,..."
         sim.set_launch_shape(**{k: int(v) for k, v in (kv.split("=") for kv in args.launch_shape.split(","))})
     elif not args.no_autotune:
         # the launch shape for the headline (warm-started) arm, picked on the developed column;
@@ -620,7 +620,7 @@ def main():
     ap.add_argument("--develop", type=int, default=150)
     ap.add_argument("--graph", type=int, default=0, help="attempts per CUDA graph before tuning")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
-    ap.add_argument("--launch-shape", default="", help="fixed launch shape of the headline arm, e.g. g2p_small=1")
+    ap.add_argument("--launch-shape", default="", help="fixed launch shape of the headline arm, e.g. g2p_variant=1")
     ap.add_argument("--log-steps", type=int, default=300)
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--kernel-steps", type=int, default=5)
