@@ -787,7 +787,7 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   ALLOC(A.nw_list, A.cap);
   ALLOC(A.nw_count, 5);
   A.tile_count = A.nw_count + 1;
-  ALLOC(A.tile_list, A.n_tiles);
+  ALLOC(A.tile_rec, A.n_tiles);
   ALLOC(A.acc, 4 * A.node_total);
   ALLOC(A.trac, 6 * A.node_total);
   ALLOC(A.blk_epoch, A.n_blk);
@@ -925,7 +925,7 @@ lp_status set_targets(Ensemble& E, double target, bool forced_reset);
 
 static lp_status set_launch_shape(Ensemble& E, const lp_launch_shape* in) {
   if (!in) return set_error(LP_INVALID, "null launch shape");
-  if (in->g2p_variant < 0 || in->g2p_variant > 3 || in->p2g_variant < 0 || in->p2g_variant > 2 || in->dynamic_tiles < 0 ||
+  if (in->g2p_variant < 0 || in->g2p_variant >= lp::G2P_VARIANTS || in->p2g_variant < 0 || in->p2g_variant >= lp::P2G_VARIANTS || in->dynamic_tiles < 0 ||
       in->dynamic_tiles > 1 || in->g2p_per_sm < 0 || in->p2g_per_sm < 0 || in->graph_attempts < 0)
     return set_error(LP_INVALID, "launch shape fields out of range");
   E.invalidate_graph();
@@ -946,7 +946,7 @@ static lp_status get_launch_shape(Ensemble& E, lp_launch_shape* out) {
   out->p2g_variant = L.p2g_variant;
   out->dynamic_tiles = L.dynamic;
   // the CTAs per SM the launches use: the request, at most the resident limit
-  const int g2p_lim = lim[5 + L.g2p_variant], p2g_lim = lim[2 + L.p2g_variant];
+  const int g2p_lim = lim[lp::LIM_G2P + L.g2p_variant], p2g_lim = lim[lp::LIM_P2G + L.p2g_variant];
   out->g2p_per_sm = (L.g2p_per_sm > 0 && L.g2p_per_sm < g2p_lim) ? L.g2p_per_sm : g2p_lim;
   out->p2g_per_sm = (L.p2g_per_sm > 0 && L.p2g_per_sm < p2g_lim) ? L.p2g_per_sm : p2g_lim;
   out->graph_attempts = E.graph_steps > 1 ? E.graph_steps : 1;
@@ -954,10 +954,12 @@ static lp_status get_launch_shape(Ensemble& E, lp_launch_shape* out) {
 }
 static std::string shape_text(const lp_launch_shape& s) {
   char b[192];
+  static const char* const g2p_names[4] = {"256", "128", "128_regs_for_5", "128_regs_for_6"};
+  const int gv = s.g2p_variant >= 0 && s.g2p_variant < 4 ? s.g2p_variant : 0;
   std::snprintf(b, sizeof(b),
-                "g2p_threads=%d%s g2p_per_sm=%d p2g_chunk=%d%s p2g_per_sm=%d dynamic_tiles=%d graph_attempts=%d",
-                s.g2p_variant ? 128 : 256,
-                s.g2p_variant == 2 ? "_regs_for_5" : (s.g2p_variant == 3 ? "_regs_for_6" : ""), s.g2p_per_sm, s.p2g_variant ? 512 : 1024, s.p2g_variant == 2 ? "_staged" : "",
+                "g2p_threads=%s g2p_per_sm=%d p2g_chunk=%d%s p2g_per_sm=%d dynamic_tiles=%d graph_attempts=%d",
+                g2p_names[gv], s.g2p_per_sm, (s.p2g_variant == 1 || s.p2g_variant == 2) ? 512 : 1024,
+                s.p2g_variant == 2 ? "_staged" : "",
                 s.p2g_per_sm, s.dynamic_tiles, s.graph_attempts);
   return b;
 }
@@ -966,9 +968,12 @@ static std::string shape_text(const lp_launch_shape& s) {
 // scheduling, G2P block shape and CTAs per SM, P2G chunk and CTAs per SM, attempts per graph
 // replay), each candidate timed over trial_steps attempts with CUDA events after two untimed
 // ones, keeping the fastest value before moving to the next knob.  The attempts are real steps:
-// time advances and every accepted step is a valid step of the trajectory.  Every candidate
-// gives the same results (the tile kernels' results do not depend on these choices), so only
-// the speed differs.
+// time advances and every accepted step is a valid step of the trajectory, so the work per
+// attempt drifts while the search runs (a collapsing column yields more from step to step).
+// Each candidate is therefore compared with the incumbent timed right before and right after it
+// (the mean of the two), which cancels a drift that is linear over the three timings.  Every
+// candidate gives the same results (the tile kernels' results do not depend on these choices),
+// so only the speed differs.
 static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t report_len) {
   if (trial_steps < 1) return set_error(LP_INVALID, "trial_steps must be at least 1");
   if (E.ctrl_h.empty() || !std::isinf(E.ctrl_h[0].target)) {
@@ -1004,11 +1009,11 @@ static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t
     float ms = 0.f;
     CUDA_CK(cudaEventElapsedTime(&ms, e0, e1));
     *ms_per_attempt = ms / (float)(reps * per);
-    rep += shape_text(s) + " ms_per_attempt=" + std::to_string(*ms_per_attempt) + "\n";
     return LP_OK;
   };
-  float best_ms = 0.f;
+  float best_ms = 0.f;  // the incumbent's latest timing
   st = measure(best, &best_ms);
+  if (st == LP_OK) rep += shape_text(best) + " ms_per_attempt=" + std::to_string(best_ms) + "\n";
   // one knob at a time; each candidate list holds complete field values for that knob
   struct Knob {
     std::vector<std::array<int, 2>> values;  // (small / dynamic / graph, per-SM) pairs
@@ -1016,7 +1021,7 @@ static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t
   };
   std::vector<Knob> knobs = {
       {{{0, 0}, {1, 0}}, 0},
-      {{{0, 0}, {0, 1}, {1, 0}, {1, std::max(1, lim[6] - 1)}, {2, 0}, {3, 0}}, 1},
+      {{{0, 0}, {0, 1}, {1, 0}, {1, std::max(1, lim[lp::LIM_G2P + 1] - 1)}, {2, 0}, {3, 0}}, 1},
       {{{0, 0}, {0, 1}, {1, 0}, {2, 0}}, 2},
       {{{1, 0}, {4, 0}, {16, 0}}, 3},
   };
@@ -1029,12 +1034,18 @@ static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t
       else if (kb.which == 2) c.p2g_variant = v[0], c.p2g_per_sm = v[1];
       else c.graph_attempts = v[0];
       if (std::memcmp(&c, &best, sizeof(c)) == 0) continue;  // measured already
-      float ms = 0.f;
+      float ms = 0.f, after = 0.f;
       st = measure(c, &ms);
+      if (st == LP_OK) st = measure(best, &after);
       if (st != LP_OK) break;
-      if (ms < best_ms) {
-        best_ms = ms;
+      const float ref = 0.5f * (best_ms + after);  // the incumbent at the candidate's time
+      rep += shape_text(c) + " ms_per_attempt=" + std::to_string(ms) + " incumbent=" + std::to_string(ref) + "\n";
+      if (ms < ref) {
         best = c;
+        st = measure(best, &best_ms);  // the new incumbent, timed next to the following candidate
+        if (st != LP_OK) break;
+      } else {
+        best_ms = after;
       }
     }
   }

@@ -241,20 +241,33 @@ __device__ int block_sum_argmax_ll(long long (&v)[K], long long value, int index
 }
 
 // Per-particle bound of the node momentum one particle can deposit (mass times speed, affine and
-// stress terms over the stencil, one gravity kick), in FP64 from the FP32 state, so that no
-// magnitude a finite FP32 state holds overflows it.  k_g2p and k_state_stats evaluate these
-// same expressions, so an imported state gets the bound of the run that wrote it.
+// stress terms over the stencil, one gravity kick).  The norms are taken in FP32 and, where a
+// square overflows FP32, again in FP64, so that no magnitude a finite FP32 state holds overflows
+// the bound; the sum is FP64.  k_g2p and k_state_stats evaluate these same expressions, so an
+// imported state gets the bound of the run that wrote it.
 __device__ __forceinline__ float affine_norm(const float Cm[9]) {
-  double c2 = 0.0;
+  float c2 = 0.f;
 #pragma unroll
-  for (int a = 0; a < 9; ++a) c2 += (double)Cm[a] * Cm[a];
-  return (float)sqrt(c2);
+  for (int a = 0; a < 9; ++a) c2 = fmaf(Cm[a], Cm[a], c2);
+  if (isfinite(c2)) return sqrtf(c2);
+  double d2 = 0.0;
+#pragma unroll
+  for (int a = 0; a < 9; ++a) d2 += (double)Cm[a] * Cm[a];
+  return (float)sqrt(d2);
 }
 __device__ __forceinline__ double momentum_bound(float m, float speed, float cn, const float tau[6], float v0,
                                                  float c_tau, float c_dx, float c_g) {
-  const double t2 = (double)tau[0] * tau[0] + (double)tau[1] * tau[1] + (double)tau[2] * tau[2] +
-                    2.0 * ((double)tau[3] * tau[3] + (double)tau[4] * tau[4] + (double)tau[5] * tau[5]);
-  return (double)m * speed + ((double)m * cn + sqrt(t2) * c_tau * v0) * c_dx + (double)m * c_g;
+  const float f2 = tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2] +
+                   2.f * (tau[3] * tau[3] + tau[4] * tau[4] + tau[5] * tau[5]);
+  double tn;
+  if (isfinite(f2)) {
+    tn = (double)sqrtf(f2);
+  } else {
+    const double t2 = (double)tau[0] * tau[0] + (double)tau[1] * tau[1] + (double)tau[2] * tau[2] +
+                      2.0 * ((double)tau[3] * tau[3] + (double)tau[4] * tau[4] + (double)tau[5] * tau[5]);
+    tn = sqrt(t2);
+  }
+  return (double)m * speed + ((double)m * cn + tn * c_tau * v0) * c_dx + (double)m * c_g;
 }
 
 // Tile loop of a persistent CTA over the entries of the attempt's occupied-tile list:
@@ -616,15 +629,15 @@ __device__ __forceinline__ void bin_sort_small(uint32_t* __restrict__ p, int n) 
 // binned order deterministic after the atomic scatter.  The committed state is itself in binned
 // order, so a particle keeps its place relative to the others of its bin from step to step.
 // Persistent CTAs of TB threads walk the occupied-tile list, one thread per bin.
-__global__ void __launch_bounds__(TB) k_bin_sort(const InstDesc* __restrict__ desc, const int* __restrict__ tile_inst,
-                                                 const uint32_t* __restrict__ start, uint32_t* __restrict__ perm,
-                                                 const uint32_t* __restrict__ tile_list,
+__global__ void __launch_bounds__(TB) k_bin_sort(const InstDesc* __restrict__ desc, const uint32_t* __restrict__ start,
+                                                 uint32_t* __restrict__ perm, const uint4* __restrict__ tile_rec,
                                                  const uint32_t* __restrict__ tile_count, uint32_t* cursor) {
   __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
   for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
-    const int tile = (int)tile_list[i];
-    const InstDesc& D = desc[tile_inst[tile]];
+    const uint4 rec = tile_rec[i];
+    const int tile = (int)rec.x;
+    const InstDesc& D = desc[rec.y];
     // a tile's keys are followed by at least the instance's outflow key, so key + 1 is valid
     const int64_t key = D.key_off + (int64_t)(tile - D.tile_off) * TB + threadIdx.x;
     const uint32_t s = start[key], e = start[key + 1];
@@ -649,21 +662,27 @@ __global__ void __launch_bounds__(TB) k_bin_sort(const InstDesc* __restrict__ de
   }
 }
 
-// The attempt's occupied tiles of the active instances, for the persistent P2G and G2P CTAs (the
-// list order does not matter: their results are per tile).  Empty tiles get zero G2P partials.
+// The attempt's occupied tiles of the active instances, for the persistent bin-sort, P2G and G2P
+// CTAs (the list order does not matter: their results are per tile).  Each entry is the record
+// (tile, instance, first sorted slot, end slot), so that a CTA learns what it needs of a tile from
+// one load.  Empty tiles get zero G2P partials.
 __global__ void k_tiles(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
                         const int* __restrict__ tile_inst, int64_t n_tiles, const uint32_t* __restrict__ start,
-                        uint32_t* __restrict__ tile_list, uint32_t* __restrict__ tile_count,
+                        uint4* __restrict__ tile_rec, uint32_t* __restrict__ tile_count,
                         ParticlePartial* __restrict__ tpart) {
   const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool busy = false;
+  int inst = 0;
+  uint32_t ts = 0, te = 0;
   if (tile < n_tiles) {
-    const int inst = tile_inst[tile];
+    inst = tile_inst[tile];
     const Control& c = ctrl[inst];
     if (c.active) {
       const InstDesc& D = desc[inst];
       const int64_t key0 = D.key_off + (tile - D.tile_off) * TB;
-      busy = start[key0 + TB] > start[key0];
+      ts = start[key0];
+      te = start[key0 + TB];
+      busy = te > ts;
       if (!busy) {
         ParticlePartial& P = tpart[tile];
         P.diss = P.bbound = P.mass = 0.0;
@@ -679,7 +698,7 @@ __global__ void k_tiles(const InstDesc* __restrict__ desc, const Control* __rest
   uint32_t base = 0u;
   if (lane == 0 && bal) base = atomicAdd(tile_count, (uint32_t)__popc(bal));
   base = __shfl_sync(0xffffffffu, base, 0);
-  if (busy) tile_list[base + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)tile;
+  if (busy) tile_rec[base + __popc(bal & ((1u << lane) - 1u))] = make_uint4((uint32_t)tile, (uint32_t)inst, ts, te);
 }
 
 // ============================================================== P2G
@@ -727,6 +746,52 @@ __device__ __forceinline__ int p2g_raw_comp(int r) {
 }
 __host__ __device__ constexpr size_t p2g_raw_bytes(int chunk) { return sizeof(float) * P2G_RAW * chunk; }
 
+// APIC record of one particle, the quantities the per-bin pass scatters: momentum q = m v, the
+// affine matrix A = C m - tau sv (sv = dt 4/dx^2 V0) and the position f relative to the stencil
+// base (floor(x/dx - 0.5)).  Every rounding is explicit, so the variants that build the record in
+// different places scatter bit-identical values.
+__device__ __forceinline__ void p2g_record(const float v[3], const float Cm[9], const float tau[6], float m, float sv,
+                                           float q[3], float A[9]) {
+  const float T[9] = {tau[0], tau[3], tau[4], tau[3], tau[1], tau[5], tau[4], tau[5], tau[2]};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) q[a] = __fmul_rn(v[a], m);
+#pragma unroll
+  for (int a = 0; a < 9; ++a) A[a] = __fmaf_rn(Cm[a], m, -__fmul_rn(T[a], sv));
+}
+__device__ __forceinline__ float p2g_frac(float x, float dx, float pow2_inv_dx) {
+  const float sc = scaled_of(x, dx, pow2_inv_dx);
+  return __fsub_rn(sc, floorf(__fsub_rn(sc, 0.5f)));
+}
+// Scatter of one record by the thread of slab `slab` (x offset) of its bin: the 9 nodes
+// (slab, b, c) x (mass, momentum), accumulated in acc9[b][c].
+__device__ __forceinline__ void p2g_scatter(float m, const float q[3], const float A[9], float fx, float fy, float fz,
+                                            int slab, float dx, float (&acc9)[3][3][4]) {
+  float w[3][3], d[3][3];
+  weights_of(fy, dx, w[1], d[1]);
+  weights_of(fz, dx, w[2], d[2]);
+  // x weight of this thread's slab only (the expressions of weights_of for offset `slab`)
+  const float ao = slab == 0 ? 1.5f - fx : (slab == 1 ? fx - 1.0f : fx - 0.5f);
+  const float wa = slab == 1 ? 0.75f - ao * ao : 0.5f * (ao * ao);
+  const float da = (fx - (float)slab) * -dx;
+  float u[3];
+#pragma unroll
+  for (int rr = 0; rr < 3; ++rr) u[rr] = q[rr] + A[3 * rr + 0] * da;
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const float wab = wa * w[1][b];
+    float ub[3];
+#pragma unroll
+    for (int rr = 0; rr < 3; ++rr) ub[rr] = u[rr] + A[3 * rr + 1] * d[1][b];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      const float ww = wab * w[2][cc];
+      acc9[b][cc][0] += ww * m;
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr) acc9[b][cc][1 + rr] += ww * (ub[rr] + A[3 * rr + 2] * d[2][cc]);
+    }
+  }
+}
+
 // Staged P2G: asynchronous copies (cp.async, 4 bytes each) of the state components of chunk
 // [c0, c0 + cn) of a tile into raw[P2G_RAW][CHUNK], particle i of the chunk copied by thread
 // i % P2G_THREADS, which is the thread that reads it back in phase 1.  The caller commits.
@@ -744,32 +809,28 @@ __device__ __forceinline__ void p2g_stage(float* __restrict__ raw, const float* 
     }
   }
 }
-// the first chunk of occupied tile `tile` (an entry of the attempt's tile list)
+// the first chunk of the occupied tile of tile-list record `rec`
 template <int CHUNK>
-__device__ __forceinline__ void p2g_stage_tile(float* __restrict__ raw, int tile, const InstDesc* __restrict__ desc,
-                                               const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
-                                               const float* __restrict__ st0, const float* __restrict__ st1,
-                                               int64_t cap, const uint32_t* __restrict__ start,
+__device__ __forceinline__ void p2g_stage_tile(float* __restrict__ raw, const uint4 rec,
+                                               const Control* __restrict__ ctrl, const float* __restrict__ st0,
+                                               const float* __restrict__ st1, int64_t cap,
                                                const uint32_t* __restrict__ perm) {
-  const int inst = tile_inst[tile];
-  const InstDesc& D = desc[inst];
-  const int64_t key0 = D.key_off + (int64_t)(tile - D.tile_off) * TB;
-  const uint32_t ts = start[key0], te = start[key0 + TB];
-  p2g_stage<CHUNK>(raw, ctrl[inst].parity ? st1 : st0, perm, cap, ts, min((uint32_t)CHUNK, te - ts));
+  p2g_stage<CHUNK>(raw, ctrl[rec.y].parity ? st1 : st0, perm, cap, rec.z, min((uint32_t)CHUNK, rec.w - rec.z));
 }
 
 // one tile of k_p2g, chunks of CHUNK particles.  STAGED: the particle state of each chunk
 // arrives by the asynchronous copies of p2g_stage, issued one chunk ahead: the tile's first
 // chunk by the caller (or the previous tile), each later chunk, and after the last one the
-// first chunk of next_tile (-1: none), right after the thread has read its copies of the
-// current chunk, so that the copies fly while the CTA scatters.
+// first chunk of the next tile (next: its tile-list record, or null), right after the thread has
+// read its copies of the current chunk, so that the copies fly while the CTA scatters.
 template <int CHUNK, bool STAGED>
-__device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restrict__ desc,
-                                         const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
-                                         const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
+__device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __restrict__ desc,
+                                         const Control* __restrict__ ctrl, const float* __restrict__ st0,
+                                         const float* __restrict__ st1, int64_t cap,
                                          const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
                                          long long* __restrict__ acc, int64_t node_total,
-                                         uint32_t* __restrict__ blk_epoch, int transport_only, int next_tile) {
+                                         uint32_t* __restrict__ blk_epoch, int transport_only,
+                                         const uint4* __restrict__ next) {
   constexpr int P2G_PER_THREAD = (CHUNK + P2G_THREADS - 1) / P2G_THREADS;  // phase-1 particles per thread
   static_assert(CHUNK % 32 == 0, "record rows rotate within 32-word segments");
   extern __shared__ float4 part[];  // particle records during the chunks, then TB * 27 partial node sums
@@ -779,16 +840,16 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
   __shared__ int redi[P2G_THREADS / 32 + 1];
 
-  const int inst = tile_inst[tile];
+  const int tile = (int)trec.x, inst = (int)trec.y;
   const Control& c = ctrl[inst];
   const InstDesc& D = desc[inst];
   const int64_t ltile = tile - D.tile_off;
   const int64_t key0 = D.key_off + ltile * TB;
-  const uint32_t ts = start[key0], te = start[key0 + TB];
+  const uint32_t ts = trec.z, te = trec.w;
   if (!c.active || ts == te) {  // inactive instance or empty tile (uniform across the CTA)
     if constexpr (STAGED) {      // the tile list holds neither, but keep the staging chain whole
       cp_async_wait<0>();        // this tile's copies land before the next tile's reuse the buffer
-      if (next_tile >= 0) p2g_stage_tile<CHUNK>(raw, next_tile, desc, ctrl, tile_inst, st0, st1, cap, start, perm);
+      if (next) p2g_stage_tile<CHUNK>(raw, *next, ctrl, st0, st1, cap, perm);
       cp_async_commit();
     }
     return;
@@ -861,21 +922,16 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
         m = cur[C_M * cap + src];
         v0 = cur[C_V0 * cap + src];
       }
-      // A = C m - tau (dt 4/dx^2 V0)
-      const float sv = stress_scale * v0;
-      const float T[9] = {tau[0], tau[3], tau[4], tau[3], tau[1], tau[5], tau[4], tau[5], tau[2]};
+      float qv[3], A[9];
+      p2g_record(v, Cm, tau, m, stress_scale * v0, qv, A);
       float* r = rec + rec_slot(i);
       r[0] = m;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) r[(1 + a) * CHUNK] = v[a] * m;
+      for (int a = 0; a < 3; ++a) r[(1 + a) * CHUNK] = qv[a];
 #pragma unroll
-      for (int a = 0; a < 9; ++a) r[(4 + a) * CHUNK] = Cm[a] * m - T[a] * sv;
-      // position relative to the particle's stencil base (its bin's base: floor(x/dx - 0.5))
+      for (int a = 0; a < 9; ++a) r[(4 + a) * CHUNK] = A[a];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float sc = scaled_of(x[a], dx, D.pow2_inv_dx);
-        r[(13 + a) * CHUNK] = sc - floorf(sc - 0.5f);
-      }
+      for (int a = 0; a < 3; ++a) r[(13 + a) * CHUNK] = p2g_frac(x[a], dx, D.pow2_inv_dx);
       // exact per-particle totals: FP64 products of the stored FP32 mass and velocity
       tot[0] += to_fixed((double)m, s_m);
       tot[1] += to_fixed((double)m * (double)v[0], s_p);
@@ -885,8 +941,8 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
     if constexpr (STAGED) {
       // this thread has read its copies: the next chunk (of this tile or of the next) may land
       if (c0 + CHUNK < te) p2g_stage<CHUNK>(raw, cur, perm, cap, c0 + CHUNK, min((uint32_t)CHUNK, te - c0 - CHUNK));
-      else if (next_tile >= 0)
-        p2g_stage_tile<CHUNK>(raw, next_tile, desc, ctrl, tile_inst, st0, st1, cap, start, perm);
+      else if (next)
+        p2g_stage_tile<CHUNK>(raw, *next, ctrl, st0, st1, cap, perm);
       cp_async_commit();
     }
     __syncthreads();
@@ -894,36 +950,11 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
     const uint32_t j0 = max(s, c0), j1 = min(e, c0 + cn);
     for (uint32_t j = j0; j < j1; ++j) {
       const float* r = rec + rec_slot(j - c0);
-      const float m = r[0];
       const float q[3] = {r[CHUNK], r[2 * CHUNK], r[3 * CHUNK]};
       float A[9];
 #pragma unroll
       for (int a = 0; a < 9; ++a) A[a] = r[(4 + a) * CHUNK];
-      float w[3][3], d[3][3];
-#pragma unroll
-      for (int a = 1; a < 3; ++a) weights_of(r[(13 + a) * CHUNK], dx, w[a], d[a]);
-      // x weight of this thread's slab only (the expressions of weights_of for offset `slab`)
-      const float fx = r[13 * CHUNK];
-      const float ao = slab == 0 ? 1.5f - fx : (slab == 1 ? fx - 1.0f : fx - 0.5f);
-      const float wa = slab == 1 ? 0.75f - ao * ao : 0.5f * (ao * ao);
-      const float da = (fx - (float)slab) * -dx;
-      float u[3];
-#pragma unroll
-      for (int rr = 0; rr < 3; ++rr) u[rr] = q[rr] + A[3 * rr + 0] * da;
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        const float wab = wa * w[1][b];
-        float ub[3];
-#pragma unroll
-        for (int rr = 0; rr < 3; ++rr) ub[rr] = u[rr] + A[3 * rr + 1] * d[1][b];
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          const float ww = wab * w[2][cc];
-          acc9[b][cc][0] += ww * m;
-#pragma unroll
-          for (int rr = 0; rr < 3; ++rr) acc9[b][cc][1 + rr] += ww * (ub[rr] + A[3 * rr + 2] * d[2][cc]);
-        }
-      }
+      p2g_scatter(r[0], q, A, r[13 * CHUNK], r[14 * CHUNK], r[15 * CHUNK], slab, dx, acc9);
     }
   }
   __syncthreads();  // the last chunk's records (aliasing part[]) are consumed
@@ -1023,17 +1054,16 @@ __device__ __forceinline__ void p2g_tile(const int tile, const InstDesc* __restr
 // and the first chunk of the next tile is copied while the current tile scatters.
 template <int CHUNK, bool STAGED>
 __global__ void __launch_bounds__(P2G_THREADS, 2)
-    k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
-          const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
+    k_p2g(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
           const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, long long* __restrict__ acc,
           int64_t node_total, uint32_t* __restrict__ blk_epoch, int transport_only,
-          const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count, uint32_t* cursor) {
+          const uint4* __restrict__ tile_rec, const uint32_t* __restrict__ tile_count, uint32_t* cursor) {
   const uint32_t n = *tile_count;
   if constexpr (!STAGED) {
     __shared__ uint32_t slot;
     for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
-      p2g_tile<CHUNK, false>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm, acc, node_total,
-                             blk_epoch, transport_only, -1);
+      p2g_tile<CHUNK, false>(tile_rec[i], desc, ctrl, st0, st1, cap, start, perm, acc, node_total, blk_epoch,
+                             transport_only, nullptr);
       __syncthreads();  // the next tile reuses the shared memory
     }
   } else {
@@ -1042,13 +1072,13 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
     float* raw = reinterpret_cast<float*>(reinterpret_cast<char*>(part) + p2g_smem(CHUNK));
     int which = 0;
     uint32_t i = tile_first(cursor, &slots[0]);
-    if (i < n) p2g_stage_tile<CHUNK>(raw, (int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm);
+    if (i < n) p2g_stage_tile<CHUNK>(raw, tile_rec[i], ctrl, st0, st1, cap, perm);
     cp_async_commit();
     while (i < n) {
       which ^= 1;
       const uint32_t nx = tile_next(cursor, i, &slots[which]);
-      p2g_tile<CHUNK, true>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, cap, start, perm, acc, node_total,
-                            blk_epoch, transport_only, nx < n ? (int)tile_list[nx] : -1);
+      p2g_tile<CHUNK, true>(tile_rec[i], desc, ctrl, st0, st1, cap, start, perm, acc, node_total, blk_epoch,
+                            transport_only, nx < n ? tile_rec + nx : nullptr);
       __syncthreads();  // the next tile reuses the shared memory
       i = nx;
     }
@@ -2148,28 +2178,26 @@ __device__ __forceinline__ void g2p_prefetch(float* __restrict__ buf, const floa
 // lane time in the Herschel-Bulkley return to clk[1], so clk[1] / clk[0] is the share of warp
 // time the return takes.
 template <bool WARM, int NT, bool CLOCKS>
-__device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restrict__ desc,
-                                         const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
-                                         float* __restrict__ st0, float* __restrict__ st1,
+__device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __restrict__ desc,
+                                         const Control* __restrict__ ctrl, float* __restrict__ st0, float* __restrict__ st1,
                                          uint32_t* __restrict__ id0, uint32_t* __restrict__ id1, int64_t cap,
-                                         const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
-                                         const float4* __restrict__ vel, ParticlePartial* __restrict__ part,
-                                         const float* __restrict__ mlp_tab, float* __restrict__ log_x,
+                                         const uint32_t* __restrict__ perm, const float4* __restrict__ vel,
+                                         ParticlePartial* __restrict__ part, const float* __restrict__ mlp_tab,
+                                         float* __restrict__ log_x,
                                          float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
                                          long long log_cap, unsigned long long* __restrict__ clk) {
   __shared__ float4 hv[HN];
   __shared__ double shd[(NT / 32) * 9 + 9];
   extern __shared__ float4 g2p_dyn[];  // prefetched inputs of two rounds
   float* pf = reinterpret_cast<float*>(g2p_dyn);
-  const int inst = tile_inst[tile];
+  const int tile = (int)rec.x, inst = (int)rec.y;
   const Control& c = ctrl[inst];
   if (!c.active) return;
   const long long clk_begin = CLOCKS ? clock64() : 0;
   unsigned long long clk_newton = 0;  // CLOCKS: this warp's return cycles in the tile
   const InstDesc& D = desc[inst];
   const int64_t ltile = tile - D.tile_off;
-  const int64_t key0 = D.key_off + ltile * TB;
-  const uint32_t s0 = start[key0], e0 = start[key0 + TB];
+  const uint32_t s0 = rec.z, e0 = rec.w;
   if (s0 == e0) {
     if (threadIdx.x == 0) {
       ParticlePartial& P = part[tile];
@@ -2181,6 +2209,27 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
     }
     return;
   }
+  const float* cur = c.parity ? st1 : st0;
+  float* nxt = c.parity ? st0 : st1;
+  const uint32_t* idc = c.parity ? id1 : id0;
+  uint32_t* idn = c.parity ? id0 : id1;
+  const bool paste = D.kind == 0, pyield = paste && D.per_particle_yield;
+  const int nround = (int)((e0 - s0 + NT - 1) / NT);
+  // slot of this thread in round r (clamped to the tile's last particle) and warp liveness
+  auto slot_of = [&](int r) -> int64_t {
+    const int64_t kk = (int64_t)s0 + (int64_t)r * NT + threadIdx.x;
+    return kk < (int64_t)e0 ? kk : (int64_t)e0 - 1;
+  };
+  auto live_of = [&](int r) -> bool {
+    return (int64_t)s0 + (int64_t)r * NT + (threadIdx.x & ~31u) < (int64_t)e0;
+  };
+  // pipeline: copies of round r+1 are in flight while round r computes; perm of round r+2 is
+  // loaded a round ahead of its copies.  The first round's copies are issued before the halo is
+  // staged, so that the two overlap.
+  int64_t src_next = 0;
+  if (live_of(0)) g2p_prefetch<NT>(pf, cur, idc, cap, perm[slot_of(0)], paste, pyield);
+  cp_async_commit();
+  if (nround > 1 && live_of(1)) src_next = perm[slot_of(1)];
   const int tz = (int)(ltile % D.tiles[2]);
   const int ty = (int)((ltile / D.tiles[2]) % D.tiles[1]);
   const int tx = (int)(ltile / ((int64_t)D.tiles[2] * D.tiles[1]));
@@ -2196,32 +2245,12 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
   const float2* tab =
       use_mlp ? reinterpret_cast<const float2*>(mlp_tab + (int64_t)inst * MLP_TAB_FLOATS + MLP_TAB_STRIDE) : nullptr;
   const float inv_k = (float)(1.0 / D.consistency);
-  const float* cur = c.parity ? st1 : st0;
-  float* nxt = c.parity ? st0 : st1;
-  const uint32_t* idc = c.parity ? id1 : id0;
-  uint32_t* idn = c.parity ? id0 : id1;
   const float dx = (float)D.dx;
   const float dt = (float)c.dt;
   double diss = 0.0, bb = 0.0, mass_sum = 0.0;
   float max_speed = 0.0f, max_disp = 0.0f;
   int fail = F_OK, iters = 0, yielded = 0;
   double fail_value = 0.0;
-  const bool paste = D.kind == 0, pyield = paste && D.per_particle_yield;
-  const int nround = (int)((e0 - s0 + NT - 1) / NT);
-  // slot of this thread in round r (clamped to the tile's last particle) and warp liveness
-  auto slot_of = [&](int r) -> int64_t {
-    const int64_t kk = (int64_t)s0 + (int64_t)r * NT + threadIdx.x;
-    return kk < (int64_t)e0 ? kk : (int64_t)e0 - 1;
-  };
-  auto live_of = [&](int r) -> bool {
-    return (int64_t)s0 + (int64_t)r * NT + (threadIdx.x & ~31u) < (int64_t)e0;
-  };
-  // pipeline: copies of round r+1 are in flight while round r computes; perm of round r+2 is
-  // loaded a round ahead of its copies
-  int64_t src_next = 0;
-  if (live_of(0)) g2p_prefetch<NT>(pf, cur, idc, cap, perm[slot_of(0)], paste, pyield);
-  cp_async_commit();
-  if (nround > 1 && live_of(1)) src_next = perm[slot_of(1)];
   const float c_tau = (float)(D.max_dt * 4.0 / (D.dx * D.dx));
   const float c_dx = (float)(2.6 * D.dx);
   const float c_g =
@@ -2426,18 +2455,17 @@ __device__ __forceinline__ void g2p_tile(const int tile, const InstDesc* __restr
 // registers a thread needs.
 template <bool WARM, int NT, int MINB = 512 / NT, bool CLOCKS = false>
 __global__ void __launch_bounds__(NT, MINB)
-    k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, const int* __restrict__ tile_inst,
-          float* __restrict__ st0, float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1,
-          int64_t cap, const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
-          const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const float* __restrict__ mlp_tab,
+    k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, float* __restrict__ st0,
+          float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1, int64_t cap,
+          const uint32_t* __restrict__ perm, const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const float* __restrict__ mlp_tab,
           float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
-          long long log_cap, const uint32_t* __restrict__ tile_list, const uint32_t* __restrict__ tile_count,
+          long long log_cap, const uint4* __restrict__ tile_rec, const uint32_t* __restrict__ tile_count,
           uint32_t* cursor, unsigned long long* __restrict__ clk) {
   __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
   for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
-    g2p_tile<WARM, NT, CLOCKS>((int)tile_list[i], desc, ctrl, tile_inst, st0, st1, id0, id1, cap, start, perm, vel,
-                               part, mlp_tab, log_x, log_y, log_n, log_cap, clk);
+    g2p_tile<WARM, NT, CLOCKS>(tile_rec[i], desc, ctrl, st0, st1, id0, id1, cap, perm, vel, part, mlp_tab, log_x,
+                               log_y, log_n, log_cap, clk);
     __syncthreads();  // the next tile reuses the shared memory
   }
 }
@@ -2967,8 +2995,8 @@ static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1)
 // Resident CTAs per SM of the persistent kernels' instantiations (from the occupancy calculator;
 // the defaults are the B200 figures) and the SM count.
 static int g_sms = 148, g_sort_per_sm = 16;
-static int g_p2g_per_sm[3] = {2, 2, 2};              // [p2g_variant]
-static int g_g2p_per_sm[4][2] = {{2, 2}, {4, 4}, {5, 5}, {6, 6}};  // [g2p_variant][warm]
+static int g_p2g_per_sm[P2G_VARIANTS] = {2, 2, 2};  // [p2g_variant]
+static int g_g2p_per_sm[G2P_VARIANTS][2] = {{2, 2}, {4, 4}, {5, 5}, {6, 6}};  // [g2p_variant][warm]
 
 // dynamic shared memory of each P2G variant: records / partials, plus the staged copies
 static size_t p2g_variant_smem(int v) {
@@ -2981,9 +3009,9 @@ static void occupancy(int* out, const void* fn, int threads, size_t smem) {
 }
 
 void configure_kernels() {
-  const void* p2g[3] = {(const void*)k_p2g<P2G_CHUNK, false>, (const void*)k_p2g<P2G_CHUNK_SMALL, false>,
-                        (const void*)k_p2g<P2G_CHUNK_SMALL, true>};
-  for (int v = 0; v < 3; ++v)
+  const void* p2g[P2G_VARIANTS] = {(const void*)k_p2g<P2G_CHUNK, false>, (const void*)k_p2g<P2G_CHUNK_SMALL, false>,
+                                   (const void*)k_p2g<P2G_CHUNK_SMALL, true>};
+  for (int v = 0; v < P2G_VARIANTS; ++v)
     cudaFuncSetAttribute(p2g[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_variant_smem(v));
   const void* g2p[4][2] = {{(const void*)k_g2p<false, G2P_THREADS>, (const void*)k_g2p<true, G2P_THREADS>},
                            {(const void*)k_g2p<false, G2P_THREADS_SMALL>, (const void*)k_g2p<true, G2P_THREADS_SMALL>},
@@ -2997,7 +3025,7 @@ void configure_kernels() {
     return;
   g_sms = sms;
   occupancy(&g_sort_per_sm, (const void*)k_bin_sort, TB, 0);
-  for (int v = 0; v < 3; ++v) occupancy(&g_p2g_per_sm[v], p2g[v], P2G_THREADS, p2g_variant_smem(v));
+  for (int v = 0; v < P2G_VARIANTS; ++v) occupancy(&g_p2g_per_sm[v], p2g[v], P2G_THREADS, p2g_variant_smem(v));
   for (int v = 0; v < 4; ++v)
     for (int w = 0; w < 2; ++w) occupancy(&g_g2p_per_sm[v][w], g2p[v][w], g2p_threads(v), g2p_smem(g2p_threads(v)));
 }
@@ -3011,8 +3039,8 @@ static unsigned persistent_ctas(int requested, int limit) {
 int launch_shape_limits(int out[LAUNCH_LIMITS]) {
   out[0] = g_sms;
   out[1] = g_sort_per_sm;
-  for (int v = 0; v < 3; ++v) out[2 + v] = g_p2g_per_sm[v];
-  for (int v = 0; v < 4; ++v) out[5 + v] = g_g2p_per_sm[v][1];
+  for (int v = 0; v < P2G_VARIANTS; ++v) out[LIM_P2G + v] = g_p2g_per_sm[v];
+  for (int v = 0; v < G2P_VARIANTS; ++v) out[LIM_G2P + v] = g_g2p_per_sm[v][1];
   return LAUNCH_LIMITS;
 }
 
@@ -3020,20 +3048,20 @@ int launch_shape_limits(int out[LAUNCH_LIMITS]) {
 static int launch_tiles_p2g(const DeviceArrays& A, cudaStream_t s, int transport_only, cudaEvent_t* ev, int& n) {
   const LaunchShape& L = A.shape;
   uint32_t* cur = L.dynamic ? A.nw_count + 2 : nullptr;  // cursors: [0] bin sort, [1] P2G, [2] G2P
-  k_tiles<<<grid_of(A.n_tiles, 256), 256, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.n_tiles, A.start, A.tile_list,
+  k_tiles<<<grid_of(A.n_tiles, 256), 256, 0, s>>>(A.desc, A.ctrl, A.tile_inst, A.n_tiles, A.start, A.tile_rec,
                                                    A.tile_count, A.tpart);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  k_bin_sort<<<(unsigned)(g_sort_per_sm * g_sms), TB, 0, s>>>(A.desc, A.tile_inst, A.start, A.perm, A.tile_list,
-                                                               A.tile_count, cur);
+  k_bin_sort<<<(unsigned)(g_sort_per_sm * g_sms), TB, 0, s>>>(A.desc, A.start, A.perm, A.tile_rec, A.tile_count,
+                                                               cur);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
-  const int v = (L.p2g_variant >= 0 && L.p2g_variant <= 2) ? L.p2g_variant : 0;
+  const int v = (L.p2g_variant >= 0 && L.p2g_variant < P2G_VARIANTS) ? L.p2g_variant : 0;
   const unsigned ctas = persistent_ctas(L.p2g_per_sm, g_p2g_per_sm[v]);
   uint32_t* pc = cur ? cur + 1 : nullptr;
 #define LP_P2G_ARGS                                                                                          \
-  A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.cap, A.start, A.perm, A.acc, A.node_total, A.blk_epoch, \
-      transport_only, A.tile_list, A.tile_count, pc
+  A.desc, A.ctrl, A.st[0], A.st[1], A.cap, A.start, A.perm, A.acc, A.node_total, A.blk_epoch, transport_only, \
+      A.tile_rec, A.tile_count, pc
   if (v == 2) k_p2g<P2G_CHUNK_SMALL, true><<<ctas, P2G_THREADS, p2g_variant_smem(2), s>>>(LP_P2G_ARGS);
   else if (v == 1) k_p2g<P2G_CHUNK_SMALL, false><<<ctas, P2G_THREADS, p2g_variant_smem(1), s>>>(LP_P2G_ARGS);
   else k_p2g<P2G_CHUNK, false><<<ctas, P2G_THREADS, p2g_variant_smem(0), s>>>(LP_P2G_ARGS);
@@ -3048,11 +3076,11 @@ static void launch_g2p(const DeviceArrays& A, bool warm, cudaStream_t s) {
   const LaunchShape& L = A.shape;
   uint32_t* cur = L.dynamic ? A.nw_count + 4 : nullptr;
   const float* tab = warm ? A.mlp_tab : nullptr;
-  const int v = (L.g2p_variant >= 0 && L.g2p_variant <= 3) ? L.g2p_variant : 0;
+  const int v = (L.g2p_variant >= 0 && L.g2p_variant < G2P_VARIANTS) ? L.g2p_variant : 0;
   const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[v][warm ? 1 : 0]);
 #define LP_G2P_ARGS                                                                                               \
-  A.desc, A.ctrl, A.tile_inst, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.start, A.perm, A.vel, A.tpart, tab, \
-      A.log_x, A.log_y, A.log_n, A.log_cap, A.tile_list, A.tile_count, cur, A.g2p_clk
+  A.desc, A.ctrl, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.perm, A.vel, A.tpart, tab, A.log_x, A.log_y, \
+      A.log_n, A.log_cap, A.tile_rec, A.tile_count, cur, A.g2p_clk
 #define LP_G2P_LAUNCH(T, MB, CLK, N) \
   (warm ? k_g2p<true, T, MB, CLK> : k_g2p<false, T, MB, CLK>)<<<N, T, g2p_smem(T), s>>>(LP_G2P_ARGS)
   if (A.g2p_clk) {  // measurement of the return's share of G2P warp time (256-thread CTAs)

@@ -49,7 +49,7 @@ struct DeviceArrays {
   uint32_t* nw_count = nullptr;    // [0] near-wall particles, [1] occupied tiles of the attempt,
                                    // [2..4] tile cursors of the bin sort, P2G and G2P
   uint32_t* tile_count = nullptr;  // = nw_count + 1
-  uint32_t* tile_list = nullptr;   // occupied tiles of the attempt (n_tiles capacity)
+  uint4* tile_rec = nullptr;       // occupied tiles of the attempt: (tile, instance, first slot, end slot)
   long long* acc = nullptr;   // 4 x node_total: mass, momentum xyz (int64 fixed point)
   long long* trac = nullptr;  // 6 x node_total: reactions per axis, low faces then high faces
   int64_t node_total = 0;
@@ -113,9 +113,11 @@ int launch_export(const HostParticleChunk& h, int64_t n, int64_t first, const fl
                   cudaStream_t s);
 uint64_t kernel_launch_count();
 void configure_kernels();              // one-time function attributes (dynamic shared memory)
-// out = SMs, resident CTAs per SM of the bin sort, of P2G variants 0-2 and of the warm G2P
-// variants 0-3; returns LAUNCH_LIMITS
-constexpr int LAUNCH_LIMITS = 9;
+// launch-shape variants of the persistent P2G and G2P kernels
+constexpr int P2G_VARIANTS = 3, G2P_VARIANTS = 4;
+// out = SMs, resident CTAs per SM of the bin sort, of the P2G variants (from out[LIM_P2G]) and of
+// the warm G2P variants (from out[LIM_G2P]); returns LAUNCH_LIMITS
+constexpr int LIM_P2G = 2, LIM_G2P = LIM_P2G + P2G_VARIANTS, LAUNCH_LIMITS = LIM_G2P + G2P_VARIANTS;
 int launch_shape_limits(int out[LAUNCH_LIMITS]);
 void set_last_error(const char* msg);  // message returned by lp_last_error()
 void add_kernel_launches(uint64_t n);

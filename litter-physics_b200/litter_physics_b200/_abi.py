@@ -271,6 +271,28 @@ def particle_buffers(count: int):
     return arrays, view
 
 
+def particle_out_view(arrays: dict, count: int) -> Particles:
+    """A `Particles` view over caller-owned output arrays for an export of `count` particles.
+
+    Every field must be present, C-contiguous, writable and of the dtype and shape that
+    `particle_buffers` allocates; a resident host particle set can then be refreshed in place,
+    without allocating (and first touching) new pages."""
+    import numpy as np
+
+    view = Particles()
+    view.count = count
+    for name, (ctype, comps) in PARTICLE_FIELDS.items():
+        arr = arrays.get(name)
+        dtype = np.uint32 if ctype is C.c_uint32 else np.float64
+        shape = (count,) if comps == 1 else (count, 3) if comps == 3 else (count, 3, 3)
+        if (arr is None or not isinstance(arr, np.ndarray) or arr.dtype != dtype or arr.shape != shape
+                or not arr.flags.c_contiguous or not arr.flags.writeable):
+            raise ValueError(f"output field {name!r} must be a writable C-contiguous {np.dtype(dtype).name} "
+                             f"array of shape {shape}")
+        setattr(view, name, arr.ctypes.data_as(C.POINTER(ctype)))
+    return view
+
+
 def particle_view(arrays: dict) -> Particles:
     """A `Particles` view over caller arrays (must be C-contiguous, dtype as above)."""
     view = Particles()

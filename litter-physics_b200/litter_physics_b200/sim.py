@@ -165,9 +165,16 @@ class Simulation:
         check(lib().lp_sim_particle_count(self._h, C.byref(n)))
         return int(n.value)
 
-    def particles(self) -> dict:
-        """Export the committed particle set (FP64 arrays in the reference layout, slot order)."""
-        arrays, view = _abi.particle_buffers(self.particle_count())
+    def particles(self, out: dict | None = None) -> dict:
+        """Export the committed particle set (FP64 arrays in the reference layout, slot order).
+
+        `out`: arrays of a resident host particle set (as returned by an earlier export) to
+        overwrite in place instead of allocating new ones."""
+        n = self.particle_count()
+        if out is None:
+            arrays, view = _abi.particle_buffers(n)
+        else:
+            arrays, view = out, _abi.particle_out_view(out, n)
         check(lib().lp_sim_export_particles(self._h, C.byref(view)))
         return arrays
 
@@ -403,9 +410,13 @@ class Batch:
         check(lib().lp_batch_get_ledger(self._h, i, C.byref(led)))
         return led
 
-    def particles(self, i: int) -> dict:
-        n = self.counters(i).particle_count
-        arrays, view = _abi.particle_buffers(int(n))
+    def particles(self, i: int, out: dict | None = None) -> dict:
+        """Export instance i's committed particle set (`out`: arrays to overwrite in place)."""
+        n = int(self.counters(i).particle_count)
+        if out is None:
+            arrays, view = _abi.particle_buffers(n)
+        else:
+            arrays, view = out, _abi.particle_out_view(out, n)
         check(lib().lp_batch_export_particles(self._h, i, C.byref(view)))
         return arrays
 

@@ -90,3 +90,28 @@ def test_compute_entry_points_fail_loudly_without_device(L):
     with pytest.raises(sim.LPError) as e:
         sim.Simulation(configs.slump(16, (4, 4, 8)))
     assert e.value.status == _abi.LP_DEVICE
+
+
+def test_export_into_caller_arrays_checks_every_field():
+    """An export into a resident host particle set takes arrays of exactly the layout a fresh
+    export allocates and refuses anything else before the library is called."""
+    import numpy as np
+
+    from litter_physics_b200 import _abi
+
+    arrays, _ = _abi.particle_buffers(5)
+    view = _abi.particle_out_view(arrays, 5)
+    assert view.count == 5
+    for name, bad in (("position", np.zeros((5, 3), np.float32)), ("deformation", np.zeros((5, 9))),
+                      ("id", np.zeros(5, np.int64)), ("mass", np.zeros(10)[::2])):
+        wrong = dict(arrays, **{name: bad})
+        with pytest.raises(ValueError, match=name):
+            _abi.particle_out_view(wrong, 5)
+    missing = {k: v for k, v in arrays.items() if k != "velocity"}
+    with pytest.raises(ValueError, match="velocity"):
+        _abi.particle_out_view(missing, 5)
+    frozen = dict(arrays)
+    frozen["mass"] = arrays["mass"].copy()
+    frozen["mass"].flags.writeable = False
+    with pytest.raises(ValueError, match="mass"):
+        _abi.particle_out_view(frozen, 5)

@@ -325,3 +325,20 @@ def test_batch_matches_single_instances(lib_built):
         pb, ps = by_id(b.particles(i)), by_id(one.particles())
         assert np.array_equal(pb["position"], ps["position"])
         assert bytes(b.ledger(i)) == bytes(one.ledger)
+
+
+def test_export_in_place_matches_a_fresh_export(lib_built):
+    """The export into a resident host particle set overwrites every field with what a fresh
+    export returns."""
+    from litter_physics_b200.sim import Simulation
+
+    spec = small_slump()
+    sim = Simulation(spec)
+    sim.advance_to(10 * spec.max_dt)
+    fresh = sim.particles()
+    host = {k: np.full_like(v, 7) for k, v in fresh.items()}  # stale contents
+    got = sim.particles(out=host)
+    assert got is host
+    for k, v in fresh.items():
+        assert np.array_equal(host[k], v), k
+    sim.close()
