@@ -249,6 +249,13 @@ lp_status lp_sim_particle_count(lp_sim* sim, uint64_t* out);
  * out->count to the buffer capacity on entry). */
 lp_status lp_sim_export_particles(lp_sim* sim, lp_particles* out);
 lp_status lp_sim_import_particles(lp_sim* sim, const lp_particles* in);
+/* Extension, no reference counterpart: page-lock (cudaHostRegister) a caller's host buffer, or
+ * release it.  Export and import move arrays that are page-locked from the first to the last
+ * byte by DMA straight between them and the device, without the library's pinned staging copy;
+ * arrays in pageable memory go through the staging copy as before.  A caller that keeps its
+ * particle set resident in host memory pins it once and reuses it for every checkpoint. */
+lp_status lp_host_pin(void* ptr, uint64_t bytes);
+lp_status lp_host_unpin(void* ptr);
 lp_status lp_sim_get_pellet(lp_sim* sim, lp_pellet* out, int32_t* has_pellet);
 lp_status lp_sim_set_pellet(lp_sim* sim, const lp_pellet* in);
 /* Pellet bed (extension, no reference counterpart): the committed state of every pellet, in

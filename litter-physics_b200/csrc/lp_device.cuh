@@ -613,7 +613,10 @@ __constant__ const float kInverse[10] = {0.0f,        1.0f,        1.0f / 2.0f, 
 // Trial part of the paste update: the Hencky strain of H_tr and its equivalent stress.  The
 // Newton start (the learned warm start) is chosen from t.trial_eq between paste_trial and
 // paste_finish, which lets a warp evaluate the network for all its lanes at one call site.
-enum { PT_SERIES = 0, PT_JACOBI = 1, PT_DONE = 2 };
+// PT_DEFER (DEFER instantiations only): the strain is outside the series path and the caller
+// leaves the particle to a separate eigen-decomposition pass, so that its own code carries no
+// call of paste_update_jacobi.
+enum { PT_SERIES = 0, PT_JACOBI = 1, PT_DONE = 2, PT_DEFER = 3 };
 struct PasteTrial {
   Sym dev;
   float mean, vol, dnorm;
@@ -621,6 +624,7 @@ struct PasteTrial {
   int path;
 };
 
+template <bool DEFER = false>
 __device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& t, PasteOut& o) {
   o.fail = F_OK;
   o.iters = 0;
@@ -636,16 +640,21 @@ __device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& 
   B.yz = Htr[5] + Htr[7] + (Htr[3] * Htr[6] + Htr[4] * Htr[7] + Htr[5] * Htr[8]);
   const float r = sym_norm(B);
   if (!(r <= 0.25f)) {  // large or non-finite strain: eigen-decomposition path
-    // the out-of-line call works on copies, so that the caller's arrays need no stack home
-    float Hj[9];
+    if constexpr (DEFER) {
+      t.path = PT_DEFER;
+      t.trial_eq = 0.0;
+    } else {
+      // the out-of-line call works on copies, so that the caller's arrays need no stack home
+      float Hj[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) Hj[i] = Htr[i];
-    PasteOut oj = o;
-    const HbConst none = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0};  // the trial stops before the return
-    paste_update_jacobi(Hj, 0.f, 0.f, mu_d, 0.0, none, 0.0, -1.0, true, oj);
-    o = oj;
-    t.path = o.fail == F_OK ? PT_JACOBI : PT_DONE;
-    t.trial_eq = o.trial;
+      for (int i = 0; i < 9; ++i) Hj[i] = Htr[i];
+      PasteOut oj = o;
+      const HbConst none = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0};  // the trial stops before the return
+      paste_update_jacobi(Hj, 0.f, 0.f, mu_d, 0.0, none, 0.0, -1.0, true, oj);
+      o = oj;
+      t.path = o.fail == F_OK ? PT_JACOBI : PT_DONE;
+      t.trial_eq = o.trial;
+    }
     return;
   }
   const float f00 = 1.f + Htr[0], f01 = Htr[1], f02 = Htr[2];
@@ -696,30 +705,17 @@ __device__ inline void paste_trial(const float Htr[9], double mu_d, PasteTrial& 
   t.path = PT_SERIES;
 }
 
-// Rest of the paste update after paste_trial: the Herschel-Bulkley return started at sigma0
-// (in (yield, trial), or -1 for the midpoint), the stress and the plastic correction of H.
+// The Herschel-Bulkley return of the series path after paste_trial, started at sigma0 (in
+// (yield, trial), or -1 for the midpoint): sets o.eq, o.trial, and for a yielding particle
+// o.dep, o.iters, o.yielded (or o.fail), and returns the deviatoric scale sigma / sigma_tr.
 // newton_cycles (measurement builds only, else null): clock64 cycles spent in the return are
 // added to it.
-__device__ inline void paste_finish(const float Htr[9], float mu, float lambda, double mu_d, double ys, const HbConst& h,
-                                    double tol, double sigma0, const PasteTrial& t, PasteOut& o,
-                                    long long* newton_cycles = nullptr) {
-  if (t.path == PT_DONE) return;
-  if (t.path == PT_JACOBI) {
-    float Hj[9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) Hj[i] = Htr[i];
-    PasteOut oj = o;
-    paste_update_jacobi(Hj, mu, lambda, mu_d, ys, h, tol, sigma0, false, oj);
-    o = oj;
-    return;
-  }
-  const Sym& dev = t.dev;
-  const float vol = t.vol, mean = t.mean;
-  const double trial_eq = t.trial_eq;
+__device__ __forceinline__ double paste_return(double trial_eq, float dnorm, double ys, const HbConst& h, double tol,
+                                               double sigma0, PasteOut& o, long long* newton_cycles = nullptr) {
   o.eq = trial_eq;
   o.trial = trial_eq;
   double scale = 1.0;
-  if (trial_eq > ys && t.dnorm > 0.f) {
+  if (trial_eq > ys && dnorm > 0.f) {
     double sigma, dep;
     int iters;
     const long long c0 = newton_cycles ? clock64() : 0;
@@ -728,13 +724,21 @@ __device__ inline void paste_finish(const float Htr[9], float mu, float lambda, 
     o.iters = iters;
     if (e != F_OK) {
       o.fail = e;
-      return;
+      return 1.0;
     }
     scale = sigma / trial_eq;
     o.dep = dep;
     o.eq = sigma;
     o.yielded = 1;
   }
+  return scale;
+}
+
+// The stress and the plastic correction of H after paste_return (series path): tau from the
+// scaled deviatoric Hencky strain, and for a yielding particle H_new = H_tr + G (I + H_tr) with
+// G = exp((scale - 1) dev E) - I.
+__device__ __forceinline__ void paste_stress(const float Htr[9], const Sym& dev, float mean, float vol, float mu,
+                                             float lambda, double scale, PasteOut& o) {
   const float sc = (float)scale;
   const float lv = lambda * vol;
   o.tau[0] = 2.f * mu * (dev.xx * sc + mean) + lv;
@@ -788,6 +792,29 @@ __device__ inline void paste_finish(const float Htr[9], float mu, float lambda, 
     for (int i = 0; i < 9; ++i) o.H[i] = Htr[i];
   }
   o.diss_density = o.eq * o.dep;
+}
+
+// Rest of the paste update after paste_trial: the return (paste_return) and the stress and
+// plastic correction (paste_stress), or the eigen-decomposition path for PT_JACOBI.
+template <bool DEFER = false>
+__device__ inline void paste_finish(const float Htr[9], float mu, float lambda, double mu_d, double ys, const HbConst& h,
+                                    double tol, double sigma0, const PasteTrial& t, PasteOut& o,
+                                    long long* newton_cycles = nullptr) {
+  if (t.path == PT_DONE || t.path == PT_DEFER) return;
+  if constexpr (!DEFER) {
+    if (t.path == PT_JACOBI) {
+      float Hj[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) Hj[i] = Htr[i];
+      PasteOut oj = o;
+      paste_update_jacobi(Hj, mu, lambda, mu_d, ys, h, tol, sigma0, false, oj);
+      o = oj;
+      return;
+    }
+  }
+  const double scale = paste_return(t.trial_eq, t.dnorm, ys, h, tol, sigma0, o, newton_cycles);
+  if (o.fail != F_OK) return;
+  paste_stress(Htr, t.dev, t.mean, t.vol, mu, lambda, scale, o);
 }
 
 // whole paste update (constitutive.rs:456-531) with the reference's midpoint Newton start

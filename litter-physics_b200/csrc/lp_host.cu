@@ -785,9 +785,10 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   ALLOC(A.chunk_base, A.n_chunks);
   ALLOC(A.perm, A.cap);
   ALLOC(A.nw_list, A.cap);
-  ALLOC(A.nw_count, 5);
+  ALLOC(A.nw_count, 6);
   A.tile_count = A.nw_count + 1;
   ALLOC(A.tile_rec, A.n_tiles);
+  ALLOC(A.defer_rec, A.n_tiles);
   ALLOC(A.acc, 4 * A.node_total);
   ALLOC(A.trac, 6 * A.node_total);
   ALLOC(A.blk_epoch, A.n_blk);
@@ -1217,6 +1218,30 @@ static inline void* host_twin(const Ensemble& E, const void* dev) {
   return (char*)E.h_stage + ((const char*)dev - (const char*)E.d_stage);
 }
 
+// A caller's host span is page-locked (cudaHostAlloc'd or cudaHostRegister'ed, for example with
+// lp_host_pin) from its first to its last byte: then import and export move it by DMA directly,
+// without the staging copy by host threads.  A wrong answer would cost speed only: a copy from
+// pageable memory is still correct.
+static bool page_locked(const void* p, size_t bytes) {
+  if (!p || bytes == 0) return true;
+  for (const char* q : {(const char*)p, (const char*)p + bytes - 1}) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (a.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
+}
+static bool particles_page_locked(const lp_particles* p, int64_t n) {
+  const size_t d1 = sizeof(double) * (size_t)n;
+  return page_locked(p->id, sizeof(uint32_t) * (size_t)n) && page_locked(p->position, 3 * d1) &&
+         page_locked(p->velocity, 3 * d1) && page_locked(p->affine, 9 * d1) && page_locked(p->deformation, 9 * d1) &&
+         page_locked(p->kirchhoff, 9 * d1) && page_locked(p->volume_ratio, d1) && page_locked(p->plastic_strain, d1) &&
+         page_locked(p->mass, d1) && page_locked(p->volume0, d1) && page_locked(p->yield_stress, d1);
+}
+
 // Export instance i's committed particles into the caller's FP64 arrays (null fields are
 // skipped).  Chunk k is converted on the device into staging slot k % 2 and copied to its pinned
 // twin (one copy per requested field); while those run, host threads copy chunk k - 1 from the
@@ -1230,6 +1255,9 @@ lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
   if ((int64_t)out->count < n) return set_error(LP_INVALID, "particle buffer too small");
   st = stage_alloc(E, n);
   if (st != LP_OK) return st;
+  // page-locked caller arrays: each chunk is converted into its staging slot and copied by DMA
+  // straight into them, all in stream order (a slot is rewritten only after its copies ran)
+  const bool direct = particles_page_locked(out, n);
   std::vector<CopySpan> pending[2];  // host copies waiting for slot s's device-to-host copies
   int64_t k = 0;
   for (int64_t first = 0; first < n; first += E.stage_particles, ++k) {
@@ -1246,6 +1274,10 @@ lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
     spans.clear();
     auto back = [&](void* dst, const void* src, size_t bytes) -> lp_status {
       if (!dst) return LP_OK;
+      if (direct) {
+        CUDA_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, E.stream));
+        return LP_OK;
+      }
       void* pinned = host_twin(E, src);
       CUDA_CK(cudaMemcpyAsync(pinned, src, bytes, cudaMemcpyDeviceToHost, E.stream));
       spans.push_back({dst, pinned, bytes});
@@ -1264,13 +1296,16 @@ lp_status export_particles(Ensemble& E, int i, lp_particles* out) {
         back(out->volume0 ? out->volume0 + first : nullptr, h.volume0, d1) != LP_OK ||
         back(out->yield_stress ? out->yield_stress + first : nullptr, h.yield_stress, d1) != LP_OK)
       return LP_DEVICE;
+    if (direct) continue;
     CUDA_CK(cudaEventRecord(E.stage_ev[slot], E.stream));
     if (k > 0) {  // chunk k - 1: its copies have landed once the other slot's event has
       CUDA_CK(cudaEventSynchronize(E.stage_ev[slot ^ 1]));
       parallel_copy(pending[slot ^ 1]);
     }
   }
-  if (k > 0) {
+  if (direct) {
+    CUDA_CK(cudaStreamSynchronize(E.stream));
+  } else if (k > 0) {
     const int last = (int)((k - 1) & 1);
     CUDA_CK(cudaEventSynchronize(E.stage_ev[last]));
     parallel_copy(pending[last]);
@@ -1300,7 +1335,9 @@ lp_status import_particles(Ensemble& E, int i, const lp_particles* in) {
   CUDA_CK(cudaMemcpyAsync(E.d_bad, &none, sizeof(none), cudaMemcpyHostToDevice, E.stream));
   // Chunk k goes through staging slot k % 2: host threads fill the slot's pinned twin while the
   // device still copies and converts chunk k - 1 from the other slot; a slot is refilled only
-  // after the event of the chunk that last used it.
+  // after the event of the chunk that last used it.  Page-locked caller arrays go to the slot by
+  // DMA directly, in stream order, with no host copy and no wait.
+  const bool direct = particles_page_locked(in, n);
   int64_t k = 0;
   for (int64_t first = 0; first < n; first += E.stage_particles, ++k) {
     const int slot = (int)(k & 1);
@@ -1308,6 +1345,31 @@ lp_status import_particles(Ensemble& E, int i, const lp_particles* in) {
     const size_t d1 = sizeof(double) * (size_t)m;
     lp::HostParticleChunk h;
     stage_slot(E, slot, h);
+    if (direct) {
+      lp::HostParticleChunk hc = h;
+      auto up = [&](void* dst, const void* src, size_t bytes) -> lp_status {
+        CUDA_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, E.stream));
+        return LP_OK;
+      };
+      if (up(h.id, in->id + first, sizeof(uint32_t) * (size_t)m) != LP_OK ||
+          up(h.position, in->position + 3 * first, 3 * d1) != LP_OK ||
+          up(h.velocity, in->velocity + 3 * first, 3 * d1) != LP_OK ||
+          up(h.affine, in->affine + 9 * first, 9 * d1) != LP_OK ||
+          up(h.deformation, in->deformation + 9 * first, 9 * d1) != LP_OK ||
+          up(h.kirchhoff, in->kirchhoff + 9 * first, 9 * d1) != LP_OK ||
+          up(h.volume_ratio, in->volume_ratio + first, d1) != LP_OK ||
+          up(h.plastic_strain, in->plastic_strain + first, d1) != LP_OK ||
+          up(h.mass, in->mass + first, d1) != LP_OK || up(h.volume0, in->volume0 + first, d1) != LP_OK)
+        return LP_DEVICE;
+      if (in->yield_stress) {
+        if (up(h.yield_stress, in->yield_stress + first, d1) != LP_OK) return LP_DEVICE;
+      } else {
+        hc.yield_stress = nullptr;
+      }
+      lp::launch_import(hc, m, first, E.A.st[par], E.A.id[par], E.A.cap, D.slot_off, D.yield, E.d_bad, E.stream);
+      CUDA_CK(cudaGetLastError());
+      continue;
+    }
     if (k >= 2) CUDA_CK(cudaEventSynchronize(E.stage_ev[slot]));
     // caller arrays -> pinned twin (host threads) -> device staging (one copy per field)
     std::vector<CopySpan> spans = {
@@ -1653,6 +1715,26 @@ lp_status lp_sim_particle_count(lp_sim* sim, uint64_t* out) {
   return LP_OK;
 }
 lp_status lp_sim_export_particles(lp_sim* sim, lp_particles* out) { return export_particles(sim->E, 0, out); }
+lp_status lp_host_pin(void* ptr, uint64_t bytes) {
+  if (!ptr || bytes == 0) return set_error(LP_INVALID, "lp_host_pin needs a non-empty buffer");
+  const cudaError_t e = cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(LP_DEVICE, std::string("cudaHostRegister: ") + cudaGetErrorString(e));
+  }
+  return LP_OK;
+}
+
+lp_status lp_host_unpin(void* ptr) {
+  if (!ptr) return set_error(LP_INVALID, "lp_host_unpin needs a buffer");
+  const cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(LP_DEVICE, std::string("cudaHostUnregister: ") + cudaGetErrorString(e));
+  }
+  return LP_OK;
+}
+
 lp_status lp_sim_import_particles(lp_sim* sim, const lp_particles* in) { return import_particles(sim->E, 0, in); }
 
 static void pellet_out(const lp::PelletState& P, lp_pellet* out) {

@@ -164,6 +164,17 @@ __device__ __forceinline__ void warp_sum_ll_multi(long long (&v)[K]) {
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
 }
+// Exact int64 sum over a full warp by the integer reduction unit (redux.sync): the value is split
+// into 22-, 22- and 20-bit (signed) limbs, whose 32-lane sums fit 32 bits; the recombination
+// is exact modulo 2^64, hence exact whenever the total fits int64.
+__device__ __forceinline__ long long warp_sum_ll_redux(long long v) {
+  const unsigned long long u = (unsigned long long)v;
+  const unsigned s0 = __reduce_add_sync(0xffffffffu, (unsigned)(u & 0x3fffffull));
+  const unsigned s1 = __reduce_add_sync(0xffffffffu, (unsigned)((u >> 22) & 0x3fffffull));
+  const int s2 = __reduce_add_sync(0xffffffffu, (int)(v >> 44));
+  return (long long)((unsigned long long)s0 + ((unsigned long long)s1 << 22) +
+                     ((unsigned long long)(long long)s2 << 44));
+}
 // TRAIL = false leaves out the closing barrier: the caller must not rewrite sh[NW K .. NW K + K)
 // before another barrier (the partial sums below it may be rewritten at once)
 template <int NT, int K, bool TRAIL = true>
@@ -255,6 +266,10 @@ __device__ __forceinline__ float affine_norm(const float Cm[9]) {
   for (int a = 0; a < 9; ++a) d2 += (double)Cm[a] * Cm[a];
   return (float)sqrt(d2);
 }
+// |v| with explicit roundings, so that k_g2p and k_g2p_defer get the same value from the same v
+__device__ __forceinline__ float particle_speed(const float v[3]) {
+  return sqrtf(__fmaf_rn(v[2], v[2], __fmaf_rn(v[1], v[1], __fmul_rn(v[0], v[0]))));
+}
 __device__ __forceinline__ double momentum_bound(float m, float speed, float cn, const float tau[6], float v0,
                                                  float c_tau, float c_dx, float c_g) {
   const float f2 = tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2] +
@@ -302,6 +317,7 @@ __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__
     nw_count[2] = 0u;  // tile cursors of the bin sort, P2G and G2P
     nw_count[3] = 0u;
     nw_count[4] = 0u;
+    nw_count[5] = 0u;  // tiles left to k_g2p_defer
   }
   if (i >= n_inst) return;
   const InstDesc& D = desc[i];
@@ -763,9 +779,12 @@ __device__ __forceinline__ float p2g_frac(float x, float dx, float pow2_inv_dx) 
   return __fsub_rn(sc, floorf(__fsub_rn(sc, 0.5f)));
 }
 // Scatter of one record by the thread of slab `slab` (x offset) of its bin: the 9 nodes
-// (slab, b, c) x (mass, momentum), accumulated in acc9[b][c].
+// (slab, b, c) x (mass, momentum), accumulated in acc[b][c] as the pairs (p_x, p_y), (p_z, m).
+// The sums run on Blackwell's paired FP32 units (fma.rn.f32x2): each lane of a pair is the
+// single-precision FMA of the scalar form, p_r += w_ab w_c (q_r + A_r0 d_a + A_r1 d_b + A_r2 d_c)
+// and m_node += w_ab w_c m, and the mass rides in the second lane of the z pair as m + 0 d.
 __device__ __forceinline__ void p2g_scatter(float m, const float q[3], const float A[9], float fx, float fy, float fz,
-                                            int slab, float dx, float (&acc9)[3][3][4]) {
+                                            int slab, float dx, float2 (&acc)[3][3][2]) {
   float w[3][3], d[3][3];
   weights_of(fy, dx, w[1], d[1]);
   weights_of(fz, dx, w[2], d[2]);
@@ -775,19 +794,22 @@ __device__ __forceinline__ void p2g_scatter(float m, const float q[3], const flo
   const float da = (fx - (float)slab) * -dx;
   float u[3];
 #pragma unroll
-  for (int rr = 0; rr < 3; ++rr) u[rr] = q[rr] + A[3 * rr + 0] * da;
+  for (int rr = 0; rr < 3; ++rr) u[rr] = __fmaf_rn(A[3 * rr + 0], da, q[rr]);
+  const float2 a14 = make_float2(A[1], A[4]), a70 = make_float2(A[7], 0.0f);
+  const float2 a25 = make_float2(A[2], A[5]), a80 = make_float2(A[8], 0.0f);
+  const float2 u01 = make_float2(u[0], u[1]), u2m = make_float2(u[2], m);
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
-    const float wab = wa * w[1][b];
-    float ub[3];
-#pragma unroll
-    for (int rr = 0; rr < 3; ++rr) ub[rr] = u[rr] + A[3 * rr + 1] * d[1][b];
+    const float wab = __fmul_rn(wa, w[1][b]);
+    const float2 db = make_float2(d[1][b], d[1][b]);
+    const float2 ub01 = __ffma2_rn(a14, db, u01);  // (q_x + .. + A_01 d_b, q_y + .. + A_11 d_b)
+    const float2 ub2m = __ffma2_rn(a70, db, u2m);  // (q_z + .. + A_21 d_b, m)
 #pragma unroll
     for (int cc = 0; cc < 3; ++cc) {
-      const float ww = wab * w[2][cc];
-      acc9[b][cc][0] += ww * m;
-#pragma unroll
-      for (int rr = 0; rr < 3; ++rr) acc9[b][cc][1 + rr] += ww * (ub[rr] + A[3 * rr + 2] * d[2][cc]);
+      const float2 dc = make_float2(d[2][cc], d[2][cc]);
+      const float2 ww = __fmul2_rn(make_float2(wab, wab), make_float2(w[2][cc], w[2][cc]));
+      acc[b][cc][0] = __ffma2_rn(ww, __ffma2_rn(a25, dc, ub01), acc[b][cc][0]);
+      acc[b][cc][1] = __ffma2_rn(ww, __ffma2_rn(a80, dc, ub2m), acc[b][cc][1]);
     }
   }
 }
@@ -838,7 +860,6 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
   // STAGED: the raw copies sit after the records / partials region
   float* raw = reinterpret_cast<float*>(reinterpret_cast<char*>(part) + p2g_smem(CHUNK));
   __shared__ long long red[(P2G_THREADS / 32) * 8 + 8];
-  __shared__ int redi[P2G_THREADS / 32 + 1];
 
   const int tile = (int)trec.x, inst = (int)trec.y;
   const Control& c = ctrl[inst];
@@ -867,14 +888,14 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
   const float stress_scale = transport_only ? 0.0f : (float)(c.dt * 4.0 / (D.dx * D.dx));
   const double s_m = D.s_mass, s_p = c.s_mom;
 
-  float acc9[3][3][4];
+  float2 acc9[3][3][2];  // per node (b, c) of the slab: (p_x, p_y), (p_z, m)
 #pragma unroll
   for (int b = 0; b < 3; ++b)
 #pragma unroll
     for (int q = 0; q < 3; ++q)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) acc9[b][q][k] = 0.0f;
-  long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // tile totals (particles) then halo sums (nodes)
+      for (int k = 0; k < 2; ++k) acc9[b][q][k] = make_float2(0.0f, 0.0f);
+  long long tot[4] = {0, 0, 0, 0};  // this thread's particle totals (mass, momentum), fixed point
 
   const uint32_t s = start[key0 + bin], e = start[key0 + bin + 1];  // this bin's sorted range
   for (uint32_t c0 = ts; c0 < te; c0 += CHUNK) {
@@ -963,7 +984,7 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
 #pragma unroll
     for (int cc = 0; cc < 3; ++cc)
       part[bin * 27 + slab * 9 + b * 3 + cc] =
-          make_float4(acc9[b][cc][0], acc9[b][cc][1], acc9[b][cc][2], acc9[b][cc][3]);
+          make_float4(acc9[b][cc][1].y, acc9[b][cc][0].x, acc9[b][cc][0].y, acc9[b][cc][1].x);
   __syncthreads();
   // one thread per halo node: sum the 27 contributing (bin, slab) partials in a fixed order
   long long nv[4] = {0, 0, 0, 0};
@@ -973,7 +994,7 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
     hz = t % HZ;
     hy = (t / HZ) % HY;
     hx = t / (HZ * HY);
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    float2 s01 = make_float2(0.f, 0.f), s23 = make_float2(0.f, 0.f);  // (mass, p_x), (p_y, p_z)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const int lbx = hx - a;
@@ -987,49 +1008,71 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
           const int lbz = hz - cc;
           if (lbz < 0 || lbz >= TZ) continue;
           const float4 q = part[((lbx * TY + lby) * TZ + lbz) * 27 + a * 9 + b * 3 + cc];
-          s0 += q.x;
-          s1 += q.y;
-          s2 += q.z;
-          s3 += q.w;
+          s01 = __fadd2_rn(s01, make_float2(q.x, q.y));
+          s23 = __fadd2_rn(s23, make_float2(q.z, q.w));
         }
       }
     }
-    nv[0] = to_fixed((double)s0, s_m);
-    nv[1] = to_fixed((double)s1, s_p);
-    nv[2] = to_fixed((double)s2, s_p);
-    nv[3] = to_fixed((double)s3, s_p);
-    tot[4] = nv[0];
-    tot[5] = nv[1];
-    tot[6] = nv[2];
-    tot[7] = nv[3];
+    nv[0] = to_fixed((double)s01.x, s_m);
+    nv[1] = to_fixed((double)s01.y, s_p);
+    nv[2] = to_fixed((double)s23.x, s_p);
+    nv[3] = to_fixed((double)s23.y, s_p);
   }
-  // no closing barrier: the pass below writes only red[0, 64), below the totals at red[96, 104)
-  constexpr int P2G_NW = P2G_THREADS / 32;
-  static_assert(P2G_NW * 4 + P2G_NW + 4 <= P2G_NW * 8,
-                "the argmax pass's scratch must stay below the totals that block_sum_ll_multi leaves in red");
-  block_sum_ll_multi<P2G_THREADS, 8, false>(tot, red);
-  const long long Dm = tot[0] - tot[4], D0 = tot[1] - tot[5], D1 = tot[2] - tot[6], D2 = tot[3] - tot[7];
-  if (Dm != 0 || D0 != 0 || D1 != 0 || D2 != 0) {
-    // distribute the discrepancy in proportion to node mass, remainder to the heaviest node
-    long long cs[4] = {0, 0, 0, 0};
-    if (has_node) {
-      const double f = tot[4] > 0 ? (double)nv[0] / (double)tot[4] : 0.0;
-      cs[0] = __double2ll_rn((double)Dm * f);
-      cs[1] = __double2ll_rn((double)D0 * f);
-      cs[2] = __double2ll_rn((double)D1 * f);
-      cs[3] = __double2ll_rn((double)D2 * f);
+  // Exact conservation per tile.  The tile's particle totals (tot, exact int64) minus its halo's
+  // node sums (nv) is the FP32 rounding discrepancy D of each component.  It is spread over the
+  // halo nodes in proportion to node mass by a telescoping rule: with P the inclusive prefix sum
+  // of the node masses in thread order and M their total, the node of thread i receives
+  // f(P_i) - f(P_i - m_i), f(P) = floor(D (P / M)) in FP64.  The shares sum to f(M) - f(0) = D
+  // exactly and each has the sign of D.  Integer sums do not depend on their order, so the warp
+  // sums may take any route; the prefix is taken in thread order.  Two barriers.
+  constexpr int NW = P2G_THREADS / 32;
+  const int lane = t & 31, w = t >> 5;
+  long long dif[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) nv[k] += cs[k];
+  for (int k = 0; k < 4; ++k) dif[k] = warp_sum_ll_redux(tot[k] - nv[k]);
+  long long pin = nv[0];  // inclusive warp prefix of node masses
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, pin, o);
+    if (lane >= o) pin += y;
+  }
+  if (lane == 31) red[w] = pin;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) red[NW + 4 * w + k] = dif[k];
+  __syncthreads();
+  if (w == 0) {
+    const long long wm = lane < NW ? red[lane] : 0;
+    long long incl = wm;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
-    const long long heavy = has_node ? nv[0] : LLONG_MIN;
-    // the sum of the shares and the heaviest node in one pass; red and redi are not written
-    // again before the barrier that ends the tile
-    const int best = block_sum_argmax_ll<P2G_THREADS, 4>(cs, heavy, t, red, redi);
-    if (t == best) {
-      nv[0] += Dm - cs[0];
-      nv[1] += D0 - cs[1];
-      nv[2] += D1 - cs[2];
-      nv[3] += D2 - cs[3];
+    long long dd[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dd[k] = warp_sum_ll_redux(lane < NW ? red[NW + 4 * lane + k] : 0);
+    const long long mtot = __shfl_sync(0xffffffffu, incl, NW - 1);
+    if (lane < NW) red[5 * NW + lane] = incl - wm;  // node mass before warp `lane`
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) red[6 * NW + k] = dd[k];
+      red[6 * NW + 4] = mtot;
+    }
+  }
+  __syncthreads();
+  static_assert(6 * NW + 5 <= NW * 8 + 8, "the conservation scratch fits red");
+  const long long Dk[4] = {red[6 * NW + 0], red[6 * NW + 1], red[6 * NW + 2], red[6 * NW + 3]};
+  if (has_node && (Dk[0] | Dk[1] | Dk[2] | Dk[3]) != 0) {
+    const long long mtot = red[6 * NW + 4];
+    if (mtot > 0) {
+      const long long p1 = red[5 * NW + w] + pin, p0 = p1 - nv[0];
+      const double r1 = (double)p1 / (double)mtot, r0 = (double)p0 / (double)mtot;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) nv[k] += __double2ll_rd((double)Dk[k] * r1) - __double2ll_rd((double)Dk[k] * r0);
+    } else if (t == 0) {  // no node mass to weigh by: the tile's first halo node takes it all
+#pragma unroll
+      for (int k = 0; k < 4; ++k) nv[k] += Dk[k];
     }
   }
   // flush to the global grid
@@ -2171,6 +2214,14 @@ __device__ __forceinline__ void g2p_prefetch(float* __restrict__ buf, const floa
   cp_async4(b + PF_ID * NT, idc + src);
 }
 
+// Paste particles whose trial strain is outside the series path of paste_trial (||B||_F > 0.25:
+// large elastic strain, or a non-finite state) take the eigen-decomposition path.  k_g2p leaves
+// them to k_g2p_defer: it stores H_tr in the trial state's H, the unchanged plastic strain, and
+// DEFER_MARK in tau_xx, and lists the tile.  So the hot kernel carries no call of
+// paste_update_jacobi (no call frame, no copies on the stack), and a strain that needs the
+// eigenvectors costs one more pass over the tiles that hold one.
+constexpr uint32_t DEFER_MARK = 0x7fc0defeu;  // a quiet NaN payload that no arithmetic produces
+
 // Warm start (WARM instantiation): each yielding lane reads the network's logit at its la8 from
 // its instance's table (k_mlp_table), interpolated between the two neighbouring nodes.
 // one tile of k_g2p, CTAs of NT threads.  CLOCKS (a measurement instantiation, not used by the
@@ -2185,9 +2236,14 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
                                          ParticlePartial* __restrict__ part, const float* __restrict__ mlp_tab,
                                          float* __restrict__ log_x,
                                          float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
-                                         long long log_cap, unsigned long long* __restrict__ clk) {
+                                         long long log_cap, unsigned long long* __restrict__ clk,
+                                         uint4* __restrict__ defer_rec, uint32_t* __restrict__ defer_count) {
   __shared__ float4 hv[HN];
   __shared__ double shd[(NT / 32) * 9 + 9];
+  __shared__ int defer_flag;  // some particle of the tile is left to k_g2p_defer
+  // per thread, the deviatoric Hencky strain (6), its mean and the volumetric strain, parked
+  // during the Herschel-Bulkley return (with H_tr, parked over the dead H of the prefetch slot)
+  __shared__ float park[8 * NT];
   extern __shared__ float4 g2p_dyn[];  // prefetched inputs of two rounds
   float* pf = reinterpret_cast<float*>(g2p_dyn);
   const int tile = (int)rec.x, inst = (int)rec.y;
@@ -2234,6 +2290,7 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
   const int ty = (int)((ltile / D.tiles[2]) % D.tiles[1]);
   const int tx = (int)(ltile / ((int64_t)D.tiles[2] * D.tiles[1]));
   const int ox = tx * TX, oy = ty * TY, oz = tz * TZ;
+  if (threadIdx.x == 0) defer_flag = 0;
   for (int n = threadIdx.x; n < HN; n += NT) {
     const int hz = n % HZ, hy = (n / HZ) % HY, hx = n / (HZ * HY);
     const int gi = ox + hx, gj = oy + hy, gk = oz + hz;
@@ -2326,7 +2383,7 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
       const float dx2_inv = 4.0f / (dx * dx);
 #pragma unroll
       for (int a = 0; a < 9; ++a) Cm[a] *= dx2_inv;
-      speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      speed = particle_speed(v);
       disp = scaled_of(speed * dt, dx, D.pow2_inv_dx);
       m = in[PF_M * NT];
       v0 = in[PF_V0 * NT];
@@ -2360,7 +2417,21 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
             Htr[3 * i + j] = H[3 * i + j] + dt * (Cm[3 * i + j] + ch);
           }
         ys = pyield ? (double)in[PF_YS * NT] : D.yield;
-        paste_trial(Htr, D.mu, pt, o);
+        paste_trial<true>(Htr, D.mu, pt, o);
+        // park what the stress update needs after the return in shared memory, written and read
+        // back through volatile accesses so that it holds no registers during the FP64 Newton
+        volatile float* pk = pf + (r & 1) * PF_SLOTS * NT + threadIdx.x;  // this thread's prefetch slot
+#pragma unroll
+        for (int a = 0; a < 9; ++a) pk[(PF_H + a) * NT] = Htr[a];
+        volatile float* pd = park + threadIdx.x;
+        pd[0 * NT] = pt.dev.xx;
+        pd[1 * NT] = pt.dev.yy;
+        pd[2 * NT] = pt.dev.zz;
+        pd[3 * NT] = pt.dev.xy;
+        pd[4 * NT] = pt.dev.xz;
+        pd[5 * NT] = pt.dev.yz;
+        pd[6 * NT] = pt.mean;
+        pd[7 * NT] = pt.vol;
       } else {
         const float jm1 = in[PF_JM1 * NT];
         LiquidOut lo;
@@ -2383,8 +2454,28 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
     }
     if (paste) {
       long long nc = 0;
-      paste_finish(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, c.hb, D.tol, sigma0, pt, o, CLOCKS ? &nc : nullptr);
+      // paste_finish of the series path, split around the parked values
+      double scale = 1.0;
+      if (pt.path == PT_SERIES) scale = paste_return(pt.trial_eq, pt.dnorm, ys, c.hb, D.tol, sigma0, o,
+                                                     CLOCKS ? &nc : nullptr);
       if constexpr (CLOCKS) clk_newton += __reduce_max_sync(0xffffffffu, (unsigned)nc);  // the warp is converged
+      const volatile float* pk = pf + (r & 1) * PF_SLOTS * NT + threadIdx.x;
+      const volatile float* pd = park + threadIdx.x;
+      float Hr[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Hr[a] = pk[(PF_H + a) * NT];
+      if (pt.path == PT_SERIES && o.fail == F_OK) {
+        const Sym dev = {pd[0 * NT], pd[1 * NT], pd[2 * NT], pd[3 * NT], pd[4 * NT], pd[5 * NT]};
+        paste_stress(Hr, dev, pd[6 * NT], pd[7 * NT], (float)D.mu, (float)D.lambda, scale, o);
+      }
+      if (pt.path == PT_DEFER) {  // k_g2p_defer finishes it (paste_trial zeroed o's scalars)
+#pragma unroll
+        for (int a = 0; a < 9; ++a) o.H[a] = Hr[a];
+        o.tau[0] = __uint_as_float(DEFER_MARK);
+#pragma unroll
+        for (int a = 1; a < 6; ++a) o.tau[a] = 0.0f;
+        if (valid) defer_flag = 1;
+      }
 #pragma unroll
       for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
       if (valid) {
@@ -2418,8 +2509,8 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
     for (int a = 0; a < 6; ++a) nxt[(C_TAU + a) * cap + k] = tau[a];
     nxt[C_EP * cap + k] = ep;
     // momentum bound of the new state for the next attempt's fixed-point scale (its factors of
-    // 2.6 and 6 leave ample room for rounding)
-    bb += momentum_bound(m, speed, cn, tau, v0, c_tau, c_dx, c_g);
+    // 2.6 and 6 leave ample room for rounding); k_g2p_defer adds the deferred particles'
+    if (pt.path != PT_DEFER) bb += momentum_bound(m, speed, cn, tau, v0, c_tau, c_dx, c_g);
     mass_sum += (double)m;
     max_speed = fmaxf(max_speed, speed);
     max_disp = fmaxf(max_disp, disp);
@@ -2440,6 +2531,8 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
     P.iterations = (int)rv[6];
     P.yielded = (int)rv[7];
     P.fail_value = rv[8];
+    // the block reduction's barrier ordered every lane's write of defer_flag before this read
+    if (defer_flag) defer_rec[atomicAdd(defer_count, 1u)] = rec;
   }
   if constexpr (CLOCKS) {
     if ((threadIdx.x & 31) == 0) {
@@ -2460,13 +2553,111 @@ __global__ void __launch_bounds__(NT, MINB)
           const uint32_t* __restrict__ perm, const float4* __restrict__ vel, ParticlePartial* __restrict__ part, const float* __restrict__ mlp_tab,
           float* __restrict__ log_x, float* __restrict__ log_y, unsigned long long* __restrict__ log_n,
           long long log_cap, const uint4* __restrict__ tile_rec, const uint32_t* __restrict__ tile_count,
-          uint32_t* cursor, unsigned long long* __restrict__ clk) {
+          uint32_t* cursor, unsigned long long* __restrict__ clk, uint4* __restrict__ defer_rec,
+          uint32_t* __restrict__ defer_count) {
   __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
   for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
     g2p_tile<WARM, NT, CLOCKS>(tile_rec[i], desc, ctrl, st0, st1, id0, id1, cap, perm, vel, part, mlp_tab, log_x,
-                               log_y, log_n, log_cap, clk);
+                               log_y, log_n, log_cap, clk, defer_rec, defer_count);
     __syncthreads();  // the next tile reuses the shared memory
+  }
+}
+
+// The eigen-decomposition path of the paste update for the particles k_g2p left (DEFER_MARK in
+// the trial state's tau_xx): one CTA per listed tile, over the tile's slots in order.  It
+// finishes each such particle as k_g2p would have (the same paste_trial / warm start /
+// paste_finish on the stored H_tr, with the call of paste_update_jacobi) and adds their plastic
+// work, momentum bound, failure, Newton iterations and yield count to the tile's partial with a
+// fixed-order block reduction, so the result does not depend on which CTA took the tile.
+constexpr int G2P_DEFER_THREADS = 128;
+template <bool WARM>
+__global__ void __launch_bounds__(G2P_DEFER_THREADS)
+    k_g2p_defer(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, float* __restrict__ st0,
+                float* __restrict__ st1, int64_t cap, ParticlePartial* __restrict__ part,
+                const float* __restrict__ mlp_tab, float* __restrict__ log_x, float* __restrict__ log_y,
+                unsigned long long* __restrict__ log_n, long long log_cap, const uint4* __restrict__ defer_rec,
+                const uint32_t* __restrict__ defer_count) {
+  constexpr int NT = G2P_DEFER_THREADS;
+  __shared__ double shd[(NT / 32) * 6 + 6];
+  const uint32_t n = *defer_count;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint4 rec = defer_rec[i];
+    const int tile = (int)rec.x, inst = (int)rec.y;
+    const Control& c = ctrl[inst];
+    const InstDesc& D = desc[inst];
+    float* nxt = c.parity ? st0 : st1;  // the trial state k_g2p wrote
+    const bool use_mlp = WARM && c.warm_start && mlp_tab != nullptr;
+    const float2* tab =
+        use_mlp ? reinterpret_cast<const float2*>(mlp_tab + (int64_t)inst * MLP_TAB_FLOATS + MLP_TAB_STRIDE) : nullptr;
+    const float inv_k = (float)(1.0 / D.consistency);
+    const float c_tau = (float)(D.max_dt * 4.0 / (D.dx * D.dx));
+    const float c_dx = (float)(2.6 * D.dx);
+    const float c_g =
+        (float)(6.0 * sqrt(D.gravity[0] * D.gravity[0] + D.gravity[1] * D.gravity[1] + D.gravity[2] * D.gravity[2]) *
+                D.max_dt);
+    double diss = 0.0, bb = 0.0, fail_value = 0.0;
+    int fail = F_OK, iters = 0, yielded = 0;
+    for (int64_t k = (int64_t)rec.z + threadIdx.x; k < (int64_t)rec.w; k += NT) {
+      if (__float_as_uint(nxt[C_TAU * cap + k]) != DEFER_MARK) continue;
+      float Htr[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Htr[a] = nxt[(C_H + a) * cap + k];
+      const double ys = D.per_particle_yield ? (double)nxt[C_YS * cap + k] : D.yield;
+      PasteTrial pt;
+      PasteOut o;
+      paste_trial<false>(Htr, D.mu, pt, o);
+      double sigma0 = -1.0;
+      if (use_mlp && pt.path != PT_DONE && pt.trial_eq > ys && pt.trial_eq > 0.0) {
+        const float t = mlp_table_fraction(tab, hb_la8(inv_k, pt.trial_eq, ys));
+        if (t > 0.0f && t < 1.0f) sigma0 = ys + (double)t * (pt.trial_eq - ys);
+      }
+      paste_finish<false>(Htr, (float)D.mu, (float)D.lambda, D.mu, ys, c.hb, D.tol, sigma0, pt, o);
+      if (o.fail != F_OK) {
+        fail = max(fail, o.fail);
+        fail_value = o.eq;
+      }
+#pragma unroll
+      for (int a = 0; a < 9; ++a) nxt[(C_H + a) * cap + k] = o.H[a];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) nxt[(C_TAU + a) * cap + k] = o.tau[a];
+      nxt[C_EP * cap + k] += (float)o.dep;
+      const float v0 = nxt[C_V0 * cap + k], m = nxt[C_M * cap + k];
+      diss += o.diss_density * (double)v0;
+      iters += o.iters;
+      yielded += o.yielded;
+      if (log_n != nullptr && o.yielded && o.fail == F_OK) {
+        const unsigned long long slot = atomicAdd(log_n, 1ull);
+        if ((long long)slot < log_cap) {
+          log_x[6 * slot + 0] = (float)o.trial;
+          log_x[6 * slot + 1] = (float)ys;
+          log_x[6 * slot + 2] = (float)D.consistency;
+          log_x[6 * slot + 3] = (float)D.flow_index;
+          log_x[6 * slot + 4] = (float)D.mu;
+          log_x[6 * slot + 5] = (float)c.dt;
+          log_y[slot] = (float)o.eq;
+        }
+      }
+      // the momentum bound k_g2p left out, from the stored velocity and affine field
+      float v[3], Cm[9];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) v[a] = nxt[(C_V + a) * cap + k];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Cm[a] = nxt[(C_C + a) * cap + k];
+      bb += momentum_bound(m, particle_speed(v), affine_norm(Cm), o.tau, v0, c_tau, c_dx, c_g);
+    }
+    double rv[6] = {diss, bb, (double)fail, (double)iters, (double)yielded, fail_value};
+    block_reduce_multi_to0<NT, 6>(rv, (1u << 2) | (1u << 5), shd);
+    if (threadIdx.x == 0) {
+      ParticlePartial& P = part[tile];
+      P.diss += rv[0];
+      P.bbound += rv[1];
+      P.fail = max(P.fail, (int)rv[2]);
+      P.iterations += (int)rv[3];
+      P.yielded += (int)rv[4];
+      P.fail_value = fmax(P.fail_value, rv[5]);
+    }
+    __syncthreads();  // shd is reused by the next tile
   }
 }
 
@@ -2704,7 +2895,7 @@ __global__ void k_state_stats(const InstDesc* __restrict__ desc, const Control* 
     const float m = cur[C_M * cap + k], v0 = cur[C_V0 * cap + k];
     // the same FP32 expressions as the end of k_g2p, so that a state imported from a
     // checkpoint gets the same speed and per-particle bound as the run that wrote it
-    const float speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const float speed = particle_speed(v);
     const float c_tau = (float)(D.max_dt * 4.0 / (D.dx * D.dx));
     const float c_dx = (float)(2.6 * D.dx);
     const float c_g =
@@ -3080,7 +3271,7 @@ static void launch_g2p(const DeviceArrays& A, bool warm, cudaStream_t s) {
   const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[v][warm ? 1 : 0]);
 #define LP_G2P_ARGS                                                                                               \
   A.desc, A.ctrl, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.perm, A.vel, A.tpart, tab, A.log_x, A.log_y, \
-      A.log_n, A.log_cap, A.tile_rec, A.tile_count, cur, A.g2p_clk
+      A.log_n, A.log_cap, A.tile_rec, A.tile_count, cur, A.g2p_clk, A.defer_rec, A.nw_count + 5
 #define LP_G2P_LAUNCH(T, MB, CLK, N) \
   (warm ? k_g2p<true, T, MB, CLK> : k_g2p<false, T, MB, CLK>)<<<N, T, g2p_smem(T), s>>>(LP_G2P_ARGS)
   if (A.g2p_clk) {  // measurement of the return's share of G2P warp time (256-thread CTAs)
@@ -3096,6 +3287,12 @@ static void launch_g2p(const DeviceArrays& A, bool warm, cudaStream_t s) {
   }
 #undef LP_G2P_LAUNCH
 #undef LP_G2P_ARGS
+}
+// the particles G2P left to the eigen-decomposition pass (normally none: every CTA exits at once)
+static void launch_g2p_defer(const DeviceArrays& A, bool warm, cudaStream_t s) {
+  (warm ? k_g2p_defer<true> : k_g2p_defer<false>)<<<(unsigned)g_sms, G2P_DEFER_THREADS, 0, s>>>(
+      A.desc, A.ctrl, A.st[0], A.st[1], A.cap, A.tpart, warm ? A.mlp_tab : nullptr, A.log_x, A.log_y, A.log_n,
+      A.log_cap, A.defer_rec, A.nw_count + 5);
 }
 uint64_t kernel_launch_count() { return g_launches; }
 void add_kernel_launches(uint64_t n) { g_launches += n; }
@@ -3166,6 +3363,9 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
     if (ev) cudaEventRecord(ev[n], s);
   }
   launch_g2p(A, warm_g2p, s);
+  ++n;
+  if (ev) cudaEventRecord(ev[n], s);
+  launch_g2p_defer(A, warm_g2p, s);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   k_segments<<<(unsigned)A.n_seg, 256, 0, s>>>(A.ctrl, A.segs, A.gpart, A.tpart, A.seg);
@@ -3247,12 +3447,12 @@ int launch_attempt(const DeviceArrays& A, cudaStream_t s) { return attempt_seque
 const char* attempt_kernel_name(int k, int any_pellet, int any_bed, int warm) {
   static const char* a[] = {"k_begin", "k_bin_count", "k_scan_instances", "k_scan_apply", "k_bin_scatter",
                             "k_tiles", "k_bin_sort", "k_p2g", "k_traction", "k_grid_update", "k_couple",
-                            "k_bed_bin", "k_bed_couple", "k_bed_step", "k_mlp_table", "k_g2p", "k_segments",
-                            "k_end"};
+                            "k_bed_bin", "k_bed_couple", "k_bed_step", "k_mlp_table", "k_g2p", "k_g2p_defer",
+                            "k_segments", "k_end"};
   if (!any_pellet && k >= 10) ++k;
   if (!any_bed && k >= 11) k += 3;
   if (!warm && k >= 14) ++k;
-  return k < 18 ? a[k] : "?";
+  return k < 19 ? a[k] : "?";
 }
 
 int launch_state_stats(const DeviceArrays& A, cudaStream_t s) {

@@ -47,9 +47,11 @@ struct DeviceArrays {
   uint32_t* perm = nullptr;
   uint32_t* nw_list = nullptr;
   uint32_t* nw_count = nullptr;    // [0] near-wall particles, [1] occupied tiles of the attempt,
-                                   // [2..4] tile cursors of the bin sort, P2G and G2P
+                                   // [2..4] tile cursors of the bin sort, P2G and G2P,
+                                   // [5] tiles listed in defer_rec
   uint32_t* tile_count = nullptr;  // = nw_count + 1
   uint4* tile_rec = nullptr;       // occupied tiles of the attempt: (tile, instance, first slot, end slot)
+  uint4* defer_rec = nullptr;      // tiles whose particles k_g2p left to the eigen-decomposition pass
   long long* acc = nullptr;   // 4 x node_total: mass, momentum xyz (int64 fixed point)
   long long* trac = nullptr;  // 6 x node_total: reactions per axis, low faces then high faces
   int64_t node_total = 0;
@@ -84,7 +86,7 @@ struct DeviceArrays {
 
 // One substep attempt for every active instance; returns the number of kernels launched.
 int launch_attempt(const DeviceArrays& A, cudaStream_t s);
-// same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 19 events)
+// same, recording ev[0] before the first kernel and ev[k] after kernel k (at most 20 events)
 int launch_attempt(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* ev);
 const char* attempt_kernel_name(int k, int any_pellet, int any_bed, int warm);
 // Energy audit of one forced-dt trial: a transport pass (binning + APIC-only deposit) and the

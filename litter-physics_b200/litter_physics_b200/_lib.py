@@ -88,6 +88,8 @@ def lib():
         "lp_sim_particle_count": ([P, C.POINTER(U64)], I32),
         "lp_sim_export_particles": ([P, C.POINTER(_abi.Particles)], I32),
         "lp_sim_import_particles": ([P, C.POINTER(_abi.Particles)], I32),
+        "lp_host_pin": ([P, U64], I32),
+        "lp_host_unpin": ([P], I32),
         "lp_sim_get_pellet": ([P, C.POINTER(_abi.Pellet), C.POINTER(I32)], I32),
         "lp_sim_set_pellet": ([P, C.POINTER(_abi.Pellet)], I32),
         "lp_sim_get_pellets": ([P, C.POINTER(_abi.Pellet), I32, C.POINTER(I32)], I32),

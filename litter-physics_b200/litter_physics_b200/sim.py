@@ -289,6 +289,39 @@ class Simulation:
         return x[: n.value], y[: n.value]
 
 
+class PinnedParticles:
+    """Page-locks the arrays of a resident host particle set (lp_host_pin) until close().
+
+    Export and import then move them by DMA straight between host and device, without the
+    library's staging copy.  Pin a set once and reuse it: page-locking is itself costly."""
+
+    def __init__(self, arrays: dict):
+        self.arrays = arrays
+        self._pinned = []
+        try:
+            for a in arrays.values():
+                if a is None or a.nbytes == 0:
+                    continue
+                if not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError("pinned particle arrays must be C-contiguous")
+                check(lib().lp_host_pin(a.ctypes.data, a.nbytes))
+                self._pinned.append(a)
+        except Exception:
+            self.close()
+            raise
+
+    def close(self) -> None:
+        while self._pinned:
+            a = self._pinned.pop()
+            check(lib().lp_host_unpin(a.ctypes.data))
+
+    def __enter__(self):
+        return self.arrays
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class Batch:
     """Many independent simulations advanced by one device launch sequence (extension)."""
 
