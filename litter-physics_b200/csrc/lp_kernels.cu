@@ -2304,10 +2304,30 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
   const float inv_k = (float)(1.0 / D.consistency);
   const float dx = (float)D.dx;
   const float dt = (float)c.dt;
-  double diss = 0.0, bb = 0.0, mass_sum = 0.0;
-  float max_speed = 0.0f, max_disp = 0.0f;
-  int fail = F_OK, iters = 0, yielded = 0;
-  double fail_value = 0.0;
+  // this thread's sums over its particles of the tile, kept in shared memory (through volatile
+  // accesses) instead of registers: each is touched once per round, and the registers are worth
+  // more to the FP64 return
+  __shared__ double acc_d[4 * NT];  // plastic work, momentum bound, mass, failure value
+  __shared__ float acc_f[2 * NT];   // largest speed, largest displacement
+  __shared__ int acc_i[3 * NT];     // failure code, Newton iterations, yielded particles
+  volatile double& diss = acc_d[threadIdx.x];
+  volatile double& bb = acc_d[NT + threadIdx.x];
+  volatile double& mass_sum = acc_d[2 * NT + threadIdx.x];
+  volatile double& fail_value = acc_d[3 * NT + threadIdx.x];
+  volatile float& max_speed = acc_f[threadIdx.x];
+  volatile float& max_disp = acc_f[NT + threadIdx.x];
+  volatile int& fail = acc_i[threadIdx.x];
+  volatile int& iters = acc_i[NT + threadIdx.x];
+  volatile int& yielded = acc_i[2 * NT + threadIdx.x];
+  diss = 0.0;
+  bb = 0.0;
+  mass_sum = 0.0;
+  fail_value = 0.0;
+  max_speed = 0.0f;
+  max_disp = 0.0f;
+  fail = F_OK;
+  iters = 0;
+  yielded = 0;
   const float c_tau = (float)(D.max_dt * 4.0 / (D.dx * D.dx));
   const float c_dx = (float)(2.6 * D.dx);
   const float c_g =
@@ -2439,7 +2459,7 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
 #pragma unroll
         for (int a = 0; a < 6; ++a) tau[a] = lo.tau[a];
         if (valid) {
-          if (lo.fail != F_OK) fail = max(fail, lo.fail);
+          if (lo.fail != F_OK) fail = max((int)fail, lo.fail);
           nxt[C_JM1 * cap + k] = lo.jm1;
         }
       }
@@ -2480,15 +2500,15 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
       for (int a = 0; a < 6; ++a) tau[a] = o.tau[a];
       if (valid) {
         if (o.fail != F_OK) {
-          fail = max(fail, o.fail);
+          fail = max((int)fail, o.fail);
           fail_value = o.eq;
         }
 #pragma unroll
         for (int a = 0; a < 9; ++a) nxt[(C_H + a) * cap + k] = o.H[a];
         ep += (float)o.dep;
-        diss += o.diss_density * (double)v0;
-        iters += o.iters;
-        yielded += o.yielded;
+        diss = diss + o.diss_density * (double)v0;
+        iters = iters + o.iters;
+        yielded = yielded + o.yielded;
         if (log_n != nullptr && o.yielded && o.fail == F_OK) {
           const unsigned long long slot = atomicAdd(log_n, 1ull);
           if ((long long)slot < log_cap) {
@@ -2510,8 +2530,8 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
     nxt[C_EP * cap + k] = ep;
     // momentum bound of the new state for the next attempt's fixed-point scale (its factors of
     // 2.6 and 6 leave ample room for rounding); k_g2p_defer adds the deferred particles'
-    if (pt.path != PT_DEFER) bb += momentum_bound(m, speed, cn, tau, v0, c_tau, c_dx, c_g);
-    mass_sum += (double)m;
+    if (pt.path != PT_DEFER) bb = bb + momentum_bound(m, speed, cn, tau, v0, c_tau, c_dx, c_g);
+    mass_sum = mass_sum + (double)m;
     max_speed = fmaxf(max_speed, speed);
     max_disp = fmaxf(max_disp, disp);
   }
@@ -3211,6 +3231,11 @@ void configure_kernels() {
   for (int v = 0; v < 4; ++v)
     for (int w = 0; w < 2; ++w)
       cudaFuncSetAttribute(g2p[v][w], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem(g2p_threads(v)));
+  // the clock-instrumented instantiations of the return-share measurement
+  const void* g2p_clk[2] = {(const void*)k_g2p<false, G2P_THREADS, 2, true>,
+                            (const void*)k_g2p<true, G2P_THREADS, 2, true>};
+  for (const void* f : g2p_clk)
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem(G2P_THREADS));
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return;

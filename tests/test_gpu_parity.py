@@ -342,3 +342,81 @@ def test_export_in_place_matches_a_fresh_export(lib_built):
     for k, v in fresh.items():
         assert np.array_equal(host[k], v), k
     sim.close()
+
+
+def test_large_strain_particles_take_the_eigen_pass(lib_built):
+    """Particles whose trial strain is outside the series path (||F F^T - I|| > 0.25) are left by
+    G2P to the eigen-decomposition pass: a developed slump where every fifth particle carries a
+    large rotated stretch matches the oracle's update_paste (constitutive.rs:456-531, Jacobi
+    373-425) for 5 substeps, and the run is bitwise repeatable (fixed-order tile partials)."""
+    import oracle
+    from litter_physics_b200.sim import Simulation
+
+    spec = small_slump()
+    sim = Simulation(spec)
+    sim.advance_to(30 * spec.max_dt)
+    state = sim.particles()
+    n = len(state["id"])
+    rng = np.random.default_rng(11)
+    big = np.arange(0, n, 5)
+    for i in big:
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        f = q @ np.diag(rng.uniform(1.15, 1.35, 3) * np.array([1.0, 0.8, 0.9])) @ q.T
+        state["deformation"][i] = f.astype(np.float32).astype(np.float64).reshape(-1)
+    state["deformation"] = np.ascontiguousarray(state["deformation"])
+    b = state["deformation"].reshape(-1, 3, 3)
+    bn = np.linalg.norm(b[big] @ b[big].transpose(0, 2, 1) - np.eye(3), axis=(1, 2))
+    assert bn.min() > 0.3  # all of them need the eigenvectors
+    steps = 5
+    runs = []
+    for _ in range(2):
+        g = Simulation(spec)
+        g.set_particles(state)
+        g.set_ledger(sim.ledger)
+        g.set_counters(sim.counters)
+        g.advance_to(sim.time + steps * spec.max_dt)
+        runs.append(g)
+    ref = oracle.OracleSim(spec)
+    ref.set_particles(state)
+    ref.set_ledger(sim.ledger)
+    ref.set_counters(sim.counters)
+    ref.advance_to(sim.time + steps * spec.max_dt)
+    gp, rp = by_id(runs[0].particles()), by_id(ref.particles())
+    assert runs[0].counters.step_count == ref.counters.step_count
+    err = compare(gp, rp, float(spec.domain[0]))
+    f_err = np.abs(gp["deformation"] - rp["deformation"]).max()
+    print(f"large strain: x {err['x']:.2e}, v {err['v']:.2e}, F {f_err:.2e}")
+    assert err["x"] <= POS_TOL and err["v"] <= VEL_TOL
+    assert f_err <= 1e-5
+    led_g, led_r = runs[0].ledger, ref.ledger
+    assert math.isclose(led_g.plastic_dissipation, led_r.plastic_dissipation, rel_tol=1e-4)
+    again = by_id(runs[1].particles())
+    for k in ("position", "velocity", "deformation", "kirchhoff", "plastic_strain"):
+        assert np.array_equal(gp[k], again[k]), k
+    assert bytes(runs[0].ledger) == bytes(runs[1].ledger)
+
+
+def test_page_locked_import_and_export_match_the_staged_path(lib_built):
+    """Export into and import from page-locked host arrays (lp_host_pin, moved by DMA) give
+    bit for bit what the staged path gives for pageable arrays."""
+    from litter_physics_b200.sim import PinnedParticles, Simulation
+
+    spec = small_slump()
+    sim = Simulation(spec)
+    sim.advance_to(10 * spec.max_dt)
+    fresh = sim.particles()
+    host = {k: np.full_like(v, 7) for k, v in fresh.items()}
+    with PinnedParticles(host) as pinned:
+        sim.particles(out=pinned)
+        for k, v in fresh.items():
+            assert np.array_equal(pinned[k], v), k
+        a, b = Simulation(spec), Simulation(spec)
+        a.set_particles(fresh)
+        b.set_particles(pinned)
+        pa, pb = a.particles(), b.particles()
+        for k in fresh:
+            assert np.array_equal(pa[k], pb[k]), k
+        a.advance_to(5 * spec.max_dt)
+        b.advance_to(5 * spec.max_dt)
+        assert np.array_equal(by_id(a.particles())["position"], by_id(b.particles())["position"])
+    sim.close()
