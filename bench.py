@@ -352,7 +352,7 @@ def config_measurement(name: str, spec, args, stream, torch, develop: int) -> di
     sim.sync()
     snap, led, cnt = sim.particles(), sim.ledger, sim.counters
     tune = None if args.no_autotune else sim.autotune(16)
-    sim.set_particles(snap)  # the tuning attempts advanced the run: time from the developed state
+    sim.set_particles(snap)  # the developed state (the autotuner puts it back too)
     sim.set_ledger(led)
     sim.set_counters(cnt)
     sim.run_substeps(args.warmup)
@@ -435,7 +435,8 @@ def ours(args, ws, rank, local):
         sim.set_launch_shape(**{k: int(v) for k, v in (kv.split("=") for kv in args.launch_shape.split(","))})
     elif not args.no_autotune:
         # the launch shape for the headline (warm-started) arm, picked on the developed column;
-        # the tuning attempts advance it, so the timed arms start again from the snapshot
+        # the autotuner times each candidate from this state and puts it back; each timed arm
+        # starts again from the snapshot all the same
         sim.set_warm_start(weights)
         tune_report = sim.autotune(16)
         sim.sync()

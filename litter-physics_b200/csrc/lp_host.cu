@@ -756,6 +756,8 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   A.n_inst = count;
   A.any_pellet = any_pellet;
   A.any_bed = any_bed;
+  A.kinds = 0;
+  for (int i = 0; i < count; ++i) A.kinds |= E.desc[i].kind == 0 ? 1 : 2;
   A.n_bed = bed_off;
   A.cap = slot_off;
   A.n_pcta = (int64_t)pcta_inst.size();
@@ -968,31 +970,79 @@ static std::string shape_text(const lp_launch_shape& s) {
 // Coordinate search over the launch shape on the live ensemble: one knob at a time (tile
 // scheduling, G2P block shape and CTAs per SM, P2G chunk and CTAs per SM, attempts per graph
 // replay), each candidate timed over trial_steps attempts with CUDA events after two untimed
-// ones, keeping the fastest value before moving to the next knob.  The attempts are real steps:
-// time advances and every accepted step is a valid step of the trajectory, so the work per
-// attempt drifts while the search runs (a collapsing column yields more from step to step).
-// Each candidate is therefore compared with the incumbent timed right before and right after it
-// (the mean of the two), which cancels a drift that is linear over the three timings.  Every
-// candidate gives the same results (the tile kernels' results do not depend on these choices),
-// so only the speed differs.
+// ones, keeping the fastest value before moving to the next knob.  The attempts are real steps,
+// and the work per attempt changes as the trajectory moves on (a collapsing column yields more
+// from step to step), so every candidate starts from the same state: the ensemble's device
+// state (both particle buffers and ids, the control blocks, the pellet-bed buffers) is copied
+// aside once and put back before each candidate and at the end.  Every candidate then runs the
+// same attempts, and since the tile kernels' results do not depend on the launch shape, only the
+// speed differs; tuning leaves the simulation where it found it.  A candidate replaces the
+// incumbent only when it is faster by more than the timing noise (TUNE_MARGIN).
 static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t report_len) {
+  constexpr float TUNE_MARGIN = 0.005f;
   if (trial_steps < 1) return set_error(LP_INVALID, "trial_steps must be at least 1");
+  lp_status st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const std::vector<Control> ctrl_before = E.ctrl_h;  // the caller's targets, put back at the end
   if (E.ctrl_h.empty() || !std::isinf(E.ctrl_h[0].target)) {
-    lp_status st = set_targets(E, std::numeric_limits<double>::infinity(), true);
+    st = set_targets(E, std::numeric_limits<double>::infinity(), true);
     if (st != LP_OK) return st;
   }
+  // the device state every candidate starts from; the control blocks are kept on the host and
+  // put back with the attempt epoch left advanced, so that node blocks marked by a tuning attempt
+  // never look active to a later one
+  st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  const std::vector<Control> ctrl_start = E.ctrl_h;
+  lp::DeviceArrays& A = E.A;
+  std::vector<std::pair<void*, size_t>> live = {
+      {A.st[0], sizeof(float) * (size_t)lp::NCOMP * A.cap}, {A.st[1], sizeof(float) * (size_t)lp::NCOMP * A.cap},
+      {A.id[0], sizeof(uint32_t) * (size_t)A.cap},           {A.id[1], sizeof(uint32_t) * (size_t)A.cap}};
+  if (A.any_bed)
+    for (int b = 0; b < 2; ++b) {
+      live.push_back({A.bed.state[b], sizeof(lp::PelletState) * (size_t)A.n_bed});
+      live.push_back({A.bed.hist[b], sizeof(lp::HmContact) * (size_t)A.n_bed * lp::HM_SLOTS});
+      live.push_back({A.bed.hist_n[b], sizeof(int) * (size_t)A.n_bed});
+    }
+  size_t total = 0;
+  for (auto& l : live) total += (l.second + 255) & ~(size_t)255;
+  char* saved = nullptr;
+  if (cudaMalloc(&saved, total) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(LP_DEVICE, "autotune needs device memory for a copy of the ensemble's state");
+  }
+  auto copy_state = [&](bool restore) -> lp_status {
+    size_t off = 0;
+    for (auto& l : live) {
+      void* dst = restore ? l.first : (void*)(saved + off);
+      const void* src = restore ? (const void*)(saved + off) : l.first;
+      CUDA_CK(cudaMemcpyAsync(dst, src, l.second, cudaMemcpyDeviceToDevice, E.stream));
+      off += (l.second + 255) & ~(size_t)255;
+    }
+    if (!restore) return LP_OK;
+    lp_status r = pull_ctrl(E);
+    if (r != LP_OK) return r;
+    for (int i = 0; i < E.n; ++i) {
+      const int epoch = E.ctrl_h[i].epoch;
+      E.ctrl_h[i] = ctrl_start[i];
+      E.ctrl_h[i].epoch = epoch;
+    }
+    return push_ctrl(E);
+  };
   int lim[lp::LAUNCH_LIMITS];
   lp::launch_shape_limits(lim);
   lp_launch_shape best;
-  lp_status st = get_launch_shape(E, &best);
-  if (st != LP_OK) return st;
+  st = get_launch_shape(E, &best);
   best.g2p_per_sm = best.p2g_per_sm = 0;  // 0: as many as fit
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  CUDA_CK(cudaEventCreate(&e0));
-  CUDA_CK(cudaEventCreate(&e1));
+  if (st == LP_OK && cudaEventCreate(&e0) != cudaSuccess) st = set_error(LP_DEVICE, "cudaEventCreate failed");
+  if (st == LP_OK && cudaEventCreate(&e1) != cudaSuccess) st = set_error(LP_DEVICE, "cudaEventCreate failed");
+  if (st == LP_OK) st = copy_state(false);
   std::string rep;
   auto measure = [&](const lp_launch_shape& s, float* ms_per_attempt) -> lp_status {
-    lp_status r = set_launch_shape(E, &s);
+    lp_status r = copy_state(true);
+    if (r != LP_OK) return r;
+    r = set_launch_shape(E, &s);
     if (r != LP_OK) return r;
     const int per = std::max(1, s.graph_attempts);
     const int reps = std::max(1, trial_steps / per);
@@ -1012,8 +1062,8 @@ static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t
     *ms_per_attempt = ms / (float)(reps * per);
     return LP_OK;
   };
-  float best_ms = 0.f;  // the incumbent's latest timing
-  st = measure(best, &best_ms);
+  float best_ms = 0.f;
+  if (st == LP_OK) st = measure(best, &best_ms);
   if (st == LP_OK) rep += shape_text(best) + " ms_per_attempt=" + std::to_string(best_ms) + "\n";
   // one knob at a time; each candidate list holds complete field values for that knob
   struct Knob {
@@ -1035,23 +1085,34 @@ static lp_status autotune(Ensemble& E, int32_t trial_steps, char* report, size_t
       else if (kb.which == 2) c.p2g_variant = v[0], c.p2g_per_sm = v[1];
       else c.graph_attempts = v[0];
       if (std::memcmp(&c, &best, sizeof(c)) == 0) continue;  // measured already
-      float ms = 0.f, after = 0.f;
+      float ms = 0.f;
       st = measure(c, &ms);
-      if (st == LP_OK) st = measure(best, &after);
       if (st != LP_OK) break;
-      const float ref = 0.5f * (best_ms + after);  // the incumbent at the candidate's time
-      rep += shape_text(c) + " ms_per_attempt=" + std::to_string(ms) + " incumbent=" + std::to_string(ref) + "\n";
-      if (ms < ref) {
+      rep += shape_text(c) + " ms_per_attempt=" + std::to_string(ms) + " incumbent=" + std::to_string(best_ms) + "\n";
+      if (ms < (1.0f - TUNE_MARGIN) * best_ms) {
         best = c;
-        st = measure(best, &best_ms);  // the new incumbent, timed next to the following candidate
-        if (st != LP_OK) break;
-      } else {
-        best_ms = after;
+        best_ms = ms;
       }
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  // back to the state and targets tuning found
+  if (saved) {
+    const lp_status r = copy_state(true);
+    if (st == LP_OK) st = r;
+    cudaStreamSynchronize(E.stream);
+    cudaFree(saved);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st != LP_OK) return st;
+  st = pull_ctrl(E);
+  if (st != LP_OK) return st;
+  for (int i = 0; i < E.n; ++i) {
+    E.ctrl_h[i].target = ctrl_before[i].target;
+    E.ctrl_h[i].status = ctrl_before[i].status;
+    E.ctrl_h[i].forced_dt = ctrl_before[i].forced_dt;
+  }
+  st = push_ctrl(E);
   if (st != LP_OK) return st;
   st = set_launch_shape(E, &best);
   if (st != LP_OK) return st;

@@ -2228,7 +2228,12 @@ constexpr uint32_t DEFER_MARK = 0x7fc0defeu;  // a quiet NaN payload that no ari
 // solver): every warp adds its clock64 cycles in the tile to clk[0] and, per round, the longest
 // lane time in the Herschel-Bulkley return to clk[1], so clk[1] / clk[0] is the share of warp
 // time the return takes.
-template <bool WARM, int NT, bool CLOCKS>
+// Material kinds a G2P instantiation handles: paste only, liquid only, or both (an ensemble whose
+// instances mix them).  The single-kind instantiations carry no code of the other kind's update,
+// which keeps the kernel small (its instruction fetch, not its arithmetic, limits it).
+enum G2pKind : int { G2P_PASTE = 0, G2P_LIQUID = 1, G2P_MIXED = 2 };
+
+template <bool WARM, int NT, bool CLOCKS, int KIND>
 __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __restrict__ desc,
                                          const Control* __restrict__ ctrl, float* __restrict__ st0, float* __restrict__ st1,
                                          uint32_t* __restrict__ id0, uint32_t* __restrict__ id1, int64_t cap,
@@ -2239,7 +2244,6 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
                                          long long log_cap, unsigned long long* __restrict__ clk,
                                          uint4* __restrict__ defer_rec, uint32_t* __restrict__ defer_count) {
   __shared__ float4 hv[HN];
-  __shared__ double shd[(NT / 32) * 9 + 9];
   __shared__ int defer_flag;  // some particle of the tile is left to k_g2p_defer
   // per thread, the deviatoric Hencky strain (6), its mean and the volumetric strain, parked
   // during the Herschel-Bulkley return (with H_tr, parked over the dead H of the prefetch slot)
@@ -2269,7 +2273,8 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
   float* nxt = c.parity ? st0 : st1;
   const uint32_t* idc = c.parity ? id1 : id0;
   uint32_t* idn = c.parity ? id0 : id1;
-  const bool paste = D.kind == 0, pyield = paste && D.per_particle_yield;
+  const bool paste = KIND == G2P_PASTE || (KIND == G2P_MIXED && D.kind == 0);
+  const bool pyield = paste && D.per_particle_yield;
   const int nround = (int)((e0 - s0 + NT - 1) / NT);
   // slot of this thread in round r (clamped to the tile's last particle) and warp liveness
   auto slot_of = [&](int r) -> int64_t {
@@ -2536,22 +2541,37 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
     max_disp = fmaxf(max_disp, disp);
   }
   cp_async_wait<0>();  // no copy may land after the CTA's shared memory is released
-  double rv[9] = {diss, bb, mass_sum, (double)max_speed, (double)max_disp, (double)fail, (double)iters,
-                  (double)yielded, fail_value};
-  // thread 0 writes the tile's partial; shd is next written after the tile-end barrier
-  block_reduce_multi_to0<NT, 9>(rv, (1u << 3) | (1u << 4) | (1u << 5) | (1u << 8), shd);
+  // the tile's sums: a fixed pairwise tree over the threads' shared-memory sums (deterministic,
+  // and a short loop instead of an unrolled shuffle reduction)
+  __syncthreads();
+#pragma unroll 1
+  for (int h = NT / 2; h > 0; h >>= 1) {
+    const int a = threadIdx.x, b = threadIdx.x + h;
+    if (a < h) {
+      acc_d[a] += acc_d[b];
+      acc_d[NT + a] += acc_d[NT + b];
+      acc_d[2 * NT + a] += acc_d[2 * NT + b];
+      acc_d[3 * NT + a] = fmax(acc_d[3 * NT + a], acc_d[3 * NT + b]);
+      acc_f[a] = fmaxf(acc_f[a], acc_f[b]);
+      acc_f[NT + a] = fmaxf(acc_f[NT + a], acc_f[NT + b]);
+      acc_i[a] = max(acc_i[a], acc_i[b]);
+      acc_i[NT + a] += acc_i[NT + b];
+      acc_i[2 * NT + a] += acc_i[2 * NT + b];
+    }
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     ParticlePartial& P = part[tile];
-    P.diss = rv[0];
-    P.bbound = rv[1];
-    P.mass = rv[2];
-    P.max_speed = (float)rv[3];
-    P.max_disp = (float)rv[4];
-    P.fail = (int)rv[5];
-    P.iterations = (int)rv[6];
-    P.yielded = (int)rv[7];
-    P.fail_value = rv[8];
-    // the block reduction's barrier ordered every lane's write of defer_flag before this read
+    P.diss = acc_d[0];
+    P.bbound = acc_d[NT];
+    P.mass = acc_d[2 * NT];
+    P.max_speed = acc_f[0];
+    P.max_disp = acc_f[NT];
+    P.fail = acc_i[0];
+    P.iterations = acc_i[NT];
+    P.yielded = acc_i[2 * NT];
+    P.fail_value = acc_d[3 * NT];
+    // the tree's barriers ordered every lane's write of defer_flag before this read
     if (defer_flag) defer_rec[atomicAdd(defer_count, 1u)] = rec;
   }
   if constexpr (CLOCKS) {
@@ -2566,7 +2586,7 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
 // walk the attempt's list of occupied tiles; the partial results are per tile, so they do not
 // depend on which CTA took which tile.  Both block shapes hold 16 warps per SM at the 128
 // registers a thread needs.
-template <bool WARM, int NT, int MINB = 512 / NT, bool CLOCKS = false>
+template <bool WARM, int NT, int MINB = 512 / NT, bool CLOCKS = false, int KIND = G2P_MIXED>
 __global__ void __launch_bounds__(NT, MINB)
     k_g2p(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl, float* __restrict__ st0,
           float* __restrict__ st1, uint32_t* __restrict__ id0, uint32_t* __restrict__ id1, int64_t cap,
@@ -2578,7 +2598,7 @@ __global__ void __launch_bounds__(NT, MINB)
   __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
   for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
-    g2p_tile<WARM, NT, CLOCKS>(tile_rec[i], desc, ctrl, st0, st1, id0, id1, cap, perm, vel, part, mlp_tab, log_x,
+    g2p_tile<WARM, NT, CLOCKS, KIND>(tile_rec[i], desc, ctrl, st0, st1, id0, id1, cap, perm, vel, part, mlp_tab, log_x,
                                log_y, log_n, log_cap, clk, defer_rec, defer_count);
     __syncthreads();  // the next tile reuses the shared memory
   }
@@ -3207,7 +3227,29 @@ static inline unsigned grid_of(int64_t n, int t) { return (unsigned)((n + t - 1)
 // the defaults are the B200 figures) and the SM count.
 static int g_sms = 148, g_sort_per_sm = 16;
 static int g_p2g_per_sm[P2G_VARIANTS] = {2, 2, 2};  // [p2g_variant]
-static int g_g2p_per_sm[G2P_VARIANTS][2] = {{2, 2}, {4, 4}, {5, 5}, {6, 6}};  // [g2p_variant][warm]
+// [kind][g2p_variant][warm] (mixed-kind ensembles run the 256-thread instantiation, variant 0)
+static int g_g2p_per_sm[3][G2P_VARIANTS][2] = {{{2, 2}, {4, 4}, {5, 5}, {6, 6}},
+                                               {{2, 2}, {4, 4}, {5, 5}, {6, 6}},
+                                               {{2, 2}, {2, 2}, {2, 2}, {2, 2}}};
+
+// The G2P instantiation of a kind, launch-shape variant and warm start (liquid: no warm start;
+// mixed kinds: the 256-thread block shape whatever the variant), as a function pointer.
+template <int KIND>
+static const void* g2p_fn(int v, bool warm) {
+  if constexpr (KIND == G2P_MIXED) {
+    return warm ? (const void*)k_g2p<true, G2P_THREADS, 2, false, KIND> : (const void*)k_g2p<false, G2P_THREADS, 2, false, KIND>;
+  } else {
+    constexpr bool W = KIND == G2P_PASTE;  // the warm instantiations exist for paste only
+    if (v == 3) return (warm && W) ? (const void*)k_g2p<W, G2P_THREADS_SMALL, 6, false, KIND> : (const void*)k_g2p<false, G2P_THREADS_SMALL, 6, false, KIND>;
+    if (v == 2) return (warm && W) ? (const void*)k_g2p<W, G2P_THREADS_SMALL, 5, false, KIND> : (const void*)k_g2p<false, G2P_THREADS_SMALL, 5, false, KIND>;
+    if (v == 1) return (warm && W) ? (const void*)k_g2p<W, G2P_THREADS_SMALL, 4, false, KIND> : (const void*)k_g2p<false, G2P_THREADS_SMALL, 4, false, KIND>;
+    return (warm && W) ? (const void*)k_g2p<W, G2P_THREADS, 2, false, KIND> : (const void*)k_g2p<false, G2P_THREADS, 2, false, KIND>;
+  }
+}
+static const void* g2p_fn(int kind, int v, bool warm) {
+  return kind == G2P_PASTE ? g2p_fn<G2P_PASTE>(v, warm) : (kind == G2P_LIQUID ? g2p_fn<G2P_LIQUID>(v, false) : g2p_fn<G2P_MIXED>(v, warm));
+}
+static int g2p_fn_threads(int kind, int v) { return kind == G2P_MIXED ? G2P_THREADS : g2p_threads(v); }
 
 // dynamic shared memory of each P2G variant: records / partials, plus the staged copies
 static size_t p2g_variant_smem(int v) {
@@ -3224,14 +3266,12 @@ void configure_kernels() {
                                    (const void*)k_p2g<P2G_CHUNK_SMALL, true>};
   for (int v = 0; v < P2G_VARIANTS; ++v)
     cudaFuncSetAttribute(p2g[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_variant_smem(v));
-  const void* g2p[4][2] = {{(const void*)k_g2p<false, G2P_THREADS>, (const void*)k_g2p<true, G2P_THREADS>},
-                           {(const void*)k_g2p<false, G2P_THREADS_SMALL>, (const void*)k_g2p<true, G2P_THREADS_SMALL>},
-                           {(const void*)k_g2p<false, G2P_THREADS_SMALL, 5>, (const void*)k_g2p<true, G2P_THREADS_SMALL, 5>},
-                           {(const void*)k_g2p<false, G2P_THREADS_SMALL, 6>, (const void*)k_g2p<true, G2P_THREADS_SMALL, 6>}};
-  for (int v = 0; v < 4; ++v)
-    for (int w = 0; w < 2; ++w)
-      cudaFuncSetAttribute(g2p[v][w], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem(g2p_threads(v)));
-  // the clock-instrumented instantiations of the return-share measurement
+  for (int k = 0; k < 3; ++k)
+    for (int v = 0; v < G2P_VARIANTS; ++v)
+      for (int w = 0; w < 2; ++w)
+        cudaFuncSetAttribute(g2p_fn(k, v, w), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)g2p_smem(g2p_fn_threads(k, v)));
+  // the clock-instrumented instantiations of the return-share measurement (any kind)
   const void* g2p_clk[2] = {(const void*)k_g2p<false, G2P_THREADS, 2, true>,
                             (const void*)k_g2p<true, G2P_THREADS, 2, true>};
   for (const void* f : g2p_clk)
@@ -3242,8 +3282,10 @@ void configure_kernels() {
   g_sms = sms;
   occupancy(&g_sort_per_sm, (const void*)k_bin_sort, TB, 0);
   for (int v = 0; v < P2G_VARIANTS; ++v) occupancy(&g_p2g_per_sm[v], p2g[v], P2G_THREADS, p2g_variant_smem(v));
-  for (int v = 0; v < 4; ++v)
-    for (int w = 0; w < 2; ++w) occupancy(&g_g2p_per_sm[v][w], g2p[v][w], g2p_threads(v), g2p_smem(g2p_threads(v)));
+  for (int k = 0; k < 3; ++k)
+    for (int v = 0; v < G2P_VARIANTS; ++v)
+      for (int w = 0; w < 2; ++w)
+        occupancy(&g_g2p_per_sm[k][v][w], g2p_fn(k, v, w), g2p_fn_threads(k, v), g2p_smem(g2p_fn_threads(k, v)));
 }
 
 // persistent grid size: the requested CTAs per SM, at most the resident limit, times the SMs
@@ -3256,7 +3298,7 @@ int launch_shape_limits(int out[LAUNCH_LIMITS]) {
   out[0] = g_sms;
   out[1] = g_sort_per_sm;
   for (int v = 0; v < P2G_VARIANTS; ++v) out[LIM_P2G + v] = g_p2g_per_sm[v];
-  for (int v = 0; v < G2P_VARIANTS; ++v) out[LIM_G2P + v] = g_g2p_per_sm[v][1];
+  for (int v = 0; v < G2P_VARIANTS; ++v) out[LIM_G2P + v] = g_g2p_per_sm[G2P_PASTE][v][1];
   return LAUNCH_LIMITS;
 }
 
@@ -3287,31 +3329,46 @@ static int launch_tiles_p2g(const DeviceArrays& A, cudaStream_t s, int transport
   return 3;
 }
 
-// G2P in the launch shape's instantiation
-static void launch_g2p(const DeviceArrays& A, bool warm, cudaStream_t s) {
+// G2P in the launch shape's instantiation for the ensemble's material kinds
+template <int KIND>
+static void launch_g2p_kind(const DeviceArrays& A, bool warm, cudaStream_t s) {
   const LaunchShape& L = A.shape;
   uint32_t* cur = L.dynamic ? A.nw_count + 4 : nullptr;
   const float* tab = warm ? A.mlp_tab : nullptr;
   const int v = (L.g2p_variant >= 0 && L.g2p_variant < G2P_VARIANTS) ? L.g2p_variant : 0;
-  const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[v][warm ? 1 : 0]);
+  const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[KIND][v][warm ? 1 : 0]);
 #define LP_G2P_ARGS                                                                                               \
   A.desc, A.ctrl, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.perm, A.vel, A.tpart, tab, A.log_x, A.log_y, \
       A.log_n, A.log_cap, A.tile_rec, A.tile_count, cur, A.g2p_clk, A.defer_rec, A.nw_count + 5
-#define LP_G2P_LAUNCH(T, MB, CLK, N) \
-  (warm ? k_g2p<true, T, MB, CLK> : k_g2p<false, T, MB, CLK>)<<<N, T, g2p_smem(T), s>>>(LP_G2P_ARGS)
-  if (A.g2p_clk) {  // measurement of the return's share of G2P warp time (256-thread CTAs)
-    LP_G2P_LAUNCH(G2P_THREADS, 2, true, persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[0][warm ? 1 : 0]));
-  } else if (v == 3) {
-    LP_G2P_LAUNCH(G2P_THREADS_SMALL, 6, false, ctas);
-  } else if (v == 2) {
-    LP_G2P_LAUNCH(G2P_THREADS_SMALL, 5, false, ctas);
-  } else if (v == 1) {
-    LP_G2P_LAUNCH(G2P_THREADS_SMALL, 4, false, ctas);
+#define LP_G2P_LAUNCH(T, MB)                                                                                 \
+  (warm ? k_g2p<KIND == G2P_LIQUID ? false : true, T, MB, false, KIND> : k_g2p<false, T, MB, false, KIND>) \
+      <<<ctas, T, g2p_smem(T), s>>>(LP_G2P_ARGS)
+  if constexpr (KIND == G2P_MIXED) {
+    LP_G2P_LAUNCH(G2P_THREADS, 2);
   } else {
-    LP_G2P_LAUNCH(G2P_THREADS, 2, false, ctas);
+    if (v == 3) LP_G2P_LAUNCH(G2P_THREADS_SMALL, 6);
+    else if (v == 2) LP_G2P_LAUNCH(G2P_THREADS_SMALL, 5);
+    else if (v == 1) LP_G2P_LAUNCH(G2P_THREADS_SMALL, 4);
+    else LP_G2P_LAUNCH(G2P_THREADS, 2);
   }
 #undef LP_G2P_LAUNCH
 #undef LP_G2P_ARGS
+}
+static void launch_g2p(const DeviceArrays& A, bool warm, cudaStream_t s) {
+  if (A.g2p_clk) {  // measurement of the return's share of G2P warp time (256-thread CTAs, any kind)
+    const LaunchShape& L = A.shape;
+    uint32_t* cur = L.dynamic ? A.nw_count + 4 : nullptr;
+    const float* tab = warm ? A.mlp_tab : nullptr;
+    const unsigned ctas = persistent_ctas(L.g2p_per_sm, g_g2p_per_sm[G2P_MIXED][0][warm ? 1 : 0]);
+    (warm ? k_g2p<true, G2P_THREADS, 2, true> : k_g2p<false, G2P_THREADS, 2, true>)<<<ctas, G2P_THREADS,
+                                                                                       g2p_smem(G2P_THREADS), s>>>(
+        A.desc, A.ctrl, A.st[0], A.st[1], A.id[0], A.id[1], A.cap, A.perm, A.vel, A.tpart, tab, A.log_x, A.log_y,
+        A.log_n, A.log_cap, A.tile_rec, A.tile_count, cur, A.g2p_clk, A.defer_rec, A.nw_count + 5);
+    return;
+  }
+  if (A.kinds == 1) launch_g2p_kind<G2P_PASTE>(A, warm, s);
+  else if (A.kinds == 2) launch_g2p_kind<G2P_LIQUID>(A, false, s);
+  else launch_g2p_kind<G2P_MIXED>(A, warm, s);
 }
 // the particles G2P left to the eigen-decomposition pass (normally none: every CTA exits at once)
 static void launch_g2p_defer(const DeviceArrays& A, bool warm, cudaStream_t s) {

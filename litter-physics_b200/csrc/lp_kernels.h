@@ -28,6 +28,7 @@ struct DeviceArrays {
   Control* ctrl = nullptr;
   int n_inst = 0;
   int any_pellet = 0;
+  int kinds = 3;  // material kinds of the instances: bit 0 paste, bit 1 liquid
   int* pcta_inst = nullptr;  // G2P / per-slot CTA -> instance
   int64_t n_pcta = 0;
   int* tile_inst = nullptr;  // P2G tile -> instance

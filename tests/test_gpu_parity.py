@@ -362,7 +362,7 @@ def test_large_strain_particles_take_the_eigen_pass(lib_built):
     for i in big:
         q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
         f = q @ np.diag(rng.uniform(1.15, 1.35, 3) * np.array([1.0, 0.8, 0.9])) @ q.T
-        state["deformation"][i] = f.astype(np.float32).astype(np.float64).reshape(-1)
+        state["deformation"][i] = f.astype(np.float32).astype(np.float64).reshape(state["deformation"][i].shape)
     state["deformation"] = np.ascontiguousarray(state["deformation"])
     b = state["deformation"].reshape(-1, 3, 3)
     bn = np.linalg.norm(b[big] @ b[big].transpose(0, 2, 1) - np.eye(3), axis=(1, 2))

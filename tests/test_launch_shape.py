@@ -1,7 +1,7 @@
 """Launch shapes and the autotuner: every shape of the persistent tile kernels gives the same
 particle state bit for bit (a tile's results do not depend on the CTA that takes it, on the
-order, on the G2P block size or on the P2G chunk size), and the autotuner keeps a valid
-trajectory.  The ledgers are identical too, except that the G2P block size changes which
+order, on the G2P block size or on the P2G chunk size), and the autotuner leaves the state
+as it found it.  The ledgers are identical too, except that the G2P block size changes which
 thread sums which particles' FP64 plastic work, so with 128-thread CTAs that one ledger entry
 agrees to rounding."""
 
@@ -125,18 +125,34 @@ def test_return_share_measurement_steps_like_the_solver():
 
 
 def test_autotuner_picks_a_shape_on_the_live_batch():
+    """The autotuner times every candidate from the same state (a device copy put back before
+    each candidate) and leaves the batch where it found it: the same particles, ledgers and
+    counters, and a continuation that matches an untuned run."""
     from litter_physics_b200 import _lib
     from litter_physics_b200.sim import Batch
 
     _lib.build()
     b = Batch(uneven_batch())
-    t0 = [b.counters(i).time for i in range(3)]
+    b.run_substeps(6)
+    b.sync()
+    before = [(by_id(b.particles(i)), bytes(b.ledger(i)), b.counters(i).step_count, b.counters(i).time)
+              for i in range(3)]
     report = b.autotune(4)
     lines = report.strip().splitlines()
     assert lines[-1].startswith("chosen: ") and len(lines) >= 8
     chosen = b.launch_shape()
     assert chosen["g2p_per_sm"] >= 1 and chosen["graph_attempts"] >= 1
-    # the tuning attempts were real steps of the trajectory
     b.sync()
-    assert all(b.counters(i).time > t0[i] for i in range(3))
+    for i, (p, led, steps, t) in enumerate(before):
+        q = by_id(b.particles(i))
+        for k in ("position", "velocity", "deformation", "kirchhoff"):
+            assert np.array_equal(p[k], q[k]), (i, k)
+        assert bytes(b.ledger(i)) == led
+        assert b.counters(i).step_count == steps and b.counters(i).time == t
+    ref = Batch(uneven_batch())
+    ref.run_substeps(14)
+    b.run_substeps(8)
+    for i in range(3):
+        assert np.array_equal(by_id(b.particles(i))["position"], by_id(ref.particles(i))["position"])
+    ref.close()
     b.close()
