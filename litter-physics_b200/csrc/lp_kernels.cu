@@ -306,6 +306,44 @@ __device__ __forceinline__ uint32_t tile_next(uint32_t* cursor, uint32_t i, uint
   return cursor ? tile_take(cursor, slot) : i + gridDim.x;
 }
 
+// L2 prefetch of [p, p + bytes) of this GPU's memory (cp.async.bulk.prefetch.L2, no data
+// returned): p 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+// The committed-state components comps[] (and, if not null, the permutation) of the particles of
+// tile-list entry `rec`, prefetched into L2 by the calling thread while the CTA still works on its
+// current tile.  The entry's sorted slots [z, w) gather their state through the permutation from
+// about the same slots of the committed buffer (the state is stored in the previous attempt's
+// sorted order, and a particle's slot moves only by the particles that changed bins), so the
+// range is widened by 64 slots on each side, kept inside the instance's slots and aligned to 16
+// bytes.
+constexpr int PF_L2_MARGIN = 64;
+__device__ __forceinline__ void prefetch_tile_l2(const uint4 rec, const InstDesc* __restrict__ desc,
+                                                 const Control* __restrict__ ctrl, const float* __restrict__ st0,
+                                                 const float* __restrict__ st1, int64_t cap, uint64_t comps,
+                                                 const uint32_t* __restrict__ extra,
+                                                 const uint32_t* __restrict__ extra2 = nullptr) {
+  const InstDesc& D = desc[rec.y];
+  const float* cur = ctrl[rec.y].parity ? st1 : st0;
+  const int64_t lo = D.slot_off, hi = D.slot_off + D.slot_cap;  // slot_off, slot_cap: multiples of 256
+  const int64_t a = max(lo, (int64_t)rec.z - PF_L2_MARGIN) & ~(int64_t)3;
+  const int64_t b = min(hi, ((int64_t)rec.w + PF_L2_MARGIN + 3) & ~(int64_t)3);
+  if (b <= a) return;
+  const uint32_t bytes = (uint32_t)((b - a) * sizeof(float));
+  for (int c = 0; c < NCOMP; ++c)
+    if ((comps >> c) & 1ull) prefetch_l2(cur + (int64_t)c * cap + a, bytes);
+  if (extra) prefetch_l2(extra + a, bytes);
+  if (extra2) prefetch_l2(extra2 + a, bytes);
+}
+// component masks of the prefetches: what P2G reads (x v C tau m V0), what paste and liquid G2P read
+__host__ __device__ constexpr uint64_t comp_bits(int first, int count) {
+  return ((count >= 64 ? ~0ull : ((1ull << count) - 1ull)) << first);
+}
+constexpr uint64_t P2G_COMPS = comp_bits(C_X, 15) | comp_bits(C_TAU, 6) | comp_bits(C_M, 2);
+constexpr uint64_t G2P_PASTE_COMPS = comp_bits(C_X, 3) | comp_bits(C_H, 9) | comp_bits(C_EP, 3);
+constexpr uint64_t G2P_LIQUID_COMPS = comp_bits(C_X, 3) | comp_bits(C_EP, 3) | comp_bits(C_JM1, 1);
+
 // ============================================================== begin
 // One thread per instance: decides whether the instance attempts a step and with which dt.
 __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, int n_inst,
@@ -1103,11 +1141,19 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
           const uint4* __restrict__ tile_rec, const uint32_t* __restrict__ tile_count, uint32_t* cursor) {
   const uint32_t n = *tile_count;
   if constexpr (!STAGED) {
-    __shared__ uint32_t slot;
-    for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
+    // the next tile is taken at the start of the current one (two cursor slots, used alternately),
+    // and thread 0 prefetches its particle state into L2 while the CTA scatters the current tile
+    __shared__ uint32_t slots[2];
+    int which = 0;
+    uint32_t i = tile_first(cursor, &slots[0]);
+    while (i < n) {
+      which ^= 1;
+      const uint32_t nx = tile_next(cursor, i, &slots[which]);
+      if (threadIdx.x == 0 && nx < n) prefetch_tile_l2(tile_rec[nx], desc, ctrl, st0, st1, cap, P2G_COMPS, perm);
       p2g_tile<CHUNK, false>(tile_rec[i], desc, ctrl, st0, st1, cap, start, perm, acc, node_total, blk_epoch,
                              transport_only, nullptr);
       __syncthreads();  // the next tile reuses the shared memory
+      i = nx;
     }
   } else {
     __shared__ uint32_t slots[2];
@@ -2595,12 +2641,28 @@ __global__ void __launch_bounds__(NT, MINB)
           long long log_cap, const uint4* __restrict__ tile_rec, const uint32_t* __restrict__ tile_count,
           uint32_t* cursor, unsigned long long* __restrict__ clk, uint4* __restrict__ defer_rec,
           uint32_t* __restrict__ defer_count) {
-  __shared__ uint32_t slot;
+  // the next tile is taken at the start of the current one (two cursor slots, used alternately),
+  // and thread 0 prefetches its particle state into L2 while the CTA works on the current tile
+  __shared__ uint32_t slots[2];
   const uint32_t n = *tile_count;
-  for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
+  int which = 0;
+  uint32_t i = tile_first(cursor, &slots[0]);
+  while (i < n) {
+    which ^= 1;
+    const uint32_t nx = tile_next(cursor, i, &slots[which]);
+    if (threadIdx.x == 0 && nx < n) {
+      const uint4 r = tile_rec[nx];
+      const Control& c = ctrl[r.y];
+      const uint32_t* idc = c.parity ? id1 : id0;
+      const InstDesc& D = desc[r.y];
+      const uint64_t comps =
+          D.kind == 0 ? (G2P_PASTE_COMPS | (D.per_particle_yield ? comp_bits(C_YS, 1) : 0ull)) : G2P_LIQUID_COMPS;
+      prefetch_tile_l2(r, desc, ctrl, st0, st1, cap, comps, perm, idc);
+    }
     g2p_tile<WARM, NT, CLOCKS, KIND>(tile_rec[i], desc, ctrl, st0, st1, id0, id1, cap, perm, vel, part, mlp_tab, log_x,
-                               log_y, log_n, log_cap, clk, defer_rec, defer_count);
+                                     log_y, log_n, log_cap, clk, defer_rec, defer_count);
     __syncthreads();  // the next tile reuses the shared memory
+    i = nx;
   }
 }
 
