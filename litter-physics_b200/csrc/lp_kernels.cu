@@ -306,44 +306,6 @@ __device__ __forceinline__ uint32_t tile_next(uint32_t* cursor, uint32_t i, uint
   return cursor ? tile_take(cursor, slot) : i + gridDim.x;
 }
 
-// L2 prefetch of [p, p + bytes) of this GPU's memory (cp.async.bulk.prefetch.L2, no data
-// returned): p 16-byte aligned, bytes a multiple of 16.
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-// The committed-state components comps[] (and, if not null, the permutation) of the particles of
-// tile-list entry `rec`, prefetched into L2 by the calling thread while the CTA still works on its
-// current tile.  The entry's sorted slots [z, w) gather their state through the permutation from
-// about the same slots of the committed buffer (the state is stored in the previous attempt's
-// sorted order, and a particle's slot moves only by the particles that changed bins), so the
-// range is widened by 64 slots on each side, kept inside the instance's slots and aligned to 16
-// bytes.
-constexpr int PF_L2_MARGIN = 64;
-__device__ __forceinline__ void prefetch_tile_l2(const uint4 rec, const InstDesc* __restrict__ desc,
-                                                 const Control* __restrict__ ctrl, const float* __restrict__ st0,
-                                                 const float* __restrict__ st1, int64_t cap, uint64_t comps,
-                                                 const uint32_t* __restrict__ extra,
-                                                 const uint32_t* __restrict__ extra2 = nullptr) {
-  const InstDesc& D = desc[rec.y];
-  const float* cur = ctrl[rec.y].parity ? st1 : st0;
-  const int64_t lo = D.slot_off, hi = D.slot_off + D.slot_cap;  // slot_off, slot_cap: multiples of 256
-  const int64_t a = max(lo, (int64_t)rec.z - PF_L2_MARGIN) & ~(int64_t)3;
-  const int64_t b = min(hi, ((int64_t)rec.w + PF_L2_MARGIN + 3) & ~(int64_t)3);
-  if (b <= a) return;
-  const uint32_t bytes = (uint32_t)((b - a) * sizeof(float));
-  for (int c = 0; c < NCOMP; ++c)
-    if ((comps >> c) & 1ull) prefetch_l2(cur + (int64_t)c * cap + a, bytes);
-  if (extra) prefetch_l2(extra + a, bytes);
-  if (extra2) prefetch_l2(extra2 + a, bytes);
-}
-// component masks of the prefetches: what P2G reads (x v C tau m V0), what paste and liquid G2P read
-__host__ __device__ constexpr uint64_t comp_bits(int first, int count) {
-  return ((count >= 64 ? ~0ull : ((1ull << count) - 1ull)) << first);
-}
-constexpr uint64_t P2G_COMPS = comp_bits(C_X, 15) | comp_bits(C_TAU, 6) | comp_bits(C_M, 2);
-constexpr uint64_t G2P_PASTE_COMPS = comp_bits(C_X, 3) | comp_bits(C_H, 9) | comp_bits(C_EP, 3);
-constexpr uint64_t G2P_LIQUID_COMPS = comp_bits(C_X, 3) | comp_bits(C_EP, 3) | comp_bits(C_JM1, 1);
-
 // ============================================================== begin
 // One thread per instance: decides whether the instance attempts a step and with which dt.
 __global__ void k_begin(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, int n_inst,
@@ -933,7 +895,12 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
     for (int q = 0; q < 3; ++q)
 #pragma unroll
       for (int k = 0; k < 2; ++k) acc9[b][q][k] = make_float2(0.0f, 0.0f);
-  long long tot[4] = {0, 0, 0, 0};  // this thread's particle totals (mass, momentum), fixed point
+  // this thread's particle totals (mass, momentum, fixed point), kept in shared memory between the
+  // chunks' load phases so that they hold no registers during the scatter
+  __shared__ long long tot_s[4 * P2G_THREADS];
+  volatile long long* tot = tot_s + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) tot[k * P2G_THREADS] = 0;
 
   const uint32_t s = start[key0 + bin], e = start[key0 + bin + 1];  // this bin's sorted range
   for (uint32_t c0 = ts; c0 < te; c0 += CHUNK) {
@@ -992,10 +959,10 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
 #pragma unroll
       for (int a = 0; a < 3; ++a) r[(13 + a) * CHUNK] = p2g_frac(x[a], dx, D.pow2_inv_dx);
       // exact per-particle totals: FP64 products of the stored FP32 mass and velocity
-      tot[0] += to_fixed((double)m, s_m);
-      tot[1] += to_fixed((double)m * (double)v[0], s_p);
-      tot[2] += to_fixed((double)m * (double)v[1], s_p);
-      tot[3] += to_fixed((double)m * (double)v[2], s_p);
+      tot[0] = tot[0] + to_fixed((double)m, s_m);
+      tot[P2G_THREADS] = tot[P2G_THREADS] + to_fixed((double)m * (double)v[0], s_p);
+      tot[2 * P2G_THREADS] = tot[2 * P2G_THREADS] + to_fixed((double)m * (double)v[1], s_p);
+      tot[3 * P2G_THREADS] = tot[3 * P2G_THREADS] + to_fixed((double)m * (double)v[2], s_p);
     }
     if constexpr (STAGED) {
       // this thread has read its copies: the next chunk (of this tile or of the next) may land
@@ -1067,7 +1034,7 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
   const int lane = t & 31, w = t >> 5;
   long long dif[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) dif[k] = warp_sum_ll_redux(tot[k] - nv[k]);
+  for (int k = 0; k < 4; ++k) dif[k] = warp_sum_ll_redux(tot[k * P2G_THREADS] - nv[k]);
   long long pin = nv[0];  // inclusive warp prefix of node masses
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -1141,19 +1108,11 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
           const uint4* __restrict__ tile_rec, const uint32_t* __restrict__ tile_count, uint32_t* cursor) {
   const uint32_t n = *tile_count;
   if constexpr (!STAGED) {
-    // the next tile is taken at the start of the current one (two cursor slots, used alternately),
-    // and thread 0 prefetches its particle state into L2 while the CTA scatters the current tile
-    __shared__ uint32_t slots[2];
-    int which = 0;
-    uint32_t i = tile_first(cursor, &slots[0]);
-    while (i < n) {
-      which ^= 1;
-      const uint32_t nx = tile_next(cursor, i, &slots[which]);
-      if (threadIdx.x == 0 && nx < n) prefetch_tile_l2(tile_rec[nx], desc, ctrl, st0, st1, cap, P2G_COMPS, perm);
+    __shared__ uint32_t slot;
+    for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
       p2g_tile<CHUNK, false>(tile_rec[i], desc, ctrl, st0, st1, cap, start, perm, acc, node_total, blk_epoch,
                              transport_only, nullptr);
       __syncthreads();  // the next tile reuses the shared memory
-      i = nx;
     }
   } else {
     __shared__ uint32_t slots[2];
@@ -2417,40 +2376,55 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
         base[a] = (int)(bf + 1.0f);
         weights_of(sc - bf, dx, w[a], d[a]);
       }
-      float v[3] = {0.f, 0.f, 0.f};
-      float Cm[9];
-#pragma unroll
-      for (int a = 0; a < 9; ++a) Cm[a] = 0.0f;
+      float v[3], Cm[9];
       const int lbx = base[0] - ox, lby = base[1] - oy, lbz = base[2] - oz;
       // separable gather: per (a, b) row, z sums S0 = sum_c w_c v and S1 = sum_c w_c d_c v, then
-      // v += w_ab S0, C[:,0] += w_ab d_a S0, C[:,1] += w_ab d_b S0, C[:,2] += w_ab S1
+      // v += w_ab S0, C[:,0] += w_ab d_a S0, C[:,1] += w_ab d_b S0, C[:,2] += w_ab S1.  The x and y
+      // components run as pairs on the paired FP32 units (fma.rn.f32x2, each lane the scalar FMA);
+      // C is held as the pairs (C_00, C_10), (C_01, C_11), (C_02, C_12) and the z row alone.
       const float wdz[3] = {w[2][0] * d[2][0], w[2][1] * d[2][1], w[2][2] * d[2][2]};
+      float2 vxy = make_float2(0.f, 0.f), c0 = vxy, c1 = vxy, c2 = vxy;
+      float vz = 0.f, cz0 = 0.f, cz1 = 0.f, cz2 = 0.f;
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
           const int row = ((lbx + a) * HY + (lby + b)) * HZ + lbz;
-          float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f};
+          float2 s0 = make_float2(0.f, 0.f), s1 = s0;
+          float s0z = 0.f, s1z = 0.f;
 #pragma unroll
           for (int cc = 0; cc < 3; ++cc) {
             const float4 nv = hv[row + cc];
-            const float nvv[3] = {nv.x, nv.y, nv.z};
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              s0[i] += w[2][cc] * nvv[i];
-              s1[i] += wdz[cc] * nvv[i];
-            }
+            const float2 nxy = make_float2(nv.x, nv.y);
+            s0 = __ffma2_rn(make_float2(w[2][cc], w[2][cc]), nxy, s0);
+            s1 = __ffma2_rn(make_float2(wdz[cc], wdz[cc]), nxy, s1);
+            s0z = __fmaf_rn(w[2][cc], nv.z, s0z);
+            s1z = __fmaf_rn(wdz[cc], nv.z, s1z);
           }
           const float wab = w[0][a] * w[1][b];
           const float wa0 = wab * d[0][a], wa1 = wab * d[1][b];
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            v[i] += wab * s0[i];
-            Cm[3 * i + 0] += wa0 * s0[i];
-            Cm[3 * i + 1] += wa1 * s0[i];
-            Cm[3 * i + 2] += wab * s1[i];
-          }
+          const float2 wab2 = make_float2(wab, wab);
+          vxy = __ffma2_rn(wab2, s0, vxy);
+          c0 = __ffma2_rn(make_float2(wa0, wa0), s0, c0);
+          c1 = __ffma2_rn(make_float2(wa1, wa1), s0, c1);
+          c2 = __ffma2_rn(wab2, s1, c2);
+          vz = __fmaf_rn(wab, s0z, vz);
+          cz0 = __fmaf_rn(wa0, s0z, cz0);
+          cz1 = __fmaf_rn(wa1, s0z, cz1);
+          cz2 = __fmaf_rn(wab, s1z, cz2);
         }
+      v[0] = vxy.x;
+      v[1] = vxy.y;
+      v[2] = vz;
+      Cm[0] = c0.x;
+      Cm[1] = c1.x;
+      Cm[2] = c2.x;
+      Cm[3] = c0.y;
+      Cm[4] = c1.y;
+      Cm[5] = c2.y;
+      Cm[6] = cz0;
+      Cm[7] = cz1;
+      Cm[8] = cz2;
       const float dx2_inv = 4.0f / (dx * dx);
 #pragma unroll
       for (int a = 0; a < 9; ++a) Cm[a] *= dx2_inv;
@@ -2641,28 +2615,12 @@ __global__ void __launch_bounds__(NT, MINB)
           long long log_cap, const uint4* __restrict__ tile_rec, const uint32_t* __restrict__ tile_count,
           uint32_t* cursor, unsigned long long* __restrict__ clk, uint4* __restrict__ defer_rec,
           uint32_t* __restrict__ defer_count) {
-  // the next tile is taken at the start of the current one (two cursor slots, used alternately),
-  // and thread 0 prefetches its particle state into L2 while the CTA works on the current tile
-  __shared__ uint32_t slots[2];
+  __shared__ uint32_t slot;
   const uint32_t n = *tile_count;
-  int which = 0;
-  uint32_t i = tile_first(cursor, &slots[0]);
-  while (i < n) {
-    which ^= 1;
-    const uint32_t nx = tile_next(cursor, i, &slots[which]);
-    if (threadIdx.x == 0 && nx < n) {
-      const uint4 r = tile_rec[nx];
-      const Control& c = ctrl[r.y];
-      const uint32_t* idc = c.parity ? id1 : id0;
-      const InstDesc& D = desc[r.y];
-      const uint64_t comps =
-          D.kind == 0 ? (G2P_PASTE_COMPS | (D.per_particle_yield ? comp_bits(C_YS, 1) : 0ull)) : G2P_LIQUID_COMPS;
-      prefetch_tile_l2(r, desc, ctrl, st0, st1, cap, comps, perm, idc);
-    }
+  for (uint32_t i = tile_first(cursor, &slot); i < n; i = tile_next(cursor, i, &slot)) {
     g2p_tile<WARM, NT, CLOCKS, KIND>(tile_rec[i], desc, ctrl, st0, st1, id0, id1, cap, perm, vel, part, mlp_tab, log_x,
                                      log_y, log_n, log_cap, clk, defer_rec, defer_count);
     __syncthreads();  // the next tile reuses the shared memory
-    i = nx;
   }
 }
 
