@@ -2561,24 +2561,51 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
     max_disp = fmaxf(max_disp, disp);
   }
   cp_async_wait<0>();  // no copy may land after the CTA's shared memory is released
-  // the tile's sums: a fixed pairwise tree over the threads' shared-memory sums (deterministic,
-  // and a short loop instead of an unrolled shuffle reduction)
-  __syncthreads();
+  // the tile's sums: a warp butterfly (one short loop over the five offsets), then thread 0 adds
+  // the warps' results in warp order (a fixed order: deterministic, one barrier)
+  {
+    double d0 = diss, d1 = bb, d2 = mass_sum, d3 = fail_value;
+    float f0 = max_speed, f1 = max_disp;
+    int i0 = fail, i1 = iters, i2 = yielded;
 #pragma unroll 1
-  for (int h = NT / 2; h > 0; h >>= 1) {
-    const int a = threadIdx.x, b = threadIdx.x + h;
-    if (a < h) {
-      acc_d[a] += acc_d[b];
-      acc_d[NT + a] += acc_d[NT + b];
-      acc_d[2 * NT + a] += acc_d[2 * NT + b];
-      acc_d[3 * NT + a] = fmax(acc_d[3 * NT + a], acc_d[3 * NT + b]);
-      acc_f[a] = fmaxf(acc_f[a], acc_f[b]);
-      acc_f[NT + a] = fmaxf(acc_f[NT + a], acc_f[NT + b]);
-      acc_i[a] = max(acc_i[a], acc_i[b]);
-      acc_i[NT + a] += acc_i[NT + b];
-      acc_i[2 * NT + a] += acc_i[2 * NT + b];
+    for (int o = 16; o > 0; o >>= 1) {
+      d0 += __shfl_xor_sync(0xffffffffu, d0, o);
+      d1 += __shfl_xor_sync(0xffffffffu, d1, o);
+      d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+      d3 = fmax(d3, __shfl_xor_sync(0xffffffffu, d3, o));
+      f0 = fmaxf(f0, __shfl_xor_sync(0xffffffffu, f0, o));
+      f1 = fmaxf(f1, __shfl_xor_sync(0xffffffffu, f1, o));
+      i0 = max(i0, __shfl_xor_sync(0xffffffffu, i0, o));
+      i1 += __shfl_xor_sync(0xffffffffu, i1, o);
+      i2 += __shfl_xor_sync(0xffffffffu, i2, o);
     }
-    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {  // the warp's sums, in lane 0's own slots (thread 32 w)
+      const int t = threadIdx.x;
+      acc_d[t] = d0;
+      acc_d[NT + t] = d1;
+      acc_d[2 * NT + t] = d2;
+      acc_d[3 * NT + t] = d3;
+      acc_f[t] = f0;
+      acc_f[NT + t] = f1;
+      acc_i[t] = i0;
+      acc_i[NT + t] = i1;
+      acc_i[2 * NT + t] = i2;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll 1
+    for (int w = 32; w < NT; w += 32) {
+      acc_d[0] += acc_d[w];
+      acc_d[NT] += acc_d[NT + w];
+      acc_d[2 * NT] += acc_d[2 * NT + w];
+      acc_d[3 * NT] = fmax(acc_d[3 * NT], acc_d[3 * NT + w]);
+      acc_f[0] = fmaxf(acc_f[0], acc_f[w]);
+      acc_f[NT] = fmaxf(acc_f[NT], acc_f[NT + w]);
+      acc_i[0] = max(acc_i[0], acc_i[w]);
+      acc_i[NT] += acc_i[NT + w];
+      acc_i[2 * NT] += acc_i[2 * NT + w];
+    }
   }
   if (threadIdx.x == 0) {
     ParticlePartial& P = part[tile];
@@ -2591,7 +2618,7 @@ __device__ __forceinline__ void g2p_tile(const uint4 rec, const InstDesc* __rest
     P.iterations = acc_i[NT];
     P.yielded = acc_i[2 * NT];
     P.fail_value = acc_d[3 * NT];
-    // the tree's barriers ordered every lane's write of defer_flag before this read
+    // the barrier above ordered every lane's write of defer_flag before this read
     if (defer_flag) defer_rec[atomicAdd(defer_count, 1u)] = rec;
   }
   if constexpr (CLOCKS) {
