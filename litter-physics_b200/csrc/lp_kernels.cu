@@ -157,34 +157,6 @@ __device__ void block_reduce_multi_to0(double (&v)[K], unsigned max_mask, double
     warp_reduce_multi<K>(v, max_mask);
   }
 }
-// The same totals to thread 0 in compact code: the warp butterfly runs as a rolled loop over the
-// five offsets, and thread 0 combines the warps' results in warp order (a fixed order, hence
-// deterministic; one barrier).  Bit k of MAXMASK selects max instead of sum for value k.  sh
-// holds NT/32 K values and must not be rewritten before the caller's next barrier.
-template <int NT, int K, unsigned MAXMASK>
-__device__ void block_reduce_rolled_to0(double (&v)[K], double* sh /* NT/32*K */) {
-  constexpr int NW = NT / 32;
-  static_assert(NT % 32 == 0 && NW <= 32, "block size");
-#pragma unroll 1
-  for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const double other = __shfl_xor_sync(0xffffffffu, v[k], o);
-      v[k] = ((MAXMASK >> k) & 1u) ? fmax(v[k], other) : v[k] + other;
-    }
-  }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < K; ++k) sh[w * K + k] = v[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll 1
-    for (int u = 1; u < NW; ++u)
-#pragma unroll
-      for (int k = 0; k < K; ++k) v[k] = ((MAXMASK >> k) & 1u) ? fmax(v[k], sh[u * K + k]) : v[k] + sh[u * K + k];
-  }
-}
 template <int K>
 __device__ __forceinline__ void warp_sum_ll_multi(long long (&v)[K]) {
 #pragma unroll
@@ -1316,11 +1288,10 @@ __global__ void __launch_bounds__(GU_THREADS)
         acc[2 * node_total + g] = 0;
         acc[3 * node_total + g] = 0;
       } else {
-        // the fixed-point scales are powers of two: a product with the reciprocal is the quotient
-        const double r_m = 1.0 / D.s_mass, r_p = 1.0 / c.s_mom;
-        const double md = (double)mf * r_m;
-        double p[3] = {(double)acc[node_total + g] * r_p, (double)acc[2 * node_total + g] * r_p,
-                       (double)acc[3 * node_total + g] * r_p};
+        const double s_m = D.s_mass, s_p = c.s_mom;
+        const double md = (double)mf / s_m;
+        double p[3] = {(double)acc[node_total + g] / s_p, (double)acc[2 * node_total + g] / s_p,
+                       (double)acc[3 * node_total + g] / s_p};
         acc[g] = 0;
         acc[node_total + g] = 0;
         acc[2 * node_total + g] = 0;
@@ -1339,7 +1310,7 @@ __global__ void __launch_bounds__(GU_THREADS)
             if (l | h) {
               trac[(int64_t)a * node_total + g] = 0;
               trac[(int64_t)(a + 3) * node_total + g] = 0;
-              const double dl = (double)l * r_p, dh = (double)h * r_p;
+              const double dl = (double)l / s_p, dh = (double)h / s_p;
               const double S = dl - dh;
               // telescoped kinetic-energy jump of the reaction deposits (grid.rs:279-295)
               tren += S * (p[a] / md + S / (2.0 * md));
@@ -1448,7 +1419,7 @@ __global__ void __launch_bounds__(GU_THREADS)
     rv[RK - 2] = e_grav;
     rv[RK - 1] = e_walls;
   }
-  block_reduce_rolled_to0<GU_THREADS, RK, 1u << 6>(rv, shd);  // kernel end: thread 0 writes
+  block_reduce_multi_to0<GU_THREADS, RK>(rv, 1u << 6, shd);  // kernel end: thread 0 writes
   wi0 = rv[0];
   wi1 = rv[1];
   wi2 = rv[2];
