@@ -156,3 +156,30 @@ def test_autotuner_picks_a_shape_on_the_live_batch():
         assert np.array_equal(by_id(b.particles(i))["position"], by_id(ref.particles(i))["position"])
     ref.close()
     b.close()
+
+
+def test_mixed_material_batch_matches_single_kind_runs():
+    """A batch that mixes a paste and a liquid instance runs the mixed-kind G2P; each member
+    matches the same instance run alone (which runs the paste-only or liquid-only G2P) bit for
+    bit."""
+    from litter_physics_b200 import _lib, configs
+    from litter_physics_b200.sim import Batch, Simulation
+
+    _lib.build()
+    paste = configs.slump(16, (4, 4, 8), seed=31)
+    liquid = configs.slump(16, (4, 4, 8), seed=32)
+    liquid.material = configs.dam_break(16, (4, 4, 8)).material
+    specs = [paste, liquid]
+    b = Batch(specs)
+    b.run_substeps(20)
+    b.sync()
+    for i, spec in enumerate(specs):
+        one = Simulation(spec)
+        one.run_substeps(20)
+        one.sync()
+        pb, ps = by_id(b.particles(i)), by_id(one.particles())
+        assert b.counters(i).step_count == one.counters.step_count
+        for k in ("position", "velocity", "deformation", "volume_ratio"):
+            assert np.array_equal(pb[k], ps[k]), (i, k)
+        one.close()
+    b.close()
