@@ -419,7 +419,8 @@ __device__ __forceinline__ uint32_t bin_key(const InstDesc& D, const float (&x)[
   return (uint32_t)(D.key_off + tile * TB + (lx * TY + ly) * TZ + lz);
 }
 
-__global__ void __launch_bounds__(BIN_THREADS)
+// 32 registers: 32 CTAs (the full 64 warps) per SM to cover the position loads
+__global__ void __launch_bounds__(BIN_THREADS, 32)
     k_bin_count(const InstDesc* __restrict__ desc, Control* __restrict__ ctrl, const int* __restrict__ pcta_inst,
                 const float* __restrict__ st0, const float* __restrict__ st1, int64_t cap,
                 uint32_t* __restrict__ keys, uint32_t* __restrict__ count, uint32_t* __restrict__ chunk_sum,
@@ -1072,7 +1073,10 @@ __device__ __forceinline__ void p2g_tile(const uint4 trec, const InstDesc* __res
     const long long mtot = red[6 * NW + 4];
     if (mtot > 0) {
       const long long p1 = red[5 * NW + w] + pin, p0 = p1 - nv[0];
-      const double r1 = (double)p1 / (double)mtot, r0 = (double)p0 / (double)mtot;
+      // f(P) = floor(D r(P)) with r(P) = P / M as a product with 1 / M, exactly 1 at P = M: r stays
+      // monotone with r(0) = 0 and r(M) = 1, so the shares still telescope to D
+      const double inv = 1.0 / (double)mtot;
+      const double r1 = p1 >= mtot ? 1.0 : (double)p1 * inv, r0 = p0 >= mtot ? 1.0 : (double)p0 * inv;
 #pragma unroll
       for (int k = 0; k < 4; ++k) nv[k] += __double2ll_rd((double)Dk[k] * r1) - __double2ll_rd((double)Dk[k] * r0);
     } else if (t == 0) {  // no node mass to weigh by: the tile's first halo node takes it all
@@ -1170,6 +1174,8 @@ __device__ void traction_particle(const InstDesc* __restrict__ desc, const Contr
 #pragma unroll
   for (int a = 0; a < 3; ++a) x[a] = cur[(C_X + a) * cap + slot];
   const double s_m = D.s_mass, s_p = c.s_mom;
+  // unrolled axis and node loops: the stencil arrays stay in registers (no stack frame)
+#pragma unroll
   for (int axis = 0; axis < 3; ++axis) {
     const float ext = (float)D.extent[axis];
     float face;
@@ -1199,8 +1205,11 @@ __device__ void traction_particle(const InstDesc* __restrict__ desc, const Contr
     if (ns >= 0.0f) continue;
     const float wm = m * gax * dt;
     long long* dst = trac + (int64_t)(axis + (inward > 0.f ? 0 : 3)) * node_total;
+#pragma unroll
     for (int a = 0; a < 3; ++a)
+#pragma unroll
       for (int b = 0; b < 3; ++b)
+#pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
           int co[3] = {base[0] + a, base[1] + b, base[2] + cc};
           const int ca = co[axis];
@@ -1244,8 +1253,12 @@ __device__ __forceinline__ void reduce_tangential(float t[3], float reduction) {
 // AUDIT (energy audit, audit.rs:72-90): each CTA also sums the grid kinetic energy after the
 // stress deposit, after wall traction, with the gravity kick, and after the wall projection and
 // friction, into audit[4 * CTA + 0..3].
+// Registers for 4 CTAs per SM (64): the update waits on its node loads, so resident warps count
+// more than registers; the FP64 tallies live in shared memory and the next live pass's sums are
+// loaded while the current pass works (0.168 -> 0.112 ms on the 16.8M-particle slump against
+// 2 CTAs per SM at 84 registers, one pass in flight).
 template <bool AUDIT>
-__global__ void __launch_bounds__(GU_THREADS)
+__global__ void __launch_bounds__(GU_THREADS, 4)
     k_grid_update(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
                   const int* __restrict__ gcta_inst, long long* __restrict__ acc, long long* __restrict__ trac,
                   int64_t node_total, const uint32_t* __restrict__ blk_epoch, float4* __restrict__ vel,
@@ -1258,29 +1271,85 @@ __global__ void __launch_bounds__(GU_THREADS)
   const InstDesc& D = desc[inst];
   const int t = threadIdx.x;
   const int64_t nblk = (int64_t)D.nblk[0] * D.nblk[1] * D.nblk[2];
-  double wi0 = 0, wi1 = 0, wi2 = 0, proj = 0, fric = 0, tren = 0;
-  double e_stress = 0, e_trac = 0, e_grav = 0, e_walls = 0;
+  // this thread's FP64 tallies, kept in shared memory (volatile accesses) so that they hold no
+  // registers while the node loads are in flight
+  constexpr int NTAL = AUDIT ? 10 : 6;
+  __shared__ double tally[10 * GU_THREADS];  // the audit tallies have their own rows in both forms
+  volatile double& wi0 = tally[0 * GU_THREADS + t];
+  volatile double& wi1 = tally[1 * GU_THREADS + t];
+  volatile double& wi2 = tally[2 * GU_THREADS + t];
+  volatile double& proj = tally[3 * GU_THREADS + t];
+  volatile double& fric = tally[4 * GU_THREADS + t];
+  volatile double& tren = tally[5 * GU_THREADS + t];
+  volatile double& e_stress = tally[6 * GU_THREADS + t];
+  volatile double& e_trac = tally[7 * GU_THREADS + t];
+  volatile double& e_grav = tally[8 * GU_THREADS + t];
+  volatile double& e_walls = tally[9 * GU_THREADS + t];
+#pragma unroll
+  for (int k = 0; k < NTAL; ++k) tally[k * GU_THREADS + t] = 0.0;
   int fail = F_OK;
-  bool any_live = false;
-  // GU_PASSES passes of GU_BLOCKS_PER_CTA node blocks each; passes without a live block are skipped
+  // GU_PASSES passes of GU_BLOCKS_PER_CTA node blocks each.  The activity marks of all the
+  // passes are read up front (independent loads, one latency), and a pass whose block holds no
+  // mass in this attempt is skipped by its two warps alone: most CTAs of a sparse grid find no
+  // live block and leave after one round trip instead of one per pass.
+  const int64_t lblk0 = ((int64_t)(blockIdx.x - D.gcta_off) * GU_PASSES) * GU_BLOCKS_PER_CTA + t / 64;
+  uint32_t live_mask = 0;
+#pragma unroll
   for (int pass = 0; pass < GU_PASSES; ++pass) {
-    const int64_t lblk = ((blockIdx.x - D.gcta_off) * GU_PASSES + pass) * GU_BLOCKS_PER_CTA + t / 64;
-    bool live = lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch;
-    int ni = 0, nj = 0, nk = 0;
-    if (live) {
-      const int bk = (int)(lblk % D.nblk[2]), bj = (int)((lblk / D.nblk[2]) % D.nblk[1]),
-                bi = (int)(lblk / ((int64_t)D.nblk[2] * D.nblk[1]));
-      const int l = t % 64;
-      ni = bi * NB + l / 16;
-      nj = bj * NB + (l / 4) % 4;
-      nk = bk * NB + l % 4;
-      live = ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2];
+    const int64_t lblk = lblk0 + (int64_t)pass * GU_BLOCKS_PER_CTA;
+    if (lblk < nblk && blk_epoch[D.blk_off + lblk] == (uint32_t)c.epoch) live_mask |= 1u << pass;
+  }
+  const bool any_live = __syncthreads_or(live_mask != 0u) != 0;  // CTA-uniform
+  // The live passes run in order; each prefetches the next live pass's four sums while it works.
+  // Every node belongs to one thread and one pass, so the prefetch never reads a node that this
+  // kernel has already written.
+  const int l64 = t % 64;
+  auto node_of = [&](int pass, int& ni, int& nj, int& nk, int64_t& g) -> bool {
+    const int64_t lblk = lblk0 + (int64_t)pass * GU_BLOCKS_PER_CTA;
+    const int bk = (int)(lblk % D.nblk[2]), bj = (int)((lblk / D.nblk[2]) % D.nblk[1]),
+              bi = (int)(lblk / ((int64_t)D.nblk[2] * D.nblk[1]));
+    ni = bi * NB + l64 / 16;
+    nj = bj * NB + (l64 / 4) % 4;
+    nk = bk * NB + l64 % 4;
+    const bool in = ni < D.nodes[0] && nj < D.nodes[1] && nk < D.nodes[2];
+    g = in ? node_index(D, ni, nj, nk) : 0;
+    return in;
+  };
+  int pass = live_mask ? __ffs(live_mask) - 1 : GU_PASSES;
+  long long q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+  int64_t qg = 0;
+  bool ql = false;
+  if (pass < GU_PASSES) {
+    int qi, qj, qk;
+    ql = node_of(pass, qi, qj, qk, qg);
+    if (ql) {
+      q0 = acc[qg];
+      q1 = acc[node_total + qg];
+      q2 = acc[2 * node_total + qg];
+      q3 = acc[3 * node_total + qg];
     }
-    if (!__syncthreads_or(live ? 1 : 0)) continue;  // CTA-uniform
-    any_live = true;
+  }
+  while (pass < GU_PASSES) {
+    const bool live = ql;
+    const int this_pass = pass;
+    const int64_t g = qg;
+    const long long mf = q0, pf0 = q1, pf1 = q2, pf2 = q3;
+    const uint32_t rest = live_mask & ~((2u << pass) - 1u);
+    pass = rest ? __ffs(rest) - 1 : GU_PASSES;
+    if (pass < GU_PASSES) {
+      int qi, qj, qk;
+      ql = node_of(pass, qi, qj, qk, qg);
+      if (ql) {
+        q0 = acc[qg];
+        q1 = acc[node_total + qg];
+        q2 = acc[2 * node_total + qg];
+        q3 = acc[3 * node_total + qg];
+      }
+    }
     if (live) {
-      const int64_t g = node_index(D, ni, nj, nk);
-      const long long mf = acc[g];
+      int ni, nj, nk;
+      int64_t g_unused;
+      node_of(this_pass, ni, nj, nk, g_unused);
       if (mf <= 0) {
         vel[g] = make_float4(0.f, 0.f, 0.f, 0.f);
         acc[g] = 0;
@@ -1290,8 +1359,7 @@ __global__ void __launch_bounds__(GU_THREADS)
       } else {
         const double s_m = D.s_mass, s_p = c.s_mom;
         const double md = (double)mf / s_m;
-        double p[3] = {(double)acc[node_total + g] / s_p, (double)acc[2 * node_total + g] / s_p,
-                       (double)acc[3 * node_total + g] / s_p};
+        double p[3] = {(double)pf0 / s_p, (double)pf1 / s_p, (double)pf2 / s_p};
         acc[g] = 0;
         acc[node_total + g] = 0;
         acc[2 * node_total + g] = 0;
@@ -1420,22 +1488,15 @@ __global__ void __launch_bounds__(GU_THREADS)
     rv[RK - 1] = e_walls;
   }
   block_reduce_multi_to0<GU_THREADS, RK>(rv, 1u << 6, shd);  // kernel end: thread 0 writes
-  wi0 = rv[0];
-  wi1 = rv[1];
-  wi2 = rv[2];
-  proj = rv[3];
-  fric = rv[4];
-  tren = rv[5];
-  fail = (int)rv[6];
   if (t == 0) {
     GridPartial& P = part[blockIdx.x];
-    P.wall_impulse[0] = wi0;
-    P.wall_impulse[1] = wi1;
-    P.wall_impulse[2] = wi2;
-    P.proj = proj;
-    P.fric = fric;
-    P.trac = tren;
-    P.fail = fail;
+    P.wall_impulse[0] = rv[0];
+    P.wall_impulse[1] = rv[1];
+    P.wall_impulse[2] = rv[2];
+    P.proj = rv[3];
+    P.fric = rv[4];
+    P.trac = rv[5];
+    P.fail = (int)rv[6];
     if (AUDIT)
       for (int k = 0; k < 4; ++k) audit[4 * (int64_t)blockIdx.x + k] = rv[RK - 4 + k];
   }
