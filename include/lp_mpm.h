@@ -305,6 +305,11 @@ lp_status lp_sim_kernel_times(lp_sim* sim, int32_t steps, double* ms, char* name
 lp_status lp_sim_g2p_return_share(lp_sim* sim, int32_t steps, double* share);
 /* Capture run_substeps into a CUDA graph of `steps` attempts (0 disables graphs). */
 lp_status lp_sim_use_graph(lp_sim* sim, int32_t steps);
+/* Build that graph now (capture and instantiate, no launch) if the launch shape asks for one and
+ * it is not built, so that the next run_substeps pays no capture.  Changing the launch shape,
+ * the stream, the warm start or the Newton log drops the graph again.  No counterpart in the
+ * reference. */
+lp_status lp_sim_prepare(lp_sim* sim);
 
 /* ---------------- batched ensembles (extension) ---------------- */
 lp_status lp_batch_create(const lp_fixture_spec* specs, int32_t count, lp_batch** out);
@@ -322,6 +327,8 @@ lp_status lp_batch_set_warm_start(lp_batch* b, const float* weights, int32_t nwe
 /* lp_sim_warm_table for member `instance` of a batch. */
 lp_status lp_batch_warm_table(lp_batch* b, int32_t instance, float* out, int32_t capacity, double* dt);
 lp_status lp_batch_use_graph(lp_batch* b, int32_t steps);
+/* lp_sim_prepare for a whole batch. */
+lp_status lp_batch_prepare(lp_batch* b);
 /* lp_sim_kernel_times for a whole batch: each kernel's mean duration over `steps` attempts of
  * every instance at once.  No counterpart in the reference. */
 lp_status lp_batch_kernel_times(lp_batch* b, int32_t steps, double* ms, char* names, int32_t capacity,

@@ -893,26 +893,35 @@ lp_status ensemble_create(const lp_fixture_spec* specs, int count, Ensemble& E) 
   return push_ctrl(E);
 }
 
+// Capture and instantiate the graph of G attempts when the launch shape asks for one and none is
+// built; launches nothing.  The kernel launches counted while capturing are taken back, so that
+// each replay counts its own.
+lp_status ensure_graph(Ensemble& E) {
+  const int G = E.graph_steps;
+  if (G <= 1 || E.graph_exec) return LP_OK;
+  const uint64_t before = lp::kernel_launch_count();
+  cudaStream_t cs = E.stream;
+  CUDA_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int kernels = 0;
+  for (int s = 0; s < G; ++s) kernels += lp::launch_attempt(E.A, cs);
+  cudaGraph_t g = nullptr;
+  CUDA_CK(cudaStreamEndCapture(cs, &g));
+  E.graph = g;
+  CUDA_CK(cudaGraphInstantiate(&E.graph_exec, g, 0));
+  E.graph_kernels = kernels;
+  lp::add_kernel_launches(before - lp::kernel_launch_count());  // unsigned wrap: subtracts the capture's count
+  return LP_OK;
+}
+
 // Queue `steps` attempts: with a graph length G > 1, floor(steps / G) replays of a CUDA graph of G
-// attempts (captured on first use) and the remainder as plain launches.
+// attempts (captured on first use unless ensure_graph built it earlier) and the remainder as plain
+// launches.
 lp_status run_attempts(Ensemble& E, int steps) {
   if (steps <= 0) return LP_OK;
   const int G = E.graph_steps;
   if (G > 1 && steps >= G) {
-    if (!E.graph_exec) {
-      cudaStream_t cs = E.stream;
-      CUDA_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-      int kernels = 0;
-      for (int s = 0; s < G; ++s) kernels += lp::launch_attempt(E.A, cs);
-      cudaGraph_t g = nullptr;
-      CUDA_CK(cudaStreamEndCapture(cs, &g));
-      E.graph = g;
-      CUDA_CK(cudaGraphInstantiate(&E.graph_exec, g, 0));
-      // kernels counted while capturing correspond to the first replay below
-      E.graph_kernels = kernels;
-      CUDA_CK(cudaGraphLaunch(E.graph_exec, E.stream));
-      steps -= G;
-    }
+    const lp_status st = ensure_graph(E);
+    if (st != LP_OK) return st;
     for (; steps >= G; steps -= G) {
       CUDA_CK(cudaGraphLaunch(E.graph_exec, E.stream));
       lp::add_kernel_launches((uint64_t)E.graph_kernels);
@@ -2246,6 +2255,8 @@ lp_status lp_sim_use_graph(lp_sim* sim, int32_t steps) {
   return LP_OK;
 }
 
+lp_status lp_sim_prepare(lp_sim* sim) { return ensure_graph(sim->E); }
+
 lp_status lp_sim_enable_newton_log(lp_sim* sim, int64_t capacity) {
   Ensemble& E = sim->E;
   E.invalidate_graph();
@@ -2404,6 +2415,7 @@ lp_status lp_batch_use_graph(lp_batch* b, int32_t steps) {
   b->E.graph_steps = steps > 0 ? steps : 0;
   return LP_OK;
 }
+lp_status lp_batch_prepare(lp_batch* b) { return ensure_graph(b->E); }
 lp_status lp_sim_g2p_return_share(lp_sim* sim, int32_t steps, double* share) {
   Ensemble& E = sim->E;
   if (!share || steps < 1) return set_error(LP_INVALID, "need steps >= 1 and an output");

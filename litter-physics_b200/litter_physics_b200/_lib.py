@@ -99,6 +99,7 @@ def lib():
         "lp_sim_set_warm_start": ([P, F, I32, I32], I32),
         "lp_sim_warm_table": ([P, F, I32, D], I32),
         "lp_sim_use_graph": ([P, I32], I32),
+        "lp_sim_prepare": ([P], I32),
         "lp_sim_grid_totals": ([P, C.c_double, D], I32),
         "lp_sim_grid_dump": ([P, C.c_double, D, D, D, I64], I32),
         "lp_sim_kernel_times": ([P, I32, D, C.c_char_p, I32, C.POINTER(I32)], I32),
@@ -117,6 +118,7 @@ def lib():
         "lp_batch_set_warm_start": ([P, F, I32, I32], I32),
         "lp_batch_warm_table": ([P, I32, F, I32, D], I32),
         "lp_batch_use_graph": ([P, I32], I32),
+        "lp_batch_prepare": ([P], I32),
         "lp_batch_autotune": ([P, I32, C.c_char_p, C.c_size_t], I32),
         "lp_sim_autotune": ([P, I32, C.c_char_p, C.c_size_t], I32),
         "lp_sim_g2p_return_share": ([P, I32, D], I32),

@@ -96,6 +96,10 @@ class Simulation:
     def use_graph(self, steps: int) -> None:
         check(lib().lp_sim_use_graph(self._h, int(steps)))
 
+    def prepare(self) -> None:
+        """Build the launch shape's CUDA graph now (no launch), so run_substeps pays no capture."""
+        check(lib().lp_sim_prepare(self._h))
+
     def autotune(self, trial_steps: int = 16) -> str:
         """Pick the launch shape on the live simulation (advances it); returns the report."""
         buf = C.create_string_buffer(8192)
@@ -406,6 +410,10 @@ class Batch:
 
     def use_graph(self, steps: int) -> None:
         check(lib().lp_batch_use_graph(self._h, int(steps)))
+
+    def prepare(self) -> None:
+        """`Simulation.prepare` for the whole batch."""
+        check(lib().lp_batch_prepare(self._h))
 
     def autotune(self, trial_steps: int = 16) -> str:
         """Pick the launch shape on the live batch (advances it); returns the tuner's report."""

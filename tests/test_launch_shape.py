@@ -183,3 +183,30 @@ def test_mixed_material_batch_matches_single_kind_runs():
             assert np.array_equal(pb[k], ps[k]), (i, k)
         one.close()
     b.close()
+
+
+def test_prepared_graph_runs_like_the_graph_captured_on_first_use():
+    """lp_batch_prepare builds the attempt graph without launching anything: the state, ledgers
+    and counters after a prepared run equal those of a run whose graph is captured on first use,
+    and both count the same kernel launches."""
+    from litter_physics_b200 import _lib
+    from litter_physics_b200.sim import Batch
+
+    results, launches = [], []
+    for prepare in (False, True):
+        b = Batch(uneven_batch())
+        b.set_launch_shape(graph_attempts=4)
+        if prepare:
+            b.prepare()
+            b.sync()
+            assert b.counters(0).step_count == 0  # nothing ran
+            b.prepare()  # already built: a no-op
+        l0 = _lib.kernel_launches()
+        b.run_substeps(10)
+        b.sync()
+        launches.append(_lib.kernel_launches() - l0)
+        results.append([(by_id(b.particles(i))["position"].tobytes(), bytes(b.ledger(i)), b.counters(i).step_count)
+                        for i in range(len(b.specs))])
+        b.close()
+    assert results[0] == results[1]
+    assert launches[0] == launches[1] > 0
