@@ -1139,27 +1139,36 @@ __global__ void __launch_bounds__(P2G_THREADS, 2)
 }
 
 // ============================================================== wall traction
-__device__ void traction_particle(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
-                                  const int* __restrict__ pcta_inst, const float* __restrict__ st0,
-                                  const float* __restrict__ st1, int64_t cap, int64_t slot,
-                                  const long long* __restrict__ acc, long long* __restrict__ trac,
-                                  int64_t node_total);
-// One thread per particle within half a cell of a face (listed while binning).
-__global__ void k_traction(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
-                           const int* __restrict__ pcta_inst, const float* __restrict__ st0,
-                           const float* __restrict__ st1, int64_t cap, const uint32_t* __restrict__ nw_list,
-                           const uint32_t* __restrict__ nw_count, const long long* __restrict__ acc,
-                           long long* __restrict__ trac, int64_t node_total) {
-  const uint32_t n = *nw_count;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    traction_particle(desc, ctrl, pcta_inst, st0, st1, cap, nw_list[i], acc, trac, node_total);
+__device__ __forceinline__ void traction_particle(const InstDesc* __restrict__ desc,
+                                                  const Control* __restrict__ ctrl,
+                                                  const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+                                                  const float* __restrict__ st1, int64_t cap, int64_t slot, int row,
+                                                  const long long* __restrict__ acc, long long* __restrict__ trac,
+                                                  int64_t node_total);
+// Nine threads per particle within half a cell of a face (listed while binning): thread `row`
+// of a particle takes the stencil row (a, b) = (row / 3, row % 3) of each face image, three
+// nodes, and issues the node loads of all three before it tests any of them.  A particle's 27
+// node reads thus overlap instead of running as one thread's chain of dependent loads.  The
+// reactions are int64 sums, so the split changes no result.
+constexpr int TRACTION_ROWS = 9, TRACTION_THREADS = 128, TRACTION_CTAS_PER_SM = 6;  // one wave at 78 registers
+__global__ void __launch_bounds__(TRACTION_THREADS)
+    k_traction(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
+               const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+               const float* __restrict__ st1, int64_t cap, const uint32_t* __restrict__ nw_list,
+               const uint32_t* __restrict__ nw_count, const long long* __restrict__ acc,
+               long long* __restrict__ trac, int64_t node_total) {
+  const uint64_t work = (uint64_t)*nw_count * TRACTION_ROWS;
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < work; g += (uint64_t)gridDim.x * blockDim.x)
+    traction_particle(desc, ctrl, pcta_inst, st0, st1, cap, nw_list[g / TRACTION_ROWS], (int)(g % TRACTION_ROWS), acc,
+                      trac, node_total);
 }
 
-__device__ void traction_particle(const InstDesc* __restrict__ desc, const Control* __restrict__ ctrl,
-                                  const int* __restrict__ pcta_inst, const float* __restrict__ st0,
-                                  const float* __restrict__ st1, int64_t cap, int64_t slot,
-                                  const long long* __restrict__ acc, long long* __restrict__ trac,
-                                  int64_t node_total) {
+__device__ __forceinline__ void traction_particle(const InstDesc* __restrict__ desc,
+                                                  const Control* __restrict__ ctrl,
+                                                  const int* __restrict__ pcta_inst, const float* __restrict__ st0,
+                                                  const float* __restrict__ st1, int64_t cap, int64_t slot, int row,
+                                                  const long long* __restrict__ acc, long long* __restrict__ trac,
+                                                  int64_t node_total) {
   const int inst = pcta_inst[slot / G2P_THREADS];
   const Control& c = ctrl[inst];
   if (!c.active) return;
@@ -1205,34 +1214,40 @@ __device__ void traction_particle(const InstDesc* __restrict__ desc, const Contr
     if (ns >= 0.0f) continue;
     const float wm = m * gax * dt;
     long long* dst = trac + (int64_t)(axis + (inward > 0.f ? 0 : 3)) * node_total;
+    // this thread's row (a, b): the three nodes' loads first, then their tests
+    const int a = row / 3, b = row % 3;
+    const int c0 = base[0] + a, c1 = base[1] + b;
+    const float wab = (a == 0 ? w[0][0] : (a == 1 ? w[0][1] : w[0][2])) * (b == 0 ? w[1][0] : (b == 1 ? w[1][1] : w[1][2]));
+    long long pmf[3], pmo[3], tmf[3];
+    int64_t tix[3];
+    bool use[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+    for (int cc = 0; cc < 3; ++cc) {
+      const int c2 = base[2] + cc;
+      const int ca = axis == 0 ? c0 : (axis == 1 ? c1 : c2);
+      use[cc] = !(ca <= 1 || ca > D.cells[axis]) && wab * w[2][cc] != 0.0f;
+      const int64_t pi = node_index(D, axis == 0 ? plane : c0, axis == 1 ? plane : c1, axis == 2 ? plane : c2);
+      tix[cc] = node_index(D, c0, c1, c2);
+      pmf[cc] = use[cc] ? acc[pi] : 0;
+      pmo[cc] = use[cc] ? acc[(1 + axis) * node_total + pi] : 0;
+      tmf[cc] = use[cc] ? acc[tix[cc]] : 0;
+    }
 #pragma unroll
-      for (int b = 0; b < 3; ++b)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          int co[3] = {base[0] + a, base[1] + b, base[2] + cc};
-          const int ca = co[axis];
-          if (ca <= 1 || ca > D.cells[axis]) continue;
-          const float wt = w[0][a] * w[1][b] * w[2][cc];
-          if (wt == 0.0f) continue;
-          int pc[3] = {co[0], co[1], co[2]};
-          pc[axis] = plane;
-          const int64_t pi = node_index(D, pc[0], pc[1], pc[2]);
-          const long long pmf = acc[pi];
-          if (pmf <= 0) continue;
-          const float pm = (float)((double)pmf / s_m);
-          const float pp = (float)((double)acc[(1 + axis) * node_total + pi] / s_p);
-          const float trial = pp / pm + gax * dt;
-          if (trial * inward >= 0.0f) continue;
-          const int o = axis == 0 ? a : (axis == 1 ? b : cc);
-          const float dist = d[axis][o];
-          const float reaction = (ns * dist * force_scale + wm) * wt * inward;
-          if (!(reaction > 0.0f)) continue;
-          const int64_t ti = node_index(D, co[0], co[1], co[2]);
-          if (acc[ti] <= 0) continue;
-          atomic_add_ll(dst + ti, to_fixed((double)reaction, s_p));
-        }
+    for (int cc = 0; cc < 3; ++cc) {
+      if (!use[cc] || pmf[cc] <= 0) continue;
+      const float wt = wab * w[2][cc];
+      const float pm = (float)((double)pmf[cc] / s_m);
+      const float pp = (float)((double)pmo[cc] / s_p);
+      const float trial = pp / pm + gax * dt;
+      if (trial * inward >= 0.0f) continue;
+      const int o = axis == 0 ? a : (axis == 1 ? b : cc);
+      const float dist = axis == 0 ? (o == 0 ? d[0][0] : (o == 1 ? d[0][1] : d[0][2]))
+                                   : (axis == 1 ? (o == 0 ? d[1][0] : (o == 1 ? d[1][1] : d[1][2])) : d[2][cc]);
+      const float reaction = (ns * dist * force_scale + wm) * wt * inward;
+      if (!(reaction > 0.0f)) continue;
+      if (tmf[cc] <= 0) continue;
+      atomic_add_ll(dst + tix[cc], to_fixed((double)reaction, s_p));
+    }
   }
 }
 
@@ -3511,7 +3526,7 @@ static int attempt_sequence(const DeviceArrays& A, cudaStream_t s, cudaEvent_t* 
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
   launch_tiles_p2g(A, s, 0, ev, n);
-  k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
+  k_traction<<<(unsigned)(g_sms * TRACTION_CTAS_PER_SM), TRACTION_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
                                      A.acc, A.trac, A.node_total);
   ++n;
   if (ev) cudaEventRecord(ev[n], s);
@@ -3609,7 +3624,7 @@ int launch_p2g_traction(const DeviceArrays& A, cudaStream_t s) {
     int nt = 0;
     launch_tiles_p2g(A, s, 0, nullptr, nt);
   }
-  k_traction<<<148 * 4, 128, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
+  k_traction<<<(unsigned)(g_sms * TRACTION_CTAS_PER_SM), TRACTION_THREADS, 0, s>>>(A.desc, A.ctrl, A.pcta_inst, A.st[0], A.st[1], A.cap, A.nw_list, A.nw_count,
                                      A.acc, A.trac, A.node_total);
   g_launches += 9;
   return 9;
